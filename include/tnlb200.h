@@ -1,0 +1,221 @@
+/*
+ * tnlb200.h -- C ABI of libtnlb200.so: TNL's sparse segments formats, the
+ * sparse matrix-vector product on them and the Krylov solvers built on it,
+ * implemented for NVIDIA B200 (sm_100a).
+ *
+ * Conventions
+ *  - Every entry point returns tnlb_status (0 = success) and never throws.
+ *    tnlb_last_error() gives a message for the calling host thread.
+ *  - Arrays named d_* are DEVICE pointers owned by the caller (values,
+ *    column indexes, vectors); the library never frees them.  Arrays named
+ *    h_* are host pointers.  Segment metadata (row pointers, slice offsets,
+ *    chunk maps, permutations, block descriptors) lives in an opaque
+ *    tnlb_segments handle created and destroyed here.
+ *  - Index type is int32 (TNL's `int` Index), sizes of storage int64.
+ *  - Work is enqueued on the given stream (0 = the calling thread's default
+ *    stream) and is asynchronous unless the entry point says otherwise.  The
+ *    reference's vectorProduct is synchronous on return
+ *    (Algorithms/Segments/detail/ReducingOperations_CSR.h:327); the C++
+ *    drop-in headers (include/tnlb/) add that synchronisation.
+ *  - Every citation below is a path inside the reference project TNL 0.4.0.
+ */
+#ifndef TNLB200_H
+#define TNLB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* tnlb_stream; /* == cudaStream_t */
+
+/* Status codes.  The C++ layer maps them onto the reference's exceptions:
+ * INVALID_ARGUMENT -> std::invalid_argument (Matrices/SparseMatrixBase.hpp:279-282),
+ * OVERFLOW -> std::overflow_error (Algorithms/Segments/Ellpack.hpp:92-95),
+ * CUDA -> Exceptions::BackendRuntimeError (Backend/Macros.h:14-24),
+ * NOT_IMPLEMENTED -> Exceptions::NotImplementedError,
+ * BREAKDOWN -> the `throw 1` of GMRES::update (Solvers/Linear/GMRES.hpp:657-667),
+ * TIMEOUT -> a bounded device-side wait gave up (no reference counterpart). */
+typedef enum {
+   TNLB_OK = 0,
+   TNLB_ERR_INVALID_ARGUMENT = 1,
+   TNLB_ERR_OVERFLOW = 2,
+   TNLB_ERR_CUDA = 3,
+   TNLB_ERR_NOT_IMPLEMENTED = 4,
+   TNLB_ERR_BREAKDOWN = 5,
+   TNLB_ERR_TIMEOUT = 6,
+   TNLB_ERR_OUT_OF_MEMORY = 7
+} tnlb_status;
+
+/* Real types of values and vectors. */
+typedef enum { TNLB_F32 = 0, TNLB_F64 = 1 } tnlb_real;
+
+/* Segment formats: Algorithms/Segments/{CSR,Ellpack,SlicedEllpack,
+ * ChunkedEllpack,BiEllpack,AdaptiveCSR}.h. */
+typedef enum {
+   TNLB_CSR = 0,
+   TNLB_ELLPACK = 1,
+   TNLB_SLICED_ELLPACK = 2,
+   TNLB_CHUNKED_ELLPACK = 3,
+   TNLB_BIELLPACK = 4,
+   TNLB_ADAPTIVE_CSR = 5
+} tnlb_format;
+
+/* ElementsOrganization (Algorithms/Segments/ElementsOrganization.h:15-32);
+ * the GPU default of the reference is column-major. */
+typedef enum { TNLB_COLUMN_MAJOR = 0, TNLB_ROW_MAJOR = 1 } tnlb_organization;
+
+/* SpMV kernel selection, mirroring Segments::LaunchConfiguration
+ * (Algorithms/Segments/LaunchConfiguration.h:18-86) and the legacy kernel
+ * classes of Algorithms/SegmentsReductionKernels (CSRScalarKernel,
+ * CSRVectorKernel, CSRLightKernel, CSRAdaptiveKernel, ...).
+ *  TNLB_KERNEL_DEFAULT   -- the tuned kernel of the format (for CSR the
+ *                           nnz-balanced tile kernel);
+ *  TNLB_KERNEL_SCALAR    -- one thread per segment (Fixed, TPS 1);
+ *  TNLB_KERNEL_VECTOR    -- `threads_per_segment` lanes per segment
+ *                           (Fixed TPS 2..32, Warp = 32, 64/128 multi-warp);
+ *  TNLB_KERNEL_LIGHT     -- TPS picked from the mean segment length as in
+ *                           LaunchConfigurationSetter_LightCSR.h:30-58;
+ *  TNLB_KERNEL_ADAPTIVE  -- the AdaptiveCSR block-descriptor kernel (CSR and
+ *                           AdaptiveCSR only).
+ * Formats other than CSR accept DEFAULT and, where the reference offers a
+ * TPS choice (Ellpack, SlicedEllpack), VECTOR. */
+typedef enum {
+   TNLB_KERNEL_DEFAULT = 0,
+   TNLB_KERNEL_SCALAR = 1,
+   TNLB_KERNEL_VECTOR = 2,
+   TNLB_KERNEL_LIGHT = 3,
+   TNLB_KERNEL_ADAPTIVE = 4
+} tnlb_kernel;
+
+typedef struct tnlb_segments tnlb_segments;
+
+/* Sizes of a built segments object (mirrors getSegmentCount, getElementCount,
+ * getStorageSize and the per-format metadata sizes). */
+typedef struct {
+   int32_t format;           /* tnlb_format */
+   int32_t organization;     /* tnlb_organization */
+   int32_t segments;         /* getSegmentCount() */
+   int32_t reserved0;
+   int64_t elements;         /* getElementCount(): sum of segment sizes */
+   int64_t storage;          /* getStorageSize(): slots incl. padding */
+   int32_t segment_size;     /* Ellpack: getSegmentSize() */
+   int32_t aligned_size;     /* Ellpack: getAlignedSize() */
+   int32_t slices;           /* SlicedEllpack slices / ChunkedEllpack numberOfSlices / BiEllpack strips */
+   int32_t chunks_in_slice;  /* ChunkedEllpack: 256 */
+   int64_t acsr_blocks[6];   /* AdaptiveCSR: descriptor count per value-size log 0..5 */
+} tnlb_segments_info;
+
+/* Metadata arrays that can be read back (tnlb_segments_read_metadata). */
+typedef enum {
+   TNLB_META_OFFSETS = 0,              /* CSR / AdaptiveCSR: int32[n+1] */
+   TNLB_META_SLICE_OFFSETS = 1,        /* SlicedEllpack: int32[slices+1] */
+   TNLB_META_SLICE_SEGMENT_SIZES = 2,  /* SlicedEllpack: int32[slices] */
+   TNLB_META_CH_SLICE_SIZE = 3,        /* ChunkedEllpack slices[].size: int32[slices] */
+   TNLB_META_CH_SLICE_CHUNK_SIZE = 4,  /* slices[].chunkSize */
+   TNLB_META_CH_SLICE_FIRST = 5,       /* slices[].firstSegment */
+   TNLB_META_CH_SLICE_POINTER = 6,     /* slices[].pointer */
+   TNLB_META_CH_SEGMENT_TO_CHUNK = 7,  /* int32[n] */
+   TNLB_META_CH_SEGMENT_TO_SLICE = 8,  /* int32[n] */
+   TNLB_META_CH_SEGMENT_POINTERS = 9,  /* int32[n+1] */
+   TNLB_META_CH_CHUNKS_TO_SEGMENTS = 10, /* int32[slices*chunks_in_slice] */
+   TNLB_META_BI_PERMUTATION = 11,      /* BiEllpack: int32[n] */
+   TNLB_META_BI_GROUP_POINTERS = 12    /* BiEllpack: int32[strips*6+1] */
+} tnlb_metadata;
+
+/* AdaptiveCSR block descriptor (non-union layout of
+ * Algorithms/Segments/detail/CSRAdaptiveKernelBlockDescriptor.h:134-199). */
+typedef struct {
+   uint8_t type; /* LONG = 0, STREAM = 1, VECTOR = 2 */
+   uint8_t warp_idx;
+   uint8_t warps_count;
+   uint8_t reserved;
+   int32_t first_segment;
+   int32_t block_size;        /* elements covered (STREAM/VECTOR) */
+   int32_t segments_in_block; /* STREAM/VECTOR */
+} tnlb_acsr_block;
+
+/* ------------------------------------------------------------ library */
+
+/* Message of the last failed call on this host thread ("" if none). */
+const char* tnlb_last_error(void);
+/* Library version string. */
+const char* tnlb_version(void);
+
+/* ------------------------------------------------------------ segments */
+
+/* Build a segments object from DEVICE segment sizes (row capacities) on the
+ * GPU.  Replaces Segments::setSegmentsSizes of every format:
+ * CSR.hpp:87-103, Ellpack.hpp:74-96, SlicedEllpack.hpp:116-150 (slice 32),
+ * ChunkedEllpack.hpp:158-380 (256 chunks per slice, desired chunk size 16),
+ * BiEllpack.hpp:106-342 (strips of 32), AdaptiveCSR.hpp:104-230.  Metadata
+ * is bit-identical to the reference's Host builders.  Blocks until built.
+ * Ellpack storage beyond int32 -> TNLB_ERR_OVERFLOW (Ellpack.hpp:92-95). */
+tnlb_status tnlb_segments_create(tnlb_format format, tnlb_organization organization, const int32_t* d_sizes,
+                                 int32_t segments, tnlb_stream stream, tnlb_segments** out);
+
+/* Release a segments object (Segments::reset). Accepts NULL. */
+tnlb_status tnlb_segments_destroy(tnlb_segments* seg);
+
+/* Sizes of a segments object. */
+tnlb_status tnlb_segments_get_info(const tnlb_segments* seg, tnlb_segments_info* info);
+
+/* Copy one metadata array to host memory (for inspection and the bit-exact
+ * checks against the reference's builders); `count` is the capacity of h_out
+ * in int32 elements.  Blocks until copied. */
+tnlb_status tnlb_segments_read_metadata(const tnlb_segments* seg, tnlb_metadata which, int32_t* h_out, int64_t count);
+
+/* Copy the AdaptiveCSR descriptors of one value-size log (0..5: 1..32 B) to
+ * host memory.  Blocks until copied. */
+tnlb_status tnlb_segments_read_acsr_blocks(const tnlb_segments* seg, int32_t size_log, tnlb_acsr_block* h_out,
+                                           int64_t count);
+
+/* Global index of (segment, local) -- Segments::getGlobalIndex
+ * (EllpackBase.hpp:110-117, SlicedEllpackBase.hpp:121-145,
+ * detail/ChunkedEllpack.h:86-113, detail/BiEllpack.h:134-163).  Computes a
+ * DEVICE array d_global[i] for the pairs (d_segment[i], d_local[i]). */
+tnlb_status tnlb_segments_global_index(const tnlb_segments* seg, const int32_t* d_segment, const int32_t* d_local,
+                                       int64_t count, int64_t* d_global, tnlb_stream stream);
+
+/* ------------------------------------------------------------ matrices */
+
+/* Fill a matrix stored in `seg` from a CSR matrix on the device: the
+ * cross-format SparseMatrix::operator= (SparseMatrix.hpp:626-629 ->
+ * copySparseToSparseMatrix, Matrices/SparseOperations.hpp:106-186).
+ * Target columns start as the padding index -1 and values as 0; source
+ * elements with value 0 or column -1 are skipped, the rest are packed into
+ * local slots 0,1,2,... of their row.  d_cols/d_values have
+ * info.storage slots.  The segment sizes of `seg` must be >= the source
+ * row lengths. */
+tnlb_status tnlb_matrix_fill_from_csr(const tnlb_segments* seg, tnlb_real real, const int32_t* d_rowptr,
+                                      const int32_t* d_src_cols, const void* d_src_values, int32_t* d_cols,
+                                      void* d_values, tnlb_stream stream);
+
+/* y[begin:end] = alpha * (A x)[begin:end] + beta * y[begin:end]
+ * -- SparseMatrixBase::vectorProduct (Matrices/SparseMatrixBase.h:1020-1035,
+ * SparseMatrixBase.hpp:270-393) for a general (non-symmetric) matrix.
+ * Padding slots (column -1) contribute 0; beta == 0 does not read y; end == 0
+ * means all rows.  `kernel` and `threads_per_segment` select the kernel as in
+ * LaunchConfiguration (threads_per_segment: power of two, 0 = automatic).
+ * x has `columns` entries, y has info.segments entries. */
+tnlb_status tnlb_spmv(const tnlb_segments* seg, tnlb_real real, const int32_t* d_cols, const void* d_values,
+                      int32_t columns, const void* d_x, void* d_y, double alpha, double beta, int32_t begin,
+                      int32_t end, tnlb_kernel kernel, int32_t threads_per_segment, tnlb_stream stream);
+
+/* Number of CUDA kernels the most recent tnlb_spmv on this host thread
+ * enqueued (for launch accounting). */
+int32_t tnlb_spmv_last_launch_count(void);
+
+/* ------------------------------------------------------------ vectors */
+
+/* Dot product (a, b) into a DEVICE scalar -- Containers/Expressions/
+ * ExpressionTemplates.h:372-387 (the reference copies it to the host). */
+tnlb_status tnlb_dot(tnlb_real real, int64_t n, const void* d_a, const void* d_b, double* d_result, tnlb_stream stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TNLB200_H */

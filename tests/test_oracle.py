@@ -1,0 +1,179 @@
+"""The oracle (oracle/tnl_oracle.c) pinned against the reference.
+
+CPU only.  Checks the C restatement against
+  * the known-answer vectors of the reference's unit tests,
+  * the golden fixtures produced by the reference itself (always), and
+  * the reference compiled here from its headers (oracle/_ref), when built.
+"""
+import hashlib
+
+import numpy as np
+import pytest
+
+from helpers import FORMATS
+from known_answers import cases as known_cases
+from tnl_b200 import generators as g
+
+KINDS = ["CSR", "Ellpack", "SlicedEllpack", "ChunkedEllpack", "BiEllpack"]
+
+
+@pytest.mark.parametrize("fmt", list(FORMATS))
+@pytest.mark.parametrize("colmajor", [True, False])
+def test_known_answers(oracle, fmt, colmajor):
+    for name, rp, c, v, nc, x, y0, expected in known_cases():
+        seg = oracle.build(FORMATS[fmt], np.diff(rp), colmajor=colmajor)
+        oc, ov = oracle.fill(seg, rp, c, v)
+        y = oracle.spmv(seg, oc, ov, x, y0)
+        assert np.array_equal(y, expected), (name, fmt)
+
+
+@pytest.mark.parametrize("kname", KINDS)
+def test_builders_match_golden(oracle, golden, kname):
+    for case in golden.size_cases():
+        sizes = golden.get(f"sizes/{case}")
+        key = f"{case}/{kname}"
+        if key not in golden.meta["builders"]:
+            continue
+        if golden.meta["builders"][key] == "overflow":
+            with pytest.raises(OverflowError):
+                oracle.build(FORMATS[kname], sizes)
+            continue
+        seg = oracle.build(FORMATS[kname], sizes)
+        for k, v in golden.meta["builders"][key].items():
+            if k == "storage":
+                assert seg.storage == v, (case, kname)
+            else:
+                assert seg.meta[k] == v, (case, kname, k)
+        prefix = f"build/{case}/{kname}/"
+        for name in golden.arrays.files:
+            if name.startswith(prefix):
+                assert np.array_equal(np.asarray(seg.meta[name[len(prefix):]]), golden.get(name)), (case, kname, name)
+
+
+def test_acsr_blocks_match_golden(oracle, golden):
+    checked = 0
+    for case in golden.size_cases():
+        sizes = golden.get(f"sizes/{case}")
+        off = np.zeros(len(sizes) + 1, np.int32)
+        off[1:] = np.cumsum(sizes)
+        for sl in range(6):
+            if golden.meta["acsr"].get(f"{case}/{sl}") in (None, "unavailable"):
+                continue
+            b = oracle.acsr_blocks(off, sl)
+            for k in b:
+                assert np.array_equal(b[k], golden.get(f"acsr/{case}/{sl}/{k}")), (case, sl, k)
+            checked += 1
+    assert checked > 20
+
+
+def _digest(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+@pytest.mark.parametrize("mname", ["powerlaw2000", "laplacian32"])
+def test_fill_and_spmv_match_golden(oracle, golden, mname):
+    rp = golden.get(f"mat/{mname}/rowptr")
+    cols = golden.get(f"mat/{mname}/cols")
+    vals = golden.get(f"mat/{mname}/vals")
+    x = golden.get(f"mat/{mname}/x")
+    for kname, kind in FORMATS.items():
+        for cm in (True, False):
+            for real in (np.float64, np.float32):
+                tag = f"{mname}/{kname}/{'col' if cm else 'row'}/{np.dtype(real).name}"
+                seg = oracle.build(kind, np.diff(rp), colmajor=cm)
+                oc, ov = oracle.fill(seg, rp, cols, vals.astype(real))
+                ref = golden.meta["fill"][tag]
+                assert seg.storage == ref["storage"], tag
+                assert _digest(oc) == ref["cols"] and _digest(ov) == ref["vals"], tag
+        seg = oracle.build(kind, np.diff(rp), colmajor=False)
+        oc, ov = oracle.fill(seg, rp, cols, vals)
+        y = oracle.spmv(seg, oc, ov, x)
+        # same per-row summation order as the Host reference -> bit-identical
+        assert np.array_equal(y, golden.get(f"spmv/{mname}/{kname}")), (mname, kname)
+
+
+def test_builders_match_reference_random(oracle, reference):
+    rng = np.random.default_rng(7)
+    for trial in range(25):
+        n = int(rng.integers(1, 3000))
+        mode = trial % 3
+        if mode == 0:
+            sizes = rng.integers(0, 64, n)
+        elif mode == 1:
+            sizes = g.zipf_lengths(n, float(rng.uniform(1.2, 2.5)), 4096, int(rng.integers(1 << 30)))
+        else:
+            sizes = np.where(rng.random(n) < 0.5, 0, rng.integers(0, 600, n))
+        sizes = sizes.astype(np.int32)
+        for kname in KINDS:
+            r = reference.build(FORMATS[kname], sizes)
+            o = oracle.build(FORMATS[kname], sizes)
+            for k, v in r.items():
+                if k == "storage":
+                    assert o.storage == v
+                else:
+                    assert np.array_equal(np.asarray(o.meta[k]), np.asarray(v)), (trial, kname, k)
+
+
+def test_ellpack_overflow_like_reference(oracle, reference):
+    sizes = np.full(40000, 60000, np.int32)  # 40000*60000 > 2^31
+    with pytest.raises(OverflowError):
+        reference.build(FORMATS["Ellpack"], sizes)
+    with pytest.raises(OverflowError):
+        oracle.build(FORMATS["Ellpack"], sizes)
+
+
+@pytest.mark.parametrize("pname", ["laplacian32", "diffusion32"])
+def test_solvers_match_golden(oracle, golden, pname):
+    class A:
+        pass
+
+    A.rowptr = golden.get(f"prob/{pname}/rowptr")
+    A.cols = golden.get(f"prob/{pname}/cols")
+    A.vals = golden.get(f"prob/{pname}/vals")
+    A.n = len(A.rowptr) - 1
+    b = golden.get(f"prob/{pname}/b")
+    for key, ref in golden.meta["solvers"].items():
+        p, solver, pre = key.split("/")
+        if p != pname:
+            continue
+        pre = int(pre)
+        r = oracle.solve(solver, A, b, precond=pre, tol=1e-8, maxit=20000, gmres_m=30, gmres_reorth=2)
+        assert r["converged"] == ref["converged"], key
+        if solver == "bicgstab":
+            # BiCGStab amplifies the reference's non-reproducible OpenMP
+            # reductions: the reference itself moves by up to ~10% of its
+            # iteration count between thread counts (1..8 threads).
+            assert abs(r["iterations"] - ref["iterations"]) <= max(5, ref["iterations"] // 10), key
+            assert r["residue"] < 1e-8
+        else:
+            assert r["iterations"] == ref["iterations"], key
+            assert r["residue"] == pytest.approx(ref["residue"], rel=1e-6), key
+            assert np.allclose(r["x"], golden.get(f"solve/{key}/x"), rtol=1e-9, atol=1e-12), key
+
+
+def test_preconditioners_match_reference(oracle, reference):
+    A = g.diffusion_2d(24, 0.1, 1.5, 4)
+    b = g.uniform_vector(A.n, 3)
+    for kind in (1, 2):
+        assert np.array_equal(oracle.prec_apply(A, kind, b), reference.prec_apply(A, kind, b)), kind
+
+
+def test_bicgstab_within_reference_spread(oracle, reference):
+    """The reference's own BiCGStab changes with its OpenMP thread count; the
+    oracle must stay inside that spread."""
+    A = g.diffusion_2d(40, 0.1, 1.0, 3)
+    b = g.uniform_vector(A.n, 1)
+    o = oracle.solve("bicgstab", A, b, precond=1, tol=1e-8, maxit=20000)
+    its = []
+    try:
+        for t in (1, 2, 3, 4, 8):
+            reference.set_threads(t)
+            r = reference.solve("bicgstab", A, b, precond=1, tol=1e-8, maxit=20000)
+            assert r["converged"]
+            its.append(r["iterations"])
+    finally:
+        reference.set_threads(reference.threads())
+    assert o["converged"]
+    spread = max(its) - min(its)
+    assert min(its) - max(2, spread) <= o["iterations"] <= max(its) + max(2, spread), (o["iterations"], its)
+    assert oracle.true_residual(A, b, o["x"]) < 1e-7

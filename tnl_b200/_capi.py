@@ -1,0 +1,110 @@
+"""ctypes binding of libtnlb200.so (the C ABI declared in include/tnlb200.h).
+
+The library is loaded from tnl_b200/_lib/libtnlb200.so.  There is no
+fallback: if the library is missing, importing this module raises
+ImportError telling how to build it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libtnlb200.so"
+
+if not LIB_PATH.exists():
+    raise ImportError(
+        f"{LIB_PATH} is missing: build the CUDA library with `python -m tnl_b200.build` "
+        "(or __graft_entry__.build()); there is no CPU fallback"
+    )
+
+lib = C.CDLL(str(LIB_PATH))
+
+# status codes (tnlb_status)
+OK, ERR_INVALID_ARGUMENT, ERR_OVERFLOW, ERR_CUDA, ERR_NOT_IMPLEMENTED, ERR_BREAKDOWN, ERR_TIMEOUT, ERR_OOM = range(8)
+F32, F64 = 0, 1
+CSR, ELLPACK, SLICED_ELLPACK, CHUNKED_ELLPACK, BIELLPACK, ADAPTIVE_CSR = range(6)
+COLUMN_MAJOR, ROW_MAJOR = 0, 1
+KERNEL_DEFAULT, KERNEL_SCALAR, KERNEL_VECTOR, KERNEL_LIGHT, KERNEL_ADAPTIVE = range(5)
+(META_OFFSETS, META_SLICE_OFFSETS, META_SLICE_SEGMENT_SIZES, META_CH_SLICE_SIZE, META_CH_SLICE_CHUNK_SIZE,
+ META_CH_SLICE_FIRST, META_CH_SLICE_POINTER, META_CH_SEGMENT_TO_CHUNK, META_CH_SEGMENT_TO_SLICE,
+ META_CH_SEGMENT_POINTERS, META_CH_CHUNKS_TO_SEGMENTS, META_BI_PERMUTATION, META_BI_GROUP_POINTERS) = range(13)
+
+
+class BackendRuntimeError(RuntimeError):
+    """A CUDA error (the reference's Exceptions::BackendRuntimeError)."""
+
+
+class BreakdownError(RuntimeError):
+    """A zero pivot in the GMRES least-squares update (the reference throws 1)."""
+
+
+class DeviceTimeoutError(RuntimeError):
+    """A bounded device-side wait gave up."""
+
+
+class SegmentsInfo(C.Structure):
+    _fields_ = [
+        ("format", C.c_int32), ("organization", C.c_int32), ("segments", C.c_int32), ("reserved0", C.c_int32),
+        ("elements", C.c_int64), ("storage", C.c_int64), ("segment_size", C.c_int32), ("aligned_size", C.c_int32),
+        ("slices", C.c_int32), ("chunks_in_slice", C.c_int32), ("acsr_blocks", C.c_int64 * 6),
+    ]
+
+
+class AcsrBlock(C.Structure):
+    _fields_ = [
+        ("type", C.c_uint8), ("warp_idx", C.c_uint8), ("warps_count", C.c_uint8), ("reserved", C.c_uint8),
+        ("first_segment", C.c_int32), ("block_size", C.c_int32), ("segments_in_block", C.c_int32),
+    ]
+
+
+_p = C.c_void_p
+_i32, _i64, _f64 = C.c_int32, C.c_int64, C.c_double
+
+
+def _sig(name, argtypes, restype=C.c_int):
+    f = getattr(lib, name)
+    f.argtypes = argtypes
+    f.restype = restype
+    return f
+
+
+tnlb_last_error = _sig("tnlb_last_error", [], C.c_char_p)
+tnlb_version = _sig("tnlb_version", [], C.c_char_p)
+tnlb_segments_create = _sig("tnlb_segments_create", [C.c_int, C.c_int, _p, _i32, _p, C.POINTER(_p)])
+tnlb_segments_destroy = _sig("tnlb_segments_destroy", [_p])
+tnlb_segments_get_info = _sig("tnlb_segments_get_info", [_p, C.POINTER(SegmentsInfo)])
+tnlb_segments_read_metadata = _sig("tnlb_segments_read_metadata", [_p, C.c_int, _p, _i64])
+tnlb_segments_read_acsr_blocks = _sig("tnlb_segments_read_acsr_blocks", [_p, _i32, _p, _i64])
+tnlb_segments_global_index = _sig("tnlb_segments_global_index", [_p, _p, _p, _i64, _p, _p])
+tnlb_matrix_fill_from_csr = _sig("tnlb_matrix_fill_from_csr", [_p, C.c_int, _p, _p, _p, _p, _p, _p])
+tnlb_spmv = _sig("tnlb_spmv", [_p, C.c_int, _p, _p, _i32, _p, _p, _f64, _f64, _i32, _i32, C.c_int, _i32, _p])
+tnlb_spmv_last_launch_count = _sig("tnlb_spmv_last_launch_count", [], _i32)
+tnlb_dot = _sig("tnlb_dot", [C.c_int, _i64, _p, _p, _p, _p])
+
+
+def check(status: int) -> None:
+    """Raise the exception the reference would throw for this status."""
+    if status == OK:
+        return
+    msg = (tnlb_last_error() or b"").decode(errors="replace")
+    if status == ERR_INVALID_ARGUMENT:
+        raise ValueError(msg)
+    if status == ERR_OVERFLOW:
+        raise OverflowError(msg)
+    if status == ERR_NOT_IMPLEMENTED:
+        raise NotImplementedError(msg)
+    if status == ERR_BREAKDOWN:
+        raise BreakdownError(msg)
+    if status == ERR_TIMEOUT:
+        raise DeviceTimeoutError(msg)
+    if status == ERR_OOM:
+        raise MemoryError(msg)
+    raise BackendRuntimeError(msg)
+
+
+def exported_symbols() -> list[str]:
+    """Names of every tnlb_* function the library exports (checked against the header)."""
+    import subprocess
+
+    out = subprocess.run(["nm", "-D", "--defined-only", str(LIB_PATH)], capture_output=True, text=True).stdout
+    return sorted({ln.split()[-1] for ln in out.splitlines() if " T " in ln and ln.split()[-1].startswith("tnlb_")})

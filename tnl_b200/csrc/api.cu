@@ -1,0 +1,266 @@
+// api.cu -- the extern "C" entry points of libtnlb200.so declared in
+// include/tnlb200.h.  No entry point throws; failures return a status and
+// leave a message for tnlb_last_error().
+#include <new>
+
+#include "internal.cuh"
+
+namespace tnlb {
+
+namespace {
+thread_local std::string g_last_error;
+thread_local int32_t g_last_launches = 0;
+}  // namespace
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+void clear_error() { g_last_error.clear(); }
+
+namespace {
+
+template <typename T>
+__global__ void k_dot(int64_t n, const T* __restrict__ a, const T* __restrict__ b, double* __restrict__ out)
+{
+   __shared__ double part[8];
+   double s = 0;
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+      s += (double)a[i] * (double)b[i];
+   s = warp_sum(s);
+   if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = s;
+   __syncthreads();
+   if (threadIdx.x < 32) {
+      s = threadIdx.x < 8 ? part[threadIdx.x] : 0.0;
+      s = warp_sum(s);
+      if (threadIdx.x == 0) atomicAdd(out, s);
+   }
+}
+
+tnlb_status copy_meta(const tnlb::DeviceBuffer& buf, int64_t elems, int32_t* h_out, int64_t count)
+{
+   TNLB_REQUIRE(count >= elems, TNLB_ERR_INVALID_ARGUMENT,
+                "metadata buffer too small: need " + std::to_string(elems) + " elements");
+   if (elems > 0) TNLB_CUDA_TRY(cudaMemcpy(h_out, buf.ptr, sizeof(int32_t) * (size_t)elems, cudaMemcpyDeviceToHost));
+   return TNLB_OK;
+}
+
+}  // namespace
+}  // namespace tnlb
+
+using namespace tnlb;
+
+extern "C" {
+
+const char* tnlb_last_error(void) { return g_last_error.c_str(); }
+
+const char* tnlb_version(void) { return "tnlb200 0.1.0 (sm_100a)"; }
+
+tnlb_status tnlb_segments_create(tnlb_format format, tnlb_organization organization, const int32_t* d_sizes,
+                                 int32_t segments, tnlb_stream stream, tnlb_segments** out)
+{
+   clear_error();
+   TNLB_REQUIRE(out != nullptr, TNLB_ERR_INVALID_ARGUMENT, "out is null");
+   *out = nullptr;
+   TNLB_REQUIRE(segments >= 0, TNLB_ERR_INVALID_ARGUMENT, "negative segment count");
+   TNLB_REQUIRE(segments == 0 || d_sizes != nullptr, TNLB_ERR_INVALID_ARGUMENT, "sizes are null");
+   TNLB_REQUIRE(format >= TNLB_CSR && format <= TNLB_ADAPTIVE_CSR, TNLB_ERR_INVALID_ARGUMENT, "unknown format");
+   TNLB_REQUIRE(organization == TNLB_COLUMN_MAJOR || organization == TNLB_ROW_MAJOR, TNLB_ERR_INVALID_ARGUMENT,
+                "unknown elements organization");
+   tnlb_segments* seg = new (std::nothrow) tnlb_segments();
+   TNLB_REQUIRE(seg != nullptr, TNLB_ERR_OUT_OF_MEMORY, "out of host memory");
+   seg->format = format;
+   seg->organization = organization;
+   seg->n = segments;
+   TNLB_CUDA_TRY(cudaGetDevice(&seg->device));
+   tnlb_status s = build_segments(seg, d_sizes, (cudaStream_t)stream);
+   if (s == TNLB_OK) {
+      cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
+      if (e != cudaSuccess) {
+         set_error(std::string("segments build: ") + cudaGetErrorString(e));
+         s = TNLB_ERR_CUDA;
+      }
+   }
+   if (s != TNLB_OK) {
+      delete seg;
+      return s;
+   }
+   *out = seg;
+   return TNLB_OK;
+}
+
+tnlb_status tnlb_segments_destroy(tnlb_segments* seg)
+{
+   clear_error();
+   delete seg;
+   return TNLB_OK;
+}
+
+tnlb_status tnlb_segments_get_info(const tnlb_segments* seg, tnlb_segments_info* info)
+{
+   clear_error();
+   TNLB_REQUIRE(seg && info, TNLB_ERR_INVALID_ARGUMENT, "null argument");
+   *info = tnlb_segments_info{};
+   info->format = seg->format;
+   info->organization = seg->organization;
+   info->segments = seg->n;
+   info->elements = seg->elements;
+   info->storage = seg->storage;
+   info->segment_size = seg->segment_size;
+   info->aligned_size = seg->aligned_size;
+   info->slices = seg->format == TNLB_SLICED_ELLPACK ? seg->slices
+                : seg->format == TNLB_CHUNKED_ELLPACK ? seg->ch_slices
+                : seg->format == TNLB_BIELLPACK ? seg->strips
+                                                : 0;
+   info->chunks_in_slice = kChunksInSlice;
+   for (int k = 0; k < 6; k++) info->acsr_blocks[k] = seg->acsr_count[k];
+   return TNLB_OK;
+}
+
+tnlb_status tnlb_segments_read_metadata(const tnlb_segments* seg, tnlb_metadata which, int32_t* h_out, int64_t count)
+{
+   clear_error();
+   TNLB_REQUIRE(seg && (h_out || count == 0), TNLB_ERR_INVALID_ARGUMENT, "null argument");
+   const int64_t n = seg->n;
+   const bool csr = seg->format == TNLB_CSR || seg->format == TNLB_ADAPTIVE_CSR;
+   const bool sell = seg->format == TNLB_SLICED_ELLPACK;
+   const bool ch = seg->format == TNLB_CHUNKED_ELLPACK;
+   const bool bi = seg->format == TNLB_BIELLPACK;
+   const int64_t cs = seg->ch_slices;
+   switch (which) {
+      case TNLB_META_OFFSETS:
+         TNLB_REQUIRE(csr, TNLB_ERR_INVALID_ARGUMENT, "not a CSR format");
+         return copy_meta(seg->offsets, n + 1, h_out, count);
+      case TNLB_META_SLICE_OFFSETS:
+         TNLB_REQUIRE(sell, TNLB_ERR_INVALID_ARGUMENT, "not SlicedEllpack");
+         return copy_meta(seg->slice_offsets, (int64_t)seg->slices + 1, h_out, count);
+      case TNLB_META_SLICE_SEGMENT_SIZES:
+         TNLB_REQUIRE(sell, TNLB_ERR_INVALID_ARGUMENT, "not SlicedEllpack");
+         return copy_meta(seg->slice_segment_sizes, seg->slices, h_out, count);
+      case TNLB_META_CH_SLICE_SIZE:
+         TNLB_REQUIRE(ch, TNLB_ERR_INVALID_ARGUMENT, "not ChunkedEllpack");
+         return copy_meta(seg->ch_slice_size, cs, h_out, count);
+      case TNLB_META_CH_SLICE_CHUNK_SIZE:
+         TNLB_REQUIRE(ch, TNLB_ERR_INVALID_ARGUMENT, "not ChunkedEllpack");
+         return copy_meta(seg->ch_slice_chunk_size, cs, h_out, count);
+      case TNLB_META_CH_SLICE_FIRST:
+         TNLB_REQUIRE(ch, TNLB_ERR_INVALID_ARGUMENT, "not ChunkedEllpack");
+         return copy_meta(seg->ch_slice_first, cs, h_out, count);
+      case TNLB_META_CH_SLICE_POINTER:
+         TNLB_REQUIRE(ch, TNLB_ERR_INVALID_ARGUMENT, "not ChunkedEllpack");
+         return copy_meta(seg->ch_slice_pointer, cs, h_out, count);
+      case TNLB_META_CH_SEGMENT_TO_CHUNK:
+         TNLB_REQUIRE(ch, TNLB_ERR_INVALID_ARGUMENT, "not ChunkedEllpack");
+         return copy_meta(seg->ch_segment_to_chunk, n, h_out, count);
+      case TNLB_META_CH_SEGMENT_TO_SLICE:
+         TNLB_REQUIRE(ch, TNLB_ERR_INVALID_ARGUMENT, "not ChunkedEllpack");
+         return copy_meta(seg->ch_segment_to_slice, n, h_out, count);
+      case TNLB_META_CH_SEGMENT_POINTERS:
+         TNLB_REQUIRE(ch, TNLB_ERR_INVALID_ARGUMENT, "not ChunkedEllpack");
+         return copy_meta(seg->ch_segment_pointers, n + 1, h_out, count);
+      case TNLB_META_CH_CHUNKS_TO_SEGMENTS:
+         TNLB_REQUIRE(ch, TNLB_ERR_INVALID_ARGUMENT, "not ChunkedEllpack");
+         return copy_meta(seg->ch_chunks_to_segments, cs * kChunksInSlice, h_out, count);
+      case TNLB_META_BI_PERMUTATION:
+         TNLB_REQUIRE(bi, TNLB_ERR_INVALID_ARGUMENT, "not BiEllpack");
+         return copy_meta(seg->bi_perm, n, h_out, count);
+      case TNLB_META_BI_GROUP_POINTERS:
+         TNLB_REQUIRE(bi, TNLB_ERR_INVALID_ARGUMENT, "not BiEllpack");
+         return copy_meta(seg->bi_group_pointers, (int64_t)seg->strips * kBiGroups + 1, h_out, count);
+   }
+   set_error("unknown metadata array");
+   return TNLB_ERR_INVALID_ARGUMENT;
+}
+
+tnlb_status tnlb_segments_read_acsr_blocks(const tnlb_segments* seg, int32_t size_log, tnlb_acsr_block* h_out,
+                                           int64_t count)
+{
+   clear_error();
+   TNLB_REQUIRE(seg != nullptr, TNLB_ERR_INVALID_ARGUMENT, "null segments");
+   TNLB_REQUIRE(seg->format == TNLB_ADAPTIVE_CSR, TNLB_ERR_INVALID_ARGUMENT, "not AdaptiveCSR");
+   TNLB_REQUIRE(size_log >= 0 && size_log < 6, TNLB_ERR_INVALID_ARGUMENT, "size_log must be 0..5");
+   const int64_t c = seg->acsr_count[size_log];
+   TNLB_REQUIRE(count >= c, TNLB_ERR_INVALID_ARGUMENT, "descriptor buffer too small");
+   if (c > 0)
+      TNLB_CUDA_TRY(cudaMemcpy(h_out, seg->acsr_blocks[size_log].ptr, sizeof(tnlb_acsr_block) * (size_t)c,
+                               cudaMemcpyDeviceToHost));
+   return TNLB_OK;
+}
+
+tnlb_status tnlb_segments_global_index(const tnlb_segments* seg, const int32_t* d_segment, const int32_t* d_local,
+                                       int64_t count, int64_t* d_global, tnlb_stream stream)
+{
+   clear_error();
+   TNLB_REQUIRE(seg != nullptr, TNLB_ERR_INVALID_ARGUMENT, "null segments");
+   TNLB_REQUIRE(count == 0 || (d_segment && d_local && d_global), TNLB_ERR_INVALID_ARGUMENT, "null array");
+   return global_index(seg, d_segment, d_local, count, d_global, (cudaStream_t)stream);
+}
+
+tnlb_status tnlb_matrix_fill_from_csr(const tnlb_segments* seg, tnlb_real real, const int32_t* d_rowptr,
+                                      const int32_t* d_src_cols, const void* d_src_values, int32_t* d_cols,
+                                      void* d_values, tnlb_stream stream)
+{
+   clear_error();
+   TNLB_REQUIRE(seg != nullptr, TNLB_ERR_INVALID_ARGUMENT, "null segments");
+   TNLB_REQUIRE(real == TNLB_F32 || real == TNLB_F64, TNLB_ERR_INVALID_ARGUMENT, "unknown real type");
+   TNLB_REQUIRE(seg->n == 0 || (d_rowptr && d_src_cols && d_src_values), TNLB_ERR_INVALID_ARGUMENT,
+                "null source array");
+   TNLB_REQUIRE(seg->storage == 0 || (d_cols && d_values), TNLB_ERR_INVALID_ARGUMENT, "null target array");
+   return fill_from_csr(seg, real, d_rowptr, d_src_cols, d_src_values, d_cols, d_values, (cudaStream_t)stream);
+}
+
+tnlb_status tnlb_spmv(const tnlb_segments* seg, tnlb_real real, const int32_t* d_cols, const void* d_values,
+                      int32_t columns, const void* d_x, void* d_y, double alpha, double beta, int32_t begin,
+                      int32_t end, tnlb_kernel kernel, int32_t threads_per_segment, tnlb_stream stream)
+{
+   clear_error();
+   g_last_launches = 0;
+   TNLB_REQUIRE(seg != nullptr, TNLB_ERR_INVALID_ARGUMENT, "null segments");
+   TNLB_REQUIRE(real == TNLB_F32 || real == TNLB_F64, TNLB_ERR_INVALID_ARGUMENT, "unknown real type");
+   TNLB_REQUIRE(columns >= 0, TNLB_ERR_INVALID_ARGUMENT,
+                "vectorProduct: size of the input vector does not match the number of matrix columns");
+   if (end == 0) end = seg->n;
+   TNLB_REQUIRE(begin >= 0 && begin <= end && end <= seg->n, TNLB_ERR_INVALID_ARGUMENT,
+                "vectorProduct: row range [begin, end) outside the matrix");
+   TNLB_REQUIRE(threads_per_segment == 0 || (threads_per_segment > 0 && threads_per_segment <= 256 &&
+                                             (threads_per_segment & (threads_per_segment - 1)) == 0),
+                TNLB_ERR_INVALID_ARGUMENT, "Threads per segment count must be a positive power of two.");
+   if (end == begin) return TNLB_OK;
+   TNLB_REQUIRE(d_y != nullptr && (seg->storage == 0 || (d_cols && d_values && d_x)), TNLB_ERR_INVALID_ARGUMENT,
+                "null array");
+   int launches = 0;
+   tnlb_status s;
+   if (seg->format == TNLB_CSR || seg->format == TNLB_ADAPTIVE_CSR) {
+      tnlb_kernel k = kernel;
+      if (seg->format == TNLB_ADAPTIVE_CSR && kernel == TNLB_KERNEL_DEFAULT) k = TNLB_KERNEL_ADAPTIVE;
+      s = spmv_csr(seg, real, d_cols, d_values, d_x, d_y, alpha, beta, begin, end, k, threads_per_segment,
+                   (cudaStream_t)stream, &launches);
+   }
+   else {
+      TNLB_REQUIRE(kernel == TNLB_KERNEL_DEFAULT || kernel == TNLB_KERNEL_VECTOR || kernel == TNLB_KERNEL_SCALAR,
+                   TNLB_ERR_INVALID_ARGUMENT, "kernel not available for this format");
+      s = spmv_ell_family(seg, real, d_cols, d_values, d_x, d_y, alpha, beta, begin, end, kernel,
+                          kernel == TNLB_KERNEL_SCALAR ? 1 : threads_per_segment, (cudaStream_t)stream, &launches);
+   }
+   g_last_launches = launches;
+   return s;
+}
+
+int32_t tnlb_spmv_last_launch_count(void) { return g_last_launches; }
+
+tnlb_status tnlb_dot(tnlb_real real, int64_t n, const void* d_a, const void* d_b, double* d_result, tnlb_stream stream)
+{
+   clear_error();
+   TNLB_REQUIRE(d_result != nullptr, TNLB_ERR_INVALID_ARGUMENT, "null result");
+   TNLB_REQUIRE(n == 0 || (d_a && d_b), TNLB_ERR_INVALID_ARGUMENT, "null vector");
+   cudaStream_t st = (cudaStream_t)stream;
+   TNLB_CUDA_TRY(cudaMemsetAsync(d_result, 0, sizeof(double), st));
+   if (n == 0) return TNLB_OK;
+   unsigned g = grid_for(n, 256 * 4);
+   if (g > 148 * 8) g = 148 * 8;
+   if (real == TNLB_F64)
+      k_dot<double><<<g, 256, 0, st>>>(n, (const double*)d_a, (const double*)d_b, d_result);
+   else
+      k_dot<float><<<g, 256, 0, st>>>(n, (const float*)d_a, (const float*)d_b, d_result);
+   TNLB_CHECK_LAUNCH();
+   return TNLB_OK;
+}
+
+}  // extern "C"

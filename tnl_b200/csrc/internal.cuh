@@ -1,0 +1,263 @@
+// internal.cuh -- shared definitions of libtnlb200 (not part of the public ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+
+#include "../../include/tnlb200.h"
+
+namespace tnlb {
+
+// ----------------------------------------------------------------- errors
+
+void set_error(const std::string& msg);
+void clear_error();
+
+#define TNLB_CUDA_TRY(expr)                                                                                    \
+   do {                                                                                                        \
+      cudaError_t _e = (expr);                                                                                 \
+      if (_e != cudaSuccess) {                                                                                 \
+         ::tnlb::set_error(std::string(#expr) + ": " + cudaGetErrorString(_e) + " (" + __FILE__ + ":" +        \
+                           std::to_string(__LINE__) + ")");                                                    \
+         return _e == cudaErrorMemoryAllocation ? TNLB_ERR_OUT_OF_MEMORY : TNLB_ERR_CUDA;                      \
+      }                                                                                                        \
+   } while (0)
+
+#define TNLB_CHECK_LAUNCH() TNLB_CUDA_TRY(cudaGetLastError())
+
+#define TNLB_REQUIRE(cond, code, msg)                                                                          \
+   do {                                                                                                        \
+      if (!(cond)) {                                                                                           \
+         ::tnlb::set_error(msg);                                                                               \
+         return code;                                                                                          \
+      }                                                                                                        \
+   } while (0)
+
+#define TNLB_TRY_STATUS(expr)                                                                                  \
+   do {                                                                                                        \
+      tnlb_status _s = (expr);                                                                                 \
+      if (_s != TNLB_OK) return _s;                                                                            \
+   } while (0)
+
+// ------------------------------------------------------------- constants
+
+constexpr int kWarp = 32;
+constexpr int kSellSlice = 32;       // SlicedEllpack SliceSize (SlicedEllpack.h:46)
+constexpr int kEllAlignment = 32;    // Ellpack Alignment (Ellpack.h:40)
+constexpr int kBiStrip = 32;         // BiEllpack WarpSize
+constexpr int kBiGroups = 6;         // log2(32) + 1
+constexpr int kChunksInSlice = 256;  // ChunkedEllpackBase.h:291
+constexpr int kDesiredChunkSize = 16;  // ChunkedEllpackBase.h:292
+
+// CSR tile kernel geometry: 256 threads, ITEMS merge items (rows + nonzeros)
+// per thread.
+constexpr int kTileThreads = 256;
+constexpr int kTileItems = 8;
+constexpr int kTileSize = kTileThreads * kTileItems;
+
+// ------------------------------------------------------- device buffers
+
+// Owned device allocation (cudaMalloc / cudaFree).
+struct DeviceBuffer {
+   void* ptr = nullptr;
+   size_t bytes = 0;
+   DeviceBuffer() = default;
+   DeviceBuffer(const DeviceBuffer&) = delete;
+   DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+   ~DeviceBuffer() { release(); }
+   void release()
+   {
+      if (ptr) cudaFree(ptr);
+      ptr = nullptr;
+      bytes = 0;
+   }
+   tnlb_status alloc(size_t nbytes)
+   {
+      release();
+      if (nbytes == 0) nbytes = 16;
+      cudaError_t e = cudaMalloc(&ptr, nbytes);
+      if (e != cudaSuccess) {
+         ptr = nullptr;
+         set_error(std::string("cudaMalloc(") + std::to_string(nbytes) + "): " + cudaGetErrorString(e));
+         return TNLB_ERR_OUT_OF_MEMORY;
+      }
+      bytes = nbytes;
+      return TNLB_OK;
+   }
+   template <typename T>
+   T* as() const
+   {
+      return static_cast<T*>(ptr);
+   }
+};
+
+}  // namespace tnlb
+
+// ------------------------------------------------------------ segments
+// The opaque handle of the C ABI.
+struct tnlb_segments {
+   int32_t format = TNLB_CSR;
+   int32_t organization = TNLB_COLUMN_MAJOR;
+   int32_t n = 0;           // segments
+   int64_t elements = 0;    // sum of sizes
+   int64_t storage = 0;     // slots
+   int32_t max_size = 0;    // largest segment size
+   int device = 0;
+
+   // CSR / AdaptiveCSR
+   tnlb::DeviceBuffer offsets;  // int32[n+1]
+   // CSR tile plan: merge-path coordinates of tile boundaries
+   int32_t tiles = 0;
+   tnlb::DeviceBuffer tile_row;    // int32[tiles+1]
+   tnlb::DeviceBuffer tile_nnz;    // int32[tiles+1]
+   tnlb::DeviceBuffer carry_row;   // int32[tiles]   (scratch, per call)
+   tnlb::DeviceBuffer carry_val;   // double[tiles]  (scratch, per call)
+   // AdaptiveCSR descriptors per value-size log
+   int64_t acsr_count[6] = {0, 0, 0, 0, 0, 0};
+   tnlb::DeviceBuffer acsr_blocks[6];  // tnlb_acsr_block[count]
+
+   // Ellpack
+   int32_t segment_size = 0;
+   int32_t aligned_size = 0;
+
+   // SlicedEllpack
+   int32_t slices = 0;
+   tnlb::DeviceBuffer slice_offsets;        // int32[slices+1]
+   tnlb::DeviceBuffer slice_segment_sizes;  // int32[slices]
+   tnlb::DeviceBuffer slice_order;          // int32[slices]: slices by width, widest first
+
+   // ChunkedEllpack
+   int32_t ch_slices = 0;
+   tnlb::DeviceBuffer ch_slice_size, ch_slice_chunk_size, ch_slice_first, ch_slice_pointer;  // int32[ch_slices]
+   tnlb::DeviceBuffer ch_segment_to_chunk, ch_segment_to_slice;                             // int32[n]
+   tnlb::DeviceBuffer ch_segment_pointers;                                                  // int32[n+1]
+   tnlb::DeviceBuffer ch_chunks_to_segments;                                                // int32[ch_slices*256]
+
+   // BiEllpack
+   int32_t strips = 0;
+   tnlb::DeviceBuffer bi_perm;            // int32[n]
+   tnlb::DeviceBuffer bi_group_pointers;  // int32[strips*6+1]
+};
+
+namespace tnlb {
+
+// ------------------------------------------------- device-side helpers
+
+// Streaming (read-once) global loads: non-coherent path, no L1 allocation.
+__device__ __forceinline__ double ld_stream(const double* p)
+{
+   double v;
+   asm volatile("ld.global.nc.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(p));
+   return v;
+}
+__device__ __forceinline__ float ld_stream(const float* p)
+{
+   float v;
+   asm volatile("ld.global.nc.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
+   return v;
+}
+__device__ __forceinline__ int32_t ld_stream(const int32_t* p)
+{
+   int32_t v;
+   asm volatile("ld.global.nc.L1::no_allocate.s32 %0, [%1];" : "=r"(v) : "l"(p));
+   return v;
+}
+// 128-bit streaming loads (address must be 16-byte aligned).
+__device__ __forceinline__ double2 ld_stream_v2(const double* p)
+{
+   double2 v;
+   asm volatile("ld.global.nc.L1::no_allocate.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "l"(p));
+   return v;
+}
+__device__ __forceinline__ float4 ld_stream_v4(const float* p)
+{
+   float4 v;
+   asm volatile("ld.global.nc.L1::no_allocate.v4.f32 {%0, %1, %2, %3}, [%4];"
+                : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+                : "l"(p));
+   return v;
+}
+__device__ __forceinline__ int4 ld_stream_v4(const int32_t* p)
+{
+   int4 v;
+   asm volatile("ld.global.nc.L1::no_allocate.v4.s32 {%0, %1, %2, %3}, [%4];"
+                : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+                : "l"(p));
+   return v;
+}
+
+// Gathered x loads go through the read-only path and may stay cached.
+template <typename T>
+__device__ __forceinline__ T ld_gather(const T* p)
+{
+   return __ldg(p);
+}
+
+__host__ __device__ __forceinline__ int64_t imin64(int64_t a, int64_t b) { return a < b ? a : b; }
+__host__ __device__ __forceinline__ int64_t imax64(int64_t a, int64_t b) { return a > b ? a : b; }
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v)
+{
+#pragma unroll
+   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+   return v;
+}
+
+// Sum within aligned groups of `G` lanes (G power of two <= 32).
+template <int G, typename T>
+__device__ __forceinline__ T group_sum(T v)
+{
+#pragma unroll
+   for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+   return v;
+}
+
+// The four keep variants of vectorProduct (SparseMatrixBase.hpp:346-392).
+template <typename Real>
+__device__ __forceinline__ void keep(Real* y, int32_t row, Real value, Real alpha, Real beta)
+{
+   if (beta == Real(0)) {
+      y[row] = (alpha == Real(1)) ? value : alpha * value;
+   }
+   else {
+      y[row] = (alpha == Real(1)) ? beta * y[row] + value : beta * y[row] + alpha * value;
+   }
+}
+
+inline unsigned grid_for(int64_t work, int per_block)
+{
+   int64_t g = (work + per_block - 1) / per_block;
+   if (g < 1) g = 1;
+   if (g > 0x7fffffff) g = 0x7fffffff;
+   return (unsigned)g;
+}
+
+// -------------------------------------------------- internal interfaces
+
+// builders.cu
+tnlb_status build_segments(tnlb_segments* seg, const int32_t* d_sizes, cudaStream_t stream);
+// scan.cu
+tnlb_status exclusive_scan_i32(const int32_t* d_in, int32_t* d_out, int64_t n, int64_t* h_total, cudaStream_t stream,
+                               bool append_total);
+tnlb_status inclusive_scan_i32_inplace(int32_t* d_data, int64_t n, cudaStream_t stream);
+tnlb_status reduce_max_i32(const int32_t* d_in, int64_t n, int32_t* h_max, cudaStream_t stream);
+tnlb_status reduce_sum_i64(const int32_t* d_in, int64_t n, int64_t* h_sum, cudaStream_t stream);
+// spmv_csr.cu / spmv_ell.cu
+tnlb_status spmv_csr(const tnlb_segments* seg, tnlb_real real, const int32_t* cols, const void* vals, const void* x,
+                     void* y, double alpha, double beta, int32_t begin, int32_t end, tnlb_kernel kernel, int32_t tps,
+                     cudaStream_t stream, int* launches);
+tnlb_status spmv_ell_family(const tnlb_segments* seg, tnlb_real real, const int32_t* cols, const void* vals,
+                            const void* x, void* y, double alpha, double beta, int32_t begin, int32_t end,
+                            tnlb_kernel kernel, int32_t tps, cudaStream_t stream, int* launches);
+tnlb_status build_csr_tile_plan(tnlb_segments* seg, cudaStream_t stream);
+// fill.cu
+tnlb_status fill_from_csr(const tnlb_segments* seg, tnlb_real real, const int32_t* rowptr, const int32_t* src_cols,
+                          const void* src_vals, int32_t* cols, void* vals, cudaStream_t stream);
+tnlb_status global_index(const tnlb_segments* seg, const int32_t* segs, const int32_t* locals, int64_t count,
+                         int64_t* out, cudaStream_t stream);
+
+}  // namespace tnlb

@@ -1,0 +1,483 @@
+// spmv_csr.cu -- y = alpha*A*x + beta*y for CSR (and AdaptiveCSR) segments.
+//
+// Kernels (the names of Algorithms/SegmentsReductionKernels and the
+// ThreadsToSegmentsMapping of Segments/LaunchConfiguration.h):
+//  * scalar   -- one thread per row (Fixed, TPS 1; ReducingOperations_CSR.h:33-77)
+//  * vector   -- G = 2..32 lanes per row, shuffle reduction
+//                (reduceSegmentsCSRVariableVectorKernel, ReducingKernels_CSR.h:63-118)
+//  * block    -- 64/128/256 threads per row through shared memory
+//                (reduceSegmentsCSRLightMultivectorKernel, :120-189)
+//  * light    -- G chosen from the mean row length
+//                (LaunchConfigurationSetter_LightCSR.h:30-58)
+//  * adaptive -- AdaptiveCSR STREAM / VECTOR / LONG block descriptors
+//                (ReducingKernels_AdaptiveCSR.h:16-134)
+//  * tile     -- the default: nnz-balanced merge-path tiles.  The merge of
+//                the row-end offsets with the nonzero indices is cut into
+//                tiles of 2048 items (rows + nonzeros) so that every block
+//                does the same work whatever the row-length distribution
+//                (Merrill & Garland, "Merge-based parallel sparse
+//                matrix-vector multiplication", SC16).  Each block streams
+//                its values/columns with coalesced non-caching loads,
+//                stages row ends and products in shared memory, walks 8
+//                merge items per thread, combines rows split between
+//                threads with a warp-shuffle segmented scan, and writes y
+//                with coalesced stores.  A row split between tiles leaves a
+//                partial sum per tile in a carry array; a second small
+//                kernel adds them (in tile order, so results are
+//                deterministic).  The tile coordinates are computed once
+//                per matrix, when the segments are built.
+#include <climits>
+
+#include "internal.cuh"
+
+namespace tnlb {
+namespace {
+
+// ------------------------------------------------------------- scalar
+
+template <typename Real>
+__global__ void k_csr_scalar(const int32_t* __restrict__ rowptr, const int32_t* __restrict__ cols,
+                             const Real* __restrict__ vals, const Real* __restrict__ x, Real* __restrict__ y,
+                             int32_t begin, int32_t end, Real alpha, Real beta)
+{
+   const int64_t row = begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+   if (row >= end) return;
+   Real sum = 0;
+   for (int32_t j = rowptr[row]; j < rowptr[row + 1]; j++) {
+      const int32_t c = cols[j];
+      if (c >= 0) sum += vals[j] * ld_gather(x + c);
+   }
+   keep(y, (int32_t)row, sum, alpha, beta);
+}
+
+// ------------------------------------------------- vector (G lanes/row)
+
+template <typename Real, int G>
+__global__ void k_csr_vector(const int32_t* __restrict__ rowptr, const int32_t* __restrict__ cols,
+                             const Real* __restrict__ vals, const Real* __restrict__ x, Real* __restrict__ y,
+                             int32_t begin, int32_t end, Real alpha, Real beta)
+{
+   const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+   const int64_t row = begin + gid / G;
+   const int lane = (int)(gid % G);
+   Real sum = 0;
+   if (row < end) {
+      const int32_t rb = rowptr[row], re = rowptr[row + 1];
+      for (int32_t j = rb + lane; j < re; j += G) {
+         const int32_t c = ld_stream(cols + j);
+         const Real v = ld_stream(vals + j);
+         if (c >= 0) sum += v * ld_gather(x + c);
+      }
+   }
+   sum = group_sum<G>(sum);
+   if (row < end && lane == 0) keep(y, (int32_t)row, sum, alpha, beta);
+}
+
+// ---------------------------------------- block (64/128/256 threads/row)
+
+template <typename Real, int G>
+__global__ void k_csr_block(const int32_t* __restrict__ rowptr, const int32_t* __restrict__ cols,
+                            const Real* __restrict__ vals, const Real* __restrict__ x, Real* __restrict__ y,
+                            int32_t begin, int32_t end, Real alpha, Real beta)
+{
+   constexpr int kRowsPerBlock = 256 / G;
+   constexpr int kWarpsPerRow = G / 32;
+   __shared__ Real part[8];
+   const int r_in_block = threadIdx.x / G;
+   const int t = threadIdx.x % G;
+   const int64_t row = begin + (int64_t)blockIdx.x * kRowsPerBlock + r_in_block;
+   Real sum = 0;
+   if (row < end) {
+      const int32_t rb = rowptr[row], re = rowptr[row + 1];
+      for (int32_t j = rb + t; j < re; j += G) {
+         const int32_t c = ld_stream(cols + j);
+         const Real v = ld_stream(vals + j);
+         if (c >= 0) sum += v * ld_gather(x + c);
+      }
+   }
+   sum = warp_sum(sum);
+   if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = sum;
+   __syncthreads();
+   if (t == 0 && row < end) {
+      Real s = 0;
+      for (int w = 0; w < kWarpsPerRow; w++) s += part[r_in_block * kWarpsPerRow + w];
+      keep(y, (int32_t)row, s, alpha, beta);
+   }
+}
+
+// ------------------------------------------------------------ adaptive
+
+template <typename Real>
+struct AcsrParams {
+   static constexpr int kStreamPerWarp = (24576 / (int)sizeof(Real)) / 8;
+};
+
+template <typename Real>
+__global__ void __launch_bounds__(256) k_csr_adaptive(const tnlb_acsr_block* __restrict__ blocks, int64_t count,
+                                                      const int32_t* __restrict__ rowptr,
+                                                      const int32_t* __restrict__ cols, const Real* __restrict__ vals,
+                                                      const Real* __restrict__ x, Real* __restrict__ y, Real alpha,
+                                                      Real beta)
+{
+   constexpr int S = AcsrParams<Real>::kStreamPerWarp;
+   __shared__ Real stream_buf[8][S];
+   __shared__ Real long_part[8];
+   const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+   const int64_t w = (int64_t)blockIdx.x * 8 + wib;
+   const bool active = w < count;
+   tnlb_acsr_block d{};
+   if (active) d = blocks[w];
+   if (active && d.type == 1) {  // STREAM: many short rows, staged per warp
+      const int32_t first = d.first_segment;
+      const int32_t b = rowptr[first];
+      for (int32_t k = lane; k < d.block_size; k += 32) {
+         const int32_t c = ld_stream(cols + b + k);
+         const Real v = ld_stream(vals + b + k);
+         stream_buf[wib][k] = c >= 0 ? v * ld_gather(x + c) : Real(0);
+      }
+      __syncwarp();
+      for (int32_t r = first + lane; r < first + d.segments_in_block; r += 32) {
+         Real s = 0;
+         const int32_t e = rowptr[r + 1] - b;
+         for (int32_t k = rowptr[r] - b; k < e; k++) s += stream_buf[wib][k];
+         keep(y, r, s, alpha, beta);
+      }
+   }
+   else if (active && d.type == 2) {  // VECTOR: one row per warp
+      const int32_t r = d.first_segment;
+      const int32_t b = rowptr[r], e = b + d.block_size;
+      Real s = 0;
+      for (int32_t k = b + lane; k < e; k += 32) {
+         const int32_t c = ld_stream(cols + k);
+         const Real v = ld_stream(vals + k);
+         if (c >= 0) s += v * ld_gather(x + c);
+      }
+      s = warp_sum(s);
+      if (lane == 0) keep(y, r, s, alpha, beta);
+   }
+   else if (active && d.type == 0) {  // LONG: several warps of this block per row
+      const int32_t r = d.first_segment;
+      const int32_t b = rowptr[r], e = rowptr[r + 1];
+      Real s = 0;
+      for (int32_t k = b + lane + 32 * d.warp_idx; k < e; k += 32 * d.warps_count) {
+         const int32_t c = ld_stream(cols + k);
+         const Real v = ld_stream(vals + k);
+         if (c >= 0) s += v * ld_gather(x + c);
+      }
+      s = warp_sum(s);
+      if (lane == 0) long_part[wib] = s;
+   }
+   __syncthreads();
+   if (active && d.type == 0 && d.warp_idx == 0 && lane == 0) {
+      Real s = 0;
+      for (int k = 0; k < d.warps_count; k++) s += long_part[wib + k];
+      keep(y, d.first_segment, s, alpha, beta);
+   }
+}
+
+// ---------------------------------------------------------------- tile
+
+__global__ void k_tile_plan(const int32_t* __restrict__ rowptr, int32_t n, int64_t nnz, int32_t tiles,
+                            int32_t* __restrict__ tile_row, int32_t* __restrict__ tile_nnz, int32_t* __restrict__ carry_row)
+{
+   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+   if (t > tiles) return;
+   const int64_t total = (int64_t)n + nnz;
+   const int64_t D = ::tnlb::imin64(t * kTileSize, total);
+   int64_t lo = ::tnlb::imax64(0, D - nnz), hi = ::tnlb::imin64(D, n);
+   while (lo < hi) {
+      const int64_t mid = (lo + hi) >> 1;
+      if ((int64_t)rowptr[mid + 1] <= D - mid - 1)
+         lo = mid + 1;
+      else
+         hi = mid;
+   }
+   tile_row[t] = (int32_t)lo;
+   tile_nnz[t] = (int32_t)(D - lo);
+   if (t < tiles) carry_row[t] = -1;
+}
+
+template <typename Real>
+__global__ void __launch_bounds__(kTileThreads) k_csr_tile(const int32_t* __restrict__ rowptr,
+                                                          const int32_t* __restrict__ cols,
+                                                          const Real* __restrict__ vals, const Real* __restrict__ x,
+                                                          Real* __restrict__ y, const int32_t* __restrict__ tile_row,
+                                                          const int32_t* __restrict__ tile_nnz, int32_t n,
+                                                          int32_t* __restrict__ carry_row, Real* __restrict__ carry_val,
+                                                          Real alpha, Real beta)
+{
+   __shared__ int32_t s_rowend[kTileSize + 1];
+   __shared__ Real s_prod[kTileSize];
+   __shared__ Real s_y[kTileSize];
+   __shared__ int32_t s_wkey[8];
+   __shared__ Real s_wval[8];
+   __shared__ int32_t s_pkey[8];
+   __shared__ Real s_pval[8];
+
+   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+   const int32_t t = blockIdx.x;
+   const int32_t r0 = tile_row[t], r1 = tile_row[t + 1];
+   const int32_t k0 = tile_nnz[t], k1 = tile_nnz[t + 1];
+   const int32_t nrows = r1 - r0, nk = k1 - k0, items = nrows + nk;
+
+   // Stage the nonzeros: coalesced streaming loads, products into shared memory.
+   {
+      int32_t c[kTileItems];
+      Real v[kTileItems];
+#pragma unroll
+      for (int i = 0; i < kTileItems; i++) {
+         const int32_t j = tid + i * kTileThreads;
+         if (j < nk) {
+            c[i] = ld_stream(cols + k0 + j);
+            v[i] = ld_stream(vals + k0 + j);
+         }
+      }
+#pragma unroll
+      for (int i = 0; i < kTileItems; i++) {
+         const int32_t j = tid + i * kTileThreads;
+         if (j < nk) s_prod[j] = c[i] >= 0 ? v[i] * ld_gather(x + c[i]) : Real(0);
+      }
+   }
+   // Stage the row ends of the rows ending in this tile (+ the open one).
+   for (int32_t i = tid; i <= nrows; i += kTileThreads) {
+      const int64_t r = (int64_t)r0 + i + 1;
+      s_rowend[i] = r <= n ? rowptr[r] : INT_MAX;
+   }
+   __syncthreads();
+
+   // Merge-path search for this thread's first item.
+   const int32_t d = min(tid * kTileItems, items);
+   int32_t lo = max(0, d - nk), hi = min(d, nrows);
+   while (lo < hi) {
+      const int32_t mid = (lo + hi) >> 1;
+      if (s_rowend[mid] <= k0 + d - mid - 1)
+         lo = mid + 1;
+      else
+         hi = mid;
+   }
+   int32_t xr = lo, yn = d - lo;
+   const int32_t x_start = xr;
+   const int32_t d_end = min(d + kTileItems, items);
+   Real acc = 0, first = 0;
+   bool emitted = false;
+#pragma unroll
+   for (int it = 0; it < kTileItems; it++) {
+      if (d + it < d_end) {
+         if (k0 + yn < s_rowend[xr]) {
+            acc += s_prod[yn];
+            yn++;
+         }
+         else {
+            if (emitted)
+               s_y[xr] = acc;
+            else
+               first = acc;
+            emitted = true;
+            acc = 0;
+            xr++;
+         }
+      }
+   }
+
+   // Segmented inclusive scan of (row in progress at the end, its partial).
+   const int32_t key = r0 + xr;
+   Real val = acc;
+#pragma unroll
+   for (int o = 1; o < 32; o <<= 1) {
+      const int32_t kk = __shfl_up_sync(0xffffffffu, key, o);
+      const Real vv = __shfl_up_sync(0xffffffffu, val, o);
+      if (lane >= o && kk == key) val += vv;
+   }
+   if (lane == 31) {
+      s_wkey[warp] = key;
+      s_wval[warp] = val;
+   }
+   __syncthreads();
+   if (warp == 0) {
+      int32_t wk = lane < 8 ? s_wkey[lane] : INT_MAX;
+      Real wv = lane < 8 ? s_wval[lane] : Real(0);
+#pragma unroll
+      for (int o = 1; o < 8; o <<= 1) {
+         const int32_t kk = __shfl_up_sync(0xffffffffu, wk, o);
+         const Real vv = __shfl_up_sync(0xffffffffu, wv, o);
+         if (lane >= o && kk == wk) wv += vv;
+      }
+      const int32_t ek = __shfl_up_sync(0xffffffffu, wk, 1);
+      const Real ev = __shfl_up_sync(0xffffffffu, wv, 1);
+      if (lane < 8) {
+         s_pkey[lane] = lane == 0 ? -1 : ek;
+         s_pval[lane] = lane == 0 ? Real(0) : ev;
+      }
+   }
+   __syncthreads();
+   if (key == s_pkey[warp]) val += s_pval[warp];
+   // carry-in of this thread = inclusive value of the previous thread
+   int32_t pk = __shfl_up_sync(0xffffffffu, key, 1);
+   Real pv = __shfl_up_sync(0xffffffffu, val, 1);
+   if (lane == 0) {
+      pk = s_pkey[warp];
+      pv = s_pval[warp];
+   }
+   if (emitted) s_y[x_start] = first + ((tid > 0 && pk == r0 + x_start) ? pv : Real(0));
+   if (tid == kTileThreads - 1) {
+      // open row at the tile end: does it own nonzeros in this tile?
+      const bool has = nk > 0 && (nrows == 0 || s_rowend[nrows - 1] < k1);
+      carry_row[t] = (has && key < n) ? key : -1;
+      carry_val[t] = val;
+   }
+   __syncthreads();
+   for (int32_t i = tid; i < nrows; i += kTileThreads) keep(y, r0 + i, s_y[i], alpha, beta);
+}
+
+// Adds the partial sums of rows split between tiles, in tile order.
+template <typename Real>
+__global__ void k_csr_tile_fixup(const int32_t* __restrict__ carry_row, const Real* __restrict__ carry_val,
+                                 int32_t tiles, Real* __restrict__ y, Real alpha)
+{
+   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+   if (t >= tiles) return;
+   const int32_t r = carry_row[t];
+   if (r < 0) return;
+   if (t > 0 && carry_row[t - 1] == r) return;
+   Real s = carry_val[t];
+   for (int64_t u = t + 1; u < tiles && carry_row[u] == r; u++) s += carry_val[u];
+   y[r] += (alpha == Real(1)) ? s : alpha * s;
+}
+
+// --------------------------------------------------------------- launch
+
+template <typename Real>
+tnlb_status launch_vector(const int32_t* rowptr, const int32_t* cols, const Real* vals, const Real* x, Real* y,
+                          int32_t begin, int32_t end, Real alpha, Real beta, int G, cudaStream_t st)
+{
+   const int64_t rows = (int64_t)end - begin;
+   if (rows <= 0) return TNLB_OK;
+#define TNLB_VEC(GG)                                                                                    \
+   case GG:                                                                                             \
+      k_csr_vector<Real, GG><<<grid_for(rows * GG, 256), 256, 0, st>>>(rowptr, cols, vals, x, y, begin, end, \
+                                                                         alpha, beta);                  \
+      break;
+   switch (G) {
+      case 1:
+         k_csr_scalar<Real><<<grid_for(rows, 256), 256, 0, st>>>(rowptr, cols, vals, x, y, begin, end, alpha, beta);
+         break;
+         TNLB_VEC(2)
+         TNLB_VEC(4)
+         TNLB_VEC(8)
+         TNLB_VEC(16)
+         TNLB_VEC(32)
+      case 64:
+         k_csr_block<Real, 64><<<grid_for(rows, 4), 256, 0, st>>>(rowptr, cols, vals, x, y, begin, end, alpha, beta);
+         break;
+      case 128:
+         k_csr_block<Real, 128><<<grid_for(rows, 2), 256, 0, st>>>(rowptr, cols, vals, x, y, begin, end, alpha, beta);
+         break;
+      case 256:
+         k_csr_block<Real, 256><<<grid_for(rows, 1), 256, 0, st>>>(rowptr, cols, vals, x, y, begin, end, alpha, beta);
+         break;
+      default: set_error("threads per segment must be a power of two in 1..256"); return TNLB_ERR_INVALID_ARGUMENT;
+   }
+#undef TNLB_VEC
+   TNLB_CHECK_LAUNCH();
+   return TNLB_OK;
+}
+
+// Light CSR: TPS from the mean row length (LaunchConfigurationSetter_LightCSR.h:30-58).
+int light_tps(int64_t storage, int32_t rows)
+{
+   if (rows <= 0) return 1;
+   const int64_t e = (storage + rows - 1) / rows;
+   if (e <= 2) return 2;
+   if (e <= 4) return 4;
+   if (e <= 8) return 8;
+   if (e <= 16) return 16;
+   return 32;
+}
+
+template <typename Real>
+tnlb_status spmv_csr_t(const tnlb_segments* seg, const int32_t* cols, const Real* vals, const Real* x, Real* y,
+                       Real alpha, Real beta, int32_t begin, int32_t end, tnlb_kernel kernel, int32_t tps,
+                       cudaStream_t st, int* launches)
+{
+   const int32_t* rowptr = seg->offsets.as<int32_t>();
+   const bool full = begin == 0 && end == seg->n;
+   *launches = 0;
+   if (end <= begin) return TNLB_OK;
+   switch (kernel) {
+      case TNLB_KERNEL_SCALAR:
+         *launches = 1;
+         return launch_vector<Real>(rowptr, cols, vals, x, y, begin, end, alpha, beta, 1, st);
+      case TNLB_KERNEL_VECTOR:
+         *launches = 1;
+         return launch_vector<Real>(rowptr, cols, vals, x, y, begin, end, alpha, beta, tps > 0 ? tps : 32, st);
+      case TNLB_KERNEL_LIGHT:
+         *launches = 1;
+         return launch_vector<Real>(rowptr, cols, vals, x, y, begin, end, alpha, beta,
+                                    tps > 0 ? tps : light_tps(seg->elements, seg->n), st);
+      case TNLB_KERNEL_ADAPTIVE: {
+         const int k = sizeof(Real) == 8 ? 3 : 2;
+         if (!full || seg->acsr_count[k] == 0 || seg->format != TNLB_ADAPTIVE_CSR) {
+            // the reference falls back to the CSR kernels (ReducingOperations_AdaptiveCSR.h:51-57)
+            *launches = 1;
+            return launch_vector<Real>(rowptr, cols, vals, x, y, begin, end, alpha, beta,
+                                       light_tps(seg->elements, seg->n), st);
+         }
+         const int64_t warps = seg->acsr_count[k] - 1;
+         k_csr_adaptive<Real><<<grid_for(warps, 8), 256, 0, st>>>(seg->acsr_blocks[k].as<tnlb_acsr_block>(), warps,
+                                                                  rowptr, cols, vals, x, y, alpha, beta);
+         TNLB_CHECK_LAUNCH();
+         *launches = 1;
+         return TNLB_OK;
+      }
+      case TNLB_KERNEL_DEFAULT:
+      default: {
+         if (!full || seg->tiles == 0) {
+            *launches = 1;
+            return launch_vector<Real>(rowptr, cols, vals, x, y, begin, end, alpha, beta,
+                                       light_tps(seg->elements, seg->n), st);
+         }
+         k_csr_tile<Real><<<seg->tiles, kTileThreads, 0, st>>>(
+            rowptr, cols, vals, x, y, seg->tile_row.as<int32_t>(), seg->tile_nnz.as<int32_t>(), seg->n,
+            seg->carry_row.as<int32_t>(), seg->carry_val.as<Real>(), alpha, beta);
+         TNLB_CHECK_LAUNCH();
+         k_csr_tile_fixup<Real><<<grid_for(seg->tiles, 256), 256, 0, st>>>(
+            seg->carry_row.as<int32_t>(), seg->carry_val.as<Real>(), seg->tiles, y, alpha);
+         TNLB_CHECK_LAUNCH();
+         *launches = 2;
+         return TNLB_OK;
+      }
+   }
+}
+
+}  // namespace
+
+tnlb_status build_csr_tile_plan(tnlb_segments* seg, cudaStream_t stream)
+{
+   const int64_t total = (int64_t)seg->n + seg->elements;
+   const int64_t tiles = (total + kTileSize - 1) / kTileSize;
+   TNLB_REQUIRE(tiles < INT32_MAX, TNLB_ERR_OVERFLOW, "too many tiles");
+   seg->tiles = (int32_t)tiles;
+   TNLB_TRY_STATUS(seg->tile_row.alloc(sizeof(int32_t) * (tiles + 1)));
+   TNLB_TRY_STATUS(seg->tile_nnz.alloc(sizeof(int32_t) * (tiles + 1)));
+   TNLB_TRY_STATUS(seg->carry_row.alloc(sizeof(int32_t) * (tiles + 1)));
+   TNLB_TRY_STATUS(seg->carry_val.alloc(sizeof(double) * (tiles + 1)));
+   k_tile_plan<<<grid_for(tiles + 1, 256), 256, 0, stream>>>(seg->offsets.as<int32_t>(), seg->n, seg->elements,
+                                                              (int32_t)tiles, seg->tile_row.as<int32_t>(),
+                                                              seg->tile_nnz.as<int32_t>(), seg->carry_row.as<int32_t>());
+   TNLB_CHECK_LAUNCH();
+   TNLB_CUDA_TRY(cudaStreamSynchronize(stream));
+   return TNLB_OK;
+}
+
+tnlb_status spmv_csr(const tnlb_segments* seg, tnlb_real real, const int32_t* cols, const void* vals, const void* x,
+                     void* y, double alpha, double beta, int32_t begin, int32_t end, tnlb_kernel kernel, int32_t tps,
+                     cudaStream_t stream, int* launches)
+{
+   if (real == TNLB_F64)
+      return spmv_csr_t<double>(seg, cols, (const double*)vals, (const double*)x, (double*)y, alpha, beta, begin, end,
+                                kernel, tps, stream, launches);
+   return spmv_csr_t<float>(seg, cols, (const float*)vals, (const float*)x, (float*)y, (float)alpha, (float)beta,
+                            begin, end, kernel, tps, stream, launches);
+}
+
+}  // namespace tnlb
