@@ -214,6 +214,112 @@ int32_t tnlb_spmv_last_launch_count(void);
  * ExpressionTemplates.h:372-387 (the reference copies it to the host). */
 tnlb_status tnlb_dot(tnlb_real real, int64_t n, const void* d_a, const void* d_b, double* d_result, tnlb_stream stream);
 
+/* ------------------------------------------------------------ solvers */
+
+typedef enum { TNLB_SOLVER_CG = 0, TNLB_SOLVER_BICGSTAB = 1, TNLB_SOLVER_GMRES = 2 } tnlb_solver_kind;
+/* Preconditioners: none, Diagonal (Jacobi), ILU0, and the factorised sparse
+ * approximate inverse M^-1 = G^T G (no counterpart in the reference; G on
+ * the lower triangle of A's pattern, Kolotilina-Yeremin values). */
+typedef enum { TNLB_PRECOND_NONE = 0, TNLB_PRECOND_JACOBI = 1, TNLB_PRECOND_ILU0 = 2, TNLB_PRECOND_FSAI = 3 } tnlb_precond_kind;
+
+typedef struct tnlb_precond tnlb_precond;
+/* GMRES::Variant (Solvers/Linear/GMRES.h:122-129). */
+typedef enum { TNLB_GMRES_CGS = 0, TNLB_GMRES_CGSR = 1, TNLB_GMRES_MGS = 2, TNLB_GMRES_MGSR = 3, TNLB_GMRES_CWY = 4 } tnlb_gmres_variant;
+
+/* Solver parameters: the setup() keys of IterativeSolver.hpp:14-36,
+ * GMRES.hpp:20-37 and BICGStab.hpp:14-21, with the reference's defaults
+ * filled in by tnlb_solver_params_default. */
+typedef struct {
+   int32_t max_iterations;       /* max-iterations, default 1e9 */
+   int32_t min_iterations;       /* min-iterations, default 0 */
+   double convergence_residue;   /* convergence-residue, default 1e-6 */
+   double divergence_residue;    /* divergence-residue, default DBL_MAX */
+   int32_t gmres_variant;        /* gmres-variant (tnlb_gmres_variant), default MGSR */
+   int32_t gmres_restarting_min; /* default 10 */
+   int32_t gmres_restarting_max; /* default 10 */
+   int32_t gmres_restarting_step_min; /* default 3 */
+   int32_t gmres_restarting_step_max; /* default 3 */
+   int32_t bicgstab_exact_residue;    /* default 0 */
+   int32_t spmv_kernel;          /* tnlb_kernel used by the solver's products */
+   int32_t reserved;
+} tnlb_solver_params;
+
+/* Result of a solve: getIterations(), getResidue() and the bool of solve(). */
+typedef struct {
+   int32_t converged;     /* solve() return value */
+   int32_t iterations;    /* getIterations() */
+   double residue;        /* getResidue(): the solver's stopping residue */
+   int32_t status_detail; /* 0, or a tnlb_status for breakdowns/timeouts */
+   int32_t reserved;
+} tnlb_solve_result;
+
+void tnlb_solver_params_default(tnlb_solver_params* p);
+
+/* Solve A x = b on the GPU -- LinearSolver::solve (Solvers/Linear/
+ * LinearSolver.h:157-158) of CG (CG.hpp:12-109), BICGStab (BICGStab.hpp:
+ * 34-122) or GMRES (GMRES.hpp:73-180) with the Diagonal (Jacobi,
+ * Preconditioners/Diagonal.hpp:15-43) or ILU0 (Preconditioners/ILU0.hpp:
+ * 15-140; the reference has no GPU ILU(0), ILU0.h:121-143) preconditioner.
+ * A is given by `seg` + d_cols/d_values (FP64 or FP32); b and x are device
+ * vectors of the same real type; x holds the initial guess.  Synchronous.
+ * Stopping rules follow IterativeSolver.hpp:98-143 exactly. */
+tnlb_status tnlb_solve(tnlb_solver_kind solver, tnlb_precond_kind precond, const tnlb_solver_params* params,
+                       const tnlb_segments* seg, tnlb_real real, const int32_t* d_cols, const void* d_values,
+                       const void* d_b, void* d_x, tnlb_stream stream, tnlb_solve_result* result);
+
+/* True residual ||b - A x|| / ||b|| in FP64 (Solvers/Linear/Utils/
+ * LinearResidueGetter.hpp:11-23), computed on the GPU.  Synchronous. */
+tnlb_status tnlb_true_residual(const tnlb_segments* seg, tnlb_real real, const int32_t* d_cols, const void* d_values,
+                               const void* d_b, const void* d_x, tnlb_stream stream, double* h_result);
+
+/* FP32-inner / FP64-outer iterative refinement for SPD matrices (no
+ * counterpart in the reference; BASELINE mixed-precision path): the FP64
+ * residual r = b - A x is formed with the FP64 values, normalised, rounded to
+ * FP32 and solved with Jacobi-preconditioned CG on an FP32 copy of the
+ * values to relative residual `inner_tolerance`; x += |r| d in FP64.
+ * The inner preconditioner is `inner` (an FP32 preconditioner of this
+ * matrix, e.g. a learned FSAI) or, when NULL, one of kind `inner_precond`
+ * built from the FP32 values.  Stops
+ * when ||b - A x|| / ||b|| < params->convergence_residue (the TRUE FP64
+ * residual) or after `max_outer` corrections.  result->iterations is the
+ * total number of inner CG iterations; *outer_iterations the corrections.
+ * Synchronous. */
+tnlb_status tnlb_solve_mixed(const tnlb_solver_params* params, const tnlb_segments* seg, const int32_t* d_cols,
+                             const double* d_values, const double* d_b, double* d_x, double inner_tolerance,
+                             int32_t max_outer, tnlb_precond_kind inner_precond, const tnlb_precond* inner,
+                             tnlb_stream stream, tnlb_solve_result* result, int32_t* outer_iterations);
+
+/* Build a preconditioner for a matrix -- Preconditioner::update
+ * (Preconditioners/Preconditioner.h:96-110; Diagonal.hpp:15-36,
+ * ILU0.hpp:15-118).  The values must stay valid while it is used.
+ * Blocks until built. */
+tnlb_status tnlb_precond_create(tnlb_precond_kind kind, const tnlb_segments* seg, tnlb_real real,
+                                const int32_t* d_cols, const void* d_values, tnlb_stream stream,
+                                tnlb_precond** out);
+
+/* x = M^{-1} b -- Preconditioner::solve (Diagonal.hpp:40-43,
+ * ILU0.hpp:121-140).  Synchronous. */
+tnlb_status tnlb_precond_solve(const tnlb_precond* precond, const void* d_b, void* d_x, tnlb_stream stream);
+
+/* Release a preconditioner.  Accepts NULL. */
+tnlb_status tnlb_precond_destroy(tnlb_precond* precond);
+
+/* tnlb_solve with a preconditioner built beforehand (NULL = none):
+ * LinearSolver::setPreconditioner (LinearSolver.h:133-137) then solve. */
+tnlb_status tnlb_solve_preconditioned(tnlb_solver_kind solver, const tnlb_precond* precond,
+                                      const tnlb_solver_params* params, const tnlb_segments* seg, tnlb_real real,
+                                      const int32_t* d_cols, const void* d_values, const void* d_b, void* d_x,
+                                      tnlb_stream stream, tnlb_solve_result* result);
+
+/* The ILU(0) factors computed on the GPU, copied to host memory: CSR pattern
+ * of A (h_rowptr n+1, h_cols nnz) with L strictly below the diagonal (unit
+ * diagonal implied) and U from the diagonal on in h_values (ILU0.hpp:15-118;
+ * the reference stores U's rows in reverse order, the values are the same).
+ * `capacity` bounds h_cols/h_values.  Synchronous. */
+tnlb_status tnlb_ilu0_factors(const tnlb_segments* seg, tnlb_real real, const int32_t* d_cols, const void* d_values,
+                              int32_t* h_rowptr, int32_t* h_cols, void* h_values, int64_t capacity,
+                              tnlb_stream stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,185 @@
+"""GPU Krylov solvers against the oracle (CG.hpp, BICGStab.hpp, GMRES.hpp
+restated in oracle/tnl_oracle.c and pinned to the reference).
+
+* ILU(0) factors and both preconditioner applications: bit-exact.
+* CG / GMRES: the same iteration count as the oracle within 2 (the GPU sums
+  dot products in another order), converged flags equal, the true FP64
+  residual below the tolerance scale, and x close to the oracle's x.
+* BiCGStab: within the spread the reference itself shows between OpenMP
+  thread counts.
+* Mixed precision (FP32 inner CG, FP64 refinement): true residual < tol.
+"""
+import numpy as np
+import pytest
+import torch
+
+from helpers import FORMATS
+
+pytestmark = pytest.mark.gpu
+
+
+def tnl():
+    import tnl_b200
+
+    return tnl_b200
+
+
+def problems():
+    from tnl_b200 import generators as g
+
+    return {"laplacian48": g.laplacian_2d(48), "diffusion40": g.diffusion_2d(40, 0.1, 1.0, 3)}
+
+
+def gpu_solve(kind, A, b, precond, fmt="CSR", real=torch.float64, tol=1e-8, maxit=20000, variant="MGSR", m=30, x0=None):
+    t = tnl()
+    M = t.SparseMatrix(t.FORMATS[fmt], real).assign(A.rowptr, A.cols, A.vals.astype(np.float64 if real == torch.float64 else np.float32))
+    S = {"cg": t.CG, "bicgstab": t.BICGStab, "gmres": t.GMRES}[kind]()
+    S.setMatrix(M)
+    S.setup({"convergence-residue": tol, "max-iterations": maxit, "gmres-variant": variant,
+             "gmres-restarting-min": m, "gmres-restarting-max": m})
+    if precond == 1:
+        P = t.Diagonal()
+        P.update(M)
+        S.setPreconditioner(P)
+    elif precond == 2:
+        P = t.ILU0()
+        P.update(M)
+        S.setPreconditioner(P)
+    bs = torch.tensor(b, dtype=real, device="cuda")
+    xs = torch.zeros(A.n, dtype=real, device="cuda") if x0 is None else torch.tensor(x0, dtype=real, device="cuda")
+    ok = S.solve(bs, xs)
+    return ok, S.getIterations(), S.getResidue(), xs.cpu().numpy().astype(np.float64), t.true_residual(M, bs, xs)
+
+
+def test_ilu0_factors_bit_exact(oracle):
+    from tnl_b200 import generators as g
+
+    t = tnl()
+    for A in (g.laplacian_2d(30), g.diffusion_2d(25, 0.1, 1.5, 4), g.convection_diffusion_3d(8)):
+        M = t.SparseMatrix(t.CSR, torch.float64).assign(A.rowptr, A.cols, A.vals)
+        P = t.ILU0()
+        P.update(M)
+        rp, cols, vals = P.factors()
+        Lp, Lc, Lv, Up, Uc, Uv = oracle.ilu0(A)
+        n = A.n
+        for i in range(n):
+            row_c = cols[rp[i]:rp[i + 1]]
+            row_v = vals[rp[i]:rp[i + 1]]
+            nl = Lp[i + 1] - Lp[i]
+            ui = n - 1 - i
+            assert np.array_equal(row_c[:nl], Lc[Lp[i]:Lp[i + 1]])
+            assert np.array_equal(row_v[:nl], Lv[Lp[i]:Lp[i + 1]]), i
+            assert np.array_equal(row_c[nl:], Uc[Up[ui]:Up[ui + 1]])
+            assert np.array_equal(row_v[nl:], Uv[Up[ui]:Up[ui + 1]]), i
+
+
+@pytest.mark.parametrize("kind", [1, 2])
+def test_preconditioner_apply_bit_exact(oracle, kind):
+    from tnl_b200 import generators as g
+
+    t = tnl()
+    A = g.diffusion_2d(33, 0.1, 2.0, 6)
+    b = g.uniform_vector(A.n, 2)
+    M = t.SparseMatrix(t.CSR, torch.float64).assign(A.rowptr, A.cols, A.vals)
+    P = (t.Diagonal if kind == 1 else t.ILU0)()
+    P.update(M)
+    bs = torch.tensor(b, device="cuda")
+    xs = torch.empty_like(bs)
+    P.solve(bs, xs)
+    assert np.array_equal(xs.cpu().numpy(), oracle.prec_apply(A, kind, b))
+
+
+@pytest.mark.parametrize("kind,precond", [("cg", 0), ("cg", 1), ("cg", 2), ("gmres", 1), ("gmres", 2), ("gmres", 0)])
+@pytest.mark.parametrize("pname", ["laplacian48", "diffusion40"])
+def test_solver_matches_oracle(oracle, kind, precond, pname):
+    from tnl_b200 import generators as g
+
+    A = problems()[pname]
+    b = g.uniform_vector(A.n, 1)
+    o = oracle.solve(kind, A, b, precond=precond, tol=1e-8, maxit=20000, gmres_m=30, gmres_reorth=2)
+    ok, it, res, x, tr = gpu_solve(kind, A, b, precond)
+    assert ok == o["converged"]
+    assert abs(it - o["iterations"]) <= 2, (it, o["iterations"])
+    assert res < 1e-8
+    assert tr < 1e-6
+    assert np.max(np.abs(x - o["x"])) <= 1e-5 * max(1.0, np.max(np.abs(o["x"])))
+
+
+@pytest.mark.parametrize("variant", ["CGS", "CGSR", "MGS", "MGSR"])
+def test_gmres_variants(oracle, variant):
+    from tnl_b200 import generators as g
+
+    A = g.convection_diffusion_3d(12)
+    b = g.uniform_vector(A.n, 1)
+    reorth = 2 if variant.endswith("R") else 1
+    if variant.startswith("MGS"):
+        o = oracle.solve("gmres", A, b, precond=1, tol=1e-8, maxit=5000, gmres_m=20, gmres_reorth=reorth)
+    ok, it, res, x, tr = gpu_solve("gmres", A, b, 1, tol=1e-8, maxit=5000, variant=variant, m=20)
+    assert ok and res < 1e-8 and tr < 1e-6
+    if variant.startswith("MGS"):
+        assert abs(it - o["iterations"]) <= 2
+
+
+@pytest.mark.parametrize("precond", [1, 2])
+def test_bicgstab(oracle, precond):
+    from tnl_b200 import generators as g
+
+    A = problems()["diffusion40"]
+    b = g.uniform_vector(A.n, 1)
+    o = oracle.solve("bicgstab", A, b, precond=precond, tol=1e-8, maxit=20000)
+    ok, it, res, x, tr = gpu_solve("bicgstab", A, b, precond)
+    assert ok and o["converged"]
+    assert abs(it - o["iterations"]) <= max(5, o["iterations"] // 10), (it, o["iterations"])
+    assert tr < 1e-6
+
+
+@pytest.mark.parametrize("fmt", ["SlicedEllpack", "Ellpack", "ChunkedEllpack", "BiEllpack", "AdaptiveCSR"])
+def test_cg_on_every_format(oracle, fmt):
+    from tnl_b200 import generators as g
+
+    A = problems()["diffusion40"]
+    b = g.uniform_vector(A.n, 1)
+    o = oracle.solve("cg", A, b, precond=1, tol=1e-8, maxit=20000)
+    ok, it, res, x, tr = gpu_solve("cg", A, b, 1, fmt=fmt)
+    assert ok and abs(it - o["iterations"]) <= 2
+
+
+def test_cg_fp32():
+    from tnl_b200 import generators as g
+
+    A = g.laplacian_2d(40)
+    b = g.uniform_vector(A.n, 1)
+    ok, it, res, x, tr = gpu_solve("cg", A, b, 1, real=torch.float32, tol=1e-5)
+    assert ok and res < 1e-5
+
+
+def test_zero_rhs_gives_zero_solution():
+    from tnl_b200 import generators as g
+
+    A = g.laplacian_2d(16)
+    ok, it, res, x, tr = gpu_solve("cg", A, np.zeros(A.n), 1, x0=np.ones(A.n))
+    assert ok and it == 0 and np.all(x == 0)
+
+
+def test_max_iterations_reports_failure():
+    from tnl_b200 import generators as g
+
+    A = g.laplacian_2d(64)
+    b = g.uniform_vector(A.n, 1)
+    ok, it, res, x, tr = gpu_solve("cg", A, b, 1, maxit=10)
+    assert not ok and it == 11 and res > 1e-8
+
+
+def test_mixed_precision_refinement_reaches_fp64_residual(oracle):
+    from tnl_b200 import generators as g
+
+    t = tnl()
+    A = g.diffusion_2d(128, 0.1, 2.0, 7)
+    b = g.uniform_vector(A.n, 1)
+    M = t.SparseMatrix(t.CSR, torch.float64).assign(A.rowptr, A.cols, A.vals)
+    bs = torch.tensor(b, device="cuda")
+    xs = torch.zeros(A.n, dtype=torch.float64, device="cuda")
+    r = t.solve_mixed(M, bs, xs, tol=1e-10, inner_tol=1e-4)
+    assert r["converged"] and r["true_residual"] < 1e-10
+    assert t.true_residual(M, bs, xs) < 1e-10
+    assert oracle.true_residual(A, b, xs.cpu().numpy()) < 1e-10

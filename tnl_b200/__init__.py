@@ -31,6 +31,7 @@ from .generators import CSRMatrix  # noqa: F401
 __all__ = [
     "CSR", "Ellpack", "SlicedEllpack", "ChunkedEllpack", "BiEllpack", "AdaptiveCSR", "SparseMatrix",
     "LaunchConfiguration", "ColumnMajorOrder", "RowMajorOrder", "CSRMatrix", "check", "BackendRuntimeError",
+    "CG", "BICGStab", "GMRES", "Diagonal", "ILU0", "FSAI", "solve_mixed", "true_residual",
 ]
 
 ColumnMajorOrder = capi.COLUMN_MAJOR
@@ -342,3 +343,204 @@ def dot(a: torch.Tensor, b: torch.Tensor) -> torch.Tensor:
     out = torch.empty(1, dtype=torch.float64, device="cuda")
     check(capi.tnlb_dot(_real_code(a.dtype), a.numel(), a.data_ptr(), b.data_ptr(), out.data_ptr(), _stream()))
     return out
+
+
+# ----------------------------------------------------------------- solvers
+
+class _Preconditioner:
+    KIND = capi.PRECOND_NONE
+
+    def __init__(self):
+        self.matrix = None
+        self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            if self._h:
+                capi.tnlb_precond_destroy(self._h)
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def update(self, matrix: SparseMatrix) -> None:
+        """Preconditioner::update (Preconditioners/Preconditioner.h:96-110)."""
+        if matrix.getRows() == 0:
+            raise ValueError(f"{type(self).__name__}::update: the matrix is empty")
+        if matrix.getRows() != matrix.getColumns():
+            raise ValueError(f"{type(self).__name__}::update: matrix must be square")
+        if self._h:
+            capi.tnlb_precond_destroy(self._h)
+            self._h = C.c_void_p()
+        h = C.c_void_p()
+        check(capi.tnlb_precond_create(self.KIND, matrix.segments.handle, _real_code(matrix.real),
+                                       matrix.columnIndexes.data_ptr(), matrix.values.data_ptr(), _stream(),
+                                       C.byref(h)))
+        self._h = h
+        self.matrix = matrix
+
+    def solve(self, b: torch.Tensor, x: torch.Tensor) -> None:
+        """Preconditioner::solve: x = M^{-1} b."""
+        check(capi.tnlb_precond_solve(self._h, b.data_ptr(), x.data_ptr(), _stream()))
+
+
+class Diagonal(_Preconditioner):
+    """Solvers::Linear::Preconditioners::Diagonal (Jacobi)."""
+    KIND = capi.PRECOND_JACOBI
+
+
+class FSAI(_Preconditioner):
+    """Factorised sparse approximate inverse M^-1 = G^T G, G on the lower
+    triangle of A's pattern with Kolotilina-Yeremin values (no counterpart in
+    the reference)."""
+    KIND = capi.PRECOND_FSAI
+
+
+class ILU0(_Preconditioner):
+    """Solvers::Linear::Preconditioners::ILU0 (on the GPU)."""
+    KIND = capi.PRECOND_ILU0
+
+    def factors(self):
+        """(rowptr, cols, values) of L (strictly lower, unit diagonal implied) and U on A's pattern."""
+        M = self.matrix
+        n = M.getRows()
+        cap = M.getValues().numel()
+        rp = np.zeros(n + 1, np.int32)
+        cols = np.zeros(max(cap, 1), np.int32)
+        vals = np.zeros(max(cap, 1), np.float64 if M.real == torch.float64 else np.float32)
+        check(capi.tnlb_ilu0_factors(M.segments.handle, _real_code(M.real), M.columnIndexes.data_ptr(),
+                                     M.values.data_ptr(), rp.ctypes.data, cols.ctypes.data, vals.ctypes.data, cap,
+                                     _stream()))
+        nnz = int(rp[-1])
+        return rp, cols[:nnz], vals[:nnz]
+
+
+class _LinearSolver:
+    """LinearSolver + IterativeSolver (Solvers/Linear/LinearSolver.h, Solvers/IterativeSolver.h)."""
+    KIND = capi.SOLVER_CG
+
+    def __init__(self):
+        self.params = capi.SolverParams()
+        capi.tnlb_solver_params_default(C.byref(self.params))
+        self.matrix = None
+        self.preconditioner = None
+        self.iterations = 0
+        self.residue = 0.0
+
+    def setMatrix(self, matrix: SparseMatrix) -> None:
+        if matrix.getRows() != matrix.getColumns():
+            raise ValueError("LinearSolver::setMatrix: matrix must be square")
+        self.matrix = matrix
+
+    def setPreconditioner(self, preconditioner) -> None:
+        self.preconditioner = preconditioner
+
+    def setConvergenceResidue(self, r: float) -> None:
+        self.params.convergence_residue = r
+
+    def setDivergenceResidue(self, r: float) -> None:
+        self.params.divergence_residue = r
+
+    def setMaxIterations(self, n: int) -> None:
+        self.params.max_iterations = n
+
+    def setMinIterations(self, n: int) -> None:
+        self.params.min_iterations = n
+
+    def getIterations(self) -> int:
+        return self.iterations
+
+    def getResidue(self) -> float:
+        return self.residue
+
+    def setup(self, parameters: dict, prefix: str = "") -> bool:
+        """setup(ParameterContainer) with the reference's keys (IterativeSolver.hpp:14-36,
+        GMRES.hpp:20-37, BICGStab.hpp:14-21)."""
+        p = self.params
+        g = lambda k: parameters.get(prefix + k)  # noqa: E731
+        if g("max-iterations") is not None:
+            p.max_iterations = int(g("max-iterations"))
+        if g("min-iterations") is not None:
+            p.min_iterations = int(g("min-iterations"))
+        if g("convergence-residue") is not None:
+            p.convergence_residue = float(g("convergence-residue"))
+        if g("divergence-residue") is not None:
+            p.divergence_residue = float(g("divergence-residue"))
+        if g("gmres-variant") is not None:
+            p.gmres_variant = {"CGS": 0, "CGSR": 1, "MGS": 2, "MGSR": 3, "CWY": 4}[g("gmres-variant")]
+        for key, field in (("gmres-restarting-min", "gmres_restarting_min"),
+                           ("gmres-restarting-max", "gmres_restarting_max"),
+                           ("gmres-restarting-step-min", "gmres_restarting_step_min"),
+                           ("gmres-restarting-step-max", "gmres_restarting_step_max")):
+            if g(key) is not None:
+                setattr(p, field, int(g(key)))
+        if g("bicgstab-exact-residue") is not None:
+            p.bicgstab_exact_residue = int(bool(g("bicgstab-exact-residue")))
+        return True
+
+    def solve(self, b: torch.Tensor, x: torch.Tensor) -> bool:
+        """LinearSolver::solve(b, x): x holds the initial guess; returns the convergence flag."""
+        M = self.matrix
+        if M is None:
+            raise RuntimeError("No matrix was set. Call setMatrix() before solve().")
+        if b.numel() != M.getRows() or x.numel() != M.getRows():
+            raise ValueError("solve: vector sizes do not match the matrix")
+        ph = self.preconditioner.handle if self.preconditioner is not None else None
+        r = capi.SolveResult()
+        check(capi.tnlb_solve_preconditioned(self.KIND, ph, C.byref(self.params), M.segments.handle,
+                                             _real_code(M.real), M.columnIndexes.data_ptr(), M.values.data_ptr(),
+                                             b.data_ptr(), x.data_ptr(), _stream(), C.byref(r)))
+        self.iterations = r.iterations
+        self.residue = r.residue
+        return bool(r.converged)
+
+
+class CG(_LinearSolver):
+    """Solvers::Linear::CG."""
+    KIND = capi.SOLVER_CG
+
+
+class BICGStab(_LinearSolver):
+    """Solvers::Linear::BICGStab."""
+    KIND = capi.SOLVER_BICGSTAB
+
+
+class GMRES(_LinearSolver):
+    """Solvers::Linear::GMRES (restarted, left-preconditioned; CGS, CGSR, MGS, MGSR)."""
+    KIND = capi.SOLVER_GMRES
+
+
+def true_residual(M: SparseMatrix, b: torch.Tensor, x: torch.Tensor) -> float:
+    """||b - A x|| / ||b|| in FP64 on the GPU (Utils/LinearResidueGetter.hpp:11-23)."""
+    out = C.c_double()
+    check(capi.tnlb_true_residual(M.segments.handle, _real_code(M.real), M.columnIndexes.data_ptr(),
+                                  M.values.data_ptr(), b.data_ptr(), x.data_ptr(), _stream(), C.byref(out)))
+    return out.value
+
+
+def solve_mixed(M: SparseMatrix, b: torch.Tensor, x: torch.Tensor, tol: float = 1e-8, inner_tol: float = 1e-4,
+                max_outer: int = 50, max_iterations: int = 1000000000, inner: str | _Preconditioner = "jacobi") -> dict:
+    """FP32 PCG inside FP64 iterative refinement (SPD matrices, FP64 matrix and vectors).
+
+    ``inner`` is "jacobi", "fsai", "ilu0", "none", or an FP32 preconditioner
+    object built for an FP32 copy of the matrix (e.g. a learned FSAI).
+    """
+    if M.real != torch.float64:
+        raise TypeError("solve_mixed takes an FP64 matrix")
+    p = capi.SolverParams()
+    capi.tnlb_solver_params_default(C.byref(p))
+    p.convergence_residue = tol
+    p.max_iterations = max_iterations
+    r = capi.SolveResult()
+    outer = C.c_int32()
+    kinds = {"none": capi.PRECOND_NONE, "jacobi": capi.PRECOND_JACOBI, "ilu0": capi.PRECOND_ILU0,
+             "fsai": capi.PRECOND_FSAI}
+    kind = kinds.get(inner, capi.PRECOND_JACOBI) if isinstance(inner, str) else capi.PRECOND_NONE
+    handle = None if isinstance(inner, str) else inner.handle
+    check(capi.tnlb_solve_mixed(C.byref(p), M.segments.handle, M.columnIndexes.data_ptr(), M.values.data_ptr(),
+                                b.data_ptr(), x.data_ptr(), inner_tol, max_outer, kind, handle, _stream(), C.byref(r),
+                                C.byref(outer)))
+    return {"converged": bool(r.converged), "inner_iterations": r.iterations, "outer_iterations": outer.value,
+            "true_residual": r.residue}

@@ -13,7 +13,7 @@ LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libtnlb200.so"
 
 if not LIB_PATH.exists():
     raise ImportError(
-        f"{LIB_PATH} is missing: build the CUDA library with `python -m tnl_b200.build` "
+        f"{LIB_PATH} is missing: build the CUDA library with `python tnl_b200/build.py` "
         "(or __graft_entry__.build()); there is no CPU fallback"
     )
 
@@ -57,6 +57,25 @@ class AcsrBlock(C.Structure):
     ]
 
 
+class SolverParams(C.Structure):
+    _fields_ = [
+        ("max_iterations", C.c_int32), ("min_iterations", C.c_int32), ("convergence_residue", C.c_double),
+        ("divergence_residue", C.c_double), ("gmres_variant", C.c_int32), ("gmres_restarting_min", C.c_int32),
+        ("gmres_restarting_max", C.c_int32), ("gmres_restarting_step_min", C.c_int32),
+        ("gmres_restarting_step_max", C.c_int32), ("bicgstab_exact_residue", C.c_int32), ("spmv_kernel", C.c_int32),
+        ("reserved", C.c_int32),
+    ]
+
+
+class SolveResult(C.Structure):
+    _fields_ = [("converged", C.c_int32), ("iterations", C.c_int32), ("residue", C.c_double),
+                ("status_detail", C.c_int32), ("reserved", C.c_int32)]
+
+
+SOLVER_CG, SOLVER_BICGSTAB, SOLVER_GMRES = range(3)
+PRECOND_NONE, PRECOND_JACOBI, PRECOND_ILU0, PRECOND_FSAI = range(4)
+GMRES_CGS, GMRES_CGSR, GMRES_MGS, GMRES_MGSR, GMRES_CWY = range(5)
+
 _p = C.c_void_p
 _i32, _i64, _f64 = C.c_int32, C.c_int64, C.c_double
 
@@ -80,6 +99,18 @@ tnlb_matrix_fill_from_csr = _sig("tnlb_matrix_fill_from_csr", [_p, C.c_int, _p, 
 tnlb_spmv = _sig("tnlb_spmv", [_p, C.c_int, _p, _p, _i32, _p, _p, _f64, _f64, _i32, _i32, C.c_int, _i32, _p])
 tnlb_spmv_last_launch_count = _sig("tnlb_spmv_last_launch_count", [], _i32)
 tnlb_dot = _sig("tnlb_dot", [C.c_int, _i64, _p, _p, _p, _p])
+tnlb_solver_params_default = _sig("tnlb_solver_params_default", [C.POINTER(SolverParams)], None)
+tnlb_solve = _sig("tnlb_solve", [C.c_int, C.c_int, C.POINTER(SolverParams), _p, C.c_int, _p, _p, _p, _p, _p,
+                                 C.POINTER(SolveResult)])
+tnlb_true_residual = _sig("tnlb_true_residual", [_p, C.c_int, _p, _p, _p, _p, _p, C.POINTER(_f64)])
+tnlb_solve_mixed = _sig("tnlb_solve_mixed", [C.POINTER(SolverParams), _p, _p, _p, _p, _p, _f64, _i32, C.c_int, _p,
+                                             _p, C.POINTER(SolveResult), C.POINTER(_i32)])
+tnlb_precond_create = _sig("tnlb_precond_create", [C.c_int, _p, C.c_int, _p, _p, _p, C.POINTER(_p)])
+tnlb_precond_solve = _sig("tnlb_precond_solve", [_p, _p, _p, _p])
+tnlb_precond_destroy = _sig("tnlb_precond_destroy", [_p])
+tnlb_solve_preconditioned = _sig("tnlb_solve_preconditioned", [C.c_int, _p, C.POINTER(SolverParams), _p, C.c_int, _p,
+                                                               _p, _p, _p, _p, C.POINTER(SolveResult)])
+tnlb_ilu0_factors = _sig("tnlb_ilu0_factors", [_p, C.c_int, _p, _p, _p, _p, _p, _i64, _p])
 
 
 def check(status: int) -> None:

@@ -1,7 +1,7 @@
 """Build libtnlb200.so (all CUDA sources under csrc/) for sm_100a, in-tree.
 
-    python -m tnl_b200.build          # incremental
-    python -m tnl_b200.build --clean  # rebuild everything
+    python tnl_b200/build.py          # incremental
+    python tnl_b200/build.py --clean  # rebuild everything
 
 Objects go to tnl_b200/_build/, the library to tnl_b200/_lib/libtnlb200.so
 (both git-ignored; the built library travels with the working tree).

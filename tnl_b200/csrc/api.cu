@@ -1,6 +1,7 @@
 // api.cu -- the extern "C" entry points of libtnlb200.so declared in
 // include/tnlb200.h.  No entry point throws; failures return a status and
 // leave a message for tnlb_last_error().
+#include <cfloat>
 #include <new>
 
 #include "internal.cuh"
@@ -261,6 +262,136 @@ tnlb_status tnlb_dot(tnlb_real real, int64_t n, const void* d_a, const void* d_b
       k_dot<float><<<g, 256, 0, st>>>(n, (const float*)d_a, (const float*)d_b, d_result);
    TNLB_CHECK_LAUNCH();
    return TNLB_OK;
+}
+
+void tnlb_solver_params_default(tnlb_solver_params* p)
+{
+   if (!p) return;
+   *p = tnlb_solver_params{};
+   p->max_iterations = 1000000000;    // IterativeSolver.h:226
+   p->min_iterations = 0;             // :228
+   p->convergence_residue = 1e-6;     // :232
+   p->divergence_residue = DBL_MAX;   // :235
+   p->gmres_variant = TNLB_GMRES_MGSR;  // GMRES.hpp:23 (configSetup default)
+   p->gmres_restarting_min = 10;      // GMRES.h:226
+   p->gmres_restarting_max = 10;      // GMRES.h:227
+   p->gmres_restarting_step_min = 3;  // GMRES.h:228
+   p->gmres_restarting_step_max = 3;  // GMRES.h:229
+   p->bicgstab_exact_residue = 0;     // BICGStab.h:102
+   p->spmv_kernel = TNLB_KERNEL_DEFAULT;
+}
+
+static tnlb_status check_solve_args(const tnlb_segments* seg, tnlb_real real, const void* b, void* x)
+{
+   TNLB_REQUIRE(seg != nullptr, TNLB_ERR_INVALID_ARGUMENT, "null segments");
+   TNLB_REQUIRE(real == TNLB_F32 || real == TNLB_F64, TNLB_ERR_INVALID_ARGUMENT, "unknown real type");
+   TNLB_REQUIRE(seg->n > 0, TNLB_ERR_INVALID_ARGUMENT, "LinearSolver::setMatrix: the matrix is empty");
+   TNLB_REQUIRE(b && x, TNLB_ERR_INVALID_ARGUMENT, "null vector");
+   return TNLB_OK;
+}
+
+tnlb_status tnlb_solve_preconditioned(tnlb_solver_kind solver, const tnlb_precond* precond,
+                                      const tnlb_solver_params* params, const tnlb_segments* seg, tnlb_real real,
+                                      const int32_t* d_cols, const void* d_values, const void* d_b, void* d_x,
+                                      tnlb_stream stream, tnlb_solve_result* result)
+{
+   clear_error();
+   TNLB_TRY_STATUS(check_solve_args(seg, real, d_b, d_x));
+   TNLB_REQUIRE(result != nullptr, TNLB_ERR_INVALID_ARGUMENT, "null result");
+   TNLB_REQUIRE(solver >= TNLB_SOLVER_CG && solver <= TNLB_SOLVER_GMRES, TNLB_ERR_INVALID_ARGUMENT, "unknown solver");
+   tnlb_solver_params p;
+   tnlb_solver_params_default(&p);
+   if (params) p = *params;
+   *result = tnlb_solve_result{};
+   tnlb_status s = tnlb::solve(solver, precond, p, seg, real, d_cols, d_values, d_b, d_x, (cudaStream_t)stream, result);
+   if (s != TNLB_OK) result->status_detail = s;
+   return s;
+}
+
+tnlb_status tnlb_solve(tnlb_solver_kind solver, tnlb_precond_kind precond, const tnlb_solver_params* params,
+                       const tnlb_segments* seg, tnlb_real real, const int32_t* d_cols, const void* d_values,
+                       const void* d_b, void* d_x, tnlb_stream stream, tnlb_solve_result* result)
+{
+   clear_error();
+   TNLB_TRY_STATUS(check_solve_args(seg, real, d_b, d_x));
+   TNLB_REQUIRE(precond >= TNLB_PRECOND_NONE && precond <= TNLB_PRECOND_FSAI, TNLB_ERR_INVALID_ARGUMENT,
+                "unknown preconditioner");
+   tnlb_precond* P = nullptr;
+   if (precond != TNLB_PRECOND_NONE)
+      TNLB_TRY_STATUS(tnlb::precond_create(precond, seg, real, d_cols, d_values, (cudaStream_t)stream, &P));
+   tnlb_status s = tnlb_solve_preconditioned(solver, P, params, seg, real, d_cols, d_values, d_b, d_x, stream, result);
+   delete P;
+   return s;
+}
+
+tnlb_status tnlb_true_residual(const tnlb_segments* seg, tnlb_real real, const int32_t* d_cols, const void* d_values,
+                               const void* d_b, const void* d_x, tnlb_stream stream, double* h_result)
+{
+   clear_error();
+   TNLB_TRY_STATUS(check_solve_args(seg, real, d_b, (void*)d_x));
+   TNLB_REQUIRE(h_result != nullptr, TNLB_ERR_INVALID_ARGUMENT, "null result");
+   return tnlb::true_residual(seg, real, d_cols, d_values, d_b, d_x, (cudaStream_t)stream, h_result);
+}
+
+tnlb_status tnlb_solve_mixed(const tnlb_solver_params* params, const tnlb_segments* seg, const int32_t* d_cols,
+                             const double* d_values, const double* d_b, double* d_x, double inner_tolerance,
+                             int32_t max_outer, tnlb_precond_kind inner_precond, const tnlb_precond* inner,
+                             tnlb_stream stream, tnlb_solve_result* result, int32_t* outer_iterations)
+{
+   clear_error();
+   TNLB_TRY_STATUS(check_solve_args(seg, TNLB_F64, d_b, d_x));
+   TNLB_REQUIRE(result && outer_iterations, TNLB_ERR_INVALID_ARGUMENT, "null result");
+   TNLB_REQUIRE(inner_tolerance > 0 && inner_tolerance < 1, TNLB_ERR_INVALID_ARGUMENT,
+                "inner tolerance must lie in (0, 1)");
+   TNLB_REQUIRE(max_outer >= 0, TNLB_ERR_INVALID_ARGUMENT, "negative max_outer");
+   TNLB_REQUIRE(inner || (inner_precond >= TNLB_PRECOND_NONE && inner_precond <= TNLB_PRECOND_FSAI),
+                TNLB_ERR_INVALID_ARGUMENT, "unknown preconditioner");
+   tnlb_solver_params p;
+   tnlb_solver_params_default(&p);
+   if (params) p = *params;
+   int32_t inner_its = 0;
+   *result = tnlb_solve_result{};
+   return tnlb::solve_mixed_cg(seg, d_cols, d_values, d_b, d_x, p, inner_tolerance, max_outer, (cudaStream_t)stream,
+                               result, &inner_its, outer_iterations, inner_precond, inner);
+}
+
+tnlb_status tnlb_precond_create(tnlb_precond_kind kind, const tnlb_segments* seg, tnlb_real real,
+                                const int32_t* d_cols, const void* d_values, tnlb_stream stream, tnlb_precond** out)
+{
+   clear_error();
+   TNLB_REQUIRE(seg && out, TNLB_ERR_INVALID_ARGUMENT, "null argument");
+   TNLB_REQUIRE(real == TNLB_F32 || real == TNLB_F64, TNLB_ERR_INVALID_ARGUMENT, "unknown real type");
+   TNLB_REQUIRE(kind >= TNLB_PRECOND_NONE && kind <= TNLB_PRECOND_FSAI, TNLB_ERR_INVALID_ARGUMENT,
+                "unknown preconditioner");
+   *out = nullptr;
+   return tnlb::precond_create(kind, seg, real, d_cols, d_values, (cudaStream_t)stream, out);
+}
+
+tnlb_status tnlb_precond_solve(const tnlb_precond* precond, const void* d_b, void* d_x, tnlb_stream stream)
+{
+   clear_error();
+   TNLB_REQUIRE(precond && d_b && d_x, TNLB_ERR_INVALID_ARGUMENT, "null argument");
+   return tnlb::precond_apply(precond, d_b, d_x, (cudaStream_t)stream);
+}
+
+tnlb_status tnlb_precond_destroy(tnlb_precond* precond)
+{
+   clear_error();
+   delete precond;
+   return TNLB_OK;
+}
+
+tnlb_status tnlb_ilu0_factors(const tnlb_segments* seg, tnlb_real real, const int32_t* d_cols, const void* d_values,
+                              int32_t* h_rowptr, int32_t* h_cols, void* h_values, int64_t capacity,
+                              tnlb_stream stream)
+{
+   clear_error();
+   TNLB_REQUIRE(seg != nullptr && h_rowptr && h_cols && h_values, TNLB_ERR_INVALID_ARGUMENT, "null argument");
+   void* ilu = nullptr;
+   tnlb_status s = tnlb::ilu0_create(seg, real, d_cols, d_values, (cudaStream_t)stream, &ilu);
+   if (s == TNLB_OK) s = tnlb::ilu0_read(ilu, h_rowptr, h_cols, h_values, capacity, real == TNLB_F64 ? 8 : 4);
+   if (ilu) tnlb::ilu0_destroy(ilu);
+   return s;
 }
 
 }  // extern "C"

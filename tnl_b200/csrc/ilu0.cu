@@ -1,0 +1,326 @@
+// ilu0.cu -- ILU(0) preconditioner on the GPU.
+//
+// The reference implements ILU(0) on the host only; its CUDA specialisation
+// throws NotImplementedError (Solvers/Linear/Preconditioners/ILU0.h:121-143).
+// Here the factorisation and both triangular solves run on the GPU,
+// scheduled by dependency levels: row i of L depends on the rows j < i it
+// references, row i of U on the rows j > i.  Levels are computed once on the
+// host (one pass over the pattern in row order), rows of a level run in
+// parallel, one kernel launch per level; the solves are captured once in a
+// CUDA graph and replayed.
+//
+// Arithmetic per row follows ILU0.hpp:59-118 (IKJ order, L_ik = A_ik/U_kk,
+// then the updates of the rest of L_i and of U_i with U(k, j) looked up in
+// row k of U, 0 if absent) and Utils/TriangularSolve.h:20-103 (ascending
+// column order, unit-diagonal L), with separately rounded multiply and
+// subtract, so the factors and the solves are bit-identical to the Host.
+#include <algorithm>
+#include <vector>
+
+#include "internal.cuh"
+#include "segview.cuh"
+
+namespace tnlb {
+namespace {
+
+template <typename Real>
+__device__ __forceinline__ Real mul_rn(Real a, Real b);
+template <>
+__device__ __forceinline__ double mul_rn<double>(double a, double b)
+{
+   return __dmul_rn(a, b);
+}
+template <>
+__device__ __forceinline__ float mul_rn<float>(float a, float b)
+{
+   return __fmul_rn(a, b);
+}
+template <typename Real>
+__device__ __forceinline__ Real sub_rn(Real a, Real b);
+template <>
+__device__ __forceinline__ double sub_rn<double>(double a, double b)
+{
+   return __dsub_rn(a, b);
+}
+template <>
+__device__ __forceinline__ float sub_rn<float>(float a, float b)
+{
+   return __fsub_rn(a, b);
+}
+template <typename Real>
+__device__ __forceinline__ Real div_rn(Real a, Real b);
+template <>
+__device__ __forceinline__ double div_rn<double>(double a, double b)
+{
+   return __ddiv_rn(a, b);
+}
+template <>
+__device__ __forceinline__ float div_rn<float>(float a, float b)
+{
+   return __fdiv_rn(a, b);
+}
+
+// One thread per row of the level.  lu holds A's values and is overwritten by
+// the factors; lstart/ustart/uend delimit the L and U parts of each row.
+template <typename Real>
+__global__ void k_factor_level(const int32_t* __restrict__ rows, int32_t count, const int32_t* __restrict__ cols,
+                               Real* __restrict__ lu, const int32_t* __restrict__ lstart,
+                               const int32_t* __restrict__ ustart, const int32_t* __restrict__ uend)
+{
+   const int32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+   if (t >= count) return;
+   const int32_t i = rows[t];
+   const int32_t l0 = lstart[i], u0 = ustart[i], u1 = uend[i];
+   for (int32_t ck = l0; ck < u0; ck++) {
+      const int32_t k = cols[ck];
+      const int32_t k0 = ustart[k], k1 = uend[k];
+      // U(k,k): getElement searches row k of U; 0 if absent
+      Real ukk = 0;
+      for (int32_t q = k0; q < k1; q++)
+         if (cols[q] == k) {
+            ukk = lu[q];
+            break;
+         }
+      const Real lik = div_rn(lu[ck], ukk);
+      lu[ck] = lik;
+      // remaining L entries and the U entries of row i, each minus L_ik*U(k,j)
+      int32_t q = k0;
+      for (int32_t cj = ck + 1; cj < u1; cj++) {
+         const int32_t j = cols[cj];
+         while (q < k1 && cols[q] < j) q++;
+         const Real ukj = (q < k1 && cols[q] == j) ? lu[q] : Real(0);
+         lu[cj] = sub_rn(lu[cj], mul_rn(lik, ukj));
+      }
+   }
+}
+
+// Forward substitution with unit-diagonal L for the rows of one level.
+template <typename Real>
+__global__ void k_lower_level(const int32_t* __restrict__ rows, int32_t count, const int32_t* __restrict__ cols,
+                              const Real* __restrict__ lu, const int32_t* __restrict__ lstart,
+                              const int32_t* __restrict__ ustart, const Real* __restrict__ b, Real* __restrict__ x)
+{
+   const int32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+   if (t >= count) return;
+   const int32_t i = rows[t];
+   Real xi = b[i];
+   for (int32_t c = lstart[i]; c < ustart[i]; c++) xi = sub_rn(xi, mul_rn(lu[c], x[cols[c]]));
+   x[i] = xi;
+}
+
+// Back substitution: x_i = (y_i - sum_{j>i} U_ij x_j) / U_ii (diagonal first in U_i).
+template <typename Real>
+__global__ void k_upper_level(const int32_t* __restrict__ rows, int32_t count, const int32_t* __restrict__ cols,
+                              const Real* __restrict__ lu, const int32_t* __restrict__ ustart,
+                              const int32_t* __restrict__ uend, Real* __restrict__ x)
+{
+   const int32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+   if (t >= count) return;
+   const int32_t i = rows[t];
+   const int32_t u0 = ustart[i];
+   Real xi = x[i];
+   for (int32_t c = u0 + 1; c < uend[i]; c++) xi = sub_rn(xi, mul_rn(lu[c], x[cols[c]]));
+   x[i] = div_rn(xi, lu[u0]);
+}
+
+struct Ilu0Base {
+   virtual ~Ilu0Base() = default;
+   virtual tnlb_status apply(const void* b, void* x, cudaStream_t st) = 0;
+};
+
+template <typename Real>
+struct Ilu0 : Ilu0Base {
+   int32_t n = 0;
+   DeviceBuffer rp, cols, lu, lstart, ustart, uend, lrows, urows, tmp;
+   std::vector<int32_t> lptr, uptr;  // level boundaries into lrows / urows
+   cudaGraphExec_t exec = nullptr;
+   const Real* g_b = nullptr;
+   Real* g_x = nullptr;
+   cudaStream_t cs = nullptr;
+
+   ~Ilu0() override
+   {
+      if (exec) cudaGraphExecDestroy(exec);
+      if (cs) cudaStreamDestroy(cs);
+   }
+
+   void enqueue(const Real* b, Real* x, cudaStream_t st)
+   {
+      for (size_t l = 0; l + 1 < lptr.size(); l++) {
+         const int32_t cnt = lptr[l + 1] - lptr[l];
+         k_lower_level<Real><<<(cnt + 127) / 128, 128, 0, st>>>(lrows.as<int32_t>() + lptr[l], cnt, cols.as<int32_t>(),
+                                                               lu.as<Real>(), lstart.as<int32_t>(),
+                                                               ustart.as<int32_t>(), b, x);
+      }
+      for (size_t l = 0; l + 1 < uptr.size(); l++) {
+         const int32_t cnt = uptr[l + 1] - uptr[l];
+         k_upper_level<Real><<<(cnt + 127) / 128, 128, 0, st>>>(urows.as<int32_t>() + uptr[l], cnt, cols.as<int32_t>(),
+                                                               lu.as<Real>(), ustart.as<int32_t>(),
+                                                               uend.as<int32_t>(), x);
+      }
+   }
+
+   tnlb_status apply(const void* bv, void* xv, cudaStream_t st) override
+   {
+      const Real* b = static_cast<const Real*>(bv);
+      Real* x = static_cast<Real*>(xv);
+      // Solves are replayed from a graph captured for fixed (b, x) buffers:
+      // copy in/out of the graph's own buffers when the caller's differ.
+      if (!exec) {
+         TNLB_TRY_STATUS(tmp.alloc(sizeof(Real) * 2 * (size_t)(n > 0 ? n : 1)));
+         g_b = tmp.as<Real>();
+         g_x = tmp.as<Real>() + n;
+         TNLB_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+         cudaGraph_t graph = nullptr;
+         TNLB_CUDA_TRY(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+         enqueue(g_b, g_x, cs);
+         TNLB_CUDA_TRY(cudaStreamEndCapture(cs, &graph));
+         cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+         cudaGraphDestroy(graph);
+         TNLB_CUDA_TRY(e);
+      }
+      cudaEvent_t ev;
+      TNLB_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+      TNLB_CUDA_TRY(cudaMemcpyAsync((void*)g_b, b, sizeof(Real) * n, cudaMemcpyDeviceToDevice, st));
+      TNLB_CUDA_TRY(cudaEventRecord(ev, st));
+      TNLB_CUDA_TRY(cudaStreamWaitEvent(cs, ev, 0));
+      TNLB_CUDA_TRY(cudaGraphLaunch(exec, cs));
+      TNLB_CUDA_TRY(cudaEventRecord(ev, cs));
+      TNLB_CUDA_TRY(cudaStreamWaitEvent(st, ev, 0));
+      TNLB_CUDA_TRY(cudaMemcpyAsync(x, g_x, sizeof(Real) * n, cudaMemcpyDeviceToDevice, st));
+      cudaEventDestroy(ev);
+      return TNLB_OK;
+   }
+};
+
+template <typename Real>
+tnlb_status create_t(const tnlb_segments* seg, const int32_t* cols_in, const Real* vals_in, cudaStream_t st,
+                     Ilu0<Real>** out)
+{
+   const int32_t n = seg->n;
+   auto* P = new Ilu0<Real>();
+   P->n = n;
+   // CSR copy of the matrix (rows in slot order, padding dropped)
+   TNLB_TRY_STATUS(gather_csr(view_of(seg), sizeof(Real) == 8 ? TNLB_F64 : TNLB_F32, cols_in, vals_in, P->rp, P->cols,
+                              P->lu, st));
+   int64_t nnz = 0;
+   {
+      int32_t t = 0;
+      TNLB_CUDA_TRY(cudaMemcpyAsync(&t, P->rp.template as<int32_t>() + n, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+      TNLB_CUDA_TRY(cudaStreamSynchronize(st));
+      nnz = t;
+   }
+   // host analysis: L/U split and dependency levels
+   std::vector<int32_t> rp(n + 1), cols(nnz);
+   TNLB_CUDA_TRY(cudaMemcpyAsync(rp.data(), P->rp.ptr, sizeof(int32_t) * (n + 1), cudaMemcpyDeviceToHost, st));
+   if (nnz) TNLB_CUDA_TRY(cudaMemcpyAsync(cols.data(), P->cols.ptr, sizeof(int32_t) * nnz, cudaMemcpyDeviceToHost, st));
+   TNLB_CUDA_TRY(cudaStreamSynchronize(st));
+   std::vector<int32_t> ls(n), us(n), ue(n), llev(n, 0), ulev(n, 0);
+   int32_t lmax = 0, umax = 0;
+   for (int32_t i = 0; i < n; i++) {
+      int32_t c = rp[i];
+      // ILU0.hpp:35-55: columns < i -> L, i <= column < N -> U (sorted rows)
+      ls[i] = c;
+      while (c < rp[i + 1] && cols[c] < i) c++;
+      us[i] = c;
+      while (c < rp[i + 1] && cols[c] < n) c++;
+      ue[i] = c;
+      int32_t lv = 0;
+      for (int32_t q = ls[i]; q < us[i]; q++) lv = std::max(lv, llev[cols[q]] + 1);
+      llev[i] = lv;
+      lmax = std::max(lmax, lv);
+   }
+   for (int32_t i = n - 1; i >= 0; i--) {
+      int32_t lv = 0;
+      for (int32_t q = us[i] + 1; q < ue[i]; q++) lv = std::max(lv, ulev[cols[q]] + 1);
+      ulev[i] = lv;
+      umax = std::max(umax, lv);
+   }
+   auto bucket = [&](const std::vector<int32_t>& lev, int32_t maxl, std::vector<int32_t>& ptr,
+                     std::vector<int32_t>& rows) {
+      ptr.assign(maxl + 2, 0);
+      for (int32_t i = 0; i < n; i++) ptr[lev[i] + 1]++;
+      for (int32_t l = 0; l <= maxl; l++) ptr[l + 1] += ptr[l];
+      rows.resize(n);
+      std::vector<int32_t> pos(ptr.begin(), ptr.end() - 1);
+      for (int32_t i = 0; i < n; i++) rows[pos[lev[i]]++] = i;
+   };
+   std::vector<int32_t> lrows, urows;
+   bucket(llev, n > 0 ? lmax : -1, P->lptr, lrows);
+   bucket(ulev, n > 0 ? umax : -1, P->uptr, urows);
+   TNLB_TRY_STATUS(P->lstart.alloc(sizeof(int32_t) * (n ? n : 1)));
+   TNLB_TRY_STATUS(P->ustart.alloc(sizeof(int32_t) * (n ? n : 1)));
+   TNLB_TRY_STATUS(P->uend.alloc(sizeof(int32_t) * (n ? n : 1)));
+   TNLB_TRY_STATUS(P->lrows.alloc(sizeof(int32_t) * (n ? n : 1)));
+   TNLB_TRY_STATUS(P->urows.alloc(sizeof(int32_t) * (n ? n : 1)));
+   TNLB_CUDA_TRY(cudaMemcpyAsync(P->lstart.ptr, ls.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
+   TNLB_CUDA_TRY(cudaMemcpyAsync(P->ustart.ptr, us.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
+   TNLB_CUDA_TRY(cudaMemcpyAsync(P->uend.ptr, ue.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
+   TNLB_CUDA_TRY(cudaMemcpyAsync(P->lrows.ptr, lrows.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
+   TNLB_CUDA_TRY(cudaMemcpyAsync(P->urows.ptr, urows.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
+   // factorisation, level by level of L
+   for (size_t l = 0; l + 1 < P->lptr.size(); l++) {
+      const int32_t c = P->lptr[l + 1] - P->lptr[l];
+      k_factor_level<Real><<<(c + 127) / 128, 128, 0, st>>>(P->lrows.template as<int32_t>() + P->lptr[l], c, P->cols.template as<int32_t>(),
+                                                           P->lu.template as<Real>(), P->lstart.template as<int32_t>(),
+                                                           P->ustart.template as<int32_t>(), P->uend.template as<int32_t>());
+   }
+   TNLB_CHECK_LAUNCH();
+   TNLB_CUDA_TRY(cudaStreamSynchronize(st));
+   *out = P;
+   return TNLB_OK;
+}
+
+}  // namespace
+
+tnlb_status ilu0_create(const tnlb_segments* seg, tnlb_real real, const int32_t* cols, const void* vals,
+                        cudaStream_t st, void** out)
+{
+   TNLB_REQUIRE(seg->n > 0, TNLB_ERR_INVALID_ARGUMENT, "ILU0::update: the matrix is empty");
+   if (real == TNLB_F64) {
+      Ilu0<double>* p = nullptr;
+      tnlb_status s = create_t<double>(seg, cols, (const double*)vals, st, &p);
+      *out = static_cast<Ilu0Base*>(p);
+      return s;
+   }
+   Ilu0<float>* p = nullptr;
+   tnlb_status s = create_t<float>(seg, cols, (const float*)vals, st, &p);
+   *out = static_cast<Ilu0Base*>(p);
+   return s;
+}
+
+tnlb_status ilu0_apply(void* ilu, const void* b, void* x, cudaStream_t st)
+{
+   return static_cast<Ilu0Base*>(ilu)->apply(b, x, st);
+}
+
+void ilu0_destroy(void* ilu) { delete static_cast<Ilu0Base*>(ilu); }
+
+// Factors for inspection: CSR pattern (rowptr n+1, cols nnz) and LU values
+// (L strictly below the diagonal, U from the diagonal on), copied to the host.
+tnlb_status ilu0_read(void* ilu, int32_t* h_rowptr, int32_t* h_cols, void* h_vals, int64_t capacity, int real_bytes)
+{
+   auto* b = static_cast<Ilu0Base*>(ilu);
+   if (real_bytes == 8) {
+      auto* p = dynamic_cast<Ilu0<double>*>(b);
+      TNLB_REQUIRE(p, TNLB_ERR_INVALID_ARGUMENT, "real type mismatch");
+      int32_t nnz = 0;
+      TNLB_CUDA_TRY(cudaMemcpy(&nnz, p->rp.as<int32_t>() + p->n, sizeof(int32_t), cudaMemcpyDeviceToHost));
+      TNLB_REQUIRE(capacity >= nnz, TNLB_ERR_INVALID_ARGUMENT, "buffer too small");
+      TNLB_CUDA_TRY(cudaMemcpy(h_rowptr, p->rp.ptr, sizeof(int32_t) * (p->n + 1), cudaMemcpyDeviceToHost));
+      TNLB_CUDA_TRY(cudaMemcpy(h_cols, p->cols.ptr, sizeof(int32_t) * nnz, cudaMemcpyDeviceToHost));
+      TNLB_CUDA_TRY(cudaMemcpy(h_vals, p->lu.ptr, sizeof(double) * nnz, cudaMemcpyDeviceToHost));
+      return TNLB_OK;
+   }
+   auto* p = dynamic_cast<Ilu0<float>*>(b);
+   TNLB_REQUIRE(p, TNLB_ERR_INVALID_ARGUMENT, "real type mismatch");
+   int32_t nnz = 0;
+   TNLB_CUDA_TRY(cudaMemcpy(&nnz, p->rp.as<int32_t>() + p->n, sizeof(int32_t), cudaMemcpyDeviceToHost));
+   TNLB_REQUIRE(capacity >= nnz, TNLB_ERR_INVALID_ARGUMENT, "buffer too small");
+   TNLB_CUDA_TRY(cudaMemcpy(h_rowptr, p->rp.ptr, sizeof(int32_t) * (p->n + 1), cudaMemcpyDeviceToHost));
+   TNLB_CUDA_TRY(cudaMemcpy(h_cols, p->cols.ptr, sizeof(int32_t) * nnz, cudaMemcpyDeviceToHost));
+   TNLB_CUDA_TRY(cudaMemcpy(h_vals, p->lu.ptr, sizeof(float) * nnz, cudaMemcpyDeviceToHost));
+   return TNLB_OK;
+}
+
+}  // namespace tnlb

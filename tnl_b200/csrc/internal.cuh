@@ -143,6 +143,22 @@ struct tnlb_segments {
 };
 
 namespace tnlb {
+struct Fsai;
+}
+
+// A preconditioner built for one matrix (Preconditioner::update), applied
+// by the solvers (Preconditioner::solve).  Opaque in the C ABI.
+struct tnlb_precond {
+   int32_t kind = TNLB_PRECOND_NONE;
+   tnlb_real real = TNLB_F64;
+   int32_t n = 0;
+   tnlb::DeviceBuffer diag;      // Jacobi
+   void* ilu = nullptr;          // ILU(0)
+   tnlb::Fsai* fsai = nullptr;   // FSAI / learned FSAI: M^-1 = G^T G
+   ~tnlb_precond();
+};
+
+namespace tnlb {
 
 // ------------------------------------------------- device-side helpers
 
@@ -249,11 +265,37 @@ tnlb_status reduce_sum_i64(const int32_t* d_in, int64_t n, int64_t* h_sum, cudaS
 // spmv_csr.cu / spmv_ell.cu
 tnlb_status spmv_csr(const tnlb_segments* seg, tnlb_real real, const int32_t* cols, const void* vals, const void* x,
                      void* y, double alpha, double beta, int32_t begin, int32_t end, tnlb_kernel kernel, int32_t tps,
-                     cudaStream_t stream, int* launches);
+                     cudaStream_t stream, int* launches, const int32_t* skip = nullptr);
 tnlb_status spmv_ell_family(const tnlb_segments* seg, tnlb_real real, const int32_t* cols, const void* vals,
                             const void* x, void* y, double alpha, double beta, int32_t begin, int32_t end,
                             tnlb_kernel kernel, int32_t tps, cudaStream_t stream, int* launches);
 tnlb_status build_csr_tile_plan(tnlb_segments* seg, cudaStream_t stream);
+// solvers.cu / ilu0.cu / fsai.cu
+tnlb_status precond_create(int kind, const tnlb_segments* seg, tnlb_real real, const int32_t* cols, const void* vals,
+                           cudaStream_t st, tnlb_precond** out);
+tnlb_status precond_apply(const tnlb_precond* P, const void* b, void* x, cudaStream_t st);
+tnlb_status solve(tnlb_solver_kind solver, const tnlb_precond* P, const tnlb_solver_params& prm,
+                  const tnlb_segments* seg, tnlb_real real, const int32_t* cols, const void* vals, const void* b,
+                  void* x, cudaStream_t st, tnlb_solve_result* res);
+tnlb_status true_residual(const tnlb_segments* seg, tnlb_real real, const int32_t* cols, const void* vals,
+                          const void* b, const void* x, cudaStream_t st, double* out);
+tnlb_status solve_mixed_cg(const tnlb_segments* seg, const int32_t* cols, const double* vals, const double* b,
+                           double* x, const tnlb_solver_params& prm, double inner_tol, int32_t max_outer,
+                           cudaStream_t st, tnlb_solve_result* res, int32_t* inner_total, int32_t* outer,
+                           int inner_kind, const tnlb_precond* inner_precond);
+tnlb_status ilu0_create(const tnlb_segments* seg, tnlb_real real, const int32_t* cols, const void* vals,
+                        cudaStream_t st, void** out);
+tnlb_status ilu0_apply(void* ilu, const void* b, void* x, cudaStream_t st);
+tnlb_status ilu0_read(void* ilu, int32_t* h_rowptr, int32_t* h_cols, void* h_vals, int64_t capacity, int real_bytes);
+void ilu0_destroy(void* ilu);
+tnlb_status fsai_create(const tnlb_segments* seg, tnlb_real real, const int32_t* cols, const void* vals,
+                        bool classical, cudaStream_t st, Fsai** out);
+tnlb_status fsai_apply(const Fsai* F, const void* r, void* z, cudaStream_t st, const int32_t* skip = nullptr);
+tnlb_status fsai_set_values(Fsai* F, const void* gvals, cudaStream_t st);
+void fsai_destroy(Fsai* F);
+tnlb_status spmv_dispatch(const tnlb_segments* seg, tnlb_real real, const int32_t* cols, const void* vals,
+                          const void* x, void* y, double alpha, double beta, cudaStream_t st,
+                          const int32_t* skip = nullptr);
 // fill.cu
 tnlb_status fill_from_csr(const tnlb_segments* seg, tnlb_real real, const int32_t* rowptr, const int32_t* src_cols,
                           const void* src_vals, int32_t* cols, void* vals, cudaStream_t stream);

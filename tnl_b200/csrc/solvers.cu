@@ -1,0 +1,1267 @@
+// solvers.cu -- CG, BiCGStab and GMRES on the GPU with the Jacobi (Diagonal)
+// and ILU(0) preconditioners, plus FP32-inner / FP64 iterative refinement.
+//
+// The iteration logic and stopping rules follow the reference exactly:
+// CG.hpp:12-109, BICGStab.hpp:34-164, GMRES.hpp:73-347/436-465/648-770,
+// IterativeSolver.hpp:98-143 (nextIteration checks, then increments; solve()
+// returns checkConvergence()).  What changes is where the scalars live: every
+// dot product and norm is reduced on the device into a DevState record, and
+// the scalar recurrences (alpha, beta, residue, the stopping test) run in the
+// last block of the reduction.  CG never waits for the host inside an
+// iteration: batches of iterations are captured once in a CUDA graph and
+// replayed; kernels of iterations past the stopping point return at once on
+// the device `done` flag, so the iteration count is exact.  BiCGStab and
+// GMRES read the state once per iteration / Arnoldi step.  GMRES keeps the
+// small Hessenberg least-squares problem (Givens rotations, back
+// substitution) on the host in FP64, as the reference does.
+#include <cfloat>
+#include <cmath>
+#include <vector>
+
+#include "internal.cuh"
+#include "reduce.cuh"
+#include "segview.cuh"
+
+namespace tnlb {
+
+// Device-resident solver scalars.
+struct DevState {
+   double normb, s1, s2, alpha, beta, omega, rho, rho_old, r_ast_sqnorm, residue;
+   double conv, div;
+   int32_t it, done, maxit, minit;
+   int32_t flag, pad;
+};
+
+__device__ __forceinline__ bool check_next(const DevState& S)
+{
+   return !(isnan(S.residue) || S.it > S.maxit || (S.residue > S.div && S.it >= S.minit) ||
+            (S.residue < S.conv && S.it >= S.minit));
+}
+
+// IterativeSolver::nextIteration (IterativeSolver.hpp:98-108).
+__device__ __forceinline__ void next_iteration(DevState& S)
+{
+   const bool c = check_next(S);
+   S.it++;
+   if (!c) S.done = 1;
+}
+
+// IterativeSolver::checkConvergence (IterativeSolver.hpp:121-143).
+static bool check_convergence(double residue, int it, int maxit, int minit, double conv, double div)
+{
+   if (std::isnan(residue)) return false;
+   if (residue > div && it > minit) return false;
+   if (it >= maxit) return false;
+   if (residue > conv) return false;
+   return true;
+}
+
+namespace {
+
+// ----------------------------------------------------------- diagonal
+// d_i = A(i,i) by a search of row i's slots (getElement semantics: 0 if absent).
+template <typename Real>
+__global__ void k_diag(SegView v, const int32_t* __restrict__ cols, const Real* __restrict__ vals, Real* __restrict__ d)
+{
+   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+   if (i >= v.n) return;
+   Real val = 0;
+   for (int32_t k = 0;; k++) {
+      const int64_t g = global_index_of(v, (int32_t)i, k);
+      if (g < 0) break;
+      if (cols[g] == i) {
+         val = vals[g];
+         break;
+      }
+   }
+   d[i] = val;
+}
+
+template <typename To, typename From>
+__global__ void k_convert(int64_t n, const From* __restrict__ a, To* __restrict__ b)
+{
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+      b[i] = (To)a[i];
+}
+
+// ------------------------------------------------------------------ CG
+// normb = ||M^-1 b|| (Jacobi) or ||b||
+template <typename Real>
+__global__ void __launch_bounds__(kRedThreads) k_normb(int64_t n, const Real* __restrict__ b, const Real* __restrict__ d,
+                                                       RedWork w, DevState* S)
+{
+   double acc = 0;
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+      const double v = d ? (double)(b[i] / d[i]) : (double)b[i];
+      acc += v * v;
+   }
+   double v[1] = {acc};
+   if (publish_and_arrive<1>(v, w)) {
+      double t[1];
+      gather_totals<1>(t, w);
+      if (threadIdx.x == 0) S->normb = sqrt(t[0]);
+   }
+}
+
+// z = M^-1 r; p = z; s1 = (r, z); residue; nextIteration.
+template <typename Real>
+__global__ void __launch_bounds__(kRedThreads) k_cg_init(int64_t n, const Real* __restrict__ r, Real* __restrict__ z,
+                                                         Real* __restrict__ p, const Real* __restrict__ d, RedWork w,
+                                                         DevState* S)
+{
+   double acc = 0;
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+      const Real ri = r[i];
+      const Real zi = d ? ri / d[i] : ri;
+      if (d) z[i] = zi;
+      p[i] = zi;
+      acc += (double)ri * (double)zi;
+   }
+   double v[1] = {acc};
+   if (publish_and_arrive<1>(v, w)) {
+      double t[1];
+      gather_totals<1>(t, w);
+      if (threadIdx.x == 0) {
+         DevState s = *S;
+         s.s1 = t[0];
+         s.residue = sqrt(s.s1) / s.normb;
+         s.it = 0;
+         s.done = 0;
+         s.flag = 0;
+         next_iteration(s);
+         *S = s;
+      }
+   }
+}
+
+// s2 = (Ap, p); s2 == 0 -> residue 0 and stop (CG.hpp:64-68); alpha = s1/s2.
+template <typename Real>
+__global__ void __launch_bounds__(kRedThreads) k_cg_s2(int64_t n, const Real* __restrict__ Ap, const Real* __restrict__ p,
+                                                       RedWork w, DevState* S)
+{
+   if (S->done) return;
+   double acc = 0;
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+      acc += (double)Ap[i] * (double)p[i];
+   double v[1] = {acc};
+   if (publish_and_arrive<1>(v, w)) {
+      double t[1];
+      gather_totals<1>(t, w);
+      if (threadIdx.x == 0) {
+         S->s2 = t[0];
+         if (t[0] == 0.0) {
+            S->residue = 0.0;
+            S->done = 1;
+            S->flag = 1;
+         }
+         else
+            S->alpha = S->s1 / t[0];
+      }
+   }
+}
+
+// x += alpha p; r -= alpha Ap; z = M^-1 r; s1 = (r, z); beta; residue; nextIteration.
+template <typename Real>
+__global__ void __launch_bounds__(kRedThreads) k_cg_update(int64_t n, Real* __restrict__ x, Real* __restrict__ r,
+                                                           const Real* __restrict__ p, const Real* __restrict__ Ap,
+                                                           Real* __restrict__ z, const Real* __restrict__ d, RedWork w,
+                                                           DevState* S)
+{
+   if (S->done) return;
+   const Real alpha = (Real)S->alpha;
+   double acc = 0;
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+      x[i] += alpha * p[i];
+      const Real ri = r[i] - alpha * Ap[i];
+      r[i] = ri;
+      Real zi = ri;
+      if (d) {
+         zi = ri / d[i];
+         z[i] = zi;
+      }
+      acc += (double)ri * (double)zi;
+   }
+   double v[1] = {acc};
+   if (publish_and_arrive<1>(v, w)) {
+      double t[1];
+      gather_totals<1>(t, w);
+      if (threadIdx.x == 0) {
+         DevState s = *S;
+         s.s2 = s.s1;
+         s.s1 = t[0];
+         s.beta = (s.s2 == 0.0) ? 0.0 : s.s1 / s.s2;
+         s.residue = sqrt(s.s1) / s.normb;
+         next_iteration(s);
+         *S = s;
+      }
+   }
+}
+
+// x += alpha p; r -= alpha Ap (z and (r, z) follow after M^-1 is applied).
+template <typename Real>
+__global__ void k_cg_xr(int64_t n, Real* __restrict__ x, Real* __restrict__ r, const Real* __restrict__ p,
+                        const Real* __restrict__ Ap, const DevState* S)
+{
+   if (S->done) return;
+   const Real alpha = (Real)S->alpha;
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+      x[i] += alpha * p[i];
+      r[i] -= alpha * Ap[i];
+   }
+}
+
+// s1 = (r, z) after z = M^-1 r; beta; residue; nextIteration.  With
+// `init`, also p = z and the first nextIteration of the solve.
+template <typename Real>
+__global__ void __launch_bounds__(kRedThreads) k_cg_rz(int64_t n, const Real* __restrict__ r,
+                                                       const Real* __restrict__ z, Real* __restrict__ p, int init,
+                                                       RedWork w, DevState* S)
+{
+   if (!init && S->done) return;
+   double acc = 0;
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+      if (init) p[i] = z[i];
+      acc += (double)r[i] * (double)z[i];
+   }
+   double v[1] = {acc};
+   if (publish_and_arrive<1>(v, w)) {
+      double t[1];
+      gather_totals<1>(t, w);
+      if (threadIdx.x == 0) {
+         DevState s = *S;
+         if (init) {
+            s.s1 = t[0];
+            s.it = 0;
+            s.done = 0;
+            s.flag = 0;
+         }
+         else {
+            s.s2 = s.s1;
+            s.s1 = t[0];
+            s.beta = (s.s2 == 0.0) ? 0.0 : s.s1 / s.s2;
+         }
+         s.residue = sqrt(s.s1) / s.normb;
+         next_iteration(s);
+         *S = s;
+      }
+   }
+}
+
+// p = z + beta p (the beta of this iteration; skipped once stopped).
+template <typename Real>
+__global__ void k_cg_p(int64_t n, Real* __restrict__ p, const Real* __restrict__ z, const DevState* S, int32_t it_expected)
+{
+   // The update belongs to iteration it_expected; if the state moved past
+   // the stop, p is no longer needed.
+   if (S->done) return;
+   const Real beta = (Real)S->beta;
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+      p[i] = z[i] + beta * p[i];
+}
+
+// ---------------------------------------------------- generic vector ops
+
+template <typename Real>
+__global__ void k_axpby(int64_t n, Real a, const Real* __restrict__ x, Real b, Real* __restrict__ y)
+{
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+      y[i] = a * x[i] + b * y[i];
+}
+
+// out = M^-1 in (Jacobi) or copy
+template <typename Real>
+__global__ void k_jacobi(int64_t n, const Real* __restrict__ in, const Real* __restrict__ d, Real* __restrict__ out)
+{
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+      out[i] = d ? in[i] / d[i] : in[i];
+}
+
+// Up to two dot products into slots of DevState-external results.
+template <typename Real>
+__global__ void __launch_bounds__(kRedThreads) k_dots(int64_t n, const Real* __restrict__ a0, const Real* __restrict__ b0,
+                                                      const Real* __restrict__ a1, const Real* __restrict__ b1, RedWork w,
+                                                      double* __restrict__ out)
+{
+   double acc0 = 0, acc1 = 0;
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+      acc0 += (double)a0[i] * (double)b0[i];
+      if (a1) acc1 += (double)a1[i] * (double)b1[i];
+   }
+   double v[2] = {acc0, acc1};
+   if (publish_and_arrive<2>(v, w)) {
+      double t[2];
+      gather_totals<2>(t, w);
+      if (threadIdx.x == 0) {
+         out[0] = t[0];
+         out[1] = t[1];
+      }
+   }
+}
+
+// ------------------------------------------------------------- BiCGStab
+
+// x += alpha p + omega s; r = s - omega As; dots (r, r_ast), (r, r)
+template <typename Real>
+__global__ void __launch_bounds__(kRedThreads) k_bicg_xr(int64_t n, Real* __restrict__ x, Real* __restrict__ r,
+                                                         const Real* __restrict__ p, const Real* __restrict__ s,
+                                                         const Real* __restrict__ As, const Real* __restrict__ r_ast,
+                                                         Real alpha, Real omega, RedWork w, double* __restrict__ out)
+{
+   double acc0 = 0, acc1 = 0;
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+      x[i] += alpha * p[i] + omega * s[i];
+      const Real ri = s[i] - omega * As[i];
+      r[i] = ri;
+      acc0 += (double)ri * (double)r_ast[i];
+      acc1 += (double)ri * (double)ri;
+   }
+   double v[2] = {acc0, acc1};
+   if (publish_and_arrive<2>(v, w)) {
+      double t[2];
+      gather_totals<2>(t, w);
+      if (threadIdx.x == 0) {
+         out[0] = t[0];
+         out[1] = t[1];
+      }
+   }
+}
+
+// p = r + beta p - (beta omega) Ap
+template <typename Real>
+__global__ void k_bicg_p(int64_t n, Real* __restrict__ p, const Real* __restrict__ r, const Real* __restrict__ Ap,
+                         Real beta, Real bo)
+{
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+      p[i] = r[i] + beta * p[i] - bo * Ap[i];
+}
+
+// ---------------------------------------------------------------- GMRES
+
+// H_l[k] = (V_k, w) for k <= i: one block-row pass over V; per-block
+// partials then the last block sums them (deterministic).
+template <typename Real>
+__global__ void __launch_bounds__(kRedThreads) k_gmres_vtw(int64_t n, int64_t ld, int cols, const Real* __restrict__ V,
+                                                           const Real* __restrict__ w, double* __restrict__ partials,
+                                                           unsigned* counter, double* __restrict__ out)
+{
+   // partials layout: [col][block]
+   __shared__ bool s_last;
+   for (int k = 0; k < cols; k++) {
+      double acc = 0;
+      const Real* vk = V + (int64_t)k * ld;
+      for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+         acc += (double)vk[i] * (double)w[i];
+      acc = block_sum(acc);
+      if (threadIdx.x == 0) partials[(int64_t)k * kRedMaxBlocks + blockIdx.x] = acc;
+   }
+   if (threadIdx.x == 0) {
+      __threadfence();
+      s_last = atomicAdd(counter, 1u) == gridDim.x - 1;
+   }
+   __syncthreads();
+   if (!s_last) return;
+   for (int k = 0; k < cols; k++) {
+      double v = 0;
+      for (unsigned b = threadIdx.x; b < gridDim.x; b += kRedThreads) v += __ldcg(partials + (int64_t)k * kRedMaxBlocks + b);
+      v = block_sum(v);
+      if (threadIdx.x == 0) out[k] = v;
+   }
+   if (threadIdx.x == 0) *counter = 0;
+}
+
+// w = w - V h (h on the device, cols entries), optional norm of the result.
+template <typename Real>
+__global__ void __launch_bounds__(kRedThreads) k_gmres_wmvh(int64_t n, int64_t ld, int cols, const Real* __restrict__ V,
+                                                            const double* __restrict__ h, Real* __restrict__ w,
+                                                            RedWork red, double* __restrict__ norm_out)
+{
+   __shared__ double sh[64];
+   if (threadIdx.x < cols && threadIdx.x < 64) sh[threadIdx.x] = h[threadIdx.x];
+   __syncthreads();
+   double acc = 0;
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+      Real s = w[i];
+      for (int k = 0; k < cols; k++) s -= (Real)sh[k] * V[(int64_t)k * ld + i];
+      w[i] = s;
+      acc += (double)s * (double)s;
+   }
+   if (!norm_out) return;
+   double v[1] = {acc};
+   if (publish_and_arrive<1>(v, red)) {
+      double t[1];
+      gather_totals<1>(t, red);
+      if (threadIdx.x == 0) *norm_out = sqrt(t[0]);
+   }
+}
+
+// w -= h[0] v (one MGS step), with (w_new, v_next) for the next step.
+template <typename Real>
+__global__ void __launch_bounds__(kRedThreads) k_mgs_step(int64_t n, const Real* __restrict__ v, const double* __restrict__ h,
+                                                          Real* __restrict__ w, const Real* __restrict__ vnext,
+                                                          RedWork red, double* __restrict__ out)
+{
+   const Real hk = h ? (Real)h[0] : Real(0);
+   double acc = 0;
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+      Real wi = w[i];
+      if (h) wi = wi - hk * v[i];
+      w[i] = wi;
+      acc += vnext ? (double)wi * (double)vnext[i] : (double)wi * (double)wi;
+   }
+   double vv[1] = {acc};
+   if (publish_and_arrive<1>(vv, red)) {
+      double t[1];
+      gather_totals<1>(t, red);
+      if (threadIdx.x == 0) out[0] = vnext ? t[0] : sqrt(t[0]);
+   }
+}
+
+// x += a * d (FP64 solution, FP32 correction)
+__global__ void k_axpby_mixed(int64_t n, double a, const float* __restrict__ d, double* __restrict__ x)
+{
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+      x[i] += a * (double)d[i];
+}
+
+// dst = scale * src
+template <typename Real>
+__global__ void k_scale(int64_t n, Real scale, const Real* __restrict__ src, Real* __restrict__ dst)
+{
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+      dst[i] = scale * src[i];
+}
+
+// x += V y (y on the device, k+1 entries)
+template <typename Real>
+__global__ void k_gmres_update(int64_t n, int64_t ld, int cols, const Real* __restrict__ V, const double* __restrict__ y,
+                               Real* __restrict__ x)
+{
+   __shared__ double sy[64];
+   if (threadIdx.x < cols && threadIdx.x < 64) sy[threadIdx.x] = y[threadIdx.x];
+   __syncthreads();
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+      double acc = 0;
+      for (int k = 0; k < cols; k++) acc += (double)V[(int64_t)k * ld + i] * sy[k];
+      x[i] = (Real)(acc + (double)x[i]);
+   }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ host
+
+tnlb_status spmv_dispatch(const tnlb_segments* seg, tnlb_real real, const int32_t* cols, const void* vals, const void* x,
+                          void* y, double alpha, double beta, cudaStream_t st, const int32_t* skip)
+{
+   int launches = 0;
+   if (seg->format == TNLB_CSR || seg->format == TNLB_ADAPTIVE_CSR)
+      return spmv_csr(seg, real, cols, vals, x, y, alpha, beta, 0, seg->n,
+                      seg->format == TNLB_ADAPTIVE_CSR ? TNLB_KERNEL_ADAPTIVE : TNLB_KERNEL_DEFAULT, 0, st, &launches,
+                      seg->format == TNLB_CSR ? skip : nullptr);
+   return spmv_ell_family(seg, real, cols, vals, x, y, alpha, beta, 0, seg->n, TNLB_KERNEL_DEFAULT, 0, st, &launches);
+}
+
+namespace {
+
+// Preconditioner view for one real type over a tnlb_precond object.
+template <typename Real>
+struct Precond {
+   const tnlb_precond* obj = nullptr;
+   int kind = TNLB_PRECOND_NONE;
+   const Real* d() const { return kind == TNLB_PRECOND_JACOBI ? obj->diag.as<Real>() : nullptr; }
+   // true when M^-1 is applied by separate kernels (FSAI: two SpMVs)
+   bool general() const { return kind == TNLB_PRECOND_FSAI; }
+   // out = M^-1 in (`skip`: the solver's done flag, for kernels in graphs)
+   tnlb_status apply(int64_t n, const Real* in, Real* out, cudaStream_t st, const int32_t* skip = nullptr) const
+   {
+      if (kind == TNLB_PRECOND_ILU0) return ilu0_apply(obj->ilu, in, out, st);
+      if (kind == TNLB_PRECOND_FSAI) return fsai_apply(obj->fsai, in, out, st, skip);
+      k_jacobi<Real><<<vec_grid(n), kRedThreads, 0, st>>>(n, in, d(), out);
+      TNLB_CHECK_LAUNCH();
+      return TNLB_OK;
+   }
+};
+
+template <typename Real>
+Precond<Real> view(const tnlb_precond* P)
+{
+   Precond<Real> v;
+   v.obj = P;
+   v.kind = P ? P->kind : TNLB_PRECOND_NONE;
+   return v;
+}
+
+struct Work {
+   DeviceBuffer state, partials, counter, scratch;
+   tnlb_status alloc()
+   {
+      TNLB_TRY_STATUS(state.alloc(sizeof(DevState)));
+      TNLB_TRY_STATUS(partials.alloc(sizeof(double) * kRedMaxBlocks * 64));
+      TNLB_TRY_STATUS(counter.alloc(sizeof(unsigned) * 4));
+      TNLB_TRY_STATUS(scratch.alloc(sizeof(double) * 256));
+      TNLB_CUDA_TRY(cudaMemset(counter.ptr, 0, sizeof(unsigned) * 4));
+      return TNLB_OK;
+   }
+   RedWork red() const { return {partials.as<double>(), counter.as<unsigned>()}; }
+   DevState* S() const { return state.as<DevState>(); }
+};
+
+DevState initial_state(const tnlb_solver_params& p)
+{
+   DevState s{};
+   s.conv = p.convergence_residue;
+   s.div = p.divergence_residue;
+   s.maxit = p.max_iterations;
+   s.minit = p.min_iterations;
+   return s;
+}
+
+template <typename Real>
+struct Ctx {
+   const tnlb_segments* seg;
+   tnlb_real real;
+   const int32_t* cols;
+   const Real* vals;
+   int64_t n;
+   cudaStream_t st;
+   tnlb_status spmv(const Real* x, Real* y, double alpha = 1.0, double beta = 0.0) const
+   {
+      return spmv_dispatch(seg, real, cols, vals, x, y, alpha, beta, st);
+   }
+};
+
+// ------------------------------------------------------------------ CG
+
+template <typename Real>
+tnlb_status cg_solve(const Ctx<Real>& c, const Precond<Real>& P, const tnlb_solver_params& prm, const Real* b, Real* x,
+                     tnlb_solve_result* res)
+{
+   const int64_t n = c.n;
+   Work W;
+   TNLB_TRY_STATUS(W.alloc());
+   DeviceBuffer r, p, Ap, z;
+   TNLB_TRY_STATUS(r.alloc(sizeof(Real) * n));
+   TNLB_TRY_STATUS(p.alloc(sizeof(Real) * n));
+   TNLB_TRY_STATUS(Ap.alloc(sizeof(Real) * n));
+   TNLB_TRY_STATUS(z.alloc(sizeof(Real) * n));
+   DevState s0 = initial_state(prm);
+   TNLB_CUDA_TRY(cudaMemcpyAsync(W.S(), &s0, sizeof(s0), cudaMemcpyHostToDevice, c.st));
+   const unsigned G = vec_grid(n);
+   const bool gen = P.general();
+   const int32_t* done = &W.S()->done;
+   // normb = ||M^-1 b|| (CG.hpp:24-29)
+   if (gen) {
+      TNLB_TRY_STATUS(P.apply(n, b, z.as<Real>(), c.st));
+      k_normb<Real><<<G, kRedThreads, 0, c.st>>>(n, z.as<Real>(), nullptr, W.red(), W.S());
+   }
+   else
+      k_normb<Real><<<G, kRedThreads, 0, c.st>>>(n, b, P.d(), W.red(), W.S());
+   TNLB_CHECK_LAUNCH();
+   DevState h{};
+   TNLB_CUDA_TRY(cudaMemcpyAsync(&h, W.S(), sizeof(h), cudaMemcpyDeviceToHost, c.st));
+   TNLB_CUDA_TRY(cudaStreamSynchronize(c.st));
+   if (h.normb == 0) {
+      TNLB_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(Real) * n, c.st));
+      TNLB_CUDA_TRY(cudaStreamSynchronize(c.st));
+      *res = tnlb_solve_result{1, 0, 0.0, 0, 0};
+      return TNLB_OK;
+   }
+   // r = b - A x; z = M^-1 r; p = z; s1 = (r, z); first nextIteration
+   TNLB_CUDA_TRY(cudaMemcpyAsync(r.ptr, b, sizeof(Real) * n, cudaMemcpyDeviceToDevice, c.st));
+   TNLB_TRY_STATUS(c.spmv(x, r.as<Real>(), -1.0, 1.0));
+   Real* zp = (P.kind == TNLB_PRECOND_NONE) ? nullptr : z.as<Real>();
+   if (gen) {
+      TNLB_TRY_STATUS(P.apply(n, r.as<Real>(), z.as<Real>(), c.st));
+      k_cg_rz<Real><<<G, kRedThreads, 0, c.st>>>(n, r.as<Real>(), z.as<Real>(), p.as<Real>(), 1, W.red(), W.S());
+   }
+   else
+      k_cg_init<Real><<<G, kRedThreads, 0, c.st>>>(n, r.as<Real>(), z.as<Real>(), p.as<Real>(), P.d(), W.red(), W.S());
+   TNLB_CHECK_LAUNCH();
+   // One iteration (CG.hpp:60-107): every kernel returns at once when the
+   // device `done` flag is set, so batches may run past the stopping point.
+   auto enqueue_iteration = [&](cudaStream_t st) -> tnlb_status {
+      TNLB_TRY_STATUS(spmv_dispatch(c.seg, c.real, c.cols, c.vals, p.as<Real>(), Ap.as<Real>(), 1.0, 0.0, st, done));
+      k_cg_s2<Real><<<G, kRedThreads, 0, st>>>(n, Ap.as<Real>(), p.as<Real>(), W.red(), W.S());
+      if (gen) {
+         k_cg_xr<Real><<<G, kRedThreads, 0, st>>>(n, x, r.as<Real>(), p.as<Real>(), Ap.as<Real>(), W.S());
+         TNLB_TRY_STATUS(P.apply(n, r.as<Real>(), z.as<Real>(), st, done));
+         k_cg_rz<Real><<<G, kRedThreads, 0, st>>>(n, r.as<Real>(), z.as<Real>(), nullptr, 0, W.red(), W.S());
+      }
+      else
+         k_cg_update<Real><<<G, kRedThreads, 0, st>>>(n, x, r.as<Real>(), p.as<Real>(), Ap.as<Real>(), zp, P.d(),
+                                                      W.red(), W.S());
+      k_cg_p<Real><<<G, kRedThreads, 0, st>>>(n, p.as<Real>(), zp ? zp : r.as<Real>(), W.S(), 0);
+      TNLB_CHECK_LAUNCH();
+      return TNLB_OK;
+   };
+   // Batches of iterations replayed from a CUDA graph (captured on a side stream).
+   const int kBatch = n < (1 << 22) ? 32 : 8;
+   cudaStream_t cs;
+   TNLB_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+   cudaEvent_t ev;
+   TNLB_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+   TNLB_CUDA_TRY(cudaEventRecord(ev, c.st));
+   TNLB_CUDA_TRY(cudaStreamWaitEvent(cs, ev, 0));
+   cudaGraph_t graph = nullptr;
+   cudaGraphExec_t exec = nullptr;
+   tnlb_status status = TNLB_OK;
+   if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+      for (int k = 0; k < kBatch && status == TNLB_OK; k++) status = enqueue_iteration(cs);
+      cudaError_t e = cudaStreamEndCapture(cs, &graph);
+      if (e == cudaSuccess && status == TNLB_OK) e = cudaGraphInstantiate(&exec, graph, 0);
+      if (e != cudaSuccess) {
+         cudaGetLastError();
+         exec = nullptr;
+      }
+      status = TNLB_OK;  // a failed capture falls back to direct launches
+      clear_error();
+   }
+   else
+      cudaGetLastError();
+   while (status == TNLB_OK) {
+      TNLB_CUDA_TRY(cudaMemcpyAsync(&h, W.S(), sizeof(h), cudaMemcpyDeviceToHost, cs));
+      TNLB_CUDA_TRY(cudaStreamSynchronize(cs));
+      if (h.done) break;
+      if (exec) {
+         TNLB_CUDA_TRY(cudaGraphLaunch(exec, cs));
+      }
+      else {
+         for (int k = 0; k < kBatch && status == TNLB_OK; k++) status = enqueue_iteration(cs);
+      }
+   }
+   if (exec) cudaGraphExecDestroy(exec);
+   if (graph) cudaGraphDestroy(graph);
+   cudaEventDestroy(ev);
+   cudaStreamSynchronize(cs);
+   cudaStreamDestroy(cs);
+   TNLB_TRY_STATUS(status);
+   res->iterations = h.it;
+   res->residue = h.residue;
+   res->converged = check_convergence(h.residue, h.it, h.maxit, h.minit, h.conv, h.div);
+   res->status_detail = 0;
+   return TNLB_OK;
+}
+
+// CG with a general preconditioner applied by a separate call (ILU(0)).
+template <typename Real>
+tnlb_status pcg_general(const Ctx<Real>& c, const Precond<Real>& P, const tnlb_solver_params& prm, const Real* b,
+                        Real* x, tnlb_solve_result* res)
+{
+   const int64_t n = c.n;
+   Work W;
+   TNLB_TRY_STATUS(W.alloc());
+   DeviceBuffer r, p, Ap, z;
+   TNLB_TRY_STATUS(r.alloc(sizeof(Real) * n));
+   TNLB_TRY_STATUS(p.alloc(sizeof(Real) * n));
+   TNLB_TRY_STATUS(Ap.alloc(sizeof(Real) * n));
+   TNLB_TRY_STATUS(z.alloc(sizeof(Real) * n));
+   double* sc = W.scratch.as<double>();
+   const unsigned G = vec_grid(n);
+   double hs[2];
+   auto dot = [&](const Real* a, const Real* bb, double* out) -> tnlb_status {
+      k_dots<Real><<<G, kRedThreads, 0, c.st>>>(n, a, bb, nullptr, nullptr, W.red(), sc);
+      TNLB_CHECK_LAUNCH();
+      TNLB_CUDA_TRY(cudaMemcpyAsync(hs, sc, sizeof(hs), cudaMemcpyDeviceToHost, c.st));
+      TNLB_CUDA_TRY(cudaStreamSynchronize(c.st));
+      *out = hs[0];
+      return TNLB_OK;
+   };
+   int it = 0;
+   double residue = 0;
+   auto check = [&]() {
+      return !(std::isnan(residue) || it > prm.max_iterations ||
+               (residue > prm.divergence_residue && it >= prm.min_iterations) ||
+               (residue < prm.convergence_residue && it >= prm.min_iterations));
+   };
+   auto next = [&]() {
+      const bool cnt = check();
+      it++;
+      return cnt;
+   };
+   double normb;
+   TNLB_TRY_STATUS(P.apply(n, b, r.as<Real>(), c.st));
+   TNLB_TRY_STATUS(dot(r.as<Real>(), r.as<Real>(), &normb));
+   normb = std::sqrt(normb);
+   if (normb == 0) {
+      TNLB_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(Real) * n, c.st));
+      *res = tnlb_solve_result{1, 0, 0.0, 0, 0};
+      return TNLB_OK;
+   }
+   TNLB_CUDA_TRY(cudaMemcpyAsync(r.ptr, b, sizeof(Real) * n, cudaMemcpyDeviceToDevice, c.st));
+   TNLB_TRY_STATUS(c.spmv(x, r.as<Real>(), -1.0, 1.0));
+   TNLB_TRY_STATUS(P.apply(n, r.as<Real>(), z.as<Real>(), c.st));
+   TNLB_CUDA_TRY(cudaMemcpyAsync(p.ptr, z.ptr, sizeof(Real) * n, cudaMemcpyDeviceToDevice, c.st));
+   double s1, s2;
+   TNLB_TRY_STATUS(dot(r.as<Real>(), z.as<Real>(), &s1));
+   residue = std::sqrt(s1) / normb;
+   while (next()) {
+      TNLB_TRY_STATUS(c.spmv(p.as<Real>(), Ap.as<Real>()));
+      TNLB_TRY_STATUS(dot(Ap.as<Real>(), p.as<Real>(), &s2));
+      if (s2 == 0.0) {
+         residue = 0;
+         break;
+      }
+      const double alpha = s1 / s2;
+      k_axpby<Real><<<G, kRedThreads, 0, c.st>>>(n, (Real)alpha, p.as<Real>(), Real(1), x);
+      k_axpby<Real><<<G, kRedThreads, 0, c.st>>>(n, (Real)-alpha, Ap.as<Real>(), Real(1), r.as<Real>());
+      TNLB_CHECK_LAUNCH();
+      TNLB_TRY_STATUS(P.apply(n, r.as<Real>(), z.as<Real>(), c.st));
+      s2 = s1;
+      TNLB_TRY_STATUS(dot(r.as<Real>(), z.as<Real>(), &s1));
+      const double beta = (s2 == 0.0) ? 0.0 : s1 / s2;
+      k_axpby<Real><<<G, kRedThreads, 0, c.st>>>(n, Real(1), z.as<Real>(), (Real)beta, p.as<Real>());
+      TNLB_CHECK_LAUNCH();
+      residue = std::sqrt(s1) / normb;
+   }
+   TNLB_CUDA_TRY(cudaStreamSynchronize(c.st));
+   res->iterations = it;
+   res->residue = residue;
+   res->converged = check_convergence(residue, it, prm.max_iterations, prm.min_iterations, prm.convergence_residue,
+                                      prm.divergence_residue);
+   res->status_detail = 0;
+   return TNLB_OK;
+}
+
+// ------------------------------------------------------------ BiCGStab
+
+template <typename Real>
+tnlb_status bicgstab_solve(const Ctx<Real>& c, const Precond<Real>& P, const tnlb_solver_params& prm, const Real* b,
+                           Real* x, tnlb_solve_result* res)
+{
+   const int64_t n = c.n;
+   Work W;
+   TNLB_TRY_STATUS(W.alloc());
+   DeviceBuffer r, r_ast, p, s, Ap, As, M_tmp;
+   for (auto* v : {&r, &r_ast, &p, &s, &Ap, &As, &M_tmp}) TNLB_TRY_STATUS(v->alloc(sizeof(Real) * n));
+   double* sc = W.scratch.as<double>();
+   const unsigned G = vec_grid(n);
+   double hs[2];
+   auto dots = [&](const Real* a0, const Real* b0, const Real* a1, const Real* b1) -> tnlb_status {
+      k_dots<Real><<<G, kRedThreads, 0, c.st>>>(n, a0, b0, a1, b1, W.red(), sc);
+      TNLB_CHECK_LAUNCH();
+      TNLB_CUDA_TRY(cudaMemcpyAsync(hs, sc, sizeof(hs), cudaMemcpyDeviceToHost, c.st));
+      TNLB_CUDA_TRY(cudaStreamSynchronize(c.st));
+      return TNLB_OK;
+   };
+   const bool pre = P.kind != TNLB_PRECOND_NONE;
+   // compute_residue: r = M^-1 (b - A x) (BICGStab.hpp:125-138)
+   auto compute_residue = [&](Real* out) -> tnlb_status {
+      Real* tgt = pre ? M_tmp.as<Real>() : out;
+      TNLB_CUDA_TRY(cudaMemcpyAsync(tgt, b, sizeof(Real) * n, cudaMemcpyDeviceToDevice, c.st));
+      TNLB_TRY_STATUS(c.spmv(x, tgt, -1.0, 1.0));
+      if (pre) TNLB_TRY_STATUS(P.apply(n, M_tmp.as<Real>(), out, c.st));
+      return TNLB_OK;
+   };
+   // preconditioned_matvec (:141-151)
+   auto pmatvec = [&](const Real* src, Real* dst) -> tnlb_status {
+      if (!pre) return c.spmv(src, dst);
+      TNLB_TRY_STATUS(c.spmv(src, M_tmp.as<Real>()));
+      return P.apply(n, M_tmp.as<Real>(), dst, c.st);
+   };
+   int it = 0;
+   double residue = 0;
+   auto check = [&]() {
+      return !(std::isnan(residue) || it > prm.max_iterations ||
+               (residue > prm.divergence_residue && it >= prm.min_iterations) ||
+               (residue < prm.convergence_residue && it >= prm.min_iterations));
+   };
+   double b_norm;
+   if (pre) {
+      TNLB_TRY_STATUS(P.apply(n, b, M_tmp.as<Real>(), c.st));
+      TNLB_TRY_STATUS(dots(M_tmp.as<Real>(), M_tmp.as<Real>(), nullptr, nullptr));
+   }
+   else
+      TNLB_TRY_STATUS(dots(b, b, nullptr, nullptr));
+   b_norm = std::sqrt(hs[0]);
+   if (b_norm == 0) {
+      TNLB_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(Real) * n, c.st));
+      *res = tnlb_solve_result{1, 0, 0.0, 0, 0};
+      return TNLB_OK;
+   }
+   TNLB_TRY_STATUS(compute_residue(r.as<Real>()));
+   TNLB_CUDA_TRY(cudaMemcpyAsync(p.ptr, r.ptr, sizeof(Real) * n, cudaMemcpyDeviceToDevice, c.st));
+   TNLB_CUDA_TRY(cudaMemcpyAsync(r_ast.ptr, r.ptr, sizeof(Real) * n, cudaMemcpyDeviceToDevice, c.st));
+   TNLB_CUDA_TRY(cudaMemsetAsync(s.ptr, 0, sizeof(Real) * n, c.st));
+   TNLB_TRY_STATUS(dots(r.as<Real>(), r_ast.as<Real>(), nullptr, nullptr));
+   double rho = hs[0], r_ast_sqnorm = hs[0];
+   const double eps2 = DBL_EPSILON * DBL_EPSILON;
+   const double eps2r = (sizeof(Real) == 4) ? (double)FLT_EPSILON * FLT_EPSILON : eps2;
+   residue = std::sqrt(rho) / b_norm;
+   while (true) {
+      const bool cont = check();
+      it++;
+      if (!cont) break;
+      TNLB_TRY_STATUS(pmatvec(p.as<Real>(), Ap.as<Real>()));
+      TNLB_TRY_STATUS(dots(Ap.as<Real>(), r_ast.as<Real>(), nullptr, nullptr));
+      const double alpha = rho / hs[0];
+      // s = r - alpha Ap
+      TNLB_CUDA_TRY(cudaMemcpyAsync(s.ptr, r.ptr, sizeof(Real) * n, cudaMemcpyDeviceToDevice, c.st));
+      k_axpby<Real><<<G, kRedThreads, 0, c.st>>>(n, (Real)-alpha, Ap.as<Real>(), Real(1), s.as<Real>());
+      TNLB_CHECK_LAUNCH();
+      TNLB_TRY_STATUS(pmatvec(s.as<Real>(), As.as<Real>()));
+      TNLB_TRY_STATUS(dots(As.as<Real>(), s.as<Real>(), As.as<Real>(), As.as<Real>()));
+      const double omega = hs[0] / hs[1];
+      k_bicg_xr<Real><<<G, kRedThreads, 0, c.st>>>(n, x, r.as<Real>(), p.as<Real>(), s.as<Real>(), As.as<Real>(),
+                                                   r_ast.as<Real>(), (Real)alpha, (Real)omega, W.red(), sc);
+      TNLB_CHECK_LAUNCH();
+      TNLB_CUDA_TRY(cudaMemcpyAsync(hs, sc, sizeof(hs), cudaMemcpyDeviceToHost, c.st));
+      TNLB_CUDA_TRY(cudaStreamSynchronize(c.st));
+      const double rho_old = rho;
+      rho = hs[0];
+      double rnorm2 = hs[1];
+      (void)eps2r;
+      if (std::fabs(rho) < eps2 * r_ast_sqnorm) {
+         TNLB_TRY_STATUS(compute_residue(r.as<Real>()));
+         TNLB_CUDA_TRY(cudaMemcpyAsync(r_ast.ptr, r.ptr, sizeof(Real) * n, cudaMemcpyDeviceToDevice, c.st));
+         TNLB_TRY_STATUS(dots(r.as<Real>(), r_ast.as<Real>(), nullptr, nullptr));
+         r_ast_sqnorm = rho = hs[0];
+         rnorm2 = hs[0];
+      }
+      const double beta = (rho / rho_old) * (alpha / omega);
+      k_bicg_p<Real><<<G, kRedThreads, 0, c.st>>>(n, p.as<Real>(), r.as<Real>(), Ap.as<Real>(), (Real)beta,
+                                                  (Real)(beta * omega));
+      TNLB_CHECK_LAUNCH();
+      if (prm.bicgstab_exact_residue) {
+         TNLB_TRY_STATUS(compute_residue(s.as<Real>()));
+         TNLB_TRY_STATUS(dots(s.as<Real>(), s.as<Real>(), nullptr, nullptr));
+         residue = std::sqrt(hs[0]) / b_norm;
+      }
+      else
+         residue = std::sqrt(rnorm2) / b_norm;
+   }
+   TNLB_CUDA_TRY(cudaStreamSynchronize(c.st));
+   res->iterations = it;
+   res->residue = residue;
+   res->converged = check_convergence(residue, it, prm.max_iterations, prm.min_iterations, prm.convergence_residue,
+                                      prm.divergence_residue);
+   res->status_detail = 0;
+   return TNLB_OK;
+}
+
+// --------------------------------------------------------------- GMRES
+
+template <typename Real>
+tnlb_status gmres_solve(const Ctx<Real>& c, const Precond<Real>& P, const tnlb_solver_params& prm, const Real* b,
+                        Real* x, tnlb_solve_result* res)
+{
+   const int64_t n = c.n;
+   const int rmin = prm.gmres_restarting_min, rmax = prm.gmres_restarting_max;
+   const int dmin = prm.gmres_restarting_step_min, dmax = prm.gmres_restarting_step_max;
+   TNLB_REQUIRE(rmin > 0 && rmax > 0 && rmin <= rmax, TNLB_ERR_INVALID_ARGUMENT,
+                "Wrong value for the GMRES restarting parameters");
+   TNLB_REQUIRE(dmin >= 0 && dmax >= 0 && dmin <= dmax, TNLB_ERR_INVALID_ARGUMENT,
+                "Wrong value for the GMRES restarting adjustment parameters");
+   TNLB_REQUIRE(rmax <= 64, TNLB_ERR_INVALID_ARGUMENT, "GMRES restarting parameter above 64 is not supported");
+   const int variant = prm.gmres_variant;
+   TNLB_REQUIRE(variant == TNLB_GMRES_CGS || variant == TNLB_GMRES_CGSR || variant == TNLB_GMRES_MGS ||
+                   variant == TNLB_GMRES_MGSR,
+                TNLB_ERR_NOT_IMPLEMENTED, "GMRES variant CWY (Householder) is not implemented on the GPU");
+   const int m_max = rmax;
+   const int64_t ld = (n + 31) / 32 * 32;  // 256-byte aligned columns in FP64
+   Work W;
+   TNLB_TRY_STATUS(W.alloc());
+   DeviceBuffer V, w, r, M_tmp, hdev, ydev;
+   TNLB_TRY_STATUS(V.alloc(sizeof(Real) * ld * (m_max + 1)));
+   TNLB_TRY_STATUS(w.alloc(sizeof(Real) * n));
+   TNLB_TRY_STATUS(r.alloc(sizeof(Real) * n));
+   TNLB_TRY_STATUS(M_tmp.alloc(sizeof(Real) * n));
+   TNLB_TRY_STATUS(hdev.alloc(sizeof(double) * 128));
+   TNLB_TRY_STATUS(ydev.alloc(sizeof(double) * 128));
+   Real* Vp = V.as<Real>();
+   double* sc = W.scratch.as<double>();
+   const unsigned G = vec_grid(n);
+   const bool pre = P.kind != TNLB_PRECOND_NONE;
+   double hs[2];
+   auto norm = [&](const Real* a, double* out) -> tnlb_status {
+      k_dots<Real><<<G, kRedThreads, 0, c.st>>>(n, a, a, nullptr, nullptr, W.red(), sc);
+      TNLB_CHECK_LAUNCH();
+      TNLB_CUDA_TRY(cudaMemcpyAsync(hs, sc, sizeof(hs), cudaMemcpyDeviceToHost, c.st));
+      TNLB_CUDA_TRY(cudaStreamSynchronize(c.st));
+      *out = std::sqrt(hs[0]);
+      return TNLB_OK;
+   };
+   auto compute_residue = [&]() -> tnlb_status {
+      Real* tgt = pre ? M_tmp.as<Real>() : r.as<Real>();
+      TNLB_CUDA_TRY(cudaMemcpyAsync(tgt, b, sizeof(Real) * n, cudaMemcpyDeviceToDevice, c.st));
+      TNLB_TRY_STATUS(c.spmv(x, tgt, -1.0, 1.0));
+      if (pre) TNLB_TRY_STATUS(P.apply(n, M_tmp.as<Real>(), r.as<Real>(), c.st));
+      return TNLB_OK;
+   };
+   int it = 0;
+   double residue = 0;
+   auto check = [&]() {
+      return !(std::isnan(residue) || it > prm.max_iterations ||
+               (residue > prm.divergence_residue && it >= prm.min_iterations) ||
+               (residue < prm.convergence_residue && it >= prm.min_iterations));
+   };
+   double normb;
+   if (pre) {
+      TNLB_TRY_STATUS(P.apply(n, b, M_tmp.as<Real>(), c.st));
+      TNLB_TRY_STATUS(norm(M_tmp.as<Real>(), &normb));
+   }
+   else
+      TNLB_TRY_STATUS(norm(b, &normb));
+   if (normb == 0) {
+      TNLB_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(Real) * n, c.st));
+      *res = tnlb_solve_result{1, 0, 0.0, 0, 0};
+      return TNLB_OK;
+   }
+   TNLB_TRY_STATUS(compute_residue());
+   double beta;
+   TNLB_TRY_STATUS(norm(r.as<Real>(), &beta));
+   residue = beta / normb;
+   std::vector<double> H((m_max + 1) * m_max), s(m_max + 1), cs(m_max + 1), sn(m_max + 1), y(m_max + 1);
+   double beta_ratio = 1;
+   const double max_beta_ratio = 0.99, min_beta_ratio = 0.175;
+   int restart_cycles = 0;
+   int m = m_max;
+   auto rot_apply = [](double& dx, double& dy, double csv, double snv) {
+      const double t = csv * dx + snv * dy;
+      dy = csv * dy - snv * dx;
+      dx = t;
+   };
+   // x += V y for the first k+1 columns (GMRES::update, GMRES.hpp:648-684)
+   auto update = [&](int k) -> tnlb_status {
+      for (int i = 0; i <= m; i++) y[i] = s[i];
+      for (int i = k; i >= 0; i--) {
+         if (H[i + i * (m + 1)] == 0) {
+            set_error("GMRES: zero diagonal element of the Hessenberg matrix (breakdown)");
+            return TNLB_ERR_BREAKDOWN;
+         }
+         y[i] /= H[i + i * (m + 1)];
+         for (int j = i - 1; j >= 0; j--) y[j] -= H[j + i * (m + 1)] * y[i];
+      }
+      TNLB_CUDA_TRY(cudaMemcpyAsync(ydev.ptr, y.data(), sizeof(double) * (k + 1), cudaMemcpyHostToDevice, c.st));
+      k_gmres_update<Real><<<vec_grid(n), kRedThreads, 0, c.st>>>(n, ld, k + 1, Vp, ydev.as<double>(), x);
+      TNLB_CHECK_LAUNCH();
+      return TNLB_OK;
+   };
+   while (check()) {
+      if (rmax > rmin && restart_cycles > 0) {
+         if (beta_ratio > max_beta_ratio)
+            m = rmax;
+         else if (beta_ratio >= min_beta_ratio) {
+            const int step = dmin + (dmax - dmin) / static_cast<float>(rmax - rmin) * (m - rmin);
+            if (m - step >= rmin)
+               m -= step;
+            else
+               m = rmax;
+         }
+      }
+      // orthogonalisation (CGS / CGSR / MGS / MGSR)
+      int o_steps = m;
+      k_scale<Real><<<vec_grid(n), kRedThreads, 0, c.st>>>(n, (Real)(1.0 / beta), r.as<Real>(), Vp);
+      TNLB_CHECK_LAUNCH();
+      std::fill(H.begin(), H.end(), 0.0);
+      std::fill(s.begin(), s.end(), 0.0);
+      s[0] = beta;
+      for (int i = 0; i < m; i++) {
+         const bool cont = check();
+         it++;
+         if (!cont) break;
+         Real* vi = Vp + (int64_t)i * ld;
+         // w = M^-1 A v_i
+         if (pre) {
+            TNLB_TRY_STATUS(c.spmv(vi, M_tmp.as<Real>()));
+            TNLB_TRY_STATUS(P.apply(n, M_tmp.as<Real>(), w.as<Real>(), c.st));
+         }
+         else
+            TNLB_TRY_STATUS(c.spmv(vi, w.as<Real>()));
+         for (int k = 0; k <= i; k++) H[k + i * (m + 1)] = 0.0;
+         const int reorth = (variant == TNLB_GMRES_CGSR || variant == TNLB_GMRES_MGSR) ? 2 : 1;
+         double normw = 0;
+         std::vector<double> hl(i + 1);
+         if (variant == TNLB_GMRES_CGS || variant == TNLB_GMRES_CGSR) {
+            for (int l = 0; l < reorth; l++) {
+               k_gmres_vtw<Real><<<vec_grid(n), kRedThreads, 0, c.st>>>(
+                  n, ld, i + 1, Vp, w.as<Real>(), W.partials.as<double>(), W.counter.as<unsigned>() + 1,
+                  hdev.as<double>());
+               TNLB_CHECK_LAUNCH();
+               const bool last = (l == reorth - 1);
+               k_gmres_wmvh<Real><<<vec_grid(n), kRedThreads, 0, c.st>>>(n, ld, i + 1, Vp, hdev.as<double>(),
+                                                                       w.as<Real>(), W.red(), last ? sc : nullptr);
+               TNLB_CHECK_LAUNCH();
+               TNLB_CUDA_TRY(cudaMemcpyAsync(hl.data(), hdev.ptr, sizeof(double) * (i + 1), cudaMemcpyDeviceToHost, c.st));
+               if (last) TNLB_CUDA_TRY(cudaMemcpyAsync(hs, sc, sizeof(double), cudaMemcpyDeviceToHost, c.st));
+               TNLB_CUDA_TRY(cudaStreamSynchronize(c.st));
+               for (int k = 0; k <= i; k++) H[k + i * (m + 1)] += hl[k];
+            }
+            normw = hs[0];
+         }
+         else {
+            // MGS: H_{k,i} = (w, v_k); w -= H_{k,i} v_k for k = 0..i, `reorth`
+            // passes.  Each kernel applies one update and computes the next
+            // dot product (or, after the last update, |w|).
+            double* hd = hdev.as<double>();  // pass l uses hd[l*64 .. l*64+i]
+            k_mgs_step<Real><<<vec_grid(n), kRedThreads, 0, c.st>>>(n, nullptr, nullptr, w.as<Real>(), Vp, W.red(),
+                                                                    hd);
+            TNLB_CHECK_LAUNCH();
+            for (int l = 0; l < reorth; l++) {
+               for (int k = 0; k <= i; k++) {
+                  const Real* vk = Vp + (int64_t)k * ld;
+                  const bool last_k = (k == i), last_l = (l == reorth - 1);
+                  const Real* next = !last_k ? Vp + (int64_t)(k + 1) * ld : (!last_l ? Vp : nullptr);
+                  double* out = !last_k ? hd + l * 64 + k + 1 : (!last_l ? hd + (l + 1) * 64 : sc);
+                  k_mgs_step<Real><<<vec_grid(n), kRedThreads, 0, c.st>>>(n, vk, hd + l * 64 + k, w.as<Real>(), next,
+                                                                          W.red(), out);
+                  TNLB_CHECK_LAUNCH();
+               }
+            }
+            std::vector<double> hall(2 * 64);
+            TNLB_CUDA_TRY(cudaMemcpyAsync(hall.data(), hd, sizeof(double) * 2 * 64, cudaMemcpyDeviceToHost, c.st));
+            TNLB_CUDA_TRY(cudaMemcpyAsync(hs, sc, sizeof(double), cudaMemcpyDeviceToHost, c.st));
+            TNLB_CUDA_TRY(cudaStreamSynchronize(c.st));
+            for (int l = 0; l < reorth; l++)
+               for (int k = 0; k <= i; k++) H[k + i * (m + 1)] += hall[l * 64 + k];
+            normw = hs[0];
+         }
+         H[i + 1 + i * (m + 1)] = normw;
+         k_scale<Real><<<vec_grid(n), kRedThreads, 0, c.st>>>(n, (Real)(1.0 / normw), w.as<Real>(),
+                                                              Vp + (int64_t)(i + 1) * ld);
+         TNLB_CHECK_LAUNCH();
+         // Givens rotations (GMRES.hpp:731-770)
+         for (int k = 0; k < i; k++) rot_apply(H[k + i * (m + 1)], H[k + 1 + i * (m + 1)], cs[k], sn[k]);
+         if (H[i + 1 + i * (m + 1)] != 0.0) {
+            const double dx = H[i + i * (m + 1)], dy = H[i + 1 + i * (m + 1)];
+            if (dy == 0.0) {
+               cs[i] = 1.0;
+               sn[i] = 0.0;
+            }
+            else if (std::fabs(dy) > std::fabs(dx)) {
+               const double t = dx / dy;
+               sn[i] = 1.0 / std::sqrt(1.0 + t * t);
+               cs[i] = t * sn[i];
+            }
+            else {
+               const double t = dy / dx;
+               cs[i] = 1.0 / std::sqrt(1.0 + t * t);
+               sn[i] = t * cs[i];
+            }
+            rot_apply(H[i + i * (m + 1)], H[i + 1 + i * (m + 1)], cs[i], sn[i]);
+            rot_apply(s[i], s[i + 1], cs[i], sn[i]);
+         }
+         residue = std::fabs(s[i + 1]) / normb;
+         if (!check()) {
+            o_steps = i;
+            break;
+         }
+      }
+      if (o_steps < m) {
+         TNLB_TRY_STATUS(update(o_steps));
+         break;
+      }
+      TNLB_TRY_STATUS(update(m - 1));
+      TNLB_TRY_STATUS(compute_residue());
+      const double beta_old = beta;
+      TNLB_TRY_STATUS(norm(r.as<Real>(), &beta));
+      residue = beta / normb;
+      ++restart_cycles;
+      beta_ratio = beta / beta_old;
+   }
+   TNLB_CUDA_TRY(cudaStreamSynchronize(c.st));
+   res->iterations = it;
+   res->residue = residue;
+   res->converged = check_convergence(residue, it, prm.max_iterations, prm.min_iterations, prm.convergence_residue,
+                                      prm.divergence_residue);
+   res->status_detail = 0;
+   return TNLB_OK;
+}
+
+template <typename Real>
+tnlb_status solve_t(tnlb_solver_kind solver, const tnlb_precond* pobj, const tnlb_solver_params& prm,
+                    const tnlb_segments* seg, tnlb_real real, const int32_t* cols, const Real* vals, const Real* b,
+                    Real* x, cudaStream_t st, tnlb_solve_result* res)
+{
+   Ctx<Real> c{seg, real, cols, vals, seg->n, st};
+   const Precond<Real> P = view<Real>(pobj);
+   switch (solver) {
+      case TNLB_SOLVER_CG:
+         if (P.kind == TNLB_PRECOND_ILU0) return pcg_general<Real>(c, P, prm, b, x, res);
+         return cg_solve<Real>(c, P, prm, b, x, res);
+      case TNLB_SOLVER_BICGSTAB: return bicgstab_solve<Real>(c, P, prm, b, x, res);
+      case TNLB_SOLVER_GMRES: return gmres_solve<Real>(c, P, prm, b, x, res);
+   }
+   set_error("unknown solver");
+   return TNLB_ERR_INVALID_ARGUMENT;
+}
+
+template <typename Real>
+__global__ void __launch_bounds__(kRedThreads) k_resid_norms(int64_t n, const Real* __restrict__ b,
+                                                             const Real* __restrict__ ax, RedWork w,
+                                                             double* __restrict__ out)
+{
+   double a0 = 0, a1 = 0;
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+      const double d = (double)b[i] - (double)ax[i];
+      a0 += d * d;
+      a1 += (double)b[i] * (double)b[i];
+   }
+   double v[2] = {a0, a1};
+   if (publish_and_arrive<2>(v, w)) {
+      double t[2];
+      gather_totals<2>(t, w);
+      if (threadIdx.x == 0) {
+         out[0] = t[0];
+         out[1] = t[1];
+      }
+   }
+}
+
+}  // namespace
+
+tnlb_status true_residual(const tnlb_segments* seg, tnlb_real real, const int32_t* cols, const void* vals,
+                          const void* b, const void* x, cudaStream_t st, double* out)
+{
+   const int64_t n = seg->n;
+   const size_t rs = real == TNLB_F64 ? 8 : 4;
+   DeviceBuffer ax;
+   Work W;
+   TNLB_TRY_STATUS(W.alloc());
+   TNLB_TRY_STATUS(ax.alloc(rs * (n > 0 ? n : 1)));
+   TNLB_TRY_STATUS(spmv_dispatch(seg, real, cols, vals, x, ax.ptr, 1.0, 0.0, st));
+   if (real == TNLB_F64)
+      k_resid_norms<double><<<vec_grid(n), kRedThreads, 0, st>>>(n, (const double*)b, ax.as<double>(), W.red(),
+                                                                  W.scratch.as<double>());
+   else
+      k_resid_norms<float><<<vec_grid(n), kRedThreads, 0, st>>>(n, (const float*)b, ax.as<float>(), W.red(),
+                                                                 W.scratch.as<double>());
+   TNLB_CHECK_LAUNCH();
+   double h[2];
+   TNLB_CUDA_TRY(cudaMemcpyAsync(h, W.scratch.ptr, sizeof(h), cudaMemcpyDeviceToHost, st));
+   TNLB_CUDA_TRY(cudaStreamSynchronize(st));
+   *out = std::sqrt(h[0]) / std::sqrt(h[1]);
+   return TNLB_OK;
+}
+
+tnlb_status precond_create(int kind, const tnlb_segments* seg, tnlb_real real, const int32_t* cols, const void* vals,
+                           cudaStream_t st, tnlb_precond** out)
+{
+   TNLB_REQUIRE(seg->n > 0, TNLB_ERR_INVALID_ARGUMENT, "Preconditioner::update: the matrix is empty");
+   auto* P = new tnlb_precond();
+   P->kind = kind;
+   P->real = real;
+   P->n = seg->n;
+   tnlb_status s = TNLB_OK;
+   if (kind == TNLB_PRECOND_JACOBI) {
+      s = P->diag.alloc((real == TNLB_F64 ? 8 : 4) * (size_t)seg->n);
+      if (s == TNLB_OK) {
+         if (real == TNLB_F64)
+            k_diag<double><<<grid_for(seg->n, 256), 256, 0, st>>>(view_of(seg), cols, (const double*)vals,
+                                                                 P->diag.as<double>());
+         else
+            k_diag<float><<<grid_for(seg->n, 256), 256, 0, st>>>(view_of(seg), cols, (const float*)vals,
+                                                                P->diag.as<float>());
+         if (cudaGetLastError() != cudaSuccess) {
+            set_error("Jacobi setup launch failed");
+            s = TNLB_ERR_CUDA;
+         }
+      }
+   }
+   else if (kind == TNLB_PRECOND_ILU0)
+      s = ilu0_create(seg, real, cols, vals, st, &P->ilu);
+   else if (kind == TNLB_PRECOND_FSAI)
+      s = fsai_create(seg, real, cols, vals, true, st, &P->fsai);
+   if (s != TNLB_OK) {
+      delete P;
+      return s;
+   }
+   *out = P;
+   return TNLB_OK;
+}
+
+tnlb_status solve(tnlb_solver_kind solver, const tnlb_precond* P, const tnlb_solver_params& prm,
+                  const tnlb_segments* seg, tnlb_real real, const int32_t* cols, const void* vals, const void* b,
+                  void* x, cudaStream_t st, tnlb_solve_result* res)
+{
+   TNLB_REQUIRE(!P || P->real == real, TNLB_ERR_INVALID_ARGUMENT, "preconditioner real type differs from the matrix");
+   TNLB_REQUIRE(!P || P->n == seg->n, TNLB_ERR_INVALID_ARGUMENT, "preconditioner size differs from the matrix");
+   if (real == TNLB_F64)
+      return solve_t<double>(solver, P, prm, seg, real, cols, (const double*)vals, (const double*)b, (double*)x, st,
+                             res);
+   return solve_t<float>(solver, P, prm, seg, real, cols, (const float*)vals, (const float*)b, (float*)x, st, res);
+}
+
+tnlb_status precond_apply(const tnlb_precond* P, const void* b, void* x, cudaStream_t st)
+{
+   if (P->real == TNLB_F64)
+      TNLB_TRY_STATUS(view<double>(P).apply(P->n, (const double*)b, (double*)x, st));
+   else
+      TNLB_TRY_STATUS(view<float>(P).apply(P->n, (const float*)b, (float*)x, st));
+   TNLB_CUDA_TRY(cudaStreamSynchronize(st));
+   return TNLB_OK;
+}
+
+// FP32 inner CG (Jacobi) inside FP64 iterative refinement.
+tnlb_status solve_mixed_cg(const tnlb_segments* seg, const int32_t* cols, const double* vals, const double* b,
+                           double* x, const tnlb_solver_params& prm, double inner_tol, int32_t max_outer,
+                           cudaStream_t st, tnlb_solve_result* res, int32_t* inner_total, int32_t* outer,
+                           int inner_kind, const tnlb_precond* inner_precond)
+{
+   const int64_t n = seg->n;
+   DeviceBuffer v32, r64, r32, d32, d64;
+   TNLB_TRY_STATUS(v32.alloc(sizeof(float) * (seg->storage > 0 ? seg->storage : 1)));
+   TNLB_TRY_STATUS(r64.alloc(sizeof(double) * n));
+   TNLB_TRY_STATUS(r32.alloc(sizeof(float) * n));
+   TNLB_TRY_STATUS(d32.alloc(sizeof(float) * n));
+   k_convert<float, double><<<grid_for(seg->storage, 256 * 8), 256, 0, st>>>(seg->storage, vals, v32.as<float>());
+   TNLB_CHECK_LAUNCH();
+   Ctx<float> c32{seg, TNLB_F32, cols, v32.as<float>(), n, st};
+   tnlb_precond* own = nullptr;
+   if (!inner_precond) TNLB_TRY_STATUS(precond_create(inner_kind, seg, TNLB_F32, cols, v32.ptr, st, &own));
+   struct Guard {
+      tnlb_precond* p;
+      ~Guard() { delete p; }
+   } guard{own};
+   const tnlb_precond* pobj = inner_precond ? inner_precond : own;
+   TNLB_REQUIRE(pobj->real == TNLB_F32, TNLB_ERR_INVALID_ARGUMENT, "the inner preconditioner must be FP32");
+   const Precond<float> P = view<float>(pobj);
+   tnlb_solver_params ip = prm;
+   ip.convergence_residue = inner_tol;
+   *inner_total = 0;
+   *outer = 0;
+   double resid = 0;
+   Work W;
+   TNLB_TRY_STATUS(W.alloc());
+   for (int o = 0; o <= max_outer; o++) {
+      // r = b - A x in FP64
+      TNLB_CUDA_TRY(cudaMemcpyAsync(r64.ptr, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+      TNLB_TRY_STATUS(spmv_dispatch(seg, TNLB_F64, cols, vals, x, r64.ptr, -1.0, 1.0, st));
+      k_dots<double><<<vec_grid(n), kRedThreads, 0, st>>>(n, r64.as<double>(), r64.as<double>(), b, b, W.red(),
+                                                          W.scratch.as<double>());
+      TNLB_CHECK_LAUNCH();
+      double h[2];
+      TNLB_CUDA_TRY(cudaMemcpyAsync(h, W.scratch.ptr, sizeof(h), cudaMemcpyDeviceToHost, st));
+      TNLB_CUDA_TRY(cudaStreamSynchronize(st));
+      const double rn = std::sqrt(h[0]), bn = std::sqrt(h[1]);
+      resid = bn > 0 ? rn / bn : 0.0;
+      if (bn == 0 || resid < prm.convergence_residue || o == max_outer) break;
+      // unit-norm FP32 residual, FP32 Jacobi-PCG correction
+      k_scale<double><<<vec_grid(n), kRedThreads, 0, st>>>(n, 1.0 / rn, r64.as<double>(), r64.as<double>());
+      k_convert<float, double><<<vec_grid(n), kRedThreads, 0, st>>>(n, r64.as<double>(), r32.as<float>());
+      TNLB_CUDA_TRY(cudaMemsetAsync(d32.ptr, 0, sizeof(float) * n, st));
+      TNLB_CHECK_LAUNCH();
+      tnlb_solve_result ir{};
+      if (P.kind == TNLB_PRECOND_ILU0)
+         TNLB_TRY_STATUS(pcg_general<float>(c32, P, ip, r32.as<float>(), d32.as<float>(), &ir));
+      else
+         TNLB_TRY_STATUS(cg_solve<float>(c32, P, ip, r32.as<float>(), d32.as<float>(), &ir));
+      *inner_total += ir.iterations;
+      (*outer)++;
+      // x += rn * d
+      k_axpby_mixed<<<vec_grid(n), kRedThreads, 0, st>>>(n, rn, d32.as<float>(), x);
+      TNLB_CHECK_LAUNCH();
+   }
+   res->iterations = *inner_total;
+   res->residue = resid;
+   res->converged = resid < prm.convergence_residue;
+   res->status_detail = 0;
+   return TNLB_OK;
+}
+
+}  // namespace tnlb
+
+tnlb_precond::~tnlb_precond()
+{
+   if (ilu) tnlb::ilu0_destroy(ilu);
+   if (fsai) tnlb::fsai_destroy(fsai);
+}

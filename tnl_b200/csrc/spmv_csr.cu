@@ -204,8 +204,10 @@ __global__ void __launch_bounds__(kTileThreads) k_csr_tile(const int32_t* __rest
                                                           Real* __restrict__ y, const int32_t* __restrict__ tile_row,
                                                           const int32_t* __restrict__ tile_nnz, int32_t n,
                                                           int32_t* __restrict__ carry_row, Real* __restrict__ carry_val,
-                                                          Real alpha, Real beta)
+                                                          Real alpha, Real beta, const int32_t* __restrict__ skip)
 {
+   // solvers pass their device `done` flag: nothing to do once they stopped
+   if (skip && *skip) return;
    __shared__ int32_t s_rowend[kTileSize + 1];
    __shared__ Real s_prod[kTileSize];
    __shared__ Real s_y[kTileSize];
@@ -332,8 +334,9 @@ __global__ void __launch_bounds__(kTileThreads) k_csr_tile(const int32_t* __rest
 // Adds the partial sums of rows split between tiles, in tile order.
 template <typename Real>
 __global__ void k_csr_tile_fixup(const int32_t* __restrict__ carry_row, const Real* __restrict__ carry_val,
-                                 int32_t tiles, Real* __restrict__ y, Real alpha)
+                                 int32_t tiles, Real* __restrict__ y, Real alpha, const int32_t* __restrict__ skip)
 {
+   if (skip && *skip) return;
    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
    if (t >= tiles) return;
    const int32_t r = carry_row[t];
@@ -397,7 +400,7 @@ int light_tps(int64_t storage, int32_t rows)
 template <typename Real>
 tnlb_status spmv_csr_t(const tnlb_segments* seg, const int32_t* cols, const Real* vals, const Real* x, Real* y,
                        Real alpha, Real beta, int32_t begin, int32_t end, tnlb_kernel kernel, int32_t tps,
-                       cudaStream_t st, int* launches)
+                       cudaStream_t st, int* launches, const int32_t* skip)
 {
    const int32_t* rowptr = seg->offsets.as<int32_t>();
    const bool full = begin == 0 && end == seg->n;
@@ -438,10 +441,10 @@ tnlb_status spmv_csr_t(const tnlb_segments* seg, const int32_t* cols, const Real
          }
          k_csr_tile<Real><<<seg->tiles, kTileThreads, 0, st>>>(
             rowptr, cols, vals, x, y, seg->tile_row.as<int32_t>(), seg->tile_nnz.as<int32_t>(), seg->n,
-            seg->carry_row.as<int32_t>(), seg->carry_val.as<Real>(), alpha, beta);
+            seg->carry_row.as<int32_t>(), seg->carry_val.as<Real>(), alpha, beta, skip);
          TNLB_CHECK_LAUNCH();
          k_csr_tile_fixup<Real><<<grid_for(seg->tiles, 256), 256, 0, st>>>(
-            seg->carry_row.as<int32_t>(), seg->carry_val.as<Real>(), seg->tiles, y, alpha);
+            seg->carry_row.as<int32_t>(), seg->carry_val.as<Real>(), seg->tiles, y, alpha, skip);
          TNLB_CHECK_LAUNCH();
          *launches = 2;
          return TNLB_OK;
@@ -471,13 +474,13 @@ tnlb_status build_csr_tile_plan(tnlb_segments* seg, cudaStream_t stream)
 
 tnlb_status spmv_csr(const tnlb_segments* seg, tnlb_real real, const int32_t* cols, const void* vals, const void* x,
                      void* y, double alpha, double beta, int32_t begin, int32_t end, tnlb_kernel kernel, int32_t tps,
-                     cudaStream_t stream, int* launches)
+                     cudaStream_t stream, int* launches, const int32_t* skip)
 {
    if (real == TNLB_F64)
       return spmv_csr_t<double>(seg, cols, (const double*)vals, (const double*)x, (double*)y, alpha, beta, begin, end,
-                                kernel, tps, stream, launches);
+                                kernel, tps, stream, launches, skip);
    return spmv_csr_t<float>(seg, cols, (const float*)vals, (const float*)x, (float*)y, (float)alpha, (float)beta,
-                            begin, end, kernel, tps, stream, launches);
+                            begin, end, kernel, tps, stream, launches, skip);
 }
 
 }  // namespace tnlb
