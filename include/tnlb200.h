@@ -320,6 +320,47 @@ tnlb_status tnlb_ilu0_factors(const tnlb_segments* seg, tnlb_real real, const in
                               int32_t* h_rowptr, int32_t* h_cols, void* h_values, int64_t capacity,
                               tnlb_stream stream);
 
+/* ------------------------------------------------- learned FSAI (new) */
+/* A per-row network (16 -> 64 -> 64 -> 64 -> 4, ReLU, BF16 weights, FP32
+ * accumulation) maps scale-free local coefficients of an SPD matrix A to the
+ * values of G on the lower triangle of A's pattern (at most 4 entries per
+ * row); M^-1 = G^T G.  No counterpart in the reference.  The features,
+ * network, output map and parameter layout are defined in
+ * oracle/lfsai_ref.py (FP64 restatement used by the tests). */
+typedef struct tnlb_lfsai tnlb_lfsai;
+
+/* Number of network parameters (9668). */
+int64_t tnlb_lfsai_num_params(void);
+/* New network with deterministic initial parameters from `seed`. */
+tnlb_status tnlb_lfsai_create(uint64_t seed, tnlb_stream stream, tnlb_lfsai** out);
+tnlb_status tnlb_lfsai_destroy(tnlb_lfsai* net);
+/* Parameters (FP32, tnlb_lfsai_num_params entries) to / from host memory;
+ * setting them resets the optimiser state. */
+tnlb_status tnlb_lfsai_get_params(const tnlb_lfsai* net, float* h_out, int64_t count);
+tnlb_status tnlb_lfsai_set_params(tnlb_lfsai* net, const float* h_in, int64_t count);
+/* Gradient of the last tnlb_lfsai_gradient call, FP32, to host memory. */
+tnlb_status tnlb_lfsai_get_grad(const tnlb_lfsai* net, float* h_out, int64_t count);
+/* Run the dense layers on tcgen05 tensor cores (1) or CUDA cores (0). */
+tnlb_status tnlb_lfsai_set_tensor_cores(tnlb_lfsai* net, int32_t enable);
+/* Loss and gradient on one matrix, kept in the handle.  mode 0: probe loss
+ * (1/(n P)) sum_p ||z_p - G A G^T z_p||^2 with P probe vectors stored one
+ * after another in d_probes (device, n*P values of `real`); mode 1: warm
+ * start, mean squared distance of the scaled outputs to the classical FSAI
+ * values.  Synchronous. */
+tnlb_status tnlb_lfsai_gradient(tnlb_lfsai* net, int32_t mode, const tnlb_segments* seg, tnlb_real real,
+                                const int32_t* d_cols, const void* d_values, const void* d_probes, int32_t nprobes,
+                                tnlb_stream stream, double* h_loss);
+/* One Adam step (beta1 0.9, beta2 0.999, eps 1e-8) with learning rate lr. */
+tnlb_status tnlb_lfsai_adam_step(tnlb_lfsai* net, double lr, tnlb_stream stream);
+/* The preconditioner M^-1 = G^T G of a matrix, G from the network. */
+tnlb_status tnlb_lfsai_precond_create(const tnlb_lfsai* net, const tnlb_segments* seg, tnlb_real real,
+                                      const int32_t* d_cols, const void* d_values, tnlb_stream stream,
+                                      tnlb_precond** out);
+/* Features (n*16) and raw network outputs (n*4) of a matrix, to host memory
+ * (either may be NULL).  Synchronous. */
+tnlb_status tnlb_lfsai_eval(const tnlb_lfsai* net, const tnlb_segments* seg, tnlb_real real, const int32_t* d_cols,
+                            const void* d_values, tnlb_stream stream, float* h_features, float* h_outputs);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,137 @@
+"""Learned FSAI on the GPU against its FP64 CPU reference (oracle/lfsai_ref.py).
+
+* features: FP32 on the GPU vs FP64, relative 1e-6;
+* network outputs and the gradient of the probe loss: the GPU accumulates in
+  FP32 and rounds layer inputs to BF16 from FP32 values, the reference from
+  FP64 ones, so a few inputs land on the other side of a BF16 rounding
+  boundary; the bound is on the relative 2-norm of the difference (2e-2)
+  and on the loss (1e-4 relative);
+* the reference backpropagation itself is checked against central finite
+  differences (BF16 rounding off) on the CPU in test_lfsai_reference_fd;
+* training lowers the loss, and the trained preconditioner needs fewer CG
+  iterations than Jacobi on an unseen problem.
+"""
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+def small_problem(N=24, seed=3):
+    from tnl_b200 import generators as g
+
+    return g.diffusion_2d(N, 0.1, 1.5, seed)
+
+
+def test_features_and_outputs_match_reference():
+    from oracle import lfsai_ref as R
+    import tnl_b200
+    from tnl_b200.lfsai import LearnedFSAI
+
+    A = small_problem()
+    M = tnl_b200.SparseMatrix.from_csr(A)
+    net = LearnedFSAI(seed=5)
+    theta = net.params().astype(np.float64)
+    assert np.array_equal(net.params(), R.init_params(5).astype(np.float32))
+    f_gpu, o_gpu = net.evaluate(M)
+    f_ref, s, pat = R.features(A)
+    assert np.allclose(f_gpu, f_ref, rtol=1e-6, atol=1e-7)
+    o_ref, _ = R.forward(theta, f_ref)
+    rel = np.linalg.norm(o_gpu - o_ref) / np.linalg.norm(o_ref)
+    assert rel < 2e-2, rel
+
+
+def test_gradient_matches_reference():
+    from oracle import lfsai_ref as R
+    import tnl_b200
+    from tnl_b200.lfsai import LearnedFSAI
+
+    A = small_problem(20, 4)
+    M = tnl_b200.SparseMatrix.from_csr(A)
+    net = LearnedFSAI(seed=9)
+    Z = LearnedFSAI.probes(M, 4, seed=1, residual_share=0.5)
+    loss = net.gradient(M, Z)
+    g_gpu = net.grad().astype(np.float64)
+    L_ref, g_ref = R.loss_and_grad(net.params().astype(np.float64), A, Z.cpu().numpy().T.copy())
+    assert loss == pytest.approx(L_ref, rel=1e-4)
+    rel = np.linalg.norm(g_gpu - g_ref) / np.linalg.norm(g_ref)
+    assert rel < 2e-2, rel
+
+
+def test_warm_start_and_training_lower_the_loss():
+    from tnl_b200.lfsai import LearnedFSAI, diffusion_problem
+
+    train = [diffusion_problem(48, s) for s in range(4)]
+    net = LearnedFSAI(seed=1)
+    fit = net.fit_classical(train, steps=150, lr=3e-3)
+    assert fit[-1] < 0.2 * fit[0]
+    probes = [LearnedFSAI.probes(M, 8, 100 + i) for i, M in enumerate(train)]
+    before = np.mean([net.gradient(M, Z) for M, Z in zip(train, probes)])
+    net.train(train, steps=200, nprobes=8, lr=5e-4)
+    after = np.mean([net.gradient(M, Z) for M, Z in zip(train, probes)])
+    assert after < before
+
+
+def test_learned_preconditioner_beats_jacobi_on_unseen_problem():
+    import tnl_b200
+    from tnl_b200 import generators as g
+    from tnl_b200.lfsai import LearnedFSAI, diffusion_problem
+
+    train = [diffusion_problem(64, s) for s in range(6)]
+    net = LearnedFSAI(seed=2)
+    net.fit_classical(train, steps=200, lr=3e-3)
+    net.train(train, steps=150, nprobes=8, lr=5e-4)
+    M = diffusion_problem(96, 1234)
+    b = torch.tensor(g.uniform_vector(M.getRows(), 1), device="cuda")
+    its = {}
+    for name in ("jacobi", "learned"):
+        S = tnl_b200.CG()
+        S.setMatrix(M)
+        S.setConvergenceResidue(1e-8)
+        P = tnl_b200.Diagonal() if name == "jacobi" else None
+        if P is not None:
+            P.update(M)
+        else:
+            P = net.preconditioner(M)
+        S.setPreconditioner(P)
+        x = torch.zeros(M.getRows(), dtype=torch.float64, device="cuda")
+        assert S.solve(b, x)
+        its[name] = S.getIterations()
+        assert tnl_b200.true_residual(M, b, x) < 1e-6
+    assert its["learned"] < 0.8 * its["jacobi"], its
+
+
+def test_mixed_precision_with_learned_preconditioner():
+    import tnl_b200
+    from tnl_b200 import generators as g
+    from tnl_b200.lfsai import LearnedFSAI, diffusion_problem
+
+    train = [diffusion_problem(48, s) for s in range(3)]
+    net = LearnedFSAI(seed=4)
+    net.fit_classical(train, steps=150, lr=3e-3)
+    M = diffusion_problem(80, 77)
+    A32 = tnl_b200.SparseMatrix(tnl_b200.CSR, torch.float32)
+    A32.assign(M.segments.getOffsets(), M.getColumnIndexes().cpu().numpy(), M.getValues().cpu().numpy())
+    P32 = net.preconditioner(A32)
+    b = torch.tensor(g.uniform_vector(M.getRows(), 1), device="cuda")
+    x = torch.zeros(M.getRows(), dtype=torch.float64, device="cuda")
+    r = tnl_b200.solve_mixed(M, b, x, tol=1e-8, inner_tol=1e-4, inner=P32)
+    assert r["converged"] and tnl_b200.true_residual(M, b, x) < 1e-8
+
+
+def test_tensor_core_forward_matches_cuda_cores():
+    """tcgen05 (BF16 in shared memory, FP32 accumulators in TMEM) against the
+    CUDA-core layers: same BF16 operands, FP32 sums in another order."""
+    from tnl_b200.lfsai import LearnedFSAI, diffusion_problem
+
+    net = LearnedFSAI(seed=3)
+    for N in (16, 64, 181):  # 256, 4096 and 32761 rows (ragged last tile)
+        M = diffusion_problem(N, 5 + N)
+        _, o_cc = net.evaluate(M)
+        net.set_tensor_cores(True)
+        _, o_tc = net.evaluate(M)
+        net.set_tensor_cores(False)
+        rel = np.linalg.norm(o_tc - o_cc) / np.linalg.norm(o_cc)
+        assert rel < 1e-3, (N, rel)
+        assert np.max(np.abs(o_tc - o_cc)) < 1e-2

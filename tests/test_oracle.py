@@ -177,3 +177,27 @@ def test_bicgstab_within_reference_spread(oracle, reference):
     spread = max(its) - min(its)
     assert min(its) - max(2, spread) <= o["iterations"] <= max(its) + max(2, spread), (o["iterations"], its)
     assert oracle.true_residual(A, b, o["x"]) < 1e-7
+
+
+def test_lfsai_reference_fd():
+    """The FP64 backpropagation of the learned-FSAI reference against central
+    finite differences (BF16 rounding off)."""
+    from oracle import lfsai_ref as R
+    from tnl_b200 import generators as g
+
+    A = g.diffusion_2d(10, 0.2, 1.0, 3)
+    theta = R.init_params(7)
+    rng = np.random.default_rng(0)
+    Z = rng.choice([-1.0, 1.0], size=(A.n, 3))
+    old = R.ROUND
+    R.ROUND = False
+    try:
+        _, grad = R.loss_and_grad(theta, A, Z)
+        idx = np.nonzero(np.abs(grad) > 1e-4 * np.abs(grad).max())[0]
+        for i in rng.choice(idx, 10, replace=False):
+            e = np.zeros_like(theta)
+            e[i] = 1e-6
+            fd = (R.loss_and_grad(theta + e, A, Z)[0] - R.loss_and_grad(theta - e, A, Z)[0]) / 2e-6
+            assert fd == pytest.approx(grad[i], rel=1e-5, abs=1e-10)
+    finally:
+        R.ROUND = old

@@ -110,6 +110,17 @@ tnlb_precond_solve = _sig("tnlb_precond_solve", [_p, _p, _p, _p])
 tnlb_precond_destroy = _sig("tnlb_precond_destroy", [_p])
 tnlb_solve_preconditioned = _sig("tnlb_solve_preconditioned", [C.c_int, _p, C.POINTER(SolverParams), _p, C.c_int, _p,
                                                                _p, _p, _p, _p, C.POINTER(SolveResult)])
+tnlb_lfsai_num_params = _sig("tnlb_lfsai_num_params", [], _i64)
+tnlb_lfsai_create = _sig("tnlb_lfsai_create", [C.c_uint64, _p, C.POINTER(_p)])
+tnlb_lfsai_destroy = _sig("tnlb_lfsai_destroy", [_p])
+tnlb_lfsai_get_params = _sig("tnlb_lfsai_get_params", [_p, _p, _i64])
+tnlb_lfsai_set_params = _sig("tnlb_lfsai_set_params", [_p, _p, _i64])
+tnlb_lfsai_get_grad = _sig("tnlb_lfsai_get_grad", [_p, _p, _i64])
+tnlb_lfsai_set_tensor_cores = _sig("tnlb_lfsai_set_tensor_cores", [_p, _i32])
+tnlb_lfsai_gradient = _sig("tnlb_lfsai_gradient", [_p, _i32, _p, C.c_int, _p, _p, _p, _i32, _p, C.POINTER(_f64)])
+tnlb_lfsai_adam_step = _sig("tnlb_lfsai_adam_step", [_p, _f64, _p])
+tnlb_lfsai_precond_create = _sig("tnlb_lfsai_precond_create", [_p, _p, C.c_int, _p, _p, _p, C.POINTER(_p)])
+tnlb_lfsai_eval = _sig("tnlb_lfsai_eval", [_p, _p, C.c_int, _p, _p, _p, _p, _p])
 tnlb_ilu0_factors = _sig("tnlb_ilu0_factors", [_p, C.c_int, _p, _p, _p, _p, _p, _i64, _p])
 
 

@@ -5,6 +5,7 @@
 #include <new>
 
 #include "internal.cuh"
+#include "lfsai.cuh"
 
 namespace tnlb {
 
@@ -392,6 +393,104 @@ tnlb_status tnlb_ilu0_factors(const tnlb_segments* seg, tnlb_real real, const in
    if (s == TNLB_OK) s = tnlb::ilu0_read(ilu, h_rowptr, h_cols, h_values, capacity, real == TNLB_F64 ? 8 : 4);
    if (ilu) tnlb::ilu0_destroy(ilu);
    return s;
+}
+
+int64_t tnlb_lfsai_num_params(void) { return kLfParams; }
+
+tnlb_status tnlb_lfsai_create(uint64_t seed, tnlb_stream stream, tnlb_lfsai** out)
+{
+   clear_error();
+   TNLB_REQUIRE(out != nullptr, TNLB_ERR_INVALID_ARGUMENT, "null argument");
+   auto* net = new (std::nothrow) tnlb_lfsai();
+   TNLB_REQUIRE(net != nullptr, TNLB_ERR_OUT_OF_MEMORY, "out of host memory");
+   tnlb_status s = lfsai_init(net, seed, (cudaStream_t)stream);
+   if (s != TNLB_OK) {
+      delete net;
+      return s;
+   }
+   *out = net;
+   return TNLB_OK;
+}
+
+tnlb_status tnlb_lfsai_destroy(tnlb_lfsai* net)
+{
+   clear_error();
+   delete net;
+   return TNLB_OK;
+}
+
+tnlb_status tnlb_lfsai_get_params(const tnlb_lfsai* net, float* h_out, int64_t count)
+{
+   clear_error();
+   TNLB_REQUIRE(net && h_out && count >= kLfParams, TNLB_ERR_INVALID_ARGUMENT, "bad arguments");
+   TNLB_CUDA_TRY(cudaMemcpy(h_out, net->theta.ptr, sizeof(float) * kLfParams, cudaMemcpyDeviceToHost));
+   return TNLB_OK;
+}
+
+tnlb_status tnlb_lfsai_set_params(tnlb_lfsai* net, const float* h_in, int64_t count)
+{
+   clear_error();
+   TNLB_REQUIRE(net && h_in && count >= kLfParams, TNLB_ERR_INVALID_ARGUMENT, "bad arguments");
+   TNLB_CUDA_TRY(cudaMemcpy(net->theta.ptr, h_in, sizeof(float) * kLfParams, cudaMemcpyHostToDevice));
+   TNLB_CUDA_TRY(cudaMemset(net->m.ptr, 0, sizeof(float) * kLfParams));
+   TNLB_CUDA_TRY(cudaMemset(net->v.ptr, 0, sizeof(float) * kLfParams));
+   net->step = 0;
+   return TNLB_OK;
+}
+
+tnlb_status tnlb_lfsai_get_grad(const tnlb_lfsai* net, float* h_out, int64_t count)
+{
+   clear_error();
+   TNLB_REQUIRE(net && h_out && count >= kLfParams, TNLB_ERR_INVALID_ARGUMENT, "bad arguments");
+   TNLB_CUDA_TRY(cudaMemcpy(h_out, net->grad.ptr, sizeof(float) * kLfParams, cudaMemcpyDeviceToHost));
+   return TNLB_OK;
+}
+
+tnlb_status tnlb_lfsai_set_tensor_cores(tnlb_lfsai* net, int32_t enable)
+{
+   clear_error();
+   TNLB_REQUIRE(net != nullptr, TNLB_ERR_INVALID_ARGUMENT, "null network");
+   net->use_tc = enable ? 1 : 0;
+   return TNLB_OK;
+}
+
+tnlb_status tnlb_lfsai_gradient(tnlb_lfsai* net, int32_t mode, const tnlb_segments* seg, tnlb_real real,
+                                const int32_t* d_cols, const void* d_values, const void* d_probes, int32_t nprobes,
+                                tnlb_stream stream, double* h_loss)
+{
+   clear_error();
+   TNLB_REQUIRE(net && seg && h_loss, TNLB_ERR_INVALID_ARGUMENT, "null argument");
+   TNLB_REQUIRE(mode == 0 || mode == 1, TNLB_ERR_INVALID_ARGUMENT, "mode must be 0 (probe loss) or 1 (warm start)");
+   TNLB_REQUIRE(mode == 1 || (d_probes && nprobes > 0), TNLB_ERR_INVALID_ARGUMENT, "probe vectors required");
+   TNLB_REQUIRE(seg->n > 0, TNLB_ERR_INVALID_ARGUMENT, "the matrix is empty");
+   return lfsai_gradient(net, seg, real, d_cols, d_values, d_probes, nprobes, mode == 1, (cudaStream_t)stream, h_loss);
+}
+
+tnlb_status tnlb_lfsai_adam_step(tnlb_lfsai* net, double lr, tnlb_stream stream)
+{
+   clear_error();
+   TNLB_REQUIRE(net != nullptr, TNLB_ERR_INVALID_ARGUMENT, "null network");
+   return lfsai_adam(net, lr, (cudaStream_t)stream);
+}
+
+tnlb_status tnlb_lfsai_precond_create(const tnlb_lfsai* net, const tnlb_segments* seg, tnlb_real real,
+                                      const int32_t* d_cols, const void* d_values, tnlb_stream stream,
+                                      tnlb_precond** out)
+{
+   clear_error();
+   TNLB_REQUIRE(net && seg && out, TNLB_ERR_INVALID_ARGUMENT, "null argument");
+   TNLB_REQUIRE(seg->n > 0, TNLB_ERR_INVALID_ARGUMENT, "the matrix is empty");
+   *out = nullptr;
+   return lfsai_precond(net, seg, real, d_cols, d_values, (cudaStream_t)stream, out);
+}
+
+tnlb_status tnlb_lfsai_eval(const tnlb_lfsai* net, const tnlb_segments* seg, tnlb_real real, const int32_t* d_cols,
+                            const void* d_values, tnlb_stream stream, float* h_features, float* h_outputs)
+{
+   clear_error();
+   TNLB_REQUIRE(net && seg, TNLB_ERR_INVALID_ARGUMENT, "null argument");
+   TNLB_REQUIRE(seg->n > 0, TNLB_ERR_INVALID_ARGUMENT, "the matrix is empty");
+   return lfsai_eval(net, seg, real, d_cols, d_values, (cudaStream_t)stream, h_features, h_outputs);
 }
 
 }  // extern "C"

@@ -14,27 +14,11 @@
 // t = G r, z = G^T t, with G^T stored explicitly (transposed once).
 #include <vector>
 
+#include "fsai.cuh"
 #include "internal.cuh"
 #include "segview.cuh"
 
 namespace tnlb {
-
-// Lower-triangular pattern + values of G and its transpose, both as CSR
-// segments the SpMV kernels run on.
-struct Fsai {
-   int32_t n = 0;
-   tnlb_real real = TNLB_F64;
-   tnlb_segments* g = nullptr;   // CSR of G
-   tnlb_segments* gt = nullptr;  // CSR of G^T
-   DeviceBuffer g_cols, g_vals, gt_cols, gt_vals, gt_src, tmp;
-   // source CSR of A (gathered) for the classical construction and features
-   DeviceBuffer a_rp, a_cols, a_vals;
-   ~Fsai()
-   {
-      delete g;
-      delete gt;
-   }
-};
 
 namespace {
 

@@ -36,9 +36,9 @@ void clear_error();
       }                                                                                                        \
    } while (0)
 
-#define TNLB_TRY_STATUS(expr)                                                                                  \
+#define TNLB_TRY_STATUS(...)                                                                                   \
    do {                                                                                                        \
-      tnlb_status _s = (expr);                                                                                 \
+      tnlb_status _s = (__VA_ARGS__);                                                                          \
       if (_s != TNLB_OK) return _s;                                                                            \
    } while (0)
 

@@ -1,0 +1,636 @@
+// lfsai.cu -- learned factorised sparse approximate inverse (no counterpart
+// in the reference library).
+//
+// A per-row network maps local, scale-free coefficients of A to the values of
+// G on the lower triangle of A's pattern (at most 4 entries per row); the
+// preconditioner is M^-1 = G^T G, applied by two SpMVs (fsai.cu), so CG stays
+// symmetric positive definite.  Training minimises the probe estimate of
+// ||I - G A G^T||_F^2 / n:
+//    L = 1/(n P) sum_p ||z_p - G A G^T z_p||^2,
+//    dL/dG = -2/(n P) sum_p (u_p w_p^T + z_p q_p^T) on G's pattern,
+// with w = A G^T z, u = z - G w, q = A G^T u -- every product a library SpMV.
+//
+// Definitions of the features, the network (16 -> 64 -> 64 -> 64 -> 4, ReLU,
+// BF16 weights and layer inputs, FP32 accumulation), the output map
+// (G'_diag = exp(o_3), G_ij = G'_ij / sqrt(a_jj)) and the parameter layout are
+// written out in the CPU reference the tests use (oracle/lfsai_ref.py); this
+// file implements exactly those.  Dense layers: the tensor-core path
+// (lfsai_tc.cu, tcgen05 with accumulators in TMEM) when `use_tc`, else the
+// CUDA-core kernels below, which also serve as its on-GPU reference.
+#include <cmath>
+#include <vector>
+
+#include "fsai.cuh"
+#include "internal.cuh"
+#include "lfsai.cuh"
+#include "reduce.cuh"
+#include "segview.cuh"
+
+namespace tnlb {
+
+namespace lf {
+
+__device__ __forceinline__ float bf16r(float x)
+{
+   // round to nearest even BF16, kept in FP32
+   uint32_t u = __float_as_uint(x);
+   u = (u + 0x7FFFu + ((u >> 16) & 1u)) & 0xFFFF0000u;
+   return __uint_as_float(u);
+}
+
+template <typename Real>
+__device__ __forceinline__ Real lookup(const int32_t* rp, const int32_t* cols, const Real* vals, int32_t r, int32_t c)
+{
+   int32_t lo = rp[r], hi = rp[r + 1] - 1;
+   while (lo <= hi) {
+      const int32_t mid = (lo + hi) >> 1;
+      const int32_t cm = cols[mid];
+      if (cm == c) return vals[mid];
+      if (cm < c)
+         lo = mid + 1;
+      else
+         hi = mid - 1;
+   }
+   return Real(0);
+}
+
+// Features (n x 16, FP32) and scaling s = 1/sqrt(diag) from A (CSR, ascending
+// columns) and G's pattern.
+template <typename Real>
+__global__ void k_features(const int32_t* __restrict__ arp, const int32_t* __restrict__ acols,
+                           const Real* __restrict__ avals, const int32_t* __restrict__ grp,
+                           const int32_t* __restrict__ gcols, int32_t n, float* __restrict__ f, Real* __restrict__ s,
+                           int32_t* __restrict__ err)
+{
+   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+   if (i >= n) return;
+   const int32_t b = grp[i], k = grp[i + 1] - b;
+   float out[kLfF];
+#pragma unroll
+   for (int q = 0; q < kLfF; q++) out[q] = 0.f;
+   if (k > kLfK || k < 1) {
+      atomicExch(err, 1);
+      for (int q = 0; q < kLfF; q++) f[i * kLfF + q] = 0.f;
+      return;
+   }
+   int32_t slot_col[kLfK];
+#pragma unroll
+   for (int t = 0; t < kLfK; t++) slot_col[t] = -1;
+   for (int t = 0; t < k; t++) slot_col[kLfK - k + t] = gcols[b + t];
+   auto sc = [&](int32_t j) -> double {
+      const double d = (double)lookup(arp, acols, avals, j, j);
+      return 1.0 / sqrt(d);
+   };
+   const int pp[6] = {0, 0, 0, 1, 1, 2}, qq[6] = {1, 2, 3, 2, 3, 3};
+   for (int m = 0; m < 6; m++) {
+      const int32_t jp = slot_col[pp[m]], jq = slot_col[qq[m]];
+      if (jp >= 0 && jq >= 0) out[m] = (float)((double)lookup(arp, acols, avals, jp, jq) * sc(jp) * sc(jq));
+   }
+   const double si = sc((int32_t)i);
+   int up = 0, nup = 0;
+   for (int32_t q = arp[i]; q < arp[i + 1]; q++) {
+      const int32_t j = acols[q];
+      if (j > i) {
+         if (up < 3) out[6 + up++] = (float)((double)avals[q] * si * sc(j));
+         nup++;
+      }
+   }
+   out[9] = (float)k / 4.f;
+   out[10] = (float)nup / 3.f;
+#pragma unroll
+   for (int q = 0; q < kLfF; q++) f[i * kLfF + q] = out[q];
+   s[i] = (Real)si;
+}
+
+// BF16-rounded copy of the weights (biases kept FP32) for the forward pass.
+__global__ void k_round_weights(const float* __restrict__ theta, float* __restrict__ wr)
+{
+   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < kLfParams; q += gridDim.x * blockDim.x) {
+      const bool bias = (q >= kLfB1 && q < kLfW2) || (q >= kLfB2 && q < kLfW3) || (q >= kLfB3 && q < kLfW4) || q >= kLfB4;
+      wr[q] = bias ? theta[q] : bf16r(theta[q]);
+   }
+}
+
+// One layer of the network on CUDA cores, one thread per row:
+// out = act(W bf16(in) + b); `in` has `fin` columns, `out` `fout`.
+// Stores the pre-rounding output (the next layer rounds it again).
+template <int FIN, int FOUT, bool RELU>
+__global__ void __launch_bounds__(128) k_layer(const float* __restrict__ in, int64_t n, const float* __restrict__ W,
+                                               const float* __restrict__ bias, float* __restrict__ out)
+{
+   __shared__ float sW[FOUT * FIN];
+   __shared__ float sb[FOUT];
+   for (int q = threadIdx.x; q < FOUT * FIN; q += blockDim.x) sW[q] = W[q];
+   for (int q = threadIdx.x; q < FOUT; q += blockDim.x) sb[q] = bias[q];
+   __syncthreads();
+   const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+   if (r >= n) return;
+   float x[FIN];
+#pragma unroll
+   for (int q = 0; q < FIN; q++) x[q] = bf16r(in[r * FIN + q]);
+   for (int o = 0; o < FOUT; o++) {
+      float acc = sb[o];
+#pragma unroll
+      for (int q = 0; q < FIN; q++) acc = fmaf(sW[o * FIN + q], x[q], acc);
+      out[r * FOUT + o] = RELU ? fmaxf(acc, 0.f) : acc;
+   }
+}
+
+// G values on G's pattern from the network outputs o (n x 4).
+template <typename Real>
+__global__ void k_g_values(const float* __restrict__ o, const Real* __restrict__ s, const int32_t* __restrict__ grp,
+                           const int32_t* __restrict__ gcols, int32_t n, Real* __restrict__ gvals)
+{
+   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+   if (i >= n) return;
+   const int32_t b = grp[i], k = grp[i + 1] - b;
+   for (int t = 0; t < k; t++) {
+      const int slot = kLfK - k + t;
+      const double gp = slot == kLfK - 1 ? exp((double)o[i * kLfK + slot]) : (double)o[i * kLfK + slot];
+      gvals[b + t] = (Real)(gp * (double)s[gcols[b + t]]);
+   }
+}
+
+// u = z - v and sum of u^2 (for the loss)
+template <typename Real>
+__global__ void __launch_bounds__(kRedThreads) k_resid(int64_t n, const Real* __restrict__ z, const Real* __restrict__ v,
+                                                       Real* __restrict__ u, RedWork w, double* __restrict__ out)
+{
+   double acc = 0;
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+      const Real ui = z[i] - v[i];
+      u[i] = ui;
+      acc += (double)ui * (double)ui;
+   }
+   double vv[1] = {acc};
+   if (publish_and_arrive<1>(vv, w)) {
+      double t[1];
+      gather_totals<1>(t, w);
+      if (threadIdx.x == 0) *out += t[0];
+   }
+}
+
+// dG_ij += c (u_i w_j + z_i q_j) on G's pattern (thread per row)
+template <typename Real>
+__global__ void k_dg(const int32_t* __restrict__ grp, const int32_t* __restrict__ gcols, int32_t n,
+                     const Real* __restrict__ u, const Real* __restrict__ w, const Real* __restrict__ z,
+                     const Real* __restrict__ q, double c, double* __restrict__ dg)
+{
+   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+   if (i >= n) return;
+   const double ui = u[i], zi = z[i];
+   for (int32_t e = grp[i]; e < grp[i + 1]; e++) {
+      const int32_t j = gcols[e];
+      dg[e] += c * (ui * (double)w[j] + zi * (double)q[j]);
+   }
+}
+
+// dL/do from dL/dG (FP32 per row, 4 slots)
+template <typename Real>
+__global__ void k_do(const double* __restrict__ dg, const float* __restrict__ o, const Real* __restrict__ s,
+                     const int32_t* __restrict__ grp, const int32_t* __restrict__ gcols, int32_t n,
+                     float* __restrict__ dout)
+{
+   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+   if (i >= n) return;
+   float d[kLfK] = {0.f, 0.f, 0.f, 0.f};
+   const int32_t b = grp[i], k = grp[i + 1] - b;
+   for (int t = 0; t < k; t++) {
+      const int slot = kLfK - k + t;
+      double v = dg[b + t] * (double)s[gcols[b + t]];
+      if (slot == kLfK - 1) v *= exp((double)o[i * kLfK + slot]);
+      d[slot] = (float)v;
+   }
+#pragma unroll
+   for (int t = 0; t < kLfK; t++) dout[i * kLfK + t] = d[t];
+}
+
+// delta_in = (W^T delta_out) masked by (h_in > 0), thread per row.
+template <int FIN, int FOUT>
+__global__ void __launch_bounds__(128) k_back_layer(const float* __restrict__ dout, const float* __restrict__ h_in,
+                                                    int64_t n, const float* __restrict__ W, float* __restrict__ din)
+{
+   __shared__ float sW[FOUT * FIN];
+   for (int q = threadIdx.x; q < FOUT * FIN; q += blockDim.x) sW[q] = W[q];
+   __syncthreads();
+   const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+   if (r >= n) return;
+   float d[FOUT];
+#pragma unroll
+   for (int o = 0; o < FOUT; o++) d[o] = dout[r * FOUT + o];
+   for (int q = 0; q < FIN; q++) {
+      float acc = 0.f;
+#pragma unroll
+      for (int o = 0; o < FOUT; o++) acc = fmaf(sW[o * FIN + q], d[o], acc);
+      din[r * FIN + q] = h_in[r * FIN + q] > 0.f ? acc : 0.f;
+   }
+}
+
+// Weight gradient of one layer: dW (FOUT x FIN) = sum_r dout_r^T bf16(in_r),
+// db = sum_r dout_r.  Per block a chunk of rows; partials then a reduction.
+template <int FIN, int FOUT>
+__global__ void __launch_bounds__(256) k_wgrad(const float* __restrict__ dout, const float* __restrict__ in, int64_t n,
+                                               int64_t rows_per_block, float* __restrict__ partial)
+{
+   constexpr int NW = FOUT * FIN + FOUT;
+   __shared__ float sd[32][FOUT];
+   __shared__ float sx[32][FIN];
+   float acc[(NW + 255) / 256];
+#pragma unroll
+   for (int q = 0; q < (NW + 255) / 256; q++) acc[q] = 0.f;
+   const int64_t r0 = (int64_t)blockIdx.x * rows_per_block;
+   const int64_t r1 = imin64(n, r0 + rows_per_block);
+   for (int64_t rb = r0; rb < r1; rb += 32) {
+      __syncthreads();
+      for (int q = threadIdx.x; q < 32 * FOUT; q += 256) {
+         const int64_t r = rb + q / FOUT;
+         sd[q / FOUT][q % FOUT] = r < r1 ? dout[r * FOUT + q % FOUT] : 0.f;
+      }
+      for (int q = threadIdx.x; q < 32 * FIN; q += 256) {
+         const int64_t r = rb + q / FIN;
+         sx[q / FIN][q % FIN] = r < r1 ? bf16r(in[r * FIN + q % FIN]) : 0.f;
+      }
+      __syncthreads();
+#pragma unroll
+      for (int q = 0; q < (NW + 255) / 256; q++) {
+         const int e = threadIdx.x + q * 256;
+         if (e < FOUT * FIN) {
+            const int o = e / FIN, c = e % FIN;
+            float a = acc[q];
+            for (int rr = 0; rr < 32; rr++) a = fmaf(sd[rr][o], sx[rr][c], a);
+            acc[q] = a;
+         }
+         else if (e < NW) {
+            const int o = e - FOUT * FIN;
+            float a = acc[q];
+            for (int rr = 0; rr < 32; rr++) a += sd[rr][o];
+            acc[q] = a;
+         }
+      }
+   }
+#pragma unroll
+   for (int q = 0; q < (NW + 255) / 256; q++) {
+      const int e = threadIdx.x + q * 256;
+      if (e < NW) partial[(int64_t)blockIdx.x * NW + e] = acc[q];
+   }
+}
+
+// Sum block partials into the gradient slice [W | b] (FP64 sums, fixed order).
+__global__ void k_sum_partials(const float* __restrict__ partial, int blocks, int nw, float* __restrict__ gW,
+                               float* __restrict__ gb, int nwW)
+{
+   const int e = blockIdx.x * blockDim.x + threadIdx.x;
+   if (e >= nw) return;
+   double s = 0;
+   for (int b = 0; b < blocks; b++) s += partial[(int64_t)b * nw + e];
+   if (e < nwW)
+      gW[e] = (float)s;
+   else
+      gb[e - nwW] = (float)s;
+}
+
+__global__ void k_adam(float* __restrict__ theta, const float* __restrict__ g, float* __restrict__ m,
+                       float* __restrict__ v, int np, float lr, float b1, float b2, float eps, float c1, float c2)
+{
+   const int q = blockIdx.x * blockDim.x + threadIdx.x;
+   if (q >= np) return;
+   const float gq = g[q];
+   const float mq = b1 * m[q] + (1.f - b1) * gq;
+   const float vq = b2 * v[q] + (1.f - b2) * gq * gq;
+   m[q] = mq;
+   v[q] = vq;
+   theta[q] -= lr * (mq / c1) / (sqrtf(vq / c2) + eps);
+}
+
+// Supervised warm start: dL/do for L = 1/n sum_rows ||G'_row - target'||^2
+// over occupied slots (target' = classical FSAI values in the scaled frame).
+template <typename Real>
+__global__ void __launch_bounds__(kRedThreads) k_fit_do(const float* __restrict__ o, const Real* __restrict__ target,
+                                                        const Real* __restrict__ s, const int32_t* __restrict__ grp,
+                                                        const int32_t* __restrict__ gcols, int32_t n,
+                                                        float* __restrict__ dout, RedWork w, double* __restrict__ loss)
+{
+   double acc = 0;
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+      float d[kLfK] = {0.f, 0.f, 0.f, 0.f};
+      const int32_t b = grp[i], k = grp[i + 1] - b;
+      for (int t = 0; t < k; t++) {
+         const int slot = kLfK - k + t;
+         const double tp = (double)target[b + t] / (double)s[gcols[b + t]];
+         const double op = o[i * kLfK + slot];
+         const double gp = slot == kLfK - 1 ? exp(op) : op;
+         const double e = gp - tp;
+         acc += e * e;
+         d[slot] = (float)(2.0 * e * (slot == kLfK - 1 ? gp : 1.0) / n);
+      }
+      for (int t = 0; t < kLfK; t++) dout[i * kLfK + t] = d[t];
+   }
+   double vv[1] = {acc};
+   if (publish_and_arrive<1>(vv, w)) {
+      double t[1];
+      gather_totals<1>(t, w);
+      if (threadIdx.x == 0) *loss = t[0] / n;
+   }
+}
+
+__global__ void k_init_params(uint64_t seed, float* __restrict__ theta)
+{
+   const int q = blockIdx.x * blockDim.x + threadIdx.x;
+   if (q >= kLfParams) return;
+   // layer of parameter q: U(-a, a), a = sqrt(6/(fan_in+fan_out)), W4 x 0.1, biases 0
+   float a = 0.f;
+   if (q < kLfB1)
+      a = sqrtf(6.f / (kLfF + kLfH));
+   else if (q >= kLfW2 && q < kLfB2)
+      a = sqrtf(6.f / (kLfH + kLfH));
+   else if (q >= kLfW3 && q < kLfB3)
+      a = sqrtf(6.f / (kLfH + kLfH));
+   else if (q >= kLfW4 && q < kLfB4)
+      a = 0.1f * sqrtf(6.f / (kLfH + kLfK));
+   uint64_t z = seed * 0x9E3779B97F4A7C15ull + (uint64_t)q;
+   z += 0x9E3779B97F4A7C15ull;
+   z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+   z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+   z ^= z >> 31;
+   const double u = (double)(z >> 11) * (1.0 / 9007199254740992.0);
+   theta[q] = (float)((2.0 * u - 1.0) * a);
+}
+
+}  // namespace lf
+
+// ------------------------------------------------------------------ host
+
+struct LfsaiMatrix {
+   Fsai* F = nullptr;      // pattern of G, transpose map, CSR of A
+   DeviceBuffer feat, s;   // n x 16 features, scaling
+   DeviceBuffer target;    // classical FSAI values (warm start)
+   ~LfsaiMatrix() { fsai_destroy(F); }
+};
+
+namespace {
+
+template <typename Real>
+tnlb_status build_matrix_ctx(const tnlb_segments* seg, tnlb_real real, const int32_t* cols, const Real* vals,
+                             cudaStream_t st, LfsaiMatrix* M)
+{
+   TNLB_TRY_STATUS(fsai_create(seg, real, cols, vals, false, st, &M->F));
+   const int32_t n = seg->n;
+   TNLB_TRY_STATUS(M->feat.alloc(sizeof(float) * (size_t)n * kLfF));
+   TNLB_TRY_STATUS(M->s.alloc(sizeof(Real) * n));
+   DeviceBuffer err;
+   TNLB_TRY_STATUS(err.alloc(sizeof(int32_t)));
+   TNLB_CUDA_TRY(cudaMemsetAsync(err.ptr, 0, sizeof(int32_t), st));
+   lf::k_features<Real><<<grid_for(n, 128), 128, 0, st>>>(
+      M->F->a_rp.as<int32_t>(), M->F->a_cols.as<int32_t>(), M->F->a_vals.as<Real>(), M->F->g->offsets.as<int32_t>(),
+      M->F->g_cols.as<int32_t>(), n, M->feat.as<float>(), M->s.as<Real>(), err.as<int32_t>());
+   TNLB_CHECK_LAUNCH();
+   int32_t h = 0;
+   TNLB_CUDA_TRY(cudaMemcpyAsync(&h, err.ptr, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+   TNLB_CUDA_TRY(cudaStreamSynchronize(st));
+   TNLB_REQUIRE(h == 0, TNLB_ERR_INVALID_ARGUMENT,
+                "learned FSAI: a row holds more than 4 stored entries in its lower triangle");
+   return TNLB_OK;
+}
+
+}  // namespace
+
+// Forward pass for all rows: o (n x 4); activations h1..h3 kept when `acts`.
+tnlb_status lfsai_forward(const tnlb_lfsai* net, const float* feat, int64_t n, float* o, float* h1, float* h2,
+                          float* h3, cudaStream_t st)
+{
+   if (net->use_tc) return lfsai_forward_tc(net, feat, n, o, h1, h2, h3, st);
+   const float* wr = net->wround.as<float>();
+   const unsigned g = grid_for(n, 128);
+   lf::k_layer<kLfF, kLfH, true><<<g, 128, 0, st>>>(feat, n, wr + kLfW1, wr + kLfB1, h1);
+   lf::k_layer<kLfH, kLfH, true><<<g, 128, 0, st>>>(h1, n, wr + kLfW2, wr + kLfB2, h2);
+   lf::k_layer<kLfH, kLfH, true><<<g, 128, 0, st>>>(h2, n, wr + kLfW3, wr + kLfB3, h3);
+   lf::k_layer<kLfH, kLfK, false><<<g, 128, 0, st>>>(h3, n, wr + kLfW4, wr + kLfB4, o);
+   TNLB_CHECK_LAUNCH();
+   return TNLB_OK;
+}
+
+namespace {
+
+// dW, db of one layer from its output deltas and (BF16-rounded) inputs.
+template <int FIN, int FOUT>
+tnlb_status wgrad_layer(const float* dout, const float* in, int64_t n, int64_t rpb, int blocks, float* part, float* gW,
+                        float* gb, cudaStream_t st)
+{
+   constexpr int nwW = FOUT * FIN;
+   lf::k_wgrad<FIN, FOUT><<<blocks, 256, 0, st>>>(dout, in, n, rpb, part);
+   lf::k_sum_partials<<<(nwW + FOUT + 255) / 256, 256, 0, st>>>(part, blocks, nwW + FOUT, gW, gb, nwW);
+   TNLB_CHECK_LAUNCH();
+   return TNLB_OK;
+}
+
+// Backward from dL/do through the network into net->grad.
+tnlb_status lfsai_backward(tnlb_lfsai* net, const float* feat, int64_t n, const float* h1, const float* h2,
+                           const float* h3, const float* dout, cudaStream_t st)
+{
+   const float* wr = net->wround.as<float>();
+   DeviceBuffer d3, d2, d1, part;
+   TNLB_TRY_STATUS(d3.alloc(sizeof(float) * n * kLfH));
+   TNLB_TRY_STATUS(d2.alloc(sizeof(float) * n * kLfH));
+   TNLB_TRY_STATUS(d1.alloc(sizeof(float) * n * kLfH));
+   const unsigned g = grid_for(n, 128);
+   lf::k_back_layer<kLfH, kLfK><<<g, 128, 0, st>>>(dout, h3, n, wr + kLfW4, d3.as<float>());
+   lf::k_back_layer<kLfH, kLfH><<<g, 128, 0, st>>>(d3.as<float>(), h2, n, wr + kLfW3, d2.as<float>());
+   lf::k_back_layer<kLfH, kLfH><<<g, 128, 0, st>>>(d2.as<float>(), h1, n, wr + kLfW2, d1.as<float>());
+   TNLB_CHECK_LAUNCH();
+   const int64_t rpb = 2048;
+   const int blocks = (int)((n + rpb - 1) / rpb);
+   TNLB_TRY_STATUS(part.alloc(sizeof(float) * (size_t)blocks * (kLfH * kLfH + kLfH)));
+   float* gr = net->grad.as<float>();
+   TNLB_TRY_STATUS(wgrad_layer<kLfH, kLfK>(dout, h3, n, rpb, blocks, part.as<float>(), gr + kLfW4, gr + kLfB4, st));
+   TNLB_TRY_STATUS(wgrad_layer<kLfH, kLfH>(d3.as<float>(), h2, n, rpb, blocks, part.as<float>(), gr + kLfW3, gr + kLfB3, st));
+   TNLB_TRY_STATUS(wgrad_layer<kLfH, kLfH>(d2.as<float>(), h1, n, rpb, blocks, part.as<float>(), gr + kLfW2, gr + kLfB2, st));
+   TNLB_TRY_STATUS(wgrad_layer<kLfF, kLfH>(d1.as<float>(), feat, n, rpb, blocks, part.as<float>(), gr + kLfW1, gr + kLfB1, st));
+   return TNLB_OK;
+}
+
+template <typename Real>
+tnlb_status gradient_t(tnlb_lfsai* net, const tnlb_segments* seg, const int32_t* cols, const Real* vals,
+                       const Real* probes, int32_t P, cudaStream_t st, double* h_loss, bool fit)
+{
+   const int32_t n = seg->n;
+   const tnlb_real real = sizeof(Real) == 8 ? TNLB_F64 : TNLB_F32;
+   LfsaiMatrix M;
+   TNLB_TRY_STATUS(build_matrix_ctx<Real>(seg, real, cols, vals, st, &M));
+   Fsai* F = M.F;
+   const int64_t gnnz = F->g->elements;
+   lf::k_round_weights<<<(kLfParams + 255) / 256, 256, 0, st>>>(net->theta.as<float>(), net->wround.as<float>());
+   DeviceBuffer o, h1, h2, h3, dout, dg, red, cnt, loss;
+   TNLB_TRY_STATUS(o.alloc(sizeof(float) * (size_t)n * kLfK));
+   TNLB_TRY_STATUS(h1.alloc(sizeof(float) * (size_t)n * kLfH));
+   TNLB_TRY_STATUS(h2.alloc(sizeof(float) * (size_t)n * kLfH));
+   TNLB_TRY_STATUS(h3.alloc(sizeof(float) * (size_t)n * kLfH));
+   TNLB_TRY_STATUS(dout.alloc(sizeof(float) * (size_t)n * kLfK));
+   TNLB_TRY_STATUS(dg.alloc(sizeof(double) * gnnz));
+   TNLB_TRY_STATUS(red.alloc(sizeof(double) * kRedMaxBlocks * kRedSlots));
+   TNLB_TRY_STATUS(cnt.alloc(sizeof(unsigned) * 2));
+   TNLB_TRY_STATUS(loss.alloc(sizeof(double)));
+   TNLB_CUDA_TRY(cudaMemsetAsync(cnt.ptr, 0, sizeof(unsigned) * 2, st));
+   TNLB_CUDA_TRY(cudaMemsetAsync(loss.ptr, 0, sizeof(double), st));
+   TNLB_CUDA_TRY(cudaMemsetAsync(dg.ptr, 0, sizeof(double) * gnnz, st));
+   RedWork rw{red.as<double>(), cnt.as<unsigned>()};
+   TNLB_TRY_STATUS(lfsai_forward(net, M.feat.as<float>(), n, o.as<float>(), h1.as<float>(), h2.as<float>(),
+                                 h3.as<float>(), st));
+   if (fit) {
+      // supervised warm start on the classical FSAI values
+      DeviceBuffer tg;
+      TNLB_TRY_STATUS(tg.alloc(sizeof(Real) * gnnz));
+      Fsai* C = nullptr;
+      TNLB_TRY_STATUS(fsai_create(seg, real, cols, vals, true, st, &C));
+      TNLB_CUDA_TRY(cudaMemcpyAsync(tg.ptr, C->g_vals.ptr, sizeof(Real) * gnnz, cudaMemcpyDeviceToDevice, st));
+      fsai_destroy(C);
+      lf::k_fit_do<Real><<<vec_grid(n), kRedThreads, 0, st>>>(o.as<float>(), tg.as<Real>(), M.s.as<Real>(),
+                                                              F->g->offsets.as<int32_t>(), F->g_cols.as<int32_t>(), n,
+                                                              dout.as<float>(), rw, loss.as<double>());
+      TNLB_CHECK_LAUNCH();
+   }
+   else {
+      lf::k_g_values<Real><<<grid_for(n, 128), 128, 0, st>>>(o.as<float>(), M.s.as<Real>(), F->g->offsets.as<int32_t>(),
+                                                             F->g_cols.as<int32_t>(), n, F->g_vals.as<Real>());
+      TNLB_CHECK_LAUNCH();
+      TNLB_TRY_STATUS(fsai_set_values(F, F->g_vals.ptr, st));
+      DeviceBuffer t, w, v, u, q;
+      for (auto* b : {&t, &w, &v, &u, &q}) TNLB_TRY_STATUS(b->alloc(sizeof(Real) * n));
+      const double c = -2.0 / ((double)n * P);
+      for (int32_t p = 0; p < P; p++) {
+         const Real* z = probes + (int64_t)p * n;
+         // w = A G^T z; v = G w; u = z - v; q = A G^T u
+         TNLB_TRY_STATUS(spmv_dispatch(F->gt, real, F->gt_cols.as<int32_t>(), F->gt_vals.ptr, z, t.ptr, 1.0, 0.0, st));
+         TNLB_TRY_STATUS(spmv_dispatch(seg, real, cols, vals, t.ptr, w.ptr, 1.0, 0.0, st));
+         TNLB_TRY_STATUS(spmv_dispatch(F->g, real, F->g_cols.as<int32_t>(), F->g_vals.ptr, w.ptr, v.ptr, 1.0, 0.0, st));
+         lf::k_resid<Real><<<vec_grid(n), kRedThreads, 0, st>>>(n, z, v.as<Real>(), u.as<Real>(), rw, loss.as<double>());
+         TNLB_TRY_STATUS(spmv_dispatch(F->gt, real, F->gt_cols.as<int32_t>(), F->gt_vals.ptr, u.ptr, t.ptr, 1.0, 0.0, st));
+         TNLB_TRY_STATUS(spmv_dispatch(seg, real, cols, vals, t.ptr, q.ptr, 1.0, 0.0, st));
+         lf::k_dg<Real><<<grid_for(n, 256), 256, 0, st>>>(F->g->offsets.as<int32_t>(), F->g_cols.as<int32_t>(), n,
+                                                          u.as<Real>(), w.as<Real>(), z, q.as<Real>(), c,
+                                                          dg.as<double>());
+         TNLB_CHECK_LAUNCH();
+      }
+      lf::k_do<Real><<<grid_for(n, 128), 128, 0, st>>>(dg.as<double>(), o.as<float>(), M.s.as<Real>(),
+                                                       F->g->offsets.as<int32_t>(), F->g_cols.as<int32_t>(), n,
+                                                       dout.as<float>());
+      TNLB_CHECK_LAUNCH();
+   }
+   TNLB_TRY_STATUS(lfsai_backward(net, M.feat.as<float>(), n, h1.as<float>(), h2.as<float>(), h3.as<float>(),
+                                  dout.as<float>(), st));
+   double hl = 0;
+   TNLB_CUDA_TRY(cudaMemcpyAsync(&hl, loss.ptr, sizeof(double), cudaMemcpyDeviceToHost, st));
+   TNLB_CUDA_TRY(cudaStreamSynchronize(st));
+   *h_loss = fit ? hl : hl / ((double)n * P);
+   return TNLB_OK;
+}
+
+template <typename Real>
+tnlb_status precond_t(const tnlb_lfsai* net, const tnlb_segments* seg, const int32_t* cols, const Real* vals,
+                      cudaStream_t st, tnlb_precond** out)
+{
+   const tnlb_real real = sizeof(Real) == 8 ? TNLB_F64 : TNLB_F32;
+   auto* M = new LfsaiMatrix();
+   tnlb_status s = build_matrix_ctx<Real>(seg, real, cols, vals, st, M);
+   if (s != TNLB_OK) {
+      delete M;
+      return s;
+   }
+   const int32_t n = seg->n;
+   DeviceBuffer o, h1, h2, h3;
+   lf::k_round_weights<<<(kLfParams + 255) / 256, 256, 0, st>>>(net->theta.as<float>(), net->wround.as<float>());
+   TNLB_TRY_STATUS(o.alloc(sizeof(float) * (size_t)n * kLfK));
+   TNLB_TRY_STATUS(h1.alloc(sizeof(float) * (size_t)n * kLfH));
+   TNLB_TRY_STATUS(h2.alloc(sizeof(float) * (size_t)n * kLfH));
+   TNLB_TRY_STATUS(h3.alloc(sizeof(float) * (size_t)n * kLfH));
+   TNLB_TRY_STATUS(lfsai_forward(net, M->feat.as<float>(), n, o.as<float>(), h1.as<float>(), h2.as<float>(),
+                                 h3.as<float>(), st));
+   lf::k_g_values<Real><<<grid_for(n, 128), 128, 0, st>>>(o.as<float>(), M->s.as<Real>(),
+                                                          M->F->g->offsets.as<int32_t>(), M->F->g_cols.as<int32_t>(), n,
+                                                          M->F->g_vals.as<Real>());
+   TNLB_CHECK_LAUNCH();
+   TNLB_TRY_STATUS(fsai_set_values(M->F, M->F->g_vals.ptr, st));
+   TNLB_CUDA_TRY(cudaStreamSynchronize(st));
+   auto* P = new tnlb_precond();
+   P->kind = TNLB_PRECOND_FSAI;
+   P->real = real;
+   P->n = n;
+   P->fsai = M->F;
+   M->F = nullptr;
+   delete M;
+   *out = P;
+   return TNLB_OK;
+}
+
+}  // namespace
+
+tnlb_status lfsai_gradient(tnlb_lfsai* net, const tnlb_segments* seg, tnlb_real real, const int32_t* cols,
+                           const void* vals, const void* probes, int32_t P, bool fit, cudaStream_t st, double* loss)
+{
+   if (real == TNLB_F64)
+      return gradient_t<double>(net, seg, cols, (const double*)vals, (const double*)probes, P, st, loss, fit);
+   return gradient_t<float>(net, seg, cols, (const float*)vals, (const float*)probes, P, st, loss, fit);
+}
+
+tnlb_status lfsai_adam(tnlb_lfsai* net, double lr, cudaStream_t st)
+{
+   net->step++;
+   const float b1 = 0.9f, b2 = 0.999f;
+   const float c1 = 1.f - std::pow(b1, (float)net->step), c2 = 1.f - std::pow(b2, (float)net->step);
+   lf::k_adam<<<(kLfParams + 255) / 256, 256, 0, st>>>(net->theta.as<float>(), net->grad.as<float>(),
+                                                       net->m.as<float>(), net->v.as<float>(), kLfParams, (float)lr, b1,
+                                                       b2, 1e-8f, c1, c2);
+   TNLB_CHECK_LAUNCH();
+   return TNLB_OK;
+}
+
+tnlb_status lfsai_init(tnlb_lfsai* net, uint64_t seed, cudaStream_t st)
+{
+   TNLB_TRY_STATUS(net->theta.alloc(sizeof(float) * kLfParams));
+   TNLB_TRY_STATUS(net->wround.alloc(sizeof(float) * kLfParams));
+   TNLB_TRY_STATUS(net->grad.alloc(sizeof(float) * kLfParams));
+   TNLB_TRY_STATUS(net->m.alloc(sizeof(float) * kLfParams));
+   TNLB_TRY_STATUS(net->v.alloc(sizeof(float) * kLfParams));
+   TNLB_CUDA_TRY(cudaMemsetAsync(net->m.ptr, 0, sizeof(float) * kLfParams, st));
+   TNLB_CUDA_TRY(cudaMemsetAsync(net->v.ptr, 0, sizeof(float) * kLfParams, st));
+   TNLB_CUDA_TRY(cudaMemsetAsync(net->grad.ptr, 0, sizeof(float) * kLfParams, st));
+   lf::k_init_params<<<(kLfParams + 255) / 256, 256, 0, st>>>(seed, net->theta.as<float>());
+   TNLB_CHECK_LAUNCH();
+   lf::k_round_weights<<<(kLfParams + 255) / 256, 256, 0, st>>>(net->theta.as<float>(), net->wround.as<float>());
+   TNLB_CHECK_LAUNCH();
+   TNLB_CUDA_TRY(cudaStreamSynchronize(st));
+   return TNLB_OK;
+}
+
+tnlb_status lfsai_precond(const tnlb_lfsai* net, const tnlb_segments* seg, tnlb_real real, const int32_t* cols,
+                          const void* vals, cudaStream_t st, tnlb_precond** out)
+{
+   if (real == TNLB_F64) return precond_t<double>(net, seg, cols, (const double*)vals, st, out);
+   return precond_t<float>(net, seg, cols, (const float*)vals, st, out);
+}
+
+// Features and network outputs for inspection (tests).
+tnlb_status lfsai_eval(const tnlb_lfsai* net, const tnlb_segments* seg, tnlb_real real, const int32_t* cols,
+                       const void* vals, cudaStream_t st, float* h_feat, float* h_out)
+{
+   LfsaiMatrix M;
+   if (real == TNLB_F64)
+      TNLB_TRY_STATUS(build_matrix_ctx<double>(seg, real, cols, (const double*)vals, st, &M));
+   else
+      TNLB_TRY_STATUS(build_matrix_ctx<float>(seg, real, cols, (const float*)vals, st, &M));
+   const int32_t n = seg->n;
+   DeviceBuffer o, h1, h2, h3;
+   lf::k_round_weights<<<(kLfParams + 255) / 256, 256, 0, st>>>(net->theta.as<float>(), net->wround.as<float>());
+   TNLB_TRY_STATUS(o.alloc(sizeof(float) * (size_t)n * kLfK));
+   TNLB_TRY_STATUS(h1.alloc(sizeof(float) * (size_t)n * kLfH));
+   TNLB_TRY_STATUS(h2.alloc(sizeof(float) * (size_t)n * kLfH));
+   TNLB_TRY_STATUS(h3.alloc(sizeof(float) * (size_t)n * kLfH));
+   TNLB_TRY_STATUS(lfsai_forward(net, M.feat.as<float>(), n, o.as<float>(), h1.as<float>(), h2.as<float>(),
+                                 h3.as<float>(), st));
+   if (h_feat)
+      TNLB_CUDA_TRY(cudaMemcpyAsync(h_feat, M.feat.ptr, sizeof(float) * (size_t)n * kLfF, cudaMemcpyDeviceToHost, st));
+   if (h_out) TNLB_CUDA_TRY(cudaMemcpyAsync(h_out, o.ptr, sizeof(float) * (size_t)n * kLfK, cudaMemcpyDeviceToHost, st));
+   TNLB_CUDA_TRY(cudaStreamSynchronize(st));
+   return TNLB_OK;
+}
+
+}  // namespace tnlb

@@ -1,0 +1,184 @@
+"""Learned FSAI preconditioner: the network handle, its training loop and
+the preconditioner it produces (no counterpart in the reference library).
+
+The network and every kernel it runs live in libtnlb200.so (lfsai.cu):
+features, forward and backward passes, the probe loss built from the
+library's SpMVs, and Adam.  This module only orchestrates them:
+
+* ``LearnedFSAI.fit_classical`` -- warm start: regress the network onto the
+  classical Kolotilina-Yeremin FSAI values of the training matrices;
+* ``LearnedFSAI.train`` -- minimise (1/(n P)) sum_p ||z_p - G A G^T z_p||^2
+  over probe vectors z_p: Rademacher vectors and residuals left by a few
+  Jacobi-PCG iterations on the same matrix (the error modes a cheap
+  preconditioner leaves behind);
+* ``LearnedFSAI.preconditioner(M)`` -- M^-1 = G^T G for a matrix, usable by
+  the solvers and by the mixed-precision refinement (FP32 matrices give an
+  FP32 preconditioner).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+import torch
+
+from . import CG, Diagonal, SparseMatrix, _real_code, _stream, check
+from . import _capi as capi
+from ._capi import lib  # noqa: F401  (fails loudly without the library)
+
+
+class LearnedPreconditioner:
+    """M^-1 = G^T G with G from the network (a tnlb_precond handle)."""
+
+    KIND = capi.PRECOND_FSAI
+
+    def __init__(self, handle, matrix):
+        self._h = handle
+        self.matrix = matrix
+
+    @property
+    def handle(self):
+        return self._h
+
+    def solve(self, b: torch.Tensor, x: torch.Tensor) -> None:
+        check(capi.tnlb_precond_solve(self._h, b.data_ptr(), x.data_ptr(), _stream()))
+
+    def __del__(self):
+        try:
+            if self._h:
+                capi.tnlb_precond_destroy(self._h)
+        except Exception:
+            pass
+
+
+class LearnedFSAI:
+    NPARAMS = 9668
+
+    def __init__(self, seed: int = 0, tensor_cores: bool = False):
+        h = C.c_void_p()
+        check(capi.tnlb_lfsai_create(seed, _stream(), C.byref(h)))
+        self._h = h
+        self.set_tensor_cores(tensor_cores)
+
+    def __del__(self):
+        try:
+            if self._h:
+                capi.tnlb_lfsai_destroy(self._h)
+        except Exception:
+            pass
+
+    def set_tensor_cores(self, enable: bool) -> None:
+        check(capi.tnlb_lfsai_set_tensor_cores(self._h, int(bool(enable))))
+
+    # -- parameters ---------------------------------------------------------
+    def params(self) -> np.ndarray:
+        out = np.zeros(self.NPARAMS, np.float32)
+        check(capi.tnlb_lfsai_get_params(self._h, out.ctypes.data, out.size))
+        return out
+
+    def set_params(self, theta) -> None:
+        t = np.ascontiguousarray(theta, np.float32)
+        check(capi.tnlb_lfsai_set_params(self._h, t.ctypes.data, t.size))
+
+    def grad(self) -> np.ndarray:
+        out = np.zeros(self.NPARAMS, np.float32)
+        check(capi.tnlb_lfsai_get_grad(self._h, out.ctypes.data, out.size))
+        return out
+
+    def save(self, path) -> None:
+        np.save(Path(path), self.params())
+
+    def load(self, path) -> None:
+        self.set_params(np.load(Path(path)))
+
+    # -- evaluation -------------------------------------------------------------
+    def evaluate(self, M: SparseMatrix):
+        """(features n x 16, outputs n x 4) of a matrix."""
+        n = M.getRows()
+        f = np.zeros((n, 16), np.float32)
+        o = np.zeros((n, 4), np.float32)
+        check(capi.tnlb_lfsai_eval(self._h, M.segments.handle, _real_code(M.real), M.columnIndexes.data_ptr(),
+                                   M.values.data_ptr(), _stream(), f.ctypes.data, o.ctypes.data))
+        return f, o
+
+    def preconditioner(self, M: SparseMatrix) -> LearnedPreconditioner:
+        h = C.c_void_p()
+        check(capi.tnlb_lfsai_precond_create(self._h, M.segments.handle, _real_code(M.real),
+                                             M.columnIndexes.data_ptr(), M.values.data_ptr(), _stream(), C.byref(h)))
+        return LearnedPreconditioner(h, M)
+
+    # -- training ---------------------------------------------------------------
+    def gradient(self, M: SparseMatrix, probes: torch.Tensor | None = None, mode: int = 0) -> float:
+        """Loss of one matrix; the gradient stays in the handle (see grad())."""
+        loss = C.c_double()
+        nprobes = 0 if probes is None else probes.shape[0]
+        check(capi.tnlb_lfsai_gradient(self._h, mode, M.segments.handle, _real_code(M.real),
+                                       M.columnIndexes.data_ptr(), M.values.data_ptr(),
+                                       probes.data_ptr() if probes is not None else None, nprobes, _stream(),
+                                       C.byref(loss)))
+        return loss.value
+
+    def adam_step(self, lr: float) -> None:
+        check(capi.tnlb_lfsai_adam_step(self._h, lr, _stream()))
+
+    def fit_classical(self, matrices, steps: int = 300, lr: float = 3e-3) -> list[float]:
+        hist = []
+        for k in range(steps):
+            M = matrices[k % len(matrices)]
+            hist.append(self.gradient(M, None, mode=1))
+            self.adam_step(lr)
+        return hist
+
+    @staticmethod
+    def probes(M: SparseMatrix, count: int, seed: int, residual_share: float = 0.5, pcg_iterations: int = 20):
+        """Probe vectors (count x n): Rademacher, and unit-RMS residuals left by a
+        few Jacobi-PCG iterations from x = 0 on Rademacher right-hand sides."""
+        n = M.getRows()
+        g = torch.Generator(device="cuda")
+        g.manual_seed(seed)
+        Z = (torch.randint(0, 2, (count, n), generator=g, device="cuda", dtype=torch.int8).to(M.real) * 2 - 1)
+        nres = int(round(count * residual_share))
+        if nres:
+            S = CG()
+            S.setMatrix(M)
+            P = Diagonal()
+            P.update(M)
+            S.setPreconditioner(P)
+            S.setMaxIterations(pcg_iterations)
+            S.setConvergenceResidue(0.0)
+            for p in range(nres):
+                b = Z[p].clone()
+                x = torch.zeros(n, dtype=M.real, device="cuda")
+                S.solve(b, x)
+                r = b.clone()
+                M.vectorProduct(x, r, -1.0, 1.0)
+                Z[p] = r * (n ** 0.5 / torch.linalg.vector_norm(r))
+        return Z.contiguous()
+
+    def train(self, matrices, steps: int = 500, nprobes: int = 8, lr: float = 1e-3, seed: int = 0,
+              probe_cache: int = 8) -> list[float]:
+        """Adam on the probe loss, cycling over the training matrices; each
+        matrix keeps a few probe sets that are reused before new ones are drawn."""
+        hist = []
+        cache: dict[int, torch.Tensor] = {}
+        for k in range(steps):
+            idx = k % len(matrices)
+            M = matrices[idx]
+            if idx not in cache or (k // len(matrices)) % probe_cache == 0:
+                cache[idx] = self.probes(M, nprobes, seed + 7919 * k + idx)
+            hist.append(self.gradient(M, cache[idx], mode=0))
+            self.adam_step(lr)
+        return hist
+
+
+def diffusion_problem(N: int, seed: int, corr_range=(0.02, 0.2), sigma_range=(1.0, 3.0)) -> SparseMatrix:
+    """One seeded 2D diffusion matrix of the learned-preconditioner workload:
+    correlation length ~ U[corr_range], sigma ~ U[sigma_range]."""
+    from .generators import diffusion_2d, uniform01
+
+    u = uniform01(seed, 99, np.arange(2, dtype=np.uint64))
+    corr = corr_range[0] + (corr_range[1] - corr_range[0]) * u[0]
+    sigma = sigma_range[0] + (sigma_range[1] - sigma_range[0]) * u[1]
+    A = diffusion_2d(N, corr, sigma, seed)
+    return SparseMatrix.from_csr(A, real=torch.float64)
