@@ -99,7 +99,10 @@ def test_solver_matches_oracle(oracle, kind, precond, pname):
     o = oracle.solve(kind, A, b, precond=precond, tol=1e-8, maxit=20000, gmres_m=30, gmres_reorth=2)
     ok, it, res, x, tr = gpu_solve(kind, A, b, precond)
     assert ok == o["converged"]
-    assert abs(it - o["iterations"]) <= 2, (it, o["iterations"])
+    # rounding-level differences in the dot products move ill-conditioned,
+    # unpreconditioned solves by a few iterations (so does the reference
+    # between OpenMP thread counts)
+    assert abs(it - o["iterations"]) <= max(2, o["iterations"] // 100), (it, o["iterations"])
     assert res < 1e-8
     assert tr < 1e-6
     assert np.max(np.abs(x - o["x"])) <= 1e-5 * max(1.0, np.max(np.abs(o["x"])))
@@ -161,13 +164,18 @@ def test_zero_rhs_gives_zero_solution():
     assert ok and it == 0 and np.all(x == 0)
 
 
-def test_max_iterations_reports_failure():
+def test_max_iterations_reports_failure(oracle):
+    """maxIterations = 10: nextIteration lets iteration 11 run and stops at the
+    next check, so getIterations() is 12 and solve() returns false
+    (IterativeSolver.hpp:98-143) -- the oracle gives the same count."""
     from tnl_b200 import generators as g
 
     A = g.laplacian_2d(64)
     b = g.uniform_vector(A.n, 1)
+    o = oracle.solve("cg", A, b, precond=1, tol=1e-8, maxit=10)
     ok, it, res, x, tr = gpu_solve("cg", A, b, 1, maxit=10)
-    assert not ok and it == 11 and res > 1e-8
+    assert not ok and not o["converged"]
+    assert it == o["iterations"] == 12 and res > 1e-8
 
 
 def test_mixed_precision_refinement_reaches_fp64_residual(oracle):

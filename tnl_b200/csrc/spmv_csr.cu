@@ -197,6 +197,59 @@ __global__ void k_tile_plan(const int32_t* __restrict__ rowptr, int32_t n, int64
    if (t < tiles) carry_row[t] = -1;
 }
 
+// L2 policies: the streamed values and column indexes are evicted first, the
+// gathered vector is kept (it is re-read once per nonzero that points at it).
+__device__ __forceinline__ uint64_t policy_evict_first()
+{
+   uint64_t p;
+   asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+   return p;
+}
+__device__ __forceinline__ uint64_t policy_evict_last()
+{
+   uint64_t p;
+   asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+   return p;
+}
+__device__ __forceinline__ int32_t ld_stream_hint(const int32_t* a, uint64_t pol)
+{
+   int32_t v;
+   asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.s32 %0, [%1], %2;" : "=r"(v) : "l"(a), "l"(pol));
+   return v;
+}
+__device__ __forceinline__ double ld_stream_hint(const double* a, uint64_t pol)
+{
+   double v;
+   asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(a), "l"(pol));
+   return v;
+}
+__device__ __forceinline__ float ld_stream_hint(const float* a, uint64_t pol)
+{
+   float v;
+   asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(a), "l"(pol));
+   return v;
+}
+__device__ __forceinline__ double ld_keep(const double* a, uint64_t pol)
+{
+   double v;
+   asm volatile("ld.global.nc.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(a), "l"(pol));
+   return v;
+}
+__device__ __forceinline__ float ld_keep(const float* a, uint64_t pol)
+{
+   float v;
+   asm volatile("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(a), "l"(pol));
+   return v;
+}
+
+// Merge-path tile: at most kTileSize rows + nonzeros.  Each warp takes an
+// equal share of the tile's nonzeros, 32 consecutive ones per step: all
+// column/value loads and x gathers of its steps are issued before any is
+// used; the row of a nonzero is found by binary search in the staged row
+// ends; per step a warp-shuffle segmented scan sums each row's products, and
+// a running carry joins a row across steps.  Rows complete inside one warp
+// are stored to shared memory directly; the (at most two) rows a warp shares
+// with its neighbours are combined in warp order by one thread.
 template <typename Real>
 __global__ void __launch_bounds__(kTileThreads) k_csr_tile(const int32_t* __restrict__ rowptr,
                                                           const int32_t* __restrict__ cols,
@@ -206,126 +259,134 @@ __global__ void __launch_bounds__(kTileThreads) k_csr_tile(const int32_t* __rest
                                                           int32_t* __restrict__ carry_row, Real* __restrict__ carry_val,
                                                           Real alpha, Real beta, const int32_t* __restrict__ skip)
 {
+   constexpr int kWarps = kTileThreads / 32;
+   constexpr int kSteps = kTileItems;  // 32-nonzero steps per warp (kTileSize / kWarps / 32)
+   __shared__ int32_t s_rowend[kTileSize + 1];
+   __shared__ Real s_y[kTileSize + 1];
+   __shared__ int32_t s_pk[2 * kWarps];
+   __shared__ Real s_pv[2 * kWarps];
+
    // solvers pass their device `done` flag: nothing to do once they stopped
    if (skip && *skip) return;
-   __shared__ int32_t s_rowend[kTileSize + 1];
-   __shared__ Real s_prod[kTileSize];
-   __shared__ Real s_y[kTileSize];
-   __shared__ int32_t s_wkey[8];
-   __shared__ Real s_wval[8];
-   __shared__ int32_t s_pkey[8];
-   __shared__ Real s_pval[8];
-
    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
    const int32_t t = blockIdx.x;
    const int32_t r0 = tile_row[t], r1 = tile_row[t + 1];
    const int32_t k0 = tile_nnz[t], k1 = tile_nnz[t + 1];
-   const int32_t nrows = r1 - r0, nk = k1 - k0, items = nrows + nk;
+   const int32_t nrows = r1 - r0, nk = k1 - k0;
+   const uint64_t pol_stream = policy_evict_first(), pol_keep = policy_evict_last();
 
-   // Stage the nonzeros: coalesced streaming loads, products into shared memory.
-   {
-      int32_t c[kTileItems];
-      Real v[kTileItems];
+   // this warp's nonzeros [wb, we)
+   const int32_t chunk = (nk + kWarps - 1) / kWarps;
+   const int32_t wb = k0 + imin64(nk, (int64_t)warp * chunk);
+   const int32_t we = k0 + imin64(nk, (int64_t)(warp + 1) * chunk);
+
+   // issue the streaming loads first
+   int32_t c[kSteps];
+   Real v[kSteps];
 #pragma unroll
-      for (int i = 0; i < kTileItems; i++) {
-         const int32_t j = tid + i * kTileThreads;
-         if (j < nk) {
-            c[i] = ld_stream(cols + k0 + j);
-            v[i] = ld_stream(vals + k0 + j);
-         }
-      }
-#pragma unroll
-      for (int i = 0; i < kTileItems; i++) {
-         const int32_t j = tid + i * kTileThreads;
-         if (j < nk) s_prod[j] = c[i] >= 0 ? v[i] * ld_gather(x + c[i]) : Real(0);
+   for (int j = 0; j < kSteps; j++) {
+      const int32_t e = wb + j * 32 + lane;
+      c[j] = -1;
+      v[j] = Real(0);
+      if (e < we) {
+         c[j] = ld_stream_hint(cols + e, pol_stream);
+         v[j] = ld_stream_hint(vals + e, pol_stream);
       }
    }
-   // Stage the row ends of the rows ending in this tile (+ the open one).
+   // row ends of the rows ending in the tile, plus the open row
    for (int32_t i = tid; i <= nrows; i += kTileThreads) {
       const int64_t r = (int64_t)r0 + i + 1;
       s_rowend[i] = r <= n ? rowptr[r] : INT_MAX;
+      s_y[i] = Real(0);
    }
+   // gathers
+   Real p[kSteps];
+#pragma unroll
+   for (int j = 0; j < kSteps; j++) p[j] = c[j] >= 0 ? v[j] * ld_keep(x + c[j], pol_keep) : Real(0);
    __syncthreads();
 
-   // Merge-path search for this thread's first item.
-   const int32_t d = min(tid * kTileItems, items);
-   int32_t lo = max(0, d - nk), hi = min(d, nrows);
-   while (lo < hi) {
-      const int32_t mid = (lo + hi) >> 1;
-      if (s_rowend[mid] <= k0 + d - mid - 1)
-         lo = mid + 1;
+   // local row of element e: first i in [0, nrows] with s_rowend[i] > e
+   auto row_of = [&](int32_t e, int32_t lo) -> int32_t {
+      int32_t hi = nrows;
+      while (lo < hi) {
+         const int32_t mid = (lo + hi) >> 1;
+         if (s_rowend[mid] > e)
+            hi = mid;
+         else
+            lo = mid + 1;
+      }
+      return lo;
+   };
+   const int32_t wfirst = wb < we ? row_of(wb, 0) : -1;
+   int32_t key[kSteps];
+#pragma unroll
+   for (int j = 0; j < kSteps; j++) {
+      const int32_t e = wb + j * 32 + lane;
+      key[j] = e < we ? row_of(e, wfirst) : INT_MAX;
+   }
+
+   int32_t carry_k = -1;
+   Real carry_v = Real(0), first_v = Real(0);
+   bool have_first = false;
+   // emit a finished row piece: the warp's first row may continue from the
+   // previous warp, so it is kept for the cross-warp combine
+   auto emit = [&](int32_t k, Real val) {
+      if (k == wfirst) {
+         first_v = val;
+         have_first = true;
+      }
       else
-         hi = mid;
-   }
-   int32_t xr = lo, yn = d - lo;
-   const int32_t x_start = xr;
-   const int32_t d_end = min(d + kTileItems, items);
-   Real acc = 0, first = 0;
-   bool emitted = false;
+         s_y[k] = val;
+   };
 #pragma unroll
-   for (int it = 0; it < kTileItems; it++) {
-      if (d + it < d_end) {
-         if (k0 + yn < s_rowend[xr]) {
-            acc += s_prod[yn];
-            yn++;
-         }
-         else {
-            if (emitted)
-               s_y[xr] = acc;
-            else
-               first = acc;
-            emitted = true;
-            acc = 0;
-            xr++;
-         }
+   for (int j = 0; j < kSteps; j++) {
+      if (wb + j * 32 >= we) break;  // warp-uniform
+      const int32_t kj = key[j];
+      Real val = p[j];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+         const int32_t kk = __shfl_up_sync(0xffffffffu, kj, o);
+         const Real vv = __shfl_up_sync(0xffffffffu, val, o);
+         if (lane >= o && kk == kj) val += vv;
       }
-   }
-
-   // Segmented inclusive scan of (row in progress at the end, its partial).
-   const int32_t key = r0 + xr;
-   Real val = acc;
-#pragma unroll
-   for (int o = 1; o < 32; o <<= 1) {
-      const int32_t kk = __shfl_up_sync(0xffffffffu, key, o);
-      const Real vv = __shfl_up_sync(0xffffffffu, val, o);
-      if (lane >= o && kk == key) val += vv;
-   }
-   if (lane == 31) {
-      s_wkey[warp] = key;
-      s_wval[warp] = val;
-   }
-   __syncthreads();
-   if (warp == 0) {
-      int32_t wk = lane < 8 ? s_wkey[lane] : INT_MAX;
-      Real wv = lane < 8 ? s_wval[lane] : Real(0);
-#pragma unroll
-      for (int o = 1; o < 8; o <<= 1) {
-         const int32_t kk = __shfl_up_sync(0xffffffffu, wk, o);
-         const Real vv = __shfl_up_sync(0xffffffffu, wv, o);
-         if (lane >= o && kk == wk) wv += vv;
+      const int32_t k_first = __shfl_sync(0xffffffffu, kj, 0);
+      if (carry_k >= 0 && carry_k != k_first) {
+         // the previous step's last row ended exactly at the step boundary
+         if (lane == 0) emit(carry_k, carry_v);
+         carry_k = -1;
       }
-      const int32_t ek = __shfl_up_sync(0xffffffffu, wk, 1);
-      const Real ev = __shfl_up_sync(0xffffffffu, wv, 1);
-      if (lane < 8) {
-         s_pkey[lane] = lane == 0 ? -1 : ek;
-         s_pval[lane] = lane == 0 ? Real(0) : ev;
+      if (carry_k >= 0 && kj == carry_k) val += carry_v;
+      // the step's last valid lane holds the row that may continue into the
+      // next step: it is carried, every other segment end is emitted
+      const unsigned valid = __ballot_sync(0xffffffffu, kj != INT_MAX);
+      const int last_lane = 31 - __clz((int)valid);
+      const int32_t k_next = __shfl_down_sync(0xffffffffu, kj, 1);
+      if (lane < last_lane && k_next != kj) emit(kj, val);
+      carry_k = __shfl_sync(0xffffffffu, kj, last_lane);
+      carry_v = __shfl_sync(0xffffffffu, val, last_lane);
+   }
+   // warp pieces: the first row if it finished inside the warp (held by the
+   // lane that emitted it), and the last row in progress
+   {
+      const unsigned who = __ballot_sync(0xffffffffu, have_first);
+      const Real fv = __shfl_sync(0xffffffffu, first_v, who ? __ffs(who) - 1 : 0);
+      if (lane == 0) {
+         s_pk[2 * warp] = who ? wfirst : -1;
+         s_pv[2 * warp] = who ? fv : Real(0);
+         s_pk[2 * warp + 1] = carry_k;
+         s_pv[2 * warp + 1] = carry_v;
       }
    }
    __syncthreads();
-   if (key == s_pkey[warp]) val += s_pval[warp];
-   // carry-in of this thread = inclusive value of the previous thread
-   int32_t pk = __shfl_up_sync(0xffffffffu, key, 1);
-   Real pv = __shfl_up_sync(0xffffffffu, val, 1);
-   if (lane == 0) {
-      pk = s_pkey[warp];
-      pv = s_pval[warp];
-   }
-   if (emitted) s_y[x_start] = first + ((tid > 0 && pk == r0 + x_start) ? pv : Real(0));
-   if (tid == kTileThreads - 1) {
-      // open row at the tile end: does it own nonzeros in this tile?
+   if (tid == 0) {
+      // combine the pieces in warp order (deterministic)
+      for (int q = 0; q < 2 * kWarps; q++) {
+         const int32_t k = s_pk[q];
+         if (k >= 0) s_y[k] += s_pv[q];
+      }
       const bool has = nk > 0 && (nrows == 0 || s_rowend[nrows - 1] < k1);
-      carry_row[t] = (has && key < n) ? key : -1;
-      carry_val[t] = val;
+      carry_row[t] = (has && r1 < n) ? r1 : -1;
+      carry_val[t] = s_y[nrows];
    }
    __syncthreads();
    for (int32_t i = tid; i < nrows; i += kTileThreads) keep(y, r0 + i, s_y[i], alpha, beta);
