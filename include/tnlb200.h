@@ -216,11 +216,27 @@ tnlb_status tnlb_dot(tnlb_real real, int64_t n, const void* d_a, const void* d_b
 
 /* ------------------------------------------------------------ solvers */
 
-typedef enum { TNLB_SOLVER_CG = 0, TNLB_SOLVER_BICGSTAB = 1, TNLB_SOLVER_GMRES = 2 } tnlb_solver_kind;
-/* Preconditioners: none, Diagonal (Jacobi), ILU0, and the factorised sparse
- * approximate inverse M^-1 = G^T G (no counterpart in the reference; G on
- * the lower triangle of A's pattern, Kolotilina-Yeremin values). */
-typedef enum { TNLB_PRECOND_NONE = 0, TNLB_PRECOND_JACOBI = 1, TNLB_PRECOND_ILU0 = 2, TNLB_PRECOND_FSAI = 3 } tnlb_precond_kind;
+/* FGMRES: restarted GMRES with right, flexible preconditioning (the
+ * preconditioned basis is kept; residues are unpreconditioned).  No
+ * counterpart in the reference; its orthogonalisation and Givens steps follow
+ * GMRES.hpp:280-347, 731-770. */
+typedef enum {
+   TNLB_SOLVER_CG = 0,
+   TNLB_SOLVER_BICGSTAB = 1,
+   TNLB_SOLVER_GMRES = 2,
+   TNLB_SOLVER_FGMRES = 3
+} tnlb_solver_kind;
+/* Preconditioners: none, Diagonal (Jacobi), ILU0, and factorised sparse
+ * approximate inverses (no counterpart in the reference; Kolotilina-Yeremin
+ * values on the lower triangle of A's pattern): FSAI M^-1 = G^T G for SPD
+ * matrices, FSAI2 M^-1 = G_U G_L (two factors) for nonsymmetric ones. */
+typedef enum {
+   TNLB_PRECOND_NONE = 0,
+   TNLB_PRECOND_JACOBI = 1,
+   TNLB_PRECOND_ILU0 = 2,
+   TNLB_PRECOND_FSAI = 3,
+   TNLB_PRECOND_FSAI2 = 4
+} tnlb_precond_kind;
 
 typedef struct tnlb_precond tnlb_precond;
 /* GMRES::Variant (Solvers/Linear/GMRES.h:122-129). */
@@ -272,11 +288,11 @@ tnlb_status tnlb_solve(tnlb_solver_kind solver, tnlb_precond_kind precond, const
 tnlb_status tnlb_true_residual(const tnlb_segments* seg, tnlb_real real, const int32_t* d_cols, const void* d_values,
                                const void* d_b, const void* d_x, tnlb_stream stream, double* h_result);
 
-/* FP32-inner / FP64-outer iterative refinement for SPD matrices (no
- * counterpart in the reference; BASELINE mixed-precision path): the FP64
- * residual r = b - A x is formed with the FP64 values, normalised, rounded to
- * FP32 and solved with Jacobi-preconditioned CG on an FP32 copy of the
- * values to relative residual `inner_tolerance`; x += |r| d in FP64.
+/* FP32-inner / FP64-outer iterative refinement (no counterpart in the
+ * reference): the FP64 residual r = b - A x is formed with the FP64 values,
+ * normalised, rounded to FP32 and solved with `inner_solver` (CG for SPD
+ * matrices, FGMRES/GMRES/BiCGStab otherwise) on an FP32 copy of the values to
+ * relative residual `inner_tolerance`; x += |r| d in FP64.
  * The inner preconditioner is `inner` (an FP32 preconditioner of this
  * matrix, e.g. a learned FSAI) or, when NULL, one of kind `inner_precond`
  * built from the FP32 values.  Stops
@@ -286,8 +302,9 @@ tnlb_status tnlb_true_residual(const tnlb_segments* seg, tnlb_real real, const i
  * Synchronous. */
 tnlb_status tnlb_solve_mixed(const tnlb_solver_params* params, const tnlb_segments* seg, const int32_t* d_cols,
                              const double* d_values, const double* d_b, double* d_x, double inner_tolerance,
-                             int32_t max_outer, tnlb_precond_kind inner_precond, const tnlb_precond* inner,
-                             tnlb_stream stream, tnlb_solve_result* result, int32_t* outer_iterations);
+                             int32_t max_outer, tnlb_solver_kind inner_solver, tnlb_precond_kind inner_precond,
+                             const tnlb_precond* inner, tnlb_stream stream, tnlb_solve_result* result,
+                             int32_t* outer_iterations);
 
 /* Build a preconditioner for a matrix -- Preconditioner::update
  * (Preconditioners/Preconditioner.h:96-110; Diagonal.hpp:15-36,
@@ -300,6 +317,13 @@ tnlb_status tnlb_precond_create(tnlb_precond_kind kind, const tnlb_segments* seg
 /* x = M^{-1} b -- Preconditioner::solve (Diagonal.hpp:40-43,
  * ILU0.hpp:121-140).  Synchronous. */
 tnlb_status tnlb_precond_solve(const tnlb_precond* precond, const void* d_b, void* d_x, tnlb_stream stream);
+
+/* The factors of an FSAI / FSAI2 / learned FSAI preconditioner, copied to
+ * host memory as CSR: which = 0 gives G (G_L), which = 1 gives the second
+ * factor as stored for the product (G^T, or G_U).  `capacity` bounds h_cols
+ * and h_values; h_rowptr has n+1 entries.  Synchronous. */
+tnlb_status tnlb_precond_read_factor(const tnlb_precond* precond, int32_t which, int32_t* h_rowptr, int32_t* h_cols,
+                                     void* h_values, int64_t capacity);
 
 /* Release a preconditioner.  Accepts NULL. */
 tnlb_status tnlb_precond_destroy(tnlb_precond* precond);

@@ -229,3 +229,36 @@ def _u01(seed, index):
         z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
         z = z ^ (z >> np.uint64(31))
     return (z >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+
+
+def fsai_classical(A):
+    """Kolotilina-Yeremin FSAI values on the lower pattern (FP64, per row:
+    A[J,J] g = e_last, G_i = g / sqrt(g_last)); CSR order of the pattern."""
+    rows = _row_dict(A)
+    out = []
+    for i in range(A.n):
+        J = sorted(j for j in rows[i] if 0 <= j <= i)
+        B = np.array([[rows[p].get(q, 0.0) for q in J] for p in J])
+        e = np.zeros(len(J))
+        e[-1] = 1.0
+        g = np.linalg.solve(B, e)
+        out.extend(g / np.sqrt(g[-1]))
+    return np.array(out)
+
+
+def fsai2_classical(A):
+    """Two-factor FSAI for nonsymmetric A: rows of G_L (B^-T e) and of
+    H = G_U^T (B^-1 e) on the lower pattern, both / sqrt((B^-1)_last,last)."""
+    rows = _row_dict(A)
+    gl, h = [], []
+    for i in range(A.n):
+        J = sorted(j for j in rows[i] if 0 <= j <= i)
+        B = np.array([[rows[p].get(q, 0.0) for q in J] for p in J])
+        e = np.zeros(len(J))
+        e[-1] = 1.0
+        u = np.linalg.solve(B, e)
+        w = np.linalg.solve(B.T, e)
+        s = 1.0 / np.sqrt(u[-1])
+        gl.extend(w * s)
+        h.extend(u * s)
+    return np.array(gl), np.array(h)

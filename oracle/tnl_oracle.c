@@ -1031,6 +1031,150 @@ done:
    return ok;
 }
 
+/* FGMRES: the GMRES below with right, flexible preconditioning -- no
+ * counterpart in the reference; z_i = M^-1 v_i is kept, w = A z_i, x += Z y,
+ * residues unpreconditioned (normb = ||b||).  Derived from GMRES::solve with the MGS / MGSR orthogonalisation
+ * (Solvers/Linear/GMRES.hpp:73-180, orthogonalize_MGS :280-347,
+ * update :648-684, Givens :731-770).  restarting_min == restarting_max
+ * (no adaptivity: the reference's defaults are equal).  reorth = 1 (MGS)
+ * or 2 (MGSR).  Returns 1 on convergence, 0 otherwise, -1 on a zero
+ * Hessenberg diagonal (the reference throws there). */
+int orc_fgmres(int32_t n, const int32_t* rowptr, const int32_t* cols, const double* vals, int precond, int32_t m,
+              int reorth, const double* b, double* x, orc_solver_state* S)
+{
+   orc_csr A = {n, rowptr, cols, vals};
+   orc_prec P;
+   prec_setup(&P, &A, precond);
+   const size_t nb = sizeof(double) * (size_t)n;
+   double *r = malloc(nb), *w = malloc(nb), *M_tmp = malloc(nb);
+   double* V = (double*)malloc(nb * (size_t)(m + 1));
+   double* Zb = (double*)malloc(nb * (size_t)(m + 1));
+   double* H = (double*)calloc((size_t)(m + 1) * m, sizeof(double));
+   double* s = (double*)calloc((size_t)m + 1, sizeof(double));
+   double* cs = (double*)calloc((size_t)m + 1, sizeof(double));
+   double* sn = (double*)calloc((size_t)m + 1, sizeof(double));
+   double* y = (double*)calloc((size_t)m + 1, sizeof(double));
+   int ok = 1;
+   double normb;
+   S->iterations = 0;
+   normb = l2(b, n);
+   if (normb == 0) {
+      for (int32_t i = 0; i < n; i++) x[i] = 0;
+      goto done;
+   }
+#define RESIDUE(R)                                                      \
+   do {                                                                 \
+      csr_mv(&A, x, (R));                                               \
+      for (int32_t i = 0; i < n; i++) (R)[i] = b[i] - (R)[i];           \
+   } while (0)
+   RESIDUE(r);
+   double beta = l2(r, n);
+   S->iterations = 0;
+   set_residue(S, beta / normb);
+   while (check_next(S)) {
+      /* orthogonalize_MGS */
+      int o_steps = m;
+      for (int32_t i = 0; i < n; i++) V[i] = (1.0 / beta) * r[i];
+      for (int32_t i = 0; i < (m + 1) * m; i++) H[i] = 0.0;
+      for (int32_t i = 0; i <= m; i++) s[i] = 0.0;
+      s[0] = beta;
+      for (int i = 0; i < m && next_iteration(S); i++) {
+         double* vi = V + (size_t)i * n;
+         double* zi = Zb + (size_t)i * n;
+         prec_apply(&P, vi, zi);
+         csr_mv(&A, zi, w);
+         for (int k = 0; k <= i; k++) H[k + i * (m + 1)] = 0.0;
+         for (int l = 0; l < reorth; l++)
+            for (int k = 0; k <= i; k++) {
+               const double* vk = V + (size_t)k * n;
+               const double hki = dot(w, vk, n);
+               H[k + i * (m + 1)] += hki;
+               for (int32_t t = 0; t < n; t++) w[t] = w[t] - hki * vk[t];
+            }
+         const double normw = l2(w, n);
+         H[i + 1 + i * (m + 1)] = normw;
+         double* vn = V + (size_t)(i + 1) * n;
+         for (int32_t t = 0; t < n; t++) vn[t] = (1.0 / normw) * w[t];
+         /* apply_givens_rotations */
+         for (int k = 0; k < i; k++) {
+            double* dx = &H[k + i * (m + 1)];
+            double* dy = &H[k + 1 + i * (m + 1)];
+            const double tmp = cs[k] * *dx + sn[k] * *dy;
+            *dy = cs[k] * *dy - sn[k] * *dx;
+            *dx = tmp;
+         }
+         if (H[i + 1 + i * (m + 1)] != 0.0) {
+            double dx = H[i + i * (m + 1)], dy = H[i + 1 + i * (m + 1)];
+            if (dy == 0.0) {
+               cs[i] = 1.0;
+               sn[i] = 0.0;
+            }
+            else if (fabs(dy) > fabs(dx)) {
+               const double t = dx / dy;
+               sn[i] = 1.0 / sqrt(1.0 + t * t);
+               cs[i] = t * sn[i];
+            }
+            else {
+               const double t = dy / dx;
+               cs[i] = 1.0 / sqrt(1.0 + t * t);
+               sn[i] = t * cs[i];
+            }
+            double* hx = &H[i + i * (m + 1)];
+            double* hy = &H[i + 1 + i * (m + 1)];
+            double tmp = cs[i] * *hx + sn[i] * *hy;
+            *hy = cs[i] * *hy - sn[i] * *hx;
+            *hx = tmp;
+            tmp = cs[i] * s[i] + sn[i] * s[i + 1];
+            s[i + 1] = cs[i] * s[i + 1] - sn[i] * s[i];
+            s[i] = tmp;
+         }
+         set_residue(S, fabs(s[i + 1]) / normb);
+         if (!check_next(S)) {
+            o_steps = i;
+            break;
+         }
+      }
+      const int k_upd = (o_steps < m) ? o_steps : m - 1;
+      /* update(k, m, H, s, V, x) */
+      for (int i = 0; i <= m; i++) y[i] = s[i];
+      for (int i = k_upd; i >= 0; i--) {
+         if (H[i + i * (m + 1)] == 0) {
+            ok = -1;
+            goto done;
+         }
+         y[i] /= H[i + i * (m + 1)];
+         for (int j = i - 1; j >= 0; j--) y[j] -= H[j + i * (m + 1)] * y[i];
+      }
+      for (int32_t t = 0; t < n; t++) {
+         double acc = 0;
+         for (int j = 0; j <= k_upd; j++) acc += Zb[(size_t)j * n + t] * y[j];
+         x[t] = acc + x[t];
+      }
+      if (o_steps < m) {
+         ok = check_convergence(S);
+         goto done;
+      }
+      RESIDUE(r);
+      beta = l2(r, n);
+      set_residue(S, beta / normb);
+   }
+#undef RESIDUE
+   ok = check_convergence(S);
+done:
+   free(r);
+   free(w);
+   free(M_tmp);
+   free(V);
+   free(Zb);
+   free(H);
+   free(s);
+   free(cs);
+   free(sn);
+   free(y);
+   prec_free(&P);
+   return ok;
+}
+
 /* True residual ||b - A x|| / ||b|| (Solvers/Linear/Utils/LinearResidueGetter.hpp:11-23). */
 double orc_true_residual(int32_t n, const int32_t* rowptr, const int32_t* cols, const double* vals, const double* b,
                          const double* x)

@@ -48,3 +48,16 @@ def test_error_status_without_gpu():
         _capi.check(_capi.ERR_INVALID_ARGUMENT)
     with pytest.raises(OverflowError):
         _capi.check(_capi.ERR_OVERFLOW)
+
+
+def test_cpp_dropin_header_compiles():
+    """The C++ drop-in header compiles against the C ABI without a GPU."""
+    import shutil
+    import subprocess
+
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    out = ROOT / "tests" / "cpp" / "_build"
+    out.mkdir(exist_ok=True)
+    r = subprocess.run([nvcc, "-std=c++17", "-c", str(ROOT / "tests" / "cpp" / "dropin.cpp"), "-I", str(ROOT / "include"),
+                        "-o", str(out / "dropin.o")], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr

@@ -191,3 +191,86 @@ def test_mixed_precision_refinement_reaches_fp64_residual(oracle):
     assert r["converged"] and r["true_residual"] < 1e-10
     assert t.true_residual(M, bs, xs) < 1e-10
     assert oracle.true_residual(A, b, xs.cpu().numpy()) < 1e-10
+
+
+def test_fsai_factors_match_reference():
+    """Classical FSAI (SPD) and two-factor FSAI (nonsymmetric) values against
+    the FP64 numpy restatement (different small dense solvers: 1e-12)."""
+    from oracle import lfsai_ref as R
+    from tnl_b200 import generators as g
+
+    t = tnl()
+    A = g.diffusion_2d(30, 0.1, 2.0, 5)
+    M = t.SparseMatrix(t.CSR, torch.float64).assign(A.rowptr, A.cols, A.vals)
+    P = t.FSAI()
+    P.update(M)
+    rp, cols, vals = P.factor(0)
+    ref = R.fsai_classical(A)
+    assert np.allclose(vals, ref, rtol=1e-12, atol=1e-14)
+    _, _, gt = P.factor(1)
+    assert np.isclose(np.sort(gt), np.sort(ref), rtol=1e-12).all()
+    C = g.convection_diffusion_3d(10)
+    M2 = t.SparseMatrix(t.CSR, torch.float64).assign(C.rowptr, C.cols, C.vals)
+    P2 = t.FSAI2()
+    P2.update(M2)
+    _, _, gl = P2.factor(0)
+    gl_ref, h_ref = R.fsai2_classical(C)
+    assert np.allclose(gl, gl_ref, rtol=1e-11, atol=1e-14)
+
+
+def test_fsai_pcg_beats_jacobi():
+    from tnl_b200 import generators as g
+
+    t = tnl()
+    A = g.diffusion_2d(96, 0.1, 2.0, 8)
+    b = g.uniform_vector(A.n, 1)
+    its = {}
+    for name, P in (("jacobi", t.Diagonal()), ("fsai", t.FSAI())):
+        M = t.SparseMatrix(t.CSR, torch.float64).assign(A.rowptr, A.cols, A.vals)
+        P.update(M)
+        S = t.CG()
+        S.setMatrix(M)
+        S.setPreconditioner(P)
+        S.setConvergenceResidue(1e-8)
+        xs = torch.zeros(A.n, dtype=torch.float64, device="cuda")
+        bs = torch.tensor(b, device="cuda")
+        assert S.solve(bs, xs)
+        its[name] = S.getIterations()
+        assert t.true_residual(M, bs, xs) < 1e-6
+    assert its["fsai"] < 0.8 * its["jacobi"], its
+
+
+@pytest.mark.parametrize("precond", [1, 2])
+def test_fgmres_matches_oracle(oracle, precond):
+    from tnl_b200 import generators as g
+
+    t = tnl()
+    A = g.convection_diffusion_3d(12)
+    b = g.uniform_vector(A.n, 1)
+    o = oracle.solve("fgmres", A, b, precond=precond, tol=1e-8, maxit=5000, gmres_m=20, gmres_reorth=2)
+    M = t.SparseMatrix(t.CSR, torch.float64).assign(A.rowptr, A.cols, A.vals)
+    S = t.FGMRES()
+    S.setMatrix(M)
+    S.setup({"convergence-residue": 1e-8, "max-iterations": 5000, "gmres-restarting-min": 20,
+             "gmres-restarting-max": 20, "gmres-variant": "MGSR"})
+    P = t.Diagonal() if precond == 1 else t.ILU0()
+    P.update(M)
+    S.setPreconditioner(P)
+    bs = torch.tensor(b, device="cuda")
+    xs = torch.zeros(A.n, dtype=torch.float64, device="cuda")
+    assert S.solve(bs, xs) and o["converged"]
+    assert abs(S.getIterations() - o["iterations"]) <= 2
+    assert t.true_residual(M, bs, xs) < 1e-8 * 1.01
+
+
+def test_fgmres_fsai2_mixed_precision():
+    from tnl_b200 import generators as g
+
+    t = tnl()
+    A = g.convection_diffusion_3d(16)
+    b = g.uniform_vector(A.n, 1)
+    M = t.SparseMatrix(t.CSR, torch.float64).assign(A.rowptr, A.cols, A.vals)
+    bs = torch.tensor(b, device="cuda")
+    xs = torch.zeros(A.n, dtype=torch.float64, device="cuda")
+    r = t.solve_mixed(M, bs, xs, tol=1e-8, inner_tol=1e-4, inner="fsai2", solver="fgmres", gmres_restart=30)
+    assert r["converged"] and t.true_residual(M, bs, xs) < 1e-8

@@ -31,7 +31,7 @@ from .generators import CSRMatrix  # noqa: F401
 __all__ = [
     "CSR", "Ellpack", "SlicedEllpack", "ChunkedEllpack", "BiEllpack", "AdaptiveCSR", "SparseMatrix",
     "LaunchConfiguration", "ColumnMajorOrder", "RowMajorOrder", "CSRMatrix", "check", "BackendRuntimeError",
-    "CG", "BICGStab", "GMRES", "Diagonal", "ILU0", "FSAI", "solve_mixed", "true_residual",
+    "CG", "BICGStab", "GMRES", "FGMRES", "Diagonal", "ILU0", "FSAI", "FSAI2", "solve_mixed", "true_residual",
 ]
 
 ColumnMajorOrder = capi.COLUMN_MAJOR
@@ -385,10 +385,27 @@ class _Preconditioner:
         """Preconditioner::solve: x = M^{-1} b."""
         check(capi.tnlb_precond_solve(self._h, b.data_ptr(), x.data_ptr(), _stream()))
 
+    def factor(self, which: int = 0):
+        """(rowptr, cols, values) of an FSAI factor: 0 = G (G_L), 1 = the second
+        factor as applied (G^T, or G_U)."""
+        n = self.matrix.getRows()
+        cap = self.matrix.getValues().numel()
+        rp = np.zeros(n + 1, np.int32)
+        cols = np.zeros(max(cap, 1), np.int32)
+        vals = np.zeros(max(cap, 1), np.float64 if self.matrix.real == torch.float64 else np.float32)
+        check(capi.tnlb_precond_read_factor(self._h, which, rp.ctypes.data, cols.ctypes.data, vals.ctypes.data, cap))
+        return rp, cols[:rp[-1]], vals[:rp[-1]]
+
 
 class Diagonal(_Preconditioner):
     """Solvers::Linear::Preconditioners::Diagonal (Jacobi)."""
     KIND = capi.PRECOND_JACOBI
+
+
+class FSAI2(_Preconditioner):
+    """Two-factor FSAI for nonsymmetric matrices, M^-1 = G_U G_L (no
+    counterpart in the reference)."""
+    KIND = capi.PRECOND_FSAI2
 
 
 class FSAI(_Preconditioner):
@@ -512,6 +529,12 @@ class GMRES(_LinearSolver):
     KIND = capi.SOLVER_GMRES
 
 
+class FGMRES(_LinearSolver):
+    """Restarted GMRES with right, flexible preconditioning (no counterpart in
+    the reference): the stopping residue is the unpreconditioned one."""
+    KIND = capi.SOLVER_FGMRES
+
+
 def true_residual(M: SparseMatrix, b: torch.Tensor, x: torch.Tensor) -> float:
     """||b - A x|| / ||b|| in FP64 on the GPU (Utils/LinearResidueGetter.hpp:11-23)."""
     out = C.c_double()
@@ -521,7 +544,8 @@ def true_residual(M: SparseMatrix, b: torch.Tensor, x: torch.Tensor) -> float:
 
 
 def solve_mixed(M: SparseMatrix, b: torch.Tensor, x: torch.Tensor, tol: float = 1e-8, inner_tol: float = 1e-4,
-                max_outer: int = 50, max_iterations: int = 1000000000, inner: str | _Preconditioner = "jacobi") -> dict:
+                max_outer: int = 50, max_iterations: int = 1000000000, inner: str | _Preconditioner = "jacobi",
+                solver: str = "cg", gmres_restart: int = 30) -> dict:
     """FP32 PCG inside FP64 iterative refinement (SPD matrices, FP64 matrix and vectors).
 
     ``inner`` is "jacobi", "fsai", "ilu0", "none", or an FP32 preconditioner
@@ -533,14 +557,17 @@ def solve_mixed(M: SparseMatrix, b: torch.Tensor, x: torch.Tensor, tol: float = 
     capi.tnlb_solver_params_default(C.byref(p))
     p.convergence_residue = tol
     p.max_iterations = max_iterations
+    p.gmres_restarting_min = p.gmres_restarting_max = gmres_restart
+    skind = {"cg": capi.SOLVER_CG, "bicgstab": capi.SOLVER_BICGSTAB, "gmres": capi.SOLVER_GMRES,
+             "fgmres": capi.SOLVER_FGMRES}[solver]
     r = capi.SolveResult()
     outer = C.c_int32()
     kinds = {"none": capi.PRECOND_NONE, "jacobi": capi.PRECOND_JACOBI, "ilu0": capi.PRECOND_ILU0,
-             "fsai": capi.PRECOND_FSAI}
+             "fsai": capi.PRECOND_FSAI, "fsai2": capi.PRECOND_FSAI2}
     kind = kinds.get(inner, capi.PRECOND_JACOBI) if isinstance(inner, str) else capi.PRECOND_NONE
     handle = None if isinstance(inner, str) else inner.handle
     check(capi.tnlb_solve_mixed(C.byref(p), M.segments.handle, M.columnIndexes.data_ptr(), M.values.data_ptr(),
-                                b.data_ptr(), x.data_ptr(), inner_tol, max_outer, kind, handle, _stream(), C.byref(r),
-                                C.byref(outer)))
+                                b.data_ptr(), x.data_ptr(), inner_tol, max_outer, skind, kind, handle, _stream(),
+                                C.byref(r), C.byref(outer)))
     return {"converged": bool(r.converged), "inner_iterations": r.iterations, "outer_iterations": outer.value,
             "true_residual": r.residue}

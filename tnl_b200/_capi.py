@@ -72,8 +72,8 @@ class SolveResult(C.Structure):
                 ("status_detail", C.c_int32), ("reserved", C.c_int32)]
 
 
-SOLVER_CG, SOLVER_BICGSTAB, SOLVER_GMRES = range(3)
-PRECOND_NONE, PRECOND_JACOBI, PRECOND_ILU0, PRECOND_FSAI = range(4)
+SOLVER_CG, SOLVER_BICGSTAB, SOLVER_GMRES, SOLVER_FGMRES = range(4)
+PRECOND_NONE, PRECOND_JACOBI, PRECOND_ILU0, PRECOND_FSAI, PRECOND_FSAI2 = range(5)
 GMRES_CGS, GMRES_CGSR, GMRES_MGS, GMRES_MGSR, GMRES_CWY = range(5)
 
 _p = C.c_void_p
@@ -103,11 +103,12 @@ tnlb_solver_params_default = _sig("tnlb_solver_params_default", [C.POINTER(Solve
 tnlb_solve = _sig("tnlb_solve", [C.c_int, C.c_int, C.POINTER(SolverParams), _p, C.c_int, _p, _p, _p, _p, _p,
                                  C.POINTER(SolveResult)])
 tnlb_true_residual = _sig("tnlb_true_residual", [_p, C.c_int, _p, _p, _p, _p, _p, C.POINTER(_f64)])
-tnlb_solve_mixed = _sig("tnlb_solve_mixed", [C.POINTER(SolverParams), _p, _p, _p, _p, _p, _f64, _i32, C.c_int, _p,
-                                             _p, C.POINTER(SolveResult), C.POINTER(_i32)])
+tnlb_solve_mixed = _sig("tnlb_solve_mixed", [C.POINTER(SolverParams), _p, _p, _p, _p, _p, _f64, _i32, C.c_int,
+                                             C.c_int, _p, _p, C.POINTER(SolveResult), C.POINTER(_i32)])
 tnlb_precond_create = _sig("tnlb_precond_create", [C.c_int, _p, C.c_int, _p, _p, _p, C.POINTER(_p)])
 tnlb_precond_solve = _sig("tnlb_precond_solve", [_p, _p, _p, _p])
 tnlb_precond_destroy = _sig("tnlb_precond_destroy", [_p])
+tnlb_precond_read_factor = _sig("tnlb_precond_read_factor", [_p, _i32, _p, _p, _p, _i64])
 tnlb_solve_preconditioned = _sig("tnlb_solve_preconditioned", [C.c_int, _p, C.POINTER(SolverParams), _p, C.c_int, _p,
                                                                _p, _p, _p, _p, C.POINTER(SolveResult)])
 tnlb_lfsai_num_params = _sig("tnlb_lfsai_num_params", [], _i64)

@@ -4,6 +4,7 @@
 #include <cfloat>
 #include <new>
 
+#include "fsai.cuh"
 #include "internal.cuh"
 #include "lfsai.cuh"
 
@@ -299,7 +300,7 @@ tnlb_status tnlb_solve_preconditioned(tnlb_solver_kind solver, const tnlb_precon
    clear_error();
    TNLB_TRY_STATUS(check_solve_args(seg, real, d_b, d_x));
    TNLB_REQUIRE(result != nullptr, TNLB_ERR_INVALID_ARGUMENT, "null result");
-   TNLB_REQUIRE(solver >= TNLB_SOLVER_CG && solver <= TNLB_SOLVER_GMRES, TNLB_ERR_INVALID_ARGUMENT, "unknown solver");
+   TNLB_REQUIRE(solver >= TNLB_SOLVER_CG && solver <= TNLB_SOLVER_FGMRES, TNLB_ERR_INVALID_ARGUMENT, "unknown solver");
    tnlb_solver_params p;
    tnlb_solver_params_default(&p);
    if (params) p = *params;
@@ -315,7 +316,7 @@ tnlb_status tnlb_solve(tnlb_solver_kind solver, tnlb_precond_kind precond, const
 {
    clear_error();
    TNLB_TRY_STATUS(check_solve_args(seg, real, d_b, d_x));
-   TNLB_REQUIRE(precond >= TNLB_PRECOND_NONE && precond <= TNLB_PRECOND_FSAI, TNLB_ERR_INVALID_ARGUMENT,
+   TNLB_REQUIRE(precond >= TNLB_PRECOND_NONE && precond <= TNLB_PRECOND_FSAI2, TNLB_ERR_INVALID_ARGUMENT,
                 "unknown preconditioner");
    tnlb_precond* P = nullptr;
    if (precond != TNLB_PRECOND_NONE)
@@ -336,8 +337,9 @@ tnlb_status tnlb_true_residual(const tnlb_segments* seg, tnlb_real real, const i
 
 tnlb_status tnlb_solve_mixed(const tnlb_solver_params* params, const tnlb_segments* seg, const int32_t* d_cols,
                              const double* d_values, const double* d_b, double* d_x, double inner_tolerance,
-                             int32_t max_outer, tnlb_precond_kind inner_precond, const tnlb_precond* inner,
-                             tnlb_stream stream, tnlb_solve_result* result, int32_t* outer_iterations)
+                             int32_t max_outer, tnlb_solver_kind inner_solver, tnlb_precond_kind inner_precond,
+                             const tnlb_precond* inner, tnlb_stream stream, tnlb_solve_result* result,
+                             int32_t* outer_iterations)
 {
    clear_error();
    TNLB_TRY_STATUS(check_solve_args(seg, TNLB_F64, d_b, d_x));
@@ -345,7 +347,9 @@ tnlb_status tnlb_solve_mixed(const tnlb_solver_params* params, const tnlb_segmen
    TNLB_REQUIRE(inner_tolerance > 0 && inner_tolerance < 1, TNLB_ERR_INVALID_ARGUMENT,
                 "inner tolerance must lie in (0, 1)");
    TNLB_REQUIRE(max_outer >= 0, TNLB_ERR_INVALID_ARGUMENT, "negative max_outer");
-   TNLB_REQUIRE(inner || (inner_precond >= TNLB_PRECOND_NONE && inner_precond <= TNLB_PRECOND_FSAI),
+   TNLB_REQUIRE(inner_solver >= TNLB_SOLVER_CG && inner_solver <= TNLB_SOLVER_FGMRES, TNLB_ERR_INVALID_ARGUMENT,
+                "unknown inner solver");
+   TNLB_REQUIRE(inner || (inner_precond >= TNLB_PRECOND_NONE && inner_precond <= TNLB_PRECOND_FSAI2),
                 TNLB_ERR_INVALID_ARGUMENT, "unknown preconditioner");
    tnlb_solver_params p;
    tnlb_solver_params_default(&p);
@@ -353,7 +357,7 @@ tnlb_status tnlb_solve_mixed(const tnlb_solver_params* params, const tnlb_segmen
    int32_t inner_its = 0;
    *result = tnlb_solve_result{};
    return tnlb::solve_mixed_cg(seg, d_cols, d_values, d_b, d_x, p, inner_tolerance, max_outer, (cudaStream_t)stream,
-                               result, &inner_its, outer_iterations, inner_precond, inner);
+                               result, &inner_its, outer_iterations, inner_precond, inner, inner_solver);
 }
 
 tnlb_status tnlb_precond_create(tnlb_precond_kind kind, const tnlb_segments* seg, tnlb_real real,
@@ -362,7 +366,7 @@ tnlb_status tnlb_precond_create(tnlb_precond_kind kind, const tnlb_segments* seg
    clear_error();
    TNLB_REQUIRE(seg && out, TNLB_ERR_INVALID_ARGUMENT, "null argument");
    TNLB_REQUIRE(real == TNLB_F32 || real == TNLB_F64, TNLB_ERR_INVALID_ARGUMENT, "unknown real type");
-   TNLB_REQUIRE(kind >= TNLB_PRECOND_NONE && kind <= TNLB_PRECOND_FSAI, TNLB_ERR_INVALID_ARGUMENT,
+   TNLB_REQUIRE(kind >= TNLB_PRECOND_NONE && kind <= TNLB_PRECOND_FSAI2, TNLB_ERR_INVALID_ARGUMENT,
                 "unknown preconditioner");
    *out = nullptr;
    return tnlb::precond_create(kind, seg, real, d_cols, d_values, (cudaStream_t)stream, out);
@@ -373,6 +377,25 @@ tnlb_status tnlb_precond_solve(const tnlb_precond* precond, const void* d_b, voi
    clear_error();
    TNLB_REQUIRE(precond && d_b && d_x, TNLB_ERR_INVALID_ARGUMENT, "null argument");
    return tnlb::precond_apply(precond, d_b, d_x, (cudaStream_t)stream);
+}
+
+tnlb_status tnlb_precond_read_factor(const tnlb_precond* precond, int32_t which, int32_t* h_rowptr, int32_t* h_cols,
+                                     void* h_values, int64_t capacity)
+{
+   clear_error();
+   TNLB_REQUIRE(precond && h_rowptr && h_cols && h_values, TNLB_ERR_INVALID_ARGUMENT, "null argument");
+   TNLB_REQUIRE(precond->fsai != nullptr, TNLB_ERR_INVALID_ARGUMENT, "not an FSAI preconditioner");
+   TNLB_REQUIRE(which == 0 || which == 1, TNLB_ERR_INVALID_ARGUMENT, "which must be 0 or 1");
+   const Fsai* F = precond->fsai;
+   const tnlb_segments* seg = which == 0 ? F->g : F->gt;
+   const int64_t nnz = seg->elements;
+   TNLB_REQUIRE(capacity >= nnz, TNLB_ERR_INVALID_ARGUMENT, "buffer too small");
+   const size_t rs = F->real == TNLB_F64 ? 8 : 4;
+   TNLB_CUDA_TRY(cudaMemcpy(h_rowptr, seg->offsets.ptr, sizeof(int32_t) * ((size_t)F->n + 1), cudaMemcpyDeviceToHost));
+   TNLB_CUDA_TRY(cudaMemcpy(h_cols, (which == 0 ? F->g_cols : F->gt_cols).ptr, sizeof(int32_t) * nnz,
+                            cudaMemcpyDeviceToHost));
+   TNLB_CUDA_TRY(cudaMemcpy(h_values, (which == 0 ? F->g_vals : F->gt_vals).ptr, rs * nnz, cudaMemcpyDeviceToHost));
+   return TNLB_OK;
 }
 
 tnlb_status tnlb_precond_destroy(tnlb_precond* precond)

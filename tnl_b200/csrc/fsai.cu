@@ -109,6 +109,75 @@ __global__ void k_fsai_rows(const int32_t* __restrict__ rp, const int32_t* __res
    for (int r = 0; r < k; r++) gvals[b + r] = (Real)(y[r] * scale);
 }
 
+// Two-factor FSAI row for a nonsymmetric A: with B = A[J,J] (J the lower
+// pattern of row i, i last), g_L = B^-T e_last is row i of G_L and
+// g_U = B^-1 e_last is column i of G_U; both are scaled by 1/sqrt(g_U,last)
+// (= 1/sqrt((B^-1)_last,last)) so that diag(G_L A G_U) = 1 on the pattern.
+// Row i of H = G_U^T (lower, same pattern) is written to hvals.  LU without
+// pivoting (the local blocks of the diagonally dominant operators are).
+template <typename Real>
+__global__ void k_fsai2_rows(const int32_t* __restrict__ rp, const int32_t* __restrict__ cols,
+                             const Real* __restrict__ vals, int32_t n, const int32_t* __restrict__ grp,
+                             const int32_t* __restrict__ gcols, Real* __restrict__ gvals, Real* __restrict__ hvals,
+                             int32_t* __restrict__ err)
+{
+   constexpr int KM = 12;
+   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+   if (i >= n) return;
+   const int32_t b = grp[i], k = grp[i + 1] - b;
+   if (k <= 0 || k > KM) {
+      atomicExch(err, 1);
+      return;
+   }
+   double B[KM][KM];
+   for (int r = 0; r < k; r++)
+      for (int c = 0; c < k; c++) B[r][c] = (double)lookup(rp, cols, vals, gcols[b + r], gcols[b + c]);
+   // in-place LU (Doolittle), B = L U
+   for (int p = 0; p < k; p++) {
+      if (B[p][p] == 0.0) {
+         atomicExch(err, 2);
+         return;
+      }
+      for (int r = p + 1; r < k; r++) {
+         const double l = B[r][p] / B[p][p];
+         B[r][p] = l;
+         for (int c = p + 1; c < k; c++) B[r][c] -= l * B[p][c];
+      }
+   }
+   // u = B^-1 e: L y = e, U u = y
+   double u[KM], w[KM];
+   for (int r = 0; r < k; r++) {
+      double sacc = (r == k - 1) ? 1.0 : 0.0;
+      for (int q = 0; q < r; q++) sacc -= B[r][q] * u[q];
+      u[r] = sacc;
+   }
+   for (int r = k - 1; r >= 0; r--) {
+      double sacc = u[r];
+      for (int q = r + 1; q < k; q++) sacc -= B[r][q] * u[q];
+      u[r] = sacc / B[r][r];
+   }
+   // w = B^-T e: U^T z = e, L^T w = z
+   for (int r = 0; r < k; r++) {
+      double sacc = (r == k - 1) ? 1.0 : 0.0;
+      for (int q = 0; q < r; q++) sacc -= B[q][r] * w[q];
+      w[r] = sacc / B[r][r];
+   }
+   for (int r = k - 1; r >= 0; r--) {
+      double sacc = w[r];
+      for (int q = r + 1; q < k; q++) sacc -= B[q][r] * w[q];
+      w[r] = sacc;
+   }
+   if (!(u[k - 1] > 0)) {
+      atomicExch(err, 2);
+      return;
+   }
+   const double scale = 1.0 / sqrt(u[k - 1]);
+   for (int r = 0; r < k; r++) {
+      gvals[b + r] = (Real)(w[r] * scale);
+      hvals[b + r] = (Real)(u[r] * scale);
+   }
+}
+
 // Transpose of a CSR matrix with ascending columns: counting by column,
 // then each row of the transpose is filled in ascending source-row order
 // (one thread per transpose row scanning a precomputed list is avoided by
@@ -197,7 +266,7 @@ tnlb_status make_csr_segments(const int32_t* d_rowptr, int32_t n, cudaStream_t s
 // values; then G^T.  The values of a learned G are written later through
 // fsai_set_values.
 tnlb_status fsai_create(const tnlb_segments* seg, tnlb_real real, const int32_t* cols, const void* vals, bool classical,
-                        cudaStream_t st, Fsai** out)
+                        cudaStream_t st, Fsai** out, bool two_factor)
 {
    const int32_t n = seg->n;
    TNLB_REQUIRE(n > 0, TNLB_ERR_INVALID_ARGUMENT, "FSAI: the matrix is empty");
@@ -224,11 +293,25 @@ tnlb_status fsai_create(const tnlb_segments* seg, tnlb_real real, const int32_t*
                                                   F->g_cols.as<int32_t>());
    TNLB_CHECK_LAUNCH();
    TNLB_TRY_STATUS(make_csr_segments(grp.as<int32_t>(), n, st, &F->g));
+   DeviceBuffer hvals;  // two-factor: row i of H = G_U^T on G's pattern
+   if (two_factor) TNLB_TRY_STATUS(hvals.alloc(rs * gnnz));
    if (classical) {
       DeviceBuffer err;
       TNLB_TRY_STATUS(err.alloc(sizeof(int32_t)));
       TNLB_CUDA_TRY(cudaMemsetAsync(err.ptr, 0, sizeof(int32_t), st));
-      if (real == TNLB_F64)
+      if (two_factor) {
+         if (real == TNLB_F64)
+            k_fsai2_rows<double><<<grid_for(n, 128), 128, 0, st>>>(F->a_rp.as<int32_t>(), F->a_cols.as<int32_t>(),
+                                                                  F->a_vals.as<double>(), n, grp.as<int32_t>(),
+                                                                  F->g_cols.as<int32_t>(), F->g_vals.as<double>(),
+                                                                  hvals.as<double>(), err.as<int32_t>());
+         else
+            k_fsai2_rows<float><<<grid_for(n, 128), 128, 0, st>>>(F->a_rp.as<int32_t>(), F->a_cols.as<int32_t>(),
+                                                                 F->a_vals.as<float>(), n, grp.as<int32_t>(),
+                                                                 F->g_cols.as<int32_t>(), F->g_vals.as<float>(),
+                                                                 hvals.as<float>(), err.as<int32_t>());
+      }
+      else if (real == TNLB_F64)
          k_fsai_rows<double><<<grid_for(n, 128), 128, 0, st>>>(F->a_rp.as<int32_t>(), F->a_cols.as<int32_t>(),
                                                               F->a_vals.as<double>(), n, grp.as<int32_t>(),
                                                               F->g_cols.as<int32_t>(), F->g_vals.as<double>(),
@@ -242,8 +325,8 @@ tnlb_status fsai_create(const tnlb_segments* seg, tnlb_real real, const int32_t*
       int32_t h = 0;
       TNLB_CUDA_TRY(cudaMemcpyAsync(&h, err.ptr, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
       TNLB_CUDA_TRY(cudaStreamSynchronize(st));
-      TNLB_REQUIRE(h != 1, TNLB_ERR_INVALID_ARGUMENT, "FSAI: a row of the pattern holds more than 32 entries");
-      TNLB_REQUIRE(h != 2, TNLB_ERR_INVALID_ARGUMENT, "FSAI: a local block A[J,J] is not positive definite");
+      TNLB_REQUIRE(h != 1, TNLB_ERR_INVALID_ARGUMENT, "FSAI: a row of the pattern holds too many entries");
+      TNLB_REQUIRE(h != 2, TNLB_ERR_INVALID_ARGUMENT, "FSAI: a local block A[J,J] is singular or not positive definite");
    }
    // transpose pattern
    DeviceBuffer tcnt, cursor;
@@ -268,12 +351,14 @@ tnlb_status fsai_create(const tnlb_segments* seg, tnlb_real real, const int32_t*
    TNLB_TRY_STATUS(make_csr_segments(trp.as<int32_t>(), n, st, &F->gt));
    TNLB_TRY_STATUS(F->tmp.alloc(rs * n));
    if (classical) {
+      // G^T from G (symmetric case), or G_U = H^T (two factors)
+      const void* src = two_factor ? hvals.ptr : F->g_vals.ptr;
       if (real == TNLB_F64)
          k_gather_vals<double><<<grid_for(gnnz, 1024), 256, 0, st>>>(F->gt_src.as<int32_t>(), gnnz,
-                                                                     F->g_vals.as<double>(), F->gt_vals.as<double>());
+                                                                     (const double*)src, F->gt_vals.as<double>());
       else
          k_gather_vals<float><<<grid_for(gnnz, 1024), 256, 0, st>>>(F->gt_src.as<int32_t>(), gnnz,
-                                                                    F->g_vals.as<float>(), F->gt_vals.as<float>());
+                                                                    (const float*)src, F->gt_vals.as<float>());
       TNLB_CHECK_LAUNCH();
    }
    TNLB_CUDA_TRY(cudaStreamSynchronize(st));

@@ -282,14 +282,14 @@ tnlb_status true_residual(const tnlb_segments* seg, tnlb_real real, const int32_
 tnlb_status solve_mixed_cg(const tnlb_segments* seg, const int32_t* cols, const double* vals, const double* b,
                            double* x, const tnlb_solver_params& prm, double inner_tol, int32_t max_outer,
                            cudaStream_t st, tnlb_solve_result* res, int32_t* inner_total, int32_t* outer,
-                           int inner_kind, const tnlb_precond* inner_precond);
+                           int inner_kind, const tnlb_precond* inner_precond, int inner_solver);
 tnlb_status ilu0_create(const tnlb_segments* seg, tnlb_real real, const int32_t* cols, const void* vals,
                         cudaStream_t st, void** out);
 tnlb_status ilu0_apply(void* ilu, const void* b, void* x, cudaStream_t st);
 tnlb_status ilu0_read(void* ilu, int32_t* h_rowptr, int32_t* h_cols, void* h_vals, int64_t capacity, int real_bytes);
 void ilu0_destroy(void* ilu);
 tnlb_status fsai_create(const tnlb_segments* seg, tnlb_real real, const int32_t* cols, const void* vals,
-                        bool classical, cudaStream_t st, Fsai** out);
+                        bool classical, cudaStream_t st, Fsai** out, bool two_factor = false);
 tnlb_status fsai_apply(const Fsai* F, const void* r, void* z, cudaStream_t st, const int32_t* skip = nullptr);
 tnlb_status fsai_set_values(Fsai* F, const void* gvals, cudaStream_t st);
 void fsai_destroy(Fsai* F);

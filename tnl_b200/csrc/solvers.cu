@@ -842,8 +842,10 @@ tnlb_status bicgstab_solve(const Ctx<Real>& c, const Precond<Real>& P, const tnl
 
 template <typename Real>
 tnlb_status gmres_solve(const Ctx<Real>& c, const Precond<Real>& P, const tnlb_solver_params& prm, const Real* b,
-                        Real* x, tnlb_solve_result* res)
+                        Real* x, tnlb_solve_result* res, bool flexible = false)
 {
+   // flexible = right preconditioning with the preconditioned basis kept
+   // (FGMRES): w = A M^-1 v_i, x += Z y; residues are unpreconditioned.
    const int64_t n = c.n;
    const int rmin = prm.gmres_restarting_min, rmax = prm.gmres_restarting_max;
    const int dmin = prm.gmres_restarting_step_min, dmax = prm.gmres_restarting_step_max;
@@ -867,10 +869,13 @@ tnlb_status gmres_solve(const Ctx<Real>& c, const Precond<Real>& P, const tnlb_s
    TNLB_TRY_STATUS(M_tmp.alloc(sizeof(Real) * n));
    TNLB_TRY_STATUS(hdev.alloc(sizeof(double) * 128));
    TNLB_TRY_STATUS(ydev.alloc(sizeof(double) * 128));
+   DeviceBuffer Z;
+   if (flexible) TNLB_TRY_STATUS(Z.alloc(sizeof(Real) * ld * m_max));
    Real* Vp = V.as<Real>();
    double* sc = W.scratch.as<double>();
    const unsigned G = vec_grid(n);
-   const bool pre = P.kind != TNLB_PRECOND_NONE;
+   const bool pre = P.kind != TNLB_PRECOND_NONE && !flexible;
+   const bool rightp = P.kind != TNLB_PRECOND_NONE && flexible;
    double hs[2];
    auto norm = [&](const Real* a, double* out) -> tnlb_status {
       k_dots<Real><<<G, kRedThreads, 0, c.st>>>(n, a, a, nullptr, nullptr, W.red(), sc);
@@ -932,7 +937,8 @@ tnlb_status gmres_solve(const Ctx<Real>& c, const Precond<Real>& P, const tnlb_s
          for (int j = i - 1; j >= 0; j--) y[j] -= H[j + i * (m + 1)] * y[i];
       }
       TNLB_CUDA_TRY(cudaMemcpyAsync(ydev.ptr, y.data(), sizeof(double) * (k + 1), cudaMemcpyHostToDevice, c.st));
-      k_gmres_update<Real><<<vec_grid(n), kRedThreads, 0, c.st>>>(n, ld, k + 1, Vp, ydev.as<double>(), x);
+      k_gmres_update<Real><<<vec_grid(n), kRedThreads, 0, c.st>>>(n, ld, k + 1, rightp ? Z.as<Real>() : Vp,
+                                                                  ydev.as<double>(), x);
       TNLB_CHECK_LAUNCH();
       return TNLB_OK;
    };
@@ -960,8 +966,13 @@ tnlb_status gmres_solve(const Ctx<Real>& c, const Precond<Real>& P, const tnlb_s
          it++;
          if (!cont) break;
          Real* vi = Vp + (int64_t)i * ld;
-         // w = M^-1 A v_i
-         if (pre) {
+         // w = M^-1 A v_i (left), or z_i = M^-1 v_i, w = A z_i (flexible)
+         if (rightp) {
+            Real* zi = Z.as<Real>() + (int64_t)i * ld;
+            TNLB_TRY_STATUS(P.apply(n, vi, zi, c.st));
+            TNLB_TRY_STATUS(c.spmv(zi, w.as<Real>()));
+         }
+         else if (pre) {
             TNLB_TRY_STATUS(c.spmv(vi, M_tmp.as<Real>()));
             TNLB_TRY_STATUS(P.apply(n, M_tmp.as<Real>(), w.as<Real>(), c.st));
          }
@@ -1080,6 +1091,7 @@ tnlb_status solve_t(tnlb_solver_kind solver, const tnlb_precond* pobj, const tnl
          return cg_solve<Real>(c, P, prm, b, x, res);
       case TNLB_SOLVER_BICGSTAB: return bicgstab_solve<Real>(c, P, prm, b, x, res);
       case TNLB_SOLVER_GMRES: return gmres_solve<Real>(c, P, prm, b, x, res);
+      case TNLB_SOLVER_FGMRES: return gmres_solve<Real>(c, P, prm, b, x, res, true);
    }
    set_error("unknown solver");
    return TNLB_ERR_INVALID_ARGUMENT;
@@ -1161,6 +1173,10 @@ tnlb_status precond_create(int kind, const tnlb_segments* seg, tnlb_real real, c
       s = ilu0_create(seg, real, cols, vals, st, &P->ilu);
    else if (kind == TNLB_PRECOND_FSAI)
       s = fsai_create(seg, real, cols, vals, true, st, &P->fsai);
+   else if (kind == TNLB_PRECOND_FSAI2) {
+      s = fsai_create(seg, real, cols, vals, true, st, &P->fsai, true);
+      P->kind = TNLB_PRECOND_FSAI;  // applied the same way: z = G_U (G_L r)
+   }
    if (s != TNLB_OK) {
       delete P;
       return s;
@@ -1191,11 +1207,11 @@ tnlb_status precond_apply(const tnlb_precond* P, const void* b, void* x, cudaStr
    return TNLB_OK;
 }
 
-// FP32 inner CG (Jacobi) inside FP64 iterative refinement.
+// FP32 inner Krylov solve inside FP64 iterative refinement.
 tnlb_status solve_mixed_cg(const tnlb_segments* seg, const int32_t* cols, const double* vals, const double* b,
                            double* x, const tnlb_solver_params& prm, double inner_tol, int32_t max_outer,
                            cudaStream_t st, tnlb_solve_result* res, int32_t* inner_total, int32_t* outer,
-                           int inner_kind, const tnlb_precond* inner_precond)
+                           int inner_kind, const tnlb_precond* inner_precond, int inner_solver)
 {
    const int64_t n = seg->n;
    DeviceBuffer v32, r64, r32, d32, d64;
@@ -1241,10 +1257,8 @@ tnlb_status solve_mixed_cg(const tnlb_segments* seg, const int32_t* cols, const 
       TNLB_CUDA_TRY(cudaMemsetAsync(d32.ptr, 0, sizeof(float) * n, st));
       TNLB_CHECK_LAUNCH();
       tnlb_solve_result ir{};
-      if (P.kind == TNLB_PRECOND_ILU0)
-         TNLB_TRY_STATUS(pcg_general<float>(c32, P, ip, r32.as<float>(), d32.as<float>(), &ir));
-      else
-         TNLB_TRY_STATUS(cg_solve<float>(c32, P, ip, r32.as<float>(), d32.as<float>(), &ir));
+      TNLB_TRY_STATUS(solve_t<float>((tnlb_solver_kind)inner_solver, pobj, ip, seg, TNLB_F32, cols, v32.as<float>(),
+                                     r32.as<float>(), d32.as<float>(), st, &ir));
       *inner_total += ir.iterations;
       (*outer)++;
       // x += rn * d
