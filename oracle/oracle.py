@@ -111,6 +111,7 @@ class Oracle:
             ("orc_bicgstab", [i32, p, p, p, C.c_int, C.c_int, p, p, C.POINTER(SolverState)], C.c_int),
             ("orc_gmres", [i32, p, p, p, C.c_int, i32, C.c_int, p, p, C.POINTER(SolverState)], C.c_int),
             ("orc_fgmres", [i32, p, p, p, C.c_int, i32, C.c_int, p, p, C.POINTER(SolverState)], C.c_int),
+            ("orc_gmres_cwy", [i32, p, p, p, C.c_int, i32, p, p, C.POINTER(SolverState)], C.c_int),
             ("orc_true_residual", [i32, p, p, p, p, p], f64),
             ("orc_ilu0_factor", [i32, p, p, p, p, p, p, p, p, p], C.c_int),
             ("orc_prec_apply", [i32, p, p, p, C.c_int, p, p], C.c_int),
@@ -237,6 +238,8 @@ class Oracle:
             ok = self.L.orc_bicgstab(*args, precond, int(bicgstab_exact), b.ctypes.data, x.ctypes.data, C.byref(S))
         elif solver == "gmres":
             ok = self.L.orc_gmres(*args, precond, gmres_m, gmres_reorth, b.ctypes.data, x.ctypes.data, C.byref(S))
+        elif solver == "gmres_cwy":
+            ok = self.L.orc_gmres_cwy(*args, precond, gmres_m, b.ctypes.data, x.ctypes.data, C.byref(S))
         elif solver == "fgmres":
             ok = self.L.orc_fgmres(*args, precond, gmres_m, gmres_reorth, b.ctypes.data, x.ctypes.data, C.byref(S))
         else:

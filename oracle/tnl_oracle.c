@@ -1031,6 +1031,217 @@ done:
    return ok;
 }
 
+/* GMRES::apply_givens_rotations (Solvers/Linear/GMRES.hpp:731-770) on
+ * column i of H (leading dimension m + 1) and on s. */
+static void givens_column(int i, int m, double* H, double* s, double* cs, double* sn)
+{
+   for (int k = 0; k < i; k++) {
+      double* dx = &H[k + i * (m + 1)];
+      double* dy = &H[k + 1 + i * (m + 1)];
+      const double tmp = cs[k] * *dx + sn[k] * *dy;
+      *dy = cs[k] * *dy - sn[k] * *dx;
+      *dx = tmp;
+   }
+   if (H[i + 1 + i * (m + 1)] != 0.0) {
+      double dx = H[i + i * (m + 1)], dy = H[i + 1 + i * (m + 1)];
+      if (dy == 0.0) {
+         cs[i] = 1.0;
+         sn[i] = 0.0;
+      }
+      else if (fabs(dy) > fabs(dx)) {
+         const double t = dx / dy;
+         sn[i] = 1.0 / sqrt(1.0 + t * t);
+         cs[i] = t * sn[i];
+      }
+      else {
+         const double t = dy / dx;
+         cs[i] = 1.0 / sqrt(1.0 + t * t);
+         sn[i] = t * cs[i];
+      }
+      double* hx = &H[i + i * (m + 1)];
+      double* hy = &H[i + 1 + i * (m + 1)];
+      double tmp = cs[i] * *hx + sn[i] * *hy;
+      *hy = cs[i] * *hy - sn[i] * *hx;
+      *hx = tmp;
+      tmp = cs[i] * s[i] + sn[i] * s[i + 1];
+      s[i + 1] = cs[i] * s[i + 1] - sn[i] * s[i];
+      s[i] = tmp;
+   }
+}
+
+/* GMRES::solve with the CWY orthogonalisation: Householder reflections
+ * P_i = I - t_i y_i y_i^T accumulated in compact WY form I - Y T Y^T
+ * (orthogonalize_CWY, Solvers/Linear/GMRES.hpp:350-423; hauseholder_generate
+ * :468-537; hauseholder_apply_trunc :539-570; hauseholder_cwy :572-604;
+ * hauseholder_cwy_transposed :606-643; the CWY branch of update :685-720).
+ * The basis vectors are not stored: v_i = (I - Y T Y^T) e_i is rebuilt when
+ * needed.  Y is n x (m+1) (column j zero above row j); YL holds its upper
+ * (m+1) x (m+1) block; T is upper triangular with leading dimension m+1.
+ * Each orthogonalisation cycle counts m+1 iterations (i = 0..m) and makes m
+ * products.  Requires n >= m + 1.  Returns as orc_gmres. */
+int orc_gmres_cwy(int32_t n, const int32_t* rowptr, const int32_t* cols, const double* vals, int precond, int32_t m,
+                  const double* b, double* x, orc_solver_state* S)
+{
+   orc_csr A = {n, rowptr, cols, vals};
+   orc_prec P;
+   prec_setup(&P, &A, precond);
+   const int L = m + 1;  /* restarting_max + 1 */
+   const size_t nb = sizeof(double) * (size_t)n;
+   double *r = malloc(nb), *w = malloc(nb), *z = malloc(nb), *v = malloc(nb), *M_tmp = malloc(nb);
+   double* Y = (double*)calloc((size_t)n * L, sizeof(double));
+   double* YL = (double*)calloc((size_t)L * L, sizeof(double));
+   double* T = (double*)calloc((size_t)L * L, sizeof(double));
+   double* H = (double*)calloc((size_t)(m + 1) * m, sizeof(double));
+   double* s = (double*)calloc((size_t)m + 1, sizeof(double));
+   double* cs = (double*)calloc((size_t)m + 1, sizeof(double));
+   double* sn = (double*)calloc((size_t)m + 1, sizeof(double));
+   double* y = (double*)calloc((size_t)m + 1, sizeof(double));
+   double* aux = (double*)calloc((size_t)L, sizeof(double));
+   int ok = 1;
+   double normb;
+   S->iterations = 0;
+   if (n < L) {
+      ok = 0;
+      goto done;
+   }
+   if (precond) {
+      prec_apply(&P, b, M_tmp);
+      normb = l2(M_tmp, n);
+   }
+   else
+      normb = l2(b, n);
+   if (normb == 0) {
+      for (int32_t i = 0; i < n; i++) x[i] = 0;
+      goto done;
+   }
+#define RESIDUE(R)                                                      \
+   do {                                                                 \
+      csr_mv(&A, x, M_tmp);                                             \
+      for (int32_t i = 0; i < n; i++) M_tmp[i] = b[i] - M_tmp[i];       \
+      prec_apply(&P, M_tmp, (R));                                       \
+   } while (0)
+   RESIDUE(r);
+   double beta = l2(r, n);
+   S->iterations = 0;
+   set_residue(S, beta / normb);
+   while (check_next(S)) {
+      int o_steps = m;
+      for (int32_t t = 0; t < n; t++) z[t] = r[t];
+      for (int32_t t = 0; t < (m + 1) * m; t++) H[t] = 0.0;
+      for (int32_t t = 0; t <= m; t++) s[t] = 0.0;
+      for (int32_t t = 0; t < L * L; t++) T[t] = 0.0;
+      for (int i = 0; i <= m && next_iteration(S); i++) {
+         double* yi = Y + (size_t)i * n;
+         /* hauseholder_generate: y_i = z truncated above row i, reflected */
+         for (int32_t j = 0; j < n; j++) yi[j] = j < i ? 0.0 : z[j];
+         const double normz = l2(yi, n);
+         const double y_ii = yi[i];
+         yi[i] = y_ii > 0.0 ? y_ii + normz : y_ii - normz;
+         const double norm_yi_squared = 2 * (normz * normz + fabs(y_ii) * normz);
+         const double t_i = 2.0 / norm_yi_squared;
+         T[i + i * L] = t_i;
+         if (i > 0) {
+            for (int k = 0; k < i; k++) aux[k] = dot(Y + (size_t)k * n, yi, n);
+            for (int k = 0; k < i; k++) {
+               T[k + i * L] = 0.0;
+               for (int j = k; j < i; j++) T[k + i * L] -= T[k + j * L] * (t_i * aux[j]);
+            }
+         }
+         /* hauseholder_apply_trunc: out = z[0..i] - y_i[0..i] (t_i (y_i, z) = 1) */
+         double* YLi = YL + (size_t)i * L;
+         for (int k = 0; k < L; k++) YLi[k] = yi[k];
+         double* out = i == 0 ? s : H + (size_t)(i - 1) * (m + 1);
+         for (int k = 0; k <= i; k++) out[k] = z[k] - YLi[k] * 1.0;
+         /* hauseholder_cwy: v = e_i - Y_i T_i Y_i^T e_i */
+         for (int k = 0; k <= i; k++) aux[k] = YL[i + k * L];
+         for (int k = 0; k <= i; k++) {
+            double a2 = 0.0;
+            for (int j = k; j <= i; j++) a2 += T[k + j * L] * aux[j];
+            aux[k] = a2;
+         }
+         for (int32_t t = 0; t < n; t++) {
+            double acc = 0;
+            for (int k = 0; k <= i; k++) acc += Y[(size_t)k * n + t] * aux[k];
+            v[t] = -1.0 * acc;
+         }
+         v[i] = 1.0 + v[i];
+         if (i < m) {
+            /* w = M^-1 A v_i; z = (I - Y_i T_i^T Y_i^T) w */
+            csr_mv(&A, v, M_tmp);
+            prec_apply(&P, M_tmp, w);
+            for (int k = 0; k <= i; k++) aux[k] = dot(Y + (size_t)k * n, w, n);
+            for (int k = i; k >= 0; k--) {
+               double a2 = 0.0;
+               for (int j = 0; j <= k; j++) a2 += T[j + k * L] * aux[j];
+               aux[k] = a2;
+            }
+            for (int32_t t = 0; t < n; t++) {
+               double acc = 0;
+               for (int k = 0; k <= i; k++) acc += Y[(size_t)k * n + t] * aux[k];
+               z[t] = -1.0 * acc + w[t];
+            }
+         }
+         if (i > 0) givens_column(i - 1, m, H, s, cs, sn);
+         set_residue(S, fabs(s[i]) / normb);
+         if (i > 0 && !check_next(S)) {
+            o_steps = i - 1;
+            break;
+         }
+      }
+      const int k_upd = (o_steps < m) ? o_steps : m - 1;
+      /* update(k, m, H, s, V, x), CWY branch */
+      for (int i = 0; i <= m; i++) y[i] = s[i];
+      for (int i = k_upd; i >= 0; i--) {
+         if (H[i + i * (m + 1)] == 0) {
+            ok = -1;
+            goto done;
+         }
+         y[i] /= H[i + i * (m + 1)];
+         for (int j = i - 1; j >= 0; j--) y[j] -= H[j + i * (m + 1)] * y[i];
+      }
+      for (int j = 0; j <= k_upd; j++) aux[j] = 0;
+      for (int j = 0; j <= k_upd; j++)
+         for (int i = 0; i <= j; i++) aux[i] += y[j] * YL[j + i * L];
+      for (int i = 0; i <= k_upd; i++) {
+         double a2 = 0.0;
+         for (int j = i; j <= k_upd; j++) a2 += T[i + j * L] * aux[j];
+         aux[i] = a2;
+      }
+      for (int32_t t = 0; t < n; t++) {
+         double acc = 0;
+         for (int k = 0; k <= k_upd; k++) acc += Y[(size_t)k * n + t] * aux[k];
+         x[t] = -1.0 * acc + x[t];
+      }
+      for (int j = 0; j <= k_upd; j++) x[j] = x[j] + y[j];  /* x += sum_j y_j e_j */
+      if (o_steps < m) {
+         ok = check_convergence(S);
+         goto done;
+      }
+      RESIDUE(r);
+      beta = l2(r, n);
+      set_residue(S, beta / normb);
+   }
+#undef RESIDUE
+   ok = check_convergence(S);
+done:
+   free(r);
+   free(w);
+   free(z);
+   free(v);
+   free(M_tmp);
+   free(Y);
+   free(YL);
+   free(T);
+   free(H);
+   free(s);
+   free(cs);
+   free(sn);
+   free(y);
+   free(aux);
+   prec_free(&P);
+   return ok;
+}
+
 /* FGMRES: the GMRES below with right, flexible preconditioning -- no
  * counterpart in the reference; z_i = M^-1 v_i is kept, w = A z_i, x += Z y,
  * residues unpreconditioned (normb = ||b||).  Derived from GMRES::solve with the MGS / MGSR orthogonalisation

@@ -101,8 +101,8 @@ def test_solver_matches_oracle(oracle, kind, precond, pname):
     assert ok == o["converged"]
     # rounding-level differences in the dot products move ill-conditioned,
     # unpreconditioned solves by a few iterations (so does the reference
-    # between OpenMP thread counts)
-    assert abs(it - o["iterations"]) <= max(2, o["iterations"] // 100), (it, o["iterations"])
+    # between OpenMP thread counts): 2 %
+    assert abs(it - o["iterations"]) <= max(2, o["iterations"] // 50), (it, o["iterations"])
     assert res < 1e-8
     assert tr < 1e-6
     assert np.max(np.abs(x - o["x"])) <= 1e-5 * max(1.0, np.max(np.abs(o["x"])))
@@ -274,3 +274,41 @@ def test_fgmres_fsai2_mixed_precision():
     xs = torch.zeros(A.n, dtype=torch.float64, device="cuda")
     r = t.solve_mixed(M, bs, xs, tol=1e-8, inner_tol=1e-4, inner="fsai2", solver="fgmres", gmres_restart=30)
     assert r["converged"] and t.true_residual(M, bs, xs) < 1e-8
+
+
+@pytest.mark.parametrize("precond", [0, 1, 2])
+@pytest.mark.parametrize("pname", ["laplacian48", "diffusion40"])
+def test_gmres_cwy_matches_oracle(oracle, pname, precond):
+    """GMRES with Householder (CWY) orthogonalisation against the oracle's
+    restatement of orthogonalize_CWY (pinned to the reference's own solves)."""
+    from tnl_b200 import generators as g
+
+    A = problems()[pname]
+    b = g.uniform_vector(A.n, 1)
+    o = oracle.solve("gmres_cwy", A, b, precond=precond, tol=1e-8, maxit=20000, gmres_m=30)
+    ok, it, res, x, tr = gpu_solve("gmres", A, b, precond, variant="CWY")
+    assert ok == o["converged"]
+    assert abs(it - o["iterations"]) <= max(2, o["iterations"] // 50), (it, o["iterations"])
+    assert res < 1e-8 and tr < 1e-7
+    assert np.allclose(x, o["x"], rtol=1e-5, atol=1e-6 * np.abs(o["x"]).max())
+
+
+def test_gmres_cwy_matches_reference_golden(golden):
+    """The reference's own CWY solves (fixtures made by tests/golden/make_golden.py)."""
+    for pname in ("laplacian32", "diffusion32"):
+        class A:
+            pass
+
+        A.rowptr = golden.get(f"prob/{pname}/rowptr")
+        A.cols = golden.get(f"prob/{pname}/cols")
+        A.vals = golden.get(f"prob/{pname}/vals")
+        A.n = len(A.rowptr) - 1
+        b = golden.get(f"prob/{pname}/b")
+        for pre in (1, 2):
+            key = f"{pname}/gmres_cwy/{pre}"
+            ref = golden.meta["solvers"][key]
+            ok, it, res, x, tr = gpu_solve("gmres", A, b, pre, variant="CWY")
+            assert ok == ref["converged"], key
+            assert abs(it - ref["iterations"]) <= 2, (key, it, ref["iterations"])
+            xr = golden.get(f"solve/{key}/x")
+            assert np.allclose(x, xr, rtol=1e-5, atol=1e-6 * np.abs(xr).max()), key

@@ -1,0 +1,220 @@
+"""SpMV and linear-solver benchmarks: the counterparts of the reference's
+tnl-benchmark-spmv (Benchmarks/SpMV/spmv.h) and
+tnl-benchmark-linear-solvers (Benchmarks/LinearSolvers/tnl-benchmark-linear-solvers.h),
+on seeded synthetic matrices.  One JSON object per line on stdout.
+
+    python -m tnl_b200.benchmarks spmv    [--configs laplacian,power_law] [--reals f64,f32] [--steps K]
+    python -m tnl_b200.benchmarks solvers [--problem laplacian|diffusion] [--N 1024]
+
+spmv: every segment format and kernel on the 1024^2 5-point Laplacian
+(n = 1,048,576) and the power-law matrix (n = 4,194,304, Zipf 1.73 row
+lengths, cap 4096, seed 2).  GB/s counts algorithmic bytes, the same for
+every format: nnz*(R+4) + (n+1)*4 + n*R (x) + n*R (y); padding therefore
+lowers the figure.  Device time per product from CUDA events: over K
+back-to-back products when the inputs exceed L2 (the power-law matrix), else
+(the Laplacian's 84 MB) each product timed alone after a 256 MB write that
+flushes the 126 MB L2.
+
+solvers: time to an FP64 true residual ||b - A x|| / ||b|| <= 1e-8 (CUDA
+events around the solve call; preconditioner set-up timed separately) for
+FP64 Jacobi-PCG, FP64 FSAI-PCG, FP32-inner refinement with FSAI, and the
+learned FSAI with FP32-inner refinement (weights from a training run on
+smaller seeded diffusion problems, or trained on the spot).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+import torch
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def spmv_bytes(n: int, ncols: int, nnz: int, real_bytes: int) -> int:
+    return nnz * (real_bytes + 4) + (n + 1) * 4 + ncols * real_bytes + n * real_bytes
+
+
+def hbm_peak() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def _matrix(config: str):
+    from . import generators as g
+
+    if config == "laplacian":
+        return g.laplacian_2d(1024)
+    if config == "power_law":
+        return g.power_law(4_194_304, 1.73, 4096, 2)
+    raise ValueError(config)
+
+
+# (label, segments class name, launch mapping, threads per segment)
+SPMV_VARIANTS = [
+    ("CSR tile", "CSR", "Default", 0),
+    ("CSR Light", "CSR", "Light", 0),
+    ("CSR Scalar", "CSR", "Scalar", 0),
+    ("CSR Vector", "CSR", "Vector", 32),
+    ("AdaptiveCSR", "AdaptiveCSR", "Adaptive", 0),
+    ("Ellpack", "Ellpack", "Default", 0),
+    ("SlicedEllpack", "SlicedEllpack", "Default", 0),
+    ("ChunkedEllpack", "ChunkedEllpack", "Default", 0),
+    ("BiEllpack", "BiEllpack", "Default", 0),
+]
+
+
+def time_spmv(M, x, y, lc, steps: int, flush: bool) -> float:
+    """Mean device milliseconds per product.  Without `flush`, over `steps`
+    back-to-back calls; with it, each call timed alone after writing a
+    256 MB buffer, so that nothing of the matrix is left in the 126 MB L2."""
+    for _ in range(3):
+        M.vectorProduct(x, y, launchConfig=lc, synchronize=False)
+    torch.cuda.synchronize()
+    if not flush:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            M.vectorProduct(x, y, launchConfig=lc, synchronize=False)
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+    scrub = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for a, b in ev:
+        scrub.fill_(1)
+        a.record()
+        M.vectorProduct(x, y, launchConfig=lc, synchronize=False)
+        b.record()
+    torch.cuda.synchronize()
+    return float(np.mean([a.elapsed_time(b) for a, b in ev]))
+
+
+def bench_spmv(configs, reals, steps: int, out=sys.stdout):
+    import tnl_b200 as t
+    from . import generators as g
+
+    peak, peak_kind = hbm_peak()
+    for config in configs:
+        A = _matrix(config)
+        xh = g.uniform_vector(A.ncols, 0)
+        for real in reals:
+            dt = torch.float64 if real == "f64" else torch.float32
+            R = 8 if real == "f64" else 4
+            nbytes = spmv_bytes(A.n, A.ncols, A.nnz, R)
+            x = torch.tensor(xh, dtype=dt, device="cuda")
+            y = torch.empty(A.n, dtype=dt, device="cuda")
+            for label, seg, mapping, tps in SPMV_VARIANTS:
+                rec = {"bench": "spmv", "config": config, "rows": A.n, "nnz": A.nnz, "real": real, "format": label}
+                try:
+                    M = t.SparseMatrix(getattr(t, seg), dt).assign(A.rowptr, A.cols, A.vals)
+                except OverflowError as e:  # Ellpack of the power-law matrix: 4096 x 4.19M > 2^31
+                    rec["error"] = f"overflow_error: {e}"
+                    print(json.dumps(rec), file=out, flush=True)
+                    continue
+                flush = nbytes < 512e6
+                ms = time_spmv(M, x, y, t.LaunchConfiguration(mapping, tps), steps, flush)
+                gbs = nbytes / (ms / 1e3) / 1e9
+                rec.update({"ms": ms, "GB/s": gbs, "frac_of_hbm": gbs / peak, "hbm_peak": f"{peak} ({peak_kind})",
+                            "storage": M.segments.getStorageSize(), "padding": M.segments.getStorageSize() / A.nnz,
+                            "l2": "flushed before each product" if flush else "inputs larger than L2"})
+                print(json.dumps(rec), file=out, flush=True)
+                del M
+                torch.cuda.empty_cache()
+
+
+def _timed(fn):
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    r = fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return r, e0.elapsed_time(e1)
+
+
+def bench_solvers(problem: str, N: int, weights: str | None, out=sys.stdout):
+    import tnl_b200 as t
+    from . import generators as g
+    from .lfsai import LearnedFSAI, diffusion_problem
+
+    if problem == "laplacian":
+        A = g.laplacian_2d(N)
+        M = t.SparseMatrix.from_csr(A)
+    else:
+        M = diffusion_problem(N, 1234)
+    n = M.getRows()
+    b = torch.tensor(g.uniform_vector(n, 1), device="cuda")
+    base = {"bench": "solver", "problem": problem, "N": N, "rows": n, "nnz": int(M.getValues().numel()),
+            "tol": 1e-8}
+
+    def pcg(P, name, setup_ms):
+        S = t.CG()
+        S.setMatrix(M)
+        S.setPreconditioner(P)
+        S.setConvergenceResidue(1e-8)
+        S.setMaxIterations(200000)
+        x = torch.zeros(n, dtype=torch.float64, device="cuda")
+        ok, ms = _timed(lambda: S.solve(b, x))
+        rec = dict(base, method=name, converged=bool(ok), iterations=S.getIterations(), solve_ms=ms,
+                   setup_ms=setup_ms, true_residual=t.true_residual(M, b, x))
+        print(json.dumps(rec), file=out, flush=True)
+        return rec
+
+    P = t.Diagonal()
+    _, s = _timed(lambda: P.update(M))
+    jac = pcg(P, "FP64 Jacobi-PCG", s)
+    P = t.FSAI()
+    _, s = _timed(lambda: P.update(M))
+    pcg(P, "FP64 FSAI-PCG", s)
+
+    A32 = t.SparseMatrix(t.CSR, torch.float32)
+    A32.assign(M.segments.getOffsets(), M.getColumnIndexes().cpu().numpy(), M.getValues().cpu().numpy())
+
+    def mixed(name, inner, setup_ms):
+        x = torch.zeros(n, dtype=torch.float64, device="cuda")
+        r, ms = _timed(lambda: t.solve_mixed(M, b, x, tol=1e-8, inner_tol=1e-4, inner=inner))
+        rec = dict(base, method=name, converged=r["converged"], iterations=r["inner_iterations"],
+                   outer_iterations=r["outer_iterations"], solve_ms=ms, setup_ms=setup_ms,
+                   true_residual=t.true_residual(M, b, x), speedup_vs_fp64_jacobi=jac["solve_ms"] / ms)
+        print(json.dumps(rec), file=out, flush=True)
+
+    mixed("FP32-inner IR, FSAI", "fsai", 0.0)
+    net = LearnedFSAI(seed=2)
+    if weights and Path(weights).exists():
+        net.load(weights)
+    else:
+        train = [diffusion_problem(128, s) for s in range(8)]
+        net.fit_classical(train, steps=400, lr=3e-3)
+        net.train(train, steps=400, nprobes=8, lr=5e-4)
+    P32, s = _timed(lambda: net.preconditioner(A32))
+    mixed("FP32-inner IR, learned FSAI", P32, s)
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(prog="python -m tnl_b200.benchmarks")
+    sub = ap.add_subparsers(dest="cmd", required=True)
+    a = sub.add_parser("spmv")
+    a.add_argument("--configs", default="laplacian,power_law")
+    a.add_argument("--reals", default="f64,f32")
+    a.add_argument("--steps", type=int, default=50)
+    b = sub.add_parser("solvers")
+    b.add_argument("--problem", default="laplacian", choices=["laplacian", "diffusion"])
+    b.add_argument("--N", type=int, default=1024)
+    b.add_argument("--weights", default=str(Path(__file__).resolve().parent / "weights" / "lfsai_diffusion.npy"))
+    args = ap.parse_args(argv)
+    if args.cmd == "spmv":
+        bench_spmv(args.configs.split(","), args.reals.split(","), args.steps)
+    else:
+        bench_solvers(args.problem, args.N, args.weights)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -166,32 +166,32 @@ namespace tnlb {
 __device__ __forceinline__ double ld_stream(const double* p)
 {
    double v;
-   asm volatile("ld.global.nc.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(p));
+   asm("ld.global.nc.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(p));
    return v;
 }
 __device__ __forceinline__ float ld_stream(const float* p)
 {
    float v;
-   asm volatile("ld.global.nc.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
+   asm("ld.global.nc.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
    return v;
 }
 __device__ __forceinline__ int32_t ld_stream(const int32_t* p)
 {
    int32_t v;
-   asm volatile("ld.global.nc.L1::no_allocate.s32 %0, [%1];" : "=r"(v) : "l"(p));
+   asm("ld.global.nc.L1::no_allocate.s32 %0, [%1];" : "=r"(v) : "l"(p));
    return v;
 }
 // 128-bit streaming loads (address must be 16-byte aligned).
 __device__ __forceinline__ double2 ld_stream_v2(const double* p)
 {
    double2 v;
-   asm volatile("ld.global.nc.L1::no_allocate.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "l"(p));
+   asm("ld.global.nc.L1::no_allocate.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "l"(p));
    return v;
 }
 __device__ __forceinline__ float4 ld_stream_v4(const float* p)
 {
    float4 v;
-   asm volatile("ld.global.nc.L1::no_allocate.v4.f32 {%0, %1, %2, %3}, [%4];"
+   asm("ld.global.nc.L1::no_allocate.v4.f32 {%0, %1, %2, %3}, [%4];"
                 : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
                 : "l"(p));
    return v;
@@ -199,7 +199,7 @@ __device__ __forceinline__ float4 ld_stream_v4(const float* p)
 __device__ __forceinline__ int4 ld_stream_v4(const int32_t* p)
 {
    int4 v;
-   asm volatile("ld.global.nc.L1::no_allocate.v4.s32 {%0, %1, %2, %3}, [%4];"
+   asm("ld.global.nc.L1::no_allocate.v4.s32 {%0, %1, %2, %3}, [%4];"
                 : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
                 : "l"(p));
    return v;

@@ -338,15 +338,16 @@ __global__ void k_init_params(uint64_t seed, float* __restrict__ theta)
    const int q = blockIdx.x * blockDim.x + threadIdx.x;
    if (q >= kLfParams) return;
    // layer of parameter q: U(-a, a), a = sqrt(6/(fan_in+fan_out)), W4 x 0.1, biases 0
-   float a = 0.f;
+   // in FP64 (correctly rounded sqrt), as the host initialiser, then rounded once to FP32
+   double a = 0.0;
    if (q < kLfB1)
-      a = sqrtf(6.f / (kLfF + kLfH));
+      a = sqrt(6.0 / (kLfF + kLfH));
    else if (q >= kLfW2 && q < kLfB2)
-      a = sqrtf(6.f / (kLfH + kLfH));
+      a = sqrt(6.0 / (kLfH + kLfH));
    else if (q >= kLfW3 && q < kLfB3)
-      a = sqrtf(6.f / (kLfH + kLfH));
+      a = sqrt(6.0 / (kLfH + kLfH));
    else if (q >= kLfW4 && q < kLfB4)
-      a = 0.1f * sqrtf(6.f / (kLfH + kLfK));
+      a = sqrt(6.0 / (kLfH + kLfK)) * 0.1;
    uint64_t z = seed * 0x9E3779B97F4A7C15ull + (uint64_t)q;
    z += 0x9E3779B97F4A7C15ull;
    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;

@@ -446,6 +446,42 @@ __global__ void k_gmres_update(int64_t n, int64_t ld, int cols, const Real* __re
    }
 }
 
+// out = alpha * Y c + beta * in (in == nullptr: beta term absent), then
+// out[unit_row] = 1 + out[unit_row] when unit_row >= 0 -- the gemv of
+// MatrixOperations::gemv (Matrices/MatrixOperations.h) as the CWY steps use
+// it; c has `cols` <= 128 entries on the device, alpha applied to c first.
+template <typename Real>
+__global__ void k_gemv_cols(int64_t n, int64_t ld, int cols, const Real* __restrict__ Y, const double* __restrict__ c,
+                            double alpha, const Real* in, double beta, Real* out, int64_t unit_row)
+{
+   __shared__ double sc[128];
+   if (threadIdx.x < cols && threadIdx.x < 128) sc[threadIdx.x] = alpha * c[threadIdx.x];
+   __syncthreads();
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+      double acc = 0;
+      for (int k = 0; k < cols; k++) acc += (double)Y[(int64_t)k * ld + i] * sc[k];
+      Real v = in ? (Real)(acc + beta * (double)in[i]) : (Real)acc;
+      if (i == unit_row) v = (Real)1 + v;
+      out[i] = v;
+   }
+}
+
+// y_i = z with the entries above row i set to zero (hauseholder_generate)
+template <typename Real>
+__global__ void k_truncate(int64_t n, int64_t i0, const Real* __restrict__ z, Real* __restrict__ y)
+{
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+      y[i] = i < i0 ? Real(0) : z[i];
+}
+
+// x[j] = x[j] + y[j] for j < k (the CWY update's x += sum_j y_j e_j)
+template <typename Real>
+__global__ void k_add_head(int k, const double* __restrict__ y, Real* __restrict__ x)
+{
+   const int j = threadIdx.x;
+   if (j < k) x[j] = x[j] + (Real)y[j];
+}
+
 }  // namespace
 
 // ------------------------------------------------------------------ host
@@ -840,6 +876,256 @@ tnlb_status bicgstab_solve(const Ctx<Real>& c, const Precond<Real>& P, const tnl
 
 // --------------------------------------------------------------- GMRES
 
+// Givens rotations on column i of H (leading dimension m + 1) and on s
+// (GMRES::apply_givens_rotations, GMRES.hpp:731-770).
+void givens_column(int i, int m, double* H, double* s, double* cs, double* sn)
+{
+   auto rot = [](double& dx, double& dy, double csv, double snv) {
+      const double t = csv * dx + snv * dy;
+      dy = csv * dy - snv * dx;
+      dx = t;
+   };
+   for (int k = 0; k < i; k++) rot(H[k + i * (m + 1)], H[k + 1 + i * (m + 1)], cs[k], sn[k]);
+   if (H[i + 1 + i * (m + 1)] != 0.0) {
+      const double dx = H[i + i * (m + 1)], dy = H[i + 1 + i * (m + 1)];
+      if (dy == 0.0) {
+         cs[i] = 1.0;
+         sn[i] = 0.0;
+      }
+      else if (std::fabs(dy) > std::fabs(dx)) {
+         const double t = dx / dy;
+         sn[i] = 1.0 / std::sqrt(1.0 + t * t);
+         cs[i] = t * sn[i];
+      }
+      else {
+         const double t = dy / dx;
+         cs[i] = 1.0 / std::sqrt(1.0 + t * t);
+         sn[i] = t * cs[i];
+      }
+      rot(H[i + i * (m + 1)], H[i + 1 + i * (m + 1)], cs[i], sn[i]);
+      rot(s[i], s[i + 1], cs[i], sn[i]);
+   }
+}
+
+// GMRES with the CWY orthogonalisation (GMRES.hpp:350-423): Householder
+// reflections P_i = I - t_i y_i y_i^T kept in compact WY form I - Y T Y^T.
+// Y (n x (m_max+1), column-major, zero above the diagonal) stays on the
+// device; T, H, s and the upper (m_max+1) x (m_max+1) block of Y (YL) are
+// small and live on the host, as in the reference.  The basis vectors are
+// not stored: v_i = (I - Y T Y^T) e_i is rebuilt (hauseholder_cwy :572-604),
+// and the update adds sum_j y_j v_j the same way (:685-725).  Each cycle
+// counts m+1 iterations (i = 0..m) and makes m products.
+template <typename Real>
+tnlb_status gmres_cwy_solve(const Ctx<Real>& c, const Precond<Real>& P, const tnlb_solver_params& prm, const Real* b,
+                            Real* x, tnlb_solve_result* res)
+{
+   const int64_t n = c.n;
+   const int rmin = prm.gmres_restarting_min, rmax = prm.gmres_restarting_max;
+   const int dmin = prm.gmres_restarting_step_min, dmax = prm.gmres_restarting_step_max;
+   const int L = rmax + 1;
+   TNLB_REQUIRE(n >= L, TNLB_ERR_INVALID_ARGUMENT,
+                "GMRES CWY needs at least restarting_max + 1 rows (the reference copies that many entries of Y)");
+   const int64_t ld = (n + 31) / 32 * 32;
+   Work W;
+   TNLB_TRY_STATUS(W.alloc());
+   DeviceBuffer Yb, z, w, v, r, M_tmp, hdev, cdev, ydev;
+   TNLB_TRY_STATUS(Yb.alloc(sizeof(Real) * ld * L));
+   TNLB_TRY_STATUS(z.alloc(sizeof(Real) * n));
+   TNLB_TRY_STATUS(w.alloc(sizeof(Real) * n));
+   TNLB_TRY_STATUS(v.alloc(sizeof(Real) * n));
+   TNLB_TRY_STATUS(r.alloc(sizeof(Real) * n));
+   TNLB_TRY_STATUS(M_tmp.alloc(sizeof(Real) * n));
+   TNLB_TRY_STATUS(hdev.alloc(sizeof(double) * 128));
+   TNLB_TRY_STATUS(cdev.alloc(sizeof(double) * 128));
+   TNLB_TRY_STATUS(ydev.alloc(sizeof(double) * 128));
+   Real* Y = Yb.as<Real>();
+   double* sc = W.scratch.as<double>();
+   const unsigned G = vec_grid(n);
+   const bool pre = P.kind != TNLB_PRECOND_NONE;
+   double hs[2];
+   auto norm = [&](const Real* a, double* out) -> tnlb_status {
+      k_dots<Real><<<G, kRedThreads, 0, c.st>>>(n, a, a, nullptr, nullptr, W.red(), sc);
+      TNLB_CHECK_LAUNCH();
+      TNLB_CUDA_TRY(cudaMemcpyAsync(hs, sc, sizeof(hs), cudaMemcpyDeviceToHost, c.st));
+      TNLB_CUDA_TRY(cudaStreamSynchronize(c.st));
+      *out = std::sqrt(hs[0]);
+      return TNLB_OK;
+   };
+   auto compute_residue = [&]() -> tnlb_status {
+      Real* tgt = pre ? M_tmp.as<Real>() : r.as<Real>();
+      TNLB_CUDA_TRY(cudaMemcpyAsync(tgt, b, sizeof(Real) * n, cudaMemcpyDeviceToDevice, c.st));
+      TNLB_TRY_STATUS(c.spmv(x, tgt, -1.0, 1.0));
+      if (pre) TNLB_TRY_STATUS(P.apply(n, M_tmp.as<Real>(), r.as<Real>(), c.st));
+      return TNLB_OK;
+   };
+   // Y_cols^T a -> host (Reduction2D in the reference)
+   std::vector<double> aux(L + 1);
+   auto ytv = [&](int cols, const Real* a) -> tnlb_status {
+      k_gmres_vtw<Real><<<G, kRedThreads, 0, c.st>>>(n, ld, cols, Y, a, W.partials.as<double>(),
+                                                    W.counter.as<unsigned>() + 1, hdev.as<double>());
+      TNLB_CHECK_LAUNCH();
+      TNLB_CUDA_TRY(cudaMemcpyAsync(aux.data(), hdev.ptr, sizeof(double) * cols, cudaMemcpyDeviceToHost, c.st));
+      return TNLB_OK;
+   };
+   // out = alpha * Y_cols aux + beta * in (+ e_unit)
+   auto gemv = [&](int cols, double alpha, const Real* in, double beta, Real* out, int64_t unit) -> tnlb_status {
+      TNLB_CUDA_TRY(cudaMemcpyAsync(cdev.ptr, aux.data(), sizeof(double) * cols, cudaMemcpyHostToDevice, c.st));
+      k_gemv_cols<Real><<<G, kRedThreads, 0, c.st>>>(n, ld, cols, Y, cdev.as<double>(), alpha, in, beta, out, unit);
+      TNLB_CHECK_LAUNCH();
+      return TNLB_OK;
+   };
+   int it = 0;
+   double residue = 0;
+   auto check = [&]() {
+      return !(std::isnan(residue) || it > prm.max_iterations ||
+               (residue > prm.divergence_residue && it >= prm.min_iterations) ||
+               (residue < prm.convergence_residue && it >= prm.min_iterations));
+   };
+   double normb;
+   if (pre) {
+      TNLB_TRY_STATUS(P.apply(n, b, M_tmp.as<Real>(), c.st));
+      TNLB_TRY_STATUS(norm(M_tmp.as<Real>(), &normb));
+   }
+   else
+      TNLB_TRY_STATUS(norm(b, &normb));
+   if (normb == 0) {
+      TNLB_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(Real) * n, c.st));
+      TNLB_CUDA_TRY(cudaStreamSynchronize(c.st));
+      *res = tnlb_solve_result{1, 0, 0.0, 0, 0};
+      return TNLB_OK;
+   }
+   TNLB_TRY_STATUS(compute_residue());
+   double beta;
+   TNLB_TRY_STATUS(norm(r.as<Real>(), &beta));
+   residue = beta / normb;
+   std::vector<double> H((size_t)(rmax + 1) * rmax), s(L + 1), cs(L + 1), sn(L + 1), y(L + 1), YL((size_t)L * L),
+      T((size_t)L * L);
+   std::vector<Real> zh(L), yl(L);
+   double beta_ratio = 1;
+   const double max_beta_ratio = 0.99, min_beta_ratio = 0.175;
+   int restart_cycles = 0;
+   int m = rmax;
+   while (check()) {
+      if (rmax > rmin && restart_cycles > 0) {
+         if (beta_ratio > max_beta_ratio)
+            m = rmax;
+         else if (beta_ratio >= min_beta_ratio) {
+            const int step = dmin + (dmax - dmin) / static_cast<float>(rmax - rmin) * (m - rmin);
+            if (m - step >= rmin)
+               m -= step;
+            else
+               m = rmax;
+         }
+      }
+      int o_steps = m;
+      TNLB_CUDA_TRY(cudaMemcpyAsync(z.ptr, r.ptr, sizeof(Real) * n, cudaMemcpyDeviceToDevice, c.st));
+      std::fill(H.begin(), H.end(), 0.0);
+      std::fill(s.begin(), s.end(), 0.0);
+      std::fill(T.begin(), T.end(), 0.0);
+      for (int i = 0; i <= m; i++) {
+         const bool cont = check();
+         it++;
+         if (!cont) break;
+         Real* yi = Y + (int64_t)i * ld;
+         // hauseholder_generate (GMRES.hpp:468-537)
+         k_truncate<Real><<<G, kRedThreads, 0, c.st>>>(n, i, z.as<Real>(), yi);
+         TNLB_CHECK_LAUNCH();
+         double normz;
+         TNLB_TRY_STATUS(norm(yi, &normz));
+         TNLB_CUDA_TRY(cudaMemcpyAsync(zh.data(), z.ptr, sizeof(Real) * (i + 1), cudaMemcpyDeviceToHost, c.st));
+         TNLB_CUDA_TRY(cudaStreamSynchronize(c.st));
+         const double y_ii = (double)zh[i];
+         const Real yii_new = (Real)(y_ii > 0.0 ? y_ii + normz : y_ii - normz);
+         TNLB_CUDA_TRY(cudaMemcpyAsync(yi + i, &yii_new, sizeof(Real), cudaMemcpyHostToDevice, c.st));
+         const double norm_yi_squared = 2 * (normz * normz + std::fabs(y_ii) * normz);
+         const double t_i = 2.0 / norm_yi_squared;
+         T[i + (size_t)i * L] = t_i;
+         if (i > 0) TNLB_TRY_STATUS(ytv(i, yi));
+         // the upper block of Y, copied to the host (hauseholder_apply_trunc)
+         TNLB_CUDA_TRY(cudaMemcpyAsync(yl.data(), yi, sizeof(Real) * L, cudaMemcpyDeviceToHost, c.st));
+         TNLB_CUDA_TRY(cudaStreamSynchronize(c.st));
+         if (i > 0)
+            for (int k = 0; k < i; k++) {
+               double tk = 0.0;
+               for (int j = k; j < i; j++) tk -= T[k + (size_t)j * L] * (t_i * aux[j]);
+               T[k + (size_t)i * L] = tk;
+            }
+         for (int k = 0; k < L; k++) YL[(size_t)i * L + k] = (double)yl[k];
+         // s = e_1^T P_0 z (i = 0) or H_{i-1} = P_i z: z[0..i] - y_i[0..i]
+         double* out = i == 0 ? s.data() : H.data() + (size_t)(i - 1) * (m + 1);
+         for (int k = 0; k <= i; k++) out[k] = (double)zh[k] - YL[(size_t)i * L + k] * 1.0;
+         // v_i = (I - Y_i T_i Y_i^T) e_i (hauseholder_cwy)
+         for (int k = 0; k <= i; k++) aux[k] = YL[i + (size_t)k * L];
+         for (int k = 0; k <= i; k++) {
+            double a2 = 0.0;
+            for (int j = k; j <= i; j++) a2 += T[k + (size_t)j * L] * aux[j];
+            aux[k] = a2;
+         }
+         TNLB_TRY_STATUS(gemv(i + 1, -1.0, nullptr, 0.0, v.as<Real>(), i));
+         if (i < m) {
+            // w = M^-1 A v_i; z = (I - Y_i T_i^T Y_i^T) w (hauseholder_cwy_transposed)
+            if (pre) {
+               TNLB_TRY_STATUS(c.spmv(v.as<Real>(), M_tmp.as<Real>()));
+               TNLB_TRY_STATUS(P.apply(n, M_tmp.as<Real>(), w.as<Real>(), c.st));
+            }
+            else
+               TNLB_TRY_STATUS(c.spmv(v.as<Real>(), w.as<Real>()));
+            TNLB_TRY_STATUS(ytv(i + 1, w.as<Real>()));
+            TNLB_CUDA_TRY(cudaStreamSynchronize(c.st));
+            for (int k = i; k >= 0; k--) {
+               double a2 = 0.0;
+               for (int j = 0; j <= k; j++) a2 += T[j + (size_t)k * L] * aux[j];
+               aux[k] = a2;
+            }
+            TNLB_TRY_STATUS(gemv(i + 1, -1.0, w.as<Real>(), 1.0, z.as<Real>(), -1));
+         }
+         if (i > 0) givens_column(i - 1, m, H.data(), s.data(), cs.data(), sn.data());
+         residue = std::fabs(s[i]) / normb;
+         if (i > 0 && !check()) {
+            o_steps = i - 1;
+            break;
+         }
+      }
+      // update (GMRES.hpp:648-725, CWY branch)
+      const int k = o_steps < m ? o_steps : m - 1;
+      for (int q = 0; q <= m; q++) y[q] = s[q];
+      for (int q = k; q >= 0; q--) {
+         if (H[q + (size_t)q * (m + 1)] == 0) {
+            set_error("GMRES: zero diagonal element of the Hessenberg matrix (breakdown)");
+            return TNLB_ERR_BREAKDOWN;
+         }
+         y[q] /= H[q + (size_t)q * (m + 1)];
+         for (int j = q - 1; j >= 0; j--) y[j] -= H[j + (size_t)q * (m + 1)] * y[q];
+      }
+      for (int j = 0; j <= k; j++) aux[j] = 0;
+      for (int j = 0; j <= k; j++)
+         for (int q = 0; q <= j; q++) aux[q] += y[j] * YL[j + (size_t)q * L];
+      for (int q = 0; q <= k; q++) {
+         double a2 = 0.0;
+         for (int j = q; j <= k; j++) a2 += T[q + (size_t)j * L] * aux[j];
+         aux[q] = a2;
+      }
+      TNLB_TRY_STATUS(gemv(k + 1, -1.0, x, 1.0, x, -1));
+      TNLB_CUDA_TRY(cudaMemcpyAsync(ydev.ptr, y.data(), sizeof(double) * (k + 1), cudaMemcpyHostToDevice, c.st));
+      k_add_head<Real><<<1, 128, 0, c.st>>>(k + 1, ydev.as<double>(), x);
+      TNLB_CHECK_LAUNCH();
+      if (o_steps < m) break;
+      TNLB_TRY_STATUS(compute_residue());
+      const double beta_old = beta;
+      TNLB_TRY_STATUS(norm(r.as<Real>(), &beta));
+      residue = beta / normb;
+      ++restart_cycles;
+      beta_ratio = beta / beta_old;
+   }
+   TNLB_CUDA_TRY(cudaStreamSynchronize(c.st));
+   res->iterations = it;
+   res->residue = residue;
+   res->converged = check_convergence(residue, it, prm.max_iterations, prm.min_iterations, prm.convergence_residue,
+                                      prm.divergence_residue);
+   res->status_detail = 0;
+   return TNLB_OK;
+}
+
 template <typename Real>
 tnlb_status gmres_solve(const Ctx<Real>& c, const Precond<Real>& P, const tnlb_solver_params& prm, const Real* b,
                         Real* x, tnlb_solve_result* res, bool flexible = false)
@@ -855,9 +1141,13 @@ tnlb_status gmres_solve(const Ctx<Real>& c, const Precond<Real>& P, const tnlb_s
                 "Wrong value for the GMRES restarting adjustment parameters");
    TNLB_REQUIRE(rmax <= 64, TNLB_ERR_INVALID_ARGUMENT, "GMRES restarting parameter above 64 is not supported");
    const int variant = prm.gmres_variant;
-   TNLB_REQUIRE(variant == TNLB_GMRES_CGS || variant == TNLB_GMRES_CGSR || variant == TNLB_GMRES_MGS ||
-                   variant == TNLB_GMRES_MGSR,
-                TNLB_ERR_NOT_IMPLEMENTED, "GMRES variant CWY (Householder) is not implemented on the GPU");
+   TNLB_REQUIRE(variant >= TNLB_GMRES_CGS && variant <= TNLB_GMRES_CWY, TNLB_ERR_INVALID_ARGUMENT,
+                "unknown GMRES variant");
+   if (variant == TNLB_GMRES_CWY) {
+      TNLB_REQUIRE(!flexible, TNLB_ERR_NOT_IMPLEMENTED,
+                   "FGMRES keeps its preconditioned basis: use the CGS, CGSR, MGS or MGSR variant");
+      return gmres_cwy_solve<Real>(c, P, prm, b, x, res);
+   }
    const int m_max = rmax;
    const int64_t ld = (n + 31) / 32 * 32;  // 256-byte aligned columns in FP64
    Work W;

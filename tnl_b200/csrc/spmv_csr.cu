@@ -214,42 +214,48 @@ __device__ __forceinline__ uint64_t policy_evict_last()
 __device__ __forceinline__ int32_t ld_stream_hint(const int32_t* a, uint64_t pol)
 {
    int32_t v;
-   asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.s32 %0, [%1], %2;" : "=r"(v) : "l"(a), "l"(pol));
+   asm("ld.global.nc.L1::no_allocate.L2::cache_hint.s32 %0, [%1], %2;" : "=r"(v) : "l"(a), "l"(pol));
    return v;
 }
 __device__ __forceinline__ double ld_stream_hint(const double* a, uint64_t pol)
 {
    double v;
-   asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(a), "l"(pol));
+   asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(a), "l"(pol));
    return v;
 }
 __device__ __forceinline__ float ld_stream_hint(const float* a, uint64_t pol)
 {
    float v;
-   asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(a), "l"(pol));
+   asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(a), "l"(pol));
    return v;
 }
 __device__ __forceinline__ double ld_keep(const double* a, uint64_t pol)
 {
    double v;
-   asm volatile("ld.global.nc.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(a), "l"(pol));
+   asm("ld.global.nc.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(a), "l"(pol));
    return v;
 }
 __device__ __forceinline__ float ld_keep(const float* a, uint64_t pol)
 {
    float v;
-   asm volatile("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(a), "l"(pol));
+   asm("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(a), "l"(pol));
    return v;
 }
 
-// Merge-path tile: at most kTileSize rows + nonzeros.  Each warp takes an
-// equal share of the tile's nonzeros, 32 consecutive ones per step: all
-// column/value loads and x gathers of its steps are issued before any is
-// used; the row of a nonzero is found by binary search in the staged row
-// ends; per step a warp-shuffle segmented scan sums each row's products, and
-// a running carry joins a row across steps.  Rows complete inside one warp
-// are stored to shared memory directly; the (at most two) rows a warp shares
-// with its neighbours are combined in warp order by one thread.
+// Merge-path tile: at most kTileSize rows + nonzeros.
+//  1. every thread loads kTileItems of the tile's nonzeros (coalesced,
+//     all loads issued before any is used), gathers x, and stores the
+//     products to shared memory; the row ends are staged beside them;
+//  2. thread i takes merge items [8i, 8i+8) of the tile -- its start is found
+//     by a merge-path binary search in shared memory -- and walks them in
+//     order: a nonzero adds its product to the running row sum, a row end
+//     stores the sum and starts the next row;
+//  3. the row each thread still has open at the end of its items is joined
+//     across threads by a segmented scan (warp shuffles, then warp totals in
+//     thread order): the thread that ends such a row adds what the earlier
+//     threads summed; the tile's own open row goes to the carry array;
+//  4. the tile's finished rows are written to y with coalesced stores.
+// Every sum is taken in a fixed order, so results are deterministic.
 template <typename Real>
 __global__ void __launch_bounds__(kTileThreads) k_csr_tile(const int32_t* __restrict__ rowptr,
                                                           const int32_t* __restrict__ cols,
@@ -259,12 +265,11 @@ __global__ void __launch_bounds__(kTileThreads) k_csr_tile(const int32_t* __rest
                                                           int32_t* __restrict__ carry_row, Real* __restrict__ carry_val,
                                                           Real alpha, Real beta, const int32_t* __restrict__ skip)
 {
-   constexpr int kWarps = kTileThreads / 32;
-   constexpr int kSteps = kTileItems;  // 32-nonzero steps per warp (kTileSize / kWarps / 32)
-   __shared__ int32_t s_rowend[kTileSize + 1];
-   __shared__ Real s_y[kTileSize + 1];
-   __shared__ int32_t s_pk[2 * kWarps];
-   __shared__ Real s_pv[2 * kWarps];
+   __shared__ Real s_prod[kTileSize];
+   __shared__ int32_t s_rowend[kTileSize];
+   __shared__ Real s_y[kTileSize];
+   __shared__ int32_t s_ck[kTileThreads];
+   __shared__ Real s_cv[kTileThreads];
 
    // solvers pass their device `done` flag: nothing to do once they stopped
    if (skip && *skip) return;
@@ -275,120 +280,99 @@ __global__ void __launch_bounds__(kTileThreads) k_csr_tile(const int32_t* __rest
    const int32_t nrows = r1 - r0, nk = k1 - k0;
    const uint64_t pol_stream = policy_evict_first(), pol_keep = policy_evict_last();
 
-   // this warp's nonzeros [wb, we)
-   const int32_t chunk = (nk + kWarps - 1) / kWarps;
-   const int32_t wb = k0 + imin64(nk, (int64_t)warp * chunk);
-   const int32_t we = k0 + imin64(nk, (int64_t)(warp + 1) * chunk);
-
-   // issue the streaming loads first
-   int32_t c[kSteps];
-   Real v[kSteps];
+   // 1. products and row ends
+   {
+      int32_t c[kTileItems];
+      Real v[kTileItems];
 #pragma unroll
-   for (int j = 0; j < kSteps; j++) {
-      const int32_t e = wb + j * 32 + lane;
-      c[j] = -1;
-      v[j] = Real(0);
-      if (e < we) {
-         c[j] = ld_stream_hint(cols + e, pol_stream);
-         v[j] = ld_stream_hint(vals + e, pol_stream);
+      for (int j = 0; j < kTileItems; j++) {
+         const int32_t e = k0 + j * kTileThreads + tid;
+         c[j] = -1;
+         v[j] = Real(0);
+         if (e < k1) {
+            c[j] = ld_stream_hint(cols + e, pol_stream);
+            v[j] = ld_stream_hint(vals + e, pol_stream);
+         }
       }
-   }
-   // row ends of the rows ending in the tile, plus the open row
-   for (int32_t i = tid; i <= nrows; i += kTileThreads) {
-      const int64_t r = (int64_t)r0 + i + 1;
-      s_rowend[i] = r <= n ? rowptr[r] : INT_MAX;
-      s_y[i] = Real(0);
-   }
-   // gathers
-   Real p[kSteps];
+      // every gather is issued before any product is stored (padding, column
+      // -1, contributes 0)
+      Real p[kTileItems];
 #pragma unroll
-   for (int j = 0; j < kSteps; j++) p[j] = c[j] >= 0 ? v[j] * ld_keep(x + c[j], pol_keep) : Real(0);
+      for (int j = 0; j < kTileItems; j++) p[j] = c[j] >= 0 ? v[j] * ld_keep(x + c[j], pol_keep) : Real(0);
+      for (int32_t i = tid; i < nrows; i += kTileThreads) s_rowend[i] = rowptr[r0 + i + 1];
+#pragma unroll
+      for (int j = 0; j < kTileItems; j++)
+         if (k0 + j * kTileThreads + tid < k1) s_prod[j * kTileThreads + tid] = p[j];
+   }
    __syncthreads();
 
-   // local row of element e: first i in [0, nrows] with s_rowend[i] > e
-   auto row_of = [&](int32_t e, int32_t lo) -> int32_t {
-      int32_t hi = nrows;
-      while (lo < hi) {
-         const int32_t mid = (lo + hi) >> 1;
-         if (s_rowend[mid] > e)
-            hi = mid;
-         else
-            lo = mid + 1;
-      }
-      return lo;
-   };
-   const int32_t wfirst = wb < we ? row_of(wb, 0) : -1;
-   int32_t key[kSteps];
+   // 2. this thread's merge items
+   const int32_t dtot = nrows + nk;
+   const int32_t d = imin64((int64_t)tid * kTileItems, dtot);
+   int32_t lo = imax64(0, d - nk), hi = imin64(d, nrows);
+   while (lo < hi) {
+      const int32_t mid = (lo + hi) >> 1;
+      if (s_rowend[mid] <= k0 + d - mid - 1)
+         lo = mid + 1;
+      else
+         hi = mid;
+   }
+   int32_t row = lo, k = d - lo;  // k local to the tile
+   int32_t first_done = -1;
+   Real acc = Real(0);
+   {
+      const int32_t dend = imin64((int64_t)d + kTileItems, dtot);
+      int32_t rend = row < nrows ? s_rowend[row] - k0 : INT_MAX;
 #pragma unroll
-   for (int j = 0; j < kSteps; j++) {
-      const int32_t e = wb + j * 32 + lane;
-      key[j] = e < we ? row_of(e, wfirst) : INT_MAX;
+      for (int it = 0; it < kTileItems; it++) {
+         if (d + it < dend) {
+            if (rend <= k) {
+               s_y[row] = acc;
+               if (first_done < 0) first_done = row;
+               acc = Real(0);
+               row++;
+               rend = row < nrows ? s_rowend[row] - k0 : INT_MAX;
+            }
+            else {
+               acc += s_prod[k];
+               k++;
+            }
+         }
+      }
    }
 
-   int32_t carry_k = -1;
-   Real carry_v = Real(0), first_v = Real(0);
-   bool have_first = false;
-   // emit a finished row piece: the warp's first row may continue from the
-   // previous warp, so it is kept for the cross-warp combine
-   auto emit = [&](int32_t k, Real val) {
-      if (k == wfirst) {
-         first_v = val;
-         have_first = true;
-      }
-      else
-         s_y[k] = val;
-   };
-#pragma unroll
-   for (int j = 0; j < kSteps; j++) {
-      if (wb + j * 32 >= we) break;  // warp-uniform
-      const int32_t kj = key[j];
-      Real val = p[j];
+   // 3. segmented scan of the open rows (keys are non-decreasing in thread order)
+   {
+      Real val = acc;
 #pragma unroll
       for (int o = 1; o < 32; o <<= 1) {
-         const int32_t kk = __shfl_up_sync(0xffffffffu, kj, o);
+         const int32_t kk = __shfl_up_sync(0xffffffffu, row, o);
          const Real vv = __shfl_up_sync(0xffffffffu, val, o);
-         if (lane >= o && kk == kj) val += vv;
+         if (lane >= o && kk == row) val += vv;
       }
-      const int32_t k_first = __shfl_sync(0xffffffffu, kj, 0);
-      if (carry_k >= 0 && carry_k != k_first) {
-         // the previous step's last row ended exactly at the step boundary
-         if (lane == 0) emit(carry_k, carry_v);
-         carry_k = -1;
-      }
-      if (carry_k >= 0 && kj == carry_k) val += carry_v;
-      // the step's last valid lane holds the row that may continue into the
-      // next step: it is carried, every other segment end is emitted
-      const unsigned valid = __ballot_sync(0xffffffffu, kj != INT_MAX);
-      const int last_lane = 31 - __clz((int)valid);
-      const int32_t k_next = __shfl_down_sync(0xffffffffu, kj, 1);
-      if (lane < last_lane && k_next != kj) emit(kj, val);
-      carry_k = __shfl_sync(0xffffffffu, kj, last_lane);
-      carry_v = __shfl_sync(0xffffffffu, val, last_lane);
-   }
-   // warp pieces: the first row if it finished inside the warp (held by the
-   // lane that emitted it), and the last row in progress
-   {
-      const unsigned who = __ballot_sync(0xffffffffu, have_first);
-      const Real fv = __shfl_sync(0xffffffffu, first_v, who ? __ffs(who) - 1 : 0);
-      if (lane == 0) {
-         s_pk[2 * warp] = who ? wfirst : -1;
-         s_pv[2 * warp] = who ? fv : Real(0);
-         s_pk[2 * warp + 1] = carry_k;
-         s_pv[2 * warp + 1] = carry_v;
-      }
+      s_ck[tid] = row;
+      s_cv[tid] = val;
    }
    __syncthreads();
-   if (tid == 0) {
-      // combine the pieces in warp order (deterministic)
-      for (int q = 0; q < 2 * kWarps; q++) {
-         const int32_t k = s_pk[q];
-         if (k >= 0) s_y[k] += s_pv[q];
-      }
+   // inclusive segmented sum up to thread u: earlier warps' totals for the
+   // same row (in warp order), then u's own within-warp sum
+   auto scanned = [&](int u) -> Real {
+      const int32_t key = s_ck[u];
+      Real s = Real(0);
+      for (int w = 0; w < (u >> 5); w++)
+         if (s_ck[w * 32 + 31] == key) s += s_cv[w * 32 + 31];
+      return s + s_cv[u];
+   };
+   if (first_done >= 0 && tid > 0 && s_ck[tid - 1] == first_done) s_y[first_done] += scanned(tid - 1);
+   if (tid == kTileThreads - 1) {
+      // the last thread ends on the tile's open row (local index nrows)
       const bool has = nk > 0 && (nrows == 0 || s_rowend[nrows - 1] < k1);
       carry_row[t] = (has && r1 < n) ? r1 : -1;
-      carry_val[t] = s_y[nrows];
+      carry_val[t] = scanned(tid);
    }
    __syncthreads();
+
+   // 4. finished rows
    for (int32_t i = tid; i < nrows; i += kTileThreads) keep(y, r0 + i, s_y[i], alpha, beta);
 }
 
@@ -545,3 +529,4 @@ tnlb_status spmv_csr(const tnlb_segments* seg, tnlb_real real, const int32_t* co
 }
 
 }  // namespace tnlb
+

@@ -182,3 +182,39 @@ def diffusion_problem(N: int, seed: int, corr_range=(0.02, 0.2), sigma_range=(1.
     sigma = sigma_range[0] + (sigma_range[1] - sigma_range[0]) * u[1]
     A = diffusion_2d(N, corr, sigma, seed)
     return SparseMatrix.from_csr(A, real=torch.float64)
+
+
+def main(argv=None):
+    """Train the learned FSAI on seeded 2D diffusion problems and save the
+    weights (float32, 9668 values):
+
+        python -m tnl_b200.lfsai --out tnl_b200/weights/lfsai_diffusion.npy
+    """
+    import argparse
+    import json
+    import sys
+    import time
+
+    ap = argparse.ArgumentParser(prog="python -m tnl_b200.lfsai")
+    ap.add_argument("--out", required=True)
+    ap.add_argument("--N", type=int, default=128, help="grid side of the training problems")
+    ap.add_argument("--problems", type=int, default=8)
+    ap.add_argument("--fit-steps", type=int, default=400)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--seed", type=int, default=2)
+    args = ap.parse_args(argv)
+    t0 = time.perf_counter()
+    train = [diffusion_problem(args.N, s) for s in range(args.problems)]
+    net = LearnedFSAI(seed=args.seed)
+    fit = net.fit_classical(train, steps=args.fit_steps, lr=3e-3)
+    hist = net.train(train, steps=args.steps, nprobes=8, lr=5e-4)
+    Path(args.out).parent.mkdir(parents=True, exist_ok=True)
+    net.save(args.out)
+    print(json.dumps({"fit_loss": [fit[0], fit[-1]], "probe_loss": [float(np.mean(hist[:len(train)])),
+                                                                    float(np.mean(hist[-len(train):]))],
+                      "seconds": time.perf_counter() - t0, "out": str(args.out)}), file=sys.stdout)
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())
