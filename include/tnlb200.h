@@ -208,6 +208,33 @@ tnlb_status tnlb_spmv(const tnlb_segments* seg, tnlb_real real, const int32_t* d
  * enqueued (for launch accounting). */
 int32_t tnlb_spmv_last_launch_count(void);
 
+/* y = alpha * A x + beta * y for a CSR matrix given as plain device arrays
+ * (row offsets d_rowptr[rows + 1], d_cols / d_values[nnz], nnz == d_rowptr[rows]),
+ * computed by the same tile kernels as tnlb_spmv on CSR segments and giving
+ * the same bits, but allocating no device memory: the tile plan and the
+ * carries of rows split between tiles go to a statically sized scratch
+ * array compiled into the library (2.6 MB per device).  No counterpart in
+ * the reference, whose SpMV takes the segments' own arrays.
+ *
+ * For callers that must not allocate: code running while a caching
+ * allocator or memory pool owns the device's free memory, code on a path
+ * where cudaMalloc / cudaFree would synchronise the device and stall other
+ * streams, and host code that holds CSR arrays from another library and no
+ * segments handle.
+ *
+ * Limit: rows + nnz <= 268,435,456 (131,072 tiles of 2048 rows + nonzeros);
+ * larger matrices are rejected with TNLB_ERR_INVALID_ARGUMENT before any
+ * launch.  Nothing in the scratch has to start at zero: every call rewrites
+ * what it reads.  The first call on each device looks up the scratch address
+ * (cudaGetSymbolAddress with that device current, which may load the
+ * library's device code there); make one call per device before capturing a
+ * stream.  Calls that overlap on one device -- on two streams, or from two
+ * host threads -- share the scratch and race: order them on one stream.
+ * Enqueues three kernels on `stream`; returns before they finish. */
+tnlb_status tnlb_spmv_csr_noalloc(tnlb_real real, int32_t rows, int32_t columns, int64_t nnz,
+                                  const int32_t* d_rowptr, const int32_t* d_cols, const void* d_values,
+                                  const void* d_x, void* d_y, double alpha, double beta, tnlb_stream stream);
+
 /* ------------------------------------------------------------ vectors */
 
 /* Dot product (a, b) into a DEVICE scalar -- Containers/Expressions/

@@ -530,3 +530,103 @@ tnlb_status spmv_csr(const tnlb_segments* seg, tnlb_real real, const int32_t* co
 
 }  // namespace tnlb
 
+// ------------------------------------------- CSR SpMV without allocation
+//
+// tnlb_spmv_csr_noalloc runs the tile kernel above on plain CSR arrays with
+// no segments handle.  Its per-call scratch -- the tile plan and the carry
+// of rows split between tiles -- lives in one statically sized device array
+// of this file, so a call allocates no device memory.  Every call rewrites
+// each scratch entry it reads (the plan kernel writes all tile coordinates
+// and resets the carry rows; the tile kernel writes every tile's carry), so
+// nothing has to start at zero.  Calls that overlap on one device share the
+// array and race.
+
+#include <mutex>
+
+namespace {
+
+constexpr int64_t kNoAllocMaxTiles = 131072;  // rows + nonzeros <= 268,435,456
+constexpr size_t kNoAllocAlign = 256;
+constexpr size_t round_up_256(size_t b) { return (b + kNoAllocAlign - 1) / kNoAllocAlign * kNoAllocAlign; }
+constexpr size_t kNoAllocCarryValBytes = round_up_256(sizeof(double) * kNoAllocMaxTiles);
+constexpr size_t kNoAllocPlanBytes = round_up_256(sizeof(int32_t) * (kNoAllocMaxTiles + 1));
+constexpr size_t kNoAllocCarryRowBytes = round_up_256(sizeof(int32_t) * kNoAllocMaxTiles);
+constexpr size_t kNoAllocBytes = kNoAllocCarryValBytes + 2 * kNoAllocPlanBytes + kNoAllocCarryRowBytes;
+constexpr int kNoAllocMaxDevices = 64;
+
+std::mutex g_noalloc_mutex;
+unsigned char* g_noalloc_base[kNoAllocMaxDevices] = {};
+
+}  // namespace
+
+// 2.6 MB: carry values (FP64 slots, FP32 uses the first half), tile rows,
+// tile nonzero offsets, carry rows.
+static __device__ __align__(256) unsigned char g_tile_scratch[kNoAllocBytes];
+
+namespace {
+
+// Address of g_tile_scratch on the current device, looked up once per device.
+tnlb_status noalloc_scratch(unsigned char** base)
+{
+   int dev = -1;
+   TNLB_CUDA_TRY(cudaGetDevice(&dev));
+   TNLB_REQUIRE(dev >= 0 && dev < kNoAllocMaxDevices, TNLB_ERR_INVALID_ARGUMENT,
+                "tnlb_spmv_csr_noalloc: device ordinal above 63");
+   std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+   if (!g_noalloc_base[dev]) {
+      void* p = nullptr;
+      TNLB_CUDA_TRY(cudaGetSymbolAddress(&p, g_tile_scratch));
+      g_noalloc_base[dev] = (unsigned char*)p;
+   }
+   *base = g_noalloc_base[dev];
+   return TNLB_OK;
+}
+
+template <typename Real>
+tnlb_status spmv_csr_noalloc_t(unsigned char* base, int32_t rows, int64_t nnz, int32_t tiles, const int32_t* rowptr,
+                               const int32_t* cols, const Real* vals, const Real* x, Real* y, Real alpha, Real beta,
+                               cudaStream_t st)
+{
+   Real* carry_val = (Real*)base;
+   int32_t* tile_row = (int32_t*)(base + kNoAllocCarryValBytes);
+   int32_t* tile_nnz = (int32_t*)(base + kNoAllocCarryValBytes + kNoAllocPlanBytes);
+   int32_t* carry_row = (int32_t*)(base + kNoAllocCarryValBytes + 2 * kNoAllocPlanBytes);
+   tnlb::k_tile_plan<<<tnlb::grid_for((int64_t)tiles + 1, 256), 256, 0, st>>>(rowptr, rows, nnz, tiles, tile_row,
+                                                                               tile_nnz, carry_row);
+   TNLB_CHECK_LAUNCH();
+   tnlb::k_csr_tile<Real><<<tiles, tnlb::kTileThreads, 0, st>>>(rowptr, cols, vals, x, y, tile_row, tile_nnz, rows,
+                                                                carry_row, carry_val, alpha, beta, nullptr);
+   TNLB_CHECK_LAUNCH();
+   tnlb::k_csr_tile_fixup<Real><<<tnlb::grid_for(tiles, 256), 256, 0, st>>>(carry_row, carry_val, tiles, y, alpha,
+                                                                             nullptr);
+   TNLB_CHECK_LAUNCH();
+   return TNLB_OK;
+}
+
+}  // namespace
+
+extern "C" tnlb_status tnlb_spmv_csr_noalloc(tnlb_real real, int32_t rows, int32_t columns, int64_t nnz,
+                                             const int32_t* d_rowptr, const int32_t* d_cols, const void* d_values,
+                                             const void* d_x, void* d_y, double alpha, double beta,
+                                             tnlb_stream stream)
+{
+   using namespace tnlb;
+   clear_error();
+   TNLB_REQUIRE(real == TNLB_F32 || real == TNLB_F64, TNLB_ERR_INVALID_ARGUMENT, "unknown real type");
+   TNLB_REQUIRE(rows >= 0 && columns >= 0 && nnz >= 0 && nnz <= INT32_MAX, TNLB_ERR_INVALID_ARGUMENT,
+                "tnlb_spmv_csr_noalloc: negative size or more than 2^31-1 nonzeros");
+   const int64_t tiles = ((int64_t)rows + nnz + kTileSize - 1) / kTileSize;
+   TNLB_REQUIRE(tiles <= kNoAllocMaxTiles, TNLB_ERR_INVALID_ARGUMENT,
+                "tnlb_spmv_csr_noalloc: rows + nonzeros exceeds the static scratch limit of 268435456 "
+                "(131072 tiles of 2048); use tnlb_spmv");
+   if (rows == 0) return TNLB_OK;
+   TNLB_REQUIRE(d_rowptr && d_y && (nnz == 0 || (d_cols && d_values && d_x)), TNLB_ERR_INVALID_ARGUMENT,
+                "null array");
+   unsigned char* base = nullptr;
+   TNLB_TRY_STATUS(noalloc_scratch(&base));
+   if (real == TNLB_F64)
+      return spmv_csr_noalloc_t<double>(base, rows, nnz, (int32_t)tiles, d_rowptr, d_cols, (const double*)d_values,
+                                        (const double*)d_x, (double*)d_y, alpha, beta, (cudaStream_t)stream);
+   return spmv_csr_noalloc_t<float>(base, rows, nnz, (int32_t)tiles, d_rowptr, d_cols, (const float*)d_values,
+                                    (const float*)d_x, (float*)d_y, (float)alpha, (float)beta, (cudaStream_t)stream);
+}
