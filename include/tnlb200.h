@@ -213,7 +213,7 @@ int32_t tnlb_spmv_last_launch_count(void);
  * computed by the same tile kernels as tnlb_spmv on CSR segments and giving
  * the same bits, but allocating no device memory: the tile plan and the
  * carries of rows split between tiles go to a statically sized scratch
- * array compiled into the library (2.6 MB per device).  No counterpart in
+ * array compiled into the library (5.2 MB per device).  No counterpart in
  * the reference, whose SpMV takes the segments' own arrays.
  *
  * For callers that must not allocate: code running while a caching
@@ -222,7 +222,7 @@ int32_t tnlb_spmv_last_launch_count(void);
  * streams, and host code that holds CSR arrays from another library and no
  * segments handle.
  *
- * Limit: rows + nnz <= 268,435,456 (131,072 tiles of 2048 rows + nonzeros);
+ * Limit: rows + nnz <= 67,108,864 (262,144 tiles of 256 rows + nonzeros);
  * larger matrices are rejected with TNLB_ERR_INVALID_ARGUMENT before any
  * launch.  Nothing in the scratch has to start at zero: every call rewrites
  * what it reads.  The first call on each device looks up the scratch address
@@ -318,8 +318,11 @@ tnlb_status tnlb_true_residual(const tnlb_segments* seg, tnlb_real real, const i
 /* FP32-inner / FP64-outer iterative refinement (no counterpart in the
  * reference): the FP64 residual r = b - A x is formed with the FP64 values,
  * normalised, rounded to FP32 and solved with `inner_solver` (CG for SPD
- * matrices, FGMRES/GMRES/BiCGStab otherwise) on an FP32 copy of the values to
- * relative residual `inner_tolerance`; x += |r| d in FP64.
+ * matrices, FGMRES/GMRES/BiCGStab otherwise) on an FP32 copy of the values;
+ * x += |r| d in FP64.  The first inner solve goes to relative residual
+ * `inner_tolerance`; later ones only as far as the outer residual still
+ * needs (a tenth of target / current residual, clamped to
+ * [inner_tolerance, 0.5]).
  * The inner preconditioner is `inner` (an FP32 preconditioner of this
  * matrix, e.g. a learned FSAI) or, when NULL, one of kind `inner_precond`
  * built from the FP32 values.  Stops

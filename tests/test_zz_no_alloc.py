@@ -12,7 +12,7 @@ import torch
 
 pytestmark = pytest.mark.gpu
 
-LIMIT = 131072 * 2048  # rows + nonzeros the static scratch holds
+LIMIT = 262144 * 256  # rows + nonzeros the static scratch holds
 
 
 def _noalloc(M, x, y, alpha, beta):

@@ -179,7 +179,7 @@ def bench_solvers(problem: str, N: int, weights: str | None, out=sys.stdout):
 
     def mixed(name, inner, setup_ms):
         x = torch.zeros(n, dtype=torch.float64, device="cuda")
-        r, ms = _timed(lambda: t.solve_mixed(M, b, x, tol=1e-8, inner_tol=1e-4, inner=inner))
+        r, ms = _timed(lambda: t.solve_mixed(M, b, x, tol=1e-8, inner_tol=1e-6, inner=inner))
         rec = dict(base, method=name, converged=r["converged"], iterations=r["inner_iterations"],
                    outer_iterations=r["outer_iterations"], solve_ms=ms, setup_ms=setup_ms,
                    true_residual=t.true_residual(M, b, x), speedup_vs_fp64_jacobi=jac["solve_ms"] / ms)

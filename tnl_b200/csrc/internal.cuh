@@ -52,11 +52,11 @@ constexpr int kBiGroups = 6;         // log2(32) + 1
 constexpr int kChunksInSlice = 256;  // ChunkedEllpackBase.h:291
 constexpr int kDesiredChunkSize = 16;  // ChunkedEllpackBase.h:292
 
-// CSR tile kernel geometry: 256 threads, ITEMS merge items (rows + nonzeros)
-// per thread.
+// CSR tile kernel geometry: a tile of kTileSize merge items (rows +
+// nonzeros) per warp, kTileItems per lane; blocks of kTileThreads threads.
 constexpr int kTileThreads = 256;
 constexpr int kTileItems = 8;
-constexpr int kTileSize = kTileThreads * kTileItems;
+constexpr int kTileSize = 32 * kTileItems;
 
 // ------------------------------------------------------- device buffers
 

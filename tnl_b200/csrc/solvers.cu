@@ -1541,6 +1541,11 @@ tnlb_status solve_mixed_cg(const tnlb_segments* seg, const int32_t* cols, const 
       const double rn = std::sqrt(h[0]), bn = std::sqrt(h[1]);
       resid = bn > 0 ? rn / bn : 0.0;
       if (bn == 0 || resid < prm.convergence_residue || o == max_outer) break;
+      // The correction only has to take the residual from `resid` to the
+      // target: after the first solve (to inner_tol) the inner tolerance is
+      // loosened to a tenth of that ratio, never below inner_tol, never
+      // above 0.5 (the tenth leaves room for the FP32 solve's own error).
+      ip.convergence_residue = std::min(0.5, std::max(inner_tol, 0.1 * prm.convergence_residue / resid));
       // unit-norm FP32 residual, FP32 Jacobi-PCG correction
       k_scale<double><<<vec_grid(n), kRedThreads, 0, st>>>(n, 1.0 / rn, r64.as<double>(), r64.as<double>());
       k_convert<float, double><<<vec_grid(n), kRedThreads, 0, st>>>(n, r64.as<double>(), r32.as<float>());

@@ -13,19 +13,17 @@
 //                (ReducingKernels_AdaptiveCSR.h:16-134)
 //  * tile     -- the default: nnz-balanced merge-path tiles.  The merge of
 //                the row-end offsets with the nonzero indices is cut into
-//                tiles of 2048 items (rows + nonzeros) so that every block
-//                does the same work whatever the row-length distribution
-//                (Merrill & Garland, "Merge-based parallel sparse
-//                matrix-vector multiplication", SC16).  Each block streams
-//                its values/columns with coalesced non-caching loads,
-//                stages row ends and products in shared memory, walks 8
-//                merge items per thread, combines rows split between
-//                threads with a warp-shuffle segmented scan, and writes y
-//                with coalesced stores.  A row split between tiles leaves a
-//                partial sum per tile in a carry array; a second small
-//                kernel adds them (in tile order, so results are
-//                deterministic).  The tile coordinates are computed once
-//                per matrix, when the segments are built.
+//                tiles of 256 items (rows + nonzeros), one per warp, so that
+//                every warp does the same work whatever the row-length
+//                distribution (Merrill & Garland, "Merge-based parallel
+//                sparse matrix-vector multiplication", SC16).  A warp keeps
+//                its tile's products in registers, marks the rows ending in
+//                the tile in a bit mask and sums rows with segmented shuffle
+//                scans.  A row split between tiles leaves a partial sum per
+//                tile in a carry array; a second small kernel adds them (in
+//                tile order, so results are deterministic).  The tile
+//                coordinates are computed once per matrix, when the
+//                segments are built.
 #include <climits>
 
 #include "internal.cuh"
@@ -242,138 +240,123 @@ __device__ __forceinline__ float ld_keep(const float* a, uint64_t pol)
    return v;
 }
 
-// Merge-path tile: at most kTileSize rows + nonzeros.
-//  1. every thread loads kTileItems of the tile's nonzeros (coalesced,
-//     all loads issued before any is used), gathers x, and stores the
-//     products to shared memory; the row ends are staged beside them;
-//  2. thread i takes merge items [8i, 8i+8) of the tile -- its start is found
-//     by a merge-path binary search in shared memory -- and walks them in
-//     order: a nonzero adds its product to the running row sum, a row end
-//     stores the sum and starts the next row;
-//  3. the row each thread still has open at the end of its items is joined
-//     across threads by a segmented scan (warp shuffles, then warp totals in
-//     thread order): the thread that ends such a row adds what the earlier
-//     threads summed; the tile's own open row goes to the carry array;
-//  4. the tile's finished rows are written to y with coalesced stores.
-// Every sum is taken in a fixed order, so results are deterministic.
+// Merge-path tile of one warp: at most kTileSize = 256 rows + nonzeros.
+// Warps work independently (no block-wide barrier), so one warp's loads
+// overlap another's arithmetic.  The tile's nonzeros stay in registers in
+// striped order (lane l holds nonzeros k0 + 32 j + l, j < 8): all loads and
+// x gathers are issued before any is used.  The rows ending in the tile are
+// marked in a 256-bit mask at the position of their last nonzero (with the
+// row index beside it); rows with no nonzero in the tile are written at once.
+// Step j then sums its 32 products per row by a segmented shuffle scan whose
+// segments the mask delimits; a lane holding a row's last nonzero writes the
+// row.  The row still open at the end of a step carries into the next one
+// (a step with no row end only adds each lane's product to a per-lane
+// partial, reduced when the row ends), and the row open at the end of the
+// tile goes to the carry array.  Every
+// sum is taken in a fixed order, so results are deterministic.
 template <typename Real>
-__global__ void __launch_bounds__(kTileThreads) k_csr_tile(const int32_t* __restrict__ rowptr,
+__global__ void __launch_bounds__(kTileThreads, 5) k_csr_tile(const int32_t* __restrict__ rowptr,
                                                           const int32_t* __restrict__ cols,
                                                           const Real* __restrict__ vals, const Real* __restrict__ x,
                                                           Real* __restrict__ y, const int32_t* __restrict__ tile_row,
-                                                          const int32_t* __restrict__ tile_nnz, int32_t n,
+                                                          const int32_t* __restrict__ tile_nnz, int32_t tiles, int32_t n,
                                                           int32_t* __restrict__ carry_row, Real* __restrict__ carry_val,
                                                           Real alpha, Real beta, const int32_t* __restrict__ skip)
 {
-   __shared__ Real s_prod[kTileSize];
-   __shared__ int32_t s_rowend[kTileSize];
-   __shared__ Real s_y[kTileSize];
-   __shared__ int32_t s_ck[kTileThreads];
-   __shared__ Real s_cv[kTileThreads];
+   constexpr int kWarps = kTileThreads / 32;
+   __shared__ uint32_t s_mask[kWarps][kTileItems];
+   __shared__ int32_t s_rowid[kWarps][kTileSize];
 
    // solvers pass their device `done` flag: nothing to do once they stopped
    if (skip && *skip) return;
-   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-   const int32_t t = blockIdx.x;
+   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+   const int64_t t = (int64_t)blockIdx.x * kWarps + warp;
+   if (t >= tiles) return;  // warp-uniform
    const int32_t r0 = tile_row[t], r1 = tile_row[t + 1];
    const int32_t k0 = tile_nnz[t], k1 = tile_nnz[t + 1];
    const int32_t nrows = r1 - r0, nk = k1 - k0;
+   uint32_t* sm = s_mask[warp];
+   int32_t* sid = s_rowid[warp];
    const uint64_t pol_stream = policy_evict_first(), pol_keep = policy_evict_last();
 
-   // 1. products and row ends
-   {
-      int32_t c[kTileItems];
-      Real v[kTileItems];
+   int32_t c[kTileItems];
+   Real v[kTileItems];
 #pragma unroll
-      for (int j = 0; j < kTileItems; j++) {
-         const int32_t e = k0 + j * kTileThreads + tid;
-         c[j] = -1;
-         v[j] = Real(0);
-         if (e < k1) {
-            c[j] = ld_stream_hint(cols + e, pol_stream);
-            v[j] = ld_stream_hint(vals + e, pol_stream);
-         }
+   for (int j = 0; j < kTileItems; j++) {
+      const int32_t e = k0 + j * 32 + lane;
+      c[j] = -1;
+      v[j] = Real(0);
+      if (e < k1) {
+         c[j] = ld_stream_hint(cols + e, pol_stream);
+         v[j] = ld_stream_hint(vals + e, pol_stream);
       }
-      // every gather is issued before any product is stored (padding, column
-      // -1, contributes 0)
-      Real p[kTileItems];
-#pragma unroll
-      for (int j = 0; j < kTileItems; j++) p[j] = c[j] >= 0 ? v[j] * ld_keep(x + c[j], pol_keep) : Real(0);
-      for (int32_t i = tid; i < nrows; i += kTileThreads) s_rowend[i] = rowptr[r0 + i + 1];
-#pragma unroll
-      for (int j = 0; j < kTileItems; j++)
-         if (k0 + j * kTileThreads + tid < k1) s_prod[j * kTileThreads + tid] = p[j];
    }
-   __syncthreads();
-
-   // 2. this thread's merge items
-   const int32_t dtot = nrows + nk;
-   const int32_t d = imin64((int64_t)tid * kTileItems, dtot);
-   int32_t lo = imax64(0, d - nk), hi = imin64(d, nrows);
-   while (lo < hi) {
-      const int32_t mid = (lo + hi) >> 1;
-      if (s_rowend[mid] <= k0 + d - mid - 1)
-         lo = mid + 1;
+   if (lane < kTileItems) sm[lane] = 0u;
+   __syncwarp();
+   // rows ending in the tile: mark the last nonzero, or write a row that has
+   // none here (empty, or all of it in earlier tiles)
+   for (int32_t i = lane; i < nrows; i += 32) {
+      const int32_t r = r0 + i;
+      const int32_t e_end = rowptr[r + 1], e_beg = rowptr[r];
+      if (e_end > k0 && e_end > e_beg) {
+         const int32_t pos = e_end - k0 - 1;
+         atomicOr(sm + (pos >> 5), 1u << (pos & 31));
+         sid[pos] = r;
+      }
       else
-         hi = mid;
+         keep(y, r, Real(0), alpha, beta);
    }
-   int32_t row = lo, k = d - lo;  // k local to the tile
-   int32_t first_done = -1;
-   Real acc = Real(0);
-   {
-      const int32_t dend = imin64((int64_t)d + kTileItems, dtot);
-      int32_t rend = row < nrows ? s_rowend[row] - k0 : INT_MAX;
 #pragma unroll
-      for (int it = 0; it < kTileItems; it++) {
-         if (d + it < dend) {
-            if (rend <= k) {
-               s_y[row] = acc;
-               if (first_done < 0) first_done = row;
-               acc = Real(0);
-               row++;
-               rend = row < nrows ? s_rowend[row] - k0 : INT_MAX;
-            }
-            else {
-               acc += s_prod[k];
-               k++;
-            }
-         }
-      }
-   }
+   for (int j = 0; j < kTileItems; j++) v[j] = c[j] >= 0 ? v[j] * ld_keep(x + c[j], pol_keep) : Real(0);
+   __syncwarp();
 
-   // 3. segmented scan of the open rows (keys are non-decreasing in thread order)
-   {
-      Real val = acc;
+   // The open row's partial sum: `carry` (one value) plus, after steps with
+   // no row end, the per-lane partials `part`, reduced only when the row
+   // ends (most nonzeros of a power-law matrix lie in steps without one).
+   Real carry = Real(0), part = Real(0);
+   bool parts = false;
+   auto reduce_parts = [&]() -> Real {
+      Real s = part;
 #pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-         const int32_t kk = __shfl_up_sync(0xffffffffu, row, o);
-         const Real vv = __shfl_up_sync(0xffffffffu, val, o);
-         if (lane >= o && kk == row) val += vv;
-      }
-      s_ck[tid] = row;
-      s_cv[tid] = val;
-   }
-   __syncthreads();
-   // inclusive segmented sum up to thread u: earlier warps' totals for the
-   // same row (in warp order), then u's own within-warp sum
-   auto scanned = [&](int u) -> Real {
-      const int32_t key = s_ck[u];
-      Real s = Real(0);
-      for (int w = 0; w < (u >> 5); w++)
-         if (s_ck[w * 32 + 31] == key) s += s_cv[w * 32 + 31];
-      return s + s_cv[u];
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+      return s;
    };
-   if (first_done >= 0 && tid > 0 && s_ck[tid - 1] == first_done) s_y[first_done] += scanned(tid - 1);
-   if (tid == kTileThreads - 1) {
-      // the last thread ends on the tile's open row (local index nrows)
-      const bool has = nk > 0 && (nrows == 0 || s_rowend[nrows - 1] < k1);
-      carry_row[t] = (has && r1 < n) ? r1 : -1;
-      carry_val[t] = scanned(tid);
+#pragma unroll
+   for (int j = 0; j < kTileItems; j++) {
+      if (j * 32 < nk) {  // warp-uniform
+         const uint32_t m = sm[j];
+         if (m == 0u) {
+            part += v[j];
+            parts = true;
+            continue;
+         }
+         Real open = carry;
+         if (parts) {
+            open += reduce_parts();
+            part = Real(0);
+            parts = false;
+         }
+         const uint32_t below = m & ((1u << lane) - 1u);
+         const int seg0 = below ? 32 - __clz(below) : 0;  // first lane of this lane's row
+         Real val = v[j];
+#pragma unroll
+         for (int o = 1; o < 32; o <<= 1) {
+            const Real vv = __shfl_up_sync(0xffffffffu, val, o);
+            if (lane - o >= seg0) val += vv;
+         }
+         if (seg0 == 0) val += open;
+         if ((m >> lane) & 1u) keep(y, sid[j * 32 + lane], val, alpha, beta);
+         const Real last = __shfl_sync(0xffffffffu, val, 31);
+         carry = (m >> 31) ? Real(0) : last;
+      }
    }
-   __syncthreads();
-
-   // 4. finished rows
-   for (int32_t i = tid; i < nrows; i += kTileThreads) keep(y, r0 + i, s_y[i], alpha, beta);
+   if (parts) carry += reduce_parts();
+   if (lane == 0) {
+      // the row open at the end of the tile (row r1) carries on
+      const bool has = nk > 0 && !((sm[(nk - 1) >> 5] >> ((nk - 1) & 31)) & 1u);
+      carry_row[t] = (has && r1 < n) ? r1 : -1;
+      carry_val[t] = carry;
+   }
 }
 
 // Adds the partial sums of rows split between tiles, in tile order.
@@ -484,8 +467,8 @@ tnlb_status spmv_csr_t(const tnlb_segments* seg, const int32_t* cols, const Real
             return launch_vector<Real>(rowptr, cols, vals, x, y, begin, end, alpha, beta,
                                        light_tps(seg->elements, seg->n), st);
          }
-         k_csr_tile<Real><<<seg->tiles, kTileThreads, 0, st>>>(
-            rowptr, cols, vals, x, y, seg->tile_row.as<int32_t>(), seg->tile_nnz.as<int32_t>(), seg->n,
+         k_csr_tile<Real><<<grid_for(seg->tiles, kTileThreads / 32), kTileThreads, 0, st>>>(
+            rowptr, cols, vals, x, y, seg->tile_row.as<int32_t>(), seg->tile_nnz.as<int32_t>(), seg->tiles, seg->n,
             seg->carry_row.as<int32_t>(), seg->carry_val.as<Real>(), alpha, beta, skip);
          TNLB_CHECK_LAUNCH();
          k_csr_tile_fixup<Real><<<grid_for(seg->tiles, 256), 256, 0, st>>>(
@@ -545,7 +528,7 @@ tnlb_status spmv_csr(const tnlb_segments* seg, tnlb_real real, const int32_t* co
 
 namespace {
 
-constexpr int64_t kNoAllocMaxTiles = 131072;  // rows + nonzeros <= 268,435,456
+constexpr int64_t kNoAllocMaxTiles = 262144;  // rows + nonzeros <= 67,108,864
 constexpr size_t kNoAllocAlign = 256;
 constexpr size_t round_up_256(size_t b) { return (b + kNoAllocAlign - 1) / kNoAllocAlign * kNoAllocAlign; }
 constexpr size_t kNoAllocCarryValBytes = round_up_256(sizeof(double) * kNoAllocMaxTiles);
@@ -559,7 +542,7 @@ unsigned char* g_noalloc_base[kNoAllocMaxDevices] = {};
 
 }  // namespace
 
-// 2.6 MB: carry values (FP64 slots, FP32 uses the first half), tile rows,
+// 5.2 MB: carry values (FP64 slots, FP32 uses the first half), tile rows,
 // tile nonzero offsets, carry rows.
 static __device__ __align__(256) unsigned char g_tile_scratch[kNoAllocBytes];
 
@@ -594,8 +577,8 @@ tnlb_status spmv_csr_noalloc_t(unsigned char* base, int32_t rows, int64_t nnz, i
    tnlb::k_tile_plan<<<tnlb::grid_for((int64_t)tiles + 1, 256), 256, 0, st>>>(rowptr, rows, nnz, tiles, tile_row,
                                                                                tile_nnz, carry_row);
    TNLB_CHECK_LAUNCH();
-   tnlb::k_csr_tile<Real><<<tiles, tnlb::kTileThreads, 0, st>>>(rowptr, cols, vals, x, y, tile_row, tile_nnz, rows,
-                                                                carry_row, carry_val, alpha, beta, nullptr);
+   tnlb::k_csr_tile<Real><<<tnlb::grid_for(tiles, tnlb::kTileThreads / 32), tnlb::kTileThreads, 0, st>>>(
+      rowptr, cols, vals, x, y, tile_row, tile_nnz, tiles, rows, carry_row, carry_val, alpha, beta, nullptr);
    TNLB_CHECK_LAUNCH();
    tnlb::k_csr_tile_fixup<Real><<<tnlb::grid_for(tiles, 256), 256, 0, st>>>(carry_row, carry_val, tiles, y, alpha,
                                                                              nullptr);
@@ -617,8 +600,8 @@ extern "C" tnlb_status tnlb_spmv_csr_noalloc(tnlb_real real, int32_t rows, int32
                 "tnlb_spmv_csr_noalloc: negative size or more than 2^31-1 nonzeros");
    const int64_t tiles = ((int64_t)rows + nnz + kTileSize - 1) / kTileSize;
    TNLB_REQUIRE(tiles <= kNoAllocMaxTiles, TNLB_ERR_INVALID_ARGUMENT,
-                "tnlb_spmv_csr_noalloc: rows + nonzeros exceeds the static scratch limit of 268435456 "
-                "(131072 tiles of 2048); use tnlb_spmv");
+                "tnlb_spmv_csr_noalloc: rows + nonzeros exceeds the static scratch limit of 67108864 "
+                "(262144 tiles of 256); use tnlb_spmv");
    if (rows == 0) return TNLB_OK;
    TNLB_REQUIRE(d_rowptr && d_y && (nnz == 0 || (d_cols && d_values && d_x)), TNLB_ERR_INVALID_ARGUMENT,
                 "null array");
