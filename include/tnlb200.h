@@ -71,15 +71,19 @@ typedef enum { TNLB_COLUMN_MAJOR = 0, TNLB_ROW_MAJOR = 1 } tnlb_organization;
  * (Algorithms/Segments/LaunchConfiguration.h:18-86) and the legacy kernel
  * classes of Algorithms/SegmentsReductionKernels (CSRScalarKernel,
  * CSRVectorKernel, CSRLightKernel, CSRAdaptiveKernel, ...).
- *  TNLB_KERNEL_DEFAULT   -- the tuned kernel of the format (for CSR the
- *                           nnz-balanced tile kernel);
+ *  TNLB_KERNEL_DEFAULT   -- the tuned kernel of the format (for CSR: one
+ *                           thread per row when no row holds more than 16
+ *                           entries, else the nnz-balanced tile kernel);
  *  TNLB_KERNEL_SCALAR    -- one thread per segment (Fixed, TPS 1);
  *  TNLB_KERNEL_VECTOR    -- `threads_per_segment` lanes per segment
  *                           (Fixed TPS 2..32, Warp = 32, 64/128 multi-warp);
  *  TNLB_KERNEL_LIGHT     -- TPS picked from the mean segment length as in
  *                           LaunchConfigurationSetter_LightCSR.h:30-58;
  *  TNLB_KERNEL_ADAPTIVE  -- the AdaptiveCSR block-descriptor kernel (CSR and
- *                           AdaptiveCSR only).
+ *                           AdaptiveCSR only);
+ *  TNLB_KERNEL_TILE      -- CSR: the nnz-balanced merge-path tile kernel
+ *                           whatever the row lengths (no reference
+ *                           counterpart; DynamicGrouping is the nearest).
  * Formats other than CSR accept DEFAULT and, where the reference offers a
  * TPS choice (Ellpack, SlicedEllpack), VECTOR. */
 typedef enum {
@@ -87,7 +91,8 @@ typedef enum {
    TNLB_KERNEL_SCALAR = 1,
    TNLB_KERNEL_VECTOR = 2,
    TNLB_KERNEL_LIGHT = 3,
-   TNLB_KERNEL_ADAPTIVE = 4
+   TNLB_KERNEL_ADAPTIVE = 4,
+   TNLB_KERNEL_TILE = 5
 } tnlb_kernel;
 
 typedef struct tnlb_segments tnlb_segments;
@@ -210,8 +215,8 @@ int32_t tnlb_spmv_last_launch_count(void);
 
 /* y = alpha * A x + beta * y for a CSR matrix given as plain device arrays
  * (row offsets d_rowptr[rows + 1], d_cols / d_values[nnz], nnz == d_rowptr[rows]),
- * computed by the same tile kernels as tnlb_spmv on CSR segments and giving
- * the same bits, but allocating no device memory: the tile plan and the
+ * computed by the same tile kernels as tnlb_spmv with TNLB_KERNEL_TILE on
+ * CSR segments and giving the same bits, but allocating no device memory: the tile plan and the
  * carries of rows split between tiles go to a statically sized scratch
  * array compiled into the library (5.2 MB per device).  No counterpart in
  * the reference, whose SpMV takes the segments' own arrays.
@@ -321,8 +326,9 @@ tnlb_status tnlb_true_residual(const tnlb_segments* seg, tnlb_real real, const i
  * matrices, FGMRES/GMRES/BiCGStab otherwise) on an FP32 copy of the values;
  * x += |r| d in FP64.  The first inner solve goes to relative residual
  * `inner_tolerance`; later ones only as far as the outer residual still
- * needs (a tenth of target / current residual, clamped to
- * [inner_tolerance, 0.5]).
+ * needs (half of target / current residual, clamped to
+ * [inner_tolerance, 0.5]).  The outer residual is computed exactly as
+ * tnlb_true_residual computes it.
  * The inner preconditioner is `inner` (an FP32 preconditioner of this
  * matrix, e.g. a learned FSAI) or, when NULL, one of kind `inner_precond`
  * built from the FP32 values.  Stops

@@ -156,7 +156,7 @@ def kernel_variants(fmt, org):
     t = tnl()
     L = t.LaunchConfiguration
     if fmt == "CSR":
-        return [L("Default"), L("Scalar"), L("Light"), L("Adaptive")] + [L("Fixed", k) for k in (2, 4, 8, 16, 32)] + [
+        return [L("Default"), L("Tile"), L("Scalar"), L("Light"), L("Adaptive")] + [L("Fixed", k) for k in (2, 4, 8, 16, 32)] + [
             L("Block", k) for k in (64, 128, 256)]
     if fmt == "AdaptiveCSR":
         return [L("Default"), L("Adaptive"), L("Light"), L("Fixed", 8)]

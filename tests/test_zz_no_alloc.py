@@ -1,5 +1,5 @@
 """tnlb_spmv_csr_noalloc (CSR SpMV with its scratch in a static device array)
-against tnlb_spmv on CSR segments: the same tile kernels and tile plan, so
+against tnlb_spmv with the tile kernel on CSR segments: the same kernels and tile plan, so
 the results must be bit-identical, on two calls in a row that reuse the
 scratch without any reset.  Collected last so that it also runs after every
 other GPU test in the same process."""
@@ -52,7 +52,7 @@ def test_noalloc_matches_tnlb_spmv_twice(real, alpha, beta):
         x = torch.tensor(g.uniform_vector(M.getColumns(), 11), dtype=real, device="cuda")
         y0 = torch.tensor(g.uniform_vector(M.getRows(), 12), dtype=real, device="cuda")
         y_ref = y0.clone()
-        M.vectorProduct(x, y_ref, alpha, beta)
+        M.vectorProduct(x, y_ref, alpha, beta, launchConfig=tnl_b200.LaunchConfiguration("Tile"))
         for call in range(2):
             y = y0.clone()
             _noalloc(M, x, y, alpha, beta)

@@ -63,7 +63,8 @@ class LaunchConfiguration:
     ``mapping`` is one of the ThreadsToSegmentsMapping names ("Fixed",
     "Warp", "Block", "BlockMerged", "DynamicGrouping") or one of the kernel
     names of SegmentsReductionKernels ("Scalar", "Vector", "Light",
-    "Adaptive", "Default").  ``threadsPerSegmentCount`` must be a positive
+    "Adaptive", "Default"), or "Tile" (CSR: the merge-path tile kernel
+    whatever the row lengths).  ``threadsPerSegmentCount`` must be a positive
     power of two (std::invalid_argument otherwise, as in the reference).
     """
 
@@ -89,6 +90,8 @@ class LaunchConfiguration:
             return capi.KERNEL_LIGHT, self.tps
         if m == "Adaptive":
             return capi.KERNEL_ADAPTIVE, 0
+        if m == "Tile":
+            return capi.KERNEL_TILE, 0
         raise ValueError(f"unknown launch mapping {m}")
 
 

@@ -24,7 +24,7 @@ OK, ERR_INVALID_ARGUMENT, ERR_OVERFLOW, ERR_CUDA, ERR_NOT_IMPLEMENTED, ERR_BREAK
 F32, F64 = 0, 1
 CSR, ELLPACK, SLICED_ELLPACK, CHUNKED_ELLPACK, BIELLPACK, ADAPTIVE_CSR = range(6)
 COLUMN_MAJOR, ROW_MAJOR = 0, 1
-KERNEL_DEFAULT, KERNEL_SCALAR, KERNEL_VECTOR, KERNEL_LIGHT, KERNEL_ADAPTIVE = range(5)
+KERNEL_DEFAULT, KERNEL_SCALAR, KERNEL_VECTOR, KERNEL_LIGHT, KERNEL_ADAPTIVE, KERNEL_TILE = range(6)
 (META_OFFSETS, META_SLICE_OFFSETS, META_SLICE_SEGMENT_SIZES, META_CH_SLICE_SIZE, META_CH_SLICE_CHUNK_SIZE,
  META_CH_SLICE_FIRST, META_CH_SLICE_POINTER, META_CH_SEGMENT_TO_CHUNK, META_CH_SEGMENT_TO_SLICE,
  META_CH_SEGMENT_POINTERS, META_CH_CHUNKS_TO_SEGMENTS, META_BI_PERMUTATION, META_BI_GROUP_POINTERS) = range(13)

@@ -7,8 +7,9 @@ on seeded synthetic matrices.  One JSON object per line on stdout.
     python -m tnl_b200.benchmarks solvers [--problem laplacian|diffusion] [--N 1024]
 
 spmv: every segment format and kernel on the 1024^2 5-point Laplacian
-(n = 1,048,576) and the power-law matrix (n = 4,194,304, Zipf 1.73 row
-lengths, cap 4096, seed 2).  GB/s counts algorithmic bytes, the same for
+(n = 1,048,576), the power-law matrix (n = 4,194,304, Zipf 1.73 row
+lengths, cap 4096, seed 2) and, with --configs diffusion3d, the 256^3
+7-point diffusion matrix (n = 16,777,216, GRF coefficients).  GB/s counts algorithmic bytes, the same for
 every format: nnz*(R+4) + (n+1)*4 + n*R (x) + n*R (y); padding therefore
 lowers the figure.  Device time per product from CUDA events: over K
 back-to-back products when the inputs exceed L2 (the power-law matrix), else
@@ -53,12 +54,15 @@ def _matrix(config: str):
         return g.laplacian_2d(1024)
     if config == "power_law":
         return g.power_law(4_194_304, 1.73, 4096, 2)
+    if config == "diffusion3d":
+        return g.diffusion_3d(256)
     raise ValueError(config)
 
 
 # (label, segments class name, launch mapping, threads per segment)
 SPMV_VARIANTS = [
-    ("CSR tile", "CSR", "Default", 0),
+    ("CSR default", "CSR", "Default", 0),
+    ("CSR tile", "CSR", "Tile", 0),
     ("CSR Light", "CSR", "Light", 0),
     ("CSR Scalar", "CSR", "Scalar", 0),
     ("CSR Vector", "CSR", "Vector", 32),

@@ -111,6 +111,7 @@ struct tnlb_segments {
    tnlb::DeviceBuffer offsets;  // int32[n+1]
    // CSR tile plan: merge-path coordinates of tile boundaries
    int32_t tiles = 0;
+   int32_t max_row = -1;  // longest row (CSR), -1 if unknown
    tnlb::DeviceBuffer tile_row;    // int32[tiles+1]
    tnlb::DeviceBuffer tile_nnz;    // int32[tiles+1]
    tnlb::DeviceBuffer carry_row;   // int32[tiles]   (scratch, per call)

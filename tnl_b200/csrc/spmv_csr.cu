@@ -173,7 +173,51 @@ __global__ void __launch_bounds__(256) k_csr_adaptive(const tnlb_acsr_block* __r
    }
 }
 
+// ------------------------------------------------------------ short rows
+
+// One thread per row for matrices whose rows hold at most L entries
+// (stencils, FSAI factors): all of a row's loads are issued before any is
+// used; consecutive threads read consecutive rows, so a warp's loads of
+// entry j share cache lines with those of entry j-1.  Sums in entry order.
+template <typename Real, int L>
+__global__ void __launch_bounds__(256) k_csr_short(const int32_t* __restrict__ rowptr, const int32_t* __restrict__ cols,
+                                                   const Real* __restrict__ vals, const Real* __restrict__ x,
+                                                   Real* __restrict__ y, int32_t n, Real alpha, Real beta,
+                                                   const int32_t* __restrict__ skip)
+{
+   if (skip && *skip) return;
+   const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+   if (r >= n) return;
+   const int32_t b = rowptr[r], e = rowptr[r + 1];
+   int32_t c[L];
+   Real v[L];
+#pragma unroll
+   for (int j = 0; j < L; j++) {
+      c[j] = -1;
+      v[j] = Real(0);
+      if (b + j < e) {
+         c[j] = __ldg(cols + b + j);
+         v[j] = __ldg(vals + b + j);
+      }
+   }
+   Real s = Real(0);
+#pragma unroll
+   for (int j = 0; j < L; j++)
+      if (c[j] >= 0) s += v[j] * __ldg(x + c[j]);
+   keep(y, (int32_t)r, s, alpha, beta);
+}
+
 // ---------------------------------------------------------------- tile
+
+__global__ void k_max_row(const int32_t* __restrict__ rowptr, int32_t n, int32_t* __restrict__ out)
+{
+   int32_t m = 0;
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+      m = max(m, rowptr[i + 1] - rowptr[i]);
+#pragma unroll
+   for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+   if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
 
 __global__ void k_tile_plan(const int32_t* __restrict__ rowptr, int32_t n, int64_t nnz, int32_t tiles,
                             int32_t* __restrict__ tile_row, int32_t* __restrict__ tile_nnz, int32_t* __restrict__ carry_row)
@@ -196,7 +240,9 @@ __global__ void k_tile_plan(const int32_t* __restrict__ rowptr, int32_t n, int64
 }
 
 // L2 policies: the streamed values and column indexes are evicted first, the
-// gathered vector is kept (it is re-read once per nonzero that points at it).
+// gathered vector is kept (it is re-read once per nonzero that points at it);
+// no load allocates in L1 (the tile kernel serves irregular matrices, whose
+// gathers rarely hit there).
 __device__ __forceinline__ uint64_t policy_evict_first()
 {
    uint64_t p;
@@ -230,13 +276,13 @@ __device__ __forceinline__ float ld_stream_hint(const float* a, uint64_t pol)
 __device__ __forceinline__ double ld_keep(const double* a, uint64_t pol)
 {
    double v;
-   asm("ld.global.nc.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(a), "l"(pol));
+   asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(a), "l"(pol));
    return v;
 }
 __device__ __forceinline__ float ld_keep(const float* a, uint64_t pol)
 {
    float v;
-   asm("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(a), "l"(pol));
+   asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(a), "l"(pol));
    return v;
 }
 
@@ -461,11 +507,24 @@ tnlb_status spmv_csr_t(const tnlb_segments* seg, const int32_t* cols, const Real
          return TNLB_OK;
       }
       case TNLB_KERNEL_DEFAULT:
+      case TNLB_KERNEL_TILE:
       default: {
          if (!full || seg->tiles == 0) {
             *launches = 1;
             return launch_vector<Real>(rowptr, cols, vals, x, y, begin, end, alpha, beta,
                                        light_tps(seg->elements, seg->n), st);
+         }
+         if (kernel != TNLB_KERNEL_TILE && seg->max_row >= 0 && seg->max_row <= 16) {
+            const unsigned g = grid_for(seg->n, 256);
+            if (seg->max_row <= 4)
+               k_csr_short<Real, 4><<<g, 256, 0, st>>>(rowptr, cols, vals, x, y, seg->n, alpha, beta, skip);
+            else if (seg->max_row <= 8)
+               k_csr_short<Real, 8><<<g, 256, 0, st>>>(rowptr, cols, vals, x, y, seg->n, alpha, beta, skip);
+            else
+               k_csr_short<Real, 16><<<g, 256, 0, st>>>(rowptr, cols, vals, x, y, seg->n, alpha, beta, skip);
+            TNLB_CHECK_LAUNCH();
+            *launches = 1;
+            return TNLB_OK;
          }
          k_csr_tile<Real><<<grid_for(seg->tiles, kTileThreads / 32), kTileThreads, 0, st>>>(
             rowptr, cols, vals, x, y, seg->tile_row.as<int32_t>(), seg->tile_nnz.as<int32_t>(), seg->tiles, seg->n,
@@ -496,7 +555,18 @@ tnlb_status build_csr_tile_plan(tnlb_segments* seg, cudaStream_t stream)
                                                               (int32_t)tiles, seg->tile_row.as<int32_t>(),
                                                               seg->tile_nnz.as<int32_t>(), seg->carry_row.as<int32_t>());
    TNLB_CHECK_LAUNCH();
+   // longest row, for the choice of the default kernel
+   DeviceBuffer mx;
+   TNLB_TRY_STATUS(mx.alloc(sizeof(int32_t)));
+   TNLB_CUDA_TRY(cudaMemsetAsync(mx.ptr, 0, sizeof(int32_t), stream));
+   if (seg->n > 0) {
+      k_max_row<<<grid_for(seg->n, 256 * 8), 256, 0, stream>>>(seg->offsets.as<int32_t>(), seg->n, mx.as<int32_t>());
+      TNLB_CHECK_LAUNCH();
+   }
+   int32_t h = 0;
+   TNLB_CUDA_TRY(cudaMemcpyAsync(&h, mx.ptr, sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
    TNLB_CUDA_TRY(cudaStreamSynchronize(stream));
+   seg->max_row = h;
    return TNLB_OK;
 }
 
