@@ -323,12 +323,9 @@ tnlb_status tnlb_true_residual(const tnlb_segments* seg, tnlb_real real, const i
 /* FP32-inner / FP64-outer iterative refinement (no counterpart in the
  * reference): the FP64 residual r = b - A x is formed with the FP64 values,
  * normalised, rounded to FP32 and solved with `inner_solver` (CG for SPD
- * matrices, FGMRES/GMRES/BiCGStab otherwise) on an FP32 copy of the values;
- * x += |r| d in FP64.  The first inner solve goes to relative residual
- * `inner_tolerance`; later ones only as far as the outer residual still
- * needs (half of target / current residual, clamped to
- * [inner_tolerance, 0.5]).  The outer residual is computed exactly as
- * tnlb_true_residual computes it.
+ * matrices, FGMRES/GMRES/BiCGStab otherwise) on an FP32 copy of the values
+ * to the inner solver's residue `inner_tolerance`; x += |r| d in FP64.  The
+ * outer residual is computed exactly as tnlb_true_residual computes it.
  * The inner preconditioner is `inner` (an FP32 preconditioner of this
  * matrix, e.g. a learned FSAI) or, when NULL, one of kind `inner_precond`
  * built from the FP32 values.  Stops

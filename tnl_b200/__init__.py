@@ -546,7 +546,7 @@ def true_residual(M: SparseMatrix, b: torch.Tensor, x: torch.Tensor) -> float:
     return out.value
 
 
-def solve_mixed(M: SparseMatrix, b: torch.Tensor, x: torch.Tensor, tol: float = 1e-8, inner_tol: float = 1e-6,
+def solve_mixed(M: SparseMatrix, b: torch.Tensor, x: torch.Tensor, tol: float = 1e-8, inner_tol: float = 1e-4,
                 max_outer: int = 50, max_iterations: int = 1000000000, inner: str | _Preconditioner = "jacobi",
                 solver: str = "cg", gmres_restart: int = 30) -> dict:
     """FP32 PCG inside FP64 iterative refinement (SPD matrices, FP64 matrix and vectors).

@@ -100,7 +100,7 @@ def time_spmv(M, x, y, lc, steps: int, flush: bool) -> float:
     return float(np.mean([a.elapsed_time(b) for a, b in ev]))
 
 
-def bench_spmv(configs, reals, steps: int, out=sys.stdout):
+def bench_spmv(configs, reals, steps: int, formats=None, out=sys.stdout):
     import tnl_b200 as t
     from . import generators as g
 
@@ -115,6 +115,8 @@ def bench_spmv(configs, reals, steps: int, out=sys.stdout):
             x = torch.tensor(xh, dtype=dt, device="cuda")
             y = torch.empty(A.n, dtype=dt, device="cuda")
             for label, seg, mapping, tps in SPMV_VARIANTS:
+                if formats and label not in formats:
+                    continue
                 rec = {"bench": "spmv", "config": config, "rows": A.n, "nnz": A.nnz, "real": real, "format": label}
                 try:
                     M = t.SparseMatrix(getattr(t, seg), dt).assign(A.rowptr, A.cols, A.vals)
@@ -183,7 +185,7 @@ def bench_solvers(problem: str, N: int, weights: str | None, out=sys.stdout):
 
     def mixed(name, inner, setup_ms):
         x = torch.zeros(n, dtype=torch.float64, device="cuda")
-        r, ms = _timed(lambda: t.solve_mixed(M, b, x, tol=1e-8, inner_tol=1e-6, inner=inner))
+        r, ms = _timed(lambda: t.solve_mixed(M, b, x, tol=1e-8, inner_tol=1e-4, inner=inner))
         rec = dict(base, method=name, converged=r["converged"], iterations=r["inner_iterations"],
                    outer_iterations=r["outer_iterations"], solve_ms=ms, setup_ms=setup_ms,
                    true_residual=t.true_residual(M, b, x), speedup_vs_fp64_jacobi=jac["solve_ms"] / ms)
@@ -208,13 +210,15 @@ def main(argv=None):
     a.add_argument("--configs", default="laplacian,power_law")
     a.add_argument("--reals", default="f64,f32")
     a.add_argument("--steps", type=int, default=50)
+    a.add_argument("--formats", default="", help="comma-separated labels, e.g. 'CSR default,SlicedEllpack'")
     b = sub.add_parser("solvers")
     b.add_argument("--problem", default="laplacian", choices=["laplacian", "diffusion"])
     b.add_argument("--N", type=int, default=1024)
     b.add_argument("--weights", default=str(Path(__file__).resolve().parent / "weights" / "lfsai_diffusion.npy"))
     args = ap.parse_args(argv)
     if args.cmd == "spmv":
-        bench_spmv(args.configs.split(","), args.reals.split(","), args.steps)
+        bench_spmv(args.configs.split(","), args.reals.split(","), args.steps,
+                   [f for f in args.formats.split(",") if f])
     else:
         bench_solvers(args.problem, args.N, args.weights)
     return 0

@@ -1548,10 +1548,6 @@ tnlb_status solve_mixed_cg(const tnlb_segments* seg, const int32_t* cols, const 
       const double rn = std::sqrt(h[0]), bn = std::sqrt(h[1]);
       resid = bn > 0 ? rn / bn : 0.0;
       if (bn == 0 || resid < prm.convergence_residue || o == max_outer) break;
-      // The correction only has to take the residual from `resid` to the
-      // target: after the first solve (to inner_tol) the inner tolerance is
-      // loosened to half that ratio, never below inner_tol, never above 0.5.
-      ip.convergence_residue = std::min(0.5, std::max(inner_tol, 0.5 * prm.convergence_residue / resid));
       // unit-norm FP32 residual, FP32 correction
       k_resid_to_f32<<<vec_grid(n), kRedThreads, 0, st>>>(n, b, r64.as<double>(), 1.0 / rn, r32.as<float>());
       TNLB_CUDA_TRY(cudaMemsetAsync(d32.ptr, 0, sizeof(float) * n, st));
