@@ -8,7 +8,7 @@
 //        (Matrices/SparseMatrix.h:41-57, SparseMatrixBase.h:1020-1035);
 //   TNL::Algorithms::Segments::{CSR, Ellpack, SlicedEllpack, ChunkedEllpack,
 //        BiEllpack, AdaptiveCSR}, LaunchConfiguration, ElementsOrganization;
-//   TNL::Solvers::Linear::{CG, BICGStab, GMRES} (+ FGMRES) with setMatrix,
+//   TNL::Solvers::Linear::{CG, BICGStab, GMRES, TFQMR, BICGStabL, IDRs} (+ FGMRES) with setMatrix,
 //        setPreconditioner, setup, setConvergenceResidue, setMaxIterations,
 //        solve, getIterations, getResidue (Solvers/Linear/LinearSolver.h);
 //   TNL::Solvers::Linear::Preconditioners::{Diagonal, ILU0} (+ FSAI) with
@@ -360,7 +360,8 @@ public:
       precond_ = pre ? pre->handle() : nullptr;
       keep_ = pre;
    }
-   // setup(ParameterContainer) keys (IterativeSolver.hpp:14-36, GMRES.hpp:20-37, BICGStab.hpp:14-21)
+   // setup(ParameterContainer) keys (IterativeSolver.hpp:14-36, GMRES.hpp:20-37, BICGStab.hpp:14-21,
+   // BICGStabL.hpp:14-33, IDRs.hpp:18-34)
    bool setup(const std::map<std::string, std::string>& prm, const std::string& prefix = "")
    {
       auto get = [&](const char* k) -> const std::string* {
@@ -380,6 +381,9 @@ public:
       if (auto v = get("gmres-restarting-step-min")) p_.gmres_restarting_step_min = std::stoi(*v);
       if (auto v = get("gmres-restarting-step-max")) p_.gmres_restarting_step_max = std::stoi(*v);
       if (auto v = get("bicgstab-exact-residue")) p_.bicgstab_exact_residue = (*v == "true" || *v == "1");
+      if (auto v = get("bicgstab-ell")) p_.bicgstab_ell = std::stoi(*v);
+      if (auto v = get("idr-s")) p_.idr_s = std::stoi(*v);
+      if (auto v = get("idr-residual-smoothing")) p_.idr_residual_smoothing = (*v == "true" || *v == "1");
       return true;
    }
    void setConvergenceResidue(double r) { p_.convergence_residue = r; }
@@ -419,6 +423,12 @@ template <typename Matrix>
 using GMRES = SolverBase<Matrix, TNLB_SOLVER_GMRES>;
 template <typename Matrix>
 using FGMRES = SolverBase<Matrix, TNLB_SOLVER_FGMRES>;
+template <typename Matrix>
+using TFQMR = SolverBase<Matrix, TNLB_SOLVER_TFQMR>;
+template <typename Matrix>
+using BICGStabL = SolverBase<Matrix, TNLB_SOLVER_BICGSTABL>;
+template <typename Matrix>
+using IDRs = SolverBase<Matrix, TNLB_SOLVER_IDRS>;
 
 }  // namespace Linear
 }  // namespace Solvers

@@ -252,11 +252,18 @@ tnlb_status tnlb_dot(tnlb_real real, int64_t n, const void* d_a, const void* d_b
  * preconditioned basis is kept; residues are unpreconditioned).  No
  * counterpart in the reference; its orthogonalisation and Givens steps follow
  * GMRES.hpp:280-347, 731-770. */
+/* TFQMR (Solvers/Linear/TFQMR.hpp:12-113), BiCGStab(ell)
+ * (Solvers/Linear/BICGStabL.hpp:36-242) and IDR(s)
+ * (Solvers/Linear/IDRs.hpp:50-250): the other solvers of the reference's
+ * linear-solver benchmark. */
 typedef enum {
    TNLB_SOLVER_CG = 0,
    TNLB_SOLVER_BICGSTAB = 1,
    TNLB_SOLVER_GMRES = 2,
-   TNLB_SOLVER_FGMRES = 3
+   TNLB_SOLVER_FGMRES = 3,
+   TNLB_SOLVER_TFQMR = 4,
+   TNLB_SOLVER_BICGSTABL = 5,
+   TNLB_SOLVER_IDRS = 6
 } tnlb_solver_kind;
 /* Preconditioners: none, Diagonal (Jacobi), ILU0, and factorised sparse
  * approximate inverses (no counterpart in the reference; Kolotilina-Yeremin
@@ -275,8 +282,9 @@ typedef struct tnlb_precond tnlb_precond;
 typedef enum { TNLB_GMRES_CGS = 0, TNLB_GMRES_CGSR = 1, TNLB_GMRES_MGS = 2, TNLB_GMRES_MGSR = 3, TNLB_GMRES_CWY = 4 } tnlb_gmres_variant;
 
 /* Solver parameters: the setup() keys of IterativeSolver.hpp:14-36,
- * GMRES.hpp:20-37 and BICGStab.hpp:14-21, with the reference's defaults
- * filled in by tnlb_solver_params_default. */
+ * GMRES.hpp:20-37, BICGStab.hpp:14-21, BICGStabL.hpp:14-33 and
+ * IDRs.hpp:18-34, with the reference's defaults filled in by
+ * tnlb_solver_params_default. */
 typedef struct {
    int32_t max_iterations;       /* max-iterations, default 1e9 */
    int32_t min_iterations;       /* min-iterations, default 0 */
@@ -289,7 +297,9 @@ typedef struct {
    int32_t gmres_restarting_step_max; /* default 3 */
    int32_t bicgstab_exact_residue;    /* default 0 */
    int32_t spmv_kernel;          /* tnlb_kernel used by the solver's products */
-   int32_t reserved;
+   int32_t bicgstab_ell;         /* bicgstab-ell (BiCGStab(ell)), default 1 */
+   int32_t idr_s;                /* idr-s (IDR(s) shadow space), default 4 */
+   int32_t idr_residual_smoothing; /* idr-residual-smoothing, default 0 */
 } tnlb_solver_params;
 
 /* Result of a solve: getIterations(), getResidue() and the bool of solve(). */

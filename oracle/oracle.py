@@ -112,6 +112,10 @@ class Oracle:
             ("orc_gmres", [i32, p, p, p, C.c_int, i32, C.c_int, p, p, C.POINTER(SolverState)], C.c_int),
             ("orc_fgmres", [i32, p, p, p, C.c_int, i32, C.c_int, p, p, C.POINTER(SolverState)], C.c_int),
             ("orc_gmres_cwy", [i32, p, p, p, C.c_int, i32, p, p, C.POINTER(SolverState)], C.c_int),
+            ("orc_tfqmr", [i32, p, p, p, C.c_int, p, p, C.POINTER(SolverState)], C.c_int),
+            ("orc_bicgstabl", [i32, p, p, p, C.c_int, C.c_int, C.c_int, p, p, C.POINTER(SolverState)], C.c_int),
+            ("orc_idrs", [i32, p, p, p, C.c_int, C.c_int, C.c_int, p, p, p, C.POINTER(SolverState)], C.c_int),
+            ("orc_idrs_shadow", [i32, i32, p], None),
             ("orc_true_residual", [i32, p, p, p, p, p], f64),
             ("orc_ilu0_factor", [i32, p, p, p, p, p, p, p, p, p], C.c_int),
             ("orc_prec_apply", [i32, p, p, p, C.c_int, p, p], C.c_int),
@@ -225,8 +229,14 @@ class Oracle:
         S.historyCap = history
         return S, hist
 
+    def idrs_shadow(self, n: int, s: int) -> np.ndarray:
+        """The IDR(s) shadow space (n x s, column-major) as the reference draws it."""
+        P = np.zeros(n * s)
+        self.L.orc_idrs_shadow(n, s, P.ctypes.data)
+        return P
+
     def solve(self, solver: str, A, b, x0=None, precond: int = 1, tol=1e-8, maxit=100000, gmres_m=30,
-              gmres_reorth=2, bicgstab_exact=False, history=0):
+              gmres_reorth=2, bicgstab_exact=False, history=0, ell=1, idr_s=4, idr_smoothing=False):
         rowptr, cols, vals = _i32(A.rowptr), _i32(A.cols), np.ascontiguousarray(A.vals, np.float64)
         b = np.ascontiguousarray(b, np.float64)
         x = np.zeros(A.n) if x0 is None else np.array(x0, np.float64, copy=True)
@@ -238,6 +248,15 @@ class Oracle:
             ok = self.L.orc_bicgstab(*args, precond, int(bicgstab_exact), b.ctypes.data, x.ctypes.data, C.byref(S))
         elif solver == "gmres":
             ok = self.L.orc_gmres(*args, precond, gmres_m, gmres_reorth, b.ctypes.data, x.ctypes.data, C.byref(S))
+        elif solver == "tfqmr":
+            ok = self.L.orc_tfqmr(*args, precond, b.ctypes.data, x.ctypes.data, C.byref(S))
+        elif solver == "bicgstabl":
+            ok = self.L.orc_bicgstabl(*args, precond, ell, int(bicgstab_exact), b.ctypes.data, x.ctypes.data,
+                                      C.byref(S))
+        elif solver == "idrs":
+            P = self.idrs_shadow(A.n, idr_s)
+            ok = self.L.orc_idrs(*args, precond, idr_s, int(idr_smoothing), P.ctypes.data, b.ctypes.data,
+                                 x.ctypes.data, C.byref(S))
         elif solver == "gmres_cwy":
             ok = self.L.orc_gmres_cwy(*args, precond, gmres_m, b.ctypes.data, x.ctypes.data, C.byref(S))
         elif solver == "fgmres":
@@ -295,6 +314,7 @@ class Reference:
             ("ref_spmv_f64", [i32, i32, i32, i32, p, p, p, p, p, f64, f64, i32, i32, i32], f64),
             ("ref_spmv_f32", [i32, i32, i32, i32, p, p, p, p, p, f64, f64, i32, i32, i32], f64),
             ("ref_solve", [i32, i32, i32, p, p, p, p, p, f64, i32, i32, i32, i32, p, p, p], C.c_int),
+            ("ref_solve_ext", [i32, i32, i32, p, p, p, p, p, f64, i32, i32, i32, p, p, p], C.c_int),
             ("ref_prec_apply", [i32, p, p, p, i32, p, p], C.c_int),
             ("ref_omp_threads", [], C.c_int),
             ("ref_set_threads", [C.c_int], None),
@@ -396,12 +416,21 @@ class Reference:
         return y, t
 
     def solve(self, solver: str, A, b, x0=None, precond: int = 1, tol=1e-8, maxit=100000, gmres_m=30,
-              gmres_variant: int = 3, bicgstab_exact=False):
-        kind = {"cg": 0, "bicgstab": 1, "gmres": 2}[solver]
+              gmres_variant: int = 3, bicgstab_exact=False, ell=1, idr_s=4, idr_smoothing=False):
         rowptr, cols, vals = _i32(A.rowptr), _i32(A.cols), np.ascontiguousarray(A.vals, np.float64)
         b = np.ascontiguousarray(b, np.float64)
         x = np.zeros(A.n) if x0 is None else np.array(x0, np.float64, copy=True)
         it, res, sec = C.c_int(), C.c_double(), C.c_double()
+        if solver in ("tfqmr", "bicgstabl", "idrs"):
+            kind = {"tfqmr": 3, "bicgstabl": 4, "idrs": 5}[solver]
+            param = ell if solver == "bicgstabl" else idr_s
+            flag = int(bicgstab_exact) if solver == "bicgstabl" else int(idr_smoothing)
+            ok = self.L.ref_solve_ext(kind, precond, A.n, rowptr.ctypes.data, cols.ctypes.data, vals.ctypes.data,
+                                      b.ctypes.data, x.ctypes.data, tol, maxit, param, flag, C.byref(it),
+                                      C.byref(res), C.byref(sec))
+            return {"x": x, "converged": ok == 1, "status": ok, "iterations": it.value, "residue": res.value,
+                    "seconds": sec.value}
+        kind = {"cg": 0, "bicgstab": 1, "gmres": 2}[solver]
         ok = self.L.ref_solve(kind, precond, A.n, rowptr.ctypes.data, cols.ctypes.data, vals.ctypes.data, b.ctypes.data,
                               x.ctypes.data, tol, maxit, gmres_m, gmres_variant, int(bicgstab_exact), C.byref(it),
                               C.byref(res), C.byref(sec))

@@ -27,6 +27,9 @@
 #include <TNL/Containers/Vector.h>
 #include <TNL/Matrices/SparseMatrix.h>
 #include <TNL/Solvers/Linear/BICGStab.h>
+#include <TNL/Solvers/Linear/BICGStabL.h>
+#include <TNL/Solvers/Linear/IDRs.h>
+#include <TNL/Solvers/Linear/TFQMR.h>
 #include <TNL/Solvers/Linear/CG.h>
 #include <TNL/Solvers/Linear/GMRES.h>
 #include <TNL/Solvers/Linear/Preconditioners/Diagonal.h>
@@ -455,6 +458,92 @@ ref_solve( int solver,
       p.addParameter< String >( "gmres-variant", names[ gmresVariant ] );
       p.addParameter< int >( "gmres-restarting-min", gmresRestart );
       p.addParameter< int >( "gmres-restarting-max", gmresRestart );
+      S.setup( p );
+      ok = run( S );
+   }
+   for( int i = 0; i < n; i++ )
+      x[ i ] = xv[ i ];
+   return ok;
+}
+
+// Solve A x = b with TNL's TFQMR (solver 3), BICGStabL (4: param = ell,
+// flag = bicgstab-exact-residue) or IDRs (5: param = s, flag =
+// idr-residual-smoothing), with no preconditioner (0), Diagonal (1) or
+// ILU0 (2).  Returns 1 if solve() returned true, 0 if false, -2 if it threw.
+int
+ref_solve_ext( int solver,
+               int precond,
+               int n,
+               const int* rowptr,
+               const int* cols,
+               const double* vals,
+               const double* b,
+               double* x,
+               double tol,
+               int maxIterations,
+               int param,
+               int flag,
+               int* iterations,
+               double* residue,
+               double* seconds )
+{
+   using M = Mat< double, Seg::CSR >;
+   auto A = std::make_shared< M >();
+   makeCSR( *A, n, n, rowptr, cols, vals );
+   Containers::Vector< double, Host, int > bv( n ), xv( n );
+   for( int i = 0; i < n; i++ ) {
+      bv[ i ] = b[ i ];
+      xv[ i ] = x[ i ];
+   }
+   auto run = [ & ]( auto& S ) -> int
+   {
+      S.setMatrix( A );
+      S.setConvergenceResidue( tol );
+      S.setMaxIterations( maxIterations );
+      std::shared_ptr< Solvers::Linear::Preconditioners::Diagonal< M > > jac;
+      std::shared_ptr< Solvers::Linear::Preconditioners::ILU0< M > > ilu;
+      auto t0 = std::chrono::steady_clock::now();
+      if( precond == 1 ) {
+         jac = std::make_shared< Solvers::Linear::Preconditioners::Diagonal< M > >();
+         jac->update( A );
+         S.setPreconditioner( jac );
+      }
+      else if( precond == 2 ) {
+         ilu = std::make_shared< Solvers::Linear::Preconditioners::ILU0< M > >();
+         ilu->update( A );
+         S.setPreconditioner( ilu );
+      }
+      int ok;
+      try {
+         ok = S.solve( bv, xv ) ? 1 : 0;
+      }
+      catch( const std::exception& ) {
+         ok = -2;
+      }
+      auto t1 = std::chrono::steady_clock::now();
+      *seconds = std::chrono::duration< double >( t1 - t0 ).count();
+      *iterations = S.getIterations();
+      *residue = S.getResidue();
+      return ok;
+   };
+   int ok = 0;
+   if( solver == 3 ) {
+      Solvers::Linear::TFQMR< M > S;
+      ok = run( S );
+   }
+   else if( solver == 4 ) {
+      Solvers::Linear::BICGStabL< M > S;
+      Config::ParameterContainer p;
+      p.addParameter< int >( "bicgstab-ell", param );
+      p.addParameter< bool >( "bicgstab-exact-residue", flag != 0 );
+      S.setup( p );
+      ok = run( S );
+   }
+   else {
+      Solvers::Linear::IDRs< M > S;
+      Config::ParameterContainer p;
+      p.addParameter< int >( "idr-s", param );
+      p.addParameter< bool >( "idr-residual-smoothing", flag != 0 );
       S.setup( p );
       ok = run( S );
    }

@@ -1402,3 +1402,407 @@ double orc_true_residual(int32_t n, const int32_t* rowptr, const int32_t* cols, 
    free(t);
    return sqrt(num) / sqrt(den);
 }
+
+/* ------------------------------------------------------------------------
+ * The other Krylov solvers of the reference's linear-solver benchmark.
+ * ---------------------------------------------------------------------- */
+
+static void prec_apply_any(const orc_prec* P, const double* b, double* x)
+{
+   if (P->kind == 0) {
+      if (x != b) memmove(x, b, sizeof(double) * (size_t)P->n);
+   }
+   else
+      prec_apply(P, b, x);
+}
+
+/* TFQMR::solve (Solvers/Linear/TFQMR.hpp:12-113), left-preconditioned;
+ * the residue is the quasi-residual bound tau*sqrt(iter+1)/||M^-1 b||.
+ * Returns 1 on convergence, 0 otherwise. */
+int orc_tfqmr(int32_t n, const int32_t* rowptr, const int32_t* cols, const double* vals, int precond,
+              const double* b, double* x, orc_solver_state* S)
+{
+   orc_csr A = {n, rowptr, cols, vals};
+   orc_prec P;
+   prec_setup(&P, &A, precond);
+   const size_t nb = sizeof(double) * (size_t)n;
+   double *d = calloc(n, sizeof(double)), *r = malloc(nb), *w = malloc(nb), *u = malloc(nb), *v = malloc(nb);
+   double *r_ast = malloc(nb), *Au = malloc(nb), *M_tmp = malloc(nb);
+   int ok = 1;
+   double b_norm;
+   S->iterations = 0;
+   if (precond) {
+      prec_apply(&P, b, M_tmp);
+      b_norm = l2(M_tmp, n);
+      csr_mv(&A, x, M_tmp);
+      for (int32_t i = 0; i < n; i++) M_tmp[i] = b[i] - M_tmp[i];
+      prec_apply(&P, M_tmp, r);
+   }
+   else {
+      b_norm = l2(b, n);
+      csr_mv(&A, x, r);
+      for (int32_t i = 0; i < n; i++) r[i] = b[i] - r[i];
+   }
+   if (b_norm == 0) {
+      for (int32_t i = 0; i < n; i++) x[i] = 0;
+      goto done;
+   }
+#define PMV(SRC, DST)                     \
+   do {                                   \
+      if (precond) {                      \
+         csr_mv(&A, (SRC), M_tmp);        \
+         prec_apply(&P, M_tmp, (DST));    \
+      }                                   \
+      else                                \
+         csr_mv(&A, (SRC), (DST));        \
+   } while (0)
+   memcpy(w, r, nb);
+   memcpy(u, r, nb);
+   PMV(u, Au);
+   memcpy(v, Au, nb);
+   double tau = l2(r, n), theta = 0.0, eta = 0.0;
+   memcpy(r_ast, r, nb);
+   double rho = dot(r_ast, r, n), alpha = 0.0;
+   S->iterations = 0;
+   set_residue(S, tau / b_norm);
+   while (next_iteration(S)) {
+      const int32_t iter = S->iterations;
+      if (iter % 2 == 1)
+         alpha = rho / dot(v, r_ast, n);
+      else
+         PMV(u, Au);
+      for (int32_t i = 0; i < n; i++) w[i] = w[i] - alpha * Au[i];
+      const double dc = theta * theta * eta / alpha;
+      for (int32_t i = 0; i < n; i++) d[i] = u[i] + dc * d[i];
+      const double w_norm = l2(w, n);
+      theta = w_norm / tau;
+      const double c = 1.0 / sqrt(1.0 + theta * theta);
+      tau = tau * theta * c;
+      eta = c * c * alpha;
+      for (int32_t i = 0; i < n; i++) x[i] = x[i] + eta * d[i];
+      set_residue(S, tau * sqrt((double)(iter + 1)) / b_norm);
+      if (iter > S->minIterations && S->residue < S->convergenceResidue) break;
+      if (iter % 2 == 0) {
+         const double rho_new = dot(w, r_ast, n);
+         const double beta = rho_new / rho;
+         rho = rho_new;
+         for (int32_t i = 0; i < n; i++) u[i] = w[i] + beta * u[i];
+         for (int32_t i = 0; i < n; i++) v[i] = beta * Au[i] + (beta * beta) * v[i];
+         PMV(u, Au);
+         for (int32_t i = 0; i < n; i++) v[i] = v[i] + Au[i];
+      }
+      else
+         for (int32_t i = 0; i < n; i++) u[i] = u[i] - alpha * v[i];
+   }
+   ok = check_convergence(S);
+done:
+   free(d);
+   free(r);
+   free(w);
+   free(u);
+   free(v);
+   free(r_ast);
+   free(Au);
+   free(M_tmp);
+   prec_free(&P);
+   return ok;
+}
+
+/* BICGStabL::solve (Solvers/Linear/BICGStabL.hpp:36-242): BiCGStab(ell),
+ * left-preconditioned; R and U hold ell+1 columns of length n; T, sigma and
+ * the g vectors live on the host.  Note sigma[j] = (r_j, r_j) for j >= 1 but
+ * sigma[0] = ||r_0|| (as in the reference).  `exact` selects the exact
+ * preconditioned residue for stopping.  Returns 1 on convergence, 0
+ * otherwise, -2 on a NaN initial residue (the reference throws). */
+int orc_bicgstabl(int32_t n, const int32_t* rowptr, const int32_t* cols, const double* vals, int precond, int ell,
+                  int exact, const double* b, double* x, orc_solver_state* S)
+{
+   orc_csr A = {n, rowptr, cols, vals};
+   orc_prec P;
+   prec_setup(&P, &A, precond);
+   const size_t nb = sizeof(double) * (size_t)n;
+   double* R = calloc((size_t)n * (ell + 1), sizeof(double));
+   double* U = calloc((size_t)n * (ell + 1), sizeof(double));
+   double *r_ast = malloc(nb), *M_tmp = malloc(nb), *res_tmp = malloc(nb);
+   double* T = calloc((size_t)ell * ell, sizeof(double));
+   double *sigma = calloc(ell + 1, sizeof(double)), *g0 = calloc(ell + 1, sizeof(double));
+   double *g1 = calloc(ell + 1, sizeof(double)), *g2 = calloc(ell + 1, sizeof(double));
+   int ok = 1;
+   double b_norm;
+   S->iterations = 0;
+   if (precond) {
+      prec_apply(&P, b, M_tmp);
+      b_norm = l2(M_tmp, n);
+   }
+   else
+      b_norm = l2(b, n);
+   if (b_norm == 0) {
+      for (int32_t i = 0; i < n; i++) x[i] = 0;
+      goto done;
+   }
+#define RESID(RV)                                                       \
+   do {                                                                 \
+      if (precond) {                                                    \
+         csr_mv(&A, x, M_tmp);                                          \
+         for (int32_t i = 0; i < n; i++) M_tmp[i] = b[i] - M_tmp[i];    \
+         prec_apply(&P, M_tmp, (RV));                                   \
+      }                                                                 \
+      else {                                                            \
+         csr_mv(&A, x, (RV));                                           \
+         for (int32_t i = 0; i < n; i++) (RV)[i] = b[i] - (RV)[i];      \
+      }                                                                 \
+   } while (0)
+   double* r0 = R;
+   double* u0 = U;
+   RESID(r0);
+   sigma[0] = l2(r0, n);
+   if (isnan(sigma[0])) {
+      ok = -2;
+      goto done;
+   }
+   for (int32_t i = 0; i < n; i++) r_ast[i] = r0[i];
+   for (int32_t i = 0; i < n; i++) r_ast[i] = r_ast[i] / sigma[0];
+   double rho_0 = 1.0, rho_1, alpha = 0.0, beta, gamma, omega = 1.0;
+   S->iterations = 0;
+   set_residue(S, sigma[0] / b_norm);
+   while (check_next(S)) {
+      rho_0 = -omega * rho_0;
+      for (int j = 0; j < ell; j++) {
+         next_iteration(S);
+         double* rj = R + (size_t)j * n;
+         rho_1 = dot(r_ast, rj, n);
+         beta = alpha * rho_1 / rho_0;
+         rho_0 = rho_1;
+         for (int c = 0; c <= j; c++)
+            for (int32_t i = 0; i < n; i++)
+               U[(size_t)c * n + i] = 1.0 * R[(size_t)c * n + i] + (-beta) * U[(size_t)c * n + i];
+         PMV(U + (size_t)j * n, U + (size_t)(j + 1) * n);
+         gamma = dot(r_ast, U + (size_t)(j + 1) * n, n);
+         alpha = rho_0 / gamma;
+         for (int c = 0; c <= j; c++)
+            for (int32_t i = 0; i < n; i++)
+               R[(size_t)c * n + i] = 1.0 * R[(size_t)c * n + i] + (-alpha) * U[(size_t)(c + 1) * n + i];
+         PMV(R + (size_t)j * n, R + (size_t)(j + 1) * n);
+         for (int32_t i = 0; i < n; i++) x[i] = x[i] + alpha * u0[i];
+      }
+      for (int j = 1; j <= ell; j++) {
+         double* rj = R + (size_t)j * n;
+         for (int i = 1; i < j; i++) {
+            const double* ri = R + (size_t)i * n;
+            const int ij = (i - 1) + (j - 1) * ell;
+            T[ij] = dot(ri, rj, n) / sigma[i];
+            for (int32_t t = 0; t < n; t++) rj[t] = rj[t] - T[ij] * ri[t];
+         }
+         sigma[j] = dot(rj, rj, n);
+         g1[j] = dot(r0, rj, n) / sigma[j];
+      }
+      omega = g1[ell];
+      for (int j = ell; j >= 1; j--) {
+         g0[j] = g1[j];
+         for (int i = j + 1; i <= ell; i++) g0[j] -= T[(j - 1) + (i - 1) * ell] * g0[i];
+      }
+      for (int j = 1; j < ell; j++) {
+         g2[j] = g0[j + 1];
+         for (int i = j + 1; i < ell; i++) g2[j] += T[(j - 1) + (i - 1) * ell] * g0[i + 1];
+      }
+      g2[0] = g0[1];
+      for (int32_t t = 0; t < n; t++) {
+         double acc = 0;
+         for (int c = 0; c < ell; c++) acc += R[(size_t)c * n + t] * g2[c];
+         x[t] = acc + x[t];
+      }
+      for (int32_t t = 0; t < n; t++) {
+         double acc = 0;
+         for (int c = 0; c < ell; c++) acc += R[(size_t)(c + 1) * n + t] * g1[c + 1];
+         r0[t] = -1.0 * acc + r0[t];
+      }
+      for (int32_t t = 0; t < n; t++) {
+         double acc = 0;
+         for (int c = 0; c < ell; c++) acc += U[(size_t)(c + 1) * n + t] * g0[c + 1];
+         u0[t] = -1.0 * acc + u0[t];
+      }
+      if (exact) {
+         RESID(res_tmp);
+         sigma[0] = l2(res_tmp, n);
+      }
+      else
+         sigma[0] = l2(r0, n);
+      set_residue(S, sigma[0] / b_norm);
+   }
+   ok = check_convergence(S);
+#undef RESID
+done:
+   free(R);
+   free(U);
+   free(r_ast);
+   free(M_tmp);
+   free(res_tmp);
+   free(T);
+   free(sigma);
+   free(g0);
+   free(g1);
+   free(g2);
+   prec_free(&P);
+   return ok;
+}
+
+/* LU_sequential_factorize / LU_sequential_solve
+ * (Matrices/Factorization/LUsequential.h:14-72): no pivoting; A is m x m,
+ * row-major with leading dimension ld. */
+static void lu_solve_small(double* A, int m, int ld, const double* bvec, double* xvec)
+{
+   for (int k = 0; k < m; k++) {
+      const double pivot = A[k * ld + k];
+      for (int j = k + 1; j < m; j++) {
+         const double factor = A[j * ld + k] / pivot;
+         A[j * ld + k] = factor;
+         for (int i = k + 1; i < m; i++) A[j * ld + i] = A[j * ld + i] - factor * A[k * ld + i];
+      }
+   }
+   for (int k = 0; k < m; k++) xvec[k] = bvec[k];
+   for (int k = 1; k < m; k++)
+      for (int j = 0; j < k; j++) xvec[k] -= A[k * ld + j] * xvec[j];
+   for (int k = m - 1; k >= 0; k--) {
+      for (int j = m - 1; j > k; j--) xvec[k] -= A[k * ld + j] * xvec[j];
+      xvec[k] /= A[k * ld + k];
+   }
+}
+
+/* IDRs::solve (Solvers/Linear/IDRs.hpp:50-250): IDR(s) with the shadow
+ * space P (n x s, column-major) drawn by the caller as IDRs::setSize does
+ * (:270-300; orc_idrs_shadow); the preconditioner is applied on the right
+ * of the update directions (psolve), residues are unpreconditioned.
+ * `smoothing` enables residual smoothing.  Returns 1 on convergence, 0
+ * otherwise (including the reference's early `return false` on a zero
+ * M(k,k) or omega), -2 on a NaN initial residue (the reference throws). */
+int orc_idrs(int32_t n, const int32_t* rowptr, const int32_t* cols, const double* vals, int precond, int s,
+             int smoothing, const double* Pm, const double* b, double* x, orc_solver_state* S)
+{
+   orc_csr A = {n, rowptr, cols, vals};
+   orc_prec Pc;
+   prec_setup(&Pc, &A, precond);
+   const size_t nb = sizeof(double) * (size_t)n;
+   double* G = calloc((size_t)n * s, sizeof(double));
+   double* U = calloc((size_t)n * s, sizeof(double));
+   double *r = malloc(nb), *v = malloc(nb), *t = malloc(nb), *x_s = malloc(nb), *r_s = malloc(nb);
+   double* M = calloc((size_t)s * s, sizeof(double));
+   double *f = calloc(s, sizeof(double)), *c = calloc(s, sizeof(double)), *Msub = calloc((size_t)s * s, sizeof(double));
+   int ok = 1;
+   S->iterations = 0;
+   const double b_norm = l2(b, n);
+   if (b_norm == 0) {
+      for (int32_t i = 0; i < n; i++) x[i] = 0;
+      goto done;
+   }
+   csr_mv(&A, x, r);
+   for (int32_t i = 0; i < n; i++) r[i] = b[i] - r[i];
+   double r_norm = l2(r, n);
+   if (isnan(r_norm)) {
+      ok = -2;
+      goto done;
+   }
+   const double angle = 0.7;
+   double omega = 1.0;
+   for (int i = 0; i < s; i++) M[i * s + i] = 1;
+   if (smoothing) {
+      memcpy(x_s, x, nb);
+      memcpy(r_s, r, nb);
+   }
+#define SMOOTH()                                                                  \
+   do {                                                                           \
+      if (smoothing) {                                                            \
+         for (int32_t q = 0; q < n; q++) t[q] = r_s[q] - r[q];                    \
+         const double gam = dot(t, r_s, n) / dot(t, t, n);                        \
+         for (int32_t q = 0; q < n; q++) r_s[q] = r_s[q] - gam * t[q];            \
+         for (int32_t q = 0; q < n; q++) x_s[q] = x_s[q] - gam * (x_s[q] - x[q]); \
+         r_norm = l2(r_s, n);                                                     \
+      }                                                                           \
+   } while (0)
+   S->iterations = 0;
+   set_residue(S, r_norm / b_norm);
+   while (check_next(S)) {
+      for (int i = 0; i < s; i++) f[i] = dot(Pm + (size_t)i * n, r, n);
+      for (int k = 0; k < s; k++) {
+         double* Uk = U + (size_t)k * n;
+         double* Gk = G + (size_t)k * n;
+         const int m = s - k;
+         for (int i = k; i < s; i++)
+            for (int j = k; j < s; j++) Msub[(i - k) * s + (j - k)] = M[i * s + j];
+         lu_solve_small(Msub, m, s, f + k, c);
+         for (int32_t q = 0; q < n; q++) {
+            double acc = 0;
+            for (int i = 0; i < m; i++) acc += G[(size_t)(k + i) * n + q] * c[i];
+            v[q] = -1.0 * acc + r[q];
+         }
+         prec_apply_any(&Pc, v, v);
+         for (int32_t q = 0; q < n; q++) {
+            double acc = 0;
+            for (int i = 0; i < m; i++) acc += U[(size_t)(k + i) * n + q] * c[i];
+            Uk[q] = acc;
+         }
+         for (int32_t q = 0; q < n; q++) Uk[q] = Uk[q] + omega * v[q];
+         csr_mv(&A, Uk, Gk);
+         for (int i = 0; i < k; i++) {
+            const double* Pi = Pm + (size_t)i * n;
+            const double* Ui = U + (size_t)i * n;
+            const double* Gi = G + (size_t)i * n;
+            const double alpha = dot(Pi, Gk, n) / M[i * s + i];
+            for (int32_t q = 0; q < n; q++) Uk[q] = Uk[q] - alpha * Ui[q];
+            for (int32_t q = 0; q < n; q++) Gk[q] = Gk[q] - alpha * Gi[q];
+         }
+         for (int i = k; i < s; i++) M[i * s + k] = dot(Pm + (size_t)i * n, Gk, n);
+         if (M[k * s + k] == 0) {
+            ok = 0;
+            goto done;
+         }
+         const double beta = f[k] / M[k * s + k];
+         for (int32_t q = 0; q < n; q++) x[q] = x[q] + beta * Uk[q];
+         for (int32_t q = 0; q < n; q++) r[q] = r[q] - beta * Gk[q];
+         r_norm = l2(r, n);
+         SMOOTH();
+         set_residue(S, r_norm / b_norm);
+         if (!next_iteration(S)) {
+            if (smoothing) memcpy(x, x_s, nb);
+            ok = check_convergence(S);
+            goto done;
+         }
+         if (k < s - 1)
+            for (int i = k + 1; i < s; i++) f[i] = f[i] - beta * M[i * s + k];
+      }
+      prec_apply_any(&Pc, r, v);
+      csr_mv(&A, v, t);
+      const double t_norm = l2(t, n);
+      const double tr = dot(t, r, n);
+      const double rho = fabs(tr / (t_norm * r_norm));
+      omega = tr / (t_norm * t_norm);
+      if (rho < angle) omega = omega * angle / rho;
+      if (omega == 0) {
+         ok = 0;
+         goto done;
+      }
+      for (int32_t q = 0; q < n; q++) x[q] = x[q] + omega * v[q];
+      for (int32_t q = 0; q < n; q++) r[q] = r[q] - omega * t[q];
+      r_norm = l2(r, n);
+      SMOOTH();
+      set_residue(S, r_norm / b_norm);
+      next_iteration(S);
+   }
+   if (smoothing) memcpy(x, x_s, nb);
+   ok = check_convergence(S);
+#undef SMOOTH
+#undef PMV
+done:
+   free(G);
+   free(U);
+   free(r);
+   free(v);
+   free(t);
+   free(x_s);
+   free(r_s);
+   free(M);
+   free(f);
+   free(c);
+   free(Msub);
+   prec_free(&Pc);
+   return ok;
+}

@@ -114,8 +114,9 @@ def main() -> None:
         arrays[f"prob/{pname}/vals"] = A.vals
         arrays[f"prob/{pname}/b"] = b
         for solver, pre in (("cg", 1), ("cg", 2), ("bicgstab", 1), ("gmres", 1), ("gmres", 2), ("gmres_cwy", 1),
-                            ("gmres_cwy", 2)):
-            # "gmres" is the MGSR variant, "gmres_cwy" the Householder (CWY) one
+                            ("gmres_cwy", 2), ("tfqmr", 1), ("tfqmr", 2), ("bicgstabl", 1), ("idrs", 1), ("idrs", 2)):
+            # "gmres" is the MGSR variant, "gmres_cwy" the Householder (CWY) one;
+            # BiCGStab(ell) and IDR(s) with their defaults ell = 1, s = 4
             variant = 4 if solver == "gmres_cwy" else 3
             r = R.solve(solver.split("_")[0], A, b, precond=pre, tol=1e-8, maxit=20000, gmres_m=30,
                         gmres_variant=variant)

@@ -139,7 +139,7 @@ def test_solvers_match_golden(oracle, golden, pname):
         pre = int(pre)
         r = oracle.solve(solver, A, b, precond=pre, tol=1e-8, maxit=20000, gmres_m=30, gmres_reorth=2)
         assert r["converged"] == ref["converged"], key
-        if solver == "bicgstab":
+        if solver in ("bicgstab", "bicgstabl"):
             # BiCGStab amplifies the reference's non-reproducible OpenMP
             # reductions: the reference itself moves by up to ~10% of its
             # iteration count between thread counts (1..8 threads).
@@ -148,7 +148,13 @@ def test_solvers_match_golden(oracle, golden, pname):
         else:
             assert r["iterations"] == ref["iterations"], key
             assert r["residue"] == pytest.approx(ref["residue"], rel=1e-6), key
-            assert np.allclose(r["x"], golden.get(f"solve/{key}/x"), rtol=1e-9, atol=1e-12), key
+            xr = golden.get(f"solve/{key}/x")
+            if solver in ("tfqmr", "idrs"):
+                # their recurrences amplify the reference's blocked dot-product
+                # order more than CG / GMRES do
+                assert np.allclose(r["x"], xr, rtol=1e-6, atol=1e-9 * np.abs(xr).max()), key
+            else:
+                assert np.allclose(r["x"], xr, rtol=1e-9, atol=1e-12), key
 
 
 def test_preconditioners_match_reference(oracle, reference):
@@ -201,3 +207,36 @@ def test_lfsai_reference_fd():
             assert fd == pytest.approx(grad[i], rel=1e-5, abs=1e-10)
     finally:
         R.ROUND = old
+
+
+@pytest.mark.parametrize("solver,kw", [("tfqmr", {}), ("bicgstabl", {"ell": 1}), ("bicgstabl", {"ell": 3}),
+                                       ("bicgstabl", {"ell": 2, "bicgstab_exact": True}), ("idrs", {"idr_s": 4}),
+                                       ("idrs", {"idr_s": 2, "idr_smoothing": True})])
+def test_more_krylov_match_reference(oracle, reference, solver, kw):
+    """TFQMR, BiCGStab(ell) and IDR(s) restated in the oracle against the
+    reference's own solvers.  The reference sums dot products in a blocked
+    order (and in OpenMP threads), the oracle sequentially: TFQMR and IDR(s)
+    stay within 2 % of the reference's iterations; BiCGStab(ell), like
+    BiCGStab, within 10 %."""
+    probs = [g.laplacian_2d(32), g.diffusion_2d(33, 0.1, 2.0, 6), g.convection_diffusion_3d(10)]
+    for A in probs:
+        b = g.uniform_vector(A.n, 1)
+        for pre in (1, 2):
+            r = reference.solve(solver, A, b, precond=pre, tol=1e-8, maxit=20000, **kw)
+            o = oracle.solve(solver, A, b, precond=pre, tol=1e-8, maxit=20000, **kw)
+            assert r["converged"] and o["converged"], (solver, kw, pre)
+            slack = max(5, r["iterations"] // 10) if solver == "bicgstabl" else max(2, r["iterations"] // 50)
+            assert abs(r["iterations"] - o["iterations"]) <= slack, (solver, kw, pre, r["iterations"], o["iterations"])
+            assert np.allclose(o["x"], r["x"], rtol=1e-5, atol=1e-6 * np.abs(r["x"]).max()), (solver, kw, pre)
+
+
+def test_idrs_shadow_space_matches_reference_draws(oracle, reference):
+    """The IDR(s) shadow space is drawn from std::mt19937 / std::normal_distribution
+    as the reference does: with a preconditioner that makes the solve short, the
+    oracle reproduces the reference's iterates to rounding."""
+    A = g.laplacian_2d(32)
+    b = g.uniform_vector(A.n, 1)
+    r = reference.solve("idrs", A, b, precond=2, tol=1e-8, maxit=100, idr_s=4)
+    o = oracle.solve("idrs", A, b, precond=2, tol=1e-8, maxit=100, idr_s=4)
+    assert r["iterations"] == o["iterations"]
+    assert np.allclose(o["x"], r["x"], rtol=1e-10, atol=1e-12)

@@ -31,7 +31,8 @@ from .generators import CSRMatrix  # noqa: F401
 __all__ = [
     "CSR", "Ellpack", "SlicedEllpack", "ChunkedEllpack", "BiEllpack", "AdaptiveCSR", "SparseMatrix",
     "LaunchConfiguration", "ColumnMajorOrder", "RowMajorOrder", "CSRMatrix", "check", "BackendRuntimeError",
-    "CG", "BICGStab", "GMRES", "FGMRES", "Diagonal", "ILU0", "FSAI", "FSAI2", "solve_mixed", "true_residual",
+    "CG", "BICGStab", "GMRES", "FGMRES", "TFQMR", "BICGStabL", "IDRs", "Diagonal", "ILU0", "FSAI", "FSAI2",
+    "solve_mixed", "true_residual",
 ]
 
 ColumnMajorOrder = capi.COLUMN_MAJOR
@@ -477,7 +478,7 @@ class _LinearSolver:
 
     def setup(self, parameters: dict, prefix: str = "") -> bool:
         """setup(ParameterContainer) with the reference's keys (IterativeSolver.hpp:14-36,
-        GMRES.hpp:20-37, BICGStab.hpp:14-21)."""
+        GMRES.hpp:20-37, BICGStab.hpp:14-21, BICGStabL.hpp:14-33, IDRs.hpp:18-34)."""
         p = self.params
         g = lambda k: parameters.get(prefix + k)  # noqa: E731
         if g("max-iterations") is not None:
@@ -498,6 +499,12 @@ class _LinearSolver:
                 setattr(p, field, int(g(key)))
         if g("bicgstab-exact-residue") is not None:
             p.bicgstab_exact_residue = int(bool(g("bicgstab-exact-residue")))
+        if g("bicgstab-ell") is not None:
+            p.bicgstab_ell = int(g("bicgstab-ell"))
+        if g("idr-s") is not None:
+            p.idr_s = int(g("idr-s"))
+        if g("idr-residual-smoothing") is not None:
+            p.idr_residual_smoothing = int(bool(g("idr-residual-smoothing")))
         return True
 
     def solve(self, b: torch.Tensor, x: torch.Tensor) -> bool:
@@ -530,6 +537,24 @@ class BICGStab(_LinearSolver):
 class GMRES(_LinearSolver):
     """Solvers::Linear::GMRES (restarted, left-preconditioned; CGS, CGSR, MGS, MGSR)."""
     KIND = capi.SOLVER_GMRES
+
+
+class TFQMR(_LinearSolver):
+    """Solvers::Linear::TFQMR (left-preconditioned; the stopping residue is
+    the quasi-residual bound of TFQMR.hpp:86)."""
+    KIND = capi.SOLVER_TFQMR
+
+
+class BICGStabL(_LinearSolver):
+    """Solvers::Linear::BICGStabL: BiCGStab(ell), keys "bicgstab-ell" and
+    "bicgstab-exact-residue"."""
+    KIND = capi.SOLVER_BICGSTABL
+
+
+class IDRs(_LinearSolver):
+    """Solvers::Linear::IDRs: IDR(s), keys "idr-s" and "idr-residual-smoothing";
+    residues are unpreconditioned, as in the reference."""
+    KIND = capi.SOLVER_IDRS
 
 
 class FGMRES(_LinearSolver):

@@ -63,7 +63,7 @@ class SolverParams(C.Structure):
         ("divergence_residue", C.c_double), ("gmres_variant", C.c_int32), ("gmres_restarting_min", C.c_int32),
         ("gmres_restarting_max", C.c_int32), ("gmres_restarting_step_min", C.c_int32),
         ("gmres_restarting_step_max", C.c_int32), ("bicgstab_exact_residue", C.c_int32), ("spmv_kernel", C.c_int32),
-        ("reserved", C.c_int32),
+        ("bicgstab_ell", C.c_int32), ("idr_s", C.c_int32), ("idr_residual_smoothing", C.c_int32),
     ]
 
 
@@ -72,7 +72,7 @@ class SolveResult(C.Structure):
                 ("status_detail", C.c_int32), ("reserved", C.c_int32)]
 
 
-SOLVER_CG, SOLVER_BICGSTAB, SOLVER_GMRES, SOLVER_FGMRES = range(4)
+SOLVER_CG, SOLVER_BICGSTAB, SOLVER_GMRES, SOLVER_FGMRES, SOLVER_TFQMR, SOLVER_BICGSTABL, SOLVER_IDRS = range(7)
 PRECOND_NONE, PRECOND_JACOBI, PRECOND_ILU0, PRECOND_FSAI, PRECOND_FSAI2 = range(5)
 GMRES_CGS, GMRES_CGSR, GMRES_MGS, GMRES_MGSR, GMRES_CWY = range(5)
 

@@ -281,6 +281,9 @@ void tnlb_solver_params_default(tnlb_solver_params* p)
    p->gmres_restarting_step_max = 3;  // GMRES.h:229
    p->bicgstab_exact_residue = 0;     // BICGStab.h:102
    p->spmv_kernel = TNLB_KERNEL_DEFAULT;
+   p->bicgstab_ell = 1;               // BICGStabL.hpp:17
+   p->idr_s = 4;                      // IDRs.hpp:21
+   p->idr_residual_smoothing = 0;     // IDRs.hpp:22
 }
 
 static tnlb_status check_solve_args(const tnlb_segments* seg, tnlb_real real, const void* b, void* x)
@@ -300,7 +303,7 @@ tnlb_status tnlb_solve_preconditioned(tnlb_solver_kind solver, const tnlb_precon
    clear_error();
    TNLB_TRY_STATUS(check_solve_args(seg, real, d_b, d_x));
    TNLB_REQUIRE(result != nullptr, TNLB_ERR_INVALID_ARGUMENT, "null result");
-   TNLB_REQUIRE(solver >= TNLB_SOLVER_CG && solver <= TNLB_SOLVER_FGMRES, TNLB_ERR_INVALID_ARGUMENT, "unknown solver");
+   TNLB_REQUIRE(solver >= TNLB_SOLVER_CG && solver <= TNLB_SOLVER_IDRS, TNLB_ERR_INVALID_ARGUMENT, "unknown solver");
    tnlb_solver_params p;
    tnlb_solver_params_default(&p);
    if (params) p = *params;
@@ -347,7 +350,7 @@ tnlb_status tnlb_solve_mixed(const tnlb_solver_params* params, const tnlb_segmen
    TNLB_REQUIRE(inner_tolerance > 0 && inner_tolerance < 1, TNLB_ERR_INVALID_ARGUMENT,
                 "inner tolerance must lie in (0, 1)");
    TNLB_REQUIRE(max_outer >= 0, TNLB_ERR_INVALID_ARGUMENT, "negative max_outer");
-   TNLB_REQUIRE(inner_solver >= TNLB_SOLVER_CG && inner_solver <= TNLB_SOLVER_FGMRES, TNLB_ERR_INVALID_ARGUMENT,
+   TNLB_REQUIRE(inner_solver >= TNLB_SOLVER_CG && inner_solver <= TNLB_SOLVER_IDRS, TNLB_ERR_INVALID_ARGUMENT,
                 "unknown inner solver");
    TNLB_REQUIRE(inner || (inner_precond >= TNLB_PRECOND_NONE && inner_precond <= TNLB_PRECOND_FSAI2),
                 TNLB_ERR_INVALID_ARGUMENT, "unknown preconditioner");

@@ -16,6 +16,7 @@
 // substitution) on the host in FP64, as the reference does.
 #include <cfloat>
 #include <cmath>
+#include <random>
 #include <vector>
 
 #include "internal.cuh"
@@ -1368,6 +1369,497 @@ tnlb_status gmres_solve(const Ctx<Real>& c, const Precond<Real>& P, const tnlb_s
    return TNLB_OK;
 }
 
+// ------------------------------------------ TFQMR, BiCGStab(ell), IDR(s)
+
+// x_s = x_s - gamma (x_s - x) (residual smoothing of IDR(s))
+template <typename Real>
+__global__ void k_smooth_x(int64_t n, Real gamma, const Real* __restrict__ x, Real* __restrict__ xs)
+{
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+      xs[i] = xs[i] - gamma * (xs[i] - x[i]);
+}
+
+// Host-driven vector operations shared by the solvers below: each dot or
+// norm is one deterministic grid reduction read back to the host.
+template <typename Real>
+struct VecOps {
+   const Ctx<Real>& c;
+   Work& W;
+   unsigned G;
+   double hs[2];
+   VecOps(const Ctx<Real>& c_, Work& W_) : c(c_), W(W_), G(vec_grid(c_.n)) {}
+   tnlb_status dot(const Real* a, const Real* b, double* out)
+   {
+      k_dots<Real><<<G, kRedThreads, 0, c.st>>>(c.n, a, b, nullptr, nullptr, W.red(), W.scratch.as<double>());
+      TNLB_CHECK_LAUNCH();
+      TNLB_CUDA_TRY(cudaMemcpyAsync(hs, W.scratch.ptr, sizeof(hs), cudaMemcpyDeviceToHost, c.st));
+      TNLB_CUDA_TRY(cudaStreamSynchronize(c.st));
+      *out = hs[0];
+      return TNLB_OK;
+   }
+   tnlb_status norm(const Real* a, double* out)
+   {
+      TNLB_TRY_STATUS(dot(a, a, out));
+      *out = std::sqrt(*out);
+      return TNLB_OK;
+   }
+   // y = a x + b y
+   tnlb_status axpby(double a, const Real* x, double b, Real* y)
+   {
+      k_axpby<Real><<<G, kRedThreads, 0, c.st>>>(c.n, (Real)a, x, (Real)b, y);
+      TNLB_CHECK_LAUNCH();
+      return TNLB_OK;
+   }
+   tnlb_status copy(Real* dst, const Real* src)
+   {
+      TNLB_CUDA_TRY(cudaMemcpyAsync(dst, src, sizeof(Real) * c.n, cudaMemcpyDeviceToDevice, c.st));
+      return TNLB_OK;
+   }
+};
+
+// The stopping rule of IterativeSolver (IterativeSolver.hpp:98-143) on host
+// scalars; next() checks, then counts the iteration, as nextIteration does.
+struct HostStop {
+   const tnlb_solver_params& prm;
+   int it = 0;
+   double residue = 0;
+   explicit HostStop(const tnlb_solver_params& p) : prm(p) {}
+   bool check() const
+   {
+      return !(std::isnan(residue) || it > prm.max_iterations ||
+               (residue > prm.divergence_residue && it >= prm.min_iterations) ||
+               (residue < prm.convergence_residue && it >= prm.min_iterations));
+   }
+   bool next()
+   {
+      const bool r = check();
+      it++;
+      return r;
+   }
+   void finish(tnlb_solve_result* res, bool ok = true) const
+   {
+      res->iterations = it;
+      res->residue = residue;
+      res->converged = ok && check_convergence(residue, it, prm.max_iterations, prm.min_iterations,
+                                               prm.convergence_residue, prm.divergence_residue);
+      res->status_detail = 0;
+   }
+};
+
+// TFQMR (Solvers/Linear/TFQMR.hpp:12-113): left-preconditioned; the
+// stopping residue is the quasi-residual bound tau sqrt(iter+1) / ||M^-1 b||.
+template <typename Real>
+tnlb_status tfqmr_solve(const Ctx<Real>& c, const Precond<Real>& P, const tnlb_solver_params& prm, const Real* b,
+                        Real* x, tnlb_solve_result* res)
+{
+   const int64_t n = c.n;
+   Work W;
+   TNLB_TRY_STATUS(W.alloc());
+   DeviceBuffer d, r, w, u, v, r_ast, Au, M_tmp;
+   for (auto* q : {&d, &r, &w, &u, &v, &r_ast, &Au, &M_tmp}) TNLB_TRY_STATUS(q->alloc(sizeof(Real) * n));
+   VecOps<Real> V(c, W);
+   const bool pre = P.kind != TNLB_PRECOND_NONE;
+   auto pmv = [&](const Real* src, Real* dst) -> tnlb_status {
+      if (!pre) return c.spmv(src, dst);
+      TNLB_TRY_STATUS(c.spmv(src, M_tmp.as<Real>()));
+      return P.apply(n, M_tmp.as<Real>(), dst, c.st);
+   };
+   HostStop S(prm);
+   double b_norm;
+   if (pre) {
+      TNLB_TRY_STATUS(P.apply(n, b, M_tmp.as<Real>(), c.st));
+      TNLB_TRY_STATUS(V.norm(M_tmp.as<Real>(), &b_norm));
+      TNLB_TRY_STATUS(V.copy(M_tmp.as<Real>(), b));
+      TNLB_TRY_STATUS(c.spmv(x, M_tmp.as<Real>(), -1.0, 1.0));
+      TNLB_TRY_STATUS(P.apply(n, M_tmp.as<Real>(), r.as<Real>(), c.st));
+   }
+   else {
+      TNLB_TRY_STATUS(V.norm(b, &b_norm));
+      TNLB_TRY_STATUS(V.copy(r.as<Real>(), b));
+      TNLB_TRY_STATUS(c.spmv(x, r.as<Real>(), -1.0, 1.0));
+   }
+   if (b_norm == 0) {
+      TNLB_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(Real) * n, c.st));
+      TNLB_CUDA_TRY(cudaStreamSynchronize(c.st));
+      *res = tnlb_solve_result{1, 0, 0.0, 0, 0};
+      return TNLB_OK;
+   }
+   TNLB_TRY_STATUS(V.copy(w.as<Real>(), r.as<Real>()));
+   TNLB_TRY_STATUS(V.copy(u.as<Real>(), r.as<Real>()));
+   TNLB_TRY_STATUS(pmv(u.as<Real>(), Au.as<Real>()));
+   TNLB_TRY_STATUS(V.copy(v.as<Real>(), Au.as<Real>()));
+   TNLB_CUDA_TRY(cudaMemsetAsync(d.ptr, 0, sizeof(Real) * n, c.st));
+   double tau, theta = 0.0, eta = 0.0, rho, alpha = 0.0;
+   TNLB_TRY_STATUS(V.norm(r.as<Real>(), &tau));
+   TNLB_TRY_STATUS(V.copy(r_ast.as<Real>(), r.as<Real>()));
+   TNLB_TRY_STATUS(V.dot(r_ast.as<Real>(), r.as<Real>(), &rho));
+   S.residue = tau / b_norm;
+   while (S.next()) {
+      const int iter = S.it;
+      if (iter % 2 == 1) {
+         double vr;
+         TNLB_TRY_STATUS(V.dot(v.as<Real>(), r_ast.as<Real>(), &vr));
+         alpha = rho / vr;
+      }
+      else
+         TNLB_TRY_STATUS(pmv(u.as<Real>(), Au.as<Real>()));
+      TNLB_TRY_STATUS(V.axpby(-alpha, Au.as<Real>(), 1.0, w.as<Real>()));
+      TNLB_TRY_STATUS(V.axpby(1.0, u.as<Real>(), theta * theta * eta / alpha, d.as<Real>()));
+      double w_norm;
+      TNLB_TRY_STATUS(V.norm(w.as<Real>(), &w_norm));
+      theta = w_norm / tau;
+      const double cc = 1.0 / std::sqrt(1.0 + theta * theta);
+      tau = tau * theta * cc;
+      eta = cc * cc * alpha;
+      TNLB_TRY_STATUS(V.axpby(eta, d.as<Real>(), 1.0, x));
+      S.residue = tau * std::sqrt((double)(iter + 1)) / b_norm;
+      if (iter > prm.min_iterations && S.residue < prm.convergence_residue) break;
+      if (iter % 2 == 0) {
+         double rho_new;
+         TNLB_TRY_STATUS(V.dot(w.as<Real>(), r_ast.as<Real>(), &rho_new));
+         const double beta = rho_new / rho;
+         rho = rho_new;
+         TNLB_TRY_STATUS(V.axpby(1.0, w.as<Real>(), beta, u.as<Real>()));
+         TNLB_TRY_STATUS(V.axpby(beta, Au.as<Real>(), beta * beta, v.as<Real>()));
+         TNLB_TRY_STATUS(pmv(u.as<Real>(), Au.as<Real>()));
+         TNLB_TRY_STATUS(V.axpby(1.0, Au.as<Real>(), 1.0, v.as<Real>()));
+      }
+      else
+         TNLB_TRY_STATUS(V.axpby(-alpha, v.as<Real>(), 1.0, u.as<Real>()));
+   }
+   TNLB_CUDA_TRY(cudaStreamSynchronize(c.st));
+   S.finish(res);
+   return TNLB_OK;
+}
+
+// BiCGStab(ell) (Solvers/Linear/BICGStabL.hpp:36-242): R and U hold ell+1
+// columns (256-byte aligned) on the device; T, sigma and the g vectors are
+// small and live on the host, as in the reference.
+template <typename Real>
+tnlb_status bicgstabl_solve(const Ctx<Real>& c, const Precond<Real>& P, const tnlb_solver_params& prm, const Real* b,
+                            Real* x, tnlb_solve_result* res)
+{
+   const int64_t n = c.n;
+   const int ell = prm.bicgstab_ell;
+   TNLB_REQUIRE(ell >= 1 && ell <= 32, TNLB_ERR_INVALID_ARGUMENT, "bicgstab-ell must lie in 1..32");
+   const int64_t ld = (n + 31) / 32 * 32;
+   Work W;
+   TNLB_TRY_STATUS(W.alloc());
+   DeviceBuffer Rb, Ub, r_ast, M_tmp, res_tmp, cdev;
+   TNLB_TRY_STATUS(Rb.alloc(sizeof(Real) * ld * (ell + 1)));
+   TNLB_TRY_STATUS(Ub.alloc(sizeof(Real) * ld * (ell + 1)));
+   for (auto* q : {&r_ast, &M_tmp, &res_tmp}) TNLB_TRY_STATUS(q->alloc(sizeof(Real) * n));
+   TNLB_TRY_STATUS(cdev.alloc(sizeof(double) * 128));
+   Real* R = Rb.as<Real>();
+   Real* U = Ub.as<Real>();
+   auto Rc = [&](int j) { return R + (int64_t)j * ld; };
+   auto Uc = [&](int j) { return U + (int64_t)j * ld; };
+   VecOps<Real> V(c, W);
+   const bool pre = P.kind != TNLB_PRECOND_NONE;
+   auto pmv = [&](const Real* src, Real* dst) -> tnlb_status {
+      if (!pre) return c.spmv(src, dst);
+      TNLB_TRY_STATUS(c.spmv(src, M_tmp.as<Real>()));
+      return P.apply(n, M_tmp.as<Real>(), dst, c.st);
+   };
+   auto compute_residue = [&](Real* out) -> tnlb_status {
+      Real* tgt = pre ? M_tmp.as<Real>() : out;
+      TNLB_TRY_STATUS(V.copy(tgt, b));
+      TNLB_TRY_STATUS(c.spmv(x, tgt, -1.0, 1.0));
+      if (pre) TNLB_TRY_STATUS(P.apply(n, M_tmp.as<Real>(), out, c.st));
+      return TNLB_OK;
+   };
+   // out = alpha * Y[:, 0:cols] coef + beta * in
+   auto gemv = [&](const Real* Y, int cols, const double* coef, double alpha, const Real* in, double beta,
+                   Real* out) -> tnlb_status {
+      TNLB_CUDA_TRY(cudaMemcpyAsync(cdev.ptr, coef, sizeof(double) * cols, cudaMemcpyHostToDevice, c.st));
+      k_gemv_cols<Real><<<V.G, kRedThreads, 0, c.st>>>(n, ld, cols, Y, cdev.as<double>(), alpha, in, beta, out, -1);
+      TNLB_CHECK_LAUNCH();
+      return TNLB_OK;
+   };
+   HostStop S(prm);
+   double b_norm;
+   if (pre) {
+      TNLB_TRY_STATUS(P.apply(n, b, M_tmp.as<Real>(), c.st));
+      TNLB_TRY_STATUS(V.norm(M_tmp.as<Real>(), &b_norm));
+   }
+   else
+      TNLB_TRY_STATUS(V.norm(b, &b_norm));
+   if (b_norm == 0) {
+      TNLB_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(Real) * n, c.st));
+      TNLB_CUDA_TRY(cudaStreamSynchronize(c.st));
+      *res = tnlb_solve_result{1, 0, 0.0, 0, 0};
+      return TNLB_OK;
+   }
+   std::vector<double> T((size_t)ell * ell, 0.0), sigma(ell + 1), g0(ell + 1), g1(ell + 1), g2(ell + 1);
+   TNLB_TRY_STATUS(compute_residue(Rc(0)));
+   TNLB_TRY_STATUS(V.norm(Rc(0), &sigma[0]));
+   TNLB_REQUIRE(!std::isnan(sigma[0]), TNLB_ERR_INVALID_ARGUMENT, "BiCGstab(ell): initial residue is NAN");
+   TNLB_TRY_STATUS(V.copy(r_ast.as<Real>(), Rc(0)));
+   TNLB_TRY_STATUS(V.axpby(0.0, r_ast.as<Real>(), 1.0 / sigma[0], r_ast.as<Real>()));
+   TNLB_CUDA_TRY(cudaMemsetAsync(Uc(0), 0, sizeof(Real) * n, c.st));
+   double rho_0 = 1.0, rho_1, alpha = 0.0, beta, gamma, omega = 1.0;
+   S.residue = sigma[0] / b_norm;
+   while (S.check()) {
+      rho_0 = -omega * rho_0;
+      for (int j = 0; j < ell; j++) {
+         S.next();
+         TNLB_TRY_STATUS(V.dot(r_ast.as<Real>(), Rc(j), &rho_1));
+         beta = alpha * rho_1 / rho_0;
+         rho_0 = rho_1;
+         for (int q = 0; q <= j; q++) TNLB_TRY_STATUS(V.axpby(1.0, Rc(q), -beta, Uc(q)));
+         TNLB_TRY_STATUS(pmv(Uc(j), Uc(j + 1)));
+         TNLB_TRY_STATUS(V.dot(r_ast.as<Real>(), Uc(j + 1), &gamma));
+         alpha = rho_0 / gamma;
+         for (int q = 0; q <= j; q++) TNLB_TRY_STATUS(V.axpby(-alpha, Uc(q + 1), 1.0, Rc(q)));
+         TNLB_TRY_STATUS(pmv(Rc(j), Rc(j + 1)));
+         TNLB_TRY_STATUS(V.axpby(alpha, Uc(0), 1.0, x));
+      }
+      for (int j = 1; j <= ell; j++) {
+         for (int i = 1; i < j; i++) {
+            const int ij = (i - 1) + (j - 1) * ell;
+            double d;
+            TNLB_TRY_STATUS(V.dot(Rc(i), Rc(j), &d));
+            T[ij] = d / sigma[i];
+            TNLB_TRY_STATUS(V.axpby(-T[ij], Rc(i), 1.0, Rc(j)));
+         }
+         TNLB_TRY_STATUS(V.dot(Rc(j), Rc(j), &sigma[j]));
+         double d;
+         TNLB_TRY_STATUS(V.dot(Rc(0), Rc(j), &d));
+         g1[j] = d / sigma[j];
+      }
+      omega = g1[ell];
+      for (int j = ell; j >= 1; j--) {
+         g0[j] = g1[j];
+         for (int i = j + 1; i <= ell; i++) g0[j] -= T[(j - 1) + (i - 1) * ell] * g0[i];
+      }
+      for (int j = 1; j < ell; j++) {
+         g2[j] = g0[j + 1];
+         for (int i = j + 1; i < ell; i++) g2[j] += T[(j - 1) + (i - 1) * ell] * g0[i + 1];
+      }
+      g2[0] = g0[1];
+      TNLB_TRY_STATUS(gemv(Rc(0), ell, g2.data(), 1.0, x, 1.0, x));
+      TNLB_TRY_STATUS(gemv(Rc(1), ell, g1.data() + 1, -1.0, Rc(0), 1.0, Rc(0)));
+      TNLB_TRY_STATUS(gemv(Uc(1), ell, g0.data() + 1, -1.0, Uc(0), 1.0, Uc(0)));
+      if (prm.bicgstab_exact_residue) {
+         TNLB_TRY_STATUS(compute_residue(res_tmp.as<Real>()));
+         TNLB_TRY_STATUS(V.norm(res_tmp.as<Real>(), &sigma[0]));
+      }
+      else
+         TNLB_TRY_STATUS(V.norm(Rc(0), &sigma[0]));
+      S.residue = sigma[0] / b_norm;
+   }
+   TNLB_CUDA_TRY(cudaStreamSynchronize(c.st));
+   S.finish(res);
+   return TNLB_OK;
+}
+
+// The shadow space of IDR(s), drawn as IDRs::setSize does
+// (Solvers/Linear/IDRs.hpp:270-300): std::mt19937 seeded 0,
+// std::normal_distribution(0, 1), s columns of length n; then, for each
+// column i and each j < i, P_i = P_i - (P_i, P_j) (the scalar subtracted from
+// every entry, as the reference does) and P_i /= ||P_i||.
+template <typename Real>
+std::vector<Real> idrs_shadow(int64_t n, int s)
+{
+   std::vector<Real> P((size_t)n * s);
+   std::mt19937 rng;
+   rng.seed(0);
+   std::normal_distribution<Real> dist(0, 1);
+   for (auto& p : P) p = dist(rng);
+   for (int i = 0; i < s; i++) {
+      Real* Pi = P.data() + (size_t)i * n;
+      for (int j = 0; j < i; j++) {
+         const Real* Pj = P.data() + (size_t)j * n;
+         double d = 0;
+         for (int64_t q = 0; q < n; q++) d += (double)Pi[q] * (double)Pj[q];
+         for (int64_t q = 0; q < n; q++) Pi[q] = (Real)(Pi[q] - d);
+      }
+      double nn = 0;
+      for (int64_t q = 0; q < n; q++) nn += (double)Pi[q] * (double)Pi[q];
+      nn = std::sqrt(nn);
+      for (int64_t q = 0; q < n; q++) Pi[q] = (Real)(Pi[q] / nn);
+   }
+   return P;
+}
+
+// IDR(s) (Solvers/Linear/IDRs.hpp:50-250): residues unpreconditioned, the
+// preconditioner applied to the update directions; P, G and U are n x s on
+// the device, M, f and the small LU solves (LUsequential.h) on the host.
+template <typename Real>
+tnlb_status idrs_solve(const Ctx<Real>& c, const Precond<Real>& Pc, const tnlb_solver_params& prm, const Real* b,
+                       Real* x, tnlb_solve_result* res)
+{
+   const int64_t n = c.n;
+   const int s = prm.idr_s;
+   TNLB_REQUIRE(s >= 1 && s <= 32, TNLB_ERR_INVALID_ARGUMENT, "idr-s must lie in 1..32");
+   const bool smoothing = prm.idr_residual_smoothing != 0;
+   const int64_t ld = (n + 31) / 32 * 32;
+   Work W;
+   TNLB_TRY_STATUS(W.alloc());
+   DeviceBuffer Pb, Gb, Ub, r, v, pv, t, x_s, r_s, cdev, hdev;
+   for (auto* q : {&Pb, &Gb, &Ub}) TNLB_TRY_STATUS(q->alloc(sizeof(Real) * ld * s));
+   for (auto* q : {&r, &v, &pv, &t, &x_s, &r_s}) TNLB_TRY_STATUS(q->alloc(sizeof(Real) * n));
+   TNLB_TRY_STATUS(cdev.alloc(sizeof(double) * 128));
+   TNLB_TRY_STATUS(hdev.alloc(sizeof(double) * 128));
+   Real* Pd = Pb.as<Real>();
+   Real* Gd = Gb.as<Real>();
+   Real* Ud = Ub.as<Real>();
+   auto col = [&](Real* Y, int j) { return Y + (int64_t)j * ld; };
+   VecOps<Real> V(c, W);
+   const bool pre = Pc.kind != TNLB_PRECOND_NONE;
+   {
+      const std::vector<Real> Ph = idrs_shadow<Real>(n, s);
+      for (int j = 0; j < s; j++)
+         TNLB_CUDA_TRY(cudaMemcpyAsync(col(Pd, j), Ph.data() + (size_t)j * n, sizeof(Real) * n,
+                                       cudaMemcpyHostToDevice, c.st));
+      TNLB_CUDA_TRY(cudaStreamSynchronize(c.st));
+   }
+   TNLB_CUDA_TRY(cudaMemsetAsync(Gd, 0, sizeof(Real) * ld * s, c.st));
+   TNLB_CUDA_TRY(cudaMemsetAsync(Ud, 0, sizeof(Real) * ld * s, c.st));
+   // P_[first:first+cnt]^T a -> host
+   std::vector<double> hv(s);
+   auto ptv = [&](int first, int cnt, const Real* a) -> tnlb_status {
+      k_gmres_vtw<Real><<<V.G, kRedThreads, 0, c.st>>>(n, ld, cnt, col(Pd, first), a, W.partials.as<double>(),
+                                                      W.counter.as<unsigned>() + 1, hdev.as<double>());
+      TNLB_CHECK_LAUNCH();
+      TNLB_CUDA_TRY(cudaMemcpyAsync(hv.data(), hdev.ptr, sizeof(double) * cnt, cudaMemcpyDeviceToHost, c.st));
+      TNLB_CUDA_TRY(cudaStreamSynchronize(c.st));
+      return TNLB_OK;
+   };
+   auto gemv = [&](const Real* Y, int cols, const double* coef, double alpha, const Real* in, double beta,
+                   Real* out) -> tnlb_status {
+      TNLB_CUDA_TRY(cudaMemcpyAsync(cdev.ptr, coef, sizeof(double) * cols, cudaMemcpyHostToDevice, c.st));
+      k_gemv_cols<Real><<<V.G, kRedThreads, 0, c.st>>>(n, ld, cols, Y, cdev.as<double>(), alpha, in, beta, out, -1);
+      TNLB_CHECK_LAUNCH();
+      return TNLB_OK;
+   };
+   // psolve(src, dst) of the reference: M^-1 src, or a copy
+   auto psolve = [&](const Real* src, Real* dst) -> tnlb_status {
+      if (!pre) return src == dst ? TNLB_OK : V.copy(dst, src);
+      TNLB_TRY_STATUS(Pc.apply(n, src, pv.as<Real>(), c.st));
+      return V.copy(dst, pv.as<Real>());
+   };
+   HostStop S(prm);
+   double b_norm, r_norm;
+   TNLB_TRY_STATUS(V.norm(b, &b_norm));
+   if (b_norm == 0) {
+      TNLB_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(Real) * n, c.st));
+      TNLB_CUDA_TRY(cudaStreamSynchronize(c.st));
+      *res = tnlb_solve_result{1, 0, 0.0, 0, 0};
+      return TNLB_OK;
+   }
+   TNLB_TRY_STATUS(V.copy(r.as<Real>(), b));
+   TNLB_TRY_STATUS(c.spmv(x, r.as<Real>(), -1.0, 1.0));
+   TNLB_TRY_STATUS(V.norm(r.as<Real>(), &r_norm));
+   TNLB_REQUIRE(!std::isnan(r_norm), TNLB_ERR_INVALID_ARGUMENT, "IDR(s): initial residue is NAN");
+   const double angle = 0.7;
+   double omega = 1.0;
+   std::vector<double> M((size_t)s * s, 0.0), f(s), cvec(s), Msub((size_t)s * s);
+   for (int i = 0; i < s; i++) M[(size_t)i * s + i] = 1;
+   if (smoothing) {
+      TNLB_TRY_STATUS(V.copy(x_s.as<Real>(), x));
+      TNLB_TRY_STATUS(V.copy(r_s.as<Real>(), r.as<Real>()));
+   }
+   auto smooth = [&]() -> tnlb_status {
+      if (!smoothing) return TNLB_OK;
+      TNLB_TRY_STATUS(V.copy(t.as<Real>(), r_s.as<Real>()));
+      TNLB_TRY_STATUS(V.axpby(-1.0, r.as<Real>(), 1.0, t.as<Real>()));
+      double tr, tt;
+      TNLB_TRY_STATUS(V.dot(t.as<Real>(), r_s.as<Real>(), &tr));
+      TNLB_TRY_STATUS(V.dot(t.as<Real>(), t.as<Real>(), &tt));
+      const double gam = tr / tt;
+      TNLB_TRY_STATUS(V.axpby(-gam, t.as<Real>(), 1.0, r_s.as<Real>()));
+      k_smooth_x<Real><<<V.G, kRedThreads, 0, c.st>>>(n, (Real)gam, x, x_s.as<Real>());
+      TNLB_CHECK_LAUNCH();
+      return V.norm(r_s.as<Real>(), &r_norm);
+   };
+   auto finish_smoothing = [&]() -> tnlb_status { return smoothing ? V.copy(x, x_s.as<Real>()) : TNLB_OK; };
+   S.residue = r_norm / b_norm;
+   while (S.check()) {
+      TNLB_TRY_STATUS(ptv(0, s, r.as<Real>()));
+      for (int i = 0; i < s; i++) f[i] = hv[i];
+      for (int k = 0; k < s; k++) {
+         Real* Uk = col(Ud, k);
+         Real* Gk = col(Gd, k);
+         const int m = s - k;
+         // c = M[k:s, k:s]^-1 f[k:s] (LU without pivoting)
+         for (int i = 0; i < m; i++)
+            for (int j = 0; j < m; j++) Msub[(size_t)i * s + j] = M[(size_t)(i + k) * s + (j + k)];
+         for (int kk = 0; kk < m; kk++) {
+            const double pivot = Msub[(size_t)kk * s + kk];
+            for (int j = kk + 1; j < m; j++) {
+               const double factor = Msub[(size_t)j * s + kk] / pivot;
+               Msub[(size_t)j * s + kk] = factor;
+               for (int i = kk + 1; i < m; i++) Msub[(size_t)j * s + i] -= factor * Msub[(size_t)kk * s + i];
+            }
+         }
+         for (int i = 0; i < m; i++) cvec[i] = f[k + i];
+         for (int kk = 1; kk < m; kk++)
+            for (int j = 0; j < kk; j++) cvec[kk] -= Msub[(size_t)kk * s + j] * cvec[j];
+         for (int kk = m - 1; kk >= 0; kk--) {
+            for (int j = m - 1; j > kk; j--) cvec[kk] -= Msub[(size_t)kk * s + j] * cvec[j];
+            cvec[kk] /= Msub[(size_t)kk * s + kk];
+         }
+         // v = M^-1 (r - G[:, k:s] c); U_k = U[:, k:s] c + omega v; G_k = A U_k
+         TNLB_TRY_STATUS(gemv(Gk, m, cvec.data(), -1.0, r.as<Real>(), 1.0, v.as<Real>()));
+         TNLB_TRY_STATUS(psolve(v.as<Real>(), v.as<Real>()));
+         TNLB_TRY_STATUS(gemv(Uk, m, cvec.data(), 1.0, nullptr, 0.0, Uk));
+         TNLB_TRY_STATUS(V.axpby(omega, v.as<Real>(), 1.0, Uk));
+         TNLB_TRY_STATUS(c.spmv(Uk, Gk));
+         for (int i = 0; i < k; i++) {
+            double pg;
+            TNLB_TRY_STATUS(V.dot(col(Pd, i), Gk, &pg));
+            const double al = pg / M[(size_t)i * s + i];
+            TNLB_TRY_STATUS(V.axpby(-al, col(Ud, i), 1.0, Uk));
+            TNLB_TRY_STATUS(V.axpby(-al, col(Gd, i), 1.0, Gk));
+         }
+         TNLB_TRY_STATUS(ptv(k, m, Gk));
+         for (int i = k; i < s; i++) M[(size_t)i * s + k] = hv[i - k];
+         if (M[(size_t)k * s + k] == 0) {
+            TNLB_CUDA_TRY(cudaStreamSynchronize(c.st));
+            S.finish(res, false);
+            return TNLB_OK;
+         }
+         const double beta = f[k] / M[(size_t)k * s + k];
+         TNLB_TRY_STATUS(V.axpby(beta, Uk, 1.0, x));
+         TNLB_TRY_STATUS(V.axpby(-beta, Gk, 1.0, r.as<Real>()));
+         TNLB_TRY_STATUS(V.norm(r.as<Real>(), &r_norm));
+         TNLB_TRY_STATUS(smooth());
+         S.residue = r_norm / b_norm;
+         if (!S.next()) {
+            TNLB_TRY_STATUS(finish_smoothing());
+            TNLB_CUDA_TRY(cudaStreamSynchronize(c.st));
+            S.finish(res);
+            return TNLB_OK;
+         }
+         for (int i = k + 1; i < s; i++) f[i] = f[i] - beta * M[(size_t)i * s + k];
+      }
+      TNLB_TRY_STATUS(psolve(r.as<Real>(), v.as<Real>()));
+      TNLB_TRY_STATUS(c.spmv(v.as<Real>(), t.as<Real>()));
+      double t_norm, tr;
+      TNLB_TRY_STATUS(V.norm(t.as<Real>(), &t_norm));
+      TNLB_TRY_STATUS(V.dot(t.as<Real>(), r.as<Real>(), &tr));
+      const double rho = std::fabs(tr / (t_norm * r_norm));
+      omega = tr / (t_norm * t_norm);
+      if (rho < angle) omega = omega * angle / rho;
+      if (omega == 0) {
+         TNLB_CUDA_TRY(cudaStreamSynchronize(c.st));
+         S.finish(res, false);
+         return TNLB_OK;
+      }
+      TNLB_TRY_STATUS(V.axpby(omega, v.as<Real>(), 1.0, x));
+      TNLB_TRY_STATUS(V.axpby(-omega, t.as<Real>(), 1.0, r.as<Real>()));
+      TNLB_TRY_STATUS(V.norm(r.as<Real>(), &r_norm));
+      TNLB_TRY_STATUS(smooth());
+      S.residue = r_norm / b_norm;
+      S.next();
+   }
+   TNLB_TRY_STATUS(finish_smoothing());
+   TNLB_CUDA_TRY(cudaStreamSynchronize(c.st));
+   S.finish(res);
+   return TNLB_OK;
+}
+
 template <typename Real>
 tnlb_status solve_t(tnlb_solver_kind solver, const tnlb_precond* pobj, const tnlb_solver_params& prm,
                     const tnlb_segments* seg, tnlb_real real, const int32_t* cols, const Real* vals, const Real* b,
@@ -1382,6 +1874,9 @@ tnlb_status solve_t(tnlb_solver_kind solver, const tnlb_precond* pobj, const tnl
       case TNLB_SOLVER_BICGSTAB: return bicgstab_solve<Real>(c, P, prm, b, x, res);
       case TNLB_SOLVER_GMRES: return gmres_solve<Real>(c, P, prm, b, x, res);
       case TNLB_SOLVER_FGMRES: return gmres_solve<Real>(c, P, prm, b, x, res, true);
+      case TNLB_SOLVER_TFQMR: return tfqmr_solve<Real>(c, P, prm, b, x, res);
+      case TNLB_SOLVER_BICGSTABL: return bicgstabl_solve<Real>(c, P, prm, b, x, res);
+      case TNLB_SOLVER_IDRS: return idrs_solve<Real>(c, P, prm, b, x, res);
    }
    set_error("unknown solver");
    return TNLB_ERR_INVALID_ARGUMENT;
