@@ -215,9 +215,11 @@ def test_lfsai_reference_fd():
 def test_more_krylov_match_reference(oracle, reference, solver, kw):
     """TFQMR, BiCGStab(ell) and IDR(s) restated in the oracle against the
     reference's own solvers.  The reference sums dot products in a blocked
-    order (and in OpenMP threads), the oracle sequentially: TFQMR and IDR(s)
-    stay within 2 % of the reference's iterations; BiCGStab(ell), like
-    BiCGStab, within 10 %."""
+    order (and in OpenMP threads, so its own counts move between runs), the
+    oracle sequentially: IDR(s) stays within 2 % of the reference's
+    iterations; BiCGStab(ell) and TFQMR, whose short recurrences amplify the
+    rounding (TFQMR moves 150-158 between runs of the reference on the
+    convection-diffusion matrix), within 10 %."""
     probs = [g.laplacian_2d(32), g.diffusion_2d(33, 0.1, 2.0, 6), g.convection_diffusion_3d(10)]
     for A in probs:
         b = g.uniform_vector(A.n, 1)
@@ -225,7 +227,7 @@ def test_more_krylov_match_reference(oracle, reference, solver, kw):
             r = reference.solve(solver, A, b, precond=pre, tol=1e-8, maxit=20000, **kw)
             o = oracle.solve(solver, A, b, precond=pre, tol=1e-8, maxit=20000, **kw)
             assert r["converged"] and o["converged"], (solver, kw, pre)
-            slack = max(5, r["iterations"] // 10) if solver == "bicgstabl" else max(2, r["iterations"] // 50)
+            slack = max(5, r["iterations"] // 10) if solver in ("bicgstabl", "tfqmr") else max(2, r["iterations"] // 50)
             assert abs(r["iterations"] - o["iterations"]) <= slack, (solver, kw, pre, r["iterations"], o["iterations"])
             assert np.allclose(o["x"], r["x"], rtol=1e-5, atol=1e-6 * np.abs(r["x"]).max()), (solver, kw, pre)
 

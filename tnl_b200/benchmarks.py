@@ -5,6 +5,8 @@ on seeded synthetic matrices.  One JSON object per line on stdout.
 
     python -m tnl_b200.benchmarks spmv    [--configs laplacian,power_law] [--reals f64,f32] [--steps K]
     python -m tnl_b200.benchmarks solvers [--problem laplacian|diffusion] [--N 1024]
+    python -m tnl_b200.benchmarks sweep   [--problem laplacian|diffusion|convection_diffusion] [--N 1024]
+    python -m tnl_b200.benchmarks configs --which c3|c5
 
 spmv: every segment format and kernel on the 1024^2 5-point Laplacian
 (n = 1,048,576), the power-law matrix (n = 4,194,304, Zipf 1.73 row
@@ -203,6 +205,113 @@ def bench_solvers(problem: str, N: int, weights: str | None, out=sys.stdout):
     mixed("FP32-inner IR, learned FSAI", P32, s)
 
 
+SOLVER_SWEEP = [
+    ("CG", "cg", "jacobi", {}), ("BICGStab", "bicgstab", "jacobi", {}), ("TFQMR", "tfqmr", "jacobi", {}),
+    ("BICGStab(2)", "bicgstabl", "jacobi", {"bicgstab-ell": 2}), ("IDR(4)", "idrs", "jacobi", {"idr-s": 4}),
+    ("GMRES(30) MGSR", "gmres", "jacobi", {"gmres-variant": "MGSR"}),
+    ("GMRES(30) CWY", "gmres", "jacobi", {"gmres-variant": "CWY"}),
+    ("GMRES(30) MGSR", "gmres", "ilu0", {"gmres-variant": "MGSR"}),
+]
+
+
+def bench_solver_sweep(problem: str, N: int, tol: float = 1e-8, max_iterations: int = 100000, out=sys.stdout):
+    """Every Krylov solver with Jacobi (and GMRES with ILU(0)) on one problem,
+    as the reference's linear-solver benchmark does: iterations, device time of
+    the solve call, set-up time of the preconditioner, true FP64 residual."""
+    import tnl_b200 as t
+    from . import generators as g
+    from .lfsai import diffusion_problem
+
+    if problem == "laplacian":
+        M = t.SparseMatrix.from_csr(g.laplacian_2d(N))
+    elif problem == "convection_diffusion":
+        M = t.SparseMatrix.from_csr(g.convection_diffusion_3d(N))
+    else:
+        M = diffusion_problem(N, 1234)
+    n = M.getRows()
+    b = torch.tensor(g.uniform_vector(n, 1), device="cuda")
+    classes = {"cg": t.CG, "bicgstab": t.BICGStab, "tfqmr": t.TFQMR, "bicgstabl": t.BICGStabL, "idrs": t.IDRs,
+               "gmres": t.GMRES}
+    precs = {"jacobi": t.Diagonal, "ilu0": t.ILU0}
+    for label, kind, pname, keys in SOLVER_SWEEP:
+        if kind == "cg" and problem == "convection_diffusion":
+            continue  # nonsymmetric
+        P = precs[pname]()
+        _, setup_ms = _timed(lambda: P.update(M))
+        S = classes[kind]()
+        S.setMatrix(M)
+        S.setPreconditioner(P)
+        S.setup({"convergence-residue": tol, "max-iterations": max_iterations, "gmres-restarting-min": 30,
+                 "gmres-restarting-max": 30, **keys})
+        x = torch.zeros(n, dtype=torch.float64, device="cuda")
+        ok, ms = _timed(lambda: S.solve(b, x))
+        rec = {"bench": "solver_sweep", "problem": problem, "N": N, "rows": n, "solver": label, "precond": pname,
+               "converged": bool(ok), "iterations": S.getIterations(), "solve_ms": ms, "setup_ms": setup_ms,
+               "ms_per_iteration": ms / max(1, S.getIterations()), "residue": S.getResidue(),
+               "true_residual": t.true_residual(M, b, x), "tol": tol}
+        print(json.dumps(rec), file=out, flush=True)
+
+
+def bench_configs(which: str, out=sys.stdout):
+    """The mixed-precision and nonsymmetric configurations:
+    c3 -- 256^3 GRF diffusion (n = 16.8M): FP32-inner Jacobi-PCG inside FP64
+          refinement vs plain FP64 Jacobi-PCG, to FP64 relative residual 1e-10;
+    c5 -- 192^3 upwind convection-diffusion (n = 7.1M): FGMRES(30) with the
+          two-factor FSAI (FP64, and as the FP32 inner solver of FP64
+          refinement) vs plain FP64 GMRES(30) + ILU(0), to 1e-8."""
+    import tnl_b200 as t
+    from . import generators as g
+
+    if which == "c3":
+        A = g.diffusion_3d(256)
+        tol = 1e-10
+    else:
+        A = g.convection_diffusion_3d(192)
+        tol = 1e-8
+    M = t.SparseMatrix.from_csr(A)
+    n = M.getRows()
+    b = torch.tensor(g.uniform_vector(n, 1), device="cuda")
+    base = {"bench": "config", "config": which, "rows": n, "nnz": A.nnz, "tol": tol}
+
+    def report(name, conv, its, ms, setup_ms, x, **extra):
+        rec = dict(base, method=name, converged=bool(conv), iterations=its, solve_ms=ms, setup_ms=setup_ms,
+                   true_residual=t.true_residual(M, b, x), **extra)
+        print(json.dumps(rec), file=out, flush=True)
+        return rec
+
+    def krylov(name, cls, P, keys):
+        S = cls()
+        S.setMatrix(M)
+        S.setPreconditioner(P)
+        S.setup({"convergence-residue": tol, "max-iterations": 20000, "gmres-restarting-min": 30,
+                 "gmres-restarting-max": 30, **keys})
+        x = torch.zeros(n, dtype=torch.float64, device="cuda")
+        ok, ms = _timed(lambda: S.solve(b, x))
+        return report(name, ok, S.getIterations(), ms, 0.0, x)
+
+    if which == "c3":
+        P = t.Diagonal()
+        P.update(M)
+        krylov("FP64 Jacobi-PCG", t.CG, P, {})
+        x = torch.zeros(n, dtype=torch.float64, device="cuda")
+        r, ms = _timed(lambda: t.solve_mixed(M, b, x, tol=tol, inner_tol=1e-4, inner="jacobi", max_outer=20))
+        report("FP32-inner Jacobi-PCG in FP64 refinement", r["converged"], r["inner_iterations"], ms, 0.0, x,
+               outer_iterations=r["outer_iterations"])
+        return
+    P = t.ILU0()
+    _, s_ilu = _timed(lambda: P.update(M))
+    rec = krylov("FP64 GMRES(30) + ILU(0)", t.GMRES, P, {"gmres-variant": "MGSR"})
+    rec["setup_ms"] = s_ilu
+    P = t.FSAI2()
+    _, s_f2 = _timed(lambda: P.update(M))
+    krylov("FP64 FGMRES(30) + two-factor FSAI", t.FGMRES, P, {"gmres-variant": "MGSR"})
+    x = torch.zeros(n, dtype=torch.float64, device="cuda")
+    r, ms = _timed(lambda: t.solve_mixed(M, b, x, tol=tol, inner_tol=1e-4, inner="fsai2", solver="fgmres",
+                                         max_outer=20))
+    report("FP32-inner FGMRES(30) + two-factor FSAI in FP64 refinement", r["converged"], r["inner_iterations"], ms,
+           s_f2, x, outer_iterations=r["outer_iterations"])
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(prog="python -m tnl_b200.benchmarks")
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -211,11 +320,23 @@ def main(argv=None):
     a.add_argument("--reals", default="f64,f32")
     a.add_argument("--steps", type=int, default=50)
     a.add_argument("--formats", default="", help="comma-separated labels, e.g. 'CSR default,SlicedEllpack'")
+    cf = sub.add_parser("configs")
+    cf.add_argument("--which", default="c3", choices=["c3", "c5"])
+    sw = sub.add_parser("sweep")
+    sw.add_argument("--problem", default="laplacian", choices=["laplacian", "diffusion", "convection_diffusion"])
+    sw.add_argument("--N", type=int, default=1024)
+    sw.add_argument("--max-iterations", type=int, default=100000)
     b = sub.add_parser("solvers")
     b.add_argument("--problem", default="laplacian", choices=["laplacian", "diffusion"])
     b.add_argument("--N", type=int, default=1024)
     b.add_argument("--weights", default=str(Path(__file__).resolve().parent / "weights" / "lfsai_diffusion.npy"))
     args = ap.parse_args(argv)
+    if args.cmd == "configs":
+        bench_configs(args.which)
+        return 0
+    if args.cmd == "sweep":
+        bench_solver_sweep(args.problem, args.N, max_iterations=args.max_iterations)
+        return 0
     if args.cmd == "spmv":
         bench_spmv(args.configs.split(","), args.reals.split(","), args.steps,
                    [f for f in args.formats.split(",") if f])

@@ -264,6 +264,15 @@ tnlb_status inclusive_scan_i32_inplace(int32_t* d_data, int64_t n, cudaStream_t 
 tnlb_status reduce_max_i32(const int32_t* d_in, int64_t n, int32_t* h_max, cudaStream_t stream);
 tnlb_status reduce_sum_i64(const int32_t* d_in, int64_t n, int64_t* h_sum, cudaStream_t stream);
 // spmv_csr.cu / spmv_ell.cu
+// y = A x with (x, y) summed in the same kernel, for CSR matrices whose rows
+// hold at most 16 entries (spmv_dot_fusable); `partials` holds
+// spmv_dot_partials(seg) doubles, `counter` starts (and ends) at zero; the
+// sum lands in *dot_out.  Deterministic.
+bool spmv_dot_fusable(const tnlb_segments* seg);
+int64_t spmv_dot_partials(const tnlb_segments* seg);
+tnlb_status spmv_dot(const tnlb_segments* seg, tnlb_real real, const int32_t* cols, const void* vals, const void* x,
+                     void* y, double* partials, unsigned* counter, double* dot_out, cudaStream_t st,
+                     const int32_t* skip);
 tnlb_status spmv_csr(const tnlb_segments* seg, tnlb_real real, const int32_t* cols, const void* vals, const void* x,
                      void* y, double alpha, double beta, int32_t begin, int32_t end, tnlb_kernel kernel, int32_t tps,
                      cudaStream_t stream, int* launches, const int32_t* skip = nullptr);

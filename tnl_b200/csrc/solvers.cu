@@ -161,6 +161,22 @@ __global__ void __launch_bounds__(kRedThreads) k_cg_s2(int64_t n, const Real* __
    }
 }
 
+// s2 = (p, Ap) from the fused product's sum; alpha = s1 / s2 (the epilogue
+// of k_cg_s2).
+__global__ void k_cg_alpha(const double* __restrict__ s2, DevState* S)
+{
+   if (S->done || threadIdx.x != 0) return;
+   const double t = *s2;
+   S->s2 = t;
+   if (t == 0.0) {
+      S->residue = 0.0;
+      S->done = 1;
+      S->flag = 1;
+   }
+   else
+      S->alpha = S->s1 / t;
+}
+
 // x += alpha p; r -= alpha Ap; z = M^-1 r; s1 = (r, z); beta; residue; nextIteration.
 template <typename Real>
 __global__ void __launch_bounds__(kRedThreads) k_cg_update(int64_t n, Real* __restrict__ x, Real* __restrict__ r,
@@ -616,9 +632,26 @@ tnlb_status cg_solve(const Ctx<Real>& c, const Precond<Real>& P, const tnlb_solv
    TNLB_CHECK_LAUNCH();
    // One iteration (CG.hpp:60-107): every kernel returns at once when the
    // device `done` flag is set, so batches may run past the stopping point.
+   // short-row CSR: (p, Ap) summed inside the product's kernel
+   const bool fused = spmv_dot_fusable(c.seg);
+   DeviceBuffer dot_parts, dot_ctr, dot_val;
+   if (fused) {
+      TNLB_TRY_STATUS(dot_parts.alloc(sizeof(double) * spmv_dot_partials(c.seg)));
+      TNLB_TRY_STATUS(dot_ctr.alloc(sizeof(unsigned)));
+      TNLB_TRY_STATUS(dot_val.alloc(sizeof(double)));
+      TNLB_CUDA_TRY(cudaMemsetAsync(dot_ctr.ptr, 0, sizeof(unsigned), c.st));
+   }
    auto enqueue_iteration = [&](cudaStream_t st) -> tnlb_status {
-      TNLB_TRY_STATUS(spmv_dispatch(c.seg, c.real, c.cols, c.vals, p.as<Real>(), Ap.as<Real>(), 1.0, 0.0, st, done));
-      k_cg_s2<Real><<<G, kRedThreads, 0, st>>>(n, Ap.as<Real>(), p.as<Real>(), W.red(), W.S());
+      if (fused) {
+         TNLB_TRY_STATUS(spmv_dot(c.seg, c.real, c.cols, c.vals, p.as<Real>(), Ap.as<Real>(), dot_parts.as<double>(),
+                                  dot_ctr.as<unsigned>(), dot_val.as<double>(), st, done));
+         k_cg_alpha<<<1, 32, 0, st>>>(dot_val.as<double>(), W.S());
+      }
+      else {
+         TNLB_TRY_STATUS(
+            spmv_dispatch(c.seg, c.real, c.cols, c.vals, p.as<Real>(), Ap.as<Real>(), 1.0, 0.0, st, done));
+         k_cg_s2<Real><<<G, kRedThreads, 0, st>>>(n, Ap.as<Real>(), p.as<Real>(), W.red(), W.S());
+      }
       if (gen) {
          k_cg_xr<Real><<<G, kRedThreads, 0, st>>>(n, x, r.as<Real>(), p.as<Real>(), Ap.as<Real>(), W.S());
          TNLB_TRY_STATUS(P.apply(n, r.as<Real>(), z.as<Real>(), st, done));

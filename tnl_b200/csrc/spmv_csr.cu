@@ -27,6 +27,7 @@
 #include <climits>
 
 #include "internal.cuh"
+#include "reduce.cuh"
 
 namespace tnlb {
 namespace {
@@ -205,6 +206,48 @@ __global__ void __launch_bounds__(256) k_csr_short(const int32_t* __restrict__ r
    for (int j = 0; j < L; j++)
       if (c[j] >= 0) s += v[j] * __ldg(x + c[j]);
    keep(y, (int32_t)r, s, alpha, beta);
+}
+
+// k_csr_short with the dot product (x, y) of the product's input and output
+// fused into it (the (p, A p) of CG): a grid-stride loop over rows on at most
+// kRedMaxBlocks blocks, each block's sum of x[r] * y[r] published, the last
+// block to arrive adding them in block order (deterministic) into *dot_out.
+// Needs alpha = 1, beta = 0.
+template <typename Real, int L>
+__global__ void __launch_bounds__(256) k_csr_short_dot(const int32_t* __restrict__ rowptr,
+                                                       const int32_t* __restrict__ cols, const Real* __restrict__ vals,
+                                                       const Real* __restrict__ x, Real* __restrict__ y, int32_t n,
+                                                       RedWork w, double* __restrict__ dot_out,
+                                                       const int32_t* __restrict__ skip)
+{
+   if (skip && *skip) return;  // every block returns: no ticket is taken
+   double d = 0.0;
+   for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+      const int32_t b = rowptr[r], e = rowptr[r + 1];
+      int32_t c[L];
+      Real v[L];
+#pragma unroll
+      for (int j = 0; j < L; j++) {
+         c[j] = -1;
+         v[j] = Real(0);
+         if (b + j < e) {
+            c[j] = __ldg(cols + b + j);
+            v[j] = __ldg(vals + b + j);
+         }
+      }
+      Real s = Real(0);
+#pragma unroll
+      for (int j = 0; j < L; j++)
+         if (c[j] >= 0) s += v[j] * __ldg(x + c[j]);
+      y[r] = s;
+      d += (double)s * (double)__ldg(x + r);
+   }
+   double vv[1] = {d};
+   if (publish_and_arrive<1>(vv, w)) {
+      double t[1];
+      gather_totals<1>(t, w);
+      if (threadIdx.x == 0) *dot_out = t[0];
+   }
 }
 
 // ---------------------------------------------------------------- tile
@@ -567,6 +610,39 @@ tnlb_status build_csr_tile_plan(tnlb_segments* seg, cudaStream_t stream)
    TNLB_CUDA_TRY(cudaMemcpyAsync(&h, mx.ptr, sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
    TNLB_CUDA_TRY(cudaStreamSynchronize(stream));
    seg->max_row = h;
+   return TNLB_OK;
+}
+
+bool spmv_dot_fusable(const tnlb_segments* seg)
+{
+   return seg->format == TNLB_CSR && seg->n > 0 && seg->max_row >= 0 && seg->max_row <= 16;
+}
+
+int64_t spmv_dot_partials(const tnlb_segments*) { return kRedMaxBlocks; }
+
+tnlb_status spmv_dot(const tnlb_segments* seg, tnlb_real real, const int32_t* cols, const void* vals, const void* x,
+                     void* y, double* partials, unsigned* counter, double* dot_out, cudaStream_t st,
+                     const int32_t* skip)
+{
+   TNLB_REQUIRE(spmv_dot_fusable(seg), TNLB_ERR_INVALID_ARGUMENT, "spmv_dot: not a short-row CSR matrix");
+   const unsigned g = vec_grid(seg->n);
+   const int32_t* rp = seg->offsets.as<int32_t>();
+   // one sum: partials[block] for each of the <= kRedMaxBlocks blocks
+   RedWork w{partials, counter};
+#define TNLB_SD(RT, LL) \
+   k_csr_short_dot<RT, LL><<<g, 256, 0, st>>>(rp, cols, (const RT*)vals, (const RT*)x, (RT*)y, seg->n, w, dot_out, skip)
+   if (real == TNLB_F64) {
+      if (seg->max_row <= 4) TNLB_SD(double, 4);
+      else if (seg->max_row <= 8) TNLB_SD(double, 8);
+      else TNLB_SD(double, 16);
+   }
+   else {
+      if (seg->max_row <= 4) TNLB_SD(float, 4);
+      else if (seg->max_row <= 8) TNLB_SD(float, 8);
+      else TNLB_SD(float, 16);
+   }
+#undef TNLB_SD
+   TNLB_CHECK_LAUNCH();
    return TNLB_OK;
 }
 
