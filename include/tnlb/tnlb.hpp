@@ -4,7 +4,8 @@
 // code changes only its includes and namespace:
 //   TNL::Matrices::SparseMatrix< Real, Devices::Cuda, int, GeneralMatrix, Segments >
 //        setDimensions, setRowCapacities, setFromCSR (the cross-format
-//        operator= from a CSR matrix), vectorProduct, getRows, getColumns
+//        operator= from a CSR matrix), vectorProduct, transposedVectorProduct,
+//        getRows, getColumns; MatrixType GeneralMatrix or SymmetricMatrix
 //        (Matrices/SparseMatrix.h:41-57, SparseMatrixBase.h:1020-1035);
 //   TNL::Algorithms::Segments::{CSR, Ellpack, SlicedEllpack, ChunkedEllpack,
 //        BiEllpack, AdaptiveCSR}, LaunchConfiguration, ElementsOrganization;
@@ -26,6 +27,7 @@
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../tnlb200.h"
@@ -211,6 +213,8 @@ struct LaunchConfiguration {
 namespace Matrices {
 
 struct GeneralMatrix {};
+// MatrixType SymmetricMatrix (Matrices/MatrixType.h:48): one triangle stored.
+struct SymmetricMatrix {};
 
 template <typename Real = double, typename Device = Devices::Cuda, typename Index = int,
           typename MatrixType = GeneralMatrix,
@@ -282,9 +286,36 @@ public:
          throw std::invalid_argument("vectorProduct: size of the input vector does not match the number of matrix columns");
       if (out.getSize() != rows_)
          throw std::invalid_argument("vectorProduct: size of the output vector does not match the number of matrix rows");
-      tnlb::check(tnlb_spmv(seg_, tnlb::real_code<Real>(), columns_idx_.getData(), values_.getData(), columns_,
-                            in.getData(), out.getData(), matrixMultiplicator, outVectorMultiplicator, begin, end,
-                            lc.kernel(), lc.tps(), nullptr));
+      if (std::is_same<MatrixType, SymmetricMatrix>::value)
+         tnlb::check(tnlb_spmv_symmetric(seg_, tnlb::real_code<Real>(), columns_idx_.getData(), values_.getData(),
+                                         in.getData(), out.getData(), matrixMultiplicator, outVectorMultiplicator,
+                                         begin, end, nullptr));
+      else
+         tnlb::check(tnlb_spmv(seg_, tnlb::real_code<Real>(), columns_idx_.getData(), values_.getData(), columns_,
+                               in.getData(), out.getData(), matrixMultiplicator, outVectorMultiplicator, begin, end,
+                               lc.kernel(), lc.tps(), nullptr));
+      tnlb::cuda_check(cudaStreamSynchronize(nullptr));
+   }
+   // y = matrixMultiplicator * A^T x + outVectorMultiplicator * y on columns
+   // [begin, end) (SparseMatrixBase.hpp:542-588); symmetric matrices use
+   // vectorProduct.  Synchronous.
+   template <typename InVector, typename OutVector>
+   void transposedVectorProduct(const InVector& in, OutVector& out, Real matrixMultiplicator = 1,
+                                Real outVectorMultiplicator = 0, Index begin = 0, Index end = 0) const
+   {
+      if (in.getSize() != rows_)
+         throw std::invalid_argument(
+            "transposedVectorProduct: size of the input vector does not match the number of matrix rows");
+      if (out.getSize() != columns_)
+         throw std::invalid_argument(
+            "transposedVectorProduct: size of the output vector does not match the number of matrix columns");
+      if (std::is_same<MatrixType, SymmetricMatrix>::value) {
+         vectorProduct(in, out, matrixMultiplicator, outVectorMultiplicator, begin, end);
+         return;
+      }
+      tnlb::check(tnlb_spmv_transposed(seg_, tnlb::real_code<Real>(), columns_idx_.getData(), values_.getData(),
+                                       columns_, in.getData(), out.getData(), matrixMultiplicator,
+                                       outVectorMultiplicator, begin, end, nullptr));
       tnlb::cuda_check(cudaStreamSynchronize(nullptr));
    }
    Index getRows() const { return rows_; }

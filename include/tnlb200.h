@@ -213,6 +213,27 @@ tnlb_status tnlb_spmv(const tnlb_segments* seg, tnlb_real real, const int32_t* d
  * enqueued (for launch accounting). */
 int32_t tnlb_spmv_last_launch_count(void);
 
+/* y = alpha * A x + beta * y for a SYMMETRIC matrix of which one triangle is
+ * stored (vectorProduct of SparseMatrix<..., SymmetricMatrix, ...>,
+ * Matrices/SparseMatrixBase.hpp:296-330): a stored a_rc with c < r also adds
+ * alpha a_rc x[r] to y[c].  As in the reference, y is first multiplied by
+ * beta unless beta == 1 (y is read even when beta == 0) and the scattered
+ * additions are atomic, so the last bits of y vary from call to call.
+ * Rows [begin, end) (end == 0: all); any segment format.  Asynchronous. */
+tnlb_status tnlb_spmv_symmetric(const tnlb_segments* seg, tnlb_real real, const int32_t* d_cols, const void* d_values,
+                                const void* d_x, void* d_y, double alpha, double beta, int32_t begin, int32_t end,
+                                tnlb_stream stream);
+
+/* y = alpha * A^T x + beta * y (SparseMatrixBase::transposedVectorProduct,
+ * Matrices/SparseMatrixBase.hpp:542-588): x has info.segments entries, y has
+ * `columns`; only output entries with index in [begin, end) receive products
+ * (end == 0: all columns), y is multiplied by beta unless beta == 1, and the
+ * additions are atomic as in the reference.  Any segment format.
+ * Asynchronous. */
+tnlb_status tnlb_spmv_transposed(const tnlb_segments* seg, tnlb_real real, const int32_t* d_cols,
+                                 const void* d_values, int32_t columns, const void* d_x, void* d_y, double alpha,
+                                 double beta, int32_t begin, int32_t end, tnlb_stream stream);
+
 /* y = alpha * A x + beta * y for a CSR matrix given as plain device arrays
  * (row offsets d_rowptr[rows + 1], d_cols / d_values[nnz], nnz == d_rowptr[rows]),
  * computed by the same tile kernels as tnlb_spmv with TNLB_KERNEL_TILE on

@@ -107,6 +107,10 @@ class Oracle:
             ("orc_fill_f32", [C.POINTER(OrcSegments), p, p, p, p, p], None),
             ("orc_spmv_f64", [C.POINTER(OrcSegments), p, p, p, p, f64, f64, i32, i32], None),
             ("orc_spmv_f32", [C.POINTER(OrcSegments), p, p, p, p, f64, f64, i32, i32], None),
+            ("orc_spmv_symmetric_f64", [C.POINTER(OrcSegments), p, p, p, p, f64, f64, i32, i32], None),
+            ("orc_spmv_symmetric_f32", [C.POINTER(OrcSegments), p, p, p, p, f64, f64, i32, i32], None),
+            ("orc_spmv_transposed_f64", [C.POINTER(OrcSegments), p, p, i32, p, p, f64, f64, i32, i32], None),
+            ("orc_spmv_transposed_f32", [C.POINTER(OrcSegments), p, p, i32, p, p, f64, f64, i32, i32], None),
             ("orc_cg", [i32, p, p, p, C.c_int, p, p, C.POINTER(SolverState)], C.c_int),
             ("orc_bicgstab", [i32, p, p, p, C.c_int, C.c_int, p, p, C.POINTER(SolverState)], C.c_int),
             ("orc_gmres", [i32, p, p, p, C.c_int, i32, C.c_int, p, p, C.POINTER(SolverState)], C.c_int),
@@ -217,6 +221,30 @@ class Oracle:
         f(C.byref(v), cols.ctypes.data, vals.ctypes.data, x.ctypes.data, y.ctypes.data, alpha, beta, begin, end)
         return y
 
+    def spmv_symmetric(self, seg: Segments, cols, vals, x, y=None, alpha=1.0, beta=0.0, begin=0, end=0):
+        """vectorProduct of a symmetric matrix stored as one triangle."""
+        cols = _i32(cols)
+        vals = np.ascontiguousarray(vals)
+        x = np.ascontiguousarray(x, dtype=vals.dtype)
+        y = np.zeros(seg.n, vals.dtype) if y is None else np.array(y, dtype=vals.dtype, copy=True)
+        v = seg.cview()
+        f = self.L.orc_spmv_symmetric_f64 if vals.dtype == np.float64 else self.L.orc_spmv_symmetric_f32
+        f(C.byref(v), cols.ctypes.data, vals.ctypes.data, x.ctypes.data, y.ctypes.data, alpha, beta, begin, end)
+        return y
+
+    def spmv_transposed(self, seg: Segments, cols, vals, columns: int, x, y=None, alpha=1.0, beta=0.0, begin=0,
+                        end=0):
+        """transposedVectorProduct: y (length `columns`) = alpha A^T x + beta y."""
+        cols = _i32(cols)
+        vals = np.ascontiguousarray(vals)
+        x = np.ascontiguousarray(x, dtype=vals.dtype)
+        y = np.zeros(columns, vals.dtype) if y is None else np.array(y, dtype=vals.dtype, copy=True)
+        v = seg.cview()
+        f = self.L.orc_spmv_transposed_f64 if vals.dtype == np.float64 else self.L.orc_spmv_transposed_f32
+        f(C.byref(v), cols.ctypes.data, vals.ctypes.data, columns, x.ctypes.data, y.ctypes.data, alpha, beta, begin,
+          end)
+        return y
+
     # ------------------------------------------------------------ solvers
     def _state(self, tol, maxit, history):
         S = SolverState()
@@ -315,6 +343,8 @@ class Reference:
             ("ref_spmv_f32", [i32, i32, i32, i32, p, p, p, p, p, f64, f64, i32, i32, i32], f64),
             ("ref_solve", [i32, i32, i32, p, p, p, p, p, f64, i32, i32, i32, i32, p, p, p], C.c_int),
             ("ref_solve_ext", [i32, i32, i32, p, p, p, p, p, f64, i32, i32, i32, p, p, p], C.c_int),
+            ("ref_spmv_symmetric_f64", [i32, p, p, p, p, p, f64, f64, i32, i32], None),
+            ("ref_spmv_transposed_f64", [i32, i32, p, p, p, p, p, f64, f64, i32, i32], None),
             ("ref_prec_apply", [i32, p, p, p, i32, p, p], C.c_int),
             ("ref_omp_threads", [], C.c_int),
             ("ref_set_threads", [C.c_int], None),
@@ -414,6 +444,26 @@ class Reference:
         t = f(kind, int(colmajor), A.n, A.ncols, rowptr.ctypes.data, cols.ctypes.data, vals.ctypes.data, x.ctypes.data,
               y.ctypes.data, alpha, beta, begin, end, reps)
         return y, t
+
+    def spmv_symmetric(self, A, x, y=None, alpha=1.0, beta=0.0, begin=0, end=0):
+        """The reference's vectorProduct of a SymmetricMatrix CSR matrix (A holds one triangle)."""
+        rowptr, cols = _i32(A.rowptr), _i32(A.cols)
+        vals = np.ascontiguousarray(A.vals, np.float64)
+        x = np.ascontiguousarray(x, np.float64)
+        y = np.zeros(A.n) if y is None else np.array(y, np.float64, copy=True)
+        self.L.ref_spmv_symmetric_f64(A.n, rowptr.ctypes.data, cols.ctypes.data, vals.ctypes.data, x.ctypes.data,
+                                      y.ctypes.data, alpha, beta, begin, end)
+        return y
+
+    def spmv_transposed(self, A, x, y=None, alpha=1.0, beta=0.0, begin=0, end=0):
+        """The reference's transposedVectorProduct of a general CSR matrix."""
+        rowptr, cols = _i32(A.rowptr), _i32(A.cols)
+        vals = np.ascontiguousarray(A.vals, np.float64)
+        x = np.ascontiguousarray(x, np.float64)
+        y = np.zeros(A.ncols) if y is None else np.array(y, np.float64, copy=True)
+        self.L.ref_spmv_transposed_f64(A.n, A.ncols, rowptr.ctypes.data, cols.ctypes.data, vals.ctypes.data,
+                                       x.ctypes.data, y.ctypes.data, alpha, beta, begin, end)
+        return y
 
     def solve(self, solver: str, A, b, x0=None, precond: int = 1, tol=1e-8, maxit=100000, gmres_m=30,
               gmres_variant: int = 3, bicgstab_exact=False, ell=1, idr_s=4, idr_smoothing=False):

@@ -382,6 +382,52 @@ ref_spmv_f32( int fmt, int colmajor, int n, int ncols, const int* rowptr, const 
    return spmvImpl< float >( fmt, colmajor, n, ncols, rowptr, cols, vals, x, y, alpha, beta, begin, end, reps );
 }
 
+// vectorProduct of a symmetric CSR matrix (only the stored triangle given in
+// rowptr/cols/vals) and transposedVectorProduct of a general CSR matrix,
+// through the reference's Host code.  y is in/out.
+void
+ref_spmv_symmetric_f64( int n, const int* rowptr, const int* cols, const double* vals, const double* x, double* y,
+                        double alpha, double beta, int begin, int end )
+{
+   using SM = Matrices::SparseMatrix< double, Host, int, Matrices::SymmetricMatrix, Seg::CSR >;
+   SM A;
+   A.setDimensions( n, n );
+   IVec caps( n );
+   for( int i = 0; i < n; i++ )
+      caps[ i ] = rowptr[ i + 1 ] - rowptr[ i ];
+   A.setRowCapacities( caps );
+   auto v = A.getValues().getView();
+   auto c = A.getColumnIndexes().getView();
+   for( int j = 0; j < rowptr[ n ]; j++ ) {
+      v[ j ] = vals[ j ];
+      c[ j ] = cols[ j ];
+   }
+   Containers::Vector< double, Host, int > xv( n ), yv( n );
+   for( int i = 0; i < n; i++ ) {
+      xv[ i ] = x[ i ];
+      yv[ i ] = y[ i ];
+   }
+   A.vectorProduct( xv, yv, alpha, beta, begin, end );
+   for( int i = 0; i < n; i++ )
+      y[ i ] = yv[ i ];
+}
+
+void
+ref_spmv_transposed_f64( int n, int ncols, const int* rowptr, const int* cols, const double* vals, const double* x,
+                         double* y, double alpha, double beta, int begin, int end )
+{
+   Mat< double, Seg::CSR > A;
+   makeCSR( A, n, ncols, rowptr, cols, vals );
+   Containers::Vector< double, Host, int > xv( n ), yv( ncols );
+   for( int i = 0; i < n; i++ )
+      xv[ i ] = x[ i ];
+   for( int i = 0; i < ncols; i++ )
+      yv[ i ] = y[ i ];
+   A.transposedVectorProduct( xv, yv, alpha, beta, begin, end );
+   for( int i = 0; i < ncols; i++ )
+      y[ i ] = yv[ i ];
+}
+
 // Solve A x = b with TNL's CG (solver 0), BICGStab (1) or GMRES (2), with no
 // preconditioner (0), Diagonal (1) or ILU0 (2).  gmresVariant: 2 MGS, 3 MGSR,
 // 4 CWY.  x holds the initial guess on entry.  Returns 1 if solve() returned

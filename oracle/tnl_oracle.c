@@ -496,6 +496,62 @@ ORC_FILL(orc_fill_f32, float)
 ORC_SPMV(orc_spmv_f64, double)
 ORC_SPMV(orc_spmv_f32, float)
 
+/* vectorProduct of a symmetric matrix (SparseMatrixBase.hpp:296-330): only
+ * one triangle is stored; y *= beta unless beta == 1 (y is read even when
+ * beta == 0, as the reference's `outVector *= outVectorMultiplicator`);
+ * then, for each row r in [begin,end), y[r] += alpha * sum_k a_k x[c_k] and,
+ * for every stored c < r, y[c] += alpha * a * x[r] (the reference adds these
+ * with atomics, so its order of additions is not fixed; here rows go in
+ * order, elements in local-index order). */
+#define ORC_SPMV_SYM(NAME, T)                                                                          \
+   void NAME(const orc_segments* s, const int32_t* cols, const T* vals, const T* x, T* y, double alpha, \
+             double beta, int32_t begin, int32_t end)                                                  \
+   {                                                                                                   \
+      if (end == 0) end = s->n;                                                                        \
+      const T a = (T)alpha, b = (T)beta;                                                               \
+      if (b != 1)                                                                                      \
+         for (int32_t i = 0; i < s->n; i++) y[i] = y[i] * b;                                           \
+      for (int32_t r = begin; r < end; r++) {                                                          \
+         const int32_t cap = orc_segment_capacity(s, r);                                               \
+         T acc = 0;                                                                                    \
+         for (int32_t k = 0; k < cap; k++) {                                                           \
+            const int64_t g = orc_global_index(s, r, k);                                               \
+            const int32_t c = cols[g];                                                                 \
+            if (c == -1) continue;                                                                     \
+            if (c < r) y[c] += a * vals[g] * x[r];                                                     \
+            acc += vals[g] * x[c];                                                                     \
+         }                                                                                             \
+         y[r] += a * acc;                                                                              \
+      }                                                                                                \
+   }
+ORC_SPMV_SYM(orc_spmv_symmetric_f64, double)
+ORC_SPMV_SYM(orc_spmv_symmetric_f32, float)
+
+/* transposedVectorProduct (SparseMatrixBase.hpp:542-588): y (length
+ * `columns`) *= beta unless beta == 1, then y[c] += alpha * x[r] * a for
+ * every stored element (r, c, a) with c in [begin,end); end == 0 means all
+ * columns.  Rows in order, elements in local-index order (the reference's
+ * atomics leave the order open). */
+#define ORC_SPMV_T(NAME, T)                                                                                 \
+   void NAME(const orc_segments* s, const int32_t* cols, const T* vals, int32_t columns, const T* x, T* y,  \
+             double alpha, double beta, int32_t begin, int32_t end)                                         \
+   {                                                                                                        \
+      if (end == 0) end = columns;                                                                          \
+      const T a = (T)alpha, b = (T)beta;                                                                    \
+      if (b != 1)                                                                                           \
+         for (int32_t i = 0; i < columns; i++) y[i] = y[i] * b;                                             \
+      for (int32_t r = 0; r < s->n; r++) {                                                                  \
+         const int32_t cap = orc_segment_capacity(s, r);                                                    \
+         for (int32_t k = 0; k < cap; k++) {                                                                \
+            const int64_t g = orc_global_index(s, r, k);                                                    \
+            const int32_t c = cols[g];                                                                      \
+            if (c >= begin && c < end && c != -1) y[c] += a * x[r] * vals[g];                               \
+         }                                                                                                  \
+      }                                                                                                     \
+   }
+ORC_SPMV_T(orc_spmv_transposed_f64, double)
+ORC_SPMV_T(orc_spmv_transposed_f32, float)
+
 /* ------------------------------------------------------------------------ */
 /* Krylov solvers on a CSR matrix (double)                                  */
 /* ------------------------------------------------------------------------ */

@@ -242,3 +242,45 @@ def test_idrs_shadow_space_matches_reference_draws(oracle, reference):
     o = oracle.solve("idrs", A, b, precond=2, tol=1e-8, maxit=100, idr_s=4)
     assert r["iterations"] == o["iterations"]
     assert np.allclose(o["x"], r["x"], rtol=1e-10, atol=1e-12)
+
+
+def _lower_triangle(A):
+    keep = np.asarray(A.cols) <= np.repeat(np.arange(A.n), np.diff(A.rowptr))
+    lens = np.add.reduceat(keep.astype(np.int64), A.rowptr[:-1]) if A.nnz else np.zeros(A.n, np.int64)
+    lens[np.diff(A.rowptr) == 0] = 0
+    rp = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    return g.CSRMatrix(rp, A.cols[keep], A.vals[keep], A.ncols)
+
+
+def test_symmetric_and_transposed_products_match_reference(oracle, reference):
+    """vectorProduct of a SymmetricMatrix and transposedVectorProduct restated
+    in the oracle against the reference's Host code run on one thread (its
+    atomic additions then come in row order): bit-exact; and both against
+    the full / transposed product."""
+    import scipy.sparse as sp
+
+    threads = reference.threads()
+    reference.set_threads(1)
+    try:
+        A = g.diffusion_2d(40, 0.1, 1.0, 3)
+        L = _lower_triangle(A)
+        seg = oracle.build(FORMATS["CSR"], L.row_lengths())
+        x, y0 = g.uniform_vector(A.n, 2), g.uniform_vector(A.n, 3)
+        for al, be, b, e in ((1.0, 0.0, 0, 0), (2.5, -0.5, 0, 0), (1.0, 1.0, 100, 900)):
+            yr = reference.spmv_symmetric(L, x, y0, al, be, b, e)
+            yo = oracle.spmv_symmetric(seg, L.cols, L.vals, x, y0, al, be, b, e)
+            assert np.array_equal(yr, yo), (al, be, b, e)
+        S = sp.csr_matrix((A.vals, A.cols, A.rowptr), shape=(A.n, A.n))
+        assert np.allclose(oracle.spmv_symmetric(seg, L.cols, L.vals, x), S @ x, rtol=1e-13, atol=1e-13)
+        P = g.power_law(3000, 1.73, 500, 4)
+        segP = oracle.build(FORMATS["CSR"], P.row_lengths())
+        xP, yP = g.uniform_vector(P.n, 5), g.uniform_vector(P.ncols, 6)
+        for al, be, b, e in ((1.0, 0.0, 0, 0), (2.5, -0.5, 0, 0), (1.0, 1.0, 100, 2000)):
+            yr = reference.spmv_transposed(P, xP, yP, al, be, b, e)
+            yo = oracle.spmv_transposed(segP, P.cols, P.vals, P.ncols, xP, yP, al, be, b, e)
+            assert np.array_equal(yr, yo), (al, be, b, e)
+        SP = sp.csr_matrix((P.vals, P.cols, P.rowptr), shape=(P.n, P.ncols))
+        assert np.allclose(oracle.spmv_transposed(segP, P.cols, P.vals, P.ncols, xP), SP.T @ xP, rtol=1e-12,
+                           atol=1e-12)
+    finally:
+        reference.set_threads(threads)

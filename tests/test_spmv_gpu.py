@@ -307,3 +307,58 @@ def test_dot():
     b = torch.randn(1_000_003, dtype=torch.float64, device="cuda")
     d = t.dot(a, b).item()
     assert d == pytest.approx(float((a * b).sum().item()), rel=1e-12, abs=1e-9)
+
+
+def _lower_triangle(A):
+    from tnl_b200 import generators as g
+
+    rows = np.repeat(np.arange(A.n), np.diff(A.rowptr))
+    keep = np.asarray(A.cols) <= rows
+    lens = np.bincount(rows[keep], minlength=A.n)
+    rp = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    return g.CSRMatrix(rp, A.cols[keep], A.vals[keep], A.ncols)
+
+
+@pytest.mark.parametrize("fmt", list(FORMATS))
+@pytest.mark.parametrize("org", ["col", "row"])
+@pytest.mark.parametrize("real", [np.float64, np.float32])
+def test_symmetric_and_transposed_products(oracle, mats, fmt, org, real):
+    """vectorProduct of a symmetric matrix (one triangle stored) and
+    transposedVectorProduct, every format, against the oracle (pinned to the
+    reference): the GPU adds the scattered terms atomically, so only the
+    order of the additions differs -- the same bound as the SpMV parity test,
+    with the scale taken over the terms each output entry receives."""
+    t = tnl()
+    tdt = torch.float64 if real == np.float64 else torch.float32
+    from tnl_b200 import generators as g
+
+    for mname, A in mats.items():
+        if mname == "laplacian64":
+            S = _lower_triangle(A)
+            vals = S.vals.astype(real)
+            M = t.SparseMatrix(t.FORMATS[fmt], tdt, ORGS[org], symmetric=True).assign(S.rowptr, S.cols, vals, S.ncols)
+            seg = oracle.build(FORMATS["CSR"], S.row_lengths())
+            x = g.uniform_vector(S.n, 0).astype(real)
+            y0 = g.uniform_vector(S.n, 9).astype(real)
+            # scale: the full (mirrored) matrix's row sums of |a x|
+            absum = row_abs_sums(A.rowptr, A.cols, A.vals.astype(real), x)
+            for alpha, beta, begin, end in ((1.0, 0.0, 0, 0), (0.75, -1.25, 0, 0), (1.0, 1.0, S.n // 3, 2 * S.n // 3)):
+                yref = oracle.spmv_symmetric(seg, S.cols, vals, x, y0, alpha, beta, begin, end)
+                xs, ys = torch.tensor(x, device="cuda"), torch.tensor(y0, device="cuda")
+                M.vectorProduct(xs, ys, alpha, beta, begin, end)
+                assert_spmv_close(ys.cpu().numpy(), yref, abs(alpha) * absum + abs(beta) * np.abs(y0), RTOL[real])
+        vals = A.vals.astype(real)
+        M = t.SparseMatrix(t.FORMATS[fmt], tdt, ORGS[org]).assign(A.rowptr, A.cols, vals, A.ncols)
+        seg = oracle.build(FORMATS["CSR"], A.row_lengths())
+        x = g.uniform_vector(A.n, 4).astype(real)
+        y0 = g.uniform_vector(A.ncols, 5).astype(real)
+        # scale per output column: sum over rows of |a_rc x_r|
+        import scipy.sparse as sp
+
+        absT = np.abs(sp.csr_matrix((np.abs(vals.astype(np.float64)), A.cols, A.rowptr), shape=(A.n, A.ncols)).T
+                      @ np.abs(x.astype(np.float64)))
+        for alpha, beta, begin, end in ((1.0, 0.0, 0, 0), (-2.5, 0.5, 0, 0), (1.0, 1.0, A.ncols // 4, A.ncols // 2)):
+            yref = oracle.spmv_transposed(seg, A.cols, vals, A.ncols, x, y0, alpha, beta, begin, end)
+            xs, ys = torch.tensor(x, device="cuda"), torch.tensor(y0, device="cuda")
+            M.transposedVectorProduct(xs, ys, alpha, beta, begin, end)
+            assert_spmv_close(ys.cpu().numpy(), yref, abs(alpha) * absT + abs(beta) * np.abs(y0), RTOL[real])

@@ -244,10 +244,13 @@ class SparseMatrix:
 
     ``segments`` is one of the format classes, ``real`` torch.float64 or
     torch.float32.  Values and column indexes are CUDA tensors of length
-    getStorageSize(); padding slots hold column -1 and value 0.
+    getStorageSize(); padding slots hold column -1 and value 0.  With
+    ``symmetric=True`` it is SparseMatrix<..., SymmetricMatrix, ...>: one
+    triangle is stored and vectorProduct adds the mirrored entries.
     """
 
-    def __init__(self, segments=CSR, real=torch.float64, organization: int | None = None):
+    def __init__(self, segments=CSR, real=torch.float64, organization: int | None = None, symmetric: bool = False):
+        self.symmetric = bool(symmetric)
         self.segments_cls = segments
         self.real = real
         self.organization = organization
@@ -293,8 +296,9 @@ class SparseMatrix:
         return self
 
     @classmethod
-    def from_csr(cls, A: CSRMatrix, segments=CSR, real=torch.float64, organization: int | None = None) -> "SparseMatrix":
-        M = cls(segments, real, organization)
+    def from_csr(cls, A: CSRMatrix, segments=CSR, real=torch.float64, organization: int | None = None,
+                 symmetric: bool = False) -> "SparseMatrix":
+        M = cls(segments, real, organization, symmetric)
         return M.assign(A.rowptr, A.cols, A.vals, A.ncols)
 
     # -- queries -------------------------------------------------------------
@@ -330,14 +334,53 @@ class SparseMatrix:
             raise TypeError("vector real type must match the matrix real type")
         if not (inVector.is_cuda and outVector.is_cuda and inVector.is_contiguous() and outVector.is_contiguous()):
             raise ValueError("vectors must be contiguous CUDA tensors")
-        k, tps = (launchConfig or LaunchConfiguration()).kernel()
         st = _stream(stream)
+        if self.symmetric:
+            # SparseMatrixBase.hpp:296-330: beta scales y, mirrored entries added atomically
+            check(capi.tnlb_spmv_symmetric(self.segments.handle, _real_code(self.real),
+                                           self.columnIndexes.data_ptr() if self.columnIndexes.numel() else None,
+                                           self.values.data_ptr() if self.values.numel() else None,
+                                           inVector.data_ptr() if inVector.numel() else None,
+                                           outVector.data_ptr() if outVector.numel() else None,
+                                           float(matrixMultiplicator), float(outVectorMultiplicator), int(begin),
+                                           int(end), st))
+            if synchronize:
+                torch.cuda.current_stream().synchronize() if stream is None else stream.synchronize()
+            return
+        k, tps = (launchConfig or LaunchConfiguration()).kernel()
         check(capi.tnlb_spmv(self.segments.handle, _real_code(self.real),
                              self.columnIndexes.data_ptr() if self.columnIndexes.numel() else None,
                              self.values.data_ptr() if self.values.numel() else None, self.columns,
                              inVector.data_ptr() if inVector.numel() else None,
                              outVector.data_ptr() if outVector.numel() else None,
                              float(matrixMultiplicator), float(outVectorMultiplicator), int(begin), int(end), k, tps, st))
+        if synchronize:
+            torch.cuda.current_stream().synchronize() if stream is None else stream.synchronize()
+
+
+    def transposedVectorProduct(self, inVector: torch.Tensor, outVector: torch.Tensor, matrixMultiplicator: float = 1.0,
+                            outVectorMultiplicator: float = 0.0, begin: int = 0, end: int = 0, stream=None,
+                            synchronize: bool = True) -> None:
+        """outVector = matrixMultiplicator * A^T * inVector + outVectorMultiplicator * outVector.
+
+        SparseMatrixBase::transposedVectorProduct (SparseMatrixBase.hpp:542-588);
+        a symmetric matrix uses vectorProduct, as the reference does."""
+        if inVector.numel() != self.rows:
+            raise ValueError("transposedVectorProduct: size of the input vector does not match the number of matrix rows")
+        if outVector.numel() != self.columns:
+            raise ValueError(
+                "transposedVectorProduct: size of the output vector does not match the number of matrix columns")
+        if self.symmetric:
+            return self.vectorProduct(inVector, outVector, matrixMultiplicator, outVectorMultiplicator, begin, end,
+                                      stream=stream, synchronize=synchronize)
+        if inVector.dtype != self.real or outVector.dtype != self.real:
+            raise TypeError("vector real type must match the matrix real type")
+        check(capi.tnlb_spmv_transposed(self.segments.handle, _real_code(self.real),
+                                        self.columnIndexes.data_ptr() if self.columnIndexes.numel() else None,
+                                        self.values.data_ptr() if self.values.numel() else None, self.columns,
+                                        inVector.data_ptr() if inVector.numel() else None,
+                                        outVector.data_ptr() if outVector.numel() else None, float(matrixMultiplicator),
+                                        float(outVectorMultiplicator), int(begin), int(end), _stream(stream)))
         if synchronize:
             torch.cuda.current_stream().synchronize() if stream is None else stream.synchronize()
 

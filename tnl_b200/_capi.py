@@ -98,6 +98,8 @@ tnlb_segments_global_index = _sig("tnlb_segments_global_index", [_p, _p, _p, _i6
 tnlb_matrix_fill_from_csr = _sig("tnlb_matrix_fill_from_csr", [_p, C.c_int, _p, _p, _p, _p, _p, _p])
 tnlb_spmv = _sig("tnlb_spmv", [_p, C.c_int, _p, _p, _i32, _p, _p, _f64, _f64, _i32, _i32, C.c_int, _i32, _p])
 tnlb_spmv_last_launch_count = _sig("tnlb_spmv_last_launch_count", [], _i32)
+tnlb_spmv_symmetric = _sig("tnlb_spmv_symmetric", [_p, C.c_int, _p, _p, _p, _p, _f64, _f64, _i32, _i32, _p])
+tnlb_spmv_transposed = _sig("tnlb_spmv_transposed", [_p, C.c_int, _p, _p, _i32, _p, _p, _f64, _f64, _i32, _i32, _p])
 tnlb_spmv_csr_noalloc = _sig("tnlb_spmv_csr_noalloc",
                              [C.c_int, _i32, _i32, C.c_int64, _p, _p, _p, _p, _p, _f64, _f64, _p])
 tnlb_dot = _sig("tnlb_dot", [C.c_int, _i64, _p, _p, _p, _p])
