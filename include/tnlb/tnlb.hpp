@@ -48,6 +48,7 @@ inline void check(tnlb_status s)
       case TNLB_ERR_OVERFLOW: throw std::overflow_error(msg);
       case TNLB_ERR_NOT_IMPLEMENTED: throw std::logic_error("not implemented: " + msg);
       case TNLB_ERR_OUT_OF_MEMORY: throw std::bad_alloc();
+      case TNLB_ERR_IO: throw std::runtime_error(msg);
       default: throw BackendRuntimeError(msg);
    }
 }
@@ -320,6 +321,18 @@ public:
    }
    Index getRows() const { return rows_; }
    Index getColumns() const { return columns_; }
+   static constexpr bool isSymmetric() { return std::is_same<MatrixType, SymmetricMatrix>::value; }
+   // The stored elements as host CSR (segment order, padding dropped) in FP64.
+   void toHostCSR(std::vector<Index>& rp, std::vector<Index>& cols, std::vector<double>& vals) const
+   {
+      tnlb_host_csr h{};
+      tnlb::check(tnlb_matrix_to_host_csr(seg_, tnlb::real_code<Real>(), columns_idx_.getData(), values_.getData(),
+                                          columns_, &h));
+      rp.assign(h.rowptr, h.rowptr + h.rows + 1);
+      cols.assign(h.cols, h.cols + h.nnz);
+      vals.assign(h.values, h.values + h.nnz);
+      tnlb_host_csr_free(&h);
+   }
    const tnlb_segments* segments() const { return seg_; }
    const Containers::Vector<Real>& getValues() const { return values_; }
    const Containers::Vector<Index>& getColumnIndexes() const { return columns_idx_; }
@@ -329,6 +342,36 @@ private:
    tnlb_segments* seg_ = nullptr;
    Containers::Vector<Real> values_;
    Containers::Vector<Index> columns_idx_;
+};
+
+// MatrixReader::readMtx / MatrixWriter::writeMtx (Matrices/MatrixReader.h,
+// MatrixWriter.h) over tnlb_mtx_read / tnlb_mtx_write.
+template <typename Matrix>
+struct MatrixReader {
+   static void readMtx(const std::string& fileName, Matrix& matrix, bool verbose = false)
+   {
+      (void)verbose;
+      tnlb_host_csr h{};
+      tnlb::check(tnlb_mtx_read(fileName.c_str(), Matrix::isSymmetric() ? 1 : 0, &h));
+      std::vector<int> rp(h.rowptr, h.rowptr + h.rows + 1), cols(h.cols, h.cols + h.nnz);
+      std::vector<typename Matrix::RealType> vals(h.values, h.values + h.nnz);
+      const int rows = h.rows, columns = h.columns;
+      tnlb_host_csr_free(&h);
+      matrix.setFromCSR(rows, columns, rp, cols, vals);
+   }
+};
+
+template <typename Matrix>
+struct MatrixWriter {
+   static void writeMtx(const std::string& fileName, const Matrix& matrix, bool verbose = false)
+   {
+      (void)verbose;
+      std::vector<int> rp, cols;
+      std::vector<double> vals;
+      matrix.toHostCSR(rp, cols, vals);
+      tnlb::check(tnlb_mtx_write(fileName.c_str(), matrix.getRows(), matrix.getColumns(), rp.data(), cols.data(),
+                                 vals.data()));
+   }
 };
 
 }  // namespace Matrices

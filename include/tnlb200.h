@@ -37,7 +37,8 @@ typedef struct CUstream_st* tnlb_stream; /* == cudaStream_t */
  * CUDA -> Exceptions::BackendRuntimeError (Backend/Macros.h:14-24),
  * NOT_IMPLEMENTED -> Exceptions::NotImplementedError,
  * BREAKDOWN -> the `throw 1` of GMRES::update (Solvers/Linear/GMRES.hpp:657-667),
- * TIMEOUT -> a bounded device-side wait gave up (no reference counterpart). */
+ * TIMEOUT -> a bounded device-side wait gave up (no reference counterpart),
+ * IO -> std::runtime_error of the MatrixMarket reader and writer. */
 typedef enum {
    TNLB_OK = 0,
    TNLB_ERR_INVALID_ARGUMENT = 1,
@@ -46,7 +47,8 @@ typedef enum {
    TNLB_ERR_NOT_IMPLEMENTED = 4,
    TNLB_ERR_BREAKDOWN = 5,
    TNLB_ERR_TIMEOUT = 6,
-   TNLB_ERR_OUT_OF_MEMORY = 7
+   TNLB_ERR_OUT_OF_MEMORY = 7,
+   TNLB_ERR_IO = 8
 } tnlb_status;
 
 /* Real types of values and vectors. */
@@ -260,6 +262,42 @@ tnlb_status tnlb_spmv_transposed(const tnlb_segments* seg, tnlb_real real, const
 tnlb_status tnlb_spmv_csr_noalloc(tnlb_real real, int32_t rows, int32_t columns, int64_t nnz,
                                   const int32_t* d_rowptr, const int32_t* d_cols, const void* d_values,
                                   const void* d_x, void* d_y, double alpha, double beta, tnlb_stream stream);
+
+/* ------------------------------------------------------------ files */
+
+/* A CSR matrix in HOST memory, as read from a file. */
+typedef struct {
+   int32_t rows;
+   int32_t columns;
+   int64_t nnz;
+   int32_t* rowptr; /* rows + 1 */
+   int32_t* cols;   /* nnz, ascending in each row */
+   double* values;  /* nnz */
+} tnlb_host_csr;
+
+/* Read a MatrixMarket file as MatrixReader::readMtx does
+ * (Matrices/MatrixReader.hpp:18-330): coordinate real / integer / pattern,
+ * general or symmetric; a repeated position keeps its last value; with
+ * symmetric_storage != 0 (a SymmetricMatrix) the lower triangle is kept,
+ * else a symmetric file is expanded to both triangles.  The arrays are
+ * allocated here; release them with tnlb_host_csr_free.  Errors (with the
+ * reader's messages) return TNLB_ERR_IO.  Host only: needs no GPU. */
+tnlb_status tnlb_mtx_read(const char* path, int32_t symmetric_storage, tnlb_host_csr* out);
+void tnlb_host_csr_free(tnlb_host_csr* m);
+
+/* The stored elements of a matrix (any format) as host CSR in segment order,
+ * padding dropped, values in FP64 -- what getRow() walks row by row.  The
+ * arrays are allocated here; release them with tnlb_host_csr_free.
+ * Synchronous. */
+tnlb_status tnlb_matrix_to_host_csr(const tnlb_segments* seg, tnlb_real real, const int32_t* d_cols,
+                                    const void* d_values, int32_t columns, tnlb_host_csr* out);
+
+/* Write host CSR arrays as MatrixWriter::writeMtx does
+ * (Matrices/MatrixWriter.hpp:107-129): "coordinate real general", 1-based
+ * "row column value" lines of widths 9, 9, 12 at default stream precision,
+ * zero values and padding (column -1) skipped.  Host only. */
+tnlb_status tnlb_mtx_write(const char* path, int32_t rows, int32_t columns, const int32_t* h_rowptr,
+                           const int32_t* h_cols, const double* h_values);
 
 /* ------------------------------------------------------------ vectors */
 

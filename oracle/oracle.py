@@ -344,6 +344,8 @@ class Reference:
             ("ref_solve", [i32, i32, i32, p, p, p, p, p, f64, i32, i32, i32, i32, p, p, p], C.c_int),
             ("ref_solve_ext", [i32, i32, i32, p, p, p, p, p, f64, i32, i32, i32, p, p, p], C.c_int),
             ("ref_spmv_symmetric_f64", [i32, p, p, p, p, p, f64, f64, i32, i32], None),
+            ("ref_mtx_read", [C.c_char_p, i32, p, p, p, p, p, p, C.c_char_p, i32], C.c_int),
+            ("ref_mtx_write", [C.c_char_p, i32, i32, p, p, p], None),
             ("ref_spmv_transposed_f64", [i32, i32, p, p, p, p, p, f64, f64, i32, i32], None),
             ("ref_prec_apply", [i32, p, p, p, i32, p, p], C.c_int),
             ("ref_omp_threads", [], C.c_int),
@@ -444,6 +446,26 @@ class Reference:
         t = f(kind, int(colmajor), A.n, A.ncols, rowptr.ctypes.data, cols.ctypes.data, vals.ctypes.data, x.ctypes.data,
               y.ctypes.data, alpha, beta, begin, end, reps)
         return y, t
+
+    def mtx_read(self, path, symmetric: bool = False):
+        """The reference's MatrixReader::readMtx: (rows, columns, rowptr, cols, vals) or RuntimeError."""
+        rows, columns, nnz = C.c_int(), C.c_int(), C.c_long()
+        err = C.create_string_buffer(512)
+        p = str(path).encode()
+        if self.L.ref_mtx_read(p, int(symmetric), C.byref(rows), C.byref(columns), C.byref(nnz), None, None, None,
+                               err, 512):
+            raise RuntimeError(err.value.decode())
+        rp = np.zeros(rows.value + 1, np.int32)
+        cols = np.zeros(max(nnz.value, 1), np.int32)
+        vals = np.zeros(max(nnz.value, 1))
+        self.L.ref_mtx_read(p, int(symmetric), C.byref(rows), C.byref(columns), C.byref(nnz), rp.ctypes.data,
+                            cols.ctypes.data, vals.ctypes.data, err, 512)
+        return rows.value, columns.value, rp, cols[:nnz.value], vals[:nnz.value]
+
+    def mtx_write(self, path, A):
+        rowptr, cols = _i32(A.rowptr), _i32(A.cols)
+        vals = np.ascontiguousarray(A.vals, np.float64)
+        self.L.ref_mtx_write(str(path).encode(), A.n, A.ncols, rowptr.ctypes.data, cols.ctypes.data, vals.ctypes.data)
 
     def spmv_symmetric(self, A, x, y=None, alpha=1.0, beta=0.0, begin=0, end=0):
         """The reference's vectorProduct of a SymmetricMatrix CSR matrix (A holds one triangle)."""

@@ -25,6 +25,8 @@
 #include <TNL/Algorithms/Segments/SlicedEllpack.h>
 #include <TNL/Config/ParameterContainer.h>
 #include <TNL/Containers/Vector.h>
+#include <TNL/Matrices/MatrixReader.h>
+#include <TNL/Matrices/MatrixWriter.h>
 #include <TNL/Matrices/SparseMatrix.h>
 #include <TNL/Solvers/Linear/BICGStab.h>
 #include <TNL/Solvers/Linear/BICGStabL.h>
@@ -426,6 +428,56 @@ ref_spmv_transposed_f64( int n, int ncols, const int* rowptr, const int* cols, c
    A.transposedVectorProduct( xv, yv, alpha, beta, begin, end );
    for( int i = 0; i < ncols; i++ )
       y[ i ] = yv[ i ];
+}
+
+// MatrixReader::readMtx into a general (symmetric == 0) or SymmetricMatrix
+// CSR matrix on the host.  First call with null arrays returns the sizes in
+// rows/columns/nnz; the second fills rowptr/cols/vals.  Returns 0, or -1
+// with the exception's message in `err` (size errLen).
+int
+ref_mtx_read( const char* path, int symmetric, int* rows, int* columns, long* nnz, int* rowptr, int* cols, double* vals,
+              char* err, int errLen )
+{
+   auto out = [ & ]( auto& A ) -> int
+   {
+      *rows = A.getRows();
+      *columns = A.getColumns();
+      const auto& off = A.getSegments().getOffsets();
+      *nnz = off[ A.getRows() ];
+      if( rowptr ) {
+         for( int i = 0; i <= A.getRows(); i++ )
+            rowptr[ i ] = off[ i ];
+         for( long k = 0; k < *nnz; k++ ) {
+            cols[ k ] = A.getColumnIndexes()[ k ];
+            vals[ k ] = A.getValues()[ k ];
+         }
+      }
+      return 0;
+   };
+   try {
+      if( symmetric ) {
+         Matrices::SparseMatrix< double, Host, int, Matrices::SymmetricMatrix, Seg::CSR > A;
+         Matrices::MatrixReader< decltype( A ) >::readMtx( path, A );
+         return out( A );
+      }
+      Mat< double, Seg::CSR > A;
+      Matrices::MatrixReader< decltype( A ) >::readMtx( path, A );
+      return out( A );
+   }
+   catch( const std::exception& e ) {
+      std::strncpy( err, e.what(), errLen - 1 );
+      err[ errLen - 1 ] = 0;
+      return -1;
+   }
+}
+
+// MatrixWriter::writeMtx of a general CSR matrix given by host arrays.
+void
+ref_mtx_write( const char* path, int n, int ncols, const int* rowptr, const int* cols, const double* vals )
+{
+   Mat< double, Seg::CSR > A;
+   makeCSR( A, n, ncols, rowptr, cols, vals );
+   Matrices::MatrixWriter< decltype( A ) >::writeMtx( path, A );
 }
 
 // Solve A x = b with TNL's CG (solver 0), BICGStab (1) or GMRES (2), with no

@@ -3,6 +3,7 @@ that include/tnlb200.h declares; host-side argument checks."""
 import re
 from pathlib import Path
 
+import numpy as np
 import pytest
 
 ROOT = Path(__file__).resolve().parents[1]
@@ -61,3 +62,65 @@ def test_cpp_dropin_header_compiles():
     r = subprocess.run([nvcc, "-std=c++17", "-c", str(ROOT / "tests" / "cpp" / "dropin.cpp"), "-I", str(ROOT / "include"),
                         "-o", str(out / "dropin.o")], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+MTX_CASES = {
+    "general": "%%MatrixMarket matrix coordinate real general\n% a comment\n4 5 6\n1 1 2.5\n2 3 -1\n4 5 1e-3\n"
+               "3 2 7\n1 4 0\n2 3 4.25\n",
+    "symmetric": "%%MatrixMarket matrix coordinate real symmetric\n3 3 4\n1 1 4\n2 1 -1\n3 3 2\n3 1 0.5\n",
+    "pattern": "%%MatrixMarket matrix coordinate pattern general\n3 3 3\n1 2\n3 1\n2 2\n",
+    "integer_spaces": "%%MatrixMarket   matrix coordinate integer general\n%\n  2   2   2\n 1  1   3\n\n2 2 -4\n",
+}
+
+
+@pytest.mark.parametrize("case", list(MTX_CASES))
+@pytest.mark.parametrize("symmetric", [False, True])
+def test_mtx_read_matches_reference(tmp_path, reference, case, symmetric):
+    """tnlb_mtx_read (host code of the library, no GPU needed) against the
+    reference's own MatrixReader::readMtx: same CSR arrays, or the same error."""
+    import tnl_b200
+
+    f = tmp_path / f"{case}.mtx"
+    f.write_text(MTX_CASES[case])
+    try:
+        r = reference.mtx_read(f, symmetric)
+    except RuntimeError as e:
+        with pytest.raises(RuntimeError) as got:
+            tnl_b200.read_mtx(f, symmetric)
+        assert str(got.value) == str(e)
+        return
+    A = tnl_b200.read_mtx(f, symmetric)
+    assert (A.n, A.ncols) == (r[0], r[1])
+    assert np.array_equal(A.rowptr, r[2]) and np.array_equal(A.cols, r[3]) and np.array_equal(A.vals, r[4])
+
+
+def test_mtx_errors_match_reference(tmp_path, reference):
+    import tnl_b200
+
+    bad = {"header": "%%MatrixMarket matrix array real general\n2 2\n1 2\n3 4\n",
+           "size": "%%MatrixMarket matrix coordinate real general\n2 2\n",
+           "outside": "%%MatrixMarket matrix coordinate real general\n2 2 1\n3 1 1.0\n",
+           "words": "%%MatrixMarket matrix coordinate real general\n2 2 1\n1 1\n"}
+    for name, text in bad.items():
+        f = tmp_path / f"{name}.mtx"
+        f.write_text(text)
+        with pytest.raises(RuntimeError) as e_ref:
+            reference.mtx_read(f, False)
+        with pytest.raises(RuntimeError) as e_ours:
+            tnl_b200.read_mtx(f, False)
+        assert str(e_ours.value) == str(e_ref.value), name
+
+
+def test_mtx_write_matches_reference_bytes(tmp_path, reference):
+    """tnlb_mtx_write writes the bytes of the reference's MatrixWriter::writeMtx."""
+    import tnl_b200
+    from tnl_b200 import generators as g
+
+    A = g.power_law(300, 1.73, 40, 3)
+    A.vals[::7] = 0.0  # zero values are skipped by both
+    ours, ref = tmp_path / "ours.mtx", tmp_path / "ref.mtx"
+    tnl_b200.write_mtx(ours, A)
+    reference.mtx_write(ref, A)
+    assert ours.read_bytes() == ref.read_bytes()
+    B = tnl_b200.read_mtx(ours)
+    assert B.n == A.n and B.ncols == A.ncols

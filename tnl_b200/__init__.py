@@ -32,7 +32,7 @@ __all__ = [
     "CSR", "Ellpack", "SlicedEllpack", "ChunkedEllpack", "BiEllpack", "AdaptiveCSR", "SparseMatrix",
     "LaunchConfiguration", "ColumnMajorOrder", "RowMajorOrder", "CSRMatrix", "check", "BackendRuntimeError",
     "CG", "BICGStab", "GMRES", "FGMRES", "TFQMR", "BICGStabL", "IDRs", "Diagonal", "ILU0", "FSAI", "FSAI2",
-    "solve_mixed", "true_residual",
+    "solve_mixed", "true_residual", "read_mtx", "write_mtx",
 ]
 
 ColumnMajorOrder = capi.COLUMN_MAJOR
@@ -358,6 +358,18 @@ class SparseMatrix:
             torch.cuda.current_stream().synchronize() if stream is None else stream.synchronize()
 
 
+    def toHostCSR(self) -> CSRMatrix:
+        """The stored elements as host CSR (segment order, padding dropped, FP64 values)."""
+        h = capi.HostCSR()
+        check(capi.tnlb_matrix_to_host_csr(self.segments.handle, _real_code(self.real),
+                                           self.columnIndexes.data_ptr() if self.columnIndexes.numel() else None,
+                                           self.values.data_ptr() if self.values.numel() else None, self.columns,
+                                           C.byref(h)))
+        try:
+            return _host_csr_to_numpy(h)
+        finally:
+            capi.tnlb_host_csr_free(C.byref(h))
+
     def transposedVectorProduct(self, inVector: torch.Tensor, outVector: torch.Tensor, matrixMultiplicator: float = 1.0,
                             outVectorMultiplicator: float = 0.0, begin: int = 0, end: int = 0, stream=None,
                             synchronize: bool = True) -> None:
@@ -383,6 +395,39 @@ class SparseMatrix:
                                         float(outVectorMultiplicator), int(begin), int(end), _stream(stream)))
         if synchronize:
             torch.cuda.current_stream().synchronize() if stream is None else stream.synchronize()
+
+
+def _host_csr_to_numpy(h: "capi.HostCSR") -> CSRMatrix:
+    nnz = int(h.nnz)
+    rp = np.ctypeslib.as_array(h.rowptr, shape=(h.rows + 1,)).copy()
+    cols = np.ctypeslib.as_array(h.cols, shape=(max(nnz, 1),))[:nnz].copy()
+    vals = np.ctypeslib.as_array(h.values, shape=(max(nnz, 1),))[:nnz].copy()
+    return CSRMatrix(rp, cols, vals, h.columns)
+
+
+def read_mtx(path, symmetric: bool = False) -> CSRMatrix:
+    """MatrixReader::readMtx (Matrices/MatrixReader.hpp): a MatrixMarket file as
+    host CSR.  ``symmetric=True`` reads into symmetric storage (the lower
+    triangle), as for a SymmetricMatrix; RuntimeError carries the reader's
+    messages."""
+    h = capi.HostCSR()
+    check(capi.tnlb_mtx_read(str(path).encode(), int(bool(symmetric)), C.byref(h)))
+    try:
+        return _host_csr_to_numpy(h)
+    finally:
+        capi.tnlb_host_csr_free(C.byref(h))
+
+
+def write_mtx(path, A) -> None:
+    """MatrixWriter::writeMtx (Matrices/MatrixWriter.hpp): a CSRMatrix or a
+    SparseMatrix written as "coordinate real general"."""
+    if isinstance(A, SparseMatrix):
+        A = A.toHostCSR()
+    rp = np.ascontiguousarray(A.rowptr, np.int32)
+    cols = np.ascontiguousarray(A.cols, np.int32)
+    vals = np.ascontiguousarray(A.vals, np.float64)
+    check(capi.tnlb_mtx_write(str(path).encode(), len(rp) - 1, int(A.ncols), rp.ctypes.data,
+                              cols.ctypes.data if cols.size else None, vals.ctypes.data if vals.size else None))
 
 
 def dot(a: torch.Tensor, b: torch.Tensor) -> torch.Tensor:

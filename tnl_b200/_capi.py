@@ -20,7 +20,7 @@ if not LIB_PATH.exists():
 lib = C.CDLL(str(LIB_PATH))
 
 # status codes (tnlb_status)
-OK, ERR_INVALID_ARGUMENT, ERR_OVERFLOW, ERR_CUDA, ERR_NOT_IMPLEMENTED, ERR_BREAKDOWN, ERR_TIMEOUT, ERR_OOM = range(8)
+OK, ERR_INVALID_ARGUMENT, ERR_OVERFLOW, ERR_CUDA, ERR_NOT_IMPLEMENTED, ERR_BREAKDOWN, ERR_TIMEOUT, ERR_OOM, ERR_IO = range(9)
 F32, F64 = 0, 1
 CSR, ELLPACK, SLICED_ELLPACK, CHUNKED_ELLPACK, BIELLPACK, ADAPTIVE_CSR = range(6)
 COLUMN_MAJOR, ROW_MAJOR = 0, 1
@@ -67,6 +67,11 @@ class SolverParams(C.Structure):
     ]
 
 
+class HostCSR(C.Structure):
+    _fields_ = [("rows", C.c_int32), ("columns", C.c_int32), ("nnz", C.c_int64), ("rowptr", C.POINTER(C.c_int32)),
+                ("cols", C.POINTER(C.c_int32)), ("values", C.POINTER(C.c_double))]
+
+
 class SolveResult(C.Structure):
     _fields_ = [("converged", C.c_int32), ("iterations", C.c_int32), ("residue", C.c_double),
                 ("status_detail", C.c_int32), ("reserved", C.c_int32)]
@@ -98,6 +103,10 @@ tnlb_segments_global_index = _sig("tnlb_segments_global_index", [_p, _p, _p, _i6
 tnlb_matrix_fill_from_csr = _sig("tnlb_matrix_fill_from_csr", [_p, C.c_int, _p, _p, _p, _p, _p, _p])
 tnlb_spmv = _sig("tnlb_spmv", [_p, C.c_int, _p, _p, _i32, _p, _p, _f64, _f64, _i32, _i32, C.c_int, _i32, _p])
 tnlb_spmv_last_launch_count = _sig("tnlb_spmv_last_launch_count", [], _i32)
+tnlb_mtx_read = _sig("tnlb_mtx_read", [C.c_char_p, _i32, C.POINTER(HostCSR)])
+tnlb_mtx_write = _sig("tnlb_mtx_write", [C.c_char_p, _i32, _i32, _p, _p, _p])
+tnlb_host_csr_free = _sig("tnlb_host_csr_free", [C.POINTER(HostCSR)], None)
+tnlb_matrix_to_host_csr = _sig("tnlb_matrix_to_host_csr", [_p, C.c_int, _p, _p, _i32, C.POINTER(HostCSR)])
 tnlb_spmv_symmetric = _sig("tnlb_spmv_symmetric", [_p, C.c_int, _p, _p, _p, _p, _f64, _f64, _i32, _i32, _p])
 tnlb_spmv_transposed = _sig("tnlb_spmv_transposed", [_p, C.c_int, _p, _p, _i32, _p, _p, _f64, _f64, _i32, _i32, _p])
 tnlb_spmv_csr_noalloc = _sig("tnlb_spmv_csr_noalloc",
@@ -146,6 +155,8 @@ def check(status: int) -> None:
         raise DeviceTimeoutError(msg)
     if status == ERR_OOM:
         raise MemoryError(msg)
+    if status == ERR_IO:
+        raise RuntimeError(msg)
     raise BackendRuntimeError(msg)
 
 
