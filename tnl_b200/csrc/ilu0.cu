@@ -7,7 +7,8 @@
 // references, row i of U on the rows j > i.  Levels are computed once on the
 // host (one pass over the pattern in row order), rows of a level run in
 // parallel, one kernel launch per level; the solves are captured once in a
-// CUDA graph and replayed.
+// CUDA graph and replayed; runs of small levels share one single-block
+// launch (a __syncthreads between levels).
 //
 // Arithmetic per row follows ILU0.hpp:59-118 (IKJ order, L_ik = A_ik/U_kk,
 // then the updates of the rest of L_i and of U_i with U(k, j) looked up in
@@ -123,6 +124,50 @@ __global__ void k_upper_level(const int32_t* __restrict__ rows, int32_t count, c
    x[i] = div_rn(xi, lu[u0]);
 }
 
+// Runs of consecutive small levels in ONE block: the block walks the levels
+// in order, a __syncthreads between levels making each level's x visible to
+// the next (the same block, so no grid-wide wait); the row arithmetic is
+// that of k_lower_level / k_upper_level.
+constexpr int kIluRunThreads = 1024;
+constexpr int32_t kIluSmallLevel = 2048;
+
+template <typename Real>
+__global__ void __launch_bounds__(kIluRunThreads)
+   k_lower_run(const int32_t* __restrict__ rows, const int32_t* __restrict__ lvl, int32_t l0, int32_t l1,
+               const int32_t* __restrict__ cols, const Real* __restrict__ lu, const int32_t* __restrict__ lstart,
+               const int32_t* __restrict__ ustart, const Real* __restrict__ b, Real* __restrict__ x)
+{
+   for (int32_t l = l0; l < l1; l++) {
+      const int32_t s0 = lvl[l], s1 = lvl[l + 1];
+      for (int32_t t = s0 + threadIdx.x; t < s1; t += blockDim.x) {
+         const int32_t i = rows[t];
+         Real xi = b[i];
+         for (int32_t c = lstart[i]; c < ustart[i]; c++) xi = sub_rn(xi, mul_rn(lu[c], x[cols[c]]));
+         x[i] = xi;
+      }
+      __syncthreads();
+   }
+}
+
+template <typename Real>
+__global__ void __launch_bounds__(kIluRunThreads)
+   k_upper_run(const int32_t* __restrict__ rows, const int32_t* __restrict__ lvl, int32_t l0, int32_t l1,
+               const int32_t* __restrict__ cols, const Real* __restrict__ lu, const int32_t* __restrict__ ustart,
+               const int32_t* __restrict__ uend, Real* __restrict__ x)
+{
+   for (int32_t l = l0; l < l1; l++) {
+      const int32_t s0 = lvl[l], s1 = lvl[l + 1];
+      for (int32_t t = s0 + threadIdx.x; t < s1; t += blockDim.x) {
+         const int32_t i = rows[t];
+         const int32_t u0 = ustart[i];
+         Real xi = x[i];
+         for (int32_t c = u0 + 1; c < uend[i]; c++) xi = sub_rn(xi, mul_rn(lu[c], x[cols[c]]));
+         x[i] = div_rn(xi, lu[u0]);
+      }
+      __syncthreads();
+   }
+}
+
 struct Ilu0Base {
    virtual ~Ilu0Base() = default;
    virtual tnlb_status apply(const void* b, void* x, cudaStream_t st) = 0;
@@ -131,7 +176,7 @@ struct Ilu0Base {
 template <typename Real>
 struct Ilu0 : Ilu0Base {
    int32_t n = 0;
-   DeviceBuffer rp, cols, lu, lstart, ustart, uend, lrows, urows, tmp;
+   DeviceBuffer rp, cols, lu, lstart, ustart, uend, lrows, urows, tmp, dlptr, duptr;
    std::vector<int32_t> lptr, uptr;  // level boundaries into lrows / urows
    cudaGraphExec_t exec = nullptr;
    const Real* g_b = nullptr;
@@ -144,19 +189,43 @@ struct Ilu0 : Ilu0Base {
       if (cs) cudaStreamDestroy(cs);
    }
 
+   // Levels in order: a run of consecutive levels of at most kIluSmallLevel
+   // rows goes to one single-block launch, a larger level to its own grid.
    void enqueue(const Real* b, Real* x, cudaStream_t st)
    {
-      for (size_t l = 0; l + 1 < lptr.size(); l++) {
+      const int32_t nl = (int32_t)lptr.size() - 1;
+      for (int32_t l = 0; l < nl;) {
+         if (lptr[l + 1] - lptr[l] <= kIluSmallLevel) {
+            int32_t e = l;
+            while (e < nl && lptr[e + 1] - lptr[e] <= kIluSmallLevel) e++;
+            k_lower_run<Real><<<1, kIluRunThreads, 0, st>>>(lrows.as<int32_t>(), dlptr.as<int32_t>(), l, e,
+                                                            cols.as<int32_t>(), lu.as<Real>(), lstart.as<int32_t>(),
+                                                            ustart.as<int32_t>(), b, x);
+            l = e;
+            continue;
+         }
          const int32_t cnt = lptr[l + 1] - lptr[l];
          k_lower_level<Real><<<(cnt + 127) / 128, 128, 0, st>>>(lrows.as<int32_t>() + lptr[l], cnt, cols.as<int32_t>(),
                                                                lu.as<Real>(), lstart.as<int32_t>(),
                                                                ustart.as<int32_t>(), b, x);
+         l++;
       }
-      for (size_t l = 0; l + 1 < uptr.size(); l++) {
+      const int32_t nu = (int32_t)uptr.size() - 1;
+      for (int32_t l = 0; l < nu;) {
+         if (uptr[l + 1] - uptr[l] <= kIluSmallLevel) {
+            int32_t e = l;
+            while (e < nu && uptr[e + 1] - uptr[e] <= kIluSmallLevel) e++;
+            k_upper_run<Real><<<1, kIluRunThreads, 0, st>>>(urows.as<int32_t>(), duptr.as<int32_t>(), l, e,
+                                                            cols.as<int32_t>(), lu.as<Real>(), ustart.as<int32_t>(),
+                                                            uend.as<int32_t>(), x);
+            l = e;
+            continue;
+         }
          const int32_t cnt = uptr[l + 1] - uptr[l];
          k_upper_level<Real><<<(cnt + 127) / 128, 128, 0, st>>>(urows.as<int32_t>() + uptr[l], cnt, cols.as<int32_t>(),
                                                                lu.as<Real>(), ustart.as<int32_t>(),
                                                                uend.as<int32_t>(), x);
+         l++;
       }
    }
 
@@ -258,6 +327,12 @@ tnlb_status create_t(const tnlb_segments* seg, const int32_t* cols_in, const Rea
    TNLB_CUDA_TRY(cudaMemcpyAsync(P->uend.ptr, ue.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
    TNLB_CUDA_TRY(cudaMemcpyAsync(P->lrows.ptr, lrows.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
    TNLB_CUDA_TRY(cudaMemcpyAsync(P->urows.ptr, urows.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
+   TNLB_TRY_STATUS(P->dlptr.alloc(sizeof(int32_t) * P->lptr.size()));
+   TNLB_TRY_STATUS(P->duptr.alloc(sizeof(int32_t) * P->uptr.size()));
+   TNLB_CUDA_TRY(cudaMemcpyAsync(P->dlptr.ptr, P->lptr.data(), sizeof(int32_t) * P->lptr.size(), cudaMemcpyHostToDevice,
+                                 st));
+   TNLB_CUDA_TRY(cudaMemcpyAsync(P->duptr.ptr, P->uptr.data(), sizeof(int32_t) * P->uptr.size(), cudaMemcpyHostToDevice,
+                                 st));
    // factorisation, level by level of L
    for (size_t l = 0; l + 1 < P->lptr.size(); l++) {
       const int32_t c = P->lptr[l + 1] - P->lptr[l];

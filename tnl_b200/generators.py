@@ -221,8 +221,10 @@ def _stencil_from_coeffs(k: np.ndarray, velocity=None) -> CSRMatrix:
     """Assemble the cell-centred finite-volume operator for coefficient field k.
 
     ``velocity`` (optional) is a tuple of face-normal velocities per axis,
-    each of shape k.shape with the last index along that axis being the
-    face on the + side; first-order upwinding adds the convective flux.
+    axis a holding the shape[a] + 1 faces along a (face i between cells i-1
+    and i, faces 0 and shape[a] on the boundary); first-order upwinding adds
+    the convective flux, inflow through a boundary face carrying the
+    Dirichlet value 0.
     Rows are in natural lexicographic order (last axis fastest) and columns
     ascend inside each row.
     """
@@ -251,17 +253,10 @@ def _stencil_from_coeffs(k: np.ndarray, velocity=None) -> CSRMatrix:
             off = -coef
             d = coef + wall
             if velocity is not None:
-                v = velocity[a]  # velocity on the + face of each cell along axis a
-                if side == 1:
-                    vf = v
-                else:
-                    vf = np.zeros(shape)
-                    src = [slice(None)] * dim
-                    src[a] = slice(0, shape[a] - 1)
-                    dst = [slice(None)] * dim
-                    dst[a] = slice(1, shape[a])
-                    vf[tuple(dst)] = v[tuple(src)]
-                    vf = -vf  # outward normal points to -a
+                v = velocity[a]  # shape[a] + 1 faces along axis a
+                face = [slice(None)] * dim
+                face[a] = slice(1, shape[a] + 1) if side == 1 else slice(0, shape[a])
+                vf = v[tuple(face)] if side == 1 else -v[tuple(face)]  # outward normal
                 out = np.maximum(vf, 0.0)
                 inn = np.minimum(vf, 0.0)
                 d = d + out
@@ -321,11 +316,11 @@ def convection_diffusion_3d(N: int, peclet_range=(10.0, 1000.0), sigma: float = 
     ux = d(psi[2], 1)[:, :, :-1] - d(psi[1], 2)[:, :-1, :]
     uy = d(psi[0], 2)[:-1, :, :] - d(psi[2], 0)[:, :, :-1]
     uz = d(psi[1], 0)[:, :-1, :] - d(psi[0], 1)[:-1, :, :]
-    vel = [ux[1:, :, :], uy[:, 1:, :], uz[:, :, 1:]]
+    vel = [ux, uy, uz]
     # one uniform factor keeps the field divergence free; it puts the
-    # geometric mean of the cell Peclet number |v| h / k at the geometric
-    # centre of peclet_range (h = 1/N)
-    speed = np.sqrt(sum(v * v for v in vel)) + 1e-300
+    # geometric mean of the cell Peclet number |v| h / k (|v| from the
+    # cell's + faces) at the geometric centre of peclet_range (h = 1/N)
+    speed = np.sqrt(ux[1:, :, :] ** 2 + uy[:, 1:, :] ** 2 + uz[:, :, 1:] ** 2) + 1e-300
     pe = speed / (N * k)
     centre = 0.5 * (np.log(peclet_range[0]) + np.log(peclet_range[1]))
     scale = np.exp(centre - np.mean(np.log(pe)))
