@@ -408,6 +408,31 @@ tnlb_status tnlb_solve_mixed(const tnlb_solver_params* params, const tnlb_segmen
                              const tnlb_precond* inner, tnlb_stream stream, tnlb_solve_result* result,
                              int32_t* outer_iterations);
 
+/* Mixed-precision PCG with reliable updates (no counterpart in the
+ * reference).  CG iterates on an FP32 copy of the values, with vectors of
+ * type `vectors` (TNLB_F32: FP32 vectors; TNLB_F64: FP64 vectors, only the
+ * matrix and preconditioner stored in FP32) and dot products accumulated in
+ * FP64.  Its correction is folded into the FP64 x, and the residual is
+ * replaced by the FP64 b - A x, whenever the recursive residual norm has
+ * fallen below max(delta * |r| at the last update,
+ * convergence_residue * |b|).  The search direction is kept across an
+ * update, so unlike tnlb_solve_mixed the Krylov space is not restarted.
+ *
+ * The preconditioner is `inner` (an FP32 Jacobi or symmetric FSAI
+ * preconditioner of this matrix, e.g. a learned FSAI) or, when NULL, one of
+ * kind `inner_precond` (NONE, JACOBI or FSAI) built from the FP32 values.
+ * Stops when ||b - A x|| / ||b|| < params->convergence_residue (the TRUE
+ * FP64 residual, computed as tnlb_true_residual computes it) or after
+ * params->max_iterations FP32 iterations.  result->iterations counts FP32
+ * iterations, result->residue is the true residual,
+ * result->status_detail = 1 on a breakdown ((p, A p) zero or not finite),
+ * and *reliable_updates counts the updates.  Synchronous. */
+tnlb_status tnlb_solve_mixed_reliable(const tnlb_solver_params* params, const tnlb_segments* seg,
+                                      const int32_t* d_cols, const double* d_values, const double* d_b, double* d_x,
+                                      double delta, tnlb_real vectors, tnlb_precond_kind inner_precond,
+                                      const tnlb_precond* inner, tnlb_stream stream, tnlb_solve_result* result,
+                                      int32_t* reliable_updates);
+
 /* Build a preconditioner for a matrix -- Preconditioner::update
  * (Preconditioners/Preconditioner.h:96-110; Diagonal.hpp:15-36,
  * ILU0.hpp:15-118).  The values must stay valid while it is used.

@@ -121,6 +121,7 @@ class Oracle:
             ("orc_idrs", [i32, p, p, p, C.c_int, C.c_int, C.c_int, p, p, p, C.POINTER(SolverState)], C.c_int),
             ("orc_idrs_shadow", [i32, i32, p], None),
             ("orc_true_residual", [i32, p, p, p, p, p], f64),
+            ("orc_pcg_reliable", [i32, p, p, p, C.c_int, p, p, f64, f64, i32, C.c_int, p, p, p], C.c_int),
             ("orc_ilu0_factor", [i32, p, p, p, p, p, p, p, p, p], C.c_int),
             ("orc_prec_apply", [i32, p, p, p, C.c_int, p, p], C.c_int),
         ]:
@@ -293,6 +294,18 @@ class Oracle:
             raise ValueError(solver)
         return {"x": x, "converged": ok == 1, "status": ok, "iterations": S.iterations, "residue": S.residue,
                 "history": hist}
+
+    def pcg_reliable(self, A, b, precond: int = 1, tol=1e-8, delta=0.1, maxit=100000, x0=None, vec64=False):
+        """The library's mixed-precision PCG with reliable updates (FP32
+        values, FP32 or FP64 vectors, FP64 updates); precond 0 none, 1 Jacobi."""
+        rowptr, cols, vals = _i32(A.rowptr), _i32(A.cols), np.ascontiguousarray(A.vals, np.float64)
+        b = np.ascontiguousarray(b, np.float64)
+        x = np.zeros(A.n) if x0 is None else np.array(x0, np.float64, copy=True)
+        it, upd, res = C.c_int32(), C.c_int32(), C.c_double()
+        ok = self.L.orc_pcg_reliable(A.n, rowptr.ctypes.data, cols.ctypes.data, vals.ctypes.data, precond,
+                                     b.ctypes.data, x.ctypes.data, tol, delta, maxit, int(vec64), C.byref(it),
+                                     C.byref(upd), C.byref(res))
+        return {"x": x, "converged": ok == 1, "iterations": it.value, "updates": upd.value, "residue": res.value}
 
     def true_residual(self, A, b, x) -> float:
         rowptr, cols, vals = _i32(A.rowptr), _i32(A.cols), np.ascontiguousarray(A.vals, np.float64)

@@ -1862,3 +1862,128 @@ done:
    prec_free(&Pc);
    return ok;
 }
+
+/* Mixed-precision PCG with reliable updates -- the library's own solver
+ * (no counterpart in the reference), restated for its tests: CG on FP32
+ * values with vectors of type VT (float or double; rows summed in VT, dot
+ * products in FP64); the correction xc is folded into the FP64 x and r
+ * replaced by (VT)(b - A x) (FP64 product) whenever the recursive |r|^2
+ * falls below max(delta |r_u|, tol |b|)^2, r_u the residual of the last
+ * update; p is kept, beta = (r, z)_new / (r, z)_old.  precond: 0 none,
+ * 1 Jacobi (diagonal of the FP32 values).  Returns 1 when the true FP64
+ * residual ||b - A x|| / ||b|| < tol. */
+#define ORC_RELIABLE(NAME, VT)                                                                                       \
+   static int NAME(int32_t n, const int32_t* rowptr, const int32_t* cols, const double* vals, int precond,         \
+                   const double* b, double* x, double tol, double delta, int32_t maxit, int32_t* iterations,      \
+                   int32_t* updates, double* resid)                                                              \
+   {                                                                                                              \
+      const int32_t nnz = rowptr[n];                                                                              \
+      float* v32 = (float*)malloc(sizeof(float) * (size_t)(nnz > 0 ? nnz : 1));                                   \
+      float* d = (float*)malloc(sizeof(float) * (size_t)n);                                                       \
+      VT *r = (VT*)malloc(sizeof(VT) * (size_t)n), *z = (VT*)malloc(sizeof(VT) * (size_t)n);                      \
+      VT *p = (VT*)calloc((size_t)n, sizeof(VT)), *Ap = (VT*)malloc(sizeof(VT) * (size_t)n);                      \
+      VT* xc = (VT*)calloc((size_t)n, sizeof(VT));                                                                \
+      for (int32_t k = 0; k < nnz; k++) v32[k] = (float)vals[k];                                                  \
+      for (int32_t i = 0; i < n; i++) {                                                                           \
+         float di = 0.0f;                                                                                         \
+         for (int32_t k = rowptr[i]; k < rowptr[i + 1]; k++)                                                      \
+            if (cols[k] == i) di = v32[k];                                                                        \
+         d[i] = di;                                                                                               \
+      }                                                                                                           \
+      double rz = 1.0, rz_cur = 0.0, res = 0.0;                                                                   \
+      int32_t it = 0, upd = 0, halt = 1, ok = 0;                                                                  \
+      for (;;) {                                                                                                  \
+         for (int32_t i = 0; i < n; i++) {                                                                        \
+            x[i] += (double)xc[i];                                                                                \
+            xc[i] = (VT)0;                                                                                        \
+         }                                                                                                        \
+         double rn2 = 0.0, bn2 = 0.0;                                                                             \
+         for (int32_t i = 0; i < n; i++) {                                                                        \
+            double acc = 0.0;                                                                                     \
+            for (int32_t k = rowptr[i]; k < rowptr[i + 1]; k++)                                                   \
+               if (cols[k] >= 0) acc += vals[k] * x[cols[k]];                                                     \
+            const double di = b[i] - acc;                                                                         \
+            r[i] = (VT)di;                                                                                        \
+            rn2 += di * di;                                                                                       \
+            bn2 += b[i] * b[i];                                                                                   \
+         }                                                                                                        \
+         const double rn = sqrt(rn2), bn = sqrt(bn2);                                                             \
+         res = bn > 0 ? rn / bn : 0.0;                                                                            \
+         if (bn == 0 || res < tol) {                                                                              \
+            ok = 1;                                                                                               \
+            break;                                                                                                \
+         }                                                                                                        \
+         if (halt == 2 || it >= maxit || !isfinite(res)) break;                                                   \
+         if (it > 0) upd++;                                                                                       \
+         const double t1 = delta * rn, t2 = tol * bn;                                                             \
+         const double trig2 = t1 > t2 ? t1 * t1 : t2 * t2;                                                        \
+         halt = 0;                                                                                                \
+         rz_cur = 0.0;                                                                                            \
+         for (int32_t i = 0; i < n; i++) {                                                                        \
+            z[i] = precond == 1 ? r[i] / (VT)d[i] : r[i];                                                         \
+            rz_cur += (double)r[i] * (double)z[i];                                                                \
+         }                                                                                                        \
+         {                                                                                                        \
+            const VT beta = (VT)(rz_cur / rz);                                                                    \
+            for (int32_t i = 0; i < n; i++) p[i] = z[i] + beta * p[i];                                            \
+         }                                                                                                        \
+         while (!halt) {                                                                                          \
+            double pap = 0.0;                                                                                     \
+            for (int32_t i = 0; i < n; i++) {                                                                     \
+               VT s = (VT)0;                                                                                      \
+               for (int32_t k = rowptr[i]; k < rowptr[i + 1]; k++)                                                \
+                  if (cols[k] >= 0) s += (VT)v32[k] * p[cols[k]];                                                 \
+               Ap[i] = s;                                                                                         \
+               pap += (double)s * (double)p[i];                                                                   \
+            }                                                                                                     \
+            rz = rz_cur;                                                                                          \
+            if (pap == 0.0 || !isfinite(pap)) {                                                                   \
+               halt = 2;                                                                                          \
+               break;                                                                                             \
+            }                                                                                                     \
+            const VT alpha = (VT)(rz / pap);                                                                      \
+            double rr = 0.0, rzn = 0.0;                                                                           \
+            for (int32_t i = 0; i < n; i++) {                                                                     \
+               xc[i] += alpha * p[i];                                                                             \
+               r[i] = r[i] - alpha * Ap[i];                                                                        \
+               rr += (double)r[i] * (double)r[i];                                                                 \
+               z[i] = precond == 1 ? r[i] / (VT)d[i] : r[i];                                                      \
+               rzn += (double)r[i] * (double)z[i];                                                                \
+            }                                                                                                     \
+            it++;                                                                                                 \
+            if (!isfinite(rr))                                                                                    \
+               halt = 2;                                                                                          \
+            else if (rr < trig2)                                                                                  \
+               halt = 1;                                                                                          \
+            else if (it >= maxit)                                                                                 \
+               halt = 3;                                                                                          \
+            if (halt) break;                                                                                      \
+            rz_cur = rzn;                                                                                         \
+            const VT beta = (VT)(rz_cur / rz);                                                                    \
+            for (int32_t i = 0; i < n; i++) p[i] = z[i] + beta * p[i];                                            \
+         }                                                                                                        \
+      }                                                                                                           \
+      *iterations = it;                                                                                           \
+      *updates = upd;                                                                                             \
+      *resid = res;                                                                                               \
+      free(v32);                                                                                                  \
+      free(d);                                                                                                    \
+      free(r);                                                                                                    \
+      free(z);                                                                                                    \
+      free(p);                                                                                                    \
+      free(Ap);                                                                                                   \
+      free(xc);                                                                                                   \
+      return ok;                                                                                                  \
+   }
+
+ORC_RELIABLE(reliable_f32, float)
+ORC_RELIABLE(reliable_f64, double)
+#undef ORC_RELIABLE
+
+int orc_pcg_reliable(int32_t n, const int32_t* rowptr, const int32_t* cols, const double* vals, int precond,
+                     const double* b, double* x, double tol, double delta, int32_t maxit, int vec64,
+                     int32_t* iterations, int32_t* updates, double* resid)
+{
+   if (vec64) return reliable_f64(n, rowptr, cols, vals, precond, b, x, tol, delta, maxit, iterations, updates, resid);
+   return reliable_f32(n, rowptr, cols, vals, precond, b, x, tol, delta, maxit, iterations, updates, resid);
+}

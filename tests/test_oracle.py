@@ -284,3 +284,25 @@ def test_symmetric_and_transposed_products_match_reference(oracle, reference):
                            atol=1e-12)
     finally:
         reference.set_threads(threads)
+
+
+def test_reliable_update_pcg_restatement(oracle):
+    """The restatement of the library's reliable-update mixed PCG (no
+    reference counterpart) reaches the FP64 tolerance on the true residual
+    with close to the FP64 Jacobi-CG iteration count, folding its FP32
+    correction into x about once per factor-10 drop of the residual."""
+    A = g.diffusion_2d(96, 0.1, 2.0, 7)
+    b = g.uniform_vector(A.n, 1)
+    f = oracle.solve("cg", A, b, precond=1, tol=1e-9)
+    r = oracle.pcg_reliable(A, b, precond=1, tol=1e-8, delta=0.1)
+    assert r["converged"] and oracle.true_residual(A, b, r["x"]) < 1e-8
+    assert abs(r["residue"] - oracle.true_residual(A, b, r["x"])) < 1e-15
+    assert r["iterations"] <= 1.3 * f["iterations"], (r["iterations"], f["iterations"])
+    assert 6 <= r["updates"] <= 10
+    # max_iterations bounds the FP32 iterations
+    s = oracle.pcg_reliable(A, b, precond=1, tol=1e-8, delta=0.1, maxit=50)
+    assert not s["converged"] and s["iterations"] == 50
+    # FP64 vectors with the FP32 values
+    v = oracle.pcg_reliable(A, b, precond=1, tol=1e-8, delta=0.1, vec64=True)
+    assert v["converged"] and oracle.true_residual(A, b, v["x"]) < 1e-8
+    assert v["iterations"] <= 1.3 * f["iterations"], (v["iterations"], f["iterations"])

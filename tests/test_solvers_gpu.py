@@ -195,6 +195,69 @@ def test_mixed_precision_refinement_reaches_fp64_residual(oracle):
     assert oracle.true_residual(A, b, xs.cpu().numpy()) < 1e-10
 
 
+@pytest.mark.parametrize("name,pc,vec64", [("laplacian48", 0, False), ("diffusion96", 1, False),
+                                           ("diffusion96", 1, True), ("laplacian48", 0, True)])
+def test_reliable_mixed_pcg_matches_oracle(oracle, name, pc, vec64):
+    """CG on FP32 values (FP32 or FP64 vectors) with reliable FP64 updates
+    against its oracle restatement: the same number of iterations and
+    updates within the slack of a different summation order, both below the
+    tolerance on the true FP64 residual."""
+    from tnl_b200 import generators as g
+
+    t = tnl()
+    A = g.laplacian_2d(48) if name == "laplacian48" else g.diffusion_2d(96, 0.1, 2.0, 7)
+    b = g.uniform_vector(A.n, 1)
+    o = oracle.pcg_reliable(A, b, precond=pc, tol=1e-8, delta=0.1, vec64=vec64)
+    M = t.SparseMatrix(t.CSR, torch.float64).assign(A.rowptr, A.cols, A.vals)
+    bs = torch.tensor(b, device="cuda")
+    xs = torch.zeros(A.n, dtype=torch.float64, device="cuda")
+    r = t.solve_mixed_reliable(M, bs, xs, tol=1e-8, delta=0.1, inner=["none", "jacobi"][pc],
+                               vectors=torch.float64 if vec64 else torch.float32)
+    assert o["converged"] and r["converged"] and not r["breakdown"]
+    assert abs(r["iterations"] - o["iterations"]) <= max(3, 0.03 * o["iterations"]), (r, o["iterations"])
+    assert abs(r["reliable_updates"] - o["updates"]) <= 1, (r, o["updates"])
+    assert r["true_residual"] < 1e-8 and oracle.true_residual(A, b, xs.cpu().numpy()) < 1e-8
+    assert abs(r["true_residual"] - t.true_residual(M, bs, xs)) <= 1e-15
+
+
+def test_reliable_mixed_pcg_with_fsai():
+    """With an FP32 FSAI the reliable-update solver reaches the FP64
+    tolerance in fewer iterations than iterative refinement (which restarts
+    CG at every correction) and within 1.5x those of FP64 FSAI-PCG run to a
+    preconditioned residue of 1e-9; a two-factor FSAI is refused."""
+    from tnl_b200 import generators as g
+
+    t = tnl()
+    A = g.diffusion_2d(128, 0.1, 2.0, 7)
+    b = g.uniform_vector(A.n, 1)
+    M = t.SparseMatrix(t.CSR, torch.float64).assign(A.rowptr, A.cols, A.vals)
+    bs = torch.tensor(b, device="cuda")
+    P = t.FSAI()
+    P.update(M)
+    S = t.CG()
+    S.setMatrix(M)
+    S.setPreconditioner(P)
+    S.setup({"convergence-residue": 1e-9, "max-iterations": 20000})
+    x64 = torch.zeros(A.n, dtype=torch.float64, device="cuda")
+    assert S.solve(bs, x64)
+    xs = torch.zeros(A.n, dtype=torch.float64, device="cuda")
+    r = t.solve_mixed_reliable(M, bs, xs, tol=1e-8, inner="fsai")
+    assert r["converged"] and t.true_residual(M, bs, xs) < 1e-8
+    assert r["iterations"] <= 1.5 * S.getIterations(), (r, S.getIterations())
+    x2 = torch.zeros(A.n, dtype=torch.float64, device="cuda")
+    r2 = t.solve_mixed_reliable(M, bs, x2, tol=1e-8, inner="fsai", vectors=torch.float64)
+    assert r2["converged"] and t.true_residual(M, bs, x2) < 1e-8
+    assert r2["iterations"] <= 1.5 * S.getIterations(), (r2, S.getIterations())
+    xi = torch.zeros(A.n, dtype=torch.float64, device="cuda")
+    ir = t.solve_mixed(M, bs, xi, tol=1e-8, inner_tol=1e-4, inner="fsai")
+    assert ir["converged"] and r["iterations"] < ir["inner_iterations"], (r, ir)
+    M32 = t.SparseMatrix(t.CSR, torch.float32).assign(A.rowptr, A.cols, A.vals.astype(np.float32))
+    P2 = t.FSAI2()
+    P2.update(M32)
+    with pytest.raises(ValueError):
+        t.solve_mixed_reliable(M, bs, torch.zeros_like(xs), inner=P2)
+
+
 def test_fsai_factors_match_reference():
     """Classical FSAI (SPD) and two-factor FSAI (nonsymmetric) values against
     the FP64 numpy restatement (different small dense solvers: 1e-12)."""

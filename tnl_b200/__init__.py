@@ -32,7 +32,7 @@ __all__ = [
     "CSR", "Ellpack", "SlicedEllpack", "ChunkedEllpack", "BiEllpack", "AdaptiveCSR", "SparseMatrix",
     "LaunchConfiguration", "ColumnMajorOrder", "RowMajorOrder", "CSRMatrix", "check", "BackendRuntimeError",
     "CG", "BICGStab", "GMRES", "FGMRES", "TFQMR", "BICGStabL", "IDRs", "Diagonal", "ILU0", "FSAI", "FSAI2",
-    "solve_mixed", "true_residual", "read_mtx", "write_mtx",
+    "solve_mixed", "solve_mixed_reliable", "true_residual", "read_mtx", "write_mtx",
 ]
 
 ColumnMajorOrder = capi.COLUMN_MAJOR
@@ -657,6 +657,39 @@ def true_residual(M: SparseMatrix, b: torch.Tensor, x: torch.Tensor) -> float:
     check(capi.tnlb_true_residual(M.segments.handle, _real_code(M.real), M.columnIndexes.data_ptr(),
                                   M.values.data_ptr(), b.data_ptr(), x.data_ptr(), _stream(), C.byref(out)))
     return out.value
+
+
+def solve_mixed_reliable(M: SparseMatrix, b: torch.Tensor, x: torch.Tensor, tol: float = 1e-8, delta: float = 0.1,
+                         max_iterations: int = 1000000, inner: str | _Preconditioner = "jacobi",
+                         vectors: torch.dtype = torch.float32) -> dict:
+    """Mixed-precision PCG with reliable updates (SPD matrices, FP64 matrix
+    and vectors): CG iterations on FP32 values (FP32 or FP64 ``vectors``)
+    whose correction is folded into the FP64 x, with the residual recomputed
+    in FP64, each time the recursive residual has fallen by ``delta``; the
+    search direction is kept across updates.
+
+    ``inner`` is "jacobi", "fsai", "none", or an FP32 Jacobi / FSAI
+    preconditioner object built for an FP32 copy of the matrix (e.g. a
+    learned FSAI).  Stops on the true FP64 residual ``tol``.
+    """
+    if M.real != torch.float64:
+        raise TypeError("solve_mixed_reliable takes an FP64 matrix")
+    p = capi.SolverParams()
+    capi.tnlb_solver_params_default(C.byref(p))
+    p.convergence_residue = tol
+    p.max_iterations = max_iterations
+    r = capi.SolveResult()
+    upd = C.c_int32()
+    kinds = {"none": capi.PRECOND_NONE, "jacobi": capi.PRECOND_JACOBI, "fsai": capi.PRECOND_FSAI}
+    if isinstance(inner, str) and inner not in kinds:
+        raise ValueError(f"solve_mixed_reliable: unknown preconditioner {inner!r}")
+    kind = kinds[inner] if isinstance(inner, str) else capi.PRECOND_NONE
+    handle = None if isinstance(inner, str) else inner.handle
+    check(capi.tnlb_solve_mixed_reliable(C.byref(p), M.segments.handle, M.columnIndexes.data_ptr(),
+                                         M.values.data_ptr(), b.data_ptr(), x.data_ptr(), delta,
+                                         _real_code(vectors), kind, handle, _stream(), C.byref(r), C.byref(upd)))
+    return {"converged": bool(r.converged), "iterations": r.iterations, "reliable_updates": upd.value,
+            "true_residual": r.residue, "breakdown": bool(r.status_detail)}
 
 
 def solve_mixed(M: SparseMatrix, b: torch.Tensor, x: torch.Tensor, tol: float = 1e-8, inner_tol: float = 1e-4,

@@ -118,6 +118,9 @@ tnlb_solve = _sig("tnlb_solve", [C.c_int, C.c_int, C.POINTER(SolverParams), _p, 
 tnlb_true_residual = _sig("tnlb_true_residual", [_p, C.c_int, _p, _p, _p, _p, _p, C.POINTER(_f64)])
 tnlb_solve_mixed = _sig("tnlb_solve_mixed", [C.POINTER(SolverParams), _p, _p, _p, _p, _p, _f64, _i32, C.c_int,
                                              C.c_int, _p, _p, C.POINTER(SolveResult), C.POINTER(_i32)])
+tnlb_solve_mixed_reliable = _sig("tnlb_solve_mixed_reliable", [C.POINTER(SolverParams), _p, _p, _p, _p, _p, _f64,
+                                                               C.c_int, C.c_int, _p, _p, C.POINTER(SolveResult),
+                                                               C.POINTER(_i32)])
 tnlb_precond_create = _sig("tnlb_precond_create", [C.c_int, _p, C.c_int, _p, _p, _p, C.POINTER(_p)])
 tnlb_precond_solve = _sig("tnlb_precond_solve", [_p, _p, _p, _p])
 tnlb_precond_destroy = _sig("tnlb_precond_destroy", [_p])

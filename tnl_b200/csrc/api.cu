@@ -363,6 +363,30 @@ tnlb_status tnlb_solve_mixed(const tnlb_solver_params* params, const tnlb_segmen
                                result, &inner_its, outer_iterations, inner_precond, inner, inner_solver);
 }
 
+tnlb_status tnlb_solve_mixed_reliable(const tnlb_solver_params* params, const tnlb_segments* seg,
+                                      const int32_t* d_cols, const double* d_values, const double* d_b, double* d_x,
+                                      double delta, tnlb_real vectors, tnlb_precond_kind inner_precond,
+                                      const tnlb_precond* inner, tnlb_stream stream, tnlb_solve_result* result,
+                                      int32_t* reliable_updates)
+{
+   clear_error();
+   TNLB_TRY_STATUS(check_solve_args(seg, TNLB_F64, d_b, d_x));
+   TNLB_REQUIRE(result && reliable_updates, TNLB_ERR_INVALID_ARGUMENT, "null result");
+   TNLB_REQUIRE(delta > 0 && delta < 1, TNLB_ERR_INVALID_ARGUMENT, "delta must lie in (0, 1)");
+   TNLB_REQUIRE(vectors == TNLB_F32 || vectors == TNLB_F64, TNLB_ERR_INVALID_ARGUMENT, "unknown vector real type");
+   TNLB_REQUIRE(inner || inner_precond == TNLB_PRECOND_NONE || inner_precond == TNLB_PRECOND_JACOBI ||
+                   inner_precond == TNLB_PRECOND_FSAI,
+                TNLB_ERR_INVALID_ARGUMENT, "the preconditioner must be none, Jacobi or FSAI");
+   tnlb_solver_params p;
+   tnlb_solver_params_default(&p);
+   if (params) p = *params;
+   TNLB_REQUIRE(p.max_iterations >= 0, TNLB_ERR_INVALID_ARGUMENT, "negative max_iterations");
+   *result = tnlb_solve_result{};
+   *reliable_updates = 0;
+   return tnlb::solve_mixed_reliable(seg, d_cols, d_values, d_b, d_x, p, delta, vectors, (cudaStream_t)stream, result,
+                                     reliable_updates, inner_precond, inner);
+}
+
 tnlb_status tnlb_precond_create(tnlb_precond_kind kind, const tnlb_segments* seg, tnlb_real real,
                                 const int32_t* d_cols, const void* d_values, tnlb_stream stream, tnlb_precond** out)
 {

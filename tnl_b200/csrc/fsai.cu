@@ -273,6 +273,7 @@ tnlb_status fsai_create(const tnlb_segments* seg, tnlb_real real, const int32_t*
    auto* F = new Fsai();
    F->n = n;
    F->real = real;
+   F->two_factor = two_factor;
    const size_t rs = real == TNLB_F64 ? 8 : 4;
    // CSR copy of A
    {
@@ -388,6 +389,31 @@ tnlb_status fsai_apply(const Fsai* F, const void* r, void* z, cudaStream_t st, c
    TNLB_TRY_STATUS(
       spmv_dispatch(F->g, F->real, F->g_cols.as<int32_t>(), F->g_vals.ptr, r, F->tmp.ptr, 1.0, 0.0, st, skip));
    return spmv_dispatch(F->gt, F->real, F->gt_cols.as<int32_t>(), F->gt_vals.ptr, F->tmp.ptr, z, 1.0, 0.0, st, skip);
+}
+
+bool fsai_two_factor(const Fsai* F) { return F->two_factor; }
+
+bool fsai_dot_fusable(const Fsai* F) { return !F->two_factor && spmv_dot_fusable(F->g) && spmv_dot_fusable(F->gt); }
+
+// t = G r with (t, t) = (r, G^T G r) summed in the same kernel; z = G^T t
+tnlb_status fsai_apply_dot(const Fsai* F, const void* r, void* z, double* partials, unsigned* counter, double* rz_out,
+                           cudaStream_t st, const int32_t* skip)
+{
+   TNLB_REQUIRE(fsai_dot_fusable(F), TNLB_ERR_INVALID_ARGUMENT, "fsai_apply_dot: not a symmetric short-row FSAI");
+   TNLB_TRY_STATUS(spmv_dot(F->g, F->real, F->g_cols.as<int32_t>(), F->g_vals.ptr, r, F->tmp.ptr, partials, counter,
+                            rz_out, st, skip, true));
+   return spmv_dispatch(F->gt, F->real, F->gt_cols.as<int32_t>(), F->gt_vals.ptr, F->tmp.ptr, z, 1.0, 0.0, st, skip);
+}
+
+tnlb_status fsai_apply_dot_xpby(const Fsai* F, tnlb_real vec, const void* r, void* p, double* partials,
+                                unsigned* counter, double* rz_out, const double* rz_old, cudaStream_t st,
+                                const int32_t* skip)
+{
+   TNLB_REQUIRE(fsai_dot_fusable(F), TNLB_ERR_INVALID_ARGUMENT, "fsai_apply_dot_xpby: not a symmetric short-row FSAI");
+   TNLB_TRY_STATUS(spmv_dot_mixed(F->g, F->real, vec, F->real, F->g_cols.as<int32_t>(), F->g_vals.ptr, r, F->tmp.ptr,
+                                  partials, counter, rz_out, st, skip, true));
+   return spmv_xpby_mixed(F->gt, F->real, F->real, vec, F->gt_cols.as<int32_t>(), F->gt_vals.ptr, F->tmp.ptr, p,
+                          rz_out, rz_old, st, skip);
 }
 
 void fsai_destroy(Fsai* F) { delete F; }

@@ -10,6 +10,7 @@ namespace tnlb {
 struct Fsai {
    int32_t n = 0;
    tnlb_real real = TNLB_F64;
+   bool two_factor = false;      // g = G_L, gt = G_U (not G_L^T)
    tnlb_segments* g = nullptr;   // CSR of G
    tnlb_segments* gt = nullptr;  // CSR of G^T
    DeviceBuffer g_cols, g_vals, gt_cols, gt_vals, gt_src, tmp;

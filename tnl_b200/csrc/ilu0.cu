@@ -168,6 +168,128 @@ __global__ void __launch_bounds__(kIluRunThreads)
    }
 }
 
+// Level-ordered packed factors: position t of the level order (row
+// rows[t]) holds its K (padded) L entries at pc/pv[t*K ..] (column -1 pads),
+// and for U its off-diagonal entries plus the diagonal at dv[t]; the
+// solve's input is permuted to the same order first (in[t] = b[rows[t]]).
+// A row then needs one load of its own data and the gathers of x.
+template <typename Real>
+__global__ void k_permute(const int32_t* __restrict__ rows, int32_t n, const Real* __restrict__ src,
+                          Real* __restrict__ dst)
+{
+   const int32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+   if (t < n) dst[t] = src[rows[t]];
+}
+
+template <typename Real>
+__global__ void k_pack_vals(const int64_t* __restrict__ src, int64_t count, const Real* __restrict__ lu,
+                            Real* __restrict__ dst)
+{
+   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+   if (k < count) dst[k] = src[k] >= 0 ? lu[src[k]] : Real(0);
+}
+
+// Rows of one (large) level, packed: x_i = in_t - sum_j L_ij x_j.
+template <typename Real, int K>
+__global__ void k_lower_packed(int32_t t0, int32_t count, const int32_t* __restrict__ rows,
+                               const int32_t* __restrict__ pc, const Real* __restrict__ pv,
+                               const Real* __restrict__ in, Real* x)
+{
+   const int32_t t = t0 + blockIdx.x * blockDim.x + threadIdx.x;
+   if (t >= t0 + count) return;
+   int32_t c[K];
+   Real v[K];
+#pragma unroll
+   for (int j = 0; j < K; j++) {
+      c[j] = pc[(int64_t)t * K + j];
+      v[j] = pv[(int64_t)t * K + j];
+   }
+   const int32_t i = rows[t];
+   Real xi = in[t];
+#pragma unroll
+   for (int j = 0; j < K; j++)
+      if (c[j] >= 0) xi = sub_rn(xi, mul_rn(v[j], x[c[j]]));
+   x[i] = xi;
+}
+
+// x_i = (in_t - sum_{j>i} U_ij x_j) / U_ii for the rows of one level, packed.
+template <typename Real, int K>
+__global__ void k_upper_packed(int32_t t0, int32_t count, const int32_t* __restrict__ rows,
+                               const int32_t* __restrict__ pc, const Real* __restrict__ pv,
+                               const Real* __restrict__ dv, const Real* __restrict__ in, Real* x)
+{
+   const int32_t t = t0 + blockIdx.x * blockDim.x + threadIdx.x;
+   if (t >= t0 + count) return;
+   int32_t c[K];
+   Real v[K];
+#pragma unroll
+   for (int j = 0; j < K; j++) {
+      c[j] = pc[(int64_t)t * K + j];
+      v[j] = pv[(int64_t)t * K + j];
+   }
+   const int32_t i = rows[t];
+   Real xi = in[t];
+#pragma unroll
+   for (int j = 0; j < K; j++)
+      if (c[j] >= 0) xi = sub_rn(xi, mul_rn(v[j], x[c[j]]));
+   x[i] = div_rn(xi, dv[t]);
+}
+
+// Runs of levels of at most kIluPipeThreads rows in one block, one row per
+// thread per level, software-pipelined: the packed data and input of a
+// thread's row in level l+1 (independent of x) are loaded while level l is
+// solved, so after each __syncthreads only the gathers of x wait.
+constexpr int kIluPipeThreads = 1024;
+constexpr int32_t kIluPipeMaxLevels = 4096;
+
+template <typename Real, int K, bool Upper>
+__global__ void __launch_bounds__(kIluPipeThreads)
+   k_solve_pipe(const int32_t* __restrict__ lvl, int32_t l0, int32_t l1, const int32_t* __restrict__ rows,
+                const int32_t* __restrict__ pc, const Real* __restrict__ pv, const Real* __restrict__ dv,
+                const Real* __restrict__ in, Real* x)
+{
+   __shared__ int32_t s_lvl[kIluPipeMaxLevels + 1];
+   for (int32_t k = threadIdx.x; k <= l1 - l0; k += blockDim.x) s_lvl[k] = lvl[l0 + k];
+   __syncthreads();
+   int32_t i_n = -1, c_n[K];
+   Real v_n[K], in_n = Real(0), d_n = Real(1);
+   auto load = [&](int32_t l) {
+      i_n = -1;
+      if (l >= l1) return;
+      const int32_t t = s_lvl[l - l0] + (int32_t)threadIdx.x;
+      if (t >= s_lvl[l - l0 + 1]) return;
+      i_n = rows[t];
+      in_n = in[t];
+      if (Upper) d_n = dv[t];
+#pragma unroll
+      for (int j = 0; j < K; j++) {
+         c_n[j] = pc[(int64_t)t * K + j];
+         v_n[j] = pv[(int64_t)t * K + j];
+      }
+   };
+   load(l0);
+   for (int32_t l = l0; l < l1; l++) {
+      const int32_t i = i_n;
+      int32_t c[K];
+      Real v[K];
+#pragma unroll
+      for (int j = 0; j < K; j++) {
+         c[j] = c_n[j];
+         v[j] = v_n[j];
+      }
+      Real xi = in_n;
+      const Real di = d_n;
+      load(l + 1);
+      if (i >= 0) {
+#pragma unroll
+         for (int j = 0; j < K; j++)
+            if (c[j] >= 0) xi = sub_rn(xi, mul_rn(v[j], x[c[j]]));
+         x[i] = Upper ? div_rn(xi, di) : xi;
+      }
+      __syncthreads();
+   }
+}
+
 struct Ilu0Base {
    virtual ~Ilu0Base() = default;
    virtual tnlb_status apply(const void* b, void* x, cudaStream_t st) = 0;
@@ -177,6 +299,10 @@ template <typename Real>
 struct Ilu0 : Ilu0Base {
    int32_t n = 0;
    DeviceBuffer rp, cols, lu, lstart, ustart, uend, lrows, urows, tmp, dlptr, duptr;
+   // packed level-ordered factors (when every row has <= 8 L and <= 8
+   // off-diagonal U entries): strides kl / ku
+   int kl = 0, ku = 0;
+   DeviceBuffer lpc, lpv, upc, upv, udv, perm;
    std::vector<int32_t> lptr, uptr;  // level boundaries into lrows / urows
    cudaGraphExec_t exec = nullptr;
    const Real* g_b = nullptr;
@@ -189,10 +315,70 @@ struct Ilu0 : Ilu0Base {
       if (cs) cudaStreamDestroy(cs);
    }
 
-   // Levels in order: a run of consecutive levels of at most kIluSmallLevel
-   // rows goes to one single-block launch, a larger level to its own grid.
+   template <int KL, int KU>
+   void enqueue_packed(const Real* b, Real* x, cudaStream_t st)
+   {
+      Real* in = perm.as<Real>();
+      const unsigned g = (unsigned)((n + 255) / 256);
+      k_permute<Real><<<g, 256, 0, st>>>(lrows.as<int32_t>(), n, b, in);
+      const int32_t nl = (int32_t)lptr.size() - 1;
+      for (int32_t l = 0; l < nl;) {
+         if (lptr[l + 1] - lptr[l] <= kIluPipeThreads) {
+            int32_t e = l;
+            while (e < nl && e - l < kIluPipeMaxLevels && lptr[e + 1] - lptr[e] <= kIluPipeThreads) e++;
+            k_solve_pipe<Real, KL, false><<<1, kIluPipeThreads, 0, st>>>(
+               dlptr.as<int32_t>(), l, e, lrows.as<int32_t>(), lpc.as<int32_t>(), lpv.as<Real>(), nullptr, in, x);
+            l = e;
+            continue;
+         }
+         const int32_t cnt = lptr[l + 1] - lptr[l];
+         k_lower_packed<Real, KL><<<(cnt + 127) / 128, 128, 0, st>>>(lptr[l], cnt, lrows.as<int32_t>(),
+                                                                     lpc.as<int32_t>(), lpv.as<Real>(), in, x);
+         l++;
+      }
+      k_permute<Real><<<g, 256, 0, st>>>(urows.as<int32_t>(), n, x, in);
+      const int32_t nu = (int32_t)uptr.size() - 1;
+      for (int32_t l = 0; l < nu;) {
+         if (uptr[l + 1] - uptr[l] <= kIluPipeThreads) {
+            int32_t e = l;
+            while (e < nu && e - l < kIluPipeMaxLevels && uptr[e + 1] - uptr[e] <= kIluPipeThreads) e++;
+            k_solve_pipe<Real, KU, true><<<1, kIluPipeThreads, 0, st>>>(
+               duptr.as<int32_t>(), l, e, urows.as<int32_t>(), upc.as<int32_t>(), upv.as<Real>(), udv.as<Real>(),
+               in, x);
+            l = e;
+            continue;
+         }
+         const int32_t cnt = uptr[l + 1] - uptr[l];
+         k_upper_packed<Real, KU><<<(cnt + 127) / 128, 128, 0, st>>>(uptr[l], cnt, urows.as<int32_t>(),
+                                                                     upc.as<int32_t>(), upv.as<Real>(),
+                                                                     udv.as<Real>(), in, x);
+         l++;
+      }
+   }
+
+   template <int KL>
+   void enqueue_packed_u(const Real* b, Real* x, cudaStream_t st)
+   {
+      if (ku <= 1) enqueue_packed<KL, 1>(b, x, st);
+      else if (ku <= 2) enqueue_packed<KL, 2>(b, x, st);
+      else if (ku <= 4) enqueue_packed<KL, 4>(b, x, st);
+      else enqueue_packed<KL, 8>(b, x, st);
+   }
+
+   // Levels in order.  Packed factors: runs of levels of at most
+   // kIluPipeThreads rows go to one pipelined single-block launch, a larger
+   // level to its own grid.  Otherwise (a row with more than 8 entries in L
+   // or U): runs of levels of at most kIluSmallLevel rows in one
+   // single-block launch, larger levels to their own grids.
    void enqueue(const Real* b, Real* x, cudaStream_t st)
    {
+      if (kl > 0) {
+         if (kl <= 1) enqueue_packed_u<1>(b, x, st);
+         else if (kl <= 2) enqueue_packed_u<2>(b, x, st);
+         else if (kl <= 4) enqueue_packed_u<4>(b, x, st);
+         else enqueue_packed_u<8>(b, x, st);
+         return;
+      }
       const int32_t nl = (int32_t)lptr.size() - 1;
       for (int32_t l = 0; l < nl;) {
          if (lptr[l + 1] - lptr[l] <= kIluSmallLevel) {
@@ -341,6 +527,57 @@ tnlb_status create_t(const tnlb_segments* seg, const int32_t* cols_in, const Rea
                                                            P->ustart.template as<int32_t>(), P->uend.template as<int32_t>());
    }
    TNLB_CHECK_LAUNCH();
+   // packed level-ordered copies of the factors
+   int32_t ml = 0, mu = 0;
+   for (int32_t i = 0; i < n; i++) {
+      ml = std::max(ml, us[i] - ls[i]);
+      mu = std::max(mu, ue[i] - us[i] - 1);
+   }
+   if (ml <= 8 && mu <= 8) {
+      auto stride = [](int32_t m) { return m <= 1 ? 1 : m <= 2 ? 2 : m <= 4 ? 4 : 8; };
+      const int kl = stride(ml), ku = stride(mu);
+      std::vector<int32_t> lpc((size_t)n * kl, -1), upc((size_t)n * ku, -1);
+      std::vector<int64_t> lsrc((size_t)n * kl, -1), usrc((size_t)n * ku, -1), dsrc(n, -1);
+      for (int32_t t = 0; t < n; t++) {
+         const int32_t i = lrows[t];
+         for (int32_t j = 0; j < us[i] - ls[i]; j++) {
+            lpc[(size_t)t * kl + j] = cols[ls[i] + j];
+            lsrc[(size_t)t * kl + j] = ls[i] + j;
+         }
+         const int32_t r = urows[t];
+         for (int32_t j = 0; j < ue[r] - us[r] - 1; j++) {
+            upc[(size_t)t * ku + j] = cols[us[r] + 1 + j];
+            usrc[(size_t)t * ku + j] = us[r] + 1 + j;
+         }
+         dsrc[t] = us[r] < ue[r] ? us[r] : -1;
+      }
+      DeviceBuffer src;
+      TNLB_TRY_STATUS(src.alloc(sizeof(int64_t) * (size_t)n * std::max(kl, ku)));
+      TNLB_TRY_STATUS(P->lpc.alloc(sizeof(int32_t) * (size_t)n * kl));
+      TNLB_TRY_STATUS(P->upc.alloc(sizeof(int32_t) * (size_t)n * ku));
+      TNLB_TRY_STATUS(P->lpv.alloc(sizeof(Real) * (size_t)n * kl));
+      TNLB_TRY_STATUS(P->upv.alloc(sizeof(Real) * (size_t)n * ku));
+      TNLB_TRY_STATUS(P->udv.alloc(sizeof(Real) * (size_t)n));
+      TNLB_TRY_STATUS(P->perm.alloc(sizeof(Real) * (size_t)n));
+      TNLB_CUDA_TRY(cudaMemcpyAsync(P->lpc.ptr, lpc.data(), sizeof(int32_t) * lpc.size(), cudaMemcpyHostToDevice, st));
+      TNLB_CUDA_TRY(cudaMemcpyAsync(P->upc.ptr, upc.data(), sizeof(int32_t) * upc.size(), cudaMemcpyHostToDevice, st));
+      // one staging buffer for the three gathers: synchronise between them
+      auto pack = [&](const std::vector<int64_t>& h, DeviceBuffer& dst) -> tnlb_status {
+         TNLB_CUDA_TRY(cudaMemcpyAsync(src.ptr, h.data(), sizeof(int64_t) * h.size(), cudaMemcpyHostToDevice, st));
+         const int64_t cnt = (int64_t)h.size();
+         k_pack_vals<Real><<<(unsigned)((cnt + 255) / 256), 256, 0, st>>>(src.as<int64_t>(), cnt,
+                                                                          P->lu.template as<Real>(),
+                                                                          dst.template as<Real>());
+         TNLB_CHECK_LAUNCH();
+         TNLB_CUDA_TRY(cudaStreamSynchronize(st));
+         return TNLB_OK;
+      };
+      TNLB_TRY_STATUS(pack(lsrc, P->lpv));
+      TNLB_TRY_STATUS(pack(usrc, P->upv));
+      TNLB_TRY_STATUS(pack(dsrc, P->udv));
+      P->kl = kl;
+      P->ku = ku;
+   }
    TNLB_CUDA_TRY(cudaStreamSynchronize(st));
    *out = P;
    return TNLB_OK;

@@ -267,12 +267,25 @@ tnlb_status reduce_sum_i64(const int32_t* d_in, int64_t n, int64_t* h_sum, cudaS
 // y = A x with (x, y) summed in the same kernel, for CSR matrices whose rows
 // hold at most 16 entries (spmv_dot_fusable); `partials` holds
 // spmv_dot_partials(seg) doubles, `counter` starts (and ends) at zero; the
-// sum lands in *dot_out.  Deterministic.
+// sum lands in *dot_out (with `self_dot`: (y, y)).  Deterministic.
 bool spmv_dot_fusable(const tnlb_segments* seg);
 int64_t spmv_dot_partials(const tnlb_segments* seg);
 tnlb_status spmv_dot(const tnlb_segments* seg, tnlb_real real, const int32_t* cols, const void* vals, const void* x,
                      void* y, double* partials, unsigned* counter, double* dot_out, cudaStream_t st,
-                     const int32_t* skip);
+                     const int32_t* skip, bool self_dot = false);
+// The same with values, input and output of different real types: FP32
+// values with FP64 vectors (F32, F64, F64), or with an FP64 input and an
+// FP32 output (F32, F64, F32); rows are summed in the input's type.
+tnlb_status spmv_dot_mixed(const tnlb_segments* seg, tnlb_real tv, tnlb_real tx, tnlb_real ty, const int32_t* cols,
+                           const void* vals, const void* x, void* y, double* partials, unsigned* counter,
+                           double* dot_out, cudaStream_t st, const int32_t* skip, bool self_dot);
+// y = A x + (*num / *den) y for the same short-row CSR matrices (types: all
+// equal, or FP32 values and input with an FP64 output).
+tnlb_status spmv_xpby_mixed(const tnlb_segments* seg, tnlb_real tv, tnlb_real tx, tnlb_real ty, const int32_t* cols,
+                            const void* vals, const void* x, void* y, const double* num, const double* den,
+                            cudaStream_t st, const int32_t* skip);
+tnlb_status spmv_xpby(const tnlb_segments* seg, tnlb_real real, const int32_t* cols, const void* vals, const void* x,
+                      void* y, const double* num, const double* den, cudaStream_t st, const int32_t* skip);
 tnlb_status spmv_csr(const tnlb_segments* seg, tnlb_real real, const int32_t* cols, const void* vals, const void* x,
                      void* y, double alpha, double beta, int32_t begin, int32_t end, tnlb_kernel kernel, int32_t tps,
                      cudaStream_t stream, int* launches, const int32_t* skip = nullptr);
@@ -293,6 +306,10 @@ tnlb_status solve_mixed_cg(const tnlb_segments* seg, const int32_t* cols, const 
                            double* x, const tnlb_solver_params& prm, double inner_tol, int32_t max_outer,
                            cudaStream_t st, tnlb_solve_result* res, int32_t* inner_total, int32_t* outer,
                            int inner_kind, const tnlb_precond* inner_precond, int inner_solver);
+tnlb_status solve_mixed_reliable(const tnlb_segments* seg, const int32_t* cols, const double* vals, const double* b,
+                                 double* x, const tnlb_solver_params& prm, double delta, tnlb_real vectors,
+                                 cudaStream_t st, tnlb_solve_result* res, int32_t* updates, int inner_kind,
+                                 const tnlb_precond* inner_precond);
 tnlb_status ilu0_create(const tnlb_segments* seg, tnlb_real real, const int32_t* cols, const void* vals,
                         cudaStream_t st, void** out);
 tnlb_status ilu0_apply(void* ilu, const void* b, void* x, cudaStream_t st);
@@ -301,6 +318,18 @@ void ilu0_destroy(void* ilu);
 tnlb_status fsai_create(const tnlb_segments* seg, tnlb_real real, const int32_t* cols, const void* vals,
                         bool classical, cudaStream_t st, Fsai** out, bool two_factor = false);
 tnlb_status fsai_apply(const Fsai* F, const void* r, void* z, cudaStream_t st, const int32_t* skip = nullptr);
+// z = G^T (G r) with (r, z) = |G r|^2 summed inside the G product (symmetric
+// FSAI whose G has rows of at most 16 entries: fsai_dot_fusable).
+bool fsai_dot_fusable(const Fsai* F);
+bool fsai_two_factor(const Fsai* F);
+tnlb_status fsai_apply_dot(const Fsai* F, const void* r, void* z, double* partials, unsigned* counter, double* rz_out,
+                           cudaStream_t st, const int32_t* skip);
+// t = G r with (t, t) into *rz_out, then p = G^T t + (*rz_out / *rz_old) p
+// (the preconditioner application and direction update of FSAI-PCG).
+// r and p of type `vec` (the factors' own type, or FP64 with FP32 factors).
+tnlb_status fsai_apply_dot_xpby(const Fsai* F, tnlb_real vec, const void* r, void* p, double* partials,
+                                unsigned* counter, double* rz_out, const double* rz_old, cudaStream_t st,
+                                const int32_t* skip);
 tnlb_status fsai_set_values(Fsai* F, const void* gvals, cudaStream_t st);
 void fsai_destroy(Fsai* F);
 tnlb_status spmv_dispatch(const tnlb_segments* seg, tnlb_real real, const int32_t* cols, const void* vals,

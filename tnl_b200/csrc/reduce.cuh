@@ -9,6 +9,9 @@
 // Algorithms/detail/Reduction.hpp:273-320).
 #pragma once
 
+#include <mutex>
+#include <unordered_map>
+
 #include "internal.cuh"
 
 namespace tnlb {
@@ -27,6 +30,47 @@ inline unsigned vec_grid(int64_t n)
    int64_t g = (n + kRedThreads * 4 - 1) / (kRedThreads * 4);
    if (g < 1) g = 1;
    if (g > kRedMaxBlocks) g = kRedMaxBlocks;
+   return (unsigned)g;
+}
+
+// Grid of a grid-stride kernel: the blocks of `threads` threads that
+// `kernel` keeps resident at once on the whole device (its occupancy times
+// the SM count, queried once per kernel), at most kRedMaxBlocks and at most
+// one block per threads * per_thread items -- so no partial last wave.
+inline unsigned resident_grid(const void* kernel, int threads, int64_t n, int64_t per_thread)
+{
+   static std::mutex mu;
+   static std::unordered_map<const void*, int> occupancy;
+   static int sms = 0;
+   int occ = 0;
+   {
+      std::lock_guard<std::mutex> lock(mu);
+      if (sms == 0) {
+         int dev = 0, v = 0;
+         if (cudaGetDevice(&dev) == cudaSuccess &&
+             cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && v > 0)
+            sms = v;
+         else
+            sms = 148;
+      }
+      auto it = occupancy.find(kernel);
+      if (it == occupancy.end()) {
+         int v = 0;
+         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, kernel, threads, 0) != cudaSuccess || v < 1) {
+            cudaGetLastError();
+            v = 1;
+         }
+         occupancy.emplace(kernel, v);
+         occ = v;
+      }
+      else
+         occ = it->second;
+   }
+   int64_t g = (n + (int64_t)threads * per_thread - 1) / ((int64_t)threads * per_thread);
+   const int64_t cap = (int64_t)occ * sms;
+   if (g > cap) g = cap;
+   if (g > kRedMaxBlocks) g = kRedMaxBlocks;
+   if (g < 1) g = 1;
    return (unsigned)g;
 }
 

@@ -641,6 +641,11 @@ tnlb_status cg_solve(const Ctx<Real>& c, const Precond<Real>& P, const tnlb_solv
       TNLB_TRY_STATUS(dot_val.alloc(sizeof(double)));
       TNLB_CUDA_TRY(cudaMemsetAsync(dot_ctr.ptr, 0, sizeof(unsigned), c.st));
    }
+   const unsigned Gs2 = resident_grid((const void*)k_cg_s2<Real>, kRedThreads, n, 4);
+   const unsigned Gxr = resident_grid((const void*)k_cg_xr<Real>, kRedThreads, n, 4);
+   const unsigned Grz = resident_grid((const void*)k_cg_rz<Real>, kRedThreads, n, 4);
+   const unsigned Gup = resident_grid((const void*)k_cg_update<Real>, kRedThreads, n, 4);
+   const unsigned Gp = resident_grid((const void*)k_cg_p<Real>, kRedThreads, n, 4);
    auto enqueue_iteration = [&](cudaStream_t st) -> tnlb_status {
       if (fused) {
          TNLB_TRY_STATUS(spmv_dot(c.seg, c.real, c.cols, c.vals, p.as<Real>(), Ap.as<Real>(), dot_parts.as<double>(),
@@ -650,17 +655,17 @@ tnlb_status cg_solve(const Ctx<Real>& c, const Precond<Real>& P, const tnlb_solv
       else {
          TNLB_TRY_STATUS(
             spmv_dispatch(c.seg, c.real, c.cols, c.vals, p.as<Real>(), Ap.as<Real>(), 1.0, 0.0, st, done));
-         k_cg_s2<Real><<<G, kRedThreads, 0, st>>>(n, Ap.as<Real>(), p.as<Real>(), W.red(), W.S());
+         k_cg_s2<Real><<<Gs2, kRedThreads, 0, st>>>(n, Ap.as<Real>(), p.as<Real>(), W.red(), W.S());
       }
       if (gen) {
-         k_cg_xr<Real><<<G, kRedThreads, 0, st>>>(n, x, r.as<Real>(), p.as<Real>(), Ap.as<Real>(), W.S());
+         k_cg_xr<Real><<<Gxr, kRedThreads, 0, st>>>(n, x, r.as<Real>(), p.as<Real>(), Ap.as<Real>(), W.S());
          TNLB_TRY_STATUS(P.apply(n, r.as<Real>(), z.as<Real>(), st, done));
-         k_cg_rz<Real><<<G, kRedThreads, 0, st>>>(n, r.as<Real>(), z.as<Real>(), nullptr, 0, W.red(), W.S());
+         k_cg_rz<Real><<<Grz, kRedThreads, 0, st>>>(n, r.as<Real>(), z.as<Real>(), nullptr, 0, W.red(), W.S());
       }
       else
-         k_cg_update<Real><<<G, kRedThreads, 0, st>>>(n, x, r.as<Real>(), p.as<Real>(), Ap.as<Real>(), zp, P.d(),
-                                                      W.red(), W.S());
-      k_cg_p<Real><<<G, kRedThreads, 0, st>>>(n, p.as<Real>(), zp ? zp : r.as<Real>(), W.S(), 0);
+         k_cg_update<Real><<<Gup, kRedThreads, 0, st>>>(n, x, r.as<Real>(), p.as<Real>(), Ap.as<Real>(), zp, P.d(),
+                                                        W.red(), W.S());
+      k_cg_p<Real><<<Gp, kRedThreads, 0, st>>>(n, p.as<Real>(), zp ? zp : r.as<Real>(), W.S(), 0);
       TNLB_CHECK_LAUNCH();
       return TNLB_OK;
    };
@@ -688,21 +693,48 @@ tnlb_status cg_solve(const Ctx<Real>& c, const Precond<Real>& P, const tnlb_solv
    }
    else
       cudaGetLastError();
-   while (status == TNLB_OK) {
-      TNLB_CUDA_TRY(cudaMemcpyAsync(&h, W.S(), sizeof(h), cudaMemcpyDeviceToHost, cs));
-      TNLB_CUDA_TRY(cudaStreamSynchronize(cs));
-      if (h.done) break;
+   // One batch stays queued ahead of the host's check of the state (a batch
+   // launched after the stop returns at once, kernel by kernel).
+   DevState* hs = nullptr;
+   cudaEvent_t copied = nullptr;
+   auto launch_batch = [&]() {
       if (exec) {
-         TNLB_CUDA_TRY(cudaGraphLaunch(exec, cs));
+         if (cudaGraphLaunch(exec, cs) != cudaSuccess) {
+            set_error("CG: graph launch failed");
+            status = TNLB_ERR_CUDA;
+         }
       }
-      else {
+      else
          for (int k = 0; k < kBatch && status == TNLB_OK; k++) status = enqueue_iteration(cs);
-      }
+   };
+   if (cudaMallocHost(&hs, sizeof(DevState)) != cudaSuccess ||
+       cudaEventCreateWithFlags(&copied, cudaEventDisableTiming) != cudaSuccess) {
+      set_error("CG: pinned state allocation failed");
+      status = TNLB_ERR_CUDA;
    }
+   if (status == TNLB_OK) {
+      launch_batch();
+      cudaMemcpyAsync(hs, W.S(), sizeof(DevState), cudaMemcpyDeviceToHost, cs);
+      cudaEventRecord(copied, cs);
+   }
+   while (status == TNLB_OK) {
+      launch_batch();
+      if (cudaEventSynchronize(copied) != cudaSuccess) {
+         set_error("CG: state read failed");
+         status = TNLB_ERR_CUDA;
+         break;
+      }
+      h = *hs;
+      if (h.done) break;
+      cudaMemcpyAsync(hs, W.S(), sizeof(DevState), cudaMemcpyDeviceToHost, cs);
+      cudaEventRecord(copied, cs);
+   }
+   cudaStreamSynchronize(cs);
+   if (hs) cudaFreeHost(hs);
+   if (copied) cudaEventDestroy(copied);
    if (exec) cudaGraphExecDestroy(exec);
    if (graph) cudaGraphDestroy(graph);
    cudaEventDestroy(ev);
-   cudaStreamSynchronize(cs);
    cudaStreamDestroy(cs);
    TNLB_TRY_STATUS(status);
    res->iterations = h.it;
@@ -2094,6 +2126,473 @@ tnlb_status solve_mixed_cg(const tnlb_segments* seg, const int32_t* cols, const 
    res->converged = resid < prm.convergence_residue;
    res->status_detail = 0;
    return TNLB_OK;
+}
+
+namespace {
+
+// State of the reliable-update PCG (solve_mixed_reliable).  `halt` stops the
+// rest of a CUDA-graph batch: 1 a reliable update is due, 2 breakdown
+// ((p, A p) zero or not finite), 3 the iteration limit.
+struct RuState {
+   double rz;     // (r, z) of the iteration whose alpha was formed last
+   double alpha;
+   double trig2;  // |r|^2 of the recursion below which an update is due
+   double rr;     // |r|^2 after the last update of r
+   int32_t it, halt, maxit, pad;
+};
+
+// (a, b) into *out, for matrices the fused product does not cover.
+template <typename VT>
+__global__ void __launch_bounds__(kRedThreads) k_ru_dot(int64_t n, const VT* __restrict__ a, const VT* __restrict__ b,
+                                                        RedWork w, double* __restrict__ out,
+                                                        const int32_t* __restrict__ skip)
+{
+   if (skip && *skip) return;
+   double acc = 0;
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+      acc += (double)a[i] * (double)b[i];
+   double v[1] = {acc};
+   if (publish_and_arrive<1>(v, w)) {
+      double t[1];
+      gather_totals<1>(t, w);
+      if (threadIdx.x == 0) *out = t[0];
+   }
+}
+
+// alpha = (r, z) / (p, A p) (a zero or non-finite (p, A p) is a breakdown:
+// alpha 0, halt 2); xc += alpha p; r -= alpha Ap; |r|^2; and for Jacobi
+// (mode 1) z = r / d with (r, z), for no preconditioner (mode 0)
+// (r, z) = |r|^2, into *rz_cur.  Every block reads *rz_cur before the last
+// block overwrites it; the last block keeps the old value in S->rz for
+// beta, counts the iteration and raises `halt` when an update is due.
+// Four consecutive entries of a 16-byte-aligned vector (the solver's own
+// buffers): one float4 or two double2 accesses.
+__device__ __forceinline__ void ld4(const float* p, float (&v)[4])
+{
+   const float4 t = *reinterpret_cast<const float4*>(p);
+   v[0] = t.x;
+   v[1] = t.y;
+   v[2] = t.z;
+   v[3] = t.w;
+}
+__device__ __forceinline__ void ld4(const double* p, double (&v)[4])
+{
+   const double2 a = *reinterpret_cast<const double2*>(p), b = *reinterpret_cast<const double2*>(p + 2);
+   v[0] = a.x;
+   v[1] = a.y;
+   v[2] = b.x;
+   v[3] = b.y;
+}
+__device__ __forceinline__ void st4(float* p, const float (&v)[4])
+{
+   *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+__device__ __forceinline__ void st4(double* p, const double (&v)[4])
+{
+   *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
+   *reinterpret_cast<double2*>(p + 2) = make_double2(v[2], v[3]);
+}
+
+// One entry of k_ru_update.
+template <typename VT>
+__device__ __forceinline__ void ru_entry(VT alpha, VT& xc, VT& r, VT p, VT ap, float d, VT& z, int mode, double& rr,
+                                         double& rzn)
+{
+   xc += alpha * p;
+   r = r - alpha * ap;
+   rr += (double)r * (double)r;
+   if (mode == 1) {
+      z = r / (VT)d;
+      rzn += (double)r * (double)z;
+   }
+}
+
+template <typename VT>
+__global__ void __launch_bounds__(kRedThreads) k_ru_update(int64_t n, VT* __restrict__ xc, VT* __restrict__ r,
+                                                           const VT* __restrict__ p, const VT* __restrict__ Ap,
+                                                           const float* __restrict__ d, VT* __restrict__ z, int mode,
+                                                           RedWork w, RuState* S, double* __restrict__ rz_cur,
+                                                           const double* __restrict__ pap)
+{
+   if (S->halt) return;
+   const double rz = *rz_cur, t = *pap;
+   const bool ok = t != 0.0 && isfinite(t);
+   const VT alpha = ok ? (VT)(rz / t) : VT(0);
+   double rr = 0, rzn = 0;
+   const int64_t stride = (int64_t)gridDim.x * blockDim.x, tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+   // four entries per thread and pass (16-byte loads), then the tail
+   for (int64_t q = tid; q < n / 4; q += stride) {
+      const int64_t i = 4 * q;
+      VT xv[4], rv[4], pv[4], av[4], zv[4];
+      float dv[4] = {1.0f, 1.0f, 1.0f, 1.0f};
+      ld4(xc + i, xv);
+      ld4(r + i, rv);
+      ld4(p + i, pv);
+      ld4(Ap + i, av);
+      if (mode == 1) ld4(d + i, dv);
+#pragma unroll
+      for (int k = 0; k < 4; k++) ru_entry(alpha, xv[k], rv[k], pv[k], av[k], dv[k], zv[k], mode, rr, rzn);
+      st4(xc + i, xv);
+      st4(r + i, rv);
+      if (mode == 1) st4(z + i, zv);
+   }
+   for (int64_t i = 4 * (n / 4) + tid; i < n; i += stride) {
+      VT xv = xc[i], rv = r[i], zv = VT(0);
+      ru_entry(alpha, xv, rv, p[i], Ap[i], mode == 1 ? d[i] : 1.0f, zv, mode, rr, rzn);
+      xc[i] = xv;
+      r[i] = rv;
+      if (mode == 1) z[i] = zv;
+   }
+   double v[2] = {rr, rzn};
+   if (publish_and_arrive<2>(v, w)) {
+      double tt[2];
+      gather_totals<2>(tt, w);
+      if (threadIdx.x == 0) {
+         S->rz = rz;
+         S->alpha = (double)alpha;
+         S->it++;
+         S->rr = tt[0];
+         if (mode != 2) *rz_cur = mode == 0 ? tt[0] : tt[1];
+         if (!ok || !isfinite(tt[0]))
+            S->halt = 2;
+         else if (tt[0] < S->trig2)
+            S->halt = 1;
+         else if (S->it >= S->maxit)
+            S->halt = 3;
+      }
+   }
+}
+
+// z and (r, z) from r alone (after a reliable update): mode 1 Jacobi, mode 0 none.
+template <typename VT>
+__global__ void __launch_bounds__(kRedThreads) k_ru_precond(int64_t n, const VT* __restrict__ r,
+                                                            const float* __restrict__ d, VT* __restrict__ z, int mode,
+                                                            RedWork w, double* __restrict__ rz_out)
+{
+   double rz = 0;
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+      const VT ri = r[i];
+      const VT zi = mode == 1 ? ri / (VT)d[i] : ri;
+      if (mode == 1) z[i] = zi;
+      rz += (double)ri * (double)zi;
+   }
+   double v[1] = {rz};
+   if (publish_and_arrive<1>(v, w)) {
+      double t[1];
+      gather_totals<1>(t, w);
+      if (threadIdx.x == 0) *rz_out = t[0];
+   }
+}
+
+// p = z + beta p with beta = (r, z)_new / (r, z)_old.
+template <typename VT>
+__global__ void k_ru_p(int64_t n, VT* __restrict__ p, const VT* __restrict__ z, const double* __restrict__ rz_cur,
+                       const RuState* S)
+{
+   if (S->halt) return;
+   const VT beta = (VT)(*rz_cur / S->rz);
+   const int64_t stride = (int64_t)gridDim.x * blockDim.x, tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+   for (int64_t q = tid; q < n / 4; q += stride) {
+      VT pv[4], zv[4];
+      ld4(p + 4 * q, pv);
+      ld4(z + 4 * q, zv);
+#pragma unroll
+      for (int k = 0; k < 4; k++) pv[k] = zv[k] + beta * pv[k];
+      st4(p + 4 * q, pv);
+   }
+   for (int64_t i = 4 * (n / 4) + tid; i < n; i += stride) p[i] = z[i] + beta * p[i];
+}
+
+// x += xc (FP64); xc = 0.
+template <typename VT>
+__global__ void k_ru_fold(int64_t n, VT* __restrict__ xc, double* __restrict__ x)
+{
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+      x[i] += (double)xc[i];
+      xc[i] = VT(0);
+   }
+}
+
+// r = (VT)(b - ax) and the sums |b - ax|^2, |b|^2 (in the order
+// k_resid_norms uses, so the residual equals tnlb_true_residual's).
+template <typename VT>
+__global__ void __launch_bounds__(kRedThreads) k_ru_resid(int64_t n, const double* __restrict__ b,
+                                                          const double* __restrict__ ax, VT* __restrict__ r, RedWork w,
+                                                          double* __restrict__ out)
+{
+   double a0 = 0, a1 = 0;
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+      const double di = (double)b[i] - (double)ax[i];
+      r[i] = (VT)di;
+      a0 += di * di;
+      a1 += (double)b[i] * (double)b[i];
+   }
+   double v[2] = {a0, a1};
+   if (publish_and_arrive<2>(v, w)) {
+      double t[2];
+      gather_totals<2>(t, w);
+      if (threadIdx.x == 0) {
+         out[0] = t[0];
+         out[1] = t[1];
+      }
+   }
+}
+
+__global__ void k_ru_set(RuState* S, double trig2)
+{
+   if (threadIdx.x != 0) return;
+   S->trig2 = trig2;
+   S->halt = 0;
+}
+
+// The solver body for vectors of type VT (float: FP32 vectors; double: FP64
+// vectors with the FP32 values); see solve_mixed_reliable.
+template <typename VT>
+tnlb_status reliable_t(const tnlb_segments* seg, const int32_t* cols, const double* vals, const double* b, double* x,
+                       const tnlb_solver_params& prm, double delta, cudaStream_t st, tnlb_solve_result* res,
+                       int32_t* updates, int inner_kind, const tnlb_precond* inner_precond)
+{
+   constexpr tnlb_real kVec = sizeof(VT) == 8 ? TNLB_F64 : TNLB_F32;
+   const int64_t n = seg->n;
+   DeviceBuffer v32, ax, r, z, p, Ap, xc, scal;
+   TNLB_TRY_STATUS(v32.alloc(sizeof(float) * (seg->storage > 0 ? seg->storage : 1)));
+   TNLB_TRY_STATUS(ax.alloc(sizeof(double) * n));
+   TNLB_TRY_STATUS(r.alloc(sizeof(VT) * n));
+   TNLB_TRY_STATUS(z.alloc(sizeof(VT) * n));
+   TNLB_TRY_STATUS(p.alloc(sizeof(VT) * n));
+   TNLB_TRY_STATUS(Ap.alloc(sizeof(VT) * n));
+   TNLB_TRY_STATUS(xc.alloc(sizeof(VT) * n));
+   TNLB_TRY_STATUS(scal.alloc(sizeof(double) * 4));  // [0] (p, Ap), [1] (r, z), [2..3] residual sums
+   k_convert<float, double><<<grid_for(seg->storage, 256 * 8), 256, 0, st>>>(seg->storage, vals, v32.as<float>());
+   TNLB_CHECK_LAUNCH();
+   tnlb_precond* own = nullptr;
+   if (!inner_precond && inner_kind != TNLB_PRECOND_NONE)
+      TNLB_TRY_STATUS(precond_create(inner_kind, seg, TNLB_F32, cols, v32.ptr, st, &own));
+   struct Guard {
+      tnlb_precond* p;
+      ~Guard() { delete p; }
+   } guard{own};
+   const tnlb_precond* pobj = inner_precond ? inner_precond : own;
+   TNLB_REQUIRE(!pobj || pobj->real == TNLB_F32, TNLB_ERR_INVALID_ARGUMENT, "the inner preconditioner must be FP32");
+   TNLB_REQUIRE(!pobj || pobj->n == n, TNLB_ERR_INVALID_ARGUMENT, "preconditioner size differs from the matrix");
+   TNLB_REQUIRE(!pobj || pobj->kind == TNLB_PRECOND_JACOBI || pobj->kind == TNLB_PRECOND_FSAI,
+                TNLB_ERR_INVALID_ARGUMENT, "solve_mixed_reliable: the preconditioner must be Jacobi or FSAI");
+   TNLB_REQUIRE(!pobj || pobj->kind != TNLB_PRECOND_FSAI || !fsai_two_factor(pobj->fsai), TNLB_ERR_INVALID_ARGUMENT,
+                "solve_mixed_reliable: a two-factor FSAI is not symmetric");
+   const int mode = !pobj ? 0 : pobj->kind == TNLB_PRECOND_JACOBI ? 1 : 2;
+   const float* d = mode == 1 ? pobj->diag.as<float>() : nullptr;
+   VT* zp = mode == 0 ? r.as<VT>() : z.as<VT>();
+   const bool fused_a = spmv_dot_fusable(seg);
+   const bool fused_m = mode == 2 && fsai_dot_fusable(pobj->fsai);
+   TNLB_REQUIRE(mode != 2 || fused_m || kVec == TNLB_F32, TNLB_ERR_INVALID_ARGUMENT,
+                "solve_mixed_reliable: FP64 vectors need an FSAI whose factors hold at most 16 entries per row");
+   Work W;  // reductions of the vector kernels
+   TNLB_TRY_STATUS(W.alloc());
+   Work WA, WM;  // reductions of the fused products
+   TNLB_TRY_STATUS(WA.alloc());
+   TNLB_TRY_STATUS(WM.alloc());
+   RuState* S = reinterpret_cast<RuState*>(W.S());
+   static_assert(sizeof(RuState) <= sizeof(DevState), "RuState must fit the state buffer");
+   double* pap = scal.as<double>();
+   double* rz_cur = pap + 1;
+   double* rsum = pap + 2;
+   const int32_t* halt = &S->halt;
+   const unsigned G = vec_grid(n);
+   // grids of the per-iteration vector kernels: resident blocks only
+   const unsigned Gu = resident_grid((const void*)k_ru_update<VT>, kRedThreads, n, 4);
+   const unsigned Gp = resident_grid((const void*)k_ru_p<VT>, kRedThreads, n, 4);
+   const unsigned Gd = resident_grid((const void*)k_ru_dot<VT>, kRedThreads, n, 4);
+   const float* v32f = v32.as<float>();
+
+   // z = M^-1 r, (r, z) into rz_cur and p = z + beta p (beta = (r, z) /
+   // S->rz); a short-row symmetric FSAI does it in two fused products
+   // (t = G r with (t, t) = (r, z); p = G^T t + beta p), z never stored
+   auto precondition = [&](cudaStream_t s, const int32_t* skip) -> tnlb_status {
+      if (fused_m)
+         return fsai_apply_dot_xpby(pobj->fsai, kVec, r.ptr, p.ptr, WM.partials.as<double>(),
+                                    WM.counter.as<unsigned>(), rz_cur, &S->rz, s, skip);
+      if (mode == 2) {
+         TNLB_TRY_STATUS(fsai_apply(pobj->fsai, r.ptr, z.ptr, s, skip));
+         k_ru_dot<VT><<<Gd, kRedThreads, 0, s>>>(n, r.as<VT>(), z.as<VT>(), WM.red(), rz_cur, skip);
+      }
+      k_ru_p<VT><<<Gp, kRedThreads, 0, s>>>(n, p.as<VT>(), zp, rz_cur, S);
+      TNLB_CHECK_LAUNCH();
+      return TNLB_OK;
+   };
+   auto iteration = [&](cudaStream_t s) -> tnlb_status {
+      if (fused_a)
+         TNLB_TRY_STATUS(spmv_dot_mixed(seg, TNLB_F32, kVec, kVec, cols, v32f, p.ptr, Ap.ptr,
+                                        WA.partials.as<double>(), WA.counter.as<unsigned>(), pap, s, halt, false));
+      else {
+         // FP32 vectors: the FP32 values; FP64 vectors: the caller's FP64 values
+         if (kVec == TNLB_F32)
+            TNLB_TRY_STATUS(spmv_dispatch(seg, TNLB_F32, cols, v32f, p.ptr, Ap.ptr, 1.0, 0.0, s, halt));
+         else
+            TNLB_TRY_STATUS(spmv_dispatch(seg, TNLB_F64, cols, vals, p.ptr, Ap.ptr, 1.0, 0.0, s, halt));
+         k_ru_dot<VT><<<Gd, kRedThreads, 0, s>>>(n, p.as<VT>(), Ap.as<VT>(), WA.red(), pap, halt);
+      }
+      k_ru_update<VT><<<Gu, kRedThreads, 0, s>>>(n, xc.as<VT>(), r.as<VT>(), p.as<VT>(), Ap.as<VT>(), d, z.as<VT>(),
+                                                 mode, W.red(), S, rz_cur, pap);
+      TNLB_CHECK_LAUNCH();
+      return precondition(s, halt);
+   };
+
+   // initial state: it = 0, halt set until the first residual is in
+   RuState s0{};
+   s0.rz = 1.0;
+   s0.maxit = prm.max_iterations;
+   s0.halt = 1;
+   TNLB_CUDA_TRY(cudaMemcpyAsync(S, &s0, sizeof(s0), cudaMemcpyHostToDevice, st));
+   TNLB_CUDA_TRY(cudaMemsetAsync(p.ptr, 0, sizeof(VT) * n, st));
+   TNLB_CUDA_TRY(cudaMemsetAsync(xc.ptr, 0, sizeof(VT) * n, st));
+
+   // CUDA graph of a batch of iterations, captured once on a side stream
+   const int kBatch = n < (1 << 22) ? 32 : 16;
+   cudaStream_t cs;
+   TNLB_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+   struct StreamGuard {
+      cudaStream_t s;
+      ~StreamGuard()
+      {
+         cudaStreamSynchronize(s);
+         cudaStreamDestroy(s);
+      }
+   } sguard{cs};
+   cudaEvent_t ev;
+   TNLB_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+   TNLB_CUDA_TRY(cudaEventRecord(ev, st));
+   TNLB_CUDA_TRY(cudaStreamWaitEvent(cs, ev, 0));
+   cudaEventDestroy(ev);
+   cudaGraph_t graph = nullptr;
+   cudaGraphExec_t exec = nullptr;
+   tnlb_status status = TNLB_OK;
+   if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+      for (int k = 0; k < kBatch && status == TNLB_OK; k++) status = iteration(cs);
+      cudaError_t e = cudaStreamEndCapture(cs, &graph);
+      if (e == cudaSuccess && status == TNLB_OK) e = cudaGraphInstantiate(&exec, graph, 0);
+      if (e != cudaSuccess) {
+         cudaGetLastError();
+         exec = nullptr;
+      }
+      status = TNLB_OK;  // a failed capture falls back to direct launches
+      clear_error();
+   }
+   else
+      cudaGetLastError();
+   struct GraphGuard {  // released after the stream has drained
+      cudaStream_t s;
+      cudaGraph_t g;
+      cudaGraphExec_t e;
+      ~GraphGuard()
+      {
+         cudaStreamSynchronize(s);
+         if (e) cudaGraphExecDestroy(e);
+         if (g) cudaGraphDestroy(g);
+      }
+   } gguard{cs, graph, exec};
+   // pinned copy of the state for reads that do not stall the stream
+   struct Pinned {  // released after the stream has drained
+      cudaStream_t s;
+      RuState* p = nullptr;
+      ~Pinned()
+      {
+         cudaStreamSynchronize(s);
+         if (p) cudaFreeHost(p);
+      }
+   } hstate{cs};
+   TNLB_CUDA_TRY(cudaMallocHost(&hstate.p, sizeof(RuState)));
+   cudaEvent_t copied;
+   TNLB_CUDA_TRY(cudaEventCreateWithFlags(&copied, cudaEventDisableTiming));
+   struct EventGuard {
+      cudaEvent_t e;
+      ~EventGuard() { cudaEventDestroy(e); }
+   } eguard{copied};
+   auto launch_batch = [&]() -> tnlb_status {
+      if (exec) {
+         TNLB_CUDA_TRY(cudaGraphLaunch(exec, cs));
+         return TNLB_OK;
+      }
+      for (int k = 0; k < kBatch; k++) TNLB_TRY_STATUS(iteration(cs));
+      return TNLB_OK;
+   };
+
+   *updates = 0;
+   double resid = 0.0, bn = 0.0;
+   RuState h{};
+   bool converged = false;
+   for (;;) {
+      // reliable update: x += xc, r = b - A x in FP64, r = (VT) r
+      k_ru_fold<VT><<<G, kRedThreads, 0, cs>>>(n, xc.as<VT>(), x);
+      TNLB_CHECK_LAUNCH();
+      TNLB_TRY_STATUS(spmv_dispatch(seg, TNLB_F64, cols, vals, x, ax.ptr, 1.0, 0.0, cs));
+      k_ru_resid<VT><<<G, kRedThreads, 0, cs>>>(n, b, ax.as<double>(), r.as<VT>(), W.red(), rsum);
+      TNLB_CHECK_LAUNCH();
+      double hs[2];
+      TNLB_CUDA_TRY(cudaMemcpyAsync(hs, rsum, sizeof(hs), cudaMemcpyDeviceToHost, cs));
+      TNLB_CUDA_TRY(cudaMemcpyAsync(&h, S, sizeof(h), cudaMemcpyDeviceToHost, cs));
+      TNLB_CUDA_TRY(cudaStreamSynchronize(cs));
+      const double rn = std::sqrt(hs[0]);
+      bn = std::sqrt(hs[1]);
+      resid = bn > 0 ? rn / bn : 0.0;
+      if (bn == 0 || resid < prm.convergence_residue) {
+         converged = true;
+         break;
+      }
+      if (h.halt == 2 || h.it >= prm.max_iterations || !std::isfinite(resid)) break;
+      if (h.it > 0) (*updates)++;
+      const double t1 = delta * rn, t2 = prm.convergence_residue * bn;
+      k_ru_set<<<1, 32, 0, cs>>>(S, t1 > t2 ? t1 * t1 : t2 * t2);
+      // z = M^-1 r, (r, z), p = z + beta p with the kept direction
+      if (mode != 2) {
+         k_ru_precond<VT><<<G, kRedThreads, 0, cs>>>(n, r.as<VT>(), d, z.as<VT>(), mode, W.red(), rz_cur);
+         TNLB_CHECK_LAUNCH();
+      }
+      TNLB_TRY_STATUS(precondition(cs, halt));
+      // iterations until an update is due, one batch queued ahead of the
+      // host's check of the state (a batch after the halt skips itself)
+      TNLB_TRY_STATUS(launch_batch());
+      TNLB_CUDA_TRY(cudaMemcpyAsync(hstate.p, S, sizeof(RuState), cudaMemcpyDeviceToHost, cs));
+      TNLB_CUDA_TRY(cudaEventRecord(copied, cs));
+      for (;;) {
+         TNLB_TRY_STATUS(launch_batch());
+         TNLB_CUDA_TRY(cudaEventSynchronize(copied));
+         h = *hstate.p;
+         if (h.halt) break;
+         TNLB_CUDA_TRY(cudaMemcpyAsync(hstate.p, S, sizeof(RuState), cudaMemcpyDeviceToHost, cs));
+         TNLB_CUDA_TRY(cudaEventRecord(copied, cs));
+      }
+   }
+   TNLB_CUDA_TRY(cudaStreamSynchronize(cs));
+   res->iterations = h.it;
+   res->residue = resid;
+   res->converged = converged ? 1 : 0;
+   res->status_detail = h.halt == 2 ? 1 : 0;
+   return TNLB_OK;
+}
+
+}  // namespace
+
+// Mixed-precision PCG with reliable updates (G. L. G. Sleijpen, H. A. van der
+// Vorst, "Reliable updated residuals in hybrid Bi-CG methods", Computing 56
+// (1996); M. A. Clark et al., "Solving lattice QCD systems of equations using
+// mixed precision solvers on GPUs", Comput. Phys. Commun. 181 (2010)).  CG
+// iterates on an FP32 copy of the values (FP32 preconditioner), with FP32 or
+// FP64 vectors and FP64 dot products; its correction xc is folded into the
+// FP64 x and the residual replaced by the FP64 b - A x whenever the
+// recursive |r| has fallen below max(delta |r_last update|, tol |b|).  The
+// search direction p is kept across an update (beta = (r, z)_new /
+// (r, z)_old), so the Krylov space is not restarted as it is by iterative
+// refinement.
+tnlb_status solve_mixed_reliable(const tnlb_segments* seg, const int32_t* cols, const double* vals, const double* b,
+                                 double* x, const tnlb_solver_params& prm, double delta, tnlb_real vectors,
+                                 cudaStream_t st, tnlb_solve_result* res, int32_t* updates, int inner_kind,
+                                 const tnlb_precond* inner_precond)
+{
+   TNLB_REQUIRE(seg->n > 0, TNLB_ERR_INVALID_ARGUMENT, "solve_mixed_reliable: the matrix is empty");
+   TNLB_REQUIRE(delta > 0.0 && delta < 1.0, TNLB_ERR_INVALID_ARGUMENT, "solve_mixed_reliable: delta must lie in (0, 1)");
+   if (vectors == TNLB_F64)
+      return reliable_t<double>(seg, cols, vals, b, x, prm, delta, st, res, updates, inner_kind, inner_precond);
+   return reliable_t<float>(seg, cols, vals, b, x, prm, delta, st, res, updates, inner_kind, inner_precond);
 }
 
 }  // namespace tnlb

@@ -212,41 +212,114 @@ __global__ void __launch_bounds__(256) k_csr_short(const int32_t* __restrict__ r
 // fused into it (the (p, A p) of CG): a grid-stride loop over rows on at most
 // kRedMaxBlocks blocks, each block's sum of x[r] * y[r] published, the last
 // block to arrive adding them in block order (deterministic) into *dot_out.
-// Needs alpha = 1, beta = 0.
-template <typename Real, int L>
+// With `self`, the sum is (y, y) instead (the (r, G^T G r) = |G r|^2 of an
+// FSAI application).  Values TV, input TX, output TY (mixed storage: FP32
+// values with FP64 vectors); rows are summed in TX.  Needs alpha = 1,
+// beta = 0.
+template <typename TV, typename TX, typename TY, int L, int R>
 __global__ void __launch_bounds__(256) k_csr_short_dot(const int32_t* __restrict__ rowptr,
-                                                       const int32_t* __restrict__ cols, const Real* __restrict__ vals,
-                                                       const Real* __restrict__ x, Real* __restrict__ y, int32_t n,
+                                                       const int32_t* __restrict__ cols, const TV* __restrict__ vals,
+                                                       const TX* __restrict__ x, TY* __restrict__ y, int32_t n,
                                                        RedWork w, double* __restrict__ dot_out,
-                                                       const int32_t* __restrict__ skip)
+                                                       const int32_t* __restrict__ skip, int self)
 {
    if (skip && *skip) return;  // every block returns: no ticket is taken
    double d = 0.0;
-   for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
-      const int32_t b = rowptr[r], e = rowptr[r + 1];
-      int32_t c[L];
-      Real v[L];
+   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+   // R rows per thread and pass (r0 + k * stride), all their loads issued
+   // before any is used: R times the loads in flight of one row
+   for (int64_t r0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r0 < n; r0 += R * stride) {
+      int32_t b[R], e[R];
 #pragma unroll
-      for (int j = 0; j < L; j++) {
-         c[j] = -1;
-         v[j] = Real(0);
-         if (b + j < e) {
-            c[j] = __ldg(cols + b + j);
-            v[j] = __ldg(vals + b + j);
+      for (int k = 0; k < R; k++) {
+         const int64_t r = r0 + k * stride;
+         b[k] = r < n ? rowptr[r] : 0;
+         e[k] = r < n ? rowptr[r + 1] : 0;
+      }
+      int32_t c[R][L];
+      TV v[R][L];
+#pragma unroll
+      for (int k = 0; k < R; k++)
+#pragma unroll
+         for (int j = 0; j < L; j++) {
+            c[k][j] = -1;
+            v[k][j] = TV(0);
+            if (b[k] + j < e[k]) {
+               c[k][j] = __ldg(cols + b[k] + j);
+               v[k][j] = __ldg(vals + b[k] + j);
+            }
+         }
+      TX s[R];
+#pragma unroll
+      for (int k = 0; k < R; k++) {
+         s[k] = TX(0);
+#pragma unroll
+         for (int j = 0; j < L; j++)
+            if (c[k][j] >= 0) s[k] += (TX)v[k][j] * __ldg(x + c[k][j]);
+      }
+#pragma unroll
+      for (int k = 0; k < R; k++) {
+         const int64_t r = r0 + k * stride;
+         if (r < n) {
+            const TY ys = (TY)s[k];
+            y[r] = ys;
+            d += (double)ys * (self ? (double)ys : (double)__ldg(x + r));
          }
       }
-      Real s = Real(0);
-#pragma unroll
-      for (int j = 0; j < L; j++)
-         if (c[j] >= 0) s += v[j] * __ldg(x + c[j]);
-      y[r] = s;
-      d += (double)s * (double)__ldg(x + r);
    }
    double vv[1] = {d};
    if (publish_and_arrive<1>(vv, w)) {
       double t[1];
       gather_totals<1>(t, w);
       if (threadIdx.x == 0) *dot_out = t[0];
+   }
+}
+
+// k_csr_short with the update y = A x + (num / den) y fused into it (the
+// p = G^T t + beta p of FSAI-preconditioned CG, beta = num / den from two
+// device scalars); one thread per row; types as k_csr_short_dot.
+template <typename TV, typename TX, typename TY, int L, int R>
+__global__ void __launch_bounds__(256) k_csr_short_xpby(const int32_t* __restrict__ rowptr,
+                                                        const int32_t* __restrict__ cols, const TV* __restrict__ vals,
+                                                        const TX* __restrict__ x, TY* __restrict__ y, int32_t n,
+                                                        const double* __restrict__ num, const double* __restrict__ den,
+                                                        const int32_t* __restrict__ skip)
+{
+   if (skip && *skip) return;
+   const TY beta = (TY)(*num / *den);
+   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+   for (int64_t r0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r0 < n; r0 += R * stride) {
+      int32_t b[R], e[R];
+      TY yo[R];
+#pragma unroll
+      for (int k = 0; k < R; k++) {
+         const int64_t r = r0 + k * stride;
+         b[k] = r < n ? rowptr[r] : 0;
+         e[k] = r < n ? rowptr[r + 1] : 0;
+         yo[k] = r < n ? y[r] : TY(0);
+      }
+      int32_t c[R][L];
+      TV v[R][L];
+#pragma unroll
+      for (int k = 0; k < R; k++)
+#pragma unroll
+         for (int j = 0; j < L; j++) {
+            c[k][j] = -1;
+            v[k][j] = TV(0);
+            if (b[k] + j < e[k]) {
+               c[k][j] = __ldg(cols + b[k] + j);
+               v[k][j] = __ldg(vals + b[k] + j);
+            }
+         }
+#pragma unroll
+      for (int k = 0; k < R; k++) {
+         TX s = TX(0);
+#pragma unroll
+         for (int j = 0; j < L; j++)
+            if (c[k][j] >= 0) s += (TX)v[k][j] * __ldg(x + c[k][j]);
+         const int64_t r = r0 + k * stride;
+         if (r < n) y[r] = (TY)s + beta * yo[k];
+      }
    }
 }
 
@@ -620,30 +693,129 @@ bool spmv_dot_fusable(const tnlb_segments* seg)
 
 int64_t spmv_dot_partials(const tnlb_segments*) { return kRedMaxBlocks; }
 
-tnlb_status spmv_dot(const tnlb_segments* seg, tnlb_real real, const int32_t* cols, const void* vals, const void* x,
-                     void* y, double* partials, unsigned* counter, double* dot_out, cudaStream_t st,
-                     const int32_t* skip)
+
+namespace {
+
+// Rows per thread and pass of the fused short-row kernels (measured on the
+// 2048^2 diffusion matrix and its FSAI factors, 4.2M rows): the FP64
+// products gain from two rows in flight per thread, the FP32 product with
+// (x, y) runs fastest with one, the FP32 product with the p update with
+// four.  The row arrays are L wide (L = 5 and 7: the 2D and 3D stencils).
+template <typename TV, int L, bool Dot>
+constexpr int short_rows()
+{
+   return L > 8 ? 1 : sizeof(TV) == 8 ? (L > 5 ? 1 : 2) : Dot ? 1 : (L > 5 ? 2 : 4);
+}
+
+// The row width for seg->max_row: 4, 5, 7, 8 or 16.
+#define TNLB_SHORT_WIDTH(seg, ...)  \
+   do {                              \
+      if ((seg)->max_row <= 4) {     \
+         constexpr int L = 4;        \
+         __VA_ARGS__;                \
+      }                              \
+      else if ((seg)->max_row <= 5) { \
+         constexpr int L = 5;        \
+         __VA_ARGS__;                \
+      }                              \
+      else if ((seg)->max_row <= 7) { \
+         constexpr int L = 7;        \
+         __VA_ARGS__;                \
+      }                              \
+      else if ((seg)->max_row <= 8) { \
+         constexpr int L = 8;        \
+         __VA_ARGS__;                \
+      }                              \
+      else {                         \
+         constexpr int L = 16;       \
+         __VA_ARGS__;                \
+      }                              \
+   } while (0)
+
+template <typename TV, typename TX, typename TY>
+void launch_short_dot(const tnlb_segments* seg, const int32_t* cols, const void* vals, const void* x, void* y, RedWork w,
+                      double* dot_out, cudaStream_t st, const int32_t* skip, int self)
+{
+   const int32_t* rp = seg->offsets.as<int32_t>();
+   const TV* v = (const TV*)vals;
+   TNLB_SHORT_WIDTH(seg, {
+      constexpr int R = short_rows<TV, L, true>();
+      auto* k = k_csr_short_dot<TV, TX, TY, L, R>;
+      const unsigned g = resident_grid((const void*)k, 256, seg->n, R);
+      k<<<g, 256, 0, st>>>(rp, cols, v, (const TX*)x, (TY*)y, seg->n, w, dot_out, skip, self);
+   });
+}
+
+template <typename TV, typename TX, typename TY>
+void launch_short_xpby(const tnlb_segments* seg, const int32_t* cols, const void* vals, const void* x, void* y,
+                       const double* num, const double* den, cudaStream_t st, const int32_t* skip)
+{
+   const int32_t* rp = seg->offsets.as<int32_t>();
+   const TV* v = (const TV*)vals;
+   TNLB_SHORT_WIDTH(seg, {
+      constexpr int R = short_rows<TV, L, false>();
+      auto* k = k_csr_short_xpby<TV, TX, TY, L, R>;
+      const unsigned g = resident_grid((const void*)k, 256, seg->n, R);
+      k<<<g, 256, 0, st>>>(rp, cols, v, (const TX*)x, (TY*)y, seg->n, num, den, skip);
+   });
+}
+#undef TNLB_SHORT_WIDTH
+
+}  // namespace
+
+tnlb_status spmv_dot_mixed(const tnlb_segments* seg, tnlb_real tv, tnlb_real tx, tnlb_real ty, const int32_t* cols,
+                           const void* vals, const void* x, void* y, double* partials, unsigned* counter,
+                           double* dot_out, cudaStream_t st, const int32_t* skip, bool self_dot)
 {
    TNLB_REQUIRE(spmv_dot_fusable(seg), TNLB_ERR_INVALID_ARGUMENT, "spmv_dot: not a short-row CSR matrix");
-   const unsigned g = vec_grid(seg->n);
-   const int32_t* rp = seg->offsets.as<int32_t>();
-   // one sum: partials[block] for each of the <= kRedMaxBlocks blocks
    RedWork w{partials, counter};
-#define TNLB_SD(RT, LL) \
-   k_csr_short_dot<RT, LL><<<g, 256, 0, st>>>(rp, cols, (const RT*)vals, (const RT*)x, (RT*)y, seg->n, w, dot_out, skip)
-   if (real == TNLB_F64) {
-      if (seg->max_row <= 4) TNLB_SD(double, 4);
-      else if (seg->max_row <= 8) TNLB_SD(double, 8);
-      else TNLB_SD(double, 16);
-   }
+   const int self = self_dot ? 1 : 0;
+   if (tv == TNLB_F64 && tx == TNLB_F64 && ty == TNLB_F64)
+      launch_short_dot<double, double, double>(seg, cols, vals, x, y, w, dot_out, st, skip, self);
+   else if (tv == TNLB_F32 && tx == TNLB_F32 && ty == TNLB_F32)
+      launch_short_dot<float, float, float>(seg, cols, vals, x, y, w, dot_out, st, skip, self);
+   else if (tv == TNLB_F32 && tx == TNLB_F64 && ty == TNLB_F64)
+      launch_short_dot<float, double, double>(seg, cols, vals, x, y, w, dot_out, st, skip, self);
+   else if (tv == TNLB_F32 && tx == TNLB_F64 && ty == TNLB_F32)
+      launch_short_dot<float, double, float>(seg, cols, vals, x, y, w, dot_out, st, skip, self);
    else {
-      if (seg->max_row <= 4) TNLB_SD(float, 4);
-      else if (seg->max_row <= 8) TNLB_SD(float, 8);
-      else TNLB_SD(float, 16);
+      set_error("spmv_dot: unsupported combination of value and vector types");
+      return TNLB_ERR_INVALID_ARGUMENT;
    }
-#undef TNLB_SD
    TNLB_CHECK_LAUNCH();
    return TNLB_OK;
+}
+
+tnlb_status spmv_dot(const tnlb_segments* seg, tnlb_real real, const int32_t* cols, const void* vals, const void* x,
+                     void* y, double* partials, unsigned* counter, double* dot_out, cudaStream_t st,
+                     const int32_t* skip, bool self_dot)
+{
+   return spmv_dot_mixed(seg, real, real, real, cols, vals, x, y, partials, counter, dot_out, st, skip, self_dot);
+}
+
+tnlb_status spmv_xpby_mixed(const tnlb_segments* seg, tnlb_real tv, tnlb_real tx, tnlb_real ty, const int32_t* cols,
+                            const void* vals, const void* x, void* y, const double* num, const double* den,
+                            cudaStream_t st, const int32_t* skip)
+{
+   TNLB_REQUIRE(spmv_dot_fusable(seg), TNLB_ERR_INVALID_ARGUMENT, "spmv_xpby: not a short-row CSR matrix");
+   if (tv == TNLB_F64 && tx == TNLB_F64 && ty == TNLB_F64)
+      launch_short_xpby<double, double, double>(seg, cols, vals, x, y, num, den, st, skip);
+   else if (tv == TNLB_F32 && tx == TNLB_F32 && ty == TNLB_F32)
+      launch_short_xpby<float, float, float>(seg, cols, vals, x, y, num, den, st, skip);
+   else if (tv == TNLB_F32 && tx == TNLB_F32 && ty == TNLB_F64)
+      launch_short_xpby<float, float, double>(seg, cols, vals, x, y, num, den, st, skip);
+   else {
+      set_error("spmv_xpby: unsupported combination of value and vector types");
+      return TNLB_ERR_INVALID_ARGUMENT;
+   }
+   TNLB_CHECK_LAUNCH();
+   return TNLB_OK;
+}
+
+tnlb_status spmv_xpby(const tnlb_segments* seg, tnlb_real real, const int32_t* cols, const void* vals, const void* x,
+                      void* y, const double* num, const double* den, cudaStream_t st, const int32_t* skip)
+{
+   return spmv_xpby_mixed(seg, real, real, real, cols, vals, x, y, num, den, st, skip);
 }
 
 tnlb_status spmv_csr(const tnlb_segments* seg, tnlb_real real, const int32_t* cols, const void* vals, const void* x,
