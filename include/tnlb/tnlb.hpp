@@ -5,6 +5,7 @@
 //   TNL::Matrices::SparseMatrix< Real, Devices::Cuda, int, GeneralMatrix, Segments >
 //        setDimensions, setRowCapacities, setFromCSR (the cross-format
 //        operator= from a CSR matrix), vectorProduct, transposedVectorProduct,
+//        getTransposition,
 //        getRows, getColumns; MatrixType GeneralMatrix or SymmetricMatrix
 //        (Matrices/SparseMatrix.h:41-57, SparseMatrixBase.h:1020-1035);
 //   TNL::Algorithms::Segments::{CSR, Ellpack, SlicedEllpack, ChunkedEllpack,
@@ -317,6 +318,33 @@ public:
       tnlb::check(tnlb_spmv_transposed(seg_, tnlb::real_code<Real>(), columns_idx_.getData(), values_.getData(),
                                        columns_, in.getData(), out.getData(), matrixMultiplicator,
                                        outVectorMultiplicator, begin, end, nullptr));
+      tnlb::cuda_check(cudaStreamSynchronize(nullptr));
+   }
+   // SparseMatrix::getTransposition (SparseMatrix.hpp:495-551): this matrix
+   // becomes matrixMultiplicator * matrix^T (any format of `matrix`, same
+   // real type), the rows in ascending column order.  Filled through the
+   // cross-format assignment: an explicitly stored zero leaves a padding slot.
+   template <typename Matrix2>
+   void getTransposition(const Matrix2& matrix, Real matrixMultiplicator = 1)
+   {
+      static_assert(std::is_same<typename Matrix2::RealType, Real>::value, "getTransposition: same real type");
+      const Index nt = matrix.getColumns();
+      Containers::Vector<Index> trp(nt + 1);
+      int64_t nnz = 0;
+      tnlb::check(tnlb_matrix_transpose_rowptr(matrix.segments(), matrix.getColumnIndexes().getData(), nt,
+                                               trp.getData(), &nnz, nullptr));
+      Containers::Vector<Index> tc((Index)(nnz > 0 ? nnz : 1));
+      Containers::Vector<Real> tv((Index)(nnz > 0 ? nnz : 1));
+      tnlb::check(tnlb_matrix_transpose_fill(matrix.segments(), tnlb::real_code<Real>(),
+                                             matrix.getColumnIndexes().getData(), matrix.getValues().getData(), nt,
+                                             (double)matrixMultiplicator, tc.getData(), tv.getData(), nullptr));
+      std::vector<Index> hrp(nt + 1), caps(nt);
+      trp.copyToHost(hrp.data());
+      for (Index i = 0; i < nt; i++) caps[i] = hrp[i + 1] - hrp[i];
+      setDimensions(nt, matrix.getRows());
+      setRowCapacities(caps);
+      tnlb::check(tnlb_matrix_fill_from_csr(seg_, tnlb::real_code<Real>(), trp.getData(), tc.getData(), tv.getData(),
+                                            columns_idx_.getData(), values_.getData(), nullptr));
       tnlb::cuda_check(cudaStreamSynchronize(nullptr));
    }
    Index getRows() const { return rows_; }

@@ -292,6 +292,22 @@ void tnlb_host_csr_free(tnlb_host_csr* m);
 tnlb_status tnlb_matrix_to_host_csr(const tnlb_segments* seg, tnlb_real real, const int32_t* d_cols,
                                     const void* d_values, int32_t columns, tnlb_host_csr* out);
 
+/* Transposition -- SparseMatrix::getTransposition (Matrices/SparseMatrix.hpp:
+ * 495-551): B = multiplicator * A^T (A of any format, `columns` columns)
+ * as device CSR arrays, B having `columns` rows.  Step 1 writes B's row
+ * pointer (columns + 1 entries) into d_trowptr and its number of entries
+ * (the stored, non-padding entries of A, zeros included) into *h_nnz; step
+ * 2 writes B's columns and values (h_nnz entries each).  The entries of a
+ * row of B come in ascending column order -- what the reference's
+ * single-threaded build gives (its multi-threaded build leaves each row in
+ * the order its atomic cursor was claimed).  A column index outside
+ * [0, columns) is an invalid argument.  Synchronous. */
+tnlb_status tnlb_matrix_transpose_rowptr(const tnlb_segments* seg, const int32_t* d_cols, int32_t columns,
+                                         int32_t* d_trowptr, int64_t* h_nnz, tnlb_stream stream);
+tnlb_status tnlb_matrix_transpose_fill(const tnlb_segments* seg, tnlb_real real, const int32_t* d_cols,
+                                       const void* d_values, int32_t columns, double multiplicator,
+                                       int32_t* d_tcols, void* d_tvalues, tnlb_stream stream);
+
 /* Write host CSR arrays as MatrixWriter::writeMtx does
  * (Matrices/MatrixWriter.hpp:107-129): "coordinate real general", 1-based
  * "row column value" lines of widths 9, 9, 12 at default stream precision,

@@ -295,6 +295,23 @@ class Oracle:
         return {"x": x, "converged": ok == 1, "status": ok, "iterations": S.iterations, "residue": S.residue,
                 "history": hist}
 
+    @staticmethod
+    def transpose(A, mult=1.0, real=np.float64):
+        """getTransposition (Matrices/SparseMatrix.hpp:495-551) restated:
+        the entries of A stably sorted by column, so each row of B = mult * A^T
+        holds its entries in ascending column order (the reference's
+        single-threaded order); values multiplied by mult in `real`.
+        Returns (rowptr, cols, vals) with ncols rows."""
+        rowptr, cols = np.asarray(A.rowptr, np.int64), np.asarray(A.cols, np.int64)
+        rows = np.repeat(np.arange(A.n, dtype=np.int64), np.diff(rowptr))
+        keep = cols != -1
+        rows, cols, vals = rows[keep], cols[keep], np.asarray(A.vals, real)[keep]
+        order = np.argsort(cols, kind="stable")
+        trp = np.zeros(A.ncols + 1, np.int64)
+        np.add.at(trp, cols + 1, 1)
+        return (np.cumsum(trp).astype(np.int32), rows[order].astype(np.int32),
+                (vals[order] * real(mult)).astype(real))
+
     def pcg_reliable(self, A, b, precond: int = 1, tol=1e-8, delta=0.1, maxit=100000, x0=None, vec64=False):
         """The library's mixed-precision PCG with reliable updates (FP32
         values, FP32 or FP64 vectors, FP64 updates); precond 0 none, 1 Jacobi."""
@@ -360,6 +377,7 @@ class Reference:
             ("ref_mtx_read", [C.c_char_p, i32, p, p, p, p, p, p, C.c_char_p, i32], C.c_int),
             ("ref_mtx_write", [C.c_char_p, i32, i32, p, p, p], None),
             ("ref_spmv_transposed_f64", [i32, i32, p, p, p, p, p, f64, f64, i32, i32], None),
+            ("ref_transpose_f64", [i32, i32, p, p, p, f64, p, p, p], C.c_long),
             ("ref_prec_apply", [i32, p, p, p, i32, p, p], C.c_int),
             ("ref_omp_threads", [], C.c_int),
             ("ref_set_threads", [C.c_int], None),
@@ -499,6 +517,20 @@ class Reference:
         self.L.ref_spmv_transposed_f64(A.n, A.ncols, rowptr.ctypes.data, cols.ctypes.data, vals.ctypes.data,
                                        x.ctypes.data, y.ctypes.data, alpha, beta, begin, end)
         return y
+
+    def transpose(self, A, mult=1.0):
+        """The reference's getTransposition of a general CSR matrix into CSR:
+        (rowptr, cols, vals) of mult * A^T, padding included."""
+        rowptr, cols = _i32(A.rowptr), _i32(A.cols)
+        vals = np.ascontiguousarray(A.vals, np.float64)
+        size = self.L.ref_transpose_f64(A.n, A.ncols, rowptr.ctypes.data, cols.ctypes.data, vals.ctypes.data, mult,
+                                        None, None, None)
+        trp = np.zeros(A.ncols + 1, np.int32)
+        tc = np.zeros(max(size, 1), np.int32)
+        tv = np.zeros(max(size, 1), np.float64)
+        self.L.ref_transpose_f64(A.n, A.ncols, rowptr.ctypes.data, cols.ctypes.data, vals.ctypes.data, mult,
+                                 trp.ctypes.data, tc.ctypes.data, tv.ctypes.data)
+        return trp, tc[:size], tv[:size]
 
     def solve(self, solver: str, A, b, x0=None, precond: int = 1, tol=1e-8, maxit=100000, gmres_m=30,
               gmres_variant: int = 3, bicgstab_exact=False, ell=1, idr_s=4, idr_smoothing=False):

@@ -430,6 +430,30 @@ ref_spmv_transposed_f64( int n, int ncols, const int* rowptr, const int* cols, c
       y[ i ] = yv[ i ];
 }
 
+// SparseMatrix::getTransposition of a CSR matrix into a CSR matrix:
+// B = mult * A^T (B has ncols rows); writes B's row pointer (ncols + 1),
+// columns and values (B's storage, padding included).  Returns B's storage
+// size.  Outputs may be null on a first, sizing call.
+long
+ref_transpose_f64( int n, int ncols, const int* rowptr, const int* cols, const double* vals, double mult, int* trowptr,
+                   int* tcols, double* tvals )
+{
+   Mat< double, Seg::CSR > A, B;
+   makeCSR( A, n, ncols, rowptr, cols, vals );
+   B.getTransposition( A, mult );
+   const auto& off = B.getSegments().getOffsets();
+   const long storage = off[ ncols ];
+   if( trowptr )
+      for( int i = 0; i <= ncols; i++ )
+         trowptr[ i ] = off[ i ];
+   if( tcols && tvals )
+      for( long j = 0; j < storage; j++ ) {
+         tcols[ j ] = B.getColumnIndexes()[ j ];
+         tvals[ j ] = B.getValues()[ j ];
+      }
+   return storage;
+}
+
 // MatrixReader::readMtx into a general (symmetric == 0) or SymmetricMatrix
 // CSR matrix on the host.  First call with null arrays returns the sizes in
 // rows/columns/nnz; the second fills rowptr/cols/vals.  Returns 0, or -1

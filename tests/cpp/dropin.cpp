@@ -52,6 +52,23 @@ int main()
    }
    catch (const std::invalid_argument&) {
    }
+   // getTransposition of the (symmetric-valued) Laplacian gives it back
+   {
+      Matrices::SparseMatrix<double, Devices::Cuda, int, Matrices::GeneralMatrix, Algorithms::Segments::CSR> T;
+      T.getTransposition(*A, 2.0);
+      std::vector<int> trp, tcols;
+      std::vector<double> tvals;
+      T.toHostCSR(trp, tcols, tvals);
+      if (T.getRows() != n || trp != rp || tcols != cols) {
+         std::printf("FAIL transposition pattern\n");
+         return 1;
+      }
+      for (size_t k = 0; k < vals.size(); k++)
+         if (tvals[k] != 2.0 * vals[k]) {
+            std::printf("FAIL transposition value %zu\n", k);
+            return 1;
+         }
+   }
    // CG + Jacobi
    Solvers::Linear::CG<Matrix> solver;
    solver.setMatrix(A);

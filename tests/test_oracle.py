@@ -306,3 +306,32 @@ def test_reliable_update_pcg_restatement(oracle):
     v = oracle.pcg_reliable(A, b, precond=1, tol=1e-8, delta=0.1, vec64=True)
     assert v["converged"] and oracle.true_residual(A, b, v["x"]) < 1e-8
     assert v["iterations"] <= 1.3 * f["iterations"], (v["iterations"], f["iterations"])
+
+
+def test_transposition_matches_reference(oracle, reference):
+    """getTransposition: the restatement (stable sort by column) equals the
+    reference's single-threaded Host result bit for bit -- row pointer,
+    columns in order and values times the multiplicator -- on square,
+    rectangular and empty-row matrices."""
+    from tnl_b200.generators import CSRMatrix
+
+    t0 = reference.threads()
+    reference.set_threads(1)
+    try:
+        P = g.power_law(3000, 1.73, 300, 5)
+        rng = np.random.default_rng(3)
+        # rectangular: 500 rows, 1700 columns, some empty rows
+        lens = rng.integers(0, 9, 500)
+        lens[::7] = 0
+        rp = np.zeros(501, np.int32)
+        rp[1:] = np.cumsum(lens)
+        cols = np.concatenate([np.sort(rng.choice(1700, k, replace=False)) for k in lens]).astype(np.int32)
+        R = CSRMatrix(rp, cols, rng.uniform(-1, 1, rp[-1]), ncols=1700)
+        for A in (g.laplacian_2d(20), P, R):
+            for mult in (1.0, -2.5):
+                trp, tc, tv = oracle.transpose(A, mult)
+                rrp, rc, rv = reference.transpose(A, mult)
+                assert np.array_equal(trp, rrp) and np.array_equal(tc, rc)
+                assert np.array_equal(tv, rv)
+    finally:
+        reference.set_threads(t0)

@@ -362,3 +362,39 @@ def test_symmetric_and_transposed_products(oracle, mats, fmt, org, real):
             xs, ys = torch.tensor(x, device="cuda"), torch.tensor(y0, device="cuda")
             M.transposedVectorProduct(xs, ys, alpha, beta, begin, end)
             assert_spmv_close(ys.cpu().numpy(), yref, abs(alpha) * absT + abs(beta) * np.abs(y0), RTOL[real])
+
+
+@pytest.mark.parametrize("fmt", list(FORMATS))
+@pytest.mark.parametrize("real", [np.float64, np.float32])
+def test_transposition(oracle, mats, fmt, real):
+    """getTransposition from every format: B's stored entries (host CSR
+    export) equal the oracle's stable-sorted transposition bit for bit --
+    row pointer, columns in ascending order, values times the multiplicator
+    in the matrix's real type -- and B's product equals A's transposed
+    product."""
+    t = tnl()
+    tdt = torch.float64 if real == np.float64 else torch.float32
+    from tnl_b200 import generators as g
+
+    for mname, A in mats.items():
+        vals = A.vals.astype(real)
+        M = t.SparseMatrix(t.FORMATS[fmt], tdt).assign(A.rowptr, A.cols, vals, A.ncols)
+        for mult in (1.0, -2.5):
+            B = M.getTransposition(mult, segments=t.CSR)
+            assert B.getRows() == A.ncols and B.getColumns() == A.n
+            h = B.toHostCSR()
+            from tnl_b200.generators import CSRMatrix
+
+            trp, tc, tv = oracle.transpose(CSRMatrix(A.rowptr, A.cols, vals, A.ncols), mult, real)
+            assert np.array_equal(h.rowptr, trp), mname
+            assert np.array_equal(h.cols, tc), mname
+            assert np.array_equal(h.vals.astype(real), tv), mname
+        # the same format as A, and its product against A^T x
+        B = M.getTransposition(1.0)
+        x = torch.tensor(g.uniform_vector(A.n, 4).astype(real), device="cuda")
+        y1 = torch.zeros(A.ncols, dtype=tdt, device="cuda")
+        y2 = torch.zeros(A.ncols, dtype=tdt, device="cuda")
+        B.vectorProduct(x, y1)
+        M.transposedVectorProduct(x, y2)
+        tol = 1e-12 if real == np.float64 else 1e-4
+        assert torch.allclose(y1, y2, rtol=tol, atol=tol * float(y2.abs().max())), mname

@@ -370,6 +370,27 @@ class SparseMatrix:
         finally:
             capi.tnlb_host_csr_free(C.byref(h))
 
+    def getTransposition(self, matrixMultiplicator: float = 1.0, segments=None) -> "SparseMatrix":
+        """B = matrixMultiplicator * A^T as a new matrix (SparseMatrix::getTransposition,
+        SparseMatrix.hpp:495-551), in ``segments`` (default: this matrix's
+        format) with this matrix's real type; rows of B in ascending column
+        order.  B is filled through the cross-format assignment, so an
+        explicitly stored zero of A (or a zero multiplicator) leaves a
+        padding slot in B where the reference stores a zero."""
+        n_t = self.columns
+        trp = torch.zeros(n_t + 1, dtype=torch.int32, device="cuda")
+        nnz = C.c_int64()
+        cols = self.columnIndexes.data_ptr() if self.columnIndexes.numel() else None
+        check(capi.tnlb_matrix_transpose_rowptr(self.segments.handle, cols, n_t, trp.data_ptr(), C.byref(nnz),
+                                                _stream()))
+        tc = torch.empty(max(nnz.value, 1), dtype=torch.int32, device="cuda")
+        tv = torch.empty(max(nnz.value, 1), dtype=self.real, device="cuda")
+        check(capi.tnlb_matrix_transpose_fill(self.segments.handle, _real_code(self.real), cols,
+                                              self.values.data_ptr() if self.values.numel() else None, n_t,
+                                              float(matrixMultiplicator), tc.data_ptr(), tv.data_ptr(), _stream()))
+        B = SparseMatrix(segments if segments is not None else self.segments_cls, self.real, self.organization)
+        return B.assign(trp, tc[:nnz.value], tv[:nnz.value], self.rows)
+
     def transposedVectorProduct(self, inVector: torch.Tensor, outVector: torch.Tensor, matrixMultiplicator: float = 1.0,
                             outVectorMultiplicator: float = 0.0, begin: int = 0, end: int = 0, stream=None,
                             synchronize: bool = True) -> None:

@@ -118,6 +118,8 @@ tnlb_solve = _sig("tnlb_solve", [C.c_int, C.c_int, C.POINTER(SolverParams), _p, 
 tnlb_true_residual = _sig("tnlb_true_residual", [_p, C.c_int, _p, _p, _p, _p, _p, C.POINTER(_f64)])
 tnlb_solve_mixed = _sig("tnlb_solve_mixed", [C.POINTER(SolverParams), _p, _p, _p, _p, _p, _f64, _i32, C.c_int,
                                              C.c_int, _p, _p, C.POINTER(SolveResult), C.POINTER(_i32)])
+tnlb_matrix_transpose_rowptr = _sig("tnlb_matrix_transpose_rowptr", [_p, _p, _i32, _p, C.POINTER(_i64), _p])
+tnlb_matrix_transpose_fill = _sig("tnlb_matrix_transpose_fill", [_p, C.c_int, _p, _p, _i32, _f64, _p, _p, _p])
 tnlb_solve_mixed_reliable = _sig("tnlb_solve_mixed_reliable", [C.POINTER(SolverParams), _p, _p, _p, _p, _p, _f64,
                                                                C.c_int, C.c_int, _p, _p, C.POINTER(SolveResult),
                                                                C.POINTER(_i32)])
