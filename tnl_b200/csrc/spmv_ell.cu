@@ -49,6 +49,24 @@ __global__ void k_ell_col(const int32_t* __restrict__ cols, const Real* __restri
    if (row >= end) return;
    Real sum = 0;
    int32_t k = 0;
+   if (width <= 8) {
+      // narrow rows (stencils): every slot's load issued at once
+      int32_t c[8];
+      Real v[8];
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+         c[u] = -1;
+         v[u] = Real(0);
+         if (u < width) {
+            c[u] = ld_stream(cols + row + (int64_t)aligned * u);
+            v[u] = ld_stream(vals + row + (int64_t)aligned * u);
+         }
+      }
+#pragma unroll
+      for (int u = 0; u < 8; u++)
+         if (c[u] >= 0) sum += v[u] * ld_gather(x + c[u]);
+      k = width;
+   }
    for (; k + 4 <= width; k += 4) {
       int32_t c[4];
       Real v[4];
@@ -98,6 +116,24 @@ __global__ void __launch_bounds__(256) k_sell_col(const int32_t* __restrict__ co
       const int64_t off = slice_off[slice] + lane;
       const int32_t w = slice_w[slice];
       int32_t k = sub;
+      if (G == 1 && w <= 8) {
+         // narrow slices (stencils): every slot's load issued at once
+         int32_t c[8];
+         Real v[8];
+#pragma unroll
+         for (int u = 0; u < 8; u++) {
+            c[u] = -1;
+            v[u] = Real(0);
+            if (u < w) {
+               c[u] = ld_stream(cols + off + (int64_t)kSellSlice * u);
+               v[u] = ld_stream(vals + off + (int64_t)kSellSlice * u);
+            }
+         }
+#pragma unroll
+         for (int u = 0; u < 8; u++)
+            if (c[u] >= 0) sum += v[u] * ld_gather(x + c[u]);
+         k = w;
+      }
       for (; k + 3 * G < w; k += 4 * G) {
          int32_t c[4];
          Real v[4];
