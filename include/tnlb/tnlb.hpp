@@ -347,6 +347,53 @@ public:
                                             columns_idx_.getData(), values_.getData(), nullptr));
       tnlb::cuda_check(cudaStreamSynchronize(nullptr));
    }
+   // The matrix type string of TNL's binary file (SparseMatrixBase.hpp:46-53).
+   static std::string getSerializationType()
+   {
+      const tnlb_format f = Segments<Device, Index, void>::format;
+      const std::string org = Organization == Algorithms::Segments::RowMajorOrder ? "RowMajorOrder" : "ColumnMajorOrder";
+      std::string seg;
+      switch (f) {
+         case TNLB_CSR: seg = "CSR< int >"; break;
+         case TNLB_ADAPTIVE_CSR: seg = "AdaptiveCSR< int >"; break;
+         case TNLB_ELLPACK: seg = "Ellpack< int, " + org + ", 32 >"; break;
+         case TNLB_SLICED_ELLPACK: seg = "SlicedEllpack< int, " + org + ", 32 >"; break;
+         case TNLB_CHUNKED_ELLPACK: seg = "ChunkedEllpack< int, " + org + " >"; break;
+         case TNLB_BIELLPACK: seg = "BiEllpack< int, " + org + ", 32 >"; break;
+      }
+      return std::string("Matrices::SparseMatrix< ") + (std::is_same<Real, double>::value ? "double" : "float") + ", " +
+             seg + ", [any_device], int, " + (isSymmetric() ? "Symmetric" : "General") +
+             ", [any_allocator], [any_allocator] >";
+   }
+   // SparseMatrix::save (SparseMatrix.hpp:632-643): the reference's bytes.
+   void save(const std::string& fileName) const
+   {
+      tnlb::check(tnlb_matrix_save(fileName.c_str(), seg_, tnlb::real_code<Real>(), columns_idx_.getData(),
+                                   values_.getData(), rows_, columns_, isSymmetric() ? 1 : 0));
+   }
+   // SparseMatrix::load (SparseMatrix.hpp:646-694): the file's type must be
+   // this matrix's type (else std::runtime_error with the reference's
+   // FileDeserializationError message); segments from the stored metadata.
+   void load(const std::string& fileName)
+   {
+      tnlb_matrix_file_info info;
+      tnlb::check(tnlb_matrix_file_info_read(fileName.c_str(), &info));
+      const std::string expected = getSerializationType();
+      if (expected != info.type)
+         throw std::runtime_error(fileName + ": object type does not match (expected " + expected + ", found " +
+                                  info.type + ").");
+      const Index slots = (Index)(info.storage > 0 ? info.storage : 1);
+      values_.setSize(slots);
+      columns_idx_.setSize(slots);
+      tnlb_segments* s = nullptr;
+      tnlb::check(tnlb_matrix_load(fileName.c_str(), &s, columns_idx_.getData(), values_.getData(), slots));
+      tnlb_segments_destroy(seg_);
+      seg_ = s;
+      rows_ = (Index)info.rows;
+      columns_ = (Index)info.columns;
+      values_.setSize((Index)info.storage);
+      columns_idx_.setSize((Index)info.storage);
+   }
    Index getRows() const { return rows_; }
    Index getColumns() const { return columns_; }
    static constexpr bool isSymmetric() { return std::is_same<MatrixType, SymmetricMatrix>::value; }

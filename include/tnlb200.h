@@ -308,6 +308,41 @@ tnlb_status tnlb_matrix_transpose_fill(const tnlb_segments* seg, tnlb_real real,
                                        const void* d_values, int32_t columns, double multiplicator,
                                        int32_t* d_tcols, void* d_tvalues, tnlb_stream stream);
 
+/* TNL's binary matrix file (SparseMatrix::save / load,
+ * Matrices/SparseMatrix.hpp:632-700, SparseMatrixBase.hpp:1148-1159): the
+ * object header "TNLMN" + the matrix type string, size_t rows and columns,
+ * the segments' own save() and the value and column arrays -- the bytes the
+ * reference writes for the same matrix.  Two arrays of the reference hold
+ * bytes it never initialises (ChunkedEllpack's slice records beyond
+ * numberOfSlices, unset fields and padding of AdaptiveCSR descriptors);
+ * those are written as zeros. */
+typedef struct {
+   int32_t format;       /* tnlb_format */
+   int32_t organization; /* tnlb_organization (column-major for the CSR formats) */
+   int32_t real;         /* tnlb_real */
+   int32_t symmetric;    /* 1 for a SymmetricMatrix */
+   int64_t rows;
+   int64_t columns;
+   int64_t storage;      /* slots of the value and column arrays */
+   char type[512];       /* the object type string */
+} tnlb_matrix_file_info;
+
+/* Save a matrix (segments + device columns/values of `real` type) to `path`.
+ * Synchronous.  I/O failure: TNLB_ERR_IO. */
+tnlb_status tnlb_matrix_save(const char* path, const tnlb_segments* seg, tnlb_real real, const int32_t* d_cols,
+                             const void* d_values, int32_t rows, int32_t columns, int32_t symmetric);
+/* The header of a matrix file: format, organization, real type, symmetry,
+ * dimensions, storage and the type string.  Host only.  A file that is not
+ * a TNL object (wrong magic number), has an unsupported type or is
+ * truncated: TNLB_ERR_IO with the reason. */
+tnlb_status tnlb_matrix_file_info_read(const char* path, tnlb_matrix_file_info* info);
+/* Load a matrix file: a new segments object built from the stored metadata
+ * (no rebuild) into *out, and the values and columns copied into device
+ * arrays of `capacity` >= info.storage slots (of the file's real type).
+ * Synchronous. */
+tnlb_status tnlb_matrix_load(const char* path, tnlb_segments** out, int32_t* d_cols, void* d_values,
+                             int64_t capacity);
+
 /* Write host CSR arrays as MatrixWriter::writeMtx does
  * (Matrices/MatrixWriter.hpp:107-129): "coordinate real general", 1-based
  * "row column value" lines of widths 9, 9, 12 at default stream precision,

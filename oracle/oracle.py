@@ -378,6 +378,7 @@ class Reference:
             ("ref_mtx_write", [C.c_char_p, i32, i32, p, p, p], None),
             ("ref_spmv_transposed_f64", [i32, i32, p, p, p, p, p, f64, f64, i32, i32], None),
             ("ref_transpose_f64", [i32, i32, p, p, p, f64, p, p, p], C.c_long),
+            ("ref_save", [C.c_int, C.c_int, C.c_int, i32, i32, p, p, p, C.c_char_p], C.c_int),
             ("ref_prec_apply", [i32, p, p, p, i32, p, p], C.c_int),
             ("ref_omp_threads", [], C.c_int),
             ("ref_set_threads", [C.c_int], None),
@@ -517,6 +518,16 @@ class Reference:
         self.L.ref_spmv_transposed_f64(A.n, A.ncols, rowptr.ctypes.data, cols.ctypes.data, vals.ctypes.data,
                                        x.ctypes.data, y.ctypes.data, alpha, beta, begin, end)
         return y
+
+    def save(self, fmt: int, A, path, colmajor=True, real64=True) -> None:
+        """The reference's SparseMatrix::save of A in format `fmt` (built by
+        its cross-format operator= from CSR)."""
+        rowptr, cols = _i32(A.rowptr), _i32(A.cols)
+        vals = np.ascontiguousarray(A.vals, np.float64)
+        rc = self.L.ref_save(fmt, int(colmajor), int(real64), A.n, A.ncols, rowptr.ctypes.data, cols.ctypes.data,
+                             vals.ctypes.data, str(path).encode())
+        if rc != 0:
+            raise RuntimeError("reference save failed")
 
     def transpose(self, A, mult=1.0):
         """The reference's getTransposition of a general CSR matrix into CSR:

@@ -13,6 +13,7 @@
 #include <cstring>
 #include <memory>
 #include <stdexcept>
+#include <vector>
 #ifdef _OPENMP
    #include <omp.h>
 #endif
@@ -452,6 +453,36 @@ ref_transpose_f64( int n, int ncols, const int* rowptr, const int* cols, const d
          tvals[ j ] = B.getValues()[ j ];
       }
    return storage;
+}
+
+// SparseMatrix::save of a matrix of format `fmt` (organization per
+// `colmajor`) built from CSR by the cross-format operator=, with FP64
+// (real64 != 0) or FP32 values.  Returns 0, or -1 on an exception.
+int
+ref_save( int fmt, int colmajor, int real64, int n, int ncols, const int* rowptr, const int* cols, const double* vals,
+          const char* path )
+{
+   try {
+      if( real64 )
+         return (int) dispatch< double >( fmt, colmajor, n, ncols, rowptr, cols, vals,
+                                          [ & ]( auto& A ) -> long
+                                          {
+                                             A.save( path );
+                                             return 0;
+                                          } );
+      std::vector< float > v32( rowptr[ n ] );
+      for( int k = 0; k < rowptr[ n ]; k++ )
+         v32[ k ] = (float) vals[ k ];
+      return (int) dispatch< float >( fmt, colmajor, n, ncols, rowptr, cols, v32.data(),
+                                      [ & ]( auto& A ) -> long
+                                      {
+                                         A.save( path );
+                                         return 0;
+                                      } );
+   }
+   catch( ... ) {
+      return -1;
+   }
 }
 
 // MatrixReader::readMtx into a general (symmetric == 0) or SymmetricMatrix

@@ -69,6 +69,30 @@ int main()
             return 1;
          }
    }
+   // save / load round trip through TNL's binary file, and the type check
+   {
+      const std::string path = "dropin_matrix.tnl";
+      A->save(path);
+      Matrix B;
+      B.load(path);
+      Containers::Vector<double> yb(n, 0.0);
+      B.vectorProduct(x, yb);
+      A->vectorProduct(x, y);
+      if (yb.toHost() != y.toHost()) {
+         std::printf("FAIL load product\n");
+         return 1;
+      }
+      try {
+         Matrices::SparseMatrix<float, Devices::Cuda, int, Matrices::GeneralMatrix, Algorithms::Segments::SlicedEllpack>
+            C;
+         C.load(path);
+         std::printf("FAIL load of another type\n");
+         return 1;
+      }
+      catch (const std::runtime_error&) {
+      }
+      std::remove(path.c_str());
+   }
    // CG + Jacobi
    Solvers::Linear::CG<Matrix> solver;
    solver.setMatrix(A);

@@ -124,3 +124,38 @@ def test_mtx_write_matches_reference_bytes(tmp_path, reference):
     assert ours.read_bytes() == ref.read_bytes()
     B = tnl_b200.read_mtx(ours)
     assert B.n == A.n and B.ncols == A.ncols
+
+
+def test_matrix_file_header_of_reference_files(tmp_path):
+    """tnlb_matrix_file_info_read (host only) on files the reference's own
+    SparseMatrix::save wrote: type string, dimensions and storage of every
+    format; a file that is no TNL object is an I/O error with the reason."""
+    import ctypes as C
+
+    from oracle.oracle import REF_SO, Reference
+    from tnl_b200 import _capi, generators as g
+
+    if not REF_SO.exists():
+        pytest.skip("the reference driver oracle/_ref is not built")
+    R = Reference()
+    A = g.laplacian_2d(7)
+    names = {0: "CSR< int >", 1: "Ellpack< int, ColumnMajorOrder, 32 >", 2: "SlicedEllpack< int, ColumnMajorOrder, 32 >",
+             3: "ChunkedEllpack< int, ColumnMajorOrder >", 4: "BiEllpack< int, ColumnMajorOrder, 32 >",
+             5: "AdaptiveCSR< int >"}
+    for fmt, seg in names.items():
+        for real64 in (True, False):
+            path = tmp_path / f"m{fmt}{int(real64)}.tnl"
+            R.save(fmt, A, path, colmajor=True, real64=real64)
+            info = _capi.MatrixFileInfo()
+            assert _capi.tnlb_matrix_file_info_read(str(path).encode(), C.byref(info)) == _capi.OK
+            real = "double" if real64 else "float"
+            assert info.type.decode() == (f"Matrices::SparseMatrix< {real}, {seg}, [any_device], int, General, "
+                                          "[any_allocator], [any_allocator] >")
+            assert info.rows == A.n and info.columns == A.ncols
+            assert info.real == (_capi.F64 if real64 else _capi.F32) and info.format == fmt
+            assert info.storage >= A.nnz
+    bad = tmp_path / "bad.tnl"
+    bad.write_bytes(b"not a tnl file")
+    info = _capi.MatrixFileInfo()
+    assert _capi.tnlb_matrix_file_info_read(str(bad).encode(), C.byref(info)) == _capi.ERR_IO
+    assert b"magic number" in _capi.tnlb_last_error()

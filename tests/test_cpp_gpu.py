@@ -21,5 +21,5 @@ def test_cpp_dropin_program():
                         "-L", str(lib), "-ltnlb200", f"-Xlinker=-rpath={lib}", "-o", str(exe)],
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
-    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120, cwd=str(out))
     assert r.returncode == 0 and r.stdout.startswith("OK"), r.stdout + r.stderr

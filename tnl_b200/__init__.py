@@ -127,6 +127,14 @@ class _Segments:
         self._h = h
         check(capi.tnlb_segments_get_info(self._h, C.byref(self._info)))
 
+    def _adopt(self, handle) -> None:
+        """Take ownership of a segments handle built elsewhere (a loaded file)."""
+        if self._h:
+            capi.tnlb_segments_destroy(self._h)
+        self._h = C.c_void_p(handle)
+        check(capi.tnlb_segments_get_info(self._h, C.byref(self._info)))
+        self.organization = self._info.organization
+
     def getSegmentCount(self) -> int:
         return self._info.segments
 
@@ -369,6 +377,46 @@ class SparseMatrix:
             return _host_csr_to_numpy(h)
         finally:
             capi.tnlb_host_csr_free(C.byref(h))
+
+    # -- files -----------------------------------------------------------------
+    def save(self, fileName) -> None:
+        """SparseMatrix::save (SparseMatrix.hpp:632-643): TNL's binary matrix
+        file, byte for byte what the reference writes for this matrix."""
+        check(capi.tnlb_matrix_save(str(fileName).encode(), self.segments.handle, _real_code(self.real),
+                                    self.columnIndexes.data_ptr() if self.columnIndexes.numel() else None,
+                                    self.values.data_ptr() if self.values.numel() else None, self.rows,
+                                    self.columns, int(self.symmetric)))
+
+    def getSerializationType(self) -> str:
+        """The matrix type string of a TNL file (SparseMatrixBase.hpp:46-53)."""
+        org = "RowMajorOrder" if self.segments.organization == RowMajorOrder else "ColumnMajorOrder"
+        seg = {CSR: "CSR< int >", AdaptiveCSR: "AdaptiveCSR< int >", Ellpack: f"Ellpack< int, {org}, 32 >",
+               SlicedEllpack: f"SlicedEllpack< int, {org}, 32 >", ChunkedEllpack: f"ChunkedEllpack< int, {org} >",
+               BiEllpack: f"BiEllpack< int, {org}, 32 >"}[self.segments_cls]
+        real = "double" if self.real == torch.float64 else "float"
+        kind = "Symmetric" if self.symmetric else "General"
+        return (f"Matrices::SparseMatrix< {real}, {seg}, [any_device], int, {kind}, [any_allocator], "
+                "[any_allocator] >")
+
+    def load(self, fileName) -> "SparseMatrix":
+        """SparseMatrix::load (SparseMatrix.hpp:646-694): the file's type must
+        be this matrix's type, else the reference's FileDeserializationError
+        message is raised (as RuntimeError); the segments come from the
+        stored metadata."""
+        info = capi.MatrixFileInfo()
+        check(capi.tnlb_matrix_file_info_read(str(fileName).encode(), C.byref(info)))
+        found, expected = info.type.decode(), self.getSerializationType()
+        if found != expected:
+            raise RuntimeError(f"{fileName}: object type does not match (expected {expected}, found {found}).")
+        cols = torch.empty(max(info.storage, 1), dtype=torch.int32, device="cuda")
+        vals = torch.empty(max(info.storage, 1), dtype=self.real, device="cuda")
+        h = C.c_void_p()
+        check(capi.tnlb_matrix_load(str(fileName).encode(), C.byref(h), cols.data_ptr(), vals.data_ptr(),
+                                    max(info.storage, 1)))
+        self.segments._adopt(h.value)
+        self.rows, self.columns = int(info.rows), int(info.columns)
+        self.columnIndexes, self.values = cols[:info.storage], vals[:info.storage]
+        return self
 
     def getTransposition(self, matrixMultiplicator: float = 1.0, segments=None) -> "SparseMatrix":
         """B = matrixMultiplicator * A^T as a new matrix (SparseMatrix::getTransposition,

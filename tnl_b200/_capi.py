@@ -72,6 +72,11 @@ class HostCSR(C.Structure):
                 ("cols", C.POINTER(C.c_int32)), ("values", C.POINTER(C.c_double))]
 
 
+class MatrixFileInfo(C.Structure):
+    _fields_ = [("format", C.c_int32), ("organization", C.c_int32), ("real", C.c_int32), ("symmetric", C.c_int32),
+                ("rows", C.c_int64), ("columns", C.c_int64), ("storage", C.c_int64), ("type", C.c_char * 512)]
+
+
 class SolveResult(C.Structure):
     _fields_ = [("converged", C.c_int32), ("iterations", C.c_int32), ("residue", C.c_double),
                 ("status_detail", C.c_int32), ("reserved", C.c_int32)]
@@ -118,6 +123,9 @@ tnlb_solve = _sig("tnlb_solve", [C.c_int, C.c_int, C.POINTER(SolverParams), _p, 
 tnlb_true_residual = _sig("tnlb_true_residual", [_p, C.c_int, _p, _p, _p, _p, _p, C.POINTER(_f64)])
 tnlb_solve_mixed = _sig("tnlb_solve_mixed", [C.POINTER(SolverParams), _p, _p, _p, _p, _p, _f64, _i32, C.c_int,
                                              C.c_int, _p, _p, C.POINTER(SolveResult), C.POINTER(_i32)])
+tnlb_matrix_save = _sig("tnlb_matrix_save", [C.c_char_p, _p, C.c_int, _p, _p, _i32, _i32, _i32])
+tnlb_matrix_file_info_read = _sig("tnlb_matrix_file_info_read", [C.c_char_p, C.POINTER(MatrixFileInfo)])
+tnlb_matrix_load = _sig("tnlb_matrix_load", [C.c_char_p, C.POINTER(_p), _p, _p, _i64])
 tnlb_matrix_transpose_rowptr = _sig("tnlb_matrix_transpose_rowptr", [_p, _p, _i32, _p, C.POINTER(_i64), _p])
 tnlb_matrix_transpose_fill = _sig("tnlb_matrix_transpose_fill", [_p, C.c_int, _p, _p, _i32, _f64, _p, _p, _p])
 tnlb_solve_mixed_reliable = _sig("tnlb_solve_mixed_reliable", [C.POINTER(SolverParams), _p, _p, _p, _p, _p, _f64,
