@@ -490,6 +490,47 @@ using ILU0 = PreconditionerBase<Matrix, TNLB_PRECOND_ILU0>;
 template <typename Matrix>
 using FSAI = PreconditionerBase<Matrix, TNLB_PRECOND_FSAI>;
 
+// Preconditioners::ILUT (ILUT.h, ILUT.hpp:27-258): factorised on the host
+// with the reference's arithmetic and selection, applied on the GPU.  Setup
+// keys "ilut-p" (default 0) and "ilut-threshold" (default 1e-4).
+template <typename Matrix>
+class ILUT {
+public:
+   using MatrixPointer = std::shared_ptr<const Matrix>;
+   ~ILUT() { tnlb_precond_destroy(p_); }
+   bool setup(const std::map<std::string, std::string>& prm, const std::string& prefix = "")
+   {
+      auto it = prm.find(prefix + "ilut-p");
+      if (it != prm.end()) ilut_p_ = std::stoi(it->second);
+      it = prm.find(prefix + "ilut-threshold");
+      if (it != prm.end()) tau_ = std::stod(it->second);
+      return true;
+   }
+   void update(const MatrixPointer& m)
+   {
+      if (m->getRows() == 0) throw std::invalid_argument("ILUT::update: the matrix is empty");
+      if (m->getRows() != m->getColumns()) throw std::invalid_argument("ILUT::update: matrix must be square");
+      tnlb_precond_destroy(p_);
+      p_ = nullptr;
+      tnlb::check(tnlb_precond_create_ilut(m->segments(), tnlb::real_code<typename Matrix::RealType>(),
+                                           m->getColumnIndexes().getData(), m->getValues().getData(), ilut_p_, tau_,
+                                           nullptr, &p_));
+      matrix_ = m;
+   }
+   template <typename V1, typename V2>
+   void solve(const V1& b, V2& x) const
+   {
+      tnlb::check(tnlb_precond_solve(p_, b.getData(), x.getData(), nullptr));
+   }
+   const tnlb_precond* handle() const { return p_; }
+
+private:
+   tnlb_precond* p_ = nullptr;
+   MatrixPointer matrix_;
+   int ilut_p_ = 0;
+   double tau_ = 1e-4;
+};
+
 }  // namespace Preconditioners
 
 template <typename Matrix, tnlb_solver_kind Kind>

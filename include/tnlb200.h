@@ -384,7 +384,8 @@ typedef enum {
    TNLB_PRECOND_JACOBI = 1,
    TNLB_PRECOND_ILU0 = 2,
    TNLB_PRECOND_FSAI = 3,
-   TNLB_PRECOND_FSAI2 = 4
+   TNLB_PRECOND_FSAI2 = 4,
+   TNLB_PRECOND_ILUT = 5
 } tnlb_precond_kind;
 
 typedef struct tnlb_precond tnlb_precond;
@@ -491,6 +492,17 @@ tnlb_status tnlb_solve_mixed_reliable(const tnlb_solver_params* params, const tn
 tnlb_status tnlb_precond_create(tnlb_precond_kind kind, const tnlb_segments* seg, tnlb_real real,
                                 const int32_t* d_cols, const void* d_values, tnlb_stream stream,
                                 tnlb_precond** out);
+
+/* Build an ILUT preconditioner (Preconditioners/ILUT.h, ILUT.hpp:27-258; the
+ * reference has it on the host only): dual threshold -- entries below
+ * tau * ||A_i|| dropped, at most (stored entries of A_i left of / from the
+ * diagonal) + p kept per row in L / U -- factorised on the host with the
+ * reference's arithmetic and selection, applied on the GPU by the
+ * level-scheduled triangular solves of ILU0.  Setup keys "ilut-p"
+ * (default 0) and "ilut-threshold" (default 1e-4).  Blocks until built. */
+tnlb_status tnlb_precond_create_ilut(const tnlb_segments* seg, tnlb_real real, const int32_t* d_cols,
+                                     const void* d_values, int32_t p, double threshold, tnlb_stream stream,
+                                     tnlb_precond** out);
 
 /* x = M^{-1} b -- Preconditioner::solve (Diagonal.hpp:40-43,
  * ILU0.hpp:121-140).  Synchronous. */

@@ -122,6 +122,8 @@ class Oracle:
             ("orc_idrs_shadow", [i32, i32, p], None),
             ("orc_true_residual", [i32, p, p, p, p, p], f64),
             ("orc_pcg_reliable", [i32, p, p, p, C.c_int, p, p, f64, f64, i32, C.c_int, p, p, p], C.c_int),
+            ("orc_ilut_factor", [i32, p, p, p, i32, f64, p, p, p], C.c_long),
+            ("orc_lu_apply", [i32, p, p, p, p, p], None),
             ("orc_ilu0_factor", [i32, p, p, p, p, p, p, p, p, p], C.c_int),
             ("orc_prec_apply", [i32, p, p, p, C.c_int, p, p], C.c_int),
         ]:
@@ -295,6 +297,29 @@ class Oracle:
         return {"x": x, "converged": ok == 1, "status": ok, "iterations": S.iterations, "residue": S.residue,
                 "history": hist}
 
+    def ilut_factor(self, A, p=0, tau=1e-4):
+        """The ILUT factors (ILUT.hpp:27-258 restated) as one CSR: row i holds
+        its L entries then its U entries.  Returns (rowptr, cols, vals)."""
+        rowptr, cols, vals = _i32(A.rowptr), _i32(A.cols), np.ascontiguousarray(A.vals, np.float64)
+        nnz = self.L.orc_ilut_factor(A.n, rowptr.ctypes.data, cols.ctypes.data, vals.ctypes.data, p, tau, None, None,
+                                     None)
+        frp = np.zeros(A.n + 1, np.int32)
+        fc = np.zeros(max(nnz, 1), np.int32)
+        fv = np.zeros(max(nnz, 1), np.float64)
+        self.L.orc_ilut_factor(A.n, rowptr.ctypes.data, cols.ctypes.data, vals.ctypes.data, p, tau, frp.ctypes.data,
+                               fc.ctypes.data, fv.ctypes.data)
+        return frp, fc[:nnz], fv[:nnz]
+
+    def lu_apply(self, frp, fc, fv, b):
+        """x = U^-1 L^-1 b for factors in the layout of ilut_factor."""
+        frp, fc = _i32(frp), _i32(fc)
+        fv = np.ascontiguousarray(fv, np.float64)
+        b = np.ascontiguousarray(b, np.float64)
+        x = np.zeros(len(frp) - 1)
+        self.L.orc_lu_apply(len(frp) - 1, frp.ctypes.data, fc.ctypes.data, fv.ctypes.data, b.ctypes.data,
+                            x.ctypes.data)
+        return x
+
     @staticmethod
     def transpose(A, mult=1.0, real=np.float64):
         """getTransposition (Matrices/SparseMatrix.hpp:495-551) restated:
@@ -379,6 +404,10 @@ class Reference:
             ("ref_spmv_transposed_f64", [i32, i32, p, p, p, p, p, f64, f64, i32, i32], None),
             ("ref_transpose_f64", [i32, i32, p, p, p, f64, p, p, p], C.c_long),
             ("ref_save", [C.c_int, C.c_int, C.c_int, i32, i32, p, p, p, C.c_char_p], C.c_int),
+            ("ref_ilut_factor", [i32, p, p, p, i32, f64, C.POINTER(C.c_long), C.POINTER(C.c_long), p, p, p, p, p, p],
+             C.c_int),
+            ("ref_ilut_apply", [i32, p, p, p, i32, f64, p, p], C.c_int),
+            ("ref_set_ilut", [i32, f64], None),
             ("ref_prec_apply", [i32, p, p, p, i32, p, p], C.c_int),
             ("ref_omp_threads", [], C.c_int),
             ("ref_set_threads", [C.c_int], None),
@@ -518,6 +547,32 @@ class Reference:
         self.L.ref_spmv_transposed_f64(A.n, A.ncols, rowptr.ctypes.data, cols.ctypes.data, vals.ctypes.data,
                                        x.ctypes.data, y.ctypes.data, alpha, beta, begin, end)
         return y
+
+    def ilut_factor(self, A, p=0, tau=1e-4):
+        """The reference's ILUT::update: (L rowptr, cols, vals), (U rowptr,
+        cols, vals) with their padding; U's rows stored reversed."""
+        rowptr, cols = _i32(A.rowptr), _i32(A.cols)
+        vals = np.ascontiguousarray(A.vals, np.float64)
+        ln, un = C.c_long(), C.c_long()
+        args = (A.n, rowptr.ctypes.data, cols.ctypes.data, vals.ctypes.data, p, tau, C.byref(ln), C.byref(un))
+        if self.L.ref_ilut_factor(*args, None, None, None, None, None, None) != 0:
+            raise RuntimeError("reference ILUT failed")
+        lrp, urp = np.zeros(A.n + 1, np.int32), np.zeros(A.n + 1, np.int32)
+        lc, uc = np.zeros(max(ln.value, 1), np.int32), np.zeros(max(un.value, 1), np.int32)
+        lv, uv = np.zeros(max(ln.value, 1)), np.zeros(max(un.value, 1))
+        self.L.ref_ilut_factor(*args, lrp.ctypes.data, lc.ctypes.data, lv.ctypes.data, urp.ctypes.data,
+                               uc.ctypes.data, uv.ctypes.data)
+        return (lrp, lc[:ln.value], lv[:ln.value]), (urp, uc[:un.value], uv[:un.value])
+
+    def ilut_apply(self, A, b, p=0, tau=1e-4):
+        rowptr, cols = _i32(A.rowptr), _i32(A.cols)
+        vals = np.ascontiguousarray(A.vals, np.float64)
+        b = np.ascontiguousarray(b, np.float64)
+        x = np.zeros(A.n)
+        if self.L.ref_ilut_apply(A.n, rowptr.ctypes.data, cols.ctypes.data, vals.ctypes.data, p, tau, b.ctypes.data,
+                                 x.ctypes.data) != 0:
+            raise RuntimeError("reference ILUT failed")
+        return x
 
     def save(self, fmt: int, A, path, colmajor=True, real64=True) -> None:
         """The reference's SparseMatrix::save of A in format `fmt` (built by

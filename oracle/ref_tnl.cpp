@@ -37,6 +37,7 @@
 #include <TNL/Solvers/Linear/GMRES.h>
 #include <TNL/Solvers/Linear/Preconditioners/Diagonal.h>
 #include <TNL/Solvers/Linear/Preconditioners/ILU0.h>
+#include <TNL/Solvers/Linear/Preconditioners/ILUT.h>
 
 using namespace TNL;
 namespace Seg = TNL::Algorithms::Segments;
@@ -62,6 +63,29 @@ using BiellC = Seg::BiEllpack< D, I, A, Seg::ColumnMajorOrder, 32 >;
 
 template< typename Real, template< typename, typename, typename > class S >
 using Mat = Matrices::SparseMatrix< Real, Host, int, Matrices::GeneralMatrix, S >;
+
+// ILUT's factors are protected members; a derived class exposes them.
+template< typename M >
+struct ILUTAccess : public Solvers::Linear::Preconditioners::ILUT< M >
+{
+   using Base = Solvers::Linear::Preconditioners::ILUT< M >;
+   using Base::L;
+   using Base::U;
+};
+
+// ILUT parameters of the solver driver (precond 3): ilut-p, ilut-threshold.
+static int g_ilutP = 0;
+static double g_ilutTau = 1e-4;
+
+template< typename M >
+static void
+setupILUT( Solvers::Linear::Preconditioners::ILUT< M >& P, int p, double tau )
+{
+   Config::ParameterContainer prm;
+   prm.addParameter< int >( "ilut-p", p );
+   prm.addParameter< double >( "ilut-threshold", tau );
+   P.setup( prm );
+}
 
 static IVec
 toVec( const int* p, int n )
@@ -574,7 +598,14 @@ ref_solve( int solver,
       (void) sizeof( P* );
       std::shared_ptr< Solvers::Linear::Preconditioners::Diagonal< M > > jac;
       std::shared_ptr< Solvers::Linear::Preconditioners::ILU0< M > > ilu;
+      std::shared_ptr< Solvers::Linear::Preconditioners::ILUT< M > > ilut;
       auto t0 = std::chrono::steady_clock::now();
+      if( precond == 3 ) {
+         ilut = std::make_shared< Solvers::Linear::Preconditioners::ILUT< M > >();
+         setupILUT( *ilut, g_ilutP, g_ilutTau );
+         ilut->update( A );
+         S.setPreconditioner( ilut );
+      }
       if( precond == 1 ) {
          jac = std::make_shared< Solvers::Linear::Preconditioners::Diagonal< M > >();
          jac->update( A );
@@ -728,6 +759,78 @@ ref_prec_apply( int n, const int* rowptr, const int* cols, const double* vals, i
    for( int i = 0; i < n; i++ )
       x[ i ] = xv[ i ];
    return 0;
+}
+
+void
+ref_set_ilut( int p, double tau )
+{
+   g_ilutP = p;
+   g_ilutTau = tau;
+}
+
+// ILUT::update on a CSR matrix: the factors L (unit lower, rows in order)
+// and U (rows stored reversed: row N-1-i holds row i, its first entry the
+// pivot), both CSR with their padding.  A first call with null outputs
+// returns the sizes in lnnz / unnz.  Returns 0, or -1 on an exception.
+int
+ref_ilut_factor( int n, const int* rowptr, const int* cols, const double* vals, int p, double tau, long* lnnz,
+                 long* unnz, int* lrp, int* lc, double* lv, int* urp, int* uc, double* uv )
+{
+   try {
+      using M = Mat< double, Seg::CSR >;
+      auto A = std::make_shared< M >();
+      makeCSR( *A, n, n, rowptr, cols, vals );
+      ILUTAccess< M > P;
+      setupILUT( P, p, tau );
+      P.update( A );
+      const auto& lo = P.L.getSegments().getOffsets();
+      const auto& uo = P.U.getSegments().getOffsets();
+      *lnnz = lo[ n ];
+      *unnz = uo[ n ];
+      if( lrp ) {
+         for( int i = 0; i <= n; i++ ) {
+            lrp[ i ] = lo[ i ];
+            urp[ i ] = uo[ i ];
+         }
+         for( long k = 0; k < *lnnz; k++ ) {
+            lc[ k ] = P.L.getColumnIndexes()[ k ];
+            lv[ k ] = P.L.getValues()[ k ];
+         }
+         for( long k = 0; k < *unnz; k++ ) {
+            uc[ k ] = P.U.getColumnIndexes()[ k ];
+            uv[ k ] = P.U.getValues()[ k ];
+         }
+      }
+      return 0;
+   }
+   catch( ... ) {
+      return -1;
+   }
+}
+
+// ILUT::update then ILUT::solve once: x = M^{-1} b.
+int
+ref_ilut_apply( int n, const int* rowptr, const int* cols, const double* vals, int p, double tau, const double* b,
+                double* x )
+{
+   try {
+      using M = Mat< double, Seg::CSR >;
+      auto A = std::make_shared< M >();
+      makeCSR( *A, n, n, rowptr, cols, vals );
+      Solvers::Linear::Preconditioners::ILUT< M > P;
+      setupILUT( P, p, tau );
+      P.update( A );
+      Containers::Vector< double, Host, int > bv( n ), xv( n );
+      for( int i = 0; i < n; i++ )
+         bv[ i ] = b[ i ];
+      P.solve( bv, xv );
+      for( int i = 0; i < n; i++ )
+         x[ i ] = xv[ i ];
+      return 0;
+   }
+   catch( ... ) {
+      return -1;
+   }
 }
 
 void

@@ -335,3 +335,37 @@ def test_transposition_matches_reference(oracle, reference):
                 assert np.array_equal(tv, rv)
     finally:
         reference.set_threads(t0)
+
+
+def _ilut_reference_as_combined(L, U, n):
+    """The reference's separate L and (row-reversed) U, padding dropped, as
+    one CSR with row i = L_i then U_i (the restatement's layout)."""
+    (lrp, lc, lv), (urp, uc, uv) = L, U
+    rp, cols, vals = [0], [], []
+    for i in range(n):
+        for q in range(lrp[i], lrp[i + 1]):
+            if lc[q] >= 0:
+                cols.append(lc[q])
+                vals.append(lv[q])
+        r = n - 1 - i
+        for q in range(urp[r], urp[r + 1]):
+            if uc[q] >= 0:
+                cols.append(uc[q])
+                vals.append(uv[q])
+        rp.append(len(cols))
+    return np.array(rp, np.int32), np.array(cols, np.int32), np.array(vals)
+
+
+@pytest.mark.parametrize("p,tau", [(0, 1e-4), (2, 1e-3), (5, 1e-2), (1, 0.0)])
+def test_ilut_restatement_matches_reference(oracle, reference, p, tau):
+    """ILUT factors of the restatement equal the reference's ILUT::update bit
+    for bit (pattern, order, values), and one application equals its solve,
+    on a Laplacian (many equal magnitudes: heap tie order), a
+    diffusion matrix and a nonsymmetric convection-diffusion matrix."""
+    for A in (g.laplacian_2d(12), g.diffusion_2d(14, 0.1, 2.0, 5), g.convection_diffusion_3d(6)):
+        frp, fc, fv = oracle.ilut_factor(A, p, tau)
+        rrp, rc, rv = _ilut_reference_as_combined(*reference.ilut_factor(A, p, tau), A.n)
+        assert np.array_equal(frp, rrp) and np.array_equal(fc, rc)
+        assert np.array_equal(fv, rv)
+        b = g.uniform_vector(A.n, 3)
+        assert np.array_equal(oracle.lu_apply(frp, fc, fv, b), reference.ilut_apply(A, b, p, tau))

@@ -435,3 +435,57 @@ def test_more_krylov_match_reference_golden(golden):
             assert abs(it - ref["iterations"]) <= slack, (key, it, ref["iterations"])
             xr = golden.get(f"solve/{key}/x")
             assert np.allclose(x, xr, rtol=1e-5, atol=1e-6 * np.abs(xr).max()), key
+
+
+@pytest.mark.parametrize("p,tau", [(0, 1e-4), (3, 1e-3)])
+def test_ilut_factors_and_application_bit_exact(oracle, p, tau):
+    """ILUT (the reference's is host-only): the factors computed by the
+    library equal the restatement (pinned to the reference) bit for bit, and
+    one application on the GPU equals the restatement's triangular solves."""
+    from tnl_b200 import generators as g
+
+    t = tnl()
+    for A in (g.laplacian_2d(30), g.diffusion_2d(25, 0.1, 1.5, 4), g.convection_diffusion_3d(8)):
+        M = t.SparseMatrix(t.CSR, torch.float64).assign(A.rowptr, A.cols, A.vals)
+        P = t.ILUT()
+        P.setup({"ilut-p": p, "ilut-threshold": tau})
+        P.update(M)
+        rp, cols, vals = P.factors()
+        orp, oc, ov = oracle.ilut_factor(A, p, tau)
+        assert np.array_equal(rp, orp) and np.array_equal(cols, oc) and np.array_equal(vals, ov)
+        b = g.uniform_vector(A.n, 7)
+        x = torch.zeros(A.n, dtype=torch.float64, device="cuda")
+        P.solve(torch.tensor(b, device="cuda"), x)
+        assert np.array_equal(x.cpu().numpy(), oracle.lu_apply(orp, oc, ov, b))
+
+
+def test_gmres_with_ilut_matches_reference(reference):
+    """GMRES(30) MGSR with ILUT on the convection-diffusion matrix: the
+    iteration count of the reference's own Host solve (one thread), and the
+    tolerance reached on the true residual."""
+    from tnl_b200 import generators as g
+
+    t = tnl()
+    A = g.convection_diffusion_3d(12)
+    b = g.uniform_vector(A.n, 1)
+    t0 = reference.threads()
+    reference.set_threads(1)
+    try:
+        reference.L.ref_set_ilut(1, 1e-3)
+        o = reference.solve("gmres", A, b, precond=3, tol=1e-8, gmres_m=30, gmres_variant=3)
+    finally:
+        reference.set_threads(t0)
+    M = t.SparseMatrix(t.CSR, torch.float64).assign(A.rowptr, A.cols, A.vals)
+    S = t.GMRES()
+    S.setMatrix(M)
+    S.setup({"convergence-residue": 1e-8, "max-iterations": 5000, "gmres-variant": "MGSR",
+             "gmres-restarting-min": 30, "gmres-restarting-max": 30})
+    P = t.ILUT()
+    P.setup({"ilut-p": 1, "ilut-threshold": 1e-3})
+    P.update(M)
+    S.setPreconditioner(P)
+    bs = torch.tensor(b, device="cuda")
+    x = torch.zeros(A.n, dtype=torch.float64, device="cuda")
+    assert S.solve(bs, x) and o["converged"]
+    assert abs(S.getIterations() - o["iterations"]) <= 2, (S.getIterations(), o["iterations"])
+    assert t.true_residual(M, bs, x) < 1e-7

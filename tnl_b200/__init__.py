@@ -32,7 +32,7 @@ __all__ = [
     "CSR", "Ellpack", "SlicedEllpack", "ChunkedEllpack", "BiEllpack", "AdaptiveCSR", "SparseMatrix",
     "LaunchConfiguration", "ColumnMajorOrder", "RowMajorOrder", "CSRMatrix", "check", "BackendRuntimeError",
     "CG", "BICGStab", "GMRES", "FGMRES", "TFQMR", "BICGStabL", "IDRs", "Diagonal", "ILU0", "FSAI", "FSAI2",
-    "solve_mixed", "solve_mixed_reliable", "true_residual", "read_mtx", "write_mtx",
+    "solve_mixed", "solve_mixed_reliable", "true_residual", "ILUT", "read_mtx", "write_mtx",
 ]
 
 ColumnMajorOrder = capi.COLUMN_MAJOR
@@ -574,6 +574,54 @@ class FSAI(_Preconditioner):
     triangle of A's pattern with Kolotilina-Yeremin values (no counterpart in
     the reference)."""
     KIND = capi.PRECOND_FSAI
+
+
+class ILUT(_Preconditioner):
+    """Solvers::Linear::Preconditioners::ILUT (ILUT.hpp:27-258): dual-threshold
+    ILU factorised on the host with the reference's arithmetic and selection
+    (the reference has no CUDA ILUT), applied on the GPU by the level-
+    scheduled triangular solves.  Setup keys "ilut-p" (default 0) and
+    "ilut-threshold" (default 1e-4)."""
+    KIND = capi.PRECOND_ILUT
+
+    def __init__(self):
+        super().__init__()
+        self.p = 0
+        self.tau = 1e-4
+
+    def setup(self, parameters: dict, prefix: str = "") -> bool:
+        if prefix + "ilut-p" in parameters:
+            self.p = int(parameters[prefix + "ilut-p"])
+        if prefix + "ilut-threshold" in parameters:
+            self.tau = float(parameters[prefix + "ilut-threshold"])
+        return True
+
+    def update(self, matrix: SparseMatrix) -> None:
+        if matrix.getRows() == 0:
+            raise ValueError("ILUT::update: the matrix is empty")
+        if matrix.getRows() != matrix.getColumns():
+            raise ValueError("ILUT::update: matrix must be square")
+        if self._h:
+            capi.tnlb_precond_destroy(self._h)
+            self._h = C.c_void_p()
+        h = C.c_void_p()
+        check(capi.tnlb_precond_create_ilut(matrix.segments.handle, _real_code(matrix.real),
+                                            matrix.columnIndexes.data_ptr(), matrix.values.data_ptr(), self.p,
+                                            self.tau, _stream(), C.byref(h)))
+        self._h = h
+        self.matrix = matrix
+
+    def factors(self):
+        """The factors as one CSR (rowptr, cols, values): row i holds its L
+        entries (columns < i, unit diagonal implied) then its U entries, the
+        first U entry the pivot."""
+        n = self.matrix.getRows()
+        cap = self.matrix.getValues().numel() * (3 + 2 * self.p) + 2 * n * (self.p + 1) + 16
+        rp = np.zeros(n + 1, np.int32)
+        cols = np.zeros(cap, np.int32)
+        vals = np.zeros(cap, np.float64 if self.matrix.real == torch.float64 else np.float32)
+        check(capi.tnlb_precond_read_factor(self._h, 0, rp.ctypes.data, cols.ctypes.data, vals.ctypes.data, cap))
+        return rp, cols[:rp[-1]], vals[:rp[-1]]
 
 
 class ILU0(_Preconditioner):

@@ -83,7 +83,7 @@ class SolveResult(C.Structure):
 
 
 SOLVER_CG, SOLVER_BICGSTAB, SOLVER_GMRES, SOLVER_FGMRES, SOLVER_TFQMR, SOLVER_BICGSTABL, SOLVER_IDRS = range(7)
-PRECOND_NONE, PRECOND_JACOBI, PRECOND_ILU0, PRECOND_FSAI, PRECOND_FSAI2 = range(5)
+PRECOND_NONE, PRECOND_JACOBI, PRECOND_ILU0, PRECOND_FSAI, PRECOND_FSAI2, PRECOND_ILUT = range(6)
 GMRES_CGS, GMRES_CGSR, GMRES_MGS, GMRES_MGSR, GMRES_CWY = range(5)
 
 _p = C.c_void_p
@@ -131,6 +131,7 @@ tnlb_matrix_transpose_fill = _sig("tnlb_matrix_transpose_fill", [_p, C.c_int, _p
 tnlb_solve_mixed_reliable = _sig("tnlb_solve_mixed_reliable", [C.POINTER(SolverParams), _p, _p, _p, _p, _p, _f64,
                                                                C.c_int, C.c_int, _p, _p, C.POINTER(SolveResult),
                                                                C.POINTER(_i32)])
+tnlb_precond_create_ilut = _sig("tnlb_precond_create_ilut", [_p, C.c_int, _p, _p, _i32, _f64, _p, C.POINTER(_p)])
 tnlb_precond_create = _sig("tnlb_precond_create", [C.c_int, _p, C.c_int, _p, _p, _p, C.POINTER(_p)])
 tnlb_precond_solve = _sig("tnlb_precond_solve", [_p, _p, _p, _p])
 tnlb_precond_destroy = _sig("tnlb_precond_destroy", [_p])

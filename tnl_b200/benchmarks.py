@@ -303,11 +303,12 @@ SOLVER_SWEEP = [
     ("GMRES(30) MGSR", "gmres", "jacobi", {"gmres-variant": "MGSR"}),
     ("GMRES(30) CWY", "gmres", "jacobi", {"gmres-variant": "CWY"}),
     ("GMRES(30) MGSR", "gmres", "ilu0", {"gmres-variant": "MGSR"}),
+    ("GMRES(30) MGSR", "gmres", "ilut", {"gmres-variant": "MGSR"}),
 ]
 
 
 def bench_solver_sweep(problem: str, N: int, tol: float = 1e-8, max_iterations: int = 100000, out=sys.stdout):
-    """Every Krylov solver with Jacobi (and GMRES with ILU(0)) on one problem,
+    """Every Krylov solver with Jacobi (and GMRES with ILU(0) and ILUT) on one problem,
     as the reference's linear-solver benchmark does: iterations, device time of
     the solve call, set-up time of the preconditioner, true FP64 residual."""
     import tnl_b200 as t
@@ -324,7 +325,7 @@ def bench_solver_sweep(problem: str, N: int, tol: float = 1e-8, max_iterations: 
     b = torch.tensor(g.uniform_vector(n, 1), device="cuda")
     classes = {"cg": t.CG, "bicgstab": t.BICGStab, "tfqmr": t.TFQMR, "bicgstabl": t.BICGStabL, "idrs": t.IDRs,
                "gmres": t.GMRES}
-    precs = {"jacobi": t.Diagonal, "ilu0": t.ILU0}
+    precs = {"jacobi": t.Diagonal, "ilu0": t.ILU0, "ilut": t.ILUT}
     for label, kind, pname, keys in SOLVER_SWEEP:
         if kind == "cg" and problem == "convection_diffusion":
             continue  # nonsymmetric

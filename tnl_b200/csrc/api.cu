@@ -399,6 +399,27 @@ tnlb_status tnlb_precond_create(tnlb_precond_kind kind, const tnlb_segments* seg
    return tnlb::precond_create(kind, seg, real, d_cols, d_values, (cudaStream_t)stream, out);
 }
 
+tnlb_status tnlb_precond_create_ilut(const tnlb_segments* seg, tnlb_real real, const int32_t* d_cols,
+                                     const void* d_values, int32_t p, double threshold, tnlb_stream stream,
+                                     tnlb_precond** out)
+{
+   clear_error();
+   TNLB_REQUIRE(seg && out, TNLB_ERR_INVALID_ARGUMENT, "null argument");
+   TNLB_REQUIRE(real == TNLB_F32 || real == TNLB_F64, TNLB_ERR_INVALID_ARGUMENT, "unknown real type");
+   *out = nullptr;
+   auto* P = new tnlb_precond();
+   P->kind = TNLB_PRECOND_ILUT;
+   P->real = real;
+   P->n = seg->n;
+   tnlb_status s = tnlb::ilut_create(seg, real, d_cols, d_values, p, threshold, (cudaStream_t)stream, &P->ilu);
+   if (s != TNLB_OK) {
+      delete P;
+      return s;
+   }
+   *out = P;
+   return TNLB_OK;
+}
+
 tnlb_status tnlb_precond_solve(const tnlb_precond* precond, const void* d_b, void* d_x, tnlb_stream stream)
 {
    clear_error();
@@ -411,7 +432,11 @@ tnlb_status tnlb_precond_read_factor(const tnlb_precond* precond, int32_t which,
 {
    clear_error();
    TNLB_REQUIRE(precond && h_rowptr && h_cols && h_values, TNLB_ERR_INVALID_ARGUMENT, "null argument");
-   TNLB_REQUIRE(precond->fsai != nullptr, TNLB_ERR_INVALID_ARGUMENT, "not an FSAI preconditioner");
+   if (precond->ilu) {  // ILU(0) / ILUT: the factors as one CSR (L entries, then U from its pivot)
+      TNLB_REQUIRE(which == 0, TNLB_ERR_INVALID_ARGUMENT, "an ILU preconditioner has one factor array (which = 0)");
+      return tnlb::ilu0_read(precond->ilu, h_rowptr, h_cols, h_values, capacity, precond->real == TNLB_F64 ? 8 : 4);
+   }
+   TNLB_REQUIRE(precond->fsai != nullptr, TNLB_ERR_INVALID_ARGUMENT, "not an FSAI or ILU preconditioner");
    TNLB_REQUIRE(which == 0 || which == 1, TNLB_ERR_INVALID_ARGUMENT, "which must be 0 or 1");
    const Fsai* F = precond->fsai;
    const tnlb_segments* seg = which == 0 ? F->g : F->gt;

@@ -121,7 +121,7 @@ __global__ void k_upper_level(const int32_t* __restrict__ rows, int32_t count, c
    const int32_t u0 = ustart[i];
    Real xi = x[i];
    for (int32_t c = u0 + 1; c < uend[i]; c++) xi = sub_rn(xi, mul_rn(lu[c], x[cols[c]]));
-   x[i] = div_rn(xi, lu[u0]);
+   x[i] = div_rn(xi, u0 < uend[i] ? lu[u0] : Real(0));  // an empty U row: pivot 0, as a padding slot
 }
 
 // Runs of consecutive small levels in ONE block: the block walks the levels
@@ -162,7 +162,7 @@ __global__ void __launch_bounds__(kIluRunThreads)
          const int32_t u0 = ustart[i];
          Real xi = x[i];
          for (int32_t c = u0 + 1; c < uend[i]; c++) xi = sub_rn(xi, mul_rn(lu[c], x[cols[c]]));
-         x[i] = div_rn(xi, lu[u0]);
+         x[i] = div_rn(xi, u0 < uend[i] ? lu[u0] : Real(0));
       }
       __syncthreads();
    }
@@ -449,6 +449,10 @@ struct Ilu0 : Ilu0Base {
 };
 
 template <typename Real>
+tnlb_status analyze_t(Ilu0<Real>* P, const std::vector<int32_t>& rp, const std::vector<int32_t>& cols, bool factorize,
+                      cudaStream_t st);
+
+template <typename Real>
 tnlb_status create_t(const tnlb_segments* seg, const int32_t* cols_in, const Real* vals_in, cudaStream_t st,
                      Ilu0<Real>** out)
 {
@@ -470,6 +474,41 @@ tnlb_status create_t(const tnlb_segments* seg, const int32_t* cols_in, const Rea
    TNLB_CUDA_TRY(cudaMemcpyAsync(rp.data(), P->rp.ptr, sizeof(int32_t) * (n + 1), cudaMemcpyDeviceToHost, st));
    if (nnz) TNLB_CUDA_TRY(cudaMemcpyAsync(cols.data(), P->cols.ptr, sizeof(int32_t) * nnz, cudaMemcpyDeviceToHost, st));
    TNLB_CUDA_TRY(cudaStreamSynchronize(st));
+   TNLB_TRY_STATUS(analyze_t(P, rp, cols, true, st));
+   *out = P;
+   return TNLB_OK;
+}
+
+// Factors given on the host (ILUT): row i holds its L entries (columns < i)
+// then its U entries, the first U entry the pivot; the level analysis,
+// packing and solves are those of ILU(0).
+template <typename Real>
+tnlb_status create_from_factors_t(int32_t n, const std::vector<int32_t>& rp, const std::vector<int32_t>& cols,
+                                  const std::vector<Real>& lu, cudaStream_t st, Ilu0<Real>** out)
+{
+   auto* P = new Ilu0<Real>();
+   P->n = n;
+   const size_t nnz = (size_t)rp[n];
+   TNLB_TRY_STATUS(P->rp.alloc(sizeof(int32_t) * ((size_t)n + 1)));
+   TNLB_TRY_STATUS(P->cols.alloc(sizeof(int32_t) * (nnz ? nnz : 1)));
+   TNLB_TRY_STATUS(P->lu.alloc(sizeof(Real) * (nnz ? nnz : 1)));
+   TNLB_CUDA_TRY(cudaMemcpyAsync(P->rp.ptr, rp.data(), sizeof(int32_t) * ((size_t)n + 1), cudaMemcpyHostToDevice, st));
+   if (nnz) {
+      TNLB_CUDA_TRY(cudaMemcpyAsync(P->cols.ptr, cols.data(), sizeof(int32_t) * nnz, cudaMemcpyHostToDevice, st));
+      TNLB_CUDA_TRY(cudaMemcpyAsync(P->lu.ptr, lu.data(), sizeof(Real) * nnz, cudaMemcpyHostToDevice, st));
+   }
+   TNLB_TRY_STATUS(analyze_t(P, rp, cols, false, st));
+   *out = P;
+   return TNLB_OK;
+}
+
+// L/U split, dependency levels, level order and packed copies of the factors;
+// with `factorize`, the ILU(0) factorisation of P->lu in place first.
+template <typename Real>
+tnlb_status analyze_t(Ilu0<Real>* P, const std::vector<int32_t>& rp, const std::vector<int32_t>& cols, bool factorize,
+                      cudaStream_t st)
+{
+   const int32_t n = P->n;
    std::vector<int32_t> ls(n), us(n), ue(n), llev(n, 0), ulev(n, 0);
    int32_t lmax = 0, umax = 0;
    for (int32_t i = 0; i < n; i++) {
@@ -520,7 +559,7 @@ tnlb_status create_t(const tnlb_segments* seg, const int32_t* cols_in, const Rea
    TNLB_CUDA_TRY(cudaMemcpyAsync(P->duptr.ptr, P->uptr.data(), sizeof(int32_t) * P->uptr.size(), cudaMemcpyHostToDevice,
                                  st));
    // factorisation, level by level of L
-   for (size_t l = 0; l + 1 < P->lptr.size(); l++) {
+   for (size_t l = 0; factorize && l + 1 < P->lptr.size(); l++) {
       const int32_t c = P->lptr[l + 1] - P->lptr[l];
       k_factor_level<Real><<<(c + 127) / 128, 128, 0, st>>>(P->lrows.template as<int32_t>() + P->lptr[l], c, P->cols.template as<int32_t>(),
                                                            P->lu.template as<Real>(), P->lstart.template as<int32_t>(),
@@ -579,7 +618,6 @@ tnlb_status create_t(const tnlb_segments* seg, const int32_t* cols_in, const Rea
       P->ku = ku;
    }
    TNLB_CUDA_TRY(cudaStreamSynchronize(st));
-   *out = P;
    return TNLB_OK;
 }
 
@@ -597,6 +635,23 @@ tnlb_status ilu0_create(const tnlb_segments* seg, tnlb_real real, const int32_t*
    }
    Ilu0<float>* p = nullptr;
    tnlb_status s = create_t<float>(seg, cols, (const float*)vals, st, &p);
+   *out = static_cast<Ilu0Base*>(p);
+   return s;
+}
+
+tnlb_status ilu_from_factors(tnlb_real real, int32_t n, const std::vector<int32_t>& rp,
+                             const std::vector<int32_t>& cols, const void* lu, cudaStream_t st, void** out)
+{
+   if (real == TNLB_F64) {
+      Ilu0<double>* p = nullptr;
+      const double* v = static_cast<const double*>(lu);
+      tnlb_status s = create_from_factors_t<double>(n, rp, cols, std::vector<double>(v, v + rp[n]), st, &p);
+      *out = static_cast<Ilu0Base*>(p);
+      return s;
+   }
+   Ilu0<float>* p = nullptr;
+   const float* v = static_cast<const float*>(lu);
+   tnlb_status s = create_from_factors_t<float>(n, rp, cols, std::vector<float>(v, v + rp[n]), st, &p);
    *out = static_cast<Ilu0Base*>(p);
    return s;
 }

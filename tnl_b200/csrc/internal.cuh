@@ -1,6 +1,8 @@
 // internal.cuh -- shared definitions of libtnlb200 (not part of the public ABI).
 #pragma once
 
+#include <vector>
+
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -313,6 +315,12 @@ tnlb_status solve_mixed_reliable(const tnlb_segments* seg, const int32_t* cols, 
 tnlb_status ilu0_create(const tnlb_segments* seg, tnlb_real real, const int32_t* cols, const void* vals,
                         cudaStream_t st, void** out);
 tnlb_status ilu0_apply(void* ilu, const void* b, void* x, cudaStream_t st);
+// An ILU object over factors computed elsewhere (ILUT): host CSR whose row i
+// holds its L entries (columns < i) then its U entries (first = pivot).
+tnlb_status ilu_from_factors(tnlb_real real, int32_t n, const std::vector<int32_t>& rp,
+                             const std::vector<int32_t>& cols, const void* lu, cudaStream_t st, void** out);
+tnlb_status ilut_create(const tnlb_segments* seg, tnlb_real real, const int32_t* cols, const void* vals, int32_t p,
+                        double tau, cudaStream_t st, void** out);
 tnlb_status ilu0_read(void* ilu, int32_t* h_rowptr, int32_t* h_cols, void* h_vals, int64_t capacity, int real_bytes);
 void ilu0_destroy(void* ilu);
 tnlb_status fsai_create(const tnlb_segments* seg, tnlb_real real, const int32_t* cols, const void* vals,

@@ -527,7 +527,7 @@ struct Precond {
    // out = M^-1 in (`skip`: the solver's done flag, for kernels in graphs)
    tnlb_status apply(int64_t n, const Real* in, Real* out, cudaStream_t st, const int32_t* skip = nullptr) const
    {
-      if (kind == TNLB_PRECOND_ILU0) return ilu0_apply(obj->ilu, in, out, st);
+      if (kind == TNLB_PRECOND_ILU0 || kind == TNLB_PRECOND_ILUT) return ilu0_apply(obj->ilu, in, out, st);
       if (kind == TNLB_PRECOND_FSAI) return fsai_apply(obj->fsai, in, out, st, skip);
       k_jacobi<Real><<<vec_grid(n), kRedThreads, 0, st>>>(n, in, d(), out);
       TNLB_CHECK_LAUNCH();
@@ -1934,7 +1934,7 @@ tnlb_status solve_t(tnlb_solver_kind solver, const tnlb_precond* pobj, const tnl
    const Precond<Real> P = view<Real>(pobj);
    switch (solver) {
       case TNLB_SOLVER_CG:
-         if (P.kind == TNLB_PRECOND_ILU0) return pcg_general<Real>(c, P, prm, b, x, res);
+         if (P.kind == TNLB_PRECOND_ILU0 || P.kind == TNLB_PRECOND_ILUT) return pcg_general<Real>(c, P, prm, b, x, res);
          return cg_solve<Real>(c, P, prm, b, x, res);
       case TNLB_SOLVER_BICGSTAB: return bicgstab_solve<Real>(c, P, prm, b, x, res);
       case TNLB_SOLVER_GMRES: return gmres_solve<Real>(c, P, prm, b, x, res);
