@@ -455,13 +455,23 @@ __global__ void __launch_bounds__(kTileThreads, 5) k_csr_tile(const int32_t* __r
          v[j] = ld_stream_hint(vals + e, pol_stream);
       }
    }
+   // the first 32 row ends of the tile, loaded before the x gathers are
+   // issued so that both latencies overlap (the gathers need only c)
+   const bool row0 = lane < nrows;
+   int32_t e_end0 = 0, e_beg0 = 0;
+   if (row0) {
+      e_beg0 = rowptr[r0 + lane];
+      e_end0 = rowptr[r0 + lane + 1];
+   }
+#pragma unroll
+   for (int j = 0; j < kTileItems; j++) v[j] = c[j] >= 0 ? v[j] * ld_keep(x + c[j], pol_keep) : Real(0);
    if (lane < kTileItems) sm[lane] = 0u;
    __syncwarp();
    // rows ending in the tile: mark the last nonzero, or write a row that has
    // none here (empty, or all of it in earlier tiles)
    for (int32_t i = lane; i < nrows; i += 32) {
       const int32_t r = r0 + i;
-      const int32_t e_end = rowptr[r + 1], e_beg = rowptr[r];
+      const int32_t e_end = i == lane ? e_end0 : rowptr[r + 1], e_beg = i == lane ? e_beg0 : rowptr[r];
       if (e_end > k0 && e_end > e_beg) {
          const int32_t pos = e_end - k0 - 1;
          atomicOr(sm + (pos >> 5), 1u << (pos & 31));
@@ -470,8 +480,6 @@ __global__ void __launch_bounds__(kTileThreads, 5) k_csr_tile(const int32_t* __r
       else
          keep(y, r, Real(0), alpha, beta);
    }
-#pragma unroll
-   for (int j = 0; j < kTileItems; j++) v[j] = c[j] >= 0 ? v[j] * ld_keep(x + c[j], pol_keep) : Real(0);
    __syncwarp();
 
    // The open row's partial sum: `carry` (one value) plus, after steps with
