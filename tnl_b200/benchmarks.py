@@ -248,7 +248,7 @@ def bench_solvers(problem: str, N: int, weights: str | None, out=sys.stdout):
         # solve, both to a true residual below 1e-8
         t.solve_mixed_reliable(M, b, torch.zeros(n, dtype=torch.float64, device="cuda"), tol=1e-8, inner=inner,
                                max_iterations=20, vectors=vectors)
-        r, x, ms, times = _median_timed(_Run(lambda x: t.solve_mixed_reliable(M, b, x, tol=1e-8, delta=0.1,
+        r, x, ms, times = _median_timed(_Run(lambda x: t.solve_mixed_reliable(M, b, x, tol=1e-8, delta=0.3,
                                                                               inner=inner, vectors=vectors), n))
         rec = dict(base, method=name, converged=r["converged"], iterations=r["iterations"],
                    reliable_updates=r["reliable_updates"], solve_ms=ms, solve_ms_runs=times, setup_ms=setup_ms,
@@ -392,7 +392,7 @@ def bench_configs(which: str, out=sys.stdout):
         report("FP32-inner Jacobi-PCG in FP64 refinement", r["converged"], r["inner_iterations"], ms, 0.0, x,
                outer_iterations=r["outer_iterations"])
         x = torch.zeros(n, dtype=torch.float64, device="cuda")
-        r, ms = _timed(lambda: t.solve_mixed_reliable(M, b, x, tol=tol, delta=0.1, inner="jacobi"))
+        r, ms = _timed(lambda: t.solve_mixed_reliable(M, b, x, tol=tol, delta=0.3, inner="jacobi"))
         report("FP32 Jacobi-PCG with reliable FP64 updates", r["converged"], r["iterations"], ms, 0.0, x,
                reliable_updates=r["reliable_updates"])
         return
