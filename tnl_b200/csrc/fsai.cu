@@ -393,6 +393,19 @@ tnlb_status fsai_apply(const Fsai* F, const void* r, void* z, cudaStream_t st, c
 
 bool fsai_two_factor(const Fsai* F) { return F->two_factor; }
 
+FsaiView fsai_view(const Fsai* F)
+{
+   FsaiView v;
+   v.g = F->g;
+   v.gt = F->gt;
+   v.gcols = F->g_cols.as<int32_t>();
+   v.gtcols = F->gt_cols.as<int32_t>();
+   v.gvals = F->g_vals.ptr;
+   v.gtvals = F->gt_vals.ptr;
+   v.tmp = F->tmp.ptr;
+   return v;
+}
+
 bool fsai_dot_fusable(const Fsai* F) { return !F->two_factor && spmv_dot_fusable(F->g) && spmv_dot_fusable(F->gt); }
 
 // t = G r with (t, t) = (r, G^T G r) summed in the same kernel; z = G^T t

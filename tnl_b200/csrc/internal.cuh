@@ -286,6 +286,23 @@ tnlb_status spmv_dot_mixed(const tnlb_segments* seg, tnlb_real tv, tnlb_real tx,
 tnlb_status spmv_xpby_mixed(const tnlb_segments* seg, tnlb_real tv, tnlb_real tx, tnlb_real ty, const int32_t* cols,
                             const void* vals, const void* x, void* y, const double* num, const double* den,
                             cudaStream_t st, const int32_t* skip);
+// A short-row CSR matrix with 16-bit column offsets (column - row) and FP32
+// or FP16 values, for the FP32 iterations of the reliable-update PCG
+// (spmv_rel.cu).  rowptr is the source segments' own.
+struct RelCsr {
+   int32_t n = 0, max_row = 0;
+   const int32_t* rowptr = nullptr;
+   bool half = false;
+   DeviceBuffer off, vals;
+};
+// Builds the compact copy; *ok is false (nothing to use) when the matrix is
+// not short-row CSR or a column lies 32768 or more from its row.
+tnlb_status rel_csr_build(const tnlb_segments* seg, const int32_t* cols, const float* vals, bool half,
+                          cudaStream_t st, RelCsr* out, bool* ok);
+tnlb_status rel_spmv_dot(const RelCsr& A, const float* x, float* y, double* partials, unsigned* counter,
+                         double* dot_out, cudaStream_t st, const int32_t* skip, bool self_dot);
+tnlb_status rel_spmv_xpby(const RelCsr& A, const float* x, float* y, const double* num, const double* den,
+                          cudaStream_t st, const int32_t* skip);
 tnlb_status spmv_xpby(const tnlb_segments* seg, tnlb_real real, const int32_t* cols, const void* vals, const void* x,
                       void* y, const double* num, const double* den, cudaStream_t st, const int32_t* skip);
 tnlb_status spmv_csr(const tnlb_segments* seg, tnlb_real real, const int32_t* cols, const void* vals, const void* x,
@@ -329,6 +346,15 @@ tnlb_status fsai_apply(const Fsai* F, const void* r, void* z, cudaStream_t st, c
 // z = G^T (G r) with (r, z) = |G r|^2 summed inside the G product (symmetric
 // FSAI whose G has rows of at most 16 entries: fsai_dot_fusable).
 bool fsai_dot_fusable(const Fsai* F);
+// The parts of an FSAI preconditioner: G and G^T (segments, columns,
+// values of the preconditioner's real type) and its work vector t.
+struct FsaiView {
+   const tnlb_segments *g = nullptr, *gt = nullptr;
+   const int32_t *gcols = nullptr, *gtcols = nullptr;
+   const void *gvals = nullptr, *gtvals = nullptr;
+   void* tmp = nullptr;
+};
+FsaiView fsai_view(const Fsai* F);
 bool fsai_two_factor(const Fsai* F);
 tnlb_status fsai_apply_dot(const Fsai* F, const void* r, void* z, double* partials, unsigned* counter, double* rz_out,
                            cudaStream_t st, const int32_t* skip);

@@ -2404,10 +2404,33 @@ tnlb_status reliable_t(const tnlb_segments* seg, const int32_t* cols, const doub
    const unsigned Gd = resident_grid((const void*)k_ru_dot<VT>, kRedThreads, n, 4);
    const float* v32f = v32.as<float>();
 
+   // FP32 vectors on stencil-like matrices: compact copies of A (FP32
+   // values) and of the FSAI factors (FP16 values: M = G^T G stays symmetric
+   // positive definite) with 16-bit column offsets, which the FP32 products
+   // read instead of the 8-byte entries
+   RelCsr relA, relG, relGT;
+   bool rel_a = false, rel_m = false;
+   if (kVec == TNLB_F32) {
+      if (fused_a) TNLB_TRY_STATUS(rel_csr_build(seg, cols, v32f, false, st, &relA, &rel_a));
+      if (fused_m) {
+         const FsaiView fv = fsai_view(pobj->fsai);
+         bool ok_g = false, ok_gt = false;
+         TNLB_TRY_STATUS(rel_csr_build(fv.g, fv.gcols, (const float*)fv.gvals, true, st, &relG, &ok_g));
+         if (ok_g) TNLB_TRY_STATUS(rel_csr_build(fv.gt, fv.gtcols, (const float*)fv.gtvals, true, st, &relGT, &ok_gt));
+         rel_m = ok_g && ok_gt;
+      }
+   }
+   float* tvec = mode == 2 ? (float*)fsai_view(pobj->fsai).tmp : nullptr;
+
    // z = M^-1 r, (r, z) into rz_cur and p = z + beta p (beta = (r, z) /
    // S->rz); a short-row symmetric FSAI does it in two fused products
    // (t = G r with (t, t) = (r, z); p = G^T t + beta p), z never stored
    auto precondition = [&](cudaStream_t s, const int32_t* skip) -> tnlb_status {
+      if (rel_m) {
+         TNLB_TRY_STATUS(rel_spmv_dot(relG, (const float*)r.ptr, tvec, WM.partials.as<double>(),
+                                      WM.counter.as<unsigned>(), rz_cur, s, skip, true));
+         return rel_spmv_xpby(relGT, tvec, (float*)p.ptr, rz_cur, &S->rz, s, skip);
+      }
       if (fused_m)
          return fsai_apply_dot_xpby(pobj->fsai, kVec, r.ptr, p.ptr, WM.partials.as<double>(),
                                     WM.counter.as<unsigned>(), rz_cur, &S->rz, s, skip);
@@ -2420,7 +2443,10 @@ tnlb_status reliable_t(const tnlb_segments* seg, const int32_t* cols, const doub
       return TNLB_OK;
    };
    auto iteration = [&](cudaStream_t s) -> tnlb_status {
-      if (fused_a)
+      if (rel_a)
+         TNLB_TRY_STATUS(rel_spmv_dot(relA, (const float*)p.ptr, (float*)Ap.ptr, WA.partials.as<double>(),
+                                      WA.counter.as<unsigned>(), pap, s, halt, false));
+      else if (fused_a)
          TNLB_TRY_STATUS(spmv_dot_mixed(seg, TNLB_F32, kVec, kVec, cols, v32f, p.ptr, Ap.ptr,
                                         WA.partials.as<double>(), WA.counter.as<unsigned>(), pap, s, halt, false));
       else {
