@@ -1870,12 +1870,18 @@ done:
  * replaced by (VT)(b - A x) (FP64 product) whenever the recursive |r|^2
  * falls below max(delta |r_u|, tol |b|)^2, r_u the residual of the last
  * update; p is kept, beta = (r, z)_new / (r, z)_old.  precond: 0 none,
- * 1 Jacobi (diagonal of the FP32 values).  Returns 1 when the true FP64
- * residual ||b - A x|| / ||b|| < tol. */
+ * 1 Jacobi (diagonal of the FP32 values), 2 FSAI z = G^T (G r) from the
+ * factor G and its transpose as the solver applies them (CSR, FP32 values;
+ * rows summed in VT in entry order) with (r, z) = |G r|^2.  Returns 1 when
+ * the true FP64 residual ||b - A x|| / ||b|| < tol. */
+typedef struct {
+   const int32_t *grp, *gcols, *gtrp, *gtcols;
+   const float *gvals, *gtvals;
+} OrcFsaiFactors;
 #define ORC_RELIABLE(NAME, VT)                                                                                       \
    static int NAME(int32_t n, const int32_t* rowptr, const int32_t* cols, const double* vals, int precond,         \
-                   const double* b, double* x, double tol, double delta, int32_t maxit, int32_t* iterations,      \
-                   int32_t* updates, double* resid)                                                              \
+                   const OrcFsaiFactors* F, const double* b, double* x, double tol, double delta, int32_t maxit,  \
+                   int32_t* iterations, int32_t* updates, double* resid)                                          \
    {                                                                                                              \
       const int32_t nnz = rowptr[n];                                                                              \
       float* v32 = (float*)malloc(sizeof(float) * (size_t)(nnz > 0 ? nnz : 1));                                   \
@@ -1883,6 +1889,7 @@ done:
       VT *r = (VT*)malloc(sizeof(VT) * (size_t)n), *z = (VT*)malloc(sizeof(VT) * (size_t)n);                      \
       VT *p = (VT*)calloc((size_t)n, sizeof(VT)), *Ap = (VT*)malloc(sizeof(VT) * (size_t)n);                      \
       VT* xc = (VT*)calloc((size_t)n, sizeof(VT));                                                                \
+      VT* t = (VT*)malloc(sizeof(VT) * (size_t)(n > 0 ? n : 1));                                                  \
       for (int32_t k = 0; k < nnz; k++) v32[k] = (float)vals[k];                                                  \
       for (int32_t i = 0; i < n; i++) {                                                                           \
          float di = 0.0f;                                                                                         \
@@ -1919,10 +1926,13 @@ done:
          const double trig2 = t1 > t2 ? t1 * t1 : t2 * t2;                                                        \
          halt = 0;                                                                                                \
          rz_cur = 0.0;                                                                                            \
-         for (int32_t i = 0; i < n; i++) {                                                                        \
-            z[i] = precond == 1 ? r[i] / (VT)d[i] : r[i];                                                         \
-            rz_cur += (double)r[i] * (double)z[i];                                                                \
-         }                                                                                                        \
+         if (precond == 2)                                                                                        \
+            rz_cur = NAME##_fsai(n, F, r, t, z);                                                                  \
+         else                                                                                                     \
+            for (int32_t i = 0; i < n; i++) {                                                                     \
+               z[i] = precond == 1 ? r[i] / (VT)d[i] : r[i];                                                      \
+               rz_cur += (double)r[i] * (double)z[i];                                                             \
+            }                                                                                                     \
          {                                                                                                        \
             const VT beta = (VT)(rz_cur / rz);                                                                    \
             for (int32_t i = 0; i < n; i++) p[i] = z[i] + beta * p[i];                                            \
@@ -1947,9 +1957,12 @@ done:
                xc[i] += alpha * p[i];                                                                             \
                r[i] = r[i] - alpha * Ap[i];                                                                        \
                rr += (double)r[i] * (double)r[i];                                                                 \
-               z[i] = precond == 1 ? r[i] / (VT)d[i] : r[i];                                                      \
-               rzn += (double)r[i] * (double)z[i];                                                                \
+               if (precond != 2) {                                                                                \
+                  z[i] = precond == 1 ? r[i] / (VT)d[i] : r[i];                                                   \
+                  rzn += (double)r[i] * (double)z[i];                                                             \
+               }                                                                                                  \
             }                                                                                                     \
+            if (precond == 2) rzn = NAME##_fsai(n, F, r, t, z);                                                   \
             it++;                                                                                                 \
             if (!isfinite(rr))                                                                                    \
                halt = 2;                                                                                          \
@@ -1973,8 +1986,31 @@ done:
       free(p);                                                                                                    \
       free(Ap);                                                                                                   \
       free(xc);                                                                                                   \
+      free(t);                                                                                                    \
       return ok;                                                                                                  \
    }
+
+/* t = G r, z = G^T t, returns (t, t) = (r, z). */
+#define ORC_FSAI_APPLY(NAME, VT)                                                                                     \
+   static double NAME(int32_t n, const OrcFsaiFactors* F, const VT* r, VT* t, VT* z)                             \
+   {                                                                                                              \
+      double rz = 0.0;                                                                                            \
+      for (int32_t i = 0; i < n; i++) {                                                                           \
+         VT s = (VT)0;                                                                                            \
+         for (int32_t k = F->grp[i]; k < F->grp[i + 1]; k++) s += (VT)F->gvals[k] * r[F->gcols[k]];                \
+         t[i] = s;                                                                                                \
+         rz += (double)s * (double)s;                                                                             \
+      }                                                                                                           \
+      for (int32_t i = 0; i < n; i++) {                                                                           \
+         VT s = (VT)0;                                                                                            \
+         for (int32_t k = F->gtrp[i]; k < F->gtrp[i + 1]; k++) s += (VT)F->gtvals[k] * t[F->gtcols[k]];           \
+         z[i] = s;                                                                                                \
+      }                                                                                                           \
+      return rz;                                                                                                  \
+   }
+ORC_FSAI_APPLY(reliable_f32_fsai, float)
+ORC_FSAI_APPLY(reliable_f64_fsai, double)
+#undef ORC_FSAI_APPLY
 
 ORC_RELIABLE(reliable_f32, float)
 ORC_RELIABLE(reliable_f64, double)
@@ -1984,6 +2020,20 @@ int orc_pcg_reliable(int32_t n, const int32_t* rowptr, const int32_t* cols, cons
                      const double* b, double* x, double tol, double delta, int32_t maxit, int vec64,
                      int32_t* iterations, int32_t* updates, double* resid)
 {
-   if (vec64) return reliable_f64(n, rowptr, cols, vals, precond, b, x, tol, delta, maxit, iterations, updates, resid);
-   return reliable_f32(n, rowptr, cols, vals, precond, b, x, tol, delta, maxit, iterations, updates, resid);
+   if (precond == 2) return 0;
+   if (vec64)
+      return reliable_f64(n, rowptr, cols, vals, precond, NULL, b, x, tol, delta, maxit, iterations, updates, resid);
+   return reliable_f32(n, rowptr, cols, vals, precond, NULL, b, x, tol, delta, maxit, iterations, updates, resid);
+}
+
+/* The same with an FSAI factor pair (precond 2). */
+int orc_pcg_reliable_fsai(int32_t n, const int32_t* rowptr, const int32_t* cols, const double* vals,
+                          const int32_t* grp, const int32_t* gcols, const float* gvals, const int32_t* gtrp,
+                          const int32_t* gtcols, const float* gtvals, const double* b, double* x, double tol,
+                          double delta, int32_t maxit, int vec64, int32_t* iterations, int32_t* updates,
+                          double* resid)
+{
+   const OrcFsaiFactors F = {grp, gcols, gtrp, gtcols, gvals, gtvals};
+   if (vec64) return reliable_f64(n, rowptr, cols, vals, 2, &F, b, x, tol, delta, maxit, iterations, updates, resid);
+   return reliable_f32(n, rowptr, cols, vals, 2, &F, b, x, tol, delta, maxit, iterations, updates, resid);
 }

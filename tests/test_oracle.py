@@ -308,6 +308,27 @@ def test_reliable_update_pcg_restatement(oracle):
     assert v["iterations"] <= 1.3 * f["iterations"], (v["iterations"], f["iterations"])
 
 
+def test_reliable_update_pcg_restatement_fsai(oracle):
+    """The FSAI form of the restatement (z = G^T G r, (r, z) = |G r|^2):
+    with G = I it takes the unpreconditioned steps bit for bit; with the
+    diagonal factor G = D^-1/2 it converges like Jacobi."""
+    A = g.diffusion_2d(64, 0.1, 2.0, 3)
+    b = g.uniform_vector(A.n, 1)
+    n = A.n
+    eye = (np.arange(n + 1, dtype=np.int32), np.arange(n, dtype=np.int32), np.ones(n, np.float32))
+    r0 = oracle.pcg_reliable(A, b, precond=0, tol=1e-8, delta=0.1)
+    ri = oracle.pcg_reliable_fsai(A, b, eye, eye, tol=1e-8, delta=0.1)
+    assert ri["converged"] and (ri["iterations"], ri["updates"]) == (r0["iterations"], r0["updates"])
+    assert np.array_equal(ri["x"], r0["x"])
+    d = np.array([A.vals[A.rowptr[i]:A.rowptr[i + 1]][A.cols[A.rowptr[i]:A.rowptr[i + 1]] == i][0]
+                  for i in range(n)])
+    gd = (eye[0], eye[1], (1.0 / np.sqrt(d)).astype(np.float32))
+    rj = oracle.pcg_reliable(A, b, precond=1, tol=1e-8, delta=0.1)
+    rd = oracle.pcg_reliable_fsai(A, b, gd, gd, tol=1e-8, delta=0.1)
+    assert rd["converged"] and oracle.true_residual(A, b, rd["x"]) < 1e-8
+    assert abs(rd["iterations"] - rj["iterations"]) <= max(3, 0.03 * rj["iterations"]), (rd, rj["iterations"])
+
+
 def test_transposition_matches_reference(oracle, reference):
     """getTransposition: the restatement (stable sort by column) equals the
     reference's single-threaded Host result bit for bit -- row pointer,

@@ -220,6 +220,38 @@ def test_reliable_mixed_pcg_matches_oracle(oracle, name, pc, vec64):
     assert abs(r["true_residual"] - t.true_residual(M, bs, xs)) <= 1e-15
 
 
+@pytest.mark.parametrize("vec64", [False, True])
+def test_reliable_mixed_pcg_fsai_matches_oracle(oracle, vec64):
+    """The reliable-update PCG with an FP32 FSAI against its oracle
+    restatement given the solver's own factors G and G^T: with FP32 vectors
+    the products read FP16 copies of the factor values (the oracle gets the
+    same FP16-rounded values) and the update of x and r is fused into them;
+    with FP64 vectors the FP32 factors are used.  Iterations and updates
+    agree within the slack of a different summation order."""
+    from tnl_b200 import generators as g
+
+    t = tnl()
+    A = g.diffusion_2d(96, 0.1, 2.0, 7)
+    b = g.uniform_vector(A.n, 1)
+    M = t.SparseMatrix(t.CSR, torch.float64).assign(A.rowptr, A.cols, A.vals)
+    M32 = t.SparseMatrix(t.CSR, torch.float32).assign(A.rowptr, A.cols, A.vals.astype(np.float32))
+    P = t.FSAI()
+    P.update(M32)
+    G, GT = P.factor(0), P.factor(1)
+    if not vec64:
+        G = (G[0], G[1], G[2].astype(np.float16).astype(np.float32))
+        GT = (GT[0], GT[1], GT[2].astype(np.float16).astype(np.float32))
+    o = oracle.pcg_reliable_fsai(A, b, G, GT, tol=1e-8, delta=0.1, vec64=vec64)
+    bs = torch.tensor(b, device="cuda")
+    xs = torch.zeros(A.n, dtype=torch.float64, device="cuda")
+    r = t.solve_mixed_reliable(M, bs, xs, tol=1e-8, delta=0.1, inner=P,
+                               vectors=torch.float64 if vec64 else torch.float32)
+    assert o["converged"] and r["converged"] and not r["breakdown"]
+    assert abs(r["iterations"] - o["iterations"]) <= max(3, 0.03 * o["iterations"]), (r, o["iterations"])
+    assert abs(r["reliable_updates"] - o["updates"]) <= 1, (r, o["updates"])
+    assert r["true_residual"] < 1e-8 and oracle.true_residual(A, b, xs.cpu().numpy()) < 1e-8
+
+
 def test_reliable_mixed_pcg_with_fsai():
     """With an FP32 FSAI the reliable-update solver reaches the FP64
     tolerance in fewer iterations than iterative refinement (which restarts

@@ -291,7 +291,12 @@ def bench_solvers(problem: str, N: int, weights: str | None, out=sys.stdout):
         train = [diffusion_problem(128, s) for s in range(8)]
         net.fit_classical(train, steps=400, lr=3e-3)
         net.train(train, steps=400, nprobes=8, lr=5e-4)
+    # set-up timed warm (the first call loads the network's kernels), fastest of 3
+    net.preconditioner(A32)
     P32, s = _timed(lambda: net.preconditioner(A32))
+    for _ in range(2):
+        P32, s2 = _timed(lambda: net.preconditioner(A32))
+        s = min(s, s2)
     mixed("FP32-inner IR, learned FSAI", P32, s)
     reliable("FP32 reliable-update PCG, learned FSAI", P32, s)
     reliable("FP32-matrix FP64-vector reliable-update PCG, learned FSAI", P32, s, torch.float64)

@@ -22,6 +22,7 @@
 #include "internal.cuh"
 #include "reduce.cuh"
 #include "segview.cuh"
+#include "spmv_rel.cuh"
 
 namespace tnlb {
 
@@ -2263,6 +2264,105 @@ __global__ void __launch_bounds__(kRedThreads) k_ru_update(int64_t n, VT* __rest
    }
 }
 
+// r - alpha Ap: one expression for the stored residual and for the copies
+// of it that k_ru_g_update gathers, so that both round alike.
+__device__ __forceinline__ float ru_rnext(float r, float alpha, float ap) { return r - alpha * ap; }
+
+// k_ru_update fused into the first FSAI factor product, on the compact copy
+// of G (16-bit column offsets): alpha = (r, z) / (p, A p) as k_ru_update
+// forms it; rn = r - alpha Ap into the other residual buffer; t = G rn, each
+// gathered rn[c] recomputed from r and Ap; |rn|^2 and (t, t) = (rn, M rn)
+// reduced together.  The last block keeps k_ru_update's books and stores
+// (t, t) as the new (r, z).  xc += alpha p is left to k_ru_gt_xpby, which
+// reads p anyway -- or, when this iteration raises `halt`, to the fold of
+// the reliable update (k_ru_fold_p).
+template <typename TV, int L, int R>
+__global__ void __launch_bounds__(kRedThreads)
+   k_ru_g_update(const int32_t* __restrict__ rowptr, const int16_t* __restrict__ off, const TV* __restrict__ vals,
+                 const float* __restrict__ r, const float* __restrict__ Ap, float* __restrict__ rn,
+                 float* __restrict__ t, int32_t n, RedWork w, RuState* S, double* __restrict__ rz_cur,
+                 const double* __restrict__ pap)
+{
+   if (S->halt) return;
+   const double rz = *rz_cur, tp = *pap;
+   const bool ok = tp != 0.0 && isfinite(tp);
+   const float alpha = ok ? (float)(rz / tp) : 0.0f;
+   const auto rv = [r, Ap, alpha](int32_t c) { return ru_rnext(__ldg(r + c), alpha, __ldg(Ap + c)); };
+   double rr = 0, tt = 0;
+   const int64_t stride = (int64_t)gridDim.x * blockDim.x * R;
+   for (int64_t r0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * R; r0 < n; r0 += stride) {
+      float s[R];
+      rel_rows_f<TV, L, R>(rowptr, off, vals, rv, r0, n, s);
+#pragma unroll
+      for (int k = 0; k < R; k++)
+         if (r0 + k < n) {
+            const float v = rv((int32_t)(r0 + k));
+            rn[r0 + k] = v;
+            t[r0 + k] = s[k];
+            rr += (double)v * (double)v;
+            tt += (double)s[k] * (double)s[k];
+         }
+   }
+   double v[2] = {rr, tt};
+   if (publish_and_arrive<2>(v, w)) {
+      double tot[2];
+      gather_totals<2>(tot, w);
+      if (threadIdx.x == 0) {
+         S->rz = rz;
+         S->alpha = (double)alpha;
+         S->it++;
+         S->rr = tot[0];
+         *rz_cur = tot[1];
+         if (!ok || !isfinite(tot[0]))
+            S->halt = 2;
+         else if (tot[0] < S->trig2)
+            S->halt = 1;
+         else if (S->it >= S->maxit)
+            S->halt = 3;
+      }
+   }
+}
+
+// p = G^T t + beta p (beta = (r, z)_new / (r, z)_old) on the compact copy of
+// G^T, and xc += alpha p with the p that alpha was formed for.
+template <typename TV, int L, int R>
+__global__ void __launch_bounds__(kRedThreads)
+   k_ru_gt_xpby(const int32_t* __restrict__ rowptr, const int16_t* __restrict__ off, const TV* __restrict__ vals,
+                const float* __restrict__ t, float* __restrict__ p, float* __restrict__ xc, int32_t n,
+                const double* __restrict__ rz_cur, const RuState* S)
+{
+   if (S->halt) return;
+   const float beta = (float)(*rz_cur / S->rz);
+   const float alpha = (float)S->alpha;
+   const int64_t stride = (int64_t)gridDim.x * blockDim.x * R;
+   for (int64_t r0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * R; r0 < n; r0 += stride) {
+      float s[R];
+      rel_rows<TV, L, R>(rowptr, off, vals, t, r0, n, s);
+#pragma unroll
+      for (int k = 0; k < R; k++)
+         if (r0 + k < n) {
+            const float po = p[r0 + k];
+            xc[r0 + k] += alpha * po;
+            p[r0 + k] = s[k] + beta * po;
+         }
+   }
+}
+
+// x += xc + alpha p, the step k_ru_gt_xpby skips when the iteration that
+// formed alpha raised `halt` (alpha is 0 before the first iteration); xc = 0.
+template <typename VT>
+__global__ void k_ru_fold_p(int64_t n, VT* __restrict__ xc, const VT* __restrict__ p, const RuState* S,
+                            double* __restrict__ x)
+{
+   const VT alpha = (VT)S->alpha;
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+      VT xv = xc[i];
+      xv += alpha * p[i];
+      x[i] += (double)xv;
+      xc[i] = VT(0);
+   }
+}
+
 // z and (r, z) from r alone (after a reliable update): mode 1 Jacobi, mode 0 none.
 template <typename VT>
 __global__ void __launch_bounds__(kRedThreads) k_ru_precond(int64_t n, const VT* __restrict__ r,
@@ -2421,6 +2521,12 @@ tnlb_status reliable_t(const tnlb_segments* seg, const int32_t* cols, const doub
       }
    }
    float* tvec = mode == 2 ? (float*)fsai_view(pobj->fsai).tmp : nullptr;
+   // with the compact FSAI copies the update of xc and r goes into the two
+   // factor products (k_ru_g_update, k_ru_gt_xpby); the new residual goes
+   // to the other of two buffers, iteration by iteration
+   const bool fused_u = rel_m && relG.half && relGT.half;
+   DeviceBuffer r2;
+   if (fused_u) TNLB_TRY_STATUS(r2.alloc(sizeof(float) * n));
 
    // z = M^-1 r, (r, z) into rz_cur and p = z + beta p (beta = (r, z) /
    // S->rz); a short-row symmetric FSAI does it in two fused products
@@ -2442,7 +2548,7 @@ tnlb_status reliable_t(const tnlb_segments* seg, const int32_t* cols, const doub
       TNLB_CHECK_LAUNCH();
       return TNLB_OK;
    };
-   auto iteration = [&](cudaStream_t s) -> tnlb_status {
+   auto iteration = [&](cudaStream_t s, int k) -> tnlb_status {
       if (rel_a)
          TNLB_TRY_STATUS(rel_spmv_dot(relA, (const float*)p.ptr, (float*)Ap.ptr, WA.partials.as<double>(),
                                       WA.counter.as<unsigned>(), pap, s, halt, false));
@@ -2456,6 +2562,28 @@ tnlb_status reliable_t(const tnlb_segments* seg, const int32_t* cols, const doub
          else
             TNLB_TRY_STATUS(spmv_dispatch(seg, TNLB_F64, cols, vals, p.ptr, Ap.ptr, 1.0, 0.0, s, halt));
          k_ru_dot<VT><<<Gd, kRedThreads, 0, s>>>(n, p.as<VT>(), Ap.as<VT>(), WA.red(), pap, halt);
+      }
+      if (fused_u) {
+         // even iterations r -> r2, odd ones r2 -> r: a batch (even) ends in r
+         const float* rin = (const float*)(k & 1 ? r2.ptr : r.ptr);
+         float* rout = (float*)(k & 1 ? r.ptr : r2.ptr);
+         TNLB_REL_WIDTH(relG.max_row, {
+            constexpr int R = rel_rows_per_thread<L>();
+            auto* kg = k_ru_g_update<__half, L, R>;
+            const unsigned g = resident_grid((const void*)kg, kRedThreads, n, R);
+            kg<<<g, kRedThreads, 0, s>>>(relG.rowptr, relG.off.as<int16_t>(), relG.vals.as<__half>(), rin,
+                                         (const float*)Ap.ptr, rout, tvec, (int32_t)n, W.red(), S, rz_cur, pap);
+         });
+         TNLB_CHECK_LAUNCH();
+         TNLB_REL_WIDTH(relGT.max_row, {
+            constexpr int R = rel_rows_per_thread<L>();
+            auto* kt = k_ru_gt_xpby<__half, L, R>;
+            const unsigned g = resident_grid((const void*)kt, kRedThreads, n, R);
+            kt<<<g, kRedThreads, 0, s>>>(relGT.rowptr, relGT.off.as<int16_t>(), relGT.vals.as<__half>(), tvec,
+                                         (float*)p.ptr, (float*)xc.ptr, (int32_t)n, rz_cur, S);
+         });
+         TNLB_CHECK_LAUNCH();
+         return TNLB_OK;
       }
       k_ru_update<VT><<<Gu, kRedThreads, 0, s>>>(n, xc.as<VT>(), r.as<VT>(), p.as<VT>(), Ap.as<VT>(), d, z.as<VT>(),
                                                  mode, W.red(), S, rz_cur, pap);
@@ -2493,7 +2621,7 @@ tnlb_status reliable_t(const tnlb_segments* seg, const int32_t* cols, const doub
    cudaGraphExec_t exec = nullptr;
    tnlb_status status = TNLB_OK;
    if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
-      for (int k = 0; k < kBatch && status == TNLB_OK; k++) status = iteration(cs);
+      for (int k = 0; k < kBatch && status == TNLB_OK; k++) status = iteration(cs, k);
       cudaError_t e = cudaStreamEndCapture(cs, &graph);
       if (e == cudaSuccess && status == TNLB_OK) e = cudaGraphInstantiate(&exec, graph, 0);
       if (e != cudaSuccess) {
@@ -2538,7 +2666,7 @@ tnlb_status reliable_t(const tnlb_segments* seg, const int32_t* cols, const doub
          TNLB_CUDA_TRY(cudaGraphLaunch(exec, cs));
          return TNLB_OK;
       }
-      for (int k = 0; k < kBatch; k++) TNLB_TRY_STATUS(iteration(cs));
+      for (int k = 0; k < kBatch; k++) TNLB_TRY_STATUS(iteration(cs, k));
       return TNLB_OK;
    };
 
@@ -2548,7 +2676,10 @@ tnlb_status reliable_t(const tnlb_segments* seg, const int32_t* cols, const doub
    bool converged = false;
    for (;;) {
       // reliable update: x += xc, r = b - A x in FP64, r = (VT) r
-      k_ru_fold<VT><<<G, kRedThreads, 0, cs>>>(n, xc.as<VT>(), x);
+      if (fused_u)
+         k_ru_fold_p<VT><<<G, kRedThreads, 0, cs>>>(n, xc.as<VT>(), p.as<VT>(), S, x);
+      else
+         k_ru_fold<VT><<<G, kRedThreads, 0, cs>>>(n, xc.as<VT>(), x);
       TNLB_CHECK_LAUNCH();
       TNLB_TRY_STATUS(spmv_dispatch(seg, TNLB_F64, cols, vals, x, ax.ptr, 1.0, 0.0, cs));
       k_ru_resid<VT><<<G, kRedThreads, 0, cs>>>(n, b, ax.as<double>(), r.as<VT>(), W.red(), rsum);

@@ -12,6 +12,7 @@
 
 #include "internal.cuh"
 #include "reduce.cuh"
+#include "spmv_rel.cuh"
 
 namespace tnlb {
 
@@ -40,34 +41,8 @@ __global__ void k_to_half(const float* __restrict__ a, int64_t n, __half* __rest
       b[i] = __float2half_rn(a[i]);
 }
 
-__device__ __forceinline__ float to_f(float v) { return v; }
-__device__ __forceinline__ float to_f(__half v) { return __half2float(v); }
-
-template <typename TV, int L>
-__device__ __forceinline__ float rel_row(const int32_t* __restrict__ rowptr, const int16_t* __restrict__ off,
-                                         const TV* __restrict__ vals, const float* __restrict__ x, int64_t r)
-{
-   const int32_t b = rowptr[r], e = rowptr[r + 1];
-   int32_t c[L];
-   float v[L];
-#pragma unroll
-   for (int j = 0; j < L; j++) {
-      c[j] = -1;
-      v[j] = 0.0f;
-      if (b + j < e) {
-         c[j] = (int32_t)r + (int32_t)__ldg(off + b + j);
-         v[j] = to_f(__ldg(vals + b + j));
-      }
-   }
-   float s = 0.0f;
-#pragma unroll
-   for (int j = 0; j < L; j++)
-      if (c[j] >= 0) s += v[j] * __ldg(x + c[j]);
-   return s;
-}
-
 // y = A x and (x, y) -- or (y, y) with `self` -- as k_csr_short_dot does.
-template <typename TV, int L>
+template <typename TV, int L, int R>
 __global__ void __launch_bounds__(256) k_rel_dot(const int32_t* __restrict__ rowptr, const int16_t* __restrict__ off,
                                                  const TV* __restrict__ vals, const float* __restrict__ x,
                                                  float* __restrict__ y, int32_t n, RedWork w,
@@ -76,10 +51,16 @@ __global__ void __launch_bounds__(256) k_rel_dot(const int32_t* __restrict__ row
 {
    if (skip && *skip) return;
    double d = 0.0;
-   for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
-      const float s = rel_row<TV, L>(rowptr, off, vals, x, r);
-      y[r] = s;
-      d += (double)s * (self ? (double)s : (double)__ldg(x + r));
+   const int64_t stride = (int64_t)gridDim.x * blockDim.x * R;
+   for (int64_t r0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * R; r0 < n; r0 += stride) {
+      float s[R];
+      rel_rows<TV, L, R>(rowptr, off, vals, x, r0, n, s);
+#pragma unroll
+      for (int k = 0; k < R; k++)
+         if (r0 + k < n) {
+            y[r0 + k] = s[k];
+            d += (double)s[k] * (self ? (double)s[k] : (double)__ldg(x + r0 + k));
+         }
    }
    double vv[1] = {d};
    if (publish_and_arrive<1>(vv, w)) {
@@ -90,7 +71,7 @@ __global__ void __launch_bounds__(256) k_rel_dot(const int32_t* __restrict__ row
 }
 
 // y = A x + (num / den) y, as k_csr_short_xpby does.
-template <typename TV, int L>
+template <typename TV, int L, int R>
 __global__ void __launch_bounds__(256) k_rel_xpby(const int32_t* __restrict__ rowptr, const int16_t* __restrict__ off,
                                                   const TV* __restrict__ vals, const float* __restrict__ x,
                                                   float* __restrict__ y, int32_t n, const double* __restrict__ num,
@@ -98,35 +79,15 @@ __global__ void __launch_bounds__(256) k_rel_xpby(const int32_t* __restrict__ ro
 {
    if (skip && *skip) return;
    const float beta = (float)(*num / *den);
-   for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
-      const float s = rel_row<TV, L>(rowptr, off, vals, x, r);
-      y[r] = s + beta * y[r];
+   const int64_t stride = (int64_t)gridDim.x * blockDim.x * R;
+   for (int64_t r0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * R; r0 < n; r0 += stride) {
+      float s[R];
+      rel_rows<TV, L, R>(rowptr, off, vals, x, r0, n, s);
+#pragma unroll
+      for (int k = 0; k < R; k++)
+         if (r0 + k < n) y[r0 + k] = s[k] + beta * y[r0 + k];
    }
 }
-
-#define TNLB_REL_WIDTH(m, ...)   \
-   do {                          \
-      if ((m) <= 4) {            \
-         constexpr int L = 4;    \
-         __VA_ARGS__;            \
-      }                          \
-      else if ((m) <= 5) {       \
-         constexpr int L = 5;    \
-         __VA_ARGS__;            \
-      }                          \
-      else if ((m) <= 7) {       \
-         constexpr int L = 7;    \
-         __VA_ARGS__;            \
-      }                          \
-      else if ((m) <= 8) {       \
-         constexpr int L = 8;    \
-         __VA_ARGS__;            \
-      }                          \
-      else {                     \
-         constexpr int L = 16;   \
-         __VA_ARGS__;            \
-      }                          \
-   } while (0)
 
 }  // namespace
 
@@ -170,14 +131,16 @@ tnlb_status rel_spmv_dot(const RelCsr& A, const float* x, float* y, double* part
    const int self = self_dot ? 1 : 0;
    if (A.half)
       TNLB_REL_WIDTH(A.max_row, {
-         auto* k = k_rel_dot<__half, L>;
-         const unsigned g = resident_grid((const void*)k, 256, A.n, 1);
+         constexpr int R = rel_rows_per_thread<L>();
+         auto* k = k_rel_dot<__half, L, R>;
+         const unsigned g = resident_grid((const void*)k, 256, A.n, R);
          k<<<g, 256, 0, st>>>(A.rowptr, A.off.as<int16_t>(), A.vals.as<__half>(), x, y, A.n, w, dot_out, skip, self);
       });
    else
       TNLB_REL_WIDTH(A.max_row, {
-         auto* k = k_rel_dot<float, L>;
-         const unsigned g = resident_grid((const void*)k, 256, A.n, 1);
+         constexpr int R = rel_rows_per_thread<L>();
+         auto* k = k_rel_dot<float, L, R>;
+         const unsigned g = resident_grid((const void*)k, 256, A.n, R);
          k<<<g, 256, 0, st>>>(A.rowptr, A.off.as<int16_t>(), A.vals.as<float>(), x, y, A.n, w, dot_out, skip, self);
       });
    TNLB_CHECK_LAUNCH();
@@ -189,14 +152,16 @@ tnlb_status rel_spmv_xpby(const RelCsr& A, const float* x, float* y, const doubl
 {
    if (A.half)
       TNLB_REL_WIDTH(A.max_row, {
-         auto* k = k_rel_xpby<__half, L>;
-         const unsigned g = resident_grid((const void*)k, 256, A.n, 1);
+         constexpr int R = rel_rows_per_thread<L>();
+         auto* k = k_rel_xpby<__half, L, R>;
+         const unsigned g = resident_grid((const void*)k, 256, A.n, R);
          k<<<g, 256, 0, st>>>(A.rowptr, A.off.as<int16_t>(), A.vals.as<__half>(), x, y, A.n, num, den, skip);
       });
    else
       TNLB_REL_WIDTH(A.max_row, {
-         auto* k = k_rel_xpby<float, L>;
-         const unsigned g = resident_grid((const void*)k, 256, A.n, 1);
+         constexpr int R = rel_rows_per_thread<L>();
+         auto* k = k_rel_xpby<float, L, R>;
+         const unsigned g = resident_grid((const void*)k, 256, A.n, R);
          k<<<g, 256, 0, st>>>(A.rowptr, A.off.as<int16_t>(), A.vals.as<float>(), x, y, A.n, num, den, skip);
       });
    TNLB_CHECK_LAUNCH();
