@@ -411,6 +411,9 @@ typedef struct {
    int32_t bicgstab_ell;         /* bicgstab-ell (BiCGStab(ell)), default 1 */
    int32_t idr_s;                /* idr-s (IDR(s) shadow space), default 4 */
    int32_t idr_residual_smoothing; /* idr-residual-smoothing, default 0 */
+   int32_t reliable_layout;      /* tnlb_solve_mixed_reliable's internal FP32 copies: 0 (default) the
+                                    diagonal layout where the matrix fits it, else CSR with 16-bit
+                                    column offsets; 1 the 16-bit offsets only */
 } tnlb_solver_params;
 
 /* Result of a solve: getIterations(), getResidue() and the bool of solve(). */

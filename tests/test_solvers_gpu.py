@@ -196,7 +196,8 @@ def test_mixed_precision_refinement_reaches_fp64_residual(oracle):
 
 
 @pytest.mark.parametrize("name,pc,vec64", [("laplacian48", 0, False), ("diffusion96", 1, False),
-                                           ("diffusion96", 1, True), ("laplacian48", 0, True)])
+                                           ("diffusion96", 1, True), ("laplacian48", 0, True),
+                                           ("ninepoint40", 1, False)])
 def test_reliable_mixed_pcg_matches_oracle(oracle, name, pc, vec64):
     """CG on FP32 values (FP32 or FP64 vectors) with reliable FP64 updates
     against its oracle restatement: the same number of iterations and
@@ -205,7 +206,8 @@ def test_reliable_mixed_pcg_matches_oracle(oracle, name, pc, vec64):
     from tnl_b200 import generators as g
 
     t = tnl()
-    A = g.laplacian_2d(48) if name == "laplacian48" else g.diffusion_2d(96, 0.1, 2.0, 7)
+    A = {"laplacian48": lambda: g.laplacian_2d(48), "diffusion96": lambda: g.diffusion_2d(96, 0.1, 2.0, 7),
+         "ninepoint40": lambda: _nine_point(40)}[name]()
     b = g.uniform_vector(A.n, 1)
     o = oracle.pcg_reliable(A, b, precond=pc, tol=1e-8, delta=0.1, vec64=vec64)
     M = t.SparseMatrix(t.CSR, torch.float64).assign(A.rowptr, A.cols, A.vals)
@@ -218,6 +220,44 @@ def test_reliable_mixed_pcg_matches_oracle(oracle, name, pc, vec64):
     assert abs(r["reliable_updates"] - o["updates"]) <= 1, (r, o["updates"])
     assert r["true_residual"] < 1e-8 and oracle.true_residual(A, b, xs.cpu().numpy()) < 1e-8
     assert abs(r["true_residual"] - t.true_residual(M, bs, xs)) <= 1e-15
+
+
+def _nine_point(N):
+    """kron(T, I) + kron(I, T) + kron(T, T), T = tridiag(-1, 2, -1): an SPD
+    matrix with 9 diagonals (more than the diagonal layout takes)."""
+    import scipy.sparse as sp
+    from tnl_b200 import generators as g
+
+    T = sp.diags([-np.ones(N - 1), 2 * np.ones(N), -np.ones(N - 1)], [-1, 0, 1])
+    E = sp.identity(N)
+    A = (sp.kron(T, E) + sp.kron(E, T) + sp.kron(T, T)).tocsr()
+    A.sort_indices()
+    return g.CSRMatrix(A.indptr.astype(np.int32), A.indices.astype(np.int32), A.data.astype(np.float64))
+
+
+@pytest.mark.parametrize("inner", ["fsai", "jacobi", "none"])
+def test_reliable_layouts_give_the_same_iterates(inner):
+    """The reliable-update PCG's internal FP32 copies by diagonal (5 for A,
+    3 for the FSAI factors here) and with 16-bit column offsets sum the same
+    terms in the same order: iterations, updates and x agree bit for bit."""
+    from tnl_b200 import generators as g
+
+    t = tnl()
+    A = g.diffusion_2d(80, 0.1, 2.0, 5)
+    b = g.uniform_vector(A.n, 1)
+    M = t.SparseMatrix(t.CSR, torch.float64).assign(A.rowptr, A.cols, A.vals)
+    bs = torch.tensor(b, device="cuda")
+    out = []
+    for layout in ("auto", "offsets"):
+        xs = torch.zeros(A.n, dtype=torch.float64, device="cuda")
+        r = t.solve_mixed_reliable(M, bs, xs, tol=1e-8, delta=0.1, inner=inner, layout=layout)
+        assert r["converged"] and not r["breakdown"]
+        out.append((r, xs))
+    (ra, xa), (ro, xo) = out
+    assert (ra["iterations"], ra["reliable_updates"]) == (ro["iterations"], ro["reliable_updates"])
+    assert torch.equal(xa, xo)
+    with pytest.raises(ValueError):
+        t.solve_mixed_reliable(M, bs, torch.zeros_like(bs), layout="dense")
 
 
 @pytest.mark.parametrize("vec64", [False, True])

@@ -778,7 +778,7 @@ def true_residual(M: SparseMatrix, b: torch.Tensor, x: torch.Tensor) -> float:
 
 def solve_mixed_reliable(M: SparseMatrix, b: torch.Tensor, x: torch.Tensor, tol: float = 1e-8, delta: float = 0.3,
                          max_iterations: int = 1000000, inner: str | _Preconditioner = "jacobi",
-                         vectors: torch.dtype = torch.float32) -> dict:
+                         vectors: torch.dtype = torch.float32, layout: str = "auto") -> dict:
     """Mixed-precision PCG with reliable updates (SPD matrices, FP64 matrix
     and vectors): CG iterations on FP32 values (FP32 or FP64 ``vectors``)
     whose correction is folded into the FP64 x, with the residual recomputed
@@ -790,11 +790,20 @@ def solve_mixed_reliable(M: SparseMatrix, b: torch.Tensor, x: torch.Tensor, tol:
     ``inner`` is "jacobi", "fsai", "none", or an FP32 Jacobi / FSAI
     preconditioner object built for an FP32 copy of the matrix (e.g. a
     learned FSAI).  Stops on the true FP64 residual ``tol``.
+
+    ``layout`` picks the internal FP32 copies of short-row matrices: "auto"
+    stores a matrix with few diagonals by diagonal, others as CSR with
+    16-bit column offsets; "offsets" always the latter.  Both give the same
+    iterates.
     """
     if M.real != torch.float64:
         raise TypeError("solve_mixed_reliable takes an FP64 matrix")
+    layouts = {"auto": 0, "offsets": 1}
+    if layout not in layouts:
+        raise ValueError(f"solve_mixed_reliable: unknown layout {layout!r}")
     p = capi.SolverParams()
     capi.tnlb_solver_params_default(C.byref(p))
+    p.reliable_layout = layouts[layout]
     p.convergence_residue = tol
     p.max_iterations = max_iterations
     r = capi.SolveResult()

@@ -243,13 +243,14 @@ def bench_solvers(problem: str, N: int, weights: str | None, out=sys.stdout):
                    true_residual=t.true_residual(M, b, x), speedup_vs_fp64_jacobi=jac["solve_ms"] / ms)
         print(json.dumps(rec), file=out, flush=True)
 
-    def reliable(name, inner, setup_ms, vectors=torch.float32):
+    def reliable(name, inner, setup_ms, vectors=torch.float32, layout="auto"):
         # speed-up on set-up + solve against the FP64 Jacobi-PCG's set-up +
         # solve, both to a true residual below 1e-8
         t.solve_mixed_reliable(M, b, torch.zeros(n, dtype=torch.float64, device="cuda"), tol=1e-8, inner=inner,
-                               max_iterations=20, vectors=vectors)
+                               max_iterations=20, vectors=vectors, layout=layout)
         r, x, ms, times = _median_timed(_Run(lambda x: t.solve_mixed_reliable(M, b, x, tol=1e-8, delta=0.3,
-                                                                              inner=inner, vectors=vectors), n))
+                                                                              inner=inner, vectors=vectors,
+                                                                              layout=layout), n))
         rec = dict(base, method=name, converged=r["converged"], iterations=r["iterations"],
                    reliable_updates=r["reliable_updates"], solve_ms=ms, solve_ms_runs=times, setup_ms=setup_ms,
                    true_residual=t.true_residual(M, b, x),
@@ -283,6 +284,7 @@ def bench_solvers(problem: str, N: int, weights: str | None, out=sys.stdout):
     mixed("FP32-inner IR, FSAI", "fsai", 0.0)
     reliable("FP32 reliable-update PCG, Jacobi", "jacobi", 0.0)
     reliable("FP32 reliable-update PCG, FSAI", "fsai", 0.0)
+    reliable("FP32 reliable-update PCG, FSAI, 16-bit-offset copies", "fsai", 0.0, layout="offsets")
     reliable("FP32-matrix FP64-vector reliable-update PCG, FSAI", "fsai", 0.0, torch.float64)
     net = LearnedFSAI(seed=2)
     if weights and Path(weights).exists():

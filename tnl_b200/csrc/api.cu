@@ -284,6 +284,7 @@ void tnlb_solver_params_default(tnlb_solver_params* p)
    p->bicgstab_ell = 1;               // BICGStabL.hpp:17
    p->idr_s = 4;                      // IDRs.hpp:21
    p->idr_residual_smoothing = 0;     // IDRs.hpp:22
+   p->reliable_layout = 0;
 }
 
 static tnlb_status check_solve_args(const tnlb_segments* seg, tnlb_real real, const void* b, void* x)

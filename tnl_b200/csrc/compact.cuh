@@ -1,0 +1,199 @@
+// compact.cuh -- device side of the compact matrix copies (compact.cu):
+// the two row layouts as "row policies" that the products of compact.cu and
+// the fused reliable-update kernels of solvers.cu are templated on.
+//
+// A policy gives each thread R rows per pass of a grid-stride loop (kept
+// rolled with `#pragma unroll 1`: left to the compiler, the loop around an
+// FP64 dot accumulator was unrolled into a schedule that took the diagonal
+// product on the 2048^2 5-point operator from 28.5 to 61.8 us):
+//   first(), step()   the loop over pass bases;
+//   row(base, k)      row k of the pass (rows at or past n are skipped);
+//   rows(base, n, xv, s)  s[k] = sum over the row's entries of v * xv(c),
+//                     xv(c) the input at column c, summed in FP32 in
+//                     ascending column order.
+// Both layouts sum the same terms in the same order -- a missing diagonal
+// slot adds fma(0, x, s) = s -- so for finite inputs their results are
+// bitwise equal.
+#pragma once
+
+#include <cuda_fp16.h>
+
+#include <cstdint>
+
+namespace tnlb {
+
+__device__ __forceinline__ float rel_to_f(float v) { return v; }
+__device__ __forceinline__ float rel_to_f(__half v) { return __half2float(v); }
+
+// CSR with 16-bit column offsets, R consecutive rows per thread (R + 1 row
+// offsets, then every entry load of the R rows issued before the gathers).
+template <typename TV, int L, int R>
+struct RelRows {
+   static constexpr int kR = R;
+   const int32_t* __restrict__ rowptr;
+   const int16_t* __restrict__ off;
+   const TV* __restrict__ vals;
+
+   __device__ __forceinline__ int64_t first() const { return ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * R; }
+   __device__ __forceinline__ int64_t step() const { return (int64_t)gridDim.x * blockDim.x * R; }
+   __device__ __forceinline__ int64_t row(int64_t base, int k) const { return base + k; }
+
+   template <typename XV>
+   __device__ __forceinline__ void rows(int64_t r0, int32_t n, const XV& xv, float (&s)[R]) const
+   {
+      int32_t bnd[R + 1];
+#pragma unroll
+      for (int k = 0; k <= R; k++) bnd[k] = r0 + k <= n ? __ldg(rowptr + r0 + k) : 0;
+      int32_t c[R][L];
+      float v[R][L];
+#pragma unroll
+      for (int k = 0; k < R; k++)
+#pragma unroll
+         for (int j = 0; j < L; j++) {
+            c[k][j] = -1;
+            v[k][j] = 0.0f;
+            if (r0 + k < n && bnd[k] + j < bnd[k + 1]) {
+               c[k][j] = (int32_t)(r0 + k) + (int32_t)__ldg(off + bnd[k] + j);
+               v[k][j] = rel_to_f(__ldg(vals + bnd[k] + j));
+            }
+         }
+#pragma unroll
+      for (int k = 0; k < R; k++) {
+         float t = 0.0f;
+#pragma unroll
+         for (int j = 0; j < L; j++)
+            if (c[k][j] >= 0) t += v[k][j] * xv(c[k][j]);
+         s[k] = t;
+      }
+   }
+};
+
+// Column offsets of the diagonals (ascending).
+struct DiaOffsets {
+   int32_t o[8];
+};
+
+// Diagonal layout, R rows per thread a block apart (every load of a warp
+// one contiguous run); all D value loads and D input loads of the R rows
+// are issued before the sums.  A column outside [0, n) has a zero value and
+// reads nothing.  Columns are formed in 32 bits (n < 2^31).
+template <typename TV, int D, int R>
+struct DiaRows {
+   static constexpr int kR = R;
+   const TV* __restrict__ vals;
+   DiaOffsets d;
+   int32_t n;
+
+   __device__ __forceinline__ int64_t first() const
+   {
+      return (int64_t)blockIdx.x * blockDim.x * R + threadIdx.x;
+   }
+   __device__ __forceinline__ int64_t step() const { return (int64_t)gridDim.x * blockDim.x * R; }
+   __device__ __forceinline__ int64_t row(int64_t base, int k) const { return base + (int64_t)k * blockDim.x; }
+
+   template <typename XV>
+   __device__ __forceinline__ void rows(int64_t base, int32_t nr, const XV& xv, float (&s)[R]) const
+   {
+      float v[R][D], x[R][D];
+#pragma unroll
+      for (int k = 0; k < R; k++) {
+         const int64_t i64 = row(base, k);
+         const bool rin = i64 < nr;
+         const int32_t i = (int32_t)i64;
+         const TV* vp = vals + i;
+#pragma unroll
+         for (int j = 0; j < D; j++) {
+            const int32_t c = i + d.o[j];
+            const bool in = rin && (uint32_t)c < (uint32_t)nr;
+            v[k][j] = in ? rel_to_f(__ldg(vp + (int64_t)j * n)) : 0.0f;
+            x[k][j] = in ? xv(c) : 0.0f;
+         }
+      }
+#pragma unroll
+      for (int k = 0; k < R; k++) {
+         float t = 0.0f;
+#pragma unroll
+         for (int j = 0; j < D; j++) t += v[k][j] * x[k][j];
+         s[k] = t;
+      }
+   }
+};
+
+// Rows per thread: two for up to 8 entries a row, as the short-row sweep on
+// the 5-point operator and its triangular factor favoured (FP16 values:
+// 25 -> 19 us on the factor).
+template <int L>
+constexpr int rel_rows_per_thread()
+{
+   return L <= 8 ? 2 : 1;
+}
+
+#define TNLB_REL_WIDTH(m, ...)   \
+   do {                          \
+      if ((m) <= 4) {            \
+         constexpr int L = 4;    \
+         __VA_ARGS__;            \
+      }                          \
+      else if ((m) <= 5) {       \
+         constexpr int L = 5;    \
+         __VA_ARGS__;            \
+      }                          \
+      else if ((m) <= 7) {       \
+         constexpr int L = 7;    \
+         __VA_ARGS__;            \
+      }                          \
+      else if ((m) <= 8) {       \
+         constexpr int L = 8;    \
+         __VA_ARGS__;            \
+      }                          \
+      else {                     \
+         constexpr int L = 16;   \
+         __VA_ARGS__;            \
+      }                          \
+   } while (0)
+
+#define TNLB_DIA_CASE(DD, ...)   \
+   case DD: {                    \
+      constexpr int D = DD;      \
+      __VA_ARGS__;               \
+      break;                     \
+   }
+#define TNLB_DIA_WIDTH(m, ...)                    \
+   do {                                           \
+      switch (m) {                                \
+         TNLB_DIA_CASE(1, __VA_ARGS__)            \
+         TNLB_DIA_CASE(2, __VA_ARGS__)            \
+         TNLB_DIA_CASE(3, __VA_ARGS__)            \
+         TNLB_DIA_CASE(4, __VA_ARGS__)            \
+         TNLB_DIA_CASE(5, __VA_ARGS__)            \
+         TNLB_DIA_CASE(6, __VA_ARGS__)            \
+         TNLB_DIA_CASE(7, __VA_ARGS__)            \
+         default: {                               \
+            constexpr int D = 8;                  \
+            __VA_ARGS__;                          \
+         }                                        \
+      }                                           \
+   } while (0)
+
+// `using Rows = <the policy of copy C with values TV>;` then the body.
+#define TNLB_COMPACT_ROWS(C, TV, ...)                                                                  \
+   do {                                                                                                \
+      if ((C).kind == CompactCopy::kDia) {                                                             \
+         TNLB_DIA_WIDTH((C).width, {                                                                   \
+            using Rows = DiaRows<TV, D, 1>;                                                            \
+            DiaOffsets dd_;                                                                            \
+            for (int q_ = 0; q_ < 8; q_++) dd_.o[q_] = (C).diag[q_];                                   \
+            const Rows rows_{(C).vals.template as<TV>(), dd_, (C).n};                                  \
+            __VA_ARGS__;                                                                               \
+         });                                                                                           \
+      }                                                                                                \
+      else {                                                                                           \
+         TNLB_REL_WIDTH((C).width, {                                                                   \
+            using Rows = RelRows<TV, L, rel_rows_per_thread<L>()>;                                     \
+            const Rows rows_{(C).rowptr, (C).off.template as<int16_t>(), (C).vals.template as<TV>()};  \
+            __VA_ARGS__;                                                                               \
+         });                                                                                           \
+      }                                                                                                \
+   } while (0)
+
+}  // namespace tnlb

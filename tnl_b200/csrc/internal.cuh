@@ -286,23 +286,35 @@ tnlb_status spmv_dot_mixed(const tnlb_segments* seg, tnlb_real tv, tnlb_real tx,
 tnlb_status spmv_xpby_mixed(const tnlb_segments* seg, tnlb_real tv, tnlb_real tx, tnlb_real ty, const int32_t* cols,
                             const void* vals, const void* x, void* y, const double* num, const double* den,
                             cudaStream_t st, const int32_t* skip);
-// A short-row CSR matrix with 16-bit column offsets (column - row) and FP32
-// or FP16 values, for the FP32 iterations of the reliable-update PCG
-// (spmv_rel.cu).  rowptr is the source segments' own.
-struct RelCsr {
-   int32_t n = 0, max_row = 0;
-   const int32_t* rowptr = nullptr;
+// Compact copy of a short-row CSR matrix with FP32 or FP16 values, for the
+// FP32 iterations of the reliable-update PCG (compact.cu), in one of two
+// layouts:
+//   kRel: CSR with 16-bit column offsets (column - row); rowptr is the
+//         source segments' own; width = the longest row;
+//   kDia: diagonals -- the matrix has `width` <= 8 distinct column - row
+//         offsets (diag[], ascending), each row's columns ascending; the
+//         value of row i on diagonal j at vals[j * n + i], 0 where the row
+//         has no such entry.
+struct CompactCopy {
+   enum Kind { kNone = 0, kRel = 1, kDia = 2 };
+   Kind kind = kNone;
+   int32_t n = 0, width = 0;
    bool half = false;
+   const int32_t* rowptr = nullptr;
+   int32_t diag[8] = {};
    DeviceBuffer off, vals;
 };
-// Builds the compact copy; *ok is false (nothing to use) when the matrix is
-// not short-row CSR or a column lies 32768 or more from its row.
-tnlb_status rel_csr_build(const tnlb_segments* seg, const int32_t* cols, const float* vals, bool half,
-                          cudaStream_t st, RelCsr* out, bool* ok);
-tnlb_status rel_spmv_dot(const RelCsr& A, const float* x, float* y, double* partials, unsigned* counter,
-                         double* dot_out, cudaStream_t st, const int32_t* skip, bool self_dot);
-tnlb_status rel_spmv_xpby(const RelCsr& A, const float* x, float* y, const double* num, const double* den,
-                          cudaStream_t st, const int32_t* skip);
+// Builds the copy (kind kNone when the matrix is not short-row CSR or a
+// column lies 32768 or more from its row): kDia when allowed and the
+// diagonals hold at least 3/4 of their slots, else kRel.
+tnlb_status compact_build(const tnlb_segments* seg, const int32_t* cols, const float* vals, bool half, bool allow_dia,
+                          cudaStream_t st, CompactCopy* out);
+// y = A x and (x, y) -- (y, y) with self_dot -- into *dot_out.
+tnlb_status compact_spmv_dot(const CompactCopy& A, const float* x, float* y, double* partials, unsigned* counter,
+                             double* dot_out, cudaStream_t st, const int32_t* skip, bool self_dot);
+// y = A x + (*num / *den) y.
+tnlb_status compact_spmv_xpby(const CompactCopy& A, const float* x, float* y, const double* num, const double* den,
+                              cudaStream_t st, const int32_t* skip);
 tnlb_status spmv_xpby(const tnlb_segments* seg, tnlb_real real, const int32_t* cols, const void* vals, const void* x,
                       void* y, const double* num, const double* den, cudaStream_t st, const int32_t* skip);
 tnlb_status spmv_csr(const tnlb_segments* seg, tnlb_real real, const int32_t* cols, const void* vals, const void* x,

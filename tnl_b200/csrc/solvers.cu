@@ -22,7 +22,7 @@
 #include "internal.cuh"
 #include "reduce.cuh"
 #include "segview.cuh"
-#include "spmv_rel.cuh"
+#include "compact.cuh"
 
 namespace tnlb {
 
@@ -2276,10 +2276,9 @@ __device__ __forceinline__ float ru_rnext(float r, float alpha, float ap) { retu
 // (t, t) as the new (r, z).  xc += alpha p is left to k_ru_gt_xpby, which
 // reads p anyway -- or, when this iteration raises `halt`, to the fold of
 // the reliable update (k_ru_fold_p).
-template <typename TV, int L, int R>
+template <typename Rows>
 __global__ void __launch_bounds__(kRedThreads)
-   k_ru_g_update(const int32_t* __restrict__ rowptr, const int16_t* __restrict__ off, const TV* __restrict__ vals,
-                 const float* __restrict__ r, const float* __restrict__ Ap, float* __restrict__ rn,
+   k_ru_g_update(Rows G, const float* __restrict__ r, const float* __restrict__ Ap, float* __restrict__ rn,
                  float* __restrict__ t, int32_t n, RedWork w, RuState* S, double* __restrict__ rz_cur,
                  const double* __restrict__ pap)
 {
@@ -2289,19 +2288,21 @@ __global__ void __launch_bounds__(kRedThreads)
    const float alpha = ok ? (float)(rz / tp) : 0.0f;
    const auto rv = [r, Ap, alpha](int32_t c) { return ru_rnext(__ldg(r + c), alpha, __ldg(Ap + c)); };
    double rr = 0, tt = 0;
-   const int64_t stride = (int64_t)gridDim.x * blockDim.x * R;
-   for (int64_t r0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * R; r0 < n; r0 += stride) {
-      float s[R];
-      rel_rows_f<TV, L, R>(rowptr, off, vals, rv, r0, n, s);
+#pragma unroll 1
+   for (int64_t base = G.first(); base < n; base += G.step()) {
+      float s[Rows::kR];
+      G.rows(base, n, rv, s);
 #pragma unroll
-      for (int k = 0; k < R; k++)
-         if (r0 + k < n) {
-            const float v = rv((int32_t)(r0 + k));
-            rn[r0 + k] = v;
-            t[r0 + k] = s[k];
+      for (int k = 0; k < Rows::kR; k++) {
+         const int64_t i = G.row(base, k);
+         if (i < n) {
+            const float v = rv((int32_t)i);
+            rn[i] = v;
+            t[i] = s[k];
             rr += (double)v * (double)v;
             tt += (double)s[k] * (double)s[k];
          }
+      }
    }
    double v[2] = {rr, tt};
    if (publish_and_arrive<2>(v, w)) {
@@ -2325,27 +2326,47 @@ __global__ void __launch_bounds__(kRedThreads)
 
 // p = G^T t + beta p (beta = (r, z)_new / (r, z)_old) on the compact copy of
 // G^T, and xc += alpha p with the p that alpha was formed for.
-template <typename TV, int L, int R>
+template <typename Rows>
 __global__ void __launch_bounds__(kRedThreads)
-   k_ru_gt_xpby(const int32_t* __restrict__ rowptr, const int16_t* __restrict__ off, const TV* __restrict__ vals,
-                const float* __restrict__ t, float* __restrict__ p, float* __restrict__ xc, int32_t n,
+   k_ru_gt_xpby(Rows GT, const float* __restrict__ t, float* __restrict__ p, float* __restrict__ xc, int32_t n,
                 const double* __restrict__ rz_cur, const RuState* S)
 {
    if (S->halt) return;
    const float beta = (float)(*rz_cur / S->rz);
    const float alpha = (float)S->alpha;
-   const int64_t stride = (int64_t)gridDim.x * blockDim.x * R;
-   for (int64_t r0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * R; r0 < n; r0 += stride) {
-      float s[R];
-      rel_rows<TV, L, R>(rowptr, off, vals, t, r0, n, s);
+   const auto tv = [t](int32_t c) { return __ldg(t + c); };
+#pragma unroll 1
+   for (int64_t base = GT.first(); base < n; base += GT.step()) {
+      float s[Rows::kR];
+      GT.rows(base, n, tv, s);
 #pragma unroll
-      for (int k = 0; k < R; k++)
-         if (r0 + k < n) {
-            const float po = p[r0 + k];
-            xc[r0 + k] += alpha * po;
-            p[r0 + k] = s[k] + beta * po;
+      for (int k = 0; k < Rows::kR; k++) {
+         const int64_t i = GT.row(base, k);
+         if (i < n) {
+            const float po = p[i];
+            xc[i] += alpha * po;
+            p[i] = s[k] + beta * po;
          }
+      }
    }
+}
+
+template <typename Rows>
+void launch_ru_g_update(const Rows& G, const float* r, const float* Ap, float* rn, float* t, int32_t n, RedWork w,
+                        RuState* S, double* rz_cur, const double* pap, cudaStream_t st)
+{
+   auto* k = k_ru_g_update<Rows>;
+   const unsigned g = resident_grid((const void*)k, kRedThreads, n, Rows::kR);
+   k<<<g, kRedThreads, 0, st>>>(G, r, Ap, rn, t, n, w, S, rz_cur, pap);
+}
+
+template <typename Rows>
+void launch_ru_gt_xpby(const Rows& GT, const float* t, float* p, float* xc, int32_t n, const double* rz_cur,
+                       const RuState* S, cudaStream_t st)
+{
+   auto* k = k_ru_gt_xpby<Rows>;
+   const unsigned g = resident_grid((const void*)k, kRedThreads, n, Rows::kR);
+   k<<<g, kRedThreads, 0, st>>>(GT, t, p, xc, n, rz_cur, S);
 }
 
 // x += xc + alpha p, the step k_ru_gt_xpby skips when the iteration that
@@ -2506,25 +2527,28 @@ tnlb_status reliable_t(const tnlb_segments* seg, const int32_t* cols, const doub
 
    // FP32 vectors on stencil-like matrices: compact copies of A (FP32
    // values) and of the FSAI factors (FP16 values: M = G^T G stays symmetric
-   // positive definite) with 16-bit column offsets, which the FP32 products
-   // read instead of the 8-byte entries
-   RelCsr relA, relG, relGT;
-   bool rel_a = false, rel_m = false;
+   // positive definite), by diagonal or with 16-bit column offsets
+   // (compact.cu), which the FP32 products read instead of the 8-byte
+   // entries
+   CompactCopy cA, cG, cGT;
+   const bool compact_dia = prm.reliable_layout == 0;
    if (kVec == TNLB_F32) {
-      if (fused_a) TNLB_TRY_STATUS(rel_csr_build(seg, cols, v32f, false, st, &relA, &rel_a));
+      if (fused_a) TNLB_TRY_STATUS(compact_build(seg, cols, v32f, false, compact_dia, st, &cA));
       if (fused_m) {
          const FsaiView fv = fsai_view(pobj->fsai);
-         bool ok_g = false, ok_gt = false;
-         TNLB_TRY_STATUS(rel_csr_build(fv.g, fv.gcols, (const float*)fv.gvals, true, st, &relG, &ok_g));
-         if (ok_g) TNLB_TRY_STATUS(rel_csr_build(fv.gt, fv.gtcols, (const float*)fv.gtvals, true, st, &relGT, &ok_gt));
-         rel_m = ok_g && ok_gt;
+         TNLB_TRY_STATUS(compact_build(fv.g, fv.gcols, (const float*)fv.gvals, true, compact_dia, st, &cG));
+         if (cG.kind != CompactCopy::kNone)
+            TNLB_TRY_STATUS(
+               compact_build(fv.gt, fv.gtcols, (const float*)fv.gtvals, true, compact_dia, st, &cGT));
       }
    }
+   const bool cmp_a = cA.kind != CompactCopy::kNone;
+   const bool cmp_m = cG.kind != CompactCopy::kNone && cGT.kind != CompactCopy::kNone;
    float* tvec = mode == 2 ? (float*)fsai_view(pobj->fsai).tmp : nullptr;
    // with the compact FSAI copies the update of xc and r goes into the two
    // factor products (k_ru_g_update, k_ru_gt_xpby); the new residual goes
    // to the other of two buffers, iteration by iteration
-   const bool fused_u = rel_m && relG.half && relGT.half;
+   const bool fused_u = cmp_m;
    DeviceBuffer r2;
    if (fused_u) TNLB_TRY_STATUS(r2.alloc(sizeof(float) * n));
 
@@ -2532,10 +2556,10 @@ tnlb_status reliable_t(const tnlb_segments* seg, const int32_t* cols, const doub
    // S->rz); a short-row symmetric FSAI does it in two fused products
    // (t = G r with (t, t) = (r, z); p = G^T t + beta p), z never stored
    auto precondition = [&](cudaStream_t s, const int32_t* skip) -> tnlb_status {
-      if (rel_m) {
-         TNLB_TRY_STATUS(rel_spmv_dot(relG, (const float*)r.ptr, tvec, WM.partials.as<double>(),
-                                      WM.counter.as<unsigned>(), rz_cur, s, skip, true));
-         return rel_spmv_xpby(relGT, tvec, (float*)p.ptr, rz_cur, &S->rz, s, skip);
+      if (cmp_m) {
+         TNLB_TRY_STATUS(compact_spmv_dot(cG, (const float*)r.ptr, tvec, WM.partials.as<double>(),
+                                          WM.counter.as<unsigned>(), rz_cur, s, skip, true));
+         return compact_spmv_xpby(cGT, tvec, (float*)p.ptr, rz_cur, &S->rz, s, skip);
       }
       if (fused_m)
          return fsai_apply_dot_xpby(pobj->fsai, kVec, r.ptr, p.ptr, WM.partials.as<double>(),
@@ -2549,9 +2573,9 @@ tnlb_status reliable_t(const tnlb_segments* seg, const int32_t* cols, const doub
       return TNLB_OK;
    };
    auto iteration = [&](cudaStream_t s, int k) -> tnlb_status {
-      if (rel_a)
-         TNLB_TRY_STATUS(rel_spmv_dot(relA, (const float*)p.ptr, (float*)Ap.ptr, WA.partials.as<double>(),
-                                      WA.counter.as<unsigned>(), pap, s, halt, false));
+      if (cmp_a)
+         TNLB_TRY_STATUS(compact_spmv_dot(cA, (const float*)p.ptr, (float*)Ap.ptr, WA.partials.as<double>(),
+                                          WA.counter.as<unsigned>(), pap, s, halt, false));
       else if (fused_a)
          TNLB_TRY_STATUS(spmv_dot_mixed(seg, TNLB_F32, kVec, kVec, cols, v32f, p.ptr, Ap.ptr,
                                         WA.partials.as<double>(), WA.counter.as<unsigned>(), pap, s, halt, false));
@@ -2567,21 +2591,12 @@ tnlb_status reliable_t(const tnlb_segments* seg, const int32_t* cols, const doub
          // even iterations r -> r2, odd ones r2 -> r: a batch (even) ends in r
          const float* rin = (const float*)(k & 1 ? r2.ptr : r.ptr);
          float* rout = (float*)(k & 1 ? r.ptr : r2.ptr);
-         TNLB_REL_WIDTH(relG.max_row, {
-            constexpr int R = rel_rows_per_thread<L>();
-            auto* kg = k_ru_g_update<__half, L, R>;
-            const unsigned g = resident_grid((const void*)kg, kRedThreads, n, R);
-            kg<<<g, kRedThreads, 0, s>>>(relG.rowptr, relG.off.as<int16_t>(), relG.vals.as<__half>(), rin,
-                                         (const float*)Ap.ptr, rout, tvec, (int32_t)n, W.red(), S, rz_cur, pap);
-         });
+         TNLB_COMPACT_ROWS(cG, __half,
+                           launch_ru_g_update(rows_, rin, (const float*)Ap.ptr, rout, tvec, (int32_t)n, W.red(), S,
+                                              rz_cur, pap, s));
          TNLB_CHECK_LAUNCH();
-         TNLB_REL_WIDTH(relGT.max_row, {
-            constexpr int R = rel_rows_per_thread<L>();
-            auto* kt = k_ru_gt_xpby<__half, L, R>;
-            const unsigned g = resident_grid((const void*)kt, kRedThreads, n, R);
-            kt<<<g, kRedThreads, 0, s>>>(relGT.rowptr, relGT.off.as<int16_t>(), relGT.vals.as<__half>(), tvec,
-                                         (float*)p.ptr, (float*)xc.ptr, (int32_t)n, rz_cur, S);
-         });
+         TNLB_COMPACT_ROWS(cGT, __half,
+                           launch_ru_gt_xpby(rows_, tvec, (float*)p.ptr, (float*)xc.ptr, (int32_t)n, rz_cur, S, s));
          TNLB_CHECK_LAUNCH();
          return TNLB_OK;
       }
