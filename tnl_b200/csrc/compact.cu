@@ -102,10 +102,12 @@ __global__ void __launch_bounds__(256) k_diag_scan(const int32_t* __restrict__ r
    if (threadIdx.x < kDiagSlots && local[threadIdx.x] != kNoDiag && !diag_insert(tab, local[threadIdx.x])) *flag = 1;
 }
 
-// vals[j * n + r] = value of row r on diagonal j (the buffer zeroed before).
+// vals[j * pitch + r] = value of row r on diagonal j (the buffer zeroed
+// before).
 template <typename TV>
 __global__ void k_diag_fill(const int32_t* __restrict__ rowptr, const int32_t* __restrict__ cols,
-                            const float* __restrict__ v, int32_t n, DiaOffsets d, int32_t nd, TV* __restrict__ out)
+                            const float* __restrict__ v, int32_t n, DiaOffsets d, int32_t nd, int64_t pitch,
+                            TV* __restrict__ out)
 {
    const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
    if (r >= n) return;
@@ -113,23 +115,35 @@ __global__ void k_diag_fill(const int32_t* __restrict__ rowptr, const int32_t* _
       const int32_t o = cols[k] - (int32_t)r;
       int32_t j = 0;
       while (j < nd - 1 && d.o[j] != o) j++;
-      out[(int64_t)j * n + r] = (TV)v[k];
+      out[(int64_t)j * pitch + r] = (TV)v[k];
    }
 }
 
 // y = A x and (x, y) -- or (y, y) with `self` -- as k_csr_short_dot does.
+// Four-row policies (kQuad) store and read the rows' own entries as
+// vectors when all four rows exist (the vectors are 16-byte aligned).
 template <typename Rows>
 __global__ void __launch_bounds__(256) k_cmp_dot(Rows A, const float* __restrict__ x, float* __restrict__ y, int32_t n,
                                                  RedWork w, double* __restrict__ dot_out,
                                                  const int32_t* __restrict__ skip, int self)
 {
    if (skip && *skip) return;
-   const auto xv = [x](int32_t c) { return __ldg(x + c); };
+   const PlainInput xv{x};
    double d = 0.0;
 #pragma unroll 1
    for (int64_t base = A.first(); base < n; base += A.step()) {
       float s[Rows::kR];
       A.rows(base, n, xv, s);
+      if constexpr (Rows::kQuad) {
+         if (base + 3 < n) {
+            *reinterpret_cast<float4*>(y + base) = make_float4(s[0], s[1], s[2], s[3]);
+            float o[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+            if (!self) xv.quad((int32_t)base, o);
+#pragma unroll
+            for (int k = 0; k < 4; k++) d += (double)s[k] * (self ? (double)s[k] : (double)o[k]);
+            continue;
+         }
+      }
 #pragma unroll
       for (int k = 0; k < Rows::kR; k++) {
          const int64_t i = A.row(base, k);
@@ -155,11 +169,19 @@ __global__ void __launch_bounds__(256) k_cmp_xpby(Rows A, const float* __restric
 {
    if (skip && *skip) return;
    const float beta = (float)(*num / *den);
-   const auto xv = [x](int32_t c) { return __ldg(x + c); };
+   const PlainInput xv{x};
 #pragma unroll 1
    for (int64_t base = A.first(); base < n; base += A.step()) {
       float s[Rows::kR];
       A.rows(base, n, xv, s);
+      if constexpr (Rows::kQuad) {
+         if (base + 3 < n) {
+            float4* yp = reinterpret_cast<float4*>(y + base);
+            const float4 yo = *yp;
+            *yp = make_float4(s[0] + beta * yo.x, s[1] + beta * yo.y, s[2] + beta * yo.z, s[3] + beta * yo.w);
+            continue;
+         }
+      }
 #pragma unroll
       for (int k = 0; k < Rows::kR; k++) {
          const int64_t i = A.row(base, k);
@@ -214,20 +236,22 @@ tnlb_status diag_build(const tnlb_segments* seg, const int32_t* cols, const floa
    std::sort(d.begin(), d.end());
    DiaOffsets dd{};
    for (size_t j = 0; j < d.size(); j++) dd.o[j] = d[j];
+   const int64_t pitch = ((int64_t)n + 3) / 4 * 4;  // four-row vector loads stay aligned
    const size_t elem = half ? sizeof(__half) : sizeof(float);
-   const size_t bytes = elem * d.size() * (size_t)n;
+   const size_t bytes = elem * d.size() * (size_t)pitch;
    TNLB_TRY_STATUS(out->vals.alloc(bytes));
    TNLB_CUDA_TRY(cudaMemsetAsync(out->vals.ptr, 0, bytes, st));
    if (half)
-      k_diag_fill<__half><<<grid_for(n, 256), 256, 0, st>>>(rp, cols, vals, n, dd, (int32_t)d.size(),
+      k_diag_fill<__half><<<grid_for(n, 256), 256, 0, st>>>(rp, cols, vals, n, dd, (int32_t)d.size(), pitch,
                                                              out->vals.as<__half>());
    else
-      k_diag_fill<float><<<grid_for(n, 256), 256, 0, st>>>(rp, cols, vals, n, dd, (int32_t)d.size(),
+      k_diag_fill<float><<<grid_for(n, 256), 256, 0, st>>>(rp, cols, vals, n, dd, (int32_t)d.size(), pitch,
                                                             out->vals.as<float>());
    TNLB_CHECK_LAUNCH();
    out->kind = CompactCopy::kDia;
    out->n = n;
    out->width = (int32_t)d.size();
+   out->pitch = pitch;
    out->half = half;
    out->rowptr = rp;
    for (int j = 0; j < 8; j++) out->diag[j] = dd.o[j];
@@ -279,6 +303,8 @@ tnlb_status compact_spmv_dot(const CompactCopy& A, const float* x, float* y, dou
                              double* dot_out, cudaStream_t st, const int32_t* skip, bool self_dot)
 {
    TNLB_REQUIRE(A.kind != CompactCopy::kNone, TNLB_ERR_INVALID_ARGUMENT, "compact_spmv_dot: no compact copy");
+   TNLB_REQUIRE(A.kind != CompactCopy::kDia || (aligned16(x) && aligned16(y)), TNLB_ERR_INVALID_ARGUMENT,
+                "compact_spmv_dot: the vectors of a diagonal copy must be 16-byte aligned");
    const RedWork w{partials, counter};
    const int self = self_dot ? 1 : 0;
    if (A.half)
@@ -293,6 +319,8 @@ tnlb_status compact_spmv_xpby(const CompactCopy& A, const float* x, float* y, co
                               cudaStream_t st, const int32_t* skip)
 {
    TNLB_REQUIRE(A.kind != CompactCopy::kNone, TNLB_ERR_INVALID_ARGUMENT, "compact_spmv_xpby: no compact copy");
+   TNLB_REQUIRE(A.kind != CompactCopy::kDia || (aligned16(x) && aligned16(y)), TNLB_ERR_INVALID_ARGUMENT,
+                "compact_spmv_xpby: the vectors of a diagonal copy must be 16-byte aligned");
    if (A.half)
       TNLB_COMPACT_ROWS(A, __half, launch_cmp_xpby(rows_, A.n, x, y, num, den, st, skip));
    else

@@ -30,6 +30,7 @@ __device__ __forceinline__ float rel_to_f(__half v) { return __half2float(v); }
 template <typename TV, int L, int R>
 struct RelRows {
    static constexpr int kR = R;
+   static constexpr bool kQuad = false;
    const int32_t* __restrict__ rowptr;
    const int16_t* __restrict__ off;
    const TV* __restrict__ vals;
@@ -73,47 +74,87 @@ struct DiaOffsets {
    int32_t o[8];
 };
 
-// Diagonal layout, R rows per thread a block apart (every load of a warp
-// one contiguous run); all D value loads and D input loads of the R rows
-// are issued before the sums.  A column outside [0, n) has a zero value and
-// reads nothing.  Columns are formed in 32 bits (n < 2^31).
-template <typename TV, int D, int R>
+// Four consecutive values of a 16-byte-aligned (FP32) or 8-byte-aligned
+// (FP16) array.
+__device__ __forceinline__ void ld_quad(const float* p, float (&o)[4])
+{
+   const float4 t = __ldg(reinterpret_cast<const float4*>(p));
+   o[0] = t.x;
+   o[1] = t.y;
+   o[2] = t.z;
+   o[3] = t.w;
+}
+__device__ __forceinline__ void ld_quad(const __half* p, float (&o)[4])
+{
+   const uint2 t = __ldg(reinterpret_cast<const uint2*>(p));
+   const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&t.x));
+   const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&t.y));
+   o[0] = a.x;
+   o[1] = a.y;
+   o[2] = b.x;
+   o[3] = b.y;
+}
+
+// The input of a product: x[c], and x[c .. c+3] for c a multiple of 4.
+struct PlainInput {
+   const float* __restrict__ x;
+   __device__ __forceinline__ float operator()(int32_t c) const { return __ldg(x + c); }
+   __device__ __forceinline__ void quad(int32_t c, float (&o)[4]) const { ld_quad(x + c, o); }
+};
+
+// Diagonal layout, four consecutive rows per thread (kQuad): the value
+// pitch is a multiple of 4, so each diagonal's four values are one vector
+// load, and so is the input of a diagonal whose offset is a multiple of 4
+// (0 and +-N on an N-wide grid); the other diagonals' inputs are four
+// scalar loads that mostly hit the same sectors.  A column outside [0, n)
+// has a zero value and reads nothing.  Columns are formed in 32 bits
+// (n < 2^31).  The input functor needs operator()(c) and quad(c, o).
+template <typename TV, int D>
 struct DiaRows {
-   static constexpr int kR = R;
+   static constexpr int kR = 4;
+   static constexpr bool kQuad = true;
    const TV* __restrict__ vals;
    DiaOffsets d;
-   int32_t n;
+   int64_t pitch;
 
    __device__ __forceinline__ int64_t first() const
    {
-      return (int64_t)blockIdx.x * blockDim.x * R + threadIdx.x;
+      return ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * 4;
    }
-   __device__ __forceinline__ int64_t step() const { return (int64_t)gridDim.x * blockDim.x * R; }
-   __device__ __forceinline__ int64_t row(int64_t base, int k) const { return base + (int64_t)k * blockDim.x; }
+   __device__ __forceinline__ int64_t step() const { return (int64_t)gridDim.x * blockDim.x * 4; }
+   __device__ __forceinline__ int64_t row(int64_t base, int k) const { return base + k; }
 
    template <typename XV>
-   __device__ __forceinline__ void rows(int64_t base, int32_t nr, const XV& xv, float (&s)[R]) const
+   __device__ __forceinline__ void rows(int64_t base, int32_t nr, const XV& xv, float (&s)[4]) const
    {
-      float v[R][D], x[R][D];
+      const int32_t i0 = (int32_t)base;
+      const bool full = base + 3 < nr;
+      float v[D][4], x[D][4];
 #pragma unroll
-      for (int k = 0; k < R; k++) {
-         const int64_t i64 = row(base, k);
-         const bool rin = i64 < nr;
-         const int32_t i = (int32_t)i64;
-         const TV* vp = vals + i;
+      for (int j = 0; j < D; j++) {
+         const TV* vp = vals + (int64_t)j * pitch + i0;
+         const int32_t c0 = i0 + d.o[j];
+         if (full)
+            ld_quad(vp, v[j]);
+         else
 #pragma unroll
-         for (int j = 0; j < D; j++) {
-            const int32_t c = i + d.o[j];
-            const bool in = rin && (uint32_t)c < (uint32_t)nr;
-            v[k][j] = in ? rel_to_f(__ldg(vp + (int64_t)j * n)) : 0.0f;
-            x[k][j] = in ? xv(c) : 0.0f;
-         }
+            for (int k = 0; k < 4; k++) v[j][k] = i0 + k < nr ? rel_to_f(__ldg(vp + k)) : 0.0f;
+         if (full && (d.o[j] & 3) == 0 && c0 >= 0 && c0 + 3 < nr)
+            xv.quad(c0, x[j]);
+         else
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+               const int32_t c = c0 + k;
+               const bool in = i0 + k < nr && (uint32_t)c < (uint32_t)nr;
+               x[j][k] = in ? xv(c) : 0.0f;
+               if (!in) v[j][k] = 0.0f;
+            }
       }
 #pragma unroll
-      for (int k = 0; k < R; k++) {
+      for (int k = 0; k < 4; k++) {
          float t = 0.0f;
 #pragma unroll
-         for (int j = 0; j < D; j++) t += v[k][j] * x[k][j];
+         for (int j = 0; j < D; j++) t += v[j][k] * x[j][k];
          s[k] = t;
       }
    }
@@ -180,10 +221,10 @@ constexpr int rel_rows_per_thread()
    do {                                                                                                \
       if ((C).kind == CompactCopy::kDia) {                                                             \
          TNLB_DIA_WIDTH((C).width, {                                                                   \
-            using Rows = DiaRows<TV, D, 1>;                                                            \
+            using Rows = DiaRows<TV, D>;                                                               \
             DiaOffsets dd_;                                                                            \
             for (int q_ = 0; q_ < 8; q_++) dd_.o[q_] = (C).diag[q_];                                   \
-            const Rows rows_{(C).vals.template as<TV>(), dd_, (C).n};                                  \
+            const Rows rows_{(C).vals.template as<TV>(), dd_, (C).pitch};                              \
             __VA_ARGS__;                                                                               \
          });                                                                                           \
       }                                                                                                \

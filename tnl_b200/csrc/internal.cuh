@@ -293,8 +293,8 @@ tnlb_status spmv_xpby_mixed(const tnlb_segments* seg, tnlb_real tv, tnlb_real tx
 //         source segments' own; width = the longest row;
 //   kDia: diagonals -- the matrix has `width` <= 8 distinct column - row
 //         offsets (diag[], ascending), each row's columns ascending; the
-//         value of row i on diagonal j at vals[j * n + i], 0 where the row
-//         has no such entry.
+//         value of row i on diagonal j at vals[j * pitch + i], 0 where the
+//         row has no such entry; the products' vectors 16-byte aligned.
 struct CompactCopy {
    enum Kind { kNone = 0, kRel = 1, kDia = 2 };
    Kind kind = kNone;
@@ -302,8 +302,10 @@ struct CompactCopy {
    bool half = false;
    const int32_t* rowptr = nullptr;
    int32_t diag[8] = {};
+   int64_t pitch = 0;  // kDia: values of diagonal j at vals[j * pitch ...], pitch a multiple of 4
    DeviceBuffer off, vals;
 };
+inline bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
 // Builds the copy (kind kNone when the matrix is not short-row CSR or a
 // column lies 32768 or more from its row): kDia when allowed and the
 // diagonals hold at least 3/4 of their slots, else kRel.

@@ -2268,8 +2268,28 @@ __global__ void __launch_bounds__(kRedThreads) k_ru_update(int64_t n, VT* __rest
 // of it that k_ru_g_update gathers, so that both round alike.
 __device__ __forceinline__ float ru_rnext(float r, float alpha, float ap) { return r - alpha * ap; }
 
-// k_ru_update fused into the first FSAI factor product, on the compact copy
-// of G (16-bit column offsets): alpha = (r, z) / (p, A p) as k_ru_update
+// The input of k_ru_g_update's product: r - alpha Ap at a column, or at four
+// (16-byte-aligned) consecutive columns.
+struct RuNextInput {
+   const float* __restrict__ r;
+   const float* __restrict__ Ap;
+   float alpha;
+   __device__ __forceinline__ float operator()(int32_t c) const
+   {
+      return ru_rnext(__ldg(r + c), alpha, __ldg(Ap + c));
+   }
+   __device__ __forceinline__ void quad(int32_t c, float (&o)[4]) const
+   {
+      float a[4], b[4];
+      ld_quad(r + c, a);
+      ld_quad(Ap + c, b);
+#pragma unroll
+      for (int k = 0; k < 4; k++) o[k] = ru_rnext(a[k], alpha, b[k]);
+   }
+};
+
+// k_ru_update fused into the first FSAI factor product, on a compact copy
+// of G (compact.cu): alpha = (r, z) / (p, A p) as k_ru_update
 // forms it; rn = r - alpha Ap into the other residual buffer; t = G rn, each
 // gathered rn[c] recomputed from r and Ap; |rn|^2 and (t, t) = (rn, M rn)
 // reduced together.  The last block keeps k_ru_update's books and stores
@@ -2286,12 +2306,26 @@ __global__ void __launch_bounds__(kRedThreads)
    const double rz = *rz_cur, tp = *pap;
    const bool ok = tp != 0.0 && isfinite(tp);
    const float alpha = ok ? (float)(rz / tp) : 0.0f;
-   const auto rv = [r, Ap, alpha](int32_t c) { return ru_rnext(__ldg(r + c), alpha, __ldg(Ap + c)); };
+   const RuNextInput rv{r, Ap, alpha};
    double rr = 0, tt = 0;
 #pragma unroll 1
    for (int64_t base = G.first(); base < n; base += G.step()) {
       float s[Rows::kR];
       G.rows(base, n, rv, s);
+      if constexpr (Rows::kQuad) {
+         if (base + 3 < n) {
+            float v[4];
+            rv.quad((int32_t)base, v);
+            *reinterpret_cast<float4*>(rn + base) = make_float4(v[0], v[1], v[2], v[3]);
+            *reinterpret_cast<float4*>(t + base) = make_float4(s[0], s[1], s[2], s[3]);
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+               rr += (double)v[k] * (double)v[k];
+               tt += (double)s[k] * (double)s[k];
+            }
+            continue;
+         }
+      }
 #pragma unroll
       for (int k = 0; k < Rows::kR; k++) {
          const int64_t i = G.row(base, k);
@@ -2334,11 +2368,26 @@ __global__ void __launch_bounds__(kRedThreads)
    if (S->halt) return;
    const float beta = (float)(*rz_cur / S->rz);
    const float alpha = (float)S->alpha;
-   const auto tv = [t](int32_t c) { return __ldg(t + c); };
+   const PlainInput tv{t};
 #pragma unroll 1
    for (int64_t base = GT.first(); base < n; base += GT.step()) {
       float s[Rows::kR];
       GT.rows(base, n, tv, s);
+      if constexpr (Rows::kQuad) {
+         if (base + 3 < n) {
+            float4* pp = reinterpret_cast<float4*>(p + base);
+            float4* xp = reinterpret_cast<float4*>(xc + base);
+            const float4 po = *pp;
+            float4 xo = *xp;
+            xo.x += alpha * po.x;
+            xo.y += alpha * po.y;
+            xo.z += alpha * po.z;
+            xo.w += alpha * po.w;
+            *xp = xo;
+            *pp = make_float4(s[0] + beta * po.x, s[1] + beta * po.y, s[2] + beta * po.z, s[3] + beta * po.w);
+            continue;
+         }
+      }
 #pragma unroll
       for (int k = 0; k < Rows::kR; k++) {
          const int64_t i = GT.row(base, k);
@@ -2551,6 +2600,8 @@ tnlb_status reliable_t(const tnlb_segments* seg, const int32_t* cols, const doub
    const bool fused_u = cmp_m;
    DeviceBuffer r2;
    if (fused_u) TNLB_TRY_STATUS(r2.alloc(sizeof(float) * n));
+   TNLB_REQUIRE(!fused_u || aligned16(tvec), TNLB_ERR_INVALID_ARGUMENT,
+                "solve_mixed_reliable: the FSAI work vector must be 16-byte aligned");
 
    // z = M^-1 r, (r, z) into rz_cur and p = z + beta p (beta = (r, z) /
    // S->rz); a short-row symmetric FSAI does it in two fused products
