@@ -794,7 +794,7 @@ def solve_mixed_reliable(M: SparseMatrix, b: torch.Tensor, x: torch.Tensor, tol:
     ``layout`` picks the internal FP32 copies of short-row matrices: "auto"
     stores a matrix with few diagonals by diagonal, others as CSR with
     16-bit column offsets; "offsets" always the latter.  Both give the same
-    iterates.
+    row sums bit for bit (their FP64 dot products group rows differently).
     """
     if M.real != torch.float64:
         raise TypeError("solve_mixed_reliable takes an FP64 matrix")
