@@ -236,14 +236,17 @@ def _nine_point(N):
 
 
 @pytest.mark.parametrize("inner", ["fsai", "jacobi", "none"])
-def test_reliable_layouts_give_the_same_iterates(inner):
-    """The reliable-update PCG's internal FP32 copies by diagonal (5 for A,
-    3 for the FSAI factors here) and with 16-bit column offsets sum the same
-    terms in the same order: iterations, updates and x agree bit for bit."""
+@pytest.mark.parametrize("dim", [2, 3])
+def test_reliable_layouts_give_the_same_iterates(inner, dim):
+    """The reliable-update PCG's internal FP32 copies by diagonal (2D: 5 for
+    A, 3 for the FSAI factors, four rows per thread; 3D: 7 for A, one row
+    per thread, 4 for the factors) and with 16-bit column offsets sum the
+    same terms in the same order: on these sizes iterations, updates and x
+    agree bit for bit."""
     from tnl_b200 import generators as g
 
     t = tnl()
-    A = g.diffusion_2d(80, 0.1, 2.0, 5)
+    A = g.diffusion_2d(80, 0.1, 2.0, 5) if dim == 2 else g.diffusion_3d(18, 0.1, 2.0, 5)
     b = g.uniform_vector(A.n, 1)
     M = t.SparseMatrix(t.CSR, torch.float64).assign(A.rowptr, A.cols, A.vals)
     bs = torch.tensor(b, device="cuda")

@@ -19,6 +19,7 @@
 #include <cuda_fp16.h>
 
 #include <cstdint>
+#include <type_traits>
 
 namespace tnlb {
 
@@ -160,6 +161,43 @@ struct DiaRows {
    }
 };
 
+// Diagonal layout, one row per thread (for 6 to 8 diagonals, where the
+// four-row form's registers -- 77 at 7 diagonals -- cut the resident warps
+// and measured slower on the 7-point 256^3 operator): every load of a warp
+// one contiguous run, the D value and D input loads issued before the sum.
+template <typename TV, int D>
+struct DiaRow1 {
+   static constexpr int kR = 1;
+   static constexpr bool kQuad = false;
+   const TV* __restrict__ vals;
+   DiaOffsets d;
+   int64_t pitch;
+
+   __device__ __forceinline__ int64_t first() const { return (int64_t)blockIdx.x * blockDim.x + threadIdx.x; }
+   __device__ __forceinline__ int64_t step() const { return (int64_t)gridDim.x * blockDim.x; }
+   __device__ __forceinline__ int64_t row(int64_t base, int) const { return base; }
+
+   template <typename XV>
+   __device__ __forceinline__ void rows(int64_t base, int32_t nr, const XV& xv, float (&s)[1]) const
+   {
+      const int32_t i = (int32_t)base;
+      const bool rin = base < nr;
+      const TV* vp = vals + i;
+      float v[D], x[D];
+#pragma unroll
+      for (int j = 0; j < D; j++) {
+         const int32_t c = i + d.o[j];
+         const bool in = rin && (uint32_t)c < (uint32_t)nr;
+         v[j] = in ? rel_to_f(__ldg(vp + (int64_t)j * pitch)) : 0.0f;
+         x[j] = in ? xv(c) : 0.0f;
+      }
+      float t = 0.0f;
+#pragma unroll
+      for (int j = 0; j < D; j++) t += v[j] * x[j];
+      s[0] = t;
+   }
+};
+
 // Rows per thread: two for up to 8 entries a row, as the short-row sweep on
 // the 5-point operator and its triangular factor favoured (FP16 values:
 // 25 -> 19 us on the factor).
@@ -221,7 +259,7 @@ constexpr int rel_rows_per_thread()
    do {                                                                                                \
       if ((C).kind == CompactCopy::kDia) {                                                             \
          TNLB_DIA_WIDTH((C).width, {                                                                   \
-            using Rows = DiaRows<TV, D>;                                                               \
+            using Rows = std::conditional_t<(D <= 5), DiaRows<TV, D>, DiaRow1<TV, D>>;                 \
             DiaOffsets dd_;                                                                            \
             for (int q_ = 0; q_ < 8; q_++) dd_.o[q_] = (C).diag[q_];                                   \
             const Rows rows_{(C).vals.template as<TV>(), dd_, (C).pitch};                              \
