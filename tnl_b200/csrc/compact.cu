@@ -132,6 +132,7 @@ __global__ void __launch_bounds__(256) k_cmp_dot(Rows A, const float* __restrict
    double d = 0.0;
 #pragma unroll 1
    for (int64_t base = A.first(); base < n; base += A.step()) {
+      A.prefetch(base + A.step(), n);
       float s[Rows::kR];
       A.rows(base, n, xv, s);
       if constexpr (Rows::kQuad) {
@@ -172,6 +173,7 @@ __global__ void __launch_bounds__(256) k_cmp_xpby(Rows A, const float* __restric
    const PlainInput xv{x};
 #pragma unroll 1
    for (int64_t base = A.first(); base < n; base += A.step()) {
+      A.prefetch(base + A.step(), n);
       float s[Rows::kR];
       A.rows(base, n, xv, s);
       if constexpr (Rows::kQuad) {

@@ -39,6 +39,7 @@ struct RelRows {
    __device__ __forceinline__ int64_t first() const { return ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * R; }
    __device__ __forceinline__ int64_t step() const { return (int64_t)gridDim.x * blockDim.x * R; }
    __device__ __forceinline__ int64_t row(int64_t base, int k) const { return base + k; }
+   __device__ __forceinline__ void prefetch(int64_t, int32_t) const {}
 
    template <typename XV>
    __device__ __forceinline__ void rows(int64_t r0, int32_t n, const XV& xv, float (&s)[R]) const
@@ -124,6 +125,16 @@ struct DiaRows {
    }
    __device__ __forceinline__ int64_t step() const { return (int64_t)gridDim.x * blockDim.x * 4; }
    __device__ __forceinline__ int64_t row(int64_t base, int k) const { return base + k; }
+   // L2 prefetch of the value lines of the pass at `base` (one thread per
+   // 128-byte line), issued a pass ahead so that its loads find them in L2.
+   __device__ __forceinline__ void prefetch(int64_t base, int32_t nr) const
+   {
+      constexpr int kPerLine = 128 / (4 * (int)sizeof(TV));
+      if (base >= nr || (threadIdx.x & (kPerLine - 1)) != 0) return;
+#pragma unroll
+      for (int j = 0; j < D; j++)
+         asm volatile("prefetch.global.L2 [%0];" ::"l"(vals + (int64_t)j * pitch + base));
+   }
 
    template <typename XV>
    __device__ __forceinline__ void rows(int64_t base, int32_t nr, const XV& xv, float (&s)[4]) const
@@ -176,6 +187,7 @@ struct DiaRow1 {
    __device__ __forceinline__ int64_t first() const { return (int64_t)blockIdx.x * blockDim.x + threadIdx.x; }
    __device__ __forceinline__ int64_t step() const { return (int64_t)gridDim.x * blockDim.x; }
    __device__ __forceinline__ int64_t row(int64_t base, int) const { return base; }
+   __device__ __forceinline__ void prefetch(int64_t, int32_t) const {}
 
    template <typename XV>
    __device__ __forceinline__ void rows(int64_t base, int32_t nr, const XV& xv, float (&s)[1]) const

@@ -2310,6 +2310,7 @@ __global__ void __launch_bounds__(kRedThreads)
    double rr = 0, tt = 0;
 #pragma unroll 1
    for (int64_t base = G.first(); base < n; base += G.step()) {
+      G.prefetch(base + G.step(), n);
       float s[Rows::kR];
       G.rows(base, n, rv, s);
       if constexpr (Rows::kQuad) {
@@ -2371,6 +2372,7 @@ __global__ void __launch_bounds__(kRedThreads)
    const PlainInput tv{t};
 #pragma unroll 1
    for (int64_t base = GT.first(); base < n; base += GT.step()) {
+      GT.prefetch(base + GT.step(), n);
       float s[Rows::kR];
       GT.rows(base, n, tv, s);
       if constexpr (Rows::kQuad) {
