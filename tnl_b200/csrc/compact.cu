@@ -123,7 +123,7 @@ __global__ void k_diag_fill(const int32_t* __restrict__ rowptr, const int32_t* _
 // Four-row policies (kQuad) store and read the rows' own entries as
 // vectors when all four rows exist (the vectors are 16-byte aligned).
 template <typename Rows>
-__global__ void __launch_bounds__(256) k_cmp_dot(Rows A, const float* __restrict__ x, float* __restrict__ y, int32_t n,
+__global__ void __launch_bounds__(256, Rows::kMinBlocks) k_cmp_dot(Rows A, const float* __restrict__ x, float* __restrict__ y, int32_t n,
                                                  RedWork w, double* __restrict__ dot_out,
                                                  const int32_t* __restrict__ skip, int self)
 {
@@ -164,7 +164,7 @@ __global__ void __launch_bounds__(256) k_cmp_dot(Rows A, const float* __restrict
 
 // y = A x + (num / den) y, as k_csr_short_xpby does.
 template <typename Rows>
-__global__ void __launch_bounds__(256) k_cmp_xpby(Rows A, const float* __restrict__ x, float* __restrict__ y,
+__global__ void __launch_bounds__(256, Rows::kMinBlocks) k_cmp_xpby(Rows A, const float* __restrict__ x, float* __restrict__ y,
                                                   int32_t n, const double* __restrict__ num,
                                                   const double* __restrict__ den, const int32_t* __restrict__ skip)
 {

@@ -32,6 +32,7 @@ template <typename TV, int L, int R>
 struct RelRows {
    static constexpr int kR = R;
    static constexpr bool kQuad = false;
+   static constexpr int kMinBlocks = 0;  // no residency asked for
    const int32_t* __restrict__ rowptr;
    const int16_t* __restrict__ off;
    const TV* __restrict__ vals;
@@ -115,6 +116,9 @@ template <typename TV, int D>
 struct DiaRows {
    static constexpr int kR = 4;
    static constexpr bool kQuad = true;
+   // resident 256-thread blocks per SM asked for (0: none); 5 for the
+   // 3-diagonal FSAI factors of a 5-point operator (48 registers)
+   static constexpr int kMinBlocks = D <= 3 ? 5 : 0;
    const TV* __restrict__ vals;
    DiaOffsets d;
    int64_t pitch;
@@ -180,6 +184,7 @@ template <typename TV, int D>
 struct DiaRow1 {
    static constexpr int kR = 1;
    static constexpr bool kQuad = false;
+   static constexpr int kMinBlocks = 0;  // no residency asked for
    const TV* __restrict__ vals;
    DiaOffsets d;
    int64_t pitch;

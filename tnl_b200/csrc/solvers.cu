@@ -2297,7 +2297,7 @@ struct RuNextInput {
 // reads p anyway -- or, when this iteration raises `halt`, to the fold of
 // the reliable update (k_ru_fold_p).
 template <typename Rows>
-__global__ void __launch_bounds__(kRedThreads)
+__global__ void __launch_bounds__(kRedThreads, Rows::kMinBlocks)
    k_ru_g_update(Rows G, const float* __restrict__ r, const float* __restrict__ Ap, float* __restrict__ rn,
                  float* __restrict__ t, int32_t n, RedWork w, RuState* S, double* __restrict__ rz_cur,
                  const double* __restrict__ pap)
@@ -2362,7 +2362,7 @@ __global__ void __launch_bounds__(kRedThreads)
 // p = G^T t + beta p (beta = (r, z)_new / (r, z)_old) on the compact copy of
 // G^T, and xc += alpha p with the p that alpha was formed for.
 template <typename Rows>
-__global__ void __launch_bounds__(kRedThreads)
+__global__ void __launch_bounds__(kRedThreads, Rows::kMinBlocks)
    k_ru_gt_xpby(Rows GT, const float* __restrict__ t, float* __restrict__ p, float* __restrict__ xc, int32_t n,
                 const double* __restrict__ rz_cur, const RuState* S)
 {
