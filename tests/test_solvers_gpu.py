@@ -263,6 +263,28 @@ def test_reliable_layouts_give_the_same_iterates(inner, dim):
         t.solve_mixed_reliable(M, bs, torch.zeros_like(bs), layout="dense")
 
 
+def test_reliable_fsai_factor_copies_do_not_overflow():
+    """The FP16 copies of the FSAI factors are stored times a power of two
+    that keeps them in range: on A * 2^-40 (factor entries near 2^20, past
+    FP16's 65504) the solve converges with the iterations and updates of the
+    unscaled one, every scaling being exact."""
+    from tnl_b200 import generators as g
+
+    t = tnl()
+    A = g.diffusion_2d(64, 0.1, 2.0, 9)
+    b = g.uniform_vector(A.n, 1)
+    bs = torch.tensor(b, device="cuda")
+    out = []
+    for scale in (1.0, 2.0 ** -40):
+        M = t.SparseMatrix(t.CSR, torch.float64).assign(A.rowptr, A.cols, A.vals * scale)
+        xs = torch.zeros(A.n, dtype=torch.float64, device="cuda")
+        r = t.solve_mixed_reliable(M, bs, xs, tol=1e-8, delta=0.1, inner="fsai")
+        assert r["converged"] and not r["breakdown"], (scale, r)
+        assert t.true_residual(M, bs, xs) < 1e-8
+        out.append(r)
+    assert (out[0]["iterations"], out[0]["reliable_updates"]) == (out[1]["iterations"], out[1]["reliable_updates"])
+
+
 @pytest.mark.parametrize("vec64", [False, True])
 def test_reliable_mixed_pcg_fsai_matches_oracle(oracle, vec64):
     """The reliable-update PCG with an FP32 FSAI against its oracle

@@ -17,6 +17,8 @@
 // kernels do; both layouts give the same bits (see compact.cuh).
 #include <algorithm>
 #include <climits>
+#include <cmath>
+#include <cstring>
 #include <vector>
 
 #include "compact.cuh"
@@ -47,10 +49,23 @@ __global__ void k_rel_offsets(const int32_t* __restrict__ rowptr, const int32_t*
    }
 }
 
-__global__ void k_to_half(const float* __restrict__ a, int64_t n, __half* __restrict__ b)
+__global__ void k_to_half(const float* __restrict__ a, int64_t n, float scale, __half* __restrict__ b)
 {
    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-      b[i] = __float2half_rn(a[i]);
+      b[i] = __float2half_rn(a[i] * scale);
+}
+
+// *out = max |a| as the bits of a non-negative float (their integer order
+// is the float order); NaN entries are skipped.
+__global__ void k_absmax(const float* __restrict__ a, int64_t n, unsigned* __restrict__ out)
+{
+   unsigned m = 0u;
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+      const float v = fabsf(a[i]);
+      if (v == v) m = max(m, __float_as_uint(v));
+   }
+   for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+   if ((threadIdx.x & 31) == 0 && m) atomicMax(out, m);
 }
 
 __global__ void k_diag_table_init(int32_t* __restrict__ tab, int32_t* __restrict__ flag)
@@ -107,7 +122,7 @@ __global__ void __launch_bounds__(256) k_diag_scan(const int32_t* __restrict__ r
 template <typename TV>
 __global__ void k_diag_fill(const int32_t* __restrict__ rowptr, const int32_t* __restrict__ cols,
                             const float* __restrict__ v, int32_t n, DiaOffsets d, int32_t nd, int64_t pitch,
-                            TV* __restrict__ out)
+                            float scale, TV* __restrict__ out)
 {
    const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
    if (r >= n) return;
@@ -115,7 +130,7 @@ __global__ void k_diag_fill(const int32_t* __restrict__ rowptr, const int32_t* _
       const int32_t o = cols[k] - (int32_t)r;
       int32_t j = 0;
       while (j < nd - 1 && d.o[j] != o) j++;
-      out[(int64_t)j * pitch + r] = (TV)v[k];
+      out[(int64_t)j * pitch + r] = (TV)(v[k] * scale);
    }
 }
 
@@ -211,8 +226,8 @@ void launch_cmp_xpby(const Rows& rows, int32_t n, const float* x, float* y, cons
 }
 
 // The diagonal layout, when the matrix has one: *ok false otherwise.
-tnlb_status diag_build(const tnlb_segments* seg, const int32_t* cols, const float* vals, bool half, cudaStream_t st,
-                       CompactCopy* out, bool* ok)
+tnlb_status diag_build(const tnlb_segments* seg, const int32_t* cols, const float* vals, bool half, float scale,
+                       cudaStream_t st, CompactCopy* out, bool* ok)
 {
    *ok = false;
    const int32_t n = seg->n;
@@ -245,10 +260,10 @@ tnlb_status diag_build(const tnlb_segments* seg, const int32_t* cols, const floa
    TNLB_CUDA_TRY(cudaMemsetAsync(out->vals.ptr, 0, bytes, st));
    if (half)
       k_diag_fill<__half><<<grid_for(n, 256), 256, 0, st>>>(rp, cols, vals, n, dd, (int32_t)d.size(), pitch,
-                                                             out->vals.as<__half>());
+                                                             scale, out->vals.as<__half>());
    else
       k_diag_fill<float><<<grid_for(n, 256), 256, 0, st>>>(rp, cols, vals, n, dd, (int32_t)d.size(), pitch,
-                                                            out->vals.as<float>());
+                                                            1.0f, out->vals.as<float>());
    TNLB_CHECK_LAUNCH();
    out->kind = CompactCopy::kDia;
    out->n = n;
@@ -263,14 +278,36 @@ tnlb_status diag_build(const tnlb_segments* seg, const int32_t* cols, const floa
 
 }  // namespace
 
-tnlb_status compact_build(const tnlb_segments* seg, const int32_t* cols, const float* vals, bool half, bool allow_dia,
-                          cudaStream_t st, CompactCopy* out)
+tnlb_status half_scale(const float* vals, int64_t nnz, cudaStream_t st, float* scale)
+{
+   *scale = 1.0f;
+   if (nnz <= 0) return TNLB_OK;
+   DeviceBuffer m;
+   TNLB_TRY_STATUS(m.alloc(sizeof(unsigned)));
+   TNLB_CUDA_TRY(cudaMemsetAsync(m.ptr, 0, sizeof(unsigned), st));
+   k_absmax<<<grid_for(nnz, 256 * 8), 256, 0, st>>>(vals, nnz, m.as<unsigned>());
+   TNLB_CHECK_LAUNCH();
+   unsigned h = 0;
+   TNLB_CUDA_TRY(cudaMemcpyAsync(&h, m.ptr, sizeof(h), cudaMemcpyDeviceToHost, st));
+   TNLB_CUDA_TRY(cudaStreamSynchronize(st));
+   float mx;
+   std::memcpy(&mx, &h, sizeof(mx));
+   if (!(mx > 0.0f) || !std::isfinite(mx)) return TNLB_OK;
+   int e = 0;
+   std::frexp(mx, &e);  // mx < 2^e
+   *scale = std::ldexp(1.0f, 14 - e);
+   return TNLB_OK;
+}
+
+tnlb_status compact_build(const tnlb_segments* seg, const int32_t* cols, const float* vals, bool half, float scale,
+                          bool allow_dia, cudaStream_t st, CompactCopy* out)
 {
    out->kind = CompactCopy::kNone;
    if (!spmv_dot_fusable(seg)) return TNLB_OK;
+   if (!half) scale = 1.0f;
    if (allow_dia) {
       bool ok = false;
-      TNLB_TRY_STATUS(diag_build(seg, cols, vals, half, st, out, &ok));
+      TNLB_TRY_STATUS(diag_build(seg, cols, vals, half, scale, st, out, &ok));
       if (ok) return TNLB_OK;
    }
    const int32_t n = seg->n;
@@ -287,7 +324,7 @@ tnlb_status compact_build(const tnlb_segments* seg, const int32_t* cols, const f
    TNLB_CHECK_LAUNCH();
    if (half) {
       TNLB_TRY_STATUS(out->vals.alloc(sizeof(__half) * (nnz > 0 ? nnz : 1)));
-      k_to_half<<<grid_for(nnz, 256 * 8), 256, 0, st>>>(vals, nnz, out->vals.as<__half>());
+      k_to_half<<<grid_for(nnz, 256 * 8), 256, 0, st>>>(vals, nnz, scale, out->vals.as<__half>());
       TNLB_CHECK_LAUNCH();
    }
    else {

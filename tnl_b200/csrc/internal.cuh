@@ -308,9 +308,14 @@ struct CompactCopy {
 inline bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
 // Builds the copy (kind kNone when the matrix is not short-row CSR or a
 // column lies 32768 or more from its row): kDia when allowed and the
-// diagonals hold at least 3/4 of their slots, else kRel.
-tnlb_status compact_build(const tnlb_segments* seg, const int32_t* cols, const float* vals, bool half, bool allow_dia,
-                          cudaStream_t st, CompactCopy* out);
+// diagonals hold at least 3/4 of their slots, else kRel.  FP16 values
+// (`half`) are stored times `scale`.
+tnlb_status compact_build(const tnlb_segments* seg, const int32_t* cols, const float* vals, bool half, float scale,
+                          bool allow_dia, cudaStream_t st, CompactCopy* out);
+// The power of two that brings the largest |vals| into [2^13, 2^14): FP16
+// copies times it neither overflow nor lose normal-range precision (1 for
+// an all-zero array).
+tnlb_status half_scale(const float* vals, int64_t nnz, cudaStream_t st, float* scale);
 // y = A x and (x, y) -- (y, y) with self_dot -- into *dot_out.
 tnlb_status compact_spmv_dot(const CompactCopy& A, const float* x, float* y, double* partials, unsigned* counter,
                              double* dot_out, cudaStream_t st, const int32_t* skip, bool self_dot);

@@ -2584,13 +2584,17 @@ tnlb_status reliable_t(const tnlb_segments* seg, const int32_t* cols, const doub
    CompactCopy cA, cG, cGT;
    const bool compact_dia = prm.reliable_layout == 0;
    if (kVec == TNLB_F32) {
-      if (fused_a) TNLB_TRY_STATUS(compact_build(seg, cols, v32f, false, compact_dia, st, &cA));
+      if (fused_a) TNLB_TRY_STATUS(compact_build(seg, cols, v32f, false, 1.0f, compact_dia, st, &cA));
       if (fused_m) {
+         // G and G^T in FP16 times one power of two (PCG's iterates do not
+         // change when M is scaled), so that no entry overflows
          const FsaiView fv = fsai_view(pobj->fsai);
-         TNLB_TRY_STATUS(compact_build(fv.g, fv.gcols, (const float*)fv.gvals, true, compact_dia, st, &cG));
+         float gs = 1.0f;
+         TNLB_TRY_STATUS(half_scale((const float*)fv.gvals, fv.g->elements, st, &gs));
+         TNLB_TRY_STATUS(compact_build(fv.g, fv.gcols, (const float*)fv.gvals, true, gs, compact_dia, st, &cG));
          if (cG.kind != CompactCopy::kNone)
             TNLB_TRY_STATUS(
-               compact_build(fv.gt, fv.gtcols, (const float*)fv.gtvals, true, compact_dia, st, &cGT));
+               compact_build(fv.gt, fv.gtcols, (const float*)fv.gtvals, true, gs, compact_dia, st, &cGT));
       }
    }
    const bool cmp_a = cA.kind != CompactCopy::kNone;
