@@ -159,3 +159,40 @@ def test_matrix_file_header_of_reference_files(tmp_path):
     info = _capi.MatrixFileInfo()
     assert _capi.tnlb_matrix_file_info_read(str(bad).encode(), C.byref(info)) == _capi.ERR_IO
     assert b"magic number" in _capi.tnlb_last_error()
+
+
+def test_ctypes_structs_match_the_c_header(tmp_path):
+    """Every struct the Python layer mirrors with ctypes has the size and
+    field offsets that a C compiler gives the declaration in
+    include/tnlb200.h (gcc on a generated probe)."""
+    import ctypes as C
+    import shutil
+    import subprocess
+
+    from tnl_b200 import _capi
+
+    if shutil.which("gcc") is None:
+        pytest.skip("no C compiler")
+    mirrors = {
+        "tnlb_solver_params": _capi.SolverParams,
+        "tnlb_solve_result": _capi.SolveResult,
+        "tnlb_segments_info": _capi.SegmentsInfo,
+        "tnlb_acsr_block": _capi.AcsrBlock,
+        "tnlb_host_csr": _capi.HostCSR,
+        "tnlb_matrix_file_info": _capi.MatrixFileInfo,
+    }
+    lines = ['#include "tnlb200.h"', "#include <stdio.h>", "#include <stddef.h>", "int main(void) {"]
+    expected = []
+    for cname, py in mirrors.items():
+        lines.append(f'   printf("%zu\\n", sizeof({cname}));')
+        expected.append(C.sizeof(py))
+        for field, _ in py._fields_:
+            lines.append(f'   printf("%zu\\n", offsetof({cname}, {field}));')
+            expected.append(getattr(py, field).offset)
+    lines += ["   return 0;", "}"]
+    src = tmp_path / "abi_probe.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "abi_probe"
+    subprocess.run(["gcc", "-std=c99", f"-I{ROOT / 'include'}", str(src), "-o", str(exe)], check=True)
+    got = [int(v) for v in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
+    assert got == expected
