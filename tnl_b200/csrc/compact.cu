@@ -14,7 +14,9 @@
 //                     plus the row offsets, against 8 in the FP32 CSR.
 //
 // Rows are summed in FP32 in ascending column order, as the CSR short-row
-// kernels do; both layouts give the same bits (see compact.cuh).
+// kernels do; both layouts give the same row sums bit for bit (see
+// compact.cuh).  FP16 copies are stored times a power of two (half_scale)
+// that keeps their largest entry below 2^14.
 #include <algorithm>
 #include <climits>
 #include <cmath>

@@ -10,10 +10,17 @@
 //   row(base, k)      row k of the pass (rows at or past n are skipped);
 //   rows(base, n, xv, s)  s[k] = sum over the row's entries of v * xv(c),
 //                     xv(c) the input at column c, summed in FP32 in
-//                     ascending column order.
-// Both layouts sum the same terms in the same order -- a missing diagonal
-// slot adds fma(0, x, s) = s -- so for finite inputs their results are
-// bitwise equal.
+//                     ascending column order;
+//   prefetch(base, n) an L2 prefetch of the values of the pass at `base`
+//                     (issued a pass ahead; a no-op where it did not pay);
+//   kQuad             four consecutive full rows may be read and written
+//                     as 16-byte vectors by the kernel's epilogue;
+//   kMinBlocks        resident blocks per SM the kernels ask for (0: none).
+// Policies: RelRows (16-bit offsets, two consecutive rows per thread),
+// DiaRows (diagonals, four consecutive rows, up to 5 diagonals), DiaRow1
+// (diagonals, one row, 6 to 8 diagonals).  All sum the same terms in the
+// same order -- a missing diagonal slot adds fma(0, x, s) = s -- so for
+// finite inputs their row sums are bitwise equal.
 #pragma once
 
 #include <cuda_fp16.h>
