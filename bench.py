@@ -23,6 +23,15 @@ cpu_baseline -- the reference's own Host/OpenMP vectorProduct on the host
              else the oracle's C restatement; a bounded sample of repeated
              products of the same matrix.
 
+solver    -- BASELINE's second metric, PCG time to an FP64 true residual of
+             1e-8 on the learned-preconditioner evaluation problem (2D
+             diffusion, 2048 x 2048, GRF coefficients): FP64 Jacobi-PCG
+             against FP32 PCG with reliable FP64 updates and the learned
+             (or classical) FSAI, with iterations, set-up time, true residual
+             and the error against a tightly converged FP64 solution.  The
+             reference arm times the reference's Host CG + Jacobi on the same
+             problem over a bounded number of iterations.
+
 With --gpus N > 1 (under torchrun) every rank runs an independent replica
 (the 1-GPU path has no exchange step); value = total bytes / max time.
 """
@@ -136,9 +145,24 @@ def dist_env():
     return world, rank, local
 
 
-def make_matrix():
-    from tnl_b200 import generators as g
+def generators():
+    """tnl_b200/generators.py loaded by path.  Importing it as a submodule of
+    the package would run tnl_b200/__init__.py, which loads libtnlb200.so;
+    the reference arm must not map the library at all."""
+    import importlib.util
 
+    mod = sys.modules.get("tnl_b200_generators_by_path")
+    if mod is None:
+        spec = importlib.util.spec_from_file_location("tnl_b200_generators_by_path",
+                                                      ROOT / "tnl_b200" / "generators.py")
+        mod = importlib.util.module_from_spec(spec)
+        sys.modules[spec.name] = mod
+        spec.loader.exec_module(mod)
+    return mod
+
+
+def make_matrix():
+    g = generators()
     A = g.power_law(N_ROWS, ZIPF, CAP, SEED_A)
     x = g.uniform_vector(A.ncols, SEED_X)
     return A, x
@@ -178,6 +202,138 @@ def cpu_baseline_run(A, x, target_seconds=10.0, max_reps=400):
                       f"({A.nnz} nonzeros), {t * 1e3:.2f} ms each"}
 
 
+SOLVER_N, SOLVER_SEED, SOLVER_TOL = 2048, 1234, 1e-8
+WEIGHTS = ROOT / "tnl_b200" / "weights" / "lfsai_diffusion.npy"
+
+
+def solver_problem():
+    """The learned-preconditioner evaluation problem: 2D 5-point diffusion on
+    a 2048 x 2048 grid (n = 4,194,304), GRF coefficients with correlation
+    length and sigma drawn from the seed, b ~ U[-1, 1) (seed 1)."""
+    g = generators()
+    A = g.diffusion_2d_problem(SOLVER_N, SOLVER_SEED)
+    return A, g.uniform_vector(A.n, 1)
+
+
+def solver_leg():
+    """PCG time to an FP64 true residual ||b - A x|| / ||b|| <= 1e-8 on one
+    B200 (CUDA events around each call on the launching stream), every
+    method warmed up by one 20-iteration run first:
+      * FP64 Jacobi-PCG, its convergence residue halved until the TRUE
+        residual is below 1e-8 (the reference's rule stops on the
+        preconditioned residue);
+      * FP32 PCG with reliable FP64 updates and the learned FSAI (network
+        inference on the GPU = set-up), and the same with classical FSAI;
+    plus each solution's error against a tightly converged FP64 solve."""
+    import torch
+
+    import tnl_b200 as t
+    from tnl_b200.lfsai import LearnedFSAI
+
+    A, bh = solver_problem()
+    M = t.SparseMatrix.from_csr(A, real=torch.float64)
+    n = A.n
+    b = torch.tensor(bh, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return r, e0.elapsed_time(e1)
+
+    def zeros():
+        return torch.zeros(n, dtype=torch.float64, device="cuda")
+
+    def pcg(P, tol, maxit=200000):
+        S = t.CG()
+        S.setMatrix(M)
+        S.setPreconditioner(P)
+        S.setConvergenceResidue(tol)
+        S.setMaxIterations(maxit)
+        return S
+
+    # FP64 reference solution for the error figures
+    Pj = t.Diagonal()
+    Pj.update(M)
+    xref = zeros()
+    pcg(Pj, 1e-13).solve(b, xref)
+    xref_norm = float(torch.linalg.vector_norm(xref))
+
+    def err(x):
+        return float(torch.linalg.vector_norm(x - xref)) / xref_norm
+
+    _, jac_setup = timed(lambda: Pj.update(M))
+    pcg(Pj, SOLVER_TOL, 20).solve(b, zeros())
+    tol = SOLVER_TOL
+    while True:
+        S = pcg(Pj, tol)
+        x = zeros()
+        S.solve(b, x)
+        if t.true_residual(M, b, x) < SOLVER_TOL or tol < 1e-12:
+            break
+        tol *= 0.5
+    x = zeros()
+    ok, ms = timed(lambda: S.solve(b, x))
+    fp64 = {"method": "FP64 Jacobi-PCG", "solve_ms": ms, "setup_ms": jac_setup, "iterations": S.getIterations(),
+            "converged": bool(ok), "true_residual": t.true_residual(M, b, x), "convergence_residue": tol,
+            "error_vs_fp64_solution": err(x)}
+
+    A32 = t.SparseMatrix(t.CSR, torch.float32)
+    A32.assign(A.rowptr, A.cols, A.vals.astype(np.float32))
+
+    def reliable(name, make_prec):
+        P, setup = make_prec()
+        t.solve_mixed_reliable(M, b, zeros(), tol=SOLVER_TOL, inner=P, max_iterations=20)
+        x = zeros()
+        r, ms = timed(lambda: t.solve_mixed_reliable(M, b, x, tol=SOLVER_TOL, delta=0.3, inner=P))
+        return {"method": name, "solve_ms": ms, "setup_ms": setup, "iterations": r["iterations"],
+                "reliable_updates": r["reliable_updates"], "converged": bool(r["converged"]),
+                "true_residual": t.true_residual(M, b, x), "error_vs_fp64_solution": err(x),
+                "speedup_vs_fp64_jacobi": fp64["solve_ms"] / ms,
+                "speedup_with_setup": (fp64["solve_ms"] + fp64["setup_ms"]) / (ms + setup)}
+
+    net = LearnedFSAI(seed=0)
+    net.load(WEIGHTS)
+
+    def learned():
+        net.preconditioner(A32)  # first call loads the network's kernels
+        return timed(lambda: net.preconditioner(A32))
+
+    def classical():
+        P = t.FSAI()
+        P.update(A32)
+        P = t.FSAI()
+        _, s = timed(lambda: P.update(A32))
+        return P, s
+
+    lrn = reliable("FP32 PCG with reliable FP64 updates, learned FSAI", learned)
+    cls = reliable("FP32 PCG with reliable FP64 updates, classical FSAI", classical)
+    return {"problem": f"2D diffusion {SOLVER_N}x{SOLVER_N} (n={n}, nnz={A.nnz}), GRF coefficients, seed "
+                       f"{SOLVER_SEED}; b ~ U[-1,1) seed 1", "tol": SOLVER_TOL,
+            "fp64_jacobi_pcg": fp64, "learned_fsai_mixed": lrn, "classical_fsai_mixed": cls}
+
+
+def reference_solver_leg(iterations=200):
+    """The reference's Host CG with Jacobi on the same problem, timed over a
+    bounded number of iterations (a full solve takes thousands)."""
+    from oracle.oracle import REF_SO, Reference  # reference arm only
+
+    if not REF_SO.exists():
+        return None
+    A, b = solver_problem()
+    R = Reference()
+    r = R.solve("cg", A, b, precond=1, tol=1e-30, maxit=iterations)
+    return {"problem": f"2D diffusion {SOLVER_N}x{SOLVER_N} (n={A.n}, nnz={A.nnz}), seed {SOLVER_SEED}",
+            "method": "reference Host CG + Diagonal (Jacobi), OpenMP", "cores": R.threads(),
+            "iterations_timed": r["iterations"], "seconds": r["seconds"],
+            "ms_per_iteration": r["seconds"] * 1e3 / max(1, r["iterations"]),
+            "sample": f"{iterations} iterations of a solve, not run to the tolerance"}
+
+
 def run_reference(args):
     world, rank, local = dist_env()
     if rank != 0:
@@ -190,6 +346,8 @@ def run_reference(args):
             "config": config_dict(A),
             "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": "GB/s", "h2d_bytes_per_step": 0,
                                         "d2h_bytes_per_step": 0}}
+    if not args.no_solver:
+        line["solver"] = reference_solver_leg()
     print(json.dumps(line), flush=True)
     return 0
 
@@ -335,6 +493,10 @@ def run_ours(args):
     }
     if not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline_run(A, x)
+    if not args.no_solver and world == 1:
+        del M, xs, ys, xd, yd
+        torch.cuda.empty_cache()
+        line["solver"] = solver_leg()
     print(json.dumps(line), flush=True)
     return 0
 
@@ -346,6 +508,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-solver", action="store_true", help="skip the PCG time-to-1e-8 leg")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -252,11 +252,14 @@ tnlb_status tnlb_spmv_transposed(const tnlb_segments* seg, tnlb_real real, const
  *
  * Limit: rows + nnz <= 67,108,864 (262,144 tiles of 256 rows + nonzeros);
  * larger matrices are rejected with TNLB_ERR_INVALID_ARGUMENT before any
- * launch.  Nothing in the scratch has to start at zero: every call rewrites
- * what it reads.  The first call on each device looks up the scratch address
- * (cudaGetSymbolAddress with that device current, which may load the
- * library's device code there); make one call per device before capturing a
- * stream.  Calls that overlap on one device -- on two streams, or from two
+ * launch.  nnz must equal d_rowptr[rows]: the value is not read back from
+ * the device, and a mismatch is undefined behaviour (the tiles are cut from
+ * nnz).  Nothing in the scratch has to start at zero: every call rewrites
+ * what it reads.  Every call looks up the scratch address in the current
+ * device's context (cudaGetSymbolAddress; nothing is cached, so a device
+ * reset leaves no stale address); the first call on a device may load the
+ * library's device code there, so make one call per device before capturing
+ * a stream.  Calls that overlap on one device -- on two streams, or from two
  * host threads -- share the scratch and race: order them on one stream.
  * Enqueues three kernels on `stream`; returns before they finish. */
 tnlb_status tnlb_spmv_csr_noalloc(tnlb_real real, int32_t rows, int32_t columns, int64_t nnz,

@@ -111,6 +111,21 @@ def test_mtx_errors_match_reference(tmp_path, reference):
         assert str(e_ours.value) == str(e_ref.value), name
 
 
+@pytest.mark.parametrize("line", ["0 1 1.0", "1 0 1.0", "-3 1 1.0", "1 -1 2.0", "x 1 1.0", "1 y 1.0",
+                                  "99999999999 1 1.0"])
+def test_mtx_rejects_positions_below_one_and_non_numbers(tmp_path, line):
+    """A row or column below 1, a word that is not a number, or one beyond
+    the int range is an I/O error, never a negative index into the CSR
+    arrays (x[-1] on the device, or a write before the row pointer)."""
+    import tnl_b200
+
+    f = tmp_path / "bad.mtx"
+    f.write_text(f"%%MatrixMarket matrix coordinate real general\n2 2 2\n1 1 4.0\n{line}\n")
+    with pytest.raises(RuntimeError) as e:
+        tnl_b200.read_mtx(f, False)
+    assert "out of the matrix dimensions" in str(e.value) or "not an integer" in str(e.value)
+
+
 def test_mtx_write_matches_reference_bytes(tmp_path, reference):
     """tnlb_mtx_write writes the bytes of the reference's MatrixWriter::writeMtx."""
     import tnl_b200

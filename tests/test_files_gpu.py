@@ -131,3 +131,27 @@ def test_load_refuses_another_type(reference, tmp_path):
         t.SparseMatrix(t.CSR, torch.float32).load(path)
     L = t.SparseMatrix(t.CSR, torch.float64).load(path)
     assert L.getRows() == A.n
+
+
+@pytest.mark.parametrize("bad_column", [-2, 100])
+def test_load_rejects_column_indexes_outside_the_matrix(tmp_path, bad_column):
+    """A file whose column array holds an index below the padding value -1
+    or at least the column count is reported as corrupt before anything is
+    copied to the device: the products gather x[column] unchecked."""
+    t = tnl()
+    from tnl_b200 import generators as g
+
+    A = g.laplacian_2d(10)
+    M = t.SparseMatrix(t.CSR, torch.float64).assign(A.rowptr, A.cols, A.vals, A.ncols)
+    good = tmp_path / "good.tnl"
+    M.save(good)
+    raw = good.read_bytes()
+    cols = np.ascontiguousarray(A.cols, np.int32).tobytes()
+    at = raw.find(cols)
+    assert at > 0 and raw.find(cols, at + 1) < 0
+    patched = raw[:at] + np.int32(bad_column).tobytes() + raw[at + 4:]
+    bad = tmp_path / "bad.tnl"
+    bad.write_bytes(patched)
+    with pytest.raises(RuntimeError, match="not a valid TNL sparse matrix file"):
+        t.SparseMatrix(t.CSR, torch.float64).load(bad)
+    assert t.SparseMatrix(t.CSR, torch.float64).load(good).getRows() == A.n

@@ -297,7 +297,10 @@ tnlb_status half_scale(const float* vals, int64_t nnz, cudaStream_t st, float* s
    if (!(mx > 0.0f) || !std::isfinite(mx)) return TNLB_OK;
    int e = 0;
    std::frexp(mx, &e);  // mx < 2^e
-   *scale = std::ldexp(1.0f, 14 - e);
+   // 2^(14-e) clamped to FP32's normal exponents, so the scale itself stays
+   // finite for entries far below 2^-113 (the copy then keeps them small
+   // rather than turning them into inf or NaN)
+   *scale = std::ldexp(1.0f, std::min(127, std::max(-126, 14 - e)));
    return TNLB_OK;
 }
 

@@ -564,7 +564,17 @@ extern "C" tnlb_status tnlb_matrix_load(const char* path, tnlb_segments** out, i
       if (!r.array(arr_real((tnlb_real)info.real), rs, vraw, &nv) || !r.array(kArrInt, 4, craw, &nc) ||
           nv != (uint64_t)info.storage || nc != (uint64_t)info.storage)
          s = corrupt(path);
-      else if (info.storage > 0) {
+      else {
+         // every stored column is padding (-1) or a column of the matrix:
+         // the products gather x[column] without a bounds check
+         const int32_t* c = reinterpret_cast<const int32_t*>(craw.data());
+         for (uint64_t k = 0; k < nc; k++)
+            if (c[k] < -1 || c[k] >= info.columns) {
+               s = corrupt(path);
+               break;
+            }
+      }
+      if (s == TNLB_OK && info.storage > 0) {
          if (cudaMemcpy(d_values, vraw.data(), vraw.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
              cudaMemcpy(d_cols, craw.data(), craw.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
             set_error("load: copy to the device failed");

@@ -6,8 +6,10 @@
 //    general|symmetric" (at least 5 space-separated words);
 //  * lines starting with '%' are comments; the size line has exactly three
 //    words; rows and columns must be positive;
-//  * words are separated by spaces only (tabs are not separators); numbers
-//    are read with atoi / atof;
+//  * words are separated by spaces only (tabs are not separators); sizes
+//    and values are read with atoi / atof; an element's row and column must
+//    start with an integer in [1, rows] and [1, columns] (an error
+//    otherwise, where the reference would index outside the matrix);
 //  * elements go through an ordered map keyed by (row, column): a repeated
 //    position keeps the last value, rows and columns come out sorted, and
 //    explicit zeros are kept;
@@ -16,6 +18,8 @@
 //    one; a general file cannot be read into symmetric storage;
 //  * the writer prints "row column value" with widths 9, 9, 12, default
 //    stream precision, 1-based, skipping zero values.
+#include <cerrno>
+#include <cstdint>
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
@@ -50,6 +54,20 @@ tnlb_status io_error(const std::string& msg)
 {
    tnlb::set_error(msg);
    return TNLB_ERR_IO;
+}
+
+// An element's row or column word, read as atoi reads it (leading digits,
+// anything after them ignored), but a word with no leading number is an
+// error rather than 0, and so is one outside the int range.
+bool parse_index(const std::string& w, int& out)
+{
+   errno = 0;
+   const char* begin = w.c_str();
+   char* end = nullptr;
+   const long v = std::strtol(begin, &end, 10);
+   if (end == begin || errno != 0 || v < INT32_MIN || v > INT32_MAX) return false;
+   out = (int)v;
+   return true;
 }
 
 }  // namespace
@@ -105,9 +123,13 @@ extern "C" tnlb_status tnlb_mtx_read(const char* path, int32_t symmetric_storage
       const auto w = split_spaces(line);
       if ((int)w.size() != 3 - (int)pattern)
          return io_error("Wrong number of parameters in the matrix row at line:" + line);
-      const int row = atoi(w[0].c_str()), column = atoi(w[1].c_str());
+      int row = 0, column = 0;
+      if (!parse_index(w[0], row) || !parse_index(w[1], column))
+         return io_error("The row or column of the element is not an integer at line:" + line);
       const double value = pattern ? 1.0 : atof(w[2].c_str());
-      if (column > columns || row > rows) {
+      // 1-based positions: a row or column below 1 is outside the matrix as
+      // much as one past its size (the reference would index row -1)
+      if (column > columns || row > rows || column < 1 || row < 1) {
          std::stringstream s;
          s << "There is an element at position " << row << ", " << column << " out of the matrix dimensions " << rows
            << " x " << columns << ".";

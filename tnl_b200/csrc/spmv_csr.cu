@@ -868,8 +868,6 @@ tnlb_status spmv_csr(const tnlb_segments* seg, tnlb_real real, const int32_t* co
 // nothing has to start at zero.  Calls that overlap on one device share the
 // array and race.
 
-#include <mutex>
-
 namespace {
 
 constexpr int64_t kNoAllocMaxTiles = 262144;  // rows + nonzeros <= 67,108,864
@@ -879,10 +877,6 @@ constexpr size_t kNoAllocCarryValBytes = round_up_256(sizeof(double) * kNoAllocM
 constexpr size_t kNoAllocPlanBytes = round_up_256(sizeof(int32_t) * (kNoAllocMaxTiles + 1));
 constexpr size_t kNoAllocCarryRowBytes = round_up_256(sizeof(int32_t) * kNoAllocMaxTiles);
 constexpr size_t kNoAllocBytes = kNoAllocCarryValBytes + 2 * kNoAllocPlanBytes + kNoAllocCarryRowBytes;
-constexpr int kNoAllocMaxDevices = 64;
-
-std::mutex g_noalloc_mutex;
-unsigned char* g_noalloc_base[kNoAllocMaxDevices] = {};
 
 }  // namespace
 
@@ -892,20 +886,15 @@ static __device__ __align__(256) unsigned char g_tile_scratch[kNoAllocBytes];
 
 namespace {
 
-// Address of g_tile_scratch on the current device, looked up once per device.
+// Address of g_tile_scratch in the current device's context.  It is looked
+// up on every call (cheap once the module is loaded) rather than cached, so
+// a device reset or another context on the same ordinal never leaves a
+// stale address behind.
 tnlb_status noalloc_scratch(unsigned char** base)
 {
-   int dev = -1;
-   TNLB_CUDA_TRY(cudaGetDevice(&dev));
-   TNLB_REQUIRE(dev >= 0 && dev < kNoAllocMaxDevices, TNLB_ERR_INVALID_ARGUMENT,
-                "tnlb_spmv_csr_noalloc: device ordinal above 63");
-   std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-   if (!g_noalloc_base[dev]) {
-      void* p = nullptr;
-      TNLB_CUDA_TRY(cudaGetSymbolAddress(&p, g_tile_scratch));
-      g_noalloc_base[dev] = (unsigned char*)p;
-   }
-   *base = g_noalloc_base[dev];
+   void* p = nullptr;
+   TNLB_CUDA_TRY(cudaGetSymbolAddress(&p, g_tile_scratch));
+   *base = (unsigned char*)p;
    return TNLB_OK;
 }
 

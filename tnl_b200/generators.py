@@ -217,6 +217,16 @@ def diffusion_2d(N: int, corr_length: float = 0.1, sigma: float = 2.0, seed: int
     return _stencil_from_coeffs(k)
 
 
+def diffusion_2d_problem(N: int, seed: int, corr_range=(0.02, 0.2), sigma_range=(1.0, 3.0)) -> CSRMatrix:
+    """One seeded problem of the learned-preconditioner workload: a 2D
+    diffusion matrix whose GRF has correlation length ~ U[corr_range] and
+    sigma ~ U[sigma_range], both drawn from the seed."""
+    u = uniform01(seed, 99, np.arange(2, dtype=np.uint64))
+    corr = corr_range[0] + (corr_range[1] - corr_range[0]) * u[0]
+    sigma = sigma_range[0] + (sigma_range[1] - sigma_range[0]) * u[1]
+    return diffusion_2d(N, corr, sigma, seed)
+
+
 def _stencil_from_coeffs(k: np.ndarray, velocity=None) -> CSRMatrix:
     """Assemble the cell-centred finite-volume operator for coefficient field k.
 

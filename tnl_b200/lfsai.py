@@ -175,13 +175,9 @@ class LearnedFSAI:
 def diffusion_problem(N: int, seed: int, corr_range=(0.02, 0.2), sigma_range=(1.0, 3.0)) -> SparseMatrix:
     """One seeded 2D diffusion matrix of the learned-preconditioner workload:
     correlation length ~ U[corr_range], sigma ~ U[sigma_range]."""
-    from .generators import diffusion_2d, uniform01
+    from .generators import diffusion_2d_problem
 
-    u = uniform01(seed, 99, np.arange(2, dtype=np.uint64))
-    corr = corr_range[0] + (corr_range[1] - corr_range[0]) * u[0]
-    sigma = sigma_range[0] + (sigma_range[1] - sigma_range[0]) * u[1]
-    A = diffusion_2d(N, corr, sigma, seed)
-    return SparseMatrix.from_csr(A, real=torch.float64)
+    return SparseMatrix.from_csr(diffusion_2d_problem(N, seed, corr_range, sigma_range), real=torch.float64)
 
 
 def main(argv=None):
