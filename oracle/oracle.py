@@ -20,6 +20,7 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 ORACLE_SO = HERE / "_build" / "liboracle.so"
 REF_SO = HERE / "_ref" / "libtnlref.so"
+REF_CUDA_SO = HERE / "_ref" / "libtnlref_cuda.so"
 
 CSR, ELLPACK, SLICED_ELLPACK, CHUNKED_ELLPACK, BIELLPACK, ADAPTIVE_CSR = range(6)
 
@@ -644,3 +645,39 @@ class Reference:
         self.L.ref_prec_apply(A.n, rowptr.ctypes.data, cols.ctypes.data, vals.ctypes.data, kind, b.ctypes.data,
                               x.ctypes.data)
         return x
+
+
+class ReferenceCuda:
+    """The reference's own CUDA vectorProduct (oracle/_ref/libtnlref_cuda.so,
+    TNL's Devices::Cuda backend compiled for sm_100a), for the secondary GPU
+    comparison.  Needs a GPU."""
+
+    def __init__(self):
+        if not REF_CUDA_SO.exists():
+            raise FileNotFoundError(f"{REF_CUDA_SO} not built (needs the reference sources)")
+        L = self.L = C.CDLL(str(REF_CUDA_SO))
+        p, i32 = C.c_void_p, C.c_int
+        L.ref_cuda_spmv.argtypes = [i32, i32, i32, i32, p, p, p, p, p, i32, C.POINTER(C.c_double),
+                                    C.POINTER(C.c_double), C.c_char_p, i32, p, i32, C.c_char_p, i32]
+        L.ref_cuda_spmv.restype = C.c_int
+
+    def spmv(self, fmt: int, A, x, real=np.float64, reps: int = 20) -> dict:
+        """y = A x by the reference's CUDA vectorProduct (fmt 0: CSR, 2:
+        column-major SlicedEllpack); mean ms per synchronous call under the
+        default launch configuration and under each of the reference's
+        reductionLaunchConfigurations."""
+        rowptr, cols = _i32(A.rowptr), _i32(A.cols)
+        vals = np.ascontiguousarray(A.vals, real)
+        x = np.ascontiguousarray(x, real)
+        y = np.zeros(A.n, real)
+        md, mb = C.c_double(), C.c_double()
+        name = C.create_string_buffer(64)
+        err = C.create_string_buffer(512)
+        allms = np.zeros(32)
+        k = self.L.ref_cuda_spmv(fmt, int(real == np.float64), A.n, A.ncols, rowptr.ctypes.data, cols.ctypes.data,
+                                 vals.ctypes.data, x.ctypes.data, y.ctypes.data, reps, C.byref(md), C.byref(mb), name,
+                                 64, allms.ctypes.data, 32, err, 512)
+        if k < 0:
+            raise RuntimeError(err.value.decode())
+        return {"y": y, "ms_default": md.value, "ms_best": mb.value, "best": name.value.decode(),
+                "ms_all": allms[:k].tolist()}

@@ -32,6 +32,34 @@
 namespace tnlb {
 namespace {
 
+// Sum of v[k] x[c[k]] over k = k0, k0 + stride, ... < k1 for one lane, four
+// entries loaded before any is used (four independent chains in flight).
+template <typename Real>
+__device__ __forceinline__ Real strided_dot(const int32_t* __restrict__ cols, const Real* __restrict__ vals,
+                                            const Real* __restrict__ x, int32_t k0, int32_t k1, int32_t stride)
+{
+   Real s = 0;
+   int32_t k = k0;
+   for (; k + 3 * stride < k1; k += 4 * stride) {
+      int32_t c[4];
+      Real v[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+         c[u] = ld_stream(cols + k + u * stride);
+         v[u] = ld_stream(vals + k + u * stride);
+      }
+#pragma unroll
+      for (int u = 0; u < 4; u++)
+         if (c[u] >= 0) s += v[u] * ld_gather(x + c[u]);
+   }
+   for (; k < k1; k += stride) {
+      const int32_t c = ld_stream(cols + k);
+      const Real v = ld_stream(vals + k);
+      if (c >= 0) s += v * ld_gather(x + c);
+   }
+   return s;
+}
+
 // ------------------------------------------------------------- scalar
 
 template <typename Real>
@@ -41,12 +69,7 @@ __global__ void k_csr_scalar(const int32_t* __restrict__ rowptr, const int32_t* 
 {
    const int64_t row = begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
    if (row >= end) return;
-   Real sum = 0;
-   for (int32_t j = rowptr[row]; j < rowptr[row + 1]; j++) {
-      const int32_t c = cols[j];
-      if (c >= 0) sum += vals[j] * ld_gather(x + c);
-   }
-   keep(y, (int32_t)row, sum, alpha, beta);
+   keep(y, (int32_t)row, strided_dot(cols, vals, x, rowptr[row], rowptr[row + 1], 1), alpha, beta);
 }
 
 // ------------------------------------------------- vector (G lanes/row)
@@ -60,14 +83,7 @@ __global__ void k_csr_vector(const int32_t* __restrict__ rowptr, const int32_t* 
    const int64_t row = begin + gid / G;
    const int lane = (int)(gid % G);
    Real sum = 0;
-   if (row < end) {
-      const int32_t rb = rowptr[row], re = rowptr[row + 1];
-      for (int32_t j = rb + lane; j < re; j += G) {
-         const int32_t c = ld_stream(cols + j);
-         const Real v = ld_stream(vals + j);
-         if (c >= 0) sum += v * ld_gather(x + c);
-      }
-   }
+   if (row < end) sum = strided_dot(cols, vals, x, rowptr[row] + lane, rowptr[row + 1], G);
    sum = group_sum<G>(sum);
    if (row < end && lane == 0) keep(y, (int32_t)row, sum, alpha, beta);
 }
@@ -86,14 +102,7 @@ __global__ void k_csr_block(const int32_t* __restrict__ rowptr, const int32_t* _
    const int t = threadIdx.x % G;
    const int64_t row = begin + (int64_t)blockIdx.x * kRowsPerBlock + r_in_block;
    Real sum = 0;
-   if (row < end) {
-      const int32_t rb = rowptr[row], re = rowptr[row + 1];
-      for (int32_t j = rb + t; j < re; j += G) {
-         const int32_t c = ld_stream(cols + j);
-         const Real v = ld_stream(vals + j);
-         if (c >= 0) sum += v * ld_gather(x + c);
-      }
-   }
+   if (row < end) sum = strided_dot(cols, vals, x, rowptr[row] + t, rowptr[row + 1], G);
    sum = warp_sum(sum);
    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = sum;
    __syncthreads();
@@ -129,10 +138,21 @@ __global__ void __launch_bounds__(256) k_csr_adaptive(const tnlb_acsr_block* __r
    if (active && d.type == 1) {  // STREAM: many short rows, staged per warp
       const int32_t first = d.first_segment;
       const int32_t b = rowptr[first];
-      for (int32_t k = lane; k < d.block_size; k += 32) {
-         const int32_t c = ld_stream(cols + b + k);
-         const Real v = ld_stream(vals + b + k);
-         stream_buf[wib][k] = c >= 0 ? v * ld_gather(x + c) : Real(0);
+      for (int32_t k = lane; k < d.block_size; k += 128) {
+         int32_t c[4];
+         Real v[4];
+#pragma unroll
+         for (int u = 0; u < 4; u++) {
+            c[u] = -1;
+            v[u] = Real(0);
+            if (k + 32 * u < d.block_size) {
+               c[u] = ld_stream(cols + b + k + 32 * u);
+               v[u] = ld_stream(vals + b + k + 32 * u);
+            }
+         }
+#pragma unroll
+         for (int u = 0; u < 4; u++)
+            if (k + 32 * u < d.block_size) stream_buf[wib][k + 32 * u] = c[u] >= 0 ? v[u] * ld_gather(x + c[u]) : Real(0);
       }
       __syncwarp();
       for (int32_t r = first + lane; r < first + d.segments_in_block; r += 32) {
@@ -145,24 +165,14 @@ __global__ void __launch_bounds__(256) k_csr_adaptive(const tnlb_acsr_block* __r
    else if (active && d.type == 2) {  // VECTOR: one row per warp
       const int32_t r = d.first_segment;
       const int32_t b = rowptr[r], e = b + d.block_size;
-      Real s = 0;
-      for (int32_t k = b + lane; k < e; k += 32) {
-         const int32_t c = ld_stream(cols + k);
-         const Real v = ld_stream(vals + k);
-         if (c >= 0) s += v * ld_gather(x + c);
-      }
+      Real s = strided_dot(cols, vals, x, b + lane, e, 32);
       s = warp_sum(s);
       if (lane == 0) keep(y, r, s, alpha, beta);
    }
    else if (active && d.type == 0) {  // LONG: several warps of this block per row
       const int32_t r = d.first_segment;
       const int32_t b = rowptr[r], e = rowptr[r + 1];
-      Real s = 0;
-      for (int32_t k = b + lane + 32 * d.warp_idx; k < e; k += 32 * d.warps_count) {
-         const int32_t c = ld_stream(cols + k);
-         const Real v = ld_stream(vals + k);
-         if (c >= 0) s += v * ld_gather(x + c);
-      }
+      Real s = strided_dot(cols, vals, x, b + lane + 32 * d.warp_idx, e, 32 * d.warps_count);
       s = warp_sum(s);
       if (lane == 0) long_part[wib] = s;
    }

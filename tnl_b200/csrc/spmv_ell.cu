@@ -285,10 +285,19 @@ __global__ void __launch_bounds__(kChunksInSlice) k_chell(const int32_t* __restr
 
 // ----------------------------------------------------------- BiEllpack
 
-template <typename Real, bool ColMajor>
-__global__ void k_biell(const int32_t* __restrict__ cols, const Real* __restrict__ vals, const Real* __restrict__ x,
-                        Real* __restrict__ y, const int32_t* __restrict__ perm, const int32_t* __restrict__ gp,
-                        int32_t n, int32_t strips, int32_t begin, int32_t end, Real alpha, Real beta)
+// Column-major strips: group g of a strip holds the h = 32 >> g widest rows
+// (sorted positions 0..h-1) with w slots each, slot (k, r) at base + k h + r.
+// All 32 lanes stride through the group's h w slots: lane l always meets
+// row l & (h-1), so it keeps one partial sum, and the partials of a row are
+// added across the lanes l, l + h, ... by log2(32/h) shuffles.  A strip with
+// one dominant row (power-law matrices) thus spreads that row over the warp
+// instead of leaving it to one lane.  Four slots per lane are loaded before
+// any is used.
+template <typename Real>
+__global__ void k_biell_col(const int32_t* __restrict__ cols, const Real* __restrict__ vals,
+                            const Real* __restrict__ x, Real* __restrict__ y, const int32_t* __restrict__ perm,
+                            const int32_t* __restrict__ gp, int32_t n, int32_t strips, int32_t begin, int32_t end,
+                            Real alpha, Real beta)
 {
    const int64_t strip = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
    const int lane = threadIdx.x & 31;  // sorted position in the strip
@@ -299,14 +308,52 @@ __global__ void k_biell(const int32_t* __restrict__ cols, const Real* __restrict
    for (int grp = 0; grp < kBiGroups; grp++, h >>= 1) {
       const int64_t base = g[grp];
       const int32_t size = g[grp + 1] - g[grp];
-      if (size == 0 || lane >= h) continue;
-      const int32_t w = size / h;
-      if (ColMajor)
-         for (int32_t k = 0; k < w; k++) sum = fma_slot(cols, vals, x, base + lane + (int64_t)k * h, sum);
-      else
-         for (int32_t k = 0; k < w; k++) sum = fma_slot(cols, vals, x, base + (int64_t)lane * w + k, sum);
+      if (size == 0) continue;  // warp-uniform
+      Real part = 0;
+      int32_t s = lane;
+      for (; s + 96 < size; s += 128) {
+         int32_t c[4];
+         Real v[4];
+#pragma unroll
+         for (int u = 0; u < 4; u++) {
+            c[u] = ld_stream(cols + base + s + 32 * u);
+            v[u] = ld_stream(vals + base + s + 32 * u);
+         }
+#pragma unroll
+         for (int u = 0; u < 4; u++)
+            if (c[u] >= 0) part += v[u] * ld_gather(x + c[u]);
+      }
+      for (; s < size; s += 32) part = fma_slot(cols, vals, x, base + s, part);
+      for (int o = 16; o >= h; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+      if (lane < h) sum += part;
    }
    const int64_t row = strip * kBiStrip + lane;  // original row of this lane
+   const int src = row < n ? perm[row] - (int32_t)(strip * kBiStrip) : 0;
+   const Real mine = __shfl_sync(0xffffffffu, sum, src);
+   if (row < n) keep_range(y, row, mine, alpha, beta, begin, end);
+}
+
+// Row-major strips: lane = sorted position walks its own w slots.
+template <typename Real>
+__global__ void k_biell_row(const int32_t* __restrict__ cols, const Real* __restrict__ vals,
+                            const Real* __restrict__ x, Real* __restrict__ y, const int32_t* __restrict__ perm,
+                            const int32_t* __restrict__ gp, int32_t n, int32_t strips, int32_t begin, int32_t end,
+                            Real alpha, Real beta)
+{
+   const int64_t strip = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+   const int lane = threadIdx.x & 31;
+   if (strip >= strips) return;
+   const int32_t* g = gp + strip * kBiGroups;
+   Real sum = 0;
+   int h = 32;
+   for (int grp = 0; grp < kBiGroups; grp++, h >>= 1) {
+      const int64_t base = g[grp];
+      const int32_t size = g[grp + 1] - g[grp];
+      if (size == 0 || lane >= h) continue;
+      const int32_t w = size / h;
+      for (int32_t k = 0; k < w; k++) sum = fma_slot(cols, vals, x, base + (int64_t)lane * w + k, sum);
+   }
+   const int64_t row = strip * kBiStrip + lane;
    const int src = row < n ? perm[row] - (int32_t)(strip * kBiStrip) : 0;
    const Real mine = __shfl_sync(0xffffffffu, sum, src);
    if (row < n) keep_range(y, row, mine, alpha, beta, begin, end);
@@ -399,7 +446,7 @@ tnlb_status launch(const tnlb_segments* seg, const int32_t* cols, const Real* va
       }
       case TNLB_BIELLPACK: {
          if (seg->strips == 0) return TNLB_OK;
-         auto kern = col ? k_biell<Real, true> : k_biell<Real, false>;
+         auto kern = col ? k_biell_col<Real> : k_biell_row<Real>;
          kern<<<grid_for(seg->strips, 8), 256, 0, st>>>(cols, vals, x, y, seg->bi_perm.as<int32_t>(),
                                                          seg->bi_group_pointers.as<int32_t>(), seg->n, seg->strips,
                                                          begin, end, alpha, beta);
