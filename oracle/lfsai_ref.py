@@ -3,37 +3,47 @@
 The learned factorised sparse approximate inverse has no counterpart in the
 reference library; this module restates, in plain numpy FP64, exactly what
 the GPU kernels of tnl_b200/csrc/lfsai.cu compute, so that the tests can
-check the GPU features, network outputs, loss and gradients, and check this
-backpropagation itself against finite differences.
+check the GPU features, network outputs, losses and gradients, and check
+this backpropagation itself against finite differences.
 
 Definitions (shared with lfsai.cu):
 
-* Pattern of G: row i holds the stored columns j <= i of A (the lower
-  triangle with the diagonal), at most 4 of them; they occupy the
-  right-aligned slots 4-k .. 3 (slot 3 is the diagonal).
+* Pattern of G, row i: level 0 -- the stored columns j <= i of A (the
+  lower triangle with the diagonal); level 1 -- the columns j <= i of the
+  pattern of A^2 (i, its neighbours and their neighbours: one level of
+  fill).  At most 8 columns per row; they occupy the right-aligned slots
+  8-k .. 7 (slot 7 is the diagonal).
 * Scaling s_j = 1/sqrt(a_jj); B = S A S has a unit diagonal.
-* Features f (16, zero padded): f[0..5] = B(J_p, J_q) for the slot pairs
-  (0,1) (0,2) (0,3) (1,2) (1,3) (2,3) (0 when a slot is empty); f[6..8] =
-  B(i, j) for the first three stored columns j > i; f[9] = k/4;
-  f[10] = (number of stored columns > i)/3.
+* Features f (32): f[0..27] = B(J_p, J_q) for the slot pairs p < q in the
+  order (0,1) (0,2) .. (0,7) (1,2) .. (6,7) (0 when a slot is empty or the
+  entry is not stored); f[28..30] = B(i, j) for the first three stored
+  columns j > i; f[31] = k/8.
 * Network: h1 = relu(W1 f + b1), h2 = relu(W2 h1 + b2), h3 = relu(W3 h2 + b3),
-  o = W4 h3 + b4 with W1 64x16, W2 W3 64x64, W4 4x64.  Every layer input
+  o = W4 h3 + b4 with W1 64x32, W2 W3 64x64, W4 8x64.  Every layer input
   and every weight is rounded to BF16 (round to nearest even) before the
   product; sums and biases are FP32 on the GPU, FP64 here.
-* G'_i: slot 3 = exp(o_3), occupied slots t < 3 = o_t.  G_ij = G'_i,slot(j) s_j,
+* G'_i: slot 7 = exp(o_7), occupied slots t < 7 = o_t.  G_ij = G'_i,slot(j) s_j,
   so G A G^T = G' B G'^T.
-* Loss over probes z_p: L = (1/(n P)) sum_p ||z_p - G A G^T z_p||^2 with
+* Probe loss over probes z_p: L = (1/(n P)) sum_p ||z_p - G A G^T z_p||^2 with
   gradient dL/dG = -(2/(n P)) sum_p (u_p w_p^T + z_p q_p^T) on the pattern,
   where w = A G^T z, u = z - G w, q = A G^T u.
+* Kaporin loss (exact, no probes): K = log(T/n) - (2/n) sum_i log G'_ii with
+  T = sum_i G'_i B[J,J] G'_i^T = trace(G A G^T); up to a constant it is the
+  log of Kaporin's condition number of G A G^T, which classical FSAI
+  minimises over a given pattern.  dK/dG'_i = (2/T) B[J,J] G'_i - (2/n)
+  e_last / G'_ii.
+* Warm start: L = (1/n) sum_i ||G'_i - target'_i||^2 over the occupied
+  slots, the target being classical FSAI on the lower pattern of A (level
+  0), zero on the fill slots of a level-1 pattern.
 
-Parameter vector layout (float32, 9668 entries): W1 (64x16 row-major), b1,
-W2 (64x64), b2, W3, b3, W4 (4x64), b4.
+Parameter vector layout (float32, 10952 entries): W1 (64x32 row-major), b1,
+W2 (64x64), b2, W3, b3, W4 (8x64), b4.
 """
 from __future__ import annotations
 
 import numpy as np
 
-F, H, K = 16, 64, 4
+F, H, K = 32, 64, 8
 SHAPES = [("W1", (H, F)), ("b1", (H,)), ("W2", (H, H)), ("b2", (H,)), ("W3", (H, H)), ("b3", (H,)),
           ("W4", (K, H)), ("b4", (K,))]
 NPARAMS = sum(int(np.prod(s)) for _, s in SHAPES)
@@ -66,17 +76,28 @@ def bf16(x):
     return u.view(np.float32).astype(np.float64)
 
 
-def pattern(A):
-    """Per row: (slots, columns) of G's pattern; raises if a row has > 4."""
+def pattern(A, level: int = 0):
+    """Per row: the sorted columns of G's pattern (level 0: lower triangle of
+    A; level 1: lower triangle of the pattern of A^2); raises if a row has
+    more than 8."""
     rp, cols = A.rowptr, A.cols
+    adj = [set(int(x) for x in cols[rp[i]:rp[i + 1]] if x >= 0) | {i} for i in range(A.n)]
     pat = []
     for i in range(A.n):
-        c = cols[rp[i]:rp[i + 1]]
-        low = sorted(int(x) for x in c if 0 <= x <= i)
+        if level == 0:
+            low = sorted(int(x) for x in cols[rp[i]:rp[i + 1]] if 0 <= x <= i)
+        else:
+            reach = set(adj[i])
+            for l in adj[i]:
+                reach |= adj[l]
+            low = sorted(j for j in reach if j <= i)
         if len(low) > K:
-            raise ValueError("learned FSAI: more than 4 stored entries in the lower triangle of a row")
+            raise ValueError("learned FSAI: more than 8 entries in a row of the pattern")
         pat.append(low)
     return pat
+
+
+PAIRS = [(p, q) for p in range(K) for q in range(p + 1, K)]
 
 
 def _row_dict(A):
@@ -84,28 +105,26 @@ def _row_dict(A):
     return [dict(zip(cols[rp[i]:rp[i + 1]].tolist(), vals[rp[i]:rp[i + 1]].tolist())) for i in range(A.n)]
 
 
-def features(A, pat=None):
-    pat = pattern(A) if pat is None else pat
+def features(A, pat=None, level: int = 0):
+    pat = pattern(A, level) if pat is None else pat
     rows = _row_dict(A)
     d = np.array([rows[i].get(i, 0.0) for i in range(A.n)], np.float64)
     s = 1.0 / np.sqrt(d)
     f = np.zeros((A.n, F))
-    pairs = [(0, 1), (0, 2), (0, 3), (1, 2), (1, 3), (2, 3)]
     for i in range(A.n):
         J = pat[i]
         k = len(J)
         slot_col = [None] * K
         for t, j in enumerate(J):
             slot_col[K - k + t] = j
-        for m, (p, q) in enumerate(pairs):
+        for m, (p, q) in enumerate(PAIRS):
             jp, jq = slot_col[p], slot_col[q]
             if jp is not None and jq is not None:
                 f[i, m] = rows[jp].get(jq, 0.0) * s[jp] * s[jq]
         upper = sorted(j for j in rows[i] if j > i)[:3]
         for m, j in enumerate(upper):
-            f[i, 6 + m] = rows[i][j] * s[i] * s[j]
-        f[i, 9] = k / 4.0
-        f[i, 10] = sum(1 for j in rows[i] if j > i) / 3.0
+            f[i, 28 + m] = rows[i][j] * s[i] * s[j]
+        f[i, 31] = k / 8.0
     return f, s, pat
 
 
@@ -133,7 +152,7 @@ def g_values(o, s, pat):
         k = len(J)
         for t, j in enumerate(J):
             slot = K - k + t
-            gp = np.exp(o[i, 3]) if slot == 3 else o[i, slot]
+            gp = np.exp(o[i, K - 1]) if slot == K - 1 else o[i, slot]
             vals.append(gp * s[j])
     return np.array(vals, np.float64)
 
@@ -181,22 +200,55 @@ def backward(theta, cache, do):
     return pack(g)
 
 
-def loss_and_grad(theta, A, probes):
-    """L and dL/dtheta (straight-through for the BF16 rounding)."""
-    f, s, pat = features(A)
-    o, cache = forward(theta, f)
-    vals = g_values(o, s, pat)
-    Gm = g_matrix(vals, pat, A.n)
-    L, dG = loss_and_grad_G(A, Gm, probes)
+def _do_from_dG(dG, o, s, pat):
+    """dL/do from dL/dG on the pattern (CSR order)."""
     do = np.zeros_like(o)
     q = 0
     for i, J in enumerate(pat):
         k = len(J)
         for t, j in enumerate(J):
             slot = K - k + t
-            dgp = dG[q] * s[j]
-            do[i, slot] += dgp * (np.exp(o[i, 3]) if slot == 3 else 1.0)
+            do[i, slot] += dG[q] * s[j] * (np.exp(o[i, K - 1]) if slot == K - 1 else 1.0)
             q += 1
+    return do
+
+
+def loss_and_grad(theta, A, probes, level: int = 0):
+    """Probe loss L and dL/dtheta (straight-through for the BF16 rounding)."""
+    f, s, pat = features(A, level=level)
+    o, cache = forward(theta, f)
+    vals = g_values(o, s, pat)
+    Gm = g_matrix(vals, pat, A.n)
+    L, dG = loss_and_grad_G(A, Gm, probes)
+    return L, backward(theta, cache, _do_from_dG(dG, o, s, pat))
+
+
+def kaporin_and_grad(theta, A, level: int = 0):
+    """Kaporin loss K and dK/dtheta (straight-through for the BF16 rounding)."""
+    f, s, pat = features(A, level=level)
+    o, cache = forward(theta, f)
+    rows = _row_dict(A)
+    n = A.n
+    gps, Bs = [], []
+    T = 0.0
+    logdiag = 0.0
+    for i, J in enumerate(pat):
+        k = len(J)
+        gp = np.array([np.exp(o[i, K - 1]) if K - k + t == K - 1 else o[i, K - k + t] for t in range(k)])
+        B = np.array([[rows[p].get(q, 0.0) * s[p] * s[q] for q in J] for p in J])
+        gps.append(gp)
+        Bs.append(B)
+        T += float(gp @ B @ gp)
+        logdiag += np.log(gp[-1])
+    L = np.log(T / n) - 2.0 * logdiag / n
+    do = np.zeros_like(o)
+    for i, J in enumerate(pat):
+        k = len(J)
+        dgp = (2.0 / T) * (Bs[i] @ gps[i])
+        dgp[-1] -= 2.0 / (n * gps[i][-1])
+        for t in range(k):
+            slot = K - k + t
+            do[i, slot] = dgp[t] * (gps[i][-1] if slot == K - 1 else 1.0)
     return L, backward(theta, cache, do)
 
 
@@ -231,18 +283,33 @@ def _u01(seed, index):
     return (z >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
 
 
-def fsai_classical(A):
-    """Kolotilina-Yeremin FSAI values on the lower pattern (FP64, per row:
-    A[J,J] g = e_last, G_i = g / sqrt(g_last)); CSR order of the pattern."""
+def fsai_classical(A, level: int = 0):
+    """Kolotilina-Yeremin FSAI values on the level-0 or level-1 lower pattern
+    (FP64, per row: A[J,J] g = e_last, G_i = g / sqrt(g_last)); CSR order of
+    the pattern."""
     rows = _row_dict(A)
     out = []
-    for i in range(A.n):
-        J = sorted(j for j in rows[i] if 0 <= j <= i)
+    for i, J in enumerate(pattern(A, level) if level else [sorted(j for j in rows[i] if 0 <= j <= i)
+                                                              for i in range(A.n)]):
         B = np.array([[rows[p].get(q, 0.0) for q in J] for p in J])
         e = np.zeros(len(J))
         e[-1] = 1.0
         g = np.linalg.solve(B, e)
         out.extend(g / np.sqrt(g[-1]))
+    return np.array(out)
+
+
+def fit_target(A, level: int = 0):
+    """Warm-start target on G's level-`level` pattern (CSR order): classical
+    FSAI of the level-0 pattern, zero on the fill slots."""
+    rows = _row_dict(A)
+    narrow = fsai_classical(A, 0)
+    out, q = [], 0
+    for i, J in enumerate(pattern(A, level)):
+        low = sorted(j for j in rows[i] if 0 <= j <= i)
+        vals = dict(zip(low, narrow[q:q + len(low)]))
+        q += len(low)
+        out.extend(vals.get(j, 0.0) for j in J)
     return np.array(out)
 
 

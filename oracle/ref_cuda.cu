@@ -115,18 +115,26 @@ spmvCuda( int n, int ncols, const int* rowptr, const int* cols, const Real* vals
    std::string best = "default";
    int k = 0;
    for( const auto& [ cfg, name ] : Seg::reductionLaunchConfigurations( D.getSegments() ) ) {
-      const double ms = timeCalls( D,
-                                   xv,
-                                   yv,
-                                   reps,
-                                   [ &cfg = cfg ]( auto& A, auto& xx, auto& yy )
-                                   {
-                                      A.vectorProduct( xx, yy, 1, 0, 0, 0, cfg );
-                                   } );
+      // a configuration the reference refuses for this matrix (e.g. more
+      // threads than its index type counts) is recorded as -1
+      double ms = -1;
+      try {
+         ms = timeCalls( D,
+                         xv,
+                         yv,
+                         reps,
+                         [ &cfg = cfg ]( auto& A, auto& xx, auto& yy )
+                         {
+                            A.vectorProduct( xx, yy, 1, 0, 0, 0, cfg );
+                         } );
+      }
+      catch( const std::exception& ) {
+         ms = -1;
+      }
       if( k < maxAll )
          msAll[ k ] = ms;
       k++;
-      if( ms < *msBest ) {
+      if( ms >= 0 && ms < *msBest ) {
          *msBest = ms;
          best = name;
       }
@@ -144,8 +152,8 @@ extern "C" {
 
 // fmt 0: CSR, 2: SlicedEllpack (column-major, slice 32).  x, y in host
 // memory; y receives the default-configuration product.  Returns the number
-// of launch configurations timed (their times in msAll), or -1 on an error
-// (message in err).
+// of launch configurations tried (their times in msAll, -1 for one the
+// reference refused), or -1 on an error (message in err).
 int
 ref_cuda_spmv( int fmt, int real64, int n, int ncols, const int* rowptr, const int* cols, const void* vals,
                const void* x, void* y, int reps, double* msDefault, double* msBest, char* bestName, int bestNameLen,

@@ -185,9 +185,11 @@ def test_bicgstab_within_reference_spread(oracle, reference):
     assert oracle.true_residual(A, b, o["x"]) < 1e-7
 
 
-def test_lfsai_reference_fd():
+@pytest.mark.parametrize("level", [0, 1])
+def test_lfsai_reference_fd(level):
     """The FP64 backpropagation of the learned-FSAI reference against central
-    finite differences (BF16 rounding off)."""
+    finite differences (BF16 rounding off), for the probe loss and the
+    Kaporin loss, on G's level-0 and level-1 patterns."""
     from oracle import lfsai_ref as R
     from tnl_b200 import generators as g
 
@@ -198,15 +200,46 @@ def test_lfsai_reference_fd():
     old = R.ROUND
     R.ROUND = False
     try:
-        _, grad = R.loss_and_grad(theta, A, Z)
-        idx = np.nonzero(np.abs(grad) > 1e-4 * np.abs(grad).max())[0]
-        for i in rng.choice(idx, 10, replace=False):
-            e = np.zeros_like(theta)
-            e[i] = 1e-6
-            fd = (R.loss_and_grad(theta + e, A, Z)[0] - R.loss_and_grad(theta - e, A, Z)[0]) / 2e-6
-            assert fd == pytest.approx(grad[i], rel=1e-5, abs=1e-10)
+        for loss in (lambda th: R.loss_and_grad(th, A, Z, level), lambda th: R.kaporin_and_grad(th, A, level)):
+            _, grad = loss(theta)
+            idx = np.nonzero(np.abs(grad) > 1e-4 * np.abs(grad).max())[0]
+            for i in rng.choice(idx, 10, replace=False):
+                e = np.zeros_like(theta)
+                e[i] = 1e-6
+                fd = (loss(theta + e)[0] - loss(theta - e)[0]) / 2e-6
+                assert fd == pytest.approx(grad[i], rel=1e-5, abs=1e-10)
     finally:
         R.ROUND = old
+
+
+def test_lfsai_reference_patterns_and_classical_fsai():
+    """Level-1 pattern of a 5-point operator: the 7 lower entries of its
+    13-point square; classical FSAI on it is the Kaporin minimiser, so it
+    has a smaller Kaporin number than FSAI on A's own pattern, and the
+    warm-start target is the level-0 FSAI padded with zeros."""
+    import scipy.sparse as sp
+
+    from oracle import lfsai_ref as R
+    from tnl_b200 import generators as g
+
+    N = 9
+    A = g.diffusion_2d(N, 0.2, 1.5, 4)
+    p1 = R.pattern(A, 1)
+    i = 4 * N + 4  # an interior cell
+    assert p1[i] == sorted([i, i - 1, i - 2, i - N, i - 2 * N, i - N + 1, i - N - 1])
+    As = sp.csr_matrix((A.vals, A.cols, A.rowptr), shape=(A.n, A.n)).toarray()
+
+    def kaporin(level, vals):
+        pat = R.pattern(A, level)
+        G = R.g_matrix(vals, pat, A.n).toarray()
+        M = G @ As @ G.T
+        ev = np.linalg.eigvalsh(M)
+        return np.mean(ev) / np.exp(np.mean(np.log(ev)))
+
+    k0 = kaporin(0, R.fsai_classical(A, 0))
+    k1 = kaporin(1, R.fsai_classical(A, 1))
+    assert k1 < k0
+    assert np.isclose(kaporin(1, R.fit_target(A, 1)), k0)
 
 
 @pytest.mark.parametrize("solver,kw", [("tfqmr", {}), ("bicgstabl", {"ell": 1}), ("bicgstabl", {"ell": 3}),

@@ -42,6 +42,57 @@ __global__ void k_copy_lower(const int32_t* __restrict__ rp, const int32_t* __re
       if (cols[q] >= 0 && cols[q] <= i) gcols[o++] = cols[q];
 }
 
+// Level-1 lower pattern of row i: the columns j <= i reached from i in at
+// most two steps through A's pattern (i itself, its neighbours, theirs),
+// i.e. the lower triangle of the pattern of A^2, sorted.  Count pass
+// (gcols == nullptr: cnt[i] = size) and fill pass.  More than kLevel1Max
+// candidates in a row sets *err = 1.
+constexpr int kLevel1Max = 64;
+
+__global__ void k_level1_lower(const int32_t* __restrict__ rp, const int32_t* __restrict__ cols, int32_t n,
+                               const int32_t* __restrict__ grp, int32_t* __restrict__ gcols, int32_t* __restrict__ cnt,
+                               int32_t* __restrict__ err)
+{
+   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+   if (i >= n) return;
+   int32_t cand[kLevel1Max];
+   int k = 0;
+   bool over = false;
+   auto push = [&](int32_t j) {
+      for (int q = 0; q < k; q++)
+         if (cand[q] == j) return;
+      if (k == kLevel1Max) {
+         over = true;
+         return;
+      }
+      // insertion keeps cand sorted
+      int q = k++;
+      while (q > 0 && cand[q - 1] > j) {
+         cand[q] = cand[q - 1];
+         q--;
+      }
+      cand[q] = j;
+   };
+   push((int32_t)i);
+   for (int32_t a = rp[i]; a < rp[i + 1]; a++) {
+      const int32_t l = cols[a];
+      if (l < 0) continue;
+      if (l <= i) push(l);
+      for (int32_t b = rp[l]; b < rp[l + 1]; b++) {
+         const int32_t j = cols[b];
+         if (j >= 0 && j <= i) push(j);
+      }
+   }
+   if (over) {
+      atomicExch(err, 1);
+      k = 0;
+   }
+   if (!gcols)
+      cnt[i] = k;
+   else
+      for (int q = 0; q < k; q++) gcols[grp[i] + q] = cand[q];
+}
+
 // a(r, c) from a CSR row with ascending columns (0 if absent).
 template <typename Real>
 __device__ __forceinline__ Real lookup(const int32_t* rp, const int32_t* cols, const Real* vals, int32_t r, int32_t c)
@@ -261,13 +312,17 @@ tnlb_status make_csr_segments(const int32_t* d_rowptr, int32_t n, cudaStream_t s
 
 }  // namespace
 
-// Gathers A into CSR (ascending columns), builds G's pattern (lower triangle
-// of A with the diagonal) and, when `classical`, the Kolotilina-Yeremin
-// values; then G^T.  The values of a learned G are written later through
-// fsai_set_values.
+// Gathers A into CSR (ascending columns), builds G's pattern (level 0: the
+// lower triangle of A with the diagonal; level 1: the lower triangle of the
+// pattern of A^2, one level of fill) and, when `classical`, the
+// Kolotilina-Yeremin values; then G^T.  The values of a learned G are
+// written later through fsai_set_values.
 tnlb_status fsai_create(const tnlb_segments* seg, tnlb_real real, const int32_t* cols, const void* vals, bool classical,
-                        cudaStream_t st, Fsai** out, bool two_factor)
+                        cudaStream_t st, Fsai** out, bool two_factor, int level)
 {
+   TNLB_REQUIRE(level == 0 || level == 1, TNLB_ERR_INVALID_ARGUMENT, "FSAI: the pattern level must be 0 or 1");
+   TNLB_REQUIRE(level == 0 || !two_factor, TNLB_ERR_INVALID_ARGUMENT,
+                "FSAI: the two-factor form uses the level-0 pattern");
    const int32_t n = seg->n;
    TNLB_REQUIRE(n > 0, TNLB_ERR_INVALID_ARGUMENT, "FSAI: the matrix is empty");
    auto* F = new Fsai();
@@ -283,15 +338,34 @@ tnlb_status fsai_create(const tnlb_segments* seg, tnlb_real real, const int32_t*
    DeviceBuffer cnt, grp;
    TNLB_TRY_STATUS(cnt.alloc(sizeof(int32_t) * n));
    TNLB_TRY_STATUS(grp.alloc(sizeof(int32_t) * ((size_t)n + 1)));
-   k_count_lower<<<grid_for(n, 256), 256, 0, st>>>(F->a_rp.as<int32_t>(), F->a_cols.as<int32_t>(), n,
-                                                   cnt.as<int32_t>());
+   DeviceBuffer perr;
+   TNLB_TRY_STATUS(perr.alloc(sizeof(int32_t)));
+   TNLB_CUDA_TRY(cudaMemsetAsync(perr.ptr, 0, sizeof(int32_t), st));
+   if (level == 0)
+      k_count_lower<<<grid_for(n, 256), 256, 0, st>>>(F->a_rp.as<int32_t>(), F->a_cols.as<int32_t>(), n,
+                                                      cnt.as<int32_t>());
+   else
+      k_level1_lower<<<grid_for(n, 128), 128, 0, st>>>(F->a_rp.as<int32_t>(), F->a_cols.as<int32_t>(), n, nullptr,
+                                                       nullptr, cnt.as<int32_t>(), perr.as<int32_t>());
    TNLB_CHECK_LAUNCH();
    int64_t gnnz = 0;
    TNLB_TRY_STATUS(exclusive_scan_i32(cnt.as<int32_t>(), grp.as<int32_t>(), n, &gnnz, st, true));
+   {
+      int32_t h = 0;
+      TNLB_CUDA_TRY(cudaMemcpyAsync(&h, perr.ptr, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+      TNLB_CUDA_TRY(cudaStreamSynchronize(st));
+      TNLB_REQUIRE(h == 0, TNLB_ERR_INVALID_ARGUMENT,
+                   "FSAI: a row of the level-1 pattern reaches more than 64 candidate columns");
+   }
    TNLB_TRY_STATUS(F->g_cols.alloc(sizeof(int32_t) * gnnz));
    TNLB_TRY_STATUS(F->g_vals.alloc(rs * gnnz));
-   k_copy_lower<<<grid_for(n, 256), 256, 0, st>>>(F->a_rp.as<int32_t>(), F->a_cols.as<int32_t>(), n, grp.as<int32_t>(),
-                                                  F->g_cols.as<int32_t>());
+   if (level == 0)
+      k_copy_lower<<<grid_for(n, 256), 256, 0, st>>>(F->a_rp.as<int32_t>(), F->a_cols.as<int32_t>(), n,
+                                                     grp.as<int32_t>(), F->g_cols.as<int32_t>());
+   else
+      k_level1_lower<<<grid_for(n, 128), 128, 0, st>>>(F->a_rp.as<int32_t>(), F->a_cols.as<int32_t>(), n,
+                                                       grp.as<int32_t>(), F->g_cols.as<int32_t>(), nullptr,
+                                                       perr.as<int32_t>());
    TNLB_CHECK_LAUNCH();
    TNLB_TRY_STATUS(make_csr_segments(grp.as<int32_t>(), n, st, &F->g));
    DeviceBuffer hvals;  // two-factor: row i of H = G_U^T on G's pattern

@@ -56,7 +56,7 @@ constexpr int kDesiredChunkSize = 16;  // ChunkedEllpackBase.h:292
 
 // CSR tile kernel geometry: a tile of kTileSize merge items (rows +
 // nonzeros) per warp, kTileItems per lane; blocks of kTileThreads threads.
-constexpr int kTileThreads = 256;
+constexpr int kTileThreads = 128;
 constexpr int kTileItems = 8;
 constexpr int kTileSize = 32 * kTileItems;
 
@@ -360,7 +360,7 @@ tnlb_status ilut_create(const tnlb_segments* seg, tnlb_real real, const int32_t*
 tnlb_status ilu0_read(void* ilu, int32_t* h_rowptr, int32_t* h_cols, void* h_vals, int64_t capacity, int real_bytes);
 void ilu0_destroy(void* ilu);
 tnlb_status fsai_create(const tnlb_segments* seg, tnlb_real real, const int32_t* cols, const void* vals,
-                        bool classical, cudaStream_t st, Fsai** out, bool two_factor = false);
+                        bool classical, cudaStream_t st, Fsai** out, bool two_factor = false, int level = 0);
 tnlb_status fsai_apply(const Fsai* F, const void* r, void* z, cudaStream_t st, const int32_t* skip = nullptr);
 // z = G^T (G r) with (r, z) = |G r|^2 summed inside the G product (symmetric
 // FSAI whose G has rows of at most 16 entries: fsai_dot_fusable).

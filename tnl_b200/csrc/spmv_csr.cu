@@ -415,32 +415,37 @@ __device__ __forceinline__ float ld_keep(const float* a, uint64_t pol)
 }
 
 // Merge-path tile of one warp: at most kTileSize = 256 rows + nonzeros.
-// Warps work independently (no block-wide barrier), so one warp's loads
-// overlap another's arithmetic.  The tile's nonzeros stay in registers in
-// striped order (lane l holds nonzeros k0 + 32 j + l, j < 8): all loads and
-// x gathers are issued before any is used.  The rows ending in the tile are
-// marked in a 256-bit mask at the position of their last nonzero (with the
-// row index beside it); rows with no nonzero in the tile are written at once.
-// Step j then sums its 32 products per row by a segmented shuffle scan whose
-// segments the mask delimits; a lane holding a row's last nonzero writes the
-// row.  The row still open at the end of a step carries into the next one
-// (a step with no row end only adds each lane's product to a per-lane
-// partial, reduced when the row ends), and the row open at the end of the
-// tile goes to the carry array.  Every
-// sum is taken in a fixed order, so results are deterministic.
+// Warps work independently (no block-wide barrier), and blocks are small
+// (four warps), so a block's slot frees as soon as its few warps are done.
+// The tile's nonzeros stay in registers in striped order (lane l holds
+// nonzeros k0 + 32 j + l, j < 8): all loads and x gathers are issued before
+// any is used.  Everything else stays in registers too:
+//  * the rows ending in the tile are marked in a 256-bit mask (eight words,
+//    one per 32-nonzero step) at the position of their last nonzero, each
+//    word an OR-reduction over the warp of the lanes holding those rows;
+//    rows with no nonzero in the tile are written at once;
+//  * step j sums its 32 products per row by a segmented shuffle scan whose
+//    segments the mask delimits, and keeps the scanned values in place of
+//    the products; the row still open at the end of a step carries into the
+//    next (a step with no row end only adds each lane's product to a
+//    per-lane partial, reduced when the row ends);
+//  * the lane of each row then fetches the row's sum from its row-end lane
+//    (one shuffle per step) and the rows are written together;
+//  * the row open at the end of the tile goes to the carry array.
+// Every sum is taken in a fixed order, so results are deterministic.  A
+// row-pointer array inconsistent with the tile plan can misplace sums but
+// never writes outside rows [r0, r1) of the tile.
 template <typename Real>
-__global__ void __launch_bounds__(kTileThreads, 5) k_csr_tile(const int32_t* __restrict__ rowptr,
-                                                          const int32_t* __restrict__ cols,
-                                                          const Real* __restrict__ vals, const Real* __restrict__ x,
-                                                          Real* __restrict__ y, const int32_t* __restrict__ tile_row,
-                                                          const int32_t* __restrict__ tile_nnz, int32_t tiles, int32_t n,
-                                                          int32_t* __restrict__ carry_row, Real* __restrict__ carry_val,
-                                                          Real alpha, Real beta, const int32_t* __restrict__ skip)
+__global__ void __launch_bounds__(kTileThreads) k_csr_tile(const int32_t* __restrict__ rowptr,
+                                                         const int32_t* __restrict__ cols,
+                                                         const Real* __restrict__ vals, const Real* __restrict__ x,
+                                                         Real* __restrict__ y, const int32_t* __restrict__ tile_row,
+                                                         const int32_t* __restrict__ tile_nnz, int32_t tiles, int32_t n,
+                                                         int32_t* __restrict__ carry_row, Real* __restrict__ carry_val,
+                                                         Real alpha, Real beta, const int32_t* __restrict__ skip)
 {
    constexpr int kWarps = kTileThreads / 32;
-   __shared__ uint32_t s_mask[kWarps][kTileItems];
-   __shared__ int32_t s_rowid[kWarps][kTileSize];
-
+   constexpr unsigned kAll = 0xffffffffu;
    // solvers pass their device `done` flag: nothing to do once they stopped
    if (skip && *skip) return;
    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -449,8 +454,6 @@ __global__ void __launch_bounds__(kTileThreads, 5) k_csr_tile(const int32_t* __r
    const int32_t r0 = tile_row[t], r1 = tile_row[t + 1];
    const int32_t k0 = tile_nnz[t], k1 = tile_nnz[t + 1];
    const int32_t nrows = r1 - r0, nk = k1 - k0;
-   uint32_t* sm = s_mask[warp];
-   int32_t* sid = s_rowid[warp];
    const uint64_t pol_stream = policy_evict_first(), pol_keep = policy_evict_last();
 
    int32_t c[kTileItems];
@@ -467,75 +470,109 @@ __global__ void __launch_bounds__(kTileThreads, 5) k_csr_tile(const int32_t* __r
    }
    // the first 32 row ends of the tile, loaded before the x gathers are
    // issued so that both latencies overlap (the gathers need only c)
-   const bool row0 = lane < nrows;
-   int32_t e_end0 = 0, e_beg0 = 0;
-   if (row0) {
-      e_beg0 = rowptr[r0 + lane];
-      e_end0 = rowptr[r0 + lane + 1];
+   int32_t eb0 = 0, ee0 = 0;
+   if (lane < nrows) {
+      eb0 = rowptr[r0 + lane];
+      ee0 = rowptr[r0 + lane + 1];
    }
 #pragma unroll
    for (int j = 0; j < kTileItems; j++) v[j] = c[j] >= 0 ? v[j] * ld_keep(x + c[j], pol_keep) : Real(0);
-   if (lane < kTileItems) sm[lane] = 0u;
-   __syncwarp();
-   // rows ending in the tile: mark the last nonzero, or write a row that has
-   // none here (empty, or all of it in earlier tiles)
-   for (int32_t i = lane; i < nrows; i += 32) {
-      const int32_t r = r0 + i;
-      const int32_t e_end = i == lane ? e_end0 : rowptr[r + 1], e_beg = i == lane ? e_beg0 : rowptr[r];
-      if (e_end > k0 && e_end > e_beg) {
-         const int32_t pos = e_end - k0 - 1;
-         atomicOr(sm + (pos >> 5), 1u << (pos & 31));
-         sid[pos] = r;
+
+   // row-end masks, chunks of 32 rows; a row of chunk q > 0 reloads its ends
+   auto row_ends = [&](int32_t q, int32_t& eb, int32_t& ee) {
+      eb = eb0;
+      ee = ee0;
+      if (q > 0) {
+         const int32_t i = q * 32 + lane;
+         eb = ee = 0;
+         if (i < nrows) {
+            eb = rowptr[r0 + i];
+            ee = rowptr[r0 + i + 1];
+         }
       }
-      else
-         keep(y, r, Real(0), alpha, beta);
+   };
+   uint32_t m[kTileItems];
+#pragma unroll
+   for (int j = 0; j < kTileItems; j++) m[j] = 0u;
+   for (int32_t q = 0; q * 32 < nrows; q++) {
+      const int32_t i = q * 32 + lane;
+      int32_t eb, ee;
+      row_ends(q, eb, ee);
+      const bool mark = i < nrows && ee > k0 && ee > eb;
+      if (i < nrows && !mark) keep(y, r0 + i, Real(0), alpha, beta);
+      const int32_t pos = mark ? ee - k0 - 1 : -1;
+#pragma unroll
+      for (int j = 0; j < kTileItems; j++) {
+         const uint32_t bit = (mark && (pos >> 5) == j) ? (1u << (pos & 31)) : 0u;
+         m[j] |= __reduce_or_sync(kAll, bit);
+      }
    }
-   __syncwarp();
 
    // The open row's partial sum: `carry` (one value) plus, after steps with
    // no row end, the per-lane partials `part`, reduced only when the row
    // ends (most nonzeros of a power-law matrix lie in steps without one).
    Real carry = Real(0), part = Real(0);
    bool parts = false;
-   auto reduce_parts = [&]() -> Real {
-      Real s = part;
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-      return s;
-   };
+   uint32_t last_mask = 0u;  // the mask word of the tile's last nonzero
 #pragma unroll
    for (int j = 0; j < kTileItems; j++) {
       if (j * 32 < nk) {  // warp-uniform
-         const uint32_t m = sm[j];
-         if (m == 0u) {
+         const uint32_t mj = m[j];
+         if (((nk - 1) >> 5) == j) last_mask = mj;
+         if (mj == 0u) {
             part += v[j];
             parts = true;
             continue;
          }
          Real open = carry;
          if (parts) {
-            open += reduce_parts();
+            Real s = part;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(kAll, s, o);
+            open += s;
             part = Real(0);
             parts = false;
          }
-         const uint32_t below = m & ((1u << lane) - 1u);
+         const uint32_t below = mj & ((1u << lane) - 1u);
          const int seg0 = below ? 32 - __clz(below) : 0;  // first lane of this lane's row
          Real val = v[j];
 #pragma unroll
          for (int o = 1; o < 32; o <<= 1) {
-            const Real vv = __shfl_up_sync(0xffffffffu, val, o);
+            const Real vv = __shfl_up_sync(kAll, val, o);
             if (lane - o >= seg0) val += vv;
          }
          if (seg0 == 0) val += open;
-         if ((m >> lane) & 1u) keep(y, sid[j * 32 + lane], val, alpha, beta);
-         const Real last = __shfl_sync(0xffffffffu, val, 31);
-         carry = (m >> 31) ? Real(0) : last;
+         v[j] = val;
+         const Real last = __shfl_sync(kAll, val, 31);
+         carry = (mj >> 31) ? Real(0) : last;
       }
    }
-   if (parts) carry += reduce_parts();
+   if (parts) {
+      Real s = part;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(kAll, s, o);
+      carry += s;
+   }
+   // each row's lane fetches the sum from its row-end lane
+   for (int32_t q = 0; q * 32 < nrows; q++) {
+      const int32_t i = q * 32 + lane;
+      int32_t eb, ee;
+      row_ends(q, eb, ee);
+      const bool mark = i < nrows && ee > k0 && ee > eb;
+      const int32_t pos = mark ? ee - k0 - 1 : 0;
+      Real res = Real(0);
+#pragma unroll
+      for (int j = 0; j < kTileItems; j++) {
+         if (j * 32 < nk) {
+            const Real tv = __shfl_sync(kAll, v[j], pos & 31);
+            if ((pos >> 5) == j) res = tv;
+         }
+      }
+      if (mark) keep(y, r0 + i, res, alpha, beta);
+   }
    if (lane == 0) {
       // the row open at the end of the tile (row r1) carries on
-      const bool has = nk > 0 && !((sm[(nk - 1) >> 5] >> ((nk - 1) & 31)) & 1u);
+      const bool has = nk > 0 && !((last_mask >> ((nk - 1) & 31)) & 1u);
       carry_row[t] = (has && r1 < n) ? r1 : -1;
       carry_val[t] = carry;
    }
