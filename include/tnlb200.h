@@ -359,6 +359,13 @@ tnlb_status tnlb_mtx_write(const char* path, int32_t rows, int32_t columns, cons
  * ExpressionTemplates.h:372-387 (the reference copies it to the host). */
 tnlb_status tnlb_dot(tnlb_real real, int64_t n, const void* d_a, const void* d_b, double* d_result, tnlb_stream stream);
 
+/* y = alpha * x + beta * y over n entries (device) -- the vector
+ * assignment y = alpha * x + beta * y of Containers/detail/
+ * VectorAssignment.h:35-203 through the expression templates; beta == 0
+ * does not read y.  Asynchronous. */
+tnlb_status tnlb_axpby(tnlb_real real, int64_t n, double alpha, const void* d_x, double beta, void* d_y,
+                       tnlb_stream stream);
+
 /* ------------------------------------------------------------ solvers */
 
 /* FGMRES: restarted GMRES with right, flexible preconditioning (the
@@ -541,15 +548,18 @@ tnlb_status tnlb_ilu0_factors(const tnlb_segments* seg, tnlb_real real, const in
                               tnlb_stream stream);
 
 /* ------------------------------------------------- learned FSAI (new) */
-/* A per-row network (16 -> 64 -> 64 -> 64 -> 4, ReLU, BF16 weights, FP32
+/* A per-row network (32 -> 64 -> 64 -> 64 -> 8, ReLU, BF16 weights, FP32
  * accumulation) maps scale-free local coefficients of an SPD matrix A to the
- * values of G on the lower triangle of A's pattern (at most 4 entries per
- * row); M^-1 = G^T G.  No counterpart in the reference.  The features,
- * network, output map and parameter layout are defined in
- * oracle/lfsai_ref.py (FP64 restatement used by the tests). */
+ * values of G on a lower-triangular pattern of at most 8 entries per row:
+ * the lower triangle of A (level 0) or of the pattern of A^2 (level 1, the
+ * default: one level of fill); M^-1 = G^T G.  No counterpart in the
+ * reference.  The features, network, output map, losses and parameter
+ * layout are defined in oracle/lfsai_ref.py (FP64 restatement used by the
+ * tests).  The dense layers run on tcgen05 tensor cores by default, forward
+ * and backward. */
 typedef struct tnlb_lfsai tnlb_lfsai;
 
-/* Number of network parameters (9668). */
+/* Number of network parameters (10952). */
 int64_t tnlb_lfsai_num_params(void);
 /* New network with deterministic initial parameters from `seed`. */
 tnlb_status tnlb_lfsai_create(uint64_t seed, tnlb_stream stream, tnlb_lfsai** out);
@@ -560,13 +570,19 @@ tnlb_status tnlb_lfsai_get_params(const tnlb_lfsai* net, float* h_out, int64_t c
 tnlb_status tnlb_lfsai_set_params(tnlb_lfsai* net, const float* h_in, int64_t count);
 /* Gradient of the last tnlb_lfsai_gradient call, FP32, to host memory. */
 tnlb_status tnlb_lfsai_get_grad(const tnlb_lfsai* net, float* h_out, int64_t count);
-/* Run the dense layers on tcgen05 tensor cores (1) or CUDA cores (0). */
+/* Run the dense layers on tcgen05 tensor cores (1, the default) or on CUDA
+ * cores (0). */
 tnlb_status tnlb_lfsai_set_tensor_cores(tnlb_lfsai* net, int32_t enable);
+/* The pattern of G the network fills: 0 (lower triangle of A) or 1 (lower
+ * triangle of the pattern of A^2, the default). */
+tnlb_status tnlb_lfsai_set_level(tnlb_lfsai* net, int32_t level);
 /* Loss and gradient on one matrix, kept in the handle.  mode 0: probe loss
  * (1/(n P)) sum_p ||z_p - G A G^T z_p||^2 with P probe vectors stored one
  * after another in d_probes (device, n*P values of `real`); mode 1: warm
  * start, mean squared distance of the scaled outputs to the classical FSAI
- * values.  Synchronous. */
+ * values of the level-0 pattern (zero on fill entries); mode 2: Kaporin
+ * loss log(trace(G A G^T)/n) - (2/n) sum_i log G'_ii, exact (no probes).
+ * Synchronous. */
 tnlb_status tnlb_lfsai_gradient(tnlb_lfsai* net, int32_t mode, const tnlb_segments* seg, tnlb_real real,
                                 const int32_t* d_cols, const void* d_values, const void* d_probes, int32_t nprobes,
                                 tnlb_stream stream, double* h_loss);
@@ -576,10 +592,17 @@ tnlb_status tnlb_lfsai_adam_step(tnlb_lfsai* net, double lr, tnlb_stream stream)
 tnlb_status tnlb_lfsai_precond_create(const tnlb_lfsai* net, const tnlb_segments* seg, tnlb_real real,
                                       const int32_t* d_cols, const void* d_values, tnlb_stream stream,
                                       tnlb_precond** out);
-/* Features (n*16) and raw network outputs (n*4) of a matrix, to host memory
+/* Features (n*32) and raw network outputs (n*8) of a matrix, to host memory
  * (either may be NULL).  Synchronous. */
 tnlb_status tnlb_lfsai_eval(const tnlb_lfsai* net, const tnlb_segments* seg, tnlb_real real, const int32_t* d_cols,
                             const void* d_values, tnlb_stream stream, float* h_features, float* h_outputs);
+
+/* Classical FSAI (Kolotilina-Yeremin, M^-1 = G^T G, SPD A) on the level-0
+ * pattern (as tnlb_precond_create with TNLB_PRECOND_FSAI) or the level-1
+ * pattern (lower triangle of the pattern of A^2, at most 32 entries per
+ * row).  No counterpart in the reference.  Blocks until built. */
+tnlb_status tnlb_precond_create_fsai(const tnlb_segments* seg, tnlb_real real, const int32_t* d_cols,
+                                     const void* d_values, int32_t level, tnlb_stream stream, tnlb_precond** out);
 
 #ifdef __cplusplus
 }

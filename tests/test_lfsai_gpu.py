@@ -1,15 +1,18 @@
 """Learned FSAI on the GPU against its FP64 CPU reference (oracle/lfsai_ref.py).
 
 * features: FP32 on the GPU vs FP64, relative 1e-6;
-* network outputs and the gradient of the probe loss: the GPU accumulates in
-  FP32 and rounds layer inputs to BF16 from FP32 values, the reference from
-  FP64 ones, so a few inputs land on the other side of a BF16 rounding
-  boundary; the bound is on the relative 2-norm of the difference (2e-2)
-  and on the loss (1e-4 relative);
+* network outputs and the gradients of the probe loss and of the Kaporin
+  loss: the GPU accumulates in FP32 and rounds layer inputs to BF16 from
+  FP32 values, the reference from FP64 ones (and the tensor-core backward
+  rounds the deltas to BF16 too), so a few inputs land on the other side of
+  a BF16 rounding boundary; the bound is on the relative 2-norm of the
+  difference (2e-2) and on the loss (1e-4 relative);
 * the reference backpropagation itself is checked against central finite
   differences (BF16 rounding off) on the CPU in test_lfsai_reference_fd;
-* training lowers the loss, and the trained preconditioner needs fewer CG
-  iterations than Jacobi on an unseen problem.
+* the tensor-core forward and backward agree with the CUDA-core layers;
+* training lowers the loss and the iteration count below the warm start,
+  and the trained preconditioner needs fewer CG iterations than Jacobi on
+  an unseen problem.
 """
 import numpy as np
 import pytest
@@ -24,39 +27,69 @@ def small_problem(N=24, seed=3):
     return g.diffusion_2d(N, 0.1, 1.5, seed)
 
 
-def test_features_and_outputs_match_reference():
+@pytest.mark.parametrize("level", [0, 1])
+def test_features_and_outputs_match_reference(level):
     from oracle import lfsai_ref as R
     import tnl_b200
     from tnl_b200.lfsai import LearnedFSAI
 
     A = small_problem()
     M = tnl_b200.SparseMatrix.from_csr(A)
-    net = LearnedFSAI(seed=5)
+    net = LearnedFSAI(seed=5, level=level)
     theta = net.params().astype(np.float64)
     assert np.array_equal(net.params(), R.init_params(5).astype(np.float32))
     f_gpu, o_gpu = net.evaluate(M)
-    f_ref, s, pat = R.features(A)
+    f_ref, s, pat = R.features(A, level=level)
     assert np.allclose(f_gpu, f_ref, rtol=1e-6, atol=1e-7)
     o_ref, _ = R.forward(theta, f_ref)
     rel = np.linalg.norm(o_gpu - o_ref) / np.linalg.norm(o_ref)
     assert rel < 2e-2, rel
 
 
-def test_gradient_matches_reference():
+@pytest.mark.parametrize("level", [0, 1])
+@pytest.mark.parametrize("tensor_cores", [True, False])
+def test_gradient_matches_reference(level, tensor_cores):
+    """Probe-loss and Kaporin-loss gradients of the GPU (tensor-core or
+    CUDA-core layers) against the FP64 reference."""
     from oracle import lfsai_ref as R
     import tnl_b200
     from tnl_b200.lfsai import LearnedFSAI
 
     A = small_problem(20, 4)
     M = tnl_b200.SparseMatrix.from_csr(A)
-    net = LearnedFSAI(seed=9)
+    net = LearnedFSAI(seed=9, level=level, tensor_cores=tensor_cores)
+    theta = net.params().astype(np.float64)
     Z = LearnedFSAI.probes(M, 4, seed=1, residual_share=0.5)
     loss = net.gradient(M, Z)
     g_gpu = net.grad().astype(np.float64)
-    L_ref, g_ref = R.loss_and_grad(net.params().astype(np.float64), A, Z.cpu().numpy().T.copy())
+    L_ref, g_ref = R.loss_and_grad(theta, A, Z.cpu().numpy().T.copy(), level)
     assert loss == pytest.approx(L_ref, rel=1e-4)
     rel = np.linalg.norm(g_gpu - g_ref) / np.linalg.norm(g_ref)
     assert rel < 2e-2, rel
+    loss = net.gradient(M, None, mode=2)
+    g_gpu = net.grad().astype(np.float64)
+    K_ref, g_ref = R.kaporin_and_grad(theta, A, level)
+    assert loss == pytest.approx(K_ref, rel=1e-4, abs=1e-6)
+    rel = np.linalg.norm(g_gpu - g_ref) / np.linalg.norm(g_ref)
+    assert rel < 2e-2, rel
+
+
+def test_level1_classical_fsai_matches_reference():
+    """Classical FSAI on the level-1 pattern (tnlb_precond_create_fsai):
+    pattern and values of G against the FP64 reference's local solves."""
+    from oracle import lfsai_ref as R
+    import tnl_b200
+
+    A = small_problem(30, 6)
+    M = tnl_b200.SparseMatrix.from_csr(A)
+    P = tnl_b200.FSAI(level=1)
+    P.update(M)
+    rp, cols, vals = P.factor(0)
+    pat = R.pattern(A, 1)
+    assert np.array_equal(np.diff(rp), [len(J) for J in pat])
+    assert np.array_equal(cols, np.concatenate([np.array(J) for J in pat]))
+    ref = R.fsai_classical(A, 1)
+    assert np.allclose(vals, ref, rtol=1e-10, atol=1e-12)
 
 
 def test_warm_start_and_training_lower_the_loss():
@@ -162,7 +195,7 @@ def test_tensor_core_forward_matches_cuda_cores():
     CUDA-core layers: same BF16 operands, FP32 sums in another order."""
     from tnl_b200.lfsai import LearnedFSAI, diffusion_problem
 
-    net = LearnedFSAI(seed=3)
+    net = LearnedFSAI(seed=3, tensor_cores=False)
     for N in (16, 64, 181):  # 256, 4096 and 32761 rows (ragged last tile)
         M = diffusion_problem(N, 5 + N)
         _, o_cc = net.evaluate(M)
@@ -172,3 +205,64 @@ def test_tensor_core_forward_matches_cuda_cores():
         rel = np.linalg.norm(o_tc - o_cc) / np.linalg.norm(o_cc)
         assert rel < 1e-3, (N, rel)
         assert np.max(np.abs(o_tc - o_cc)) < 1e-2
+
+
+def test_tensor_core_backward_matches_cuda_cores():
+    """The tcgen05 backward pass and weight gradients against the CUDA-core
+    kernels on the same forward pass (the tensor-core path also rounds the
+    deltas to BF16), for the probe loss and the Kaporin loss, on ragged row
+    counts."""
+    from tnl_b200.lfsai import LearnedFSAI, diffusion_problem
+
+    net = LearnedFSAI(seed=11)
+    net.fit_classical([diffusion_problem(32, 1)], steps=20, lr=3e-3)  # non-trivial deltas
+    for N in (16, 64, 181):
+        M = diffusion_problem(N, 7 + N)
+        Z = LearnedFSAI.probes(M, 4, seed=N)
+        for mode, probes in ((0, Z), (2, None)):
+            net.set_tensor_cores(False)
+            l_cc = net.gradient(M, probes, mode=mode)
+            g_cc = net.grad().astype(np.float64)
+            net.set_tensor_cores(True)
+            l_tc = net.gradient(M, probes, mode=mode)
+            g_tc = net.grad().astype(np.float64)
+            assert l_tc == pytest.approx(l_cc, rel=1e-3, abs=1e-6), (N, mode)
+            rel = np.linalg.norm(g_tc - g_cc) / np.linalg.norm(g_cc)
+            assert rel < 1e-2, (N, mode, rel)
+
+
+def _pcg_iterations(M, P, b):
+    import tnl_b200
+
+    S = tnl_b200.CG()
+    S.setMatrix(M)
+    S.setPreconditioner(P)
+    S.setup({"convergence-residue": 1e-8, "max-iterations": 50000})
+    x = torch.zeros(M.getRows(), dtype=torch.float64, device="cuda")
+    assert S.solve(b, x)
+    return S.getIterations()
+
+
+def test_training_lowers_iterations_below_the_warm_start():
+    """The warm start reproduces classical FSAI on A's own pattern; training
+    on the Kaporin loss over the wider level-1 pattern must then cut the
+    PCG iteration count on an unseen problem below the warm start's (and so
+    below classical FSAI's on A's pattern)."""
+    import tnl_b200
+    from tnl_b200 import generators as g
+    from tnl_b200.lfsai import LearnedFSAI, diffusion_problem
+
+    train = [diffusion_problem(64, s) for s in range(8)]
+    net = LearnedFSAI(seed=2)
+    net.fit_classical(train, steps=400, lr=3e-3)
+    M = diffusion_problem(128, 4321)
+    b = torch.tensor(g.uniform_vector(M.getRows(), 1), device="cuda")
+    warm = _pcg_iterations(M, net.preconditioner(M), b)
+    P0 = tnl_b200.FSAI()
+    P0.update(M)
+    classical = _pcg_iterations(M, P0, b)
+    assert warm <= 1.25 * classical, (warm, classical)
+    hist = net.train_kaporin(train, steps=400, lr=1e-3)
+    assert np.mean(hist[-8:]) < np.mean(hist[:8])
+    trained = _pcg_iterations(M, net.preconditioner(M), b)
+    assert trained < 0.95 * warm, (trained, warm, classical)

@@ -550,7 +550,7 @@ class _Preconditioner:
         """(rowptr, cols, values) of an FSAI factor: 0 = G (G_L), 1 = the second
         factor as applied (G^T, or G_U)."""
         n = self.matrix.getRows()
-        cap = self.matrix.getValues().numel()
+        cap = max(self.matrix.getValues().numel(), 32 * n)  # a level-1 FSAI factor outgrows A
         rp = np.zeros(n + 1, np.int32)
         cols = np.zeros(max(cap, 1), np.int32)
         vals = np.zeros(max(cap, 1), np.float64 if self.matrix.real == torch.float64 else np.float32)
@@ -570,10 +570,34 @@ class FSAI2(_Preconditioner):
 
 
 class FSAI(_Preconditioner):
-    """Factorised sparse approximate inverse M^-1 = G^T G, G on the lower
-    triangle of A's pattern with Kolotilina-Yeremin values (no counterpart in
-    the reference)."""
+    """Factorised sparse approximate inverse M^-1 = G^T G with
+    Kolotilina-Yeremin values (no counterpart in the reference); G on the
+    lower triangle of A's pattern (``level=0``, the default) or of the
+    pattern of A^2 (``level=1``: one level of fill)."""
     KIND = capi.PRECOND_FSAI
+
+    def __init__(self, level: int = 0):
+        super().__init__()
+        if level not in (0, 1):
+            raise ValueError("FSAI: the pattern level must be 0 or 1")
+        self.level = level
+
+    def update(self, matrix: SparseMatrix) -> None:
+        if self.level == 0:
+            return super().update(matrix)
+        if matrix.getRows() == 0:
+            raise ValueError("FSAI::update: the matrix is empty")
+        if matrix.getRows() != matrix.getColumns():
+            raise ValueError("FSAI::update: matrix must be square")
+        if self._h:
+            capi.tnlb_precond_destroy(self._h)
+            self._h = C.c_void_p()
+        h = C.c_void_p()
+        check(capi.tnlb_precond_create_fsai(matrix.segments.handle, _real_code(matrix.real),
+                                            matrix.columnIndexes.data_ptr(), matrix.values.data_ptr(), self.level,
+                                            _stream(), C.byref(h)))
+        self._h = h
+        self.matrix = matrix
 
 
 class ILUT(_Preconditioner):
@@ -616,7 +640,7 @@ class ILUT(_Preconditioner):
         entries (columns < i, unit diagonal implied) then its U entries, the
         first U entry the pivot."""
         n = self.matrix.getRows()
-        cap = self.matrix.getValues().numel() * (3 + 2 * self.p) + 2 * n * (self.p + 1) + 16
+        cap = max(self.matrix.getValues().numel(), 32 * n)  # a level-1 FSAI factor outgrows A * (3 + 2 * self.p) + 2 * n * (self.p + 1) + 16
         rp = np.zeros(n + 1, np.int32)
         cols = np.zeros(cap, np.int32)
         vals = np.zeros(cap, np.float64 if self.matrix.real == torch.float64 else np.float32)

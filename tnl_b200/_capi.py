@@ -118,6 +118,7 @@ tnlb_spmv_transposed = _sig("tnlb_spmv_transposed", [_p, C.c_int, _p, _p, _i32, 
 tnlb_spmv_csr_noalloc = _sig("tnlb_spmv_csr_noalloc",
                              [C.c_int, _i32, _i32, C.c_int64, _p, _p, _p, _p, _p, _f64, _f64, _p])
 tnlb_dot = _sig("tnlb_dot", [C.c_int, _i64, _p, _p, _p, _p])
+tnlb_axpby = _sig("tnlb_axpby", [C.c_int, _i64, _f64, _p, _f64, _p, _p])
 tnlb_solver_params_default = _sig("tnlb_solver_params_default", [C.POINTER(SolverParams)], None)
 tnlb_solve = _sig("tnlb_solve", [C.c_int, C.c_int, C.POINTER(SolverParams), _p, C.c_int, _p, _p, _p, _p, _p,
                                  C.POINTER(SolveResult)])
@@ -133,6 +134,7 @@ tnlb_solve_mixed_reliable = _sig("tnlb_solve_mixed_reliable", [C.POINTER(SolverP
                                                                C.c_int, C.c_int, _p, _p, C.POINTER(SolveResult),
                                                                C.POINTER(_i32)])
 tnlb_precond_create_ilut = _sig("tnlb_precond_create_ilut", [_p, C.c_int, _p, _p, _i32, _f64, _p, C.POINTER(_p)])
+tnlb_precond_create_fsai = _sig("tnlb_precond_create_fsai", [_p, C.c_int, _p, _p, _i32, _p, C.POINTER(_p)])
 tnlb_precond_create = _sig("tnlb_precond_create", [C.c_int, _p, C.c_int, _p, _p, _p, C.POINTER(_p)])
 tnlb_precond_solve = _sig("tnlb_precond_solve", [_p, _p, _p, _p])
 tnlb_precond_destroy = _sig("tnlb_precond_destroy", [_p])
@@ -146,6 +148,7 @@ tnlb_lfsai_get_params = _sig("tnlb_lfsai_get_params", [_p, _p, _i64])
 tnlb_lfsai_set_params = _sig("tnlb_lfsai_set_params", [_p, _p, _i64])
 tnlb_lfsai_get_grad = _sig("tnlb_lfsai_get_grad", [_p, _p, _i64])
 tnlb_lfsai_set_tensor_cores = _sig("tnlb_lfsai_set_tensor_cores", [_p, _i32])
+tnlb_lfsai_set_level = _sig("tnlb_lfsai_set_level", [_p, _i32])
 tnlb_lfsai_gradient = _sig("tnlb_lfsai_gradient", [_p, _i32, _p, C.c_int, _p, _p, _p, _i32, _p, C.POINTER(_f64)])
 tnlb_lfsai_adam_step = _sig("tnlb_lfsai_adam_step", [_p, _f64, _p])
 tnlb_lfsai_precond_create = _sig("tnlb_lfsai_precond_create", [_p, _p, C.c_int, _p, _p, _p, C.POINTER(_p)])

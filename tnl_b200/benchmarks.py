@@ -454,6 +454,118 @@ def profile_solvers(problem: str, N: int, iterations: int, out=sys.stdout):
     print(json.dumps({"method": "FP64 FSAI-PCG", "iterations": S.getIterations()}), file=out)
 
 
+def bench_learned_eval(count: int, N: int, weights: str, ilu_count: int = 4, first_seed: int = 10000,
+                       out=sys.stdout):
+    """The learned preconditioner's evaluation: `count` unseen 2D diffusion
+    problems (seeds first_seed.., GRF correlation length ~ U[0.02, 0.2],
+    sigma ~ U[1, 3]) on N x N grids, each solved to an FP64 true residual of
+    1e-8 by
+      * FP64 Jacobi-PCG (convergence residue halved until the true residual
+        is below 1e-8) -- the baseline,
+      * FP32 PCG with reliable FP64 updates and the learned FSAI (network
+        inference = set-up time), the classical FSAI of A's pattern, and the
+        classical FSAI of the level-1 pattern,
+      * FP64 ILU(0)-PCG on the first `ilu_count` problems (its level-
+        scheduled triangular solves make it slow at this size);
+    one JSON line per problem and method, then a summary line with the
+    distribution (min / median / max) of iterations and speed-ups."""
+    import tnl_b200 as t
+    from . import generators as g
+    from .lfsai import LearnedFSAI
+
+    net = LearnedFSAI(seed=0)
+    net.load(weights)
+    rows = []
+    for q in range(count):
+        seed = first_seed + q
+        A = g.diffusion_2d_problem(N, seed)
+        M = t.SparseMatrix.from_csr(A)
+        A32 = t.SparseMatrix(t.CSR, torch.float32).assign(A.rowptr, A.cols, A.vals.astype(np.float32))
+        n = A.n
+        b = torch.tensor(g.uniform_vector(n, 1), device="cuda")
+
+        def zeros():
+            return torch.zeros(n, dtype=torch.float64, device="cuda")
+
+        rec = {"bench": "learned_eval", "problem": seed, "N": N}
+        # FP64 Jacobi-PCG to a true residual of 1e-8
+        P = t.Diagonal()
+        P.update(M)
+        tol = 1e-8
+        while True:
+            S = t.CG()
+            S.setMatrix(M)
+            S.setPreconditioner(P)
+            S.setConvergenceResidue(tol)
+            S.setMaxIterations(200000)
+            x = zeros()
+            ok, ms = _timed(lambda: S.solve(b, x))
+            if t.true_residual(M, b, x) < 1e-8 or tol < 1e-12:
+                break
+            tol *= 0.5
+        rec["fp64_jacobi"] = {"iterations": S.getIterations(), "solve_ms": ms, "converged": bool(ok),
+                              "true_residual": t.true_residual(M, b, x)}
+
+        def reliable(key, make):
+            Pm, setup = make()
+            t.solve_mixed_reliable(M, b, zeros(), tol=1e-8, inner=Pm, max_iterations=20)
+            x = zeros()
+            r, ms = _timed(lambda: t.solve_mixed_reliable(M, b, x, tol=1e-8, delta=0.3, inner=Pm))
+            rec[key] = {"iterations": r["iterations"], "solve_ms": ms, "setup_ms": setup,
+                        "converged": bool(r["converged"]), "true_residual": t.true_residual(M, b, x),
+                        "speedup_vs_fp64_jacobi": rec["fp64_jacobi"]["solve_ms"] / ms,
+                        "speedup_with_setup": rec["fp64_jacobi"]["solve_ms"] / (ms + setup)}
+
+        def learned():
+            net.preconditioner(A32)
+            return _timed(lambda: net.preconditioner(A32))
+
+        def classical(level):
+            def make():
+                Pc = t.FSAI(level)
+                _, s = _timed(lambda: Pc.update(A32))
+                return Pc, s
+            return make
+
+        reliable("fp32_learned_fsai", learned)
+        reliable("fp32_fsai_level0", classical(0))
+        reliable("fp32_fsai_level1", classical(1))
+        if q < ilu_count:
+            P = t.ILU0()
+            _, setup = _timed(lambda: P.update(M))
+            S = t.CG()
+            S.setMatrix(M)
+            S.setPreconditioner(P)
+            S.setConvergenceResidue(1e-8)
+            S.setMaxIterations(200000)
+            x = zeros()
+            ok, ms = _timed(lambda: S.solve(b, x))
+            rec["fp64_ilu0"] = {"iterations": S.getIterations(), "solve_ms": ms, "setup_ms": setup,
+                                "converged": bool(ok), "true_residual": t.true_residual(M, b, x)}
+        print(json.dumps(rec), file=out, flush=True)
+        rows.append(rec)
+        del M, A32
+        torch.cuda.empty_cache()
+    summary = {"bench": "learned_eval_summary", "problems": len(rows), "N": N}
+    for key in ("fp64_jacobi", "fp32_learned_fsai", "fp32_fsai_level0", "fp32_fsai_level1", "fp64_ilu0"):
+        its = [r[key]["iterations"] for r in rows if key in r]
+        if not its:
+            continue
+        ent = {"iterations": [int(np.min(its)), float(np.median(its)), int(np.max(its))],
+               "all_converged": all(r[key]["converged"] for r in rows if key in r)}
+        ms = [r[key]["solve_ms"] for r in rows if key in r]
+        ent["solve_ms"] = [float(np.min(ms)), float(np.median(ms)), float(np.max(ms))]
+        if key.startswith("fp32"):
+            sp = [r[key]["speedup_with_setup"] for r in rows]
+            ent["speedup_with_setup_vs_fp64_jacobi"] = [float(np.min(sp)), float(np.median(sp)), float(np.max(sp))]
+            ent["setup_ms_median"] = float(np.median([r[key]["setup_ms"] for r in rows]))
+        summary[key] = ent
+    summary["learned_vs_fsai_level0_iterations_median"] = float(np.median(
+        [r["fp32_learned_fsai"]["iterations"] / r["fp32_fsai_level0"]["iterations"] for r in rows]))
+    print(json.dumps(summary), file=out, flush=True)
+    return summary
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(prog="python -m tnl_b200.benchmarks")
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -472,11 +584,19 @@ def main(argv=None):
     b.add_argument("--problem", default="laplacian", choices=["laplacian", "diffusion"])
     b.add_argument("--N", type=int, default=1024)
     b.add_argument("--weights", default=str(Path(__file__).resolve().parent / "weights" / "lfsai_diffusion.npy"))
+    le = sub.add_parser("learned-eval")
+    le.add_argument("--count", type=int, default=64)
+    le.add_argument("--N", type=int, default=2048)
+    le.add_argument("--ilu-count", type=int, default=4)
+    le.add_argument("--weights", default=str(Path(__file__).resolve().parent / "weights" / "lfsai_diffusion.npy"))
     pr = sub.add_parser("profile-solvers")
     pr.add_argument("--problem", default="diffusion", choices=["laplacian", "diffusion"])
     pr.add_argument("--N", type=int, default=2048)
     pr.add_argument("--iterations", type=int, default=40)
     args = ap.parse_args(argv)
+    if args.cmd == "learned-eval":
+        bench_learned_eval(args.count, args.N, args.weights, args.ilu_count)
+        return 0
     if args.cmd == "profile-solvers":
         profile_solvers(args.problem, args.N, args.iterations)
         return 0

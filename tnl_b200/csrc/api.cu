@@ -20,6 +20,14 @@ void clear_error() { g_last_error.clear(); }
 
 namespace {
 
+// y = alpha x + beta y (beta == 0: y is not read)
+template <typename Real>
+__global__ void k_axpby(int64_t n, Real alpha, const Real* __restrict__ x, Real beta, Real* __restrict__ y)
+{
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+      y[i] = beta == Real(0) ? alpha * x[i] : alpha * x[i] + beta * y[i];
+}
+
 template <typename T>
 __global__ void k_dot(int64_t n, const T* __restrict__ a, const T* __restrict__ b, double* __restrict__ out)
 {
@@ -248,6 +256,25 @@ tnlb_status tnlb_spmv(const tnlb_segments* seg, tnlb_real real, const int32_t* d
 
 int32_t tnlb_spmv_last_launch_count(void) { return g_last_launches; }
 
+tnlb_status tnlb_axpby(tnlb_real real, int64_t n, double alpha, const void* d_x, double beta, void* d_y,
+                       tnlb_stream stream)
+{
+   clear_error();
+   TNLB_REQUIRE(real == TNLB_F32 || real == TNLB_F64, TNLB_ERR_INVALID_ARGUMENT, "unknown real type");
+   TNLB_REQUIRE(n >= 0, TNLB_ERR_INVALID_ARGUMENT, "negative size");
+   if (n == 0) return TNLB_OK;
+   TNLB_REQUIRE(d_x && d_y, TNLB_ERR_INVALID_ARGUMENT, "null vector");
+   cudaStream_t st = (cudaStream_t)stream;
+   unsigned g = grid_for(n, 256 * 4);
+   if (g > 148 * 8) g = 148 * 8;
+   if (real == TNLB_F64)
+      k_axpby<double><<<g, 256, 0, st>>>(n, alpha, (const double*)d_x, beta, (double*)d_y);
+   else
+      k_axpby<float><<<g, 256, 0, st>>>(n, (float)alpha, (const float*)d_x, (float)beta, (float*)d_y);
+   TNLB_CHECK_LAUNCH();
+   return TNLB_OK;
+}
+
 tnlb_status tnlb_dot(tnlb_real real, int64_t n, const void* d_a, const void* d_b, double* d_result, tnlb_stream stream)
 {
    clear_error();
@@ -400,6 +427,29 @@ tnlb_status tnlb_precond_create(tnlb_precond_kind kind, const tnlb_segments* seg
    return tnlb::precond_create(kind, seg, real, d_cols, d_values, (cudaStream_t)stream, out);
 }
 
+tnlb_status tnlb_precond_create_fsai(const tnlb_segments* seg, tnlb_real real, const int32_t* d_cols,
+                                     const void* d_values, int32_t level, tnlb_stream stream, tnlb_precond** out)
+{
+   clear_error();
+   TNLB_REQUIRE(seg && out, TNLB_ERR_INVALID_ARGUMENT, "null argument");
+   TNLB_REQUIRE(real == TNLB_F32 || real == TNLB_F64, TNLB_ERR_INVALID_ARGUMENT, "unknown real type");
+   TNLB_REQUIRE(level == 0 || level == 1, TNLB_ERR_INVALID_ARGUMENT, "the pattern level must be 0 or 1");
+   TNLB_REQUIRE(seg->n > 0, TNLB_ERR_INVALID_ARGUMENT, "Preconditioner::update: the matrix is empty");
+   *out = nullptr;
+   auto* P = new tnlb_precond();
+   P->kind = TNLB_PRECOND_FSAI;
+   P->real = real;
+   P->n = seg->n;
+   const tnlb_status s = tnlb::fsai_create(seg, real, d_cols, d_values, true, (cudaStream_t)stream, &P->fsai, false,
+                                           level);
+   if (s != TNLB_OK) {
+      delete P;
+      return s;
+   }
+   *out = P;
+   return TNLB_OK;
+}
+
 tnlb_status tnlb_precond_create_ilut(const tnlb_segments* seg, tnlb_real real, const int32_t* d_cols,
                                      const void* d_values, int32_t p, double threshold, tnlb_stream stream,
                                      tnlb_precond** out)
@@ -530,16 +580,26 @@ tnlb_status tnlb_lfsai_set_tensor_cores(tnlb_lfsai* net, int32_t enable)
    return TNLB_OK;
 }
 
+tnlb_status tnlb_lfsai_set_level(tnlb_lfsai* net, int32_t level)
+{
+   clear_error();
+   TNLB_REQUIRE(net != nullptr, TNLB_ERR_INVALID_ARGUMENT, "null network");
+   TNLB_REQUIRE(level == 0 || level == 1, TNLB_ERR_INVALID_ARGUMENT, "the pattern level must be 0 or 1");
+   net->level = level;
+   return TNLB_OK;
+}
+
 tnlb_status tnlb_lfsai_gradient(tnlb_lfsai* net, int32_t mode, const tnlb_segments* seg, tnlb_real real,
                                 const int32_t* d_cols, const void* d_values, const void* d_probes, int32_t nprobes,
                                 tnlb_stream stream, double* h_loss)
 {
    clear_error();
    TNLB_REQUIRE(net && seg && h_loss, TNLB_ERR_INVALID_ARGUMENT, "null argument");
-   TNLB_REQUIRE(mode == 0 || mode == 1, TNLB_ERR_INVALID_ARGUMENT, "mode must be 0 (probe loss) or 1 (warm start)");
-   TNLB_REQUIRE(mode == 1 || (d_probes && nprobes > 0), TNLB_ERR_INVALID_ARGUMENT, "probe vectors required");
+   TNLB_REQUIRE(mode >= 0 && mode <= 2, TNLB_ERR_INVALID_ARGUMENT,
+                "mode must be 0 (probe loss), 1 (warm start) or 2 (Kaporin loss)");
+   TNLB_REQUIRE(mode != 0 || (d_probes && nprobes > 0), TNLB_ERR_INVALID_ARGUMENT, "probe vectors required");
    TNLB_REQUIRE(seg->n > 0, TNLB_ERR_INVALID_ARGUMENT, "the matrix is empty");
-   return lfsai_gradient(net, seg, real, d_cols, d_values, d_probes, nprobes, mode == 1, (cudaStream_t)stream, h_loss);
+   return lfsai_gradient(net, seg, real, d_cols, d_values, d_probes, nprobes, mode, (cudaStream_t)stream, h_loss);
 }
 
 tnlb_status tnlb_lfsai_adam_step(tnlb_lfsai* net, double lr, tnlb_stream stream)

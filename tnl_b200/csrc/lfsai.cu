@@ -2,21 +2,32 @@
 // in the reference library).
 //
 // A per-row network maps local, scale-free coefficients of A to the values of
-// G on the lower triangle of A's pattern (at most 4 entries per row); the
-// preconditioner is M^-1 = G^T G, applied by two SpMVs (fsai.cu), so CG stays
-// symmetric positive definite.  Training minimises the probe estimate of
-// ||I - G A G^T||_F^2 / n:
-//    L = 1/(n P) sum_p ||z_p - G A G^T z_p||^2,
-//    dL/dG = -2/(n P) sum_p (u_p w_p^T + z_p q_p^T) on G's pattern,
-// with w = A G^T z, u = z - G w, q = A G^T u -- every product a library SpMV.
+// G on a lower-triangular pattern with at most 8 entries per row: the lower
+// triangle of A (level 0) or of the pattern of A^2 (level 1: one level of
+// fill, 7 entries per row of a 5-point operator).  The preconditioner is
+// M^-1 = G^T G, applied by two SpMVs (fsai.cu), so CG stays symmetric
+// positive definite.  Three training objectives, each with its gradient
+// dL/dG on the pattern:
+//  * the probe estimate of ||I - G A G^T||_F^2 / n,
+//       L = 1/(n P) sum_p ||z_p - G A G^T z_p||^2,
+//       dL/dG = -2/(n P) sum_p (u_p w_p^T + z_p q_p^T),
+//    with w = A G^T z, u = z - G w, q = A G^T u -- every product a library
+//    SpMV; the probes are Rademacher vectors and residuals the solver leaves;
+//  * the Kaporin loss K = log(trace(G A G^T)/n) - (2/n) sum_i log G_ii (+ a
+//    constant): the log of Kaporin's condition number of G A G^T, exact,
+//    from the local blocks A[J,J] (classical FSAI is its minimiser on a
+//    given pattern);
+//  * the warm start: regression onto classical FSAI of the level-0 pattern
+//    (zero on the fill entries of a level-1 pattern).
 //
-// Definitions of the features, the network (16 -> 64 -> 64 -> 64 -> 4, ReLU,
+// Definitions of the features, the network (32 -> 64 -> 64 -> 64 -> 8, ReLU,
 // BF16 weights and layer inputs, FP32 accumulation), the output map
-// (G'_diag = exp(o_3), G_ij = G'_ij / sqrt(a_jj)) and the parameter layout are
-// written out in the CPU reference the tests use (oracle/lfsai_ref.py); this
-// file implements exactly those.  Dense layers: the tensor-core path
-// (lfsai_tc.cu, tcgen05 with accumulators in TMEM) when `use_tc`, else the
-// CUDA-core kernels below, which also serve as its on-GPU reference.
+// (G'_diag = exp(o_7), G_ij = G'_ij / sqrt(a_jj)) and the parameter layout
+// are written out in the CPU reference the tests use (oracle/lfsai_ref.py);
+// this file implements exactly those.  Dense layers, forward and backward:
+// the tensor-core path (lfsai_tc.cu, tcgen05 with accumulators in TMEM) by
+// default, else the CUDA-core kernels below, which also serve as its
+// on-GPU reference.
 #include <cmath>
 #include <vector>
 
@@ -54,8 +65,9 @@ __device__ __forceinline__ Real lookup(const int32_t* rp, const int32_t* cols, c
    return Real(0);
 }
 
-// Features (n x 16, FP32) and scaling s = 1/sqrt(diag) from A (CSR, ascending
-// columns) and G's pattern.
+// Features (n x 32, FP32) and scaling s = 1/sqrt(diag) from A (CSR, ascending
+// columns) and G's pattern: the scaled entries B(J_p, J_q) of the 28 slot
+// pairs p < q, the first three scaled entries right of the diagonal, k/8.
 template <typename Real>
 __global__ void k_features(const int32_t* __restrict__ arp, const int32_t* __restrict__ acols,
                            const Real* __restrict__ avals, const int32_t* __restrict__ grp,
@@ -65,40 +77,42 @@ __global__ void k_features(const int32_t* __restrict__ arp, const int32_t* __res
    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
    if (i >= n) return;
    const int32_t b = grp[i], k = grp[i + 1] - b;
-   float out[kLfF];
-#pragma unroll
-   for (int q = 0; q < kLfF; q++) out[q] = 0.f;
    if (k > kLfK || k < 1) {
       atomicExch(err, 1);
       for (int q = 0; q < kLfF; q++) f[i * kLfF + q] = 0.f;
       return;
    }
    int32_t slot_col[kLfK];
+   double slot_s[kLfK];
 #pragma unroll
-   for (int t = 0; t < kLfK; t++) slot_col[t] = -1;
-   for (int t = 0; t < k; t++) slot_col[kLfK - k + t] = gcols[b + t];
-   auto sc = [&](int32_t j) -> double {
-      const double d = (double)lookup(arp, acols, avals, j, j);
-      return 1.0 / sqrt(d);
-   };
-   const int pp[6] = {0, 0, 0, 1, 1, 2}, qq[6] = {1, 2, 3, 2, 3, 3};
-   for (int m = 0; m < 6; m++) {
-      const int32_t jp = slot_col[pp[m]], jq = slot_col[qq[m]];
-      if (jp >= 0 && jq >= 0) out[m] = (float)((double)lookup(arp, acols, avals, jp, jq) * sc(jp) * sc(jq));
+   for (int t = 0; t < kLfK; t++) {
+      slot_col[t] = -1;
+      slot_s[t] = 0.0;
    }
-   const double si = sc((int32_t)i);
-   int up = 0, nup = 0;
-   for (int32_t q = arp[i]; q < arp[i + 1]; q++) {
+   for (int t = 0; t < k; t++) {
+      const int32_t j = gcols[b + t];
+      slot_col[kLfK - k + t] = j;
+      slot_s[kLfK - k + t] = 1.0 / sqrt((double)lookup(arp, acols, avals, j, j));
+   }
+   int m = 0;
+   for (int p = 0; p < kLfK; p++)
+      for (int q = p + 1; q < kLfK; q++, m++) {
+         const int32_t jp = slot_col[p], jq = slot_col[q];
+         float v = 0.f;
+         if (jp >= 0 && jq >= 0) v = (float)((double)lookup(arp, acols, avals, jp, jq) * slot_s[p] * slot_s[q]);
+         f[i * kLfF + m] = v;
+      }
+   const double si = slot_s[kLfK - 1];
+   int up = 0;
+   for (int32_t q = arp[i]; q < arp[i + 1] && up < 3; q++) {
       const int32_t j = acols[q];
       if (j > i) {
-         if (up < 3) out[6 + up++] = (float)((double)avals[q] * si * sc(j));
-         nup++;
+         const double sj = 1.0 / sqrt((double)lookup(arp, acols, avals, j, j));
+         f[i * kLfF + kLfPairs + up++] = (float)((double)avals[q] * si * sj);
       }
    }
-   out[9] = (float)k / 4.f;
-   out[10] = (float)nup / 3.f;
-#pragma unroll
-   for (int q = 0; q < kLfF; q++) f[i * kLfF + q] = out[q];
+   for (; up < 3; up++) f[i * kLfF + kLfPairs + up] = 0.f;
+   f[i * kLfF + kLfF - 1] = (float)k / (float)kLfK;
    s[i] = (Real)si;
 }
 
@@ -193,7 +207,9 @@ __global__ void k_do(const double* __restrict__ dg, const float* __restrict__ o,
 {
    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
    if (i >= n) return;
-   float d[kLfK] = {0.f, 0.f, 0.f, 0.f};
+   float d[kLfK];
+#pragma unroll
+   for (int t = 0; t < kLfK; t++) d[t] = 0.f;
    const int32_t b = grp[i], k = grp[i + 1] - b;
    for (int t = 0; t < k; t++) {
       const int slot = kLfK - k + t;
@@ -312,7 +328,9 @@ __global__ void __launch_bounds__(kRedThreads) k_fit_do(const float* __restrict_
 {
    double acc = 0;
    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-      float d[kLfK] = {0.f, 0.f, 0.f, 0.f};
+      float d[kLfK];
+#pragma unroll
+      for (int t = 0; t < kLfK; t++) d[t] = 0.f;
       const int32_t b = grp[i], k = grp[i + 1] - b;
       for (int t = 0; t < k; t++) {
          const int slot = kLfK - k + t;
@@ -330,6 +348,105 @@ __global__ void __launch_bounds__(kRedThreads) k_fit_do(const float* __restrict_
       double t[1];
       gather_totals<1>(t, w);
       if (threadIdx.x == 0) *loss = t[0] / n;
+   }
+}
+
+// Kaporin loss, pass 1: per row q_i = G'_i B[J,J] G'_i^T (B = S A S) and
+// log G'_ii = o_7, summed over all rows in a fixed block order into
+// tot[0] = T = trace(G A G^T) and tot[1] = sum_i log G'_ii.
+template <typename Real>
+__device__ __forceinline__ int kap_row(const int32_t* arp, const int32_t* acols, const Real* avals,
+                                       const int32_t* grp, const int32_t* gcols, const float* o, int64_t i,
+                                       int32_t (&col)[kLfK], double (&sc)[kLfK], double (&g)[kLfK])
+{
+   const int32_t b = grp[i], k = grp[i + 1] - b;
+   for (int t = 0; t < k; t++) {
+      col[t] = gcols[b + t];
+      sc[t] = 1.0 / sqrt((double)lookup(arp, acols, avals, col[t], col[t]));
+      const int slot = kLfK - k + t;
+      g[t] = slot == kLfK - 1 ? exp((double)o[i * kLfK + slot]) : (double)o[i * kLfK + slot];
+   }
+   return k;
+}
+
+template <typename Real>
+__global__ void __launch_bounds__(kRedThreads) k_kap_sums(const int32_t* __restrict__ arp,
+                                                          const int32_t* __restrict__ acols,
+                                                          const Real* __restrict__ avals,
+                                                          const int32_t* __restrict__ grp,
+                                                          const int32_t* __restrict__ gcols, int32_t n,
+                                                          const float* __restrict__ o, RedWork w,
+                                                          double* __restrict__ tot)
+{
+   double tr = 0, ld = 0;
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+      int32_t col[kLfK];
+      double sc[kLfK], g[kLfK];
+      const int k = kap_row(arp, acols, avals, grp, gcols, o, i, col, sc, g);
+      double q = 0;
+      for (int p = 0; p < k; p++) {
+         double r = 0;
+         for (int c = 0; c < k; c++) r += (double)lookup(arp, acols, avals, col[p], col[c]) * sc[p] * sc[c] * g[c];
+         q += g[p] * r;
+      }
+      tr += q;
+      ld += (double)o[i * kLfK + kLfK - 1];
+   }
+   double vv[2] = {tr, ld};
+   if (publish_and_arrive<2>(vv, w)) {
+      double t[2];
+      gather_totals<2>(t, w);
+      if (threadIdx.x == 0) {
+         tot[0] = t[0];
+         tot[1] = t[1];
+      }
+   }
+}
+
+// Kaporin loss, pass 2: dK/do per row from dK/dG'_i = (2/T) B[J,J] G'_i -
+// (2/n) e_last / G'_ii (the diagonal slot through G'_ii = exp(o_7)).
+template <typename Real>
+__global__ void k_kap_do(const int32_t* __restrict__ arp, const int32_t* __restrict__ acols,
+                         const Real* __restrict__ avals, const int32_t* __restrict__ grp,
+                         const int32_t* __restrict__ gcols, int32_t n, const float* __restrict__ o,
+                         const double* __restrict__ tot, float* __restrict__ dout)
+{
+   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+   if (i >= n) return;
+   const double T = tot[0];
+   int32_t col[kLfK];
+   double sc[kLfK], g[kLfK];
+   const int k = kap_row(arp, acols, avals, grp, gcols, o, i, col, sc, g);
+   float d[kLfK];
+#pragma unroll
+   for (int t = 0; t < kLfK; t++) d[t] = 0.f;
+   for (int p = 0; p < k; p++) {
+      double r = 0;
+      for (int c = 0; c < k; c++) r += (double)lookup(arp, acols, avals, col[p], col[c]) * sc[p] * sc[c] * g[c];
+      double dg = (2.0 / T) * r;
+      if (p == k - 1) dg = (dg - 2.0 / ((double)n * g[k - 1])) * g[k - 1];
+      d[kLfK - k + p] = (float)dg;
+   }
+#pragma unroll
+   for (int t = 0; t < kLfK; t++) dout[i * kLfK + t] = d[t];
+}
+
+// Warm-start target on G's pattern: the values of `src` (classical FSAI of
+// the level-0 pattern, rows sorted by column) where its pattern has the
+// column, zero on the fill entries.
+template <typename Real>
+__global__ void k_map_target(const int32_t* __restrict__ grp, const int32_t* __restrict__ gcols,
+                             const int32_t* __restrict__ srp, const int32_t* __restrict__ scols,
+                             const Real* __restrict__ svals, int32_t n, Real* __restrict__ out)
+{
+   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+   if (i >= n) return;
+   int32_t q = srp[i];
+   const int32_t qe = srp[i + 1];
+   for (int32_t e = grp[i]; e < grp[i + 1]; e++) {
+      const int32_t j = gcols[e];
+      while (q < qe && scols[q] < j) q++;
+      out[e] = (q < qe && scols[q] == j) ? svals[q] : Real(0);
    }
 }
 
@@ -372,9 +489,9 @@ namespace {
 
 template <typename Real>
 tnlb_status build_matrix_ctx(const tnlb_segments* seg, tnlb_real real, const int32_t* cols, const Real* vals,
-                             cudaStream_t st, LfsaiMatrix* M)
+                             int level, cudaStream_t st, LfsaiMatrix* M)
 {
-   TNLB_TRY_STATUS(fsai_create(seg, real, cols, vals, false, st, &M->F));
+   TNLB_TRY_STATUS(fsai_create(seg, real, cols, vals, false, st, &M->F, false, level));
    const int32_t n = seg->n;
    TNLB_TRY_STATUS(M->feat.alloc(sizeof(float) * (size_t)n * kLfF));
    TNLB_TRY_STATUS(M->s.alloc(sizeof(Real) * n));
@@ -389,7 +506,7 @@ tnlb_status build_matrix_ctx(const tnlb_segments* seg, tnlb_real real, const int
    TNLB_CUDA_TRY(cudaMemcpyAsync(&h, err.ptr, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
    TNLB_CUDA_TRY(cudaStreamSynchronize(st));
    TNLB_REQUIRE(h == 0, TNLB_ERR_INVALID_ARGUMENT,
-                "learned FSAI: a row holds more than 4 stored entries in its lower triangle");
+                "learned FSAI: a row of G's pattern holds more than 8 entries");
    return TNLB_OK;
 }
 
@@ -428,6 +545,7 @@ tnlb_status wgrad_layer(const float* dout, const float* in, int64_t n, int64_t r
 tnlb_status lfsai_backward(tnlb_lfsai* net, const float* feat, int64_t n, const float* h1, const float* h2,
                            const float* h3, const float* dout, cudaStream_t st)
 {
+   if (net->use_tc) return lfsai_backward_tc(net, feat, n, h1, h2, h3, dout, st);
    const float* wr = net->wround.as<float>();
    DeviceBuffer d3, d2, d1, part;
    TNLB_TRY_STATUS(d3.alloc(sizeof(float) * n * kLfH));
@@ -451,12 +569,13 @@ tnlb_status lfsai_backward(tnlb_lfsai* net, const float* feat, int64_t n, const 
 
 template <typename Real>
 tnlb_status gradient_t(tnlb_lfsai* net, const tnlb_segments* seg, const int32_t* cols, const Real* vals,
-                       const Real* probes, int32_t P, cudaStream_t st, double* h_loss, bool fit)
+                       const Real* probes, int32_t P, cudaStream_t st, double* h_loss, int mode)
 {
    const int32_t n = seg->n;
    const tnlb_real real = sizeof(Real) == 8 ? TNLB_F64 : TNLB_F32;
+   const bool fit = mode == 1;
    LfsaiMatrix M;
-   TNLB_TRY_STATUS(build_matrix_ctx<Real>(seg, real, cols, vals, st, &M));
+   TNLB_TRY_STATUS(build_matrix_ctx<Real>(seg, real, cols, vals, net->level, st, &M));
    Fsai* F = M.F;
    const int64_t gnnz = F->g->elements;
    lf::k_round_weights<<<(kLfParams + 255) / 256, 256, 0, st>>>(net->theta.as<float>(), net->wround.as<float>());
@@ -476,18 +595,43 @@ tnlb_status gradient_t(tnlb_lfsai* net, const tnlb_segments* seg, const int32_t*
    RedWork rw{red.as<double>(), cnt.as<unsigned>()};
    TNLB_TRY_STATUS(lfsai_forward(net, M.feat.as<float>(), n, o.as<float>(), h1.as<float>(), h2.as<float>(),
                                  h3.as<float>(), st));
+   double kap_n = 0.0;  // Kaporin loss: n, for the host-side value
    if (fit) {
-      // supervised warm start on the classical FSAI values
+      // supervised warm start on the classical FSAI values of the level-0
+      // pattern (zero on fill entries)
       DeviceBuffer tg;
       TNLB_TRY_STATUS(tg.alloc(sizeof(Real) * gnnz));
       Fsai* C = nullptr;
       TNLB_TRY_STATUS(fsai_create(seg, real, cols, vals, true, st, &C));
-      TNLB_CUDA_TRY(cudaMemcpyAsync(tg.ptr, C->g_vals.ptr, sizeof(Real) * gnnz, cudaMemcpyDeviceToDevice, st));
+      lf::k_map_target<Real><<<grid_for(n, 128), 128, 0, st>>>(
+         F->g->offsets.as<int32_t>(), F->g_cols.as<int32_t>(), C->g->offsets.as<int32_t>(), C->g_cols.as<int32_t>(),
+         C->g_vals.as<Real>(), n, tg.as<Real>());
+      TNLB_CHECK_LAUNCH();
+      TNLB_CUDA_TRY(cudaStreamSynchronize(st));
       fsai_destroy(C);
       lf::k_fit_do<Real><<<vec_grid(n), kRedThreads, 0, st>>>(o.as<float>(), tg.as<Real>(), M.s.as<Real>(),
                                                               F->g->offsets.as<int32_t>(), F->g_cols.as<int32_t>(), n,
                                                               dout.as<float>(), rw, loss.as<double>());
       TNLB_CHECK_LAUNCH();
+   }
+   else if (mode == 2) {
+      // Kaporin loss: T and sum log G'_ii, then dK/do
+      DeviceBuffer tot;
+      TNLB_TRY_STATUS(tot.alloc(sizeof(double) * 2));
+      lf::k_kap_sums<Real><<<vec_grid(n), kRedThreads, 0, st>>>(
+         F->a_rp.as<int32_t>(), F->a_cols.as<int32_t>(), F->a_vals.as<Real>(), F->g->offsets.as<int32_t>(),
+         F->g_cols.as<int32_t>(), n, o.as<float>(), rw, tot.as<double>());
+      TNLB_CHECK_LAUNCH();
+      lf::k_kap_do<Real><<<grid_for(n, 128), 128, 0, st>>>(F->a_rp.as<int32_t>(), F->a_cols.as<int32_t>(),
+                                                           F->a_vals.as<Real>(), F->g->offsets.as<int32_t>(),
+                                                           F->g_cols.as<int32_t>(), n, o.as<float>(),
+                                                           tot.as<double>(), dout.as<float>());
+      TNLB_CHECK_LAUNCH();
+      double ht[2] = {0, 0};
+      TNLB_CUDA_TRY(cudaMemcpyAsync(ht, tot.ptr, sizeof(ht), cudaMemcpyDeviceToHost, st));
+      TNLB_CUDA_TRY(cudaStreamSynchronize(st));
+      TNLB_REQUIRE(ht[0] > 0, TNLB_ERR_BREAKDOWN, "learned FSAI: trace(G A G^T) is not positive");
+      kap_n = std::log(ht[0] / n) - 2.0 * ht[1] / n;
    }
    else {
       lf::k_g_values<Real><<<grid_for(n, 128), 128, 0, st>>>(o.as<float>(), M.s.as<Real>(), F->g->offsets.as<int32_t>(),
@@ -521,7 +665,7 @@ tnlb_status gradient_t(tnlb_lfsai* net, const tnlb_segments* seg, const int32_t*
    double hl = 0;
    TNLB_CUDA_TRY(cudaMemcpyAsync(&hl, loss.ptr, sizeof(double), cudaMemcpyDeviceToHost, st));
    TNLB_CUDA_TRY(cudaStreamSynchronize(st));
-   *h_loss = fit ? hl : hl / ((double)n * P);
+   *h_loss = mode == 2 ? kap_n : fit ? hl : hl / ((double)n * P);
    return TNLB_OK;
 }
 
@@ -531,7 +675,7 @@ tnlb_status precond_t(const tnlb_lfsai* net, const tnlb_segments* seg, const int
 {
    const tnlb_real real = sizeof(Real) == 8 ? TNLB_F64 : TNLB_F32;
    auto* M = new LfsaiMatrix();
-   tnlb_status s = build_matrix_ctx<Real>(seg, real, cols, vals, st, M);
+   tnlb_status s = build_matrix_ctx<Real>(seg, real, cols, vals, net->level, st, M);
    if (s != TNLB_OK) {
       delete M;
       return s;
@@ -565,11 +709,13 @@ tnlb_status precond_t(const tnlb_lfsai* net, const tnlb_segments* seg, const int
 }  // namespace
 
 tnlb_status lfsai_gradient(tnlb_lfsai* net, const tnlb_segments* seg, tnlb_real real, const int32_t* cols,
-                           const void* vals, const void* probes, int32_t P, bool fit, cudaStream_t st, double* loss)
+                           const void* vals, const void* probes, int32_t P, int mode, cudaStream_t st, double* loss)
 {
+   TNLB_REQUIRE(mode >= 0 && mode <= 2, TNLB_ERR_INVALID_ARGUMENT, "learned FSAI: unknown training mode");
+   TNLB_REQUIRE(mode != 0 || (probes && P > 0), TNLB_ERR_INVALID_ARGUMENT, "learned FSAI: the probe loss needs probes");
    if (real == TNLB_F64)
-      return gradient_t<double>(net, seg, cols, (const double*)vals, (const double*)probes, P, st, loss, fit);
-   return gradient_t<float>(net, seg, cols, (const float*)vals, (const float*)probes, P, st, loss, fit);
+      return gradient_t<double>(net, seg, cols, (const double*)vals, (const double*)probes, P, st, loss, mode);
+   return gradient_t<float>(net, seg, cols, (const float*)vals, (const float*)probes, P, st, loss, mode);
 }
 
 tnlb_status lfsai_adam(tnlb_lfsai* net, double lr, cudaStream_t st)
@@ -615,9 +761,9 @@ tnlb_status lfsai_eval(const tnlb_lfsai* net, const tnlb_segments* seg, tnlb_rea
 {
    LfsaiMatrix M;
    if (real == TNLB_F64)
-      TNLB_TRY_STATUS(build_matrix_ctx<double>(seg, real, cols, (const double*)vals, st, &M));
+      TNLB_TRY_STATUS(build_matrix_ctx<double>(seg, real, cols, (const double*)vals, net->level, st, &M));
    else
-      TNLB_TRY_STATUS(build_matrix_ctx<float>(seg, real, cols, (const float*)vals, st, &M));
+      TNLB_TRY_STATUS(build_matrix_ctx<float>(seg, real, cols, (const float*)vals, net->level, st, &M));
    const int32_t n = seg->n;
    DeviceBuffer o, h1, h2, h3;
    lf::k_round_weights<<<(kLfParams + 255) / 256, 256, 0, st>>>(net->theta.as<float>(), net->wround.as<float>());

@@ -7,7 +7,7 @@
 // 16 bytes per core matrix; neighbouring core matrices 128 B apart along K,
 // 8-row groups K/8*128 B apart); one elected thread issues
 // tcgen05.mma.cta_group::1.kind::f16 (M=128, N=64 or 16, K=16 per
-// instruction) into an FP32 accumulator in tensor memory, commits to an
+// instruction; 2 instructions for the 32 features of layer 1) into an FP32 accumulator in tensor memory, commits to an
 // mbarrier, and every thread reads its row back with tcgen05.ld (32x32b: warp
 // w reads TMEM lanes 32w..32w+31), adds the bias, applies ReLU and writes the
 // next layer's BF16 input.  Waits on the mbarrier are bounded: on timeout the
@@ -15,6 +15,18 @@
 //
 // The same arithmetic as the CUDA-core kernels of lfsai.cu (BF16 products,
 // FP32 sums) up to the summation order inside the tensor core.
+//
+// Training runs on the tensor cores too:
+//  * k_backward_tc: per 128-row tile, the deltas d3 = (dL/do W4) .* (h3 > 0),
+//    d2 = (d3 W3) .* (h2 > 0), d1 = (d2 W2) .* (h1 > 0) as three MMAs with
+//    the transposed weights as B operands (K = 16, 64, 64), the deltas
+//    rounded to BF16 as the next MMA's A operand and kept in FP32 for the
+//    weight gradients;
+//  * k_wgrad_tc: dW = sum_r d_r^T bf16(x_r) with the rows as the K
+//    dimension: A = d^T (FOUT <= 64 of the 128 M rows used), B = x^T plus a
+//    row of ones, so the bias gradient sum_r d_r comes out of the same MMA
+//    as column FIN; each CTA accumulates its rows in TMEM and writes one
+//    partial, summed in a fixed order afterwards.
 #include <cuda_bf16.h>
 
 #include "internal.cuh"
@@ -105,11 +117,11 @@ __device__ __forceinline__ void store_bf16(uint8_t* base, uint32_t off, float v)
 }
 
 struct Smem {
-   alignas(1024) uint8_t a[kRows * kLfH * 2];  // layer input tile, 128 x 64 BF16 (layer 1 uses 128 x 16)
-   alignas(1024) uint8_t w1[kLfH * kLfF * 2];  // 64 x 16
+   alignas(1024) uint8_t a[kRows * kLfH * 2];  // layer input tile, 128 x 64 BF16 (layer 1 uses 128 x 32)
+   alignas(1024) uint8_t w1[kLfH * kLfF * 2];  // 64 x 32
    alignas(1024) uint8_t w2[kLfH * kLfH * 2];  // 64 x 64
    alignas(1024) uint8_t w3[kLfH * kLfH * 2];
-   alignas(1024) uint8_t w4[16 * kLfH * 2];    // 4 x 64 padded to 16 rows
+   alignas(1024) uint8_t w4[16 * kLfH * 2];    // 8 x 64 padded to 16 rows
    float b[3 * kLfH + 16];
    alignas(8) uint64_t bar;
    uint32_t taddr;
@@ -117,7 +129,7 @@ struct Smem {
 };
 
 // Forward pass of the network over n rows.  h1..h3 (n x 64, FP32 after ReLU)
-// are written when non-null; o (n x 4) always.
+// are written when non-null; o (n x 8) always.
 __global__ void __launch_bounds__(kRows) k_forward_tc(const float* __restrict__ feat, int64_t n,
                                                       const float* __restrict__ wr, float* __restrict__ h1,
                                                       float* __restrict__ h2, float* __restrict__ h3,
@@ -228,6 +240,228 @@ __global__ void __launch_bounds__(kRows) k_forward_tc(const float* __restrict__ 
    }
 }
 
+struct SmemBack {
+   alignas(1024) uint8_t a[kRows * kLfH * 2];  // delta tile, 128 x 64 BF16 (first MMA: 128 x 16)
+   alignas(1024) uint8_t w4t[kLfH * 16 * 2];   // W4^T, 64 x 16 (K = outputs, 8 used)
+   alignas(1024) uint8_t w3t[kLfH * kLfH * 2]; // W3^T, 64 x 64
+   alignas(1024) uint8_t w2t[kLfH * kLfH * 2]; // W2^T
+   alignas(8) uint64_t bar;
+   uint32_t taddr;
+   int32_t fail;
+};
+
+// Deltas of the three hidden layers for all rows (see the file comment).
+__global__ void __launch_bounds__(kRows) k_backward_tc(const float* __restrict__ dout, int64_t n,
+                                                       const float* __restrict__ wr, const float* __restrict__ h1,
+                                                       const float* __restrict__ h2, const float* __restrict__ h3,
+                                                       float* __restrict__ d1, float* __restrict__ d2,
+                                                       float* __restrict__ d3, int32_t* __restrict__ err)
+{
+   extern __shared__ uint8_t dyn[];
+   SmemBack& S = *reinterpret_cast<SmemBack*>((reinterpret_cast<uintptr_t>(dyn) + 1023) & ~uintptr_t(1023));
+   const int t = threadIdx.x, warp = t >> 5;
+   // B operands: element (n, k) = W[k][n], K-major core-matrix layout
+   for (int e = t; e < kLfH * 16; e += kRows) {
+      const int nn = e / 16, k = e % 16;
+      store_bf16(S.w4t, core_off(nn, k, 2), k < kLfK ? wr[kLfW4 + k * kLfH + nn] : 0.f);
+   }
+   for (int e = t; e < kLfH * kLfH; e += kRows) {
+      const int nn = e / kLfH, k = e % kLfH;
+      store_bf16(S.w3t, core_off(nn, k, kLfH / 8), wr[kLfW3 + k * kLfH + nn]);
+      store_bf16(S.w2t, core_off(nn, k, kLfH / 8), wr[kLfW2 + k * kLfH + nn]);
+   }
+   if (t == 0) {
+      S.fail = 0;
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&S.bar)), "r"(1));
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+   }
+   if (warp == 0) {
+      asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&S.taddr)),
+                   "r"(kTmemCols));
+      asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+   }
+   fence_before();
+   __syncthreads();
+   fence_after();
+   const uint32_t tmem = S.taddr;
+   const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+   const uint32_t a_addr = smem_u32(S.a);
+   uint32_t phase = 0;
+   bool ok = true;
+   for (int64_t tile = blockIdx.x; ok && tile * kRows < n; tile += gridDim.x) {
+      const int64_t row = tile * kRows + t;
+      const bool live = row < n;
+      // first A operand: dL/do (8 outputs) padded to K = 16
+#pragma unroll
+      for (int k = 0; k < 16; k++) store_bf16(S.a, core_off(t, k, 2), (live && k < kLfK) ? dout[row * kLfK + k] : 0.f);
+      for (int layer = 3; layer >= 1 && ok; layer--) {
+         const int K = layer == 3 ? 16 : kLfH;
+         const uint8_t* W = layer == 3 ? S.w4t : layer == 2 ? S.w3t : S.w2t;
+         fence_async_smem();
+         fence_before();
+         __syncthreads();
+         if (t == 0) {
+            fence_after();
+            const uint32_t idesc = instr_desc(kRows, kLfH);
+            const uint32_t sbo = (uint32_t)(K / 8) * 128u;
+            for (int kk = 0; kk < K / 16; kk++) {
+               const uint64_t ad = smem_desc(a_addr + kk * 256u, 128u, sbo);
+               const uint64_t bd = smem_desc(smem_u32(W) + kk * 256u, 128u, sbo);
+               mma_bf16(tmem, ad, bd, idesc, kk > 0 ? 1u : 0u);
+            }
+            commit(&S.bar);
+         }
+         const int mine = wait_bar(&S.bar, phase) ? 1 : 0;
+         if (!__syncthreads_and(mine)) {
+            ok = false;
+            if (t == 0) S.fail = 1;
+            break;
+         }
+         phase ^= 1u;
+         fence_after();
+         const float* hin = layer == 3 ? h3 : layer == 2 ? h2 : h1;
+         float* dst = layer == 3 ? d3 : layer == 2 ? d2 : d1;
+         for (int c0 = 0; c0 < kLfH; c0 += 16) {
+            float v[16];
+            ld16(tmem + lane_base + (uint32_t)c0, v);
+            wait_ld();
+#pragma unroll
+            for (int q = 0; q < 16; q++) {
+               const float d = (live && hin[row * kLfH + c0 + q] > 0.f) ? v[q] : 0.f;
+               if (live) dst[row * kLfH + c0 + q] = d;
+               store_bf16(S.a, core_off(t, c0 + q, kLfH / 8), d);
+            }
+         }
+      }
+   }
+   fence_before();
+   __syncthreads();
+   if (S.fail && t == 0) atomicExch(err, 1);
+   if (warp == 0) {
+      fence_after();
+      asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
+   }
+}
+
+struct SmemWgrad {
+   alignas(1024) uint8_t a[kRows * kRows * 2];        // d^T: 128 (M, outputs) x 128 (K, rows)
+   alignas(1024) uint8_t b[(kLfH + 16) * kRows * 2];  // x^T and a row of ones: (FIN + 16) x 128
+   alignas(8) uint64_t bar;
+   uint32_t taddr;
+   int32_t fail;
+};
+
+// Weight and bias gradient of one layer, one partial per CTA:
+// partial[cta] = [dW (FOUT x FIN) | db (FOUT)] over rows
+// [cta * rows_per_cta, (cta + 1) * rows_per_cta) (a multiple of 128).
+template <int FIN, int FOUT>
+__global__ void __launch_bounds__(kRows) k_wgrad_tc(const float* __restrict__ d, const float* __restrict__ x,
+                                                    int64_t n, int64_t rows_per_cta, float* __restrict__ partial,
+                                                    int32_t* __restrict__ err)
+{
+   constexpr int N = FIN + 16;  // x^T rows, then the ones row and padding
+   static_assert(N % 16 == 0 && N <= 256 && FOUT <= kRows, "MMA shape");
+   extern __shared__ uint8_t dyn[];
+   SmemWgrad& S = *reinterpret_cast<SmemWgrad*>((reinterpret_cast<uintptr_t>(dyn) + 1023) & ~uintptr_t(1023));
+   const int t = threadIdx.x, warp = t >> 5;
+   // the M rows FOUT..127 of A and the padding rows of B stay zero; the
+   // ones row of B is set once
+   for (int e = t; e < kRows * kRows; e += kRows) {
+      const int m = e / kRows, k = e % kRows;
+      if (m >= FOUT) store_bf16(S.a, core_off(m, k, kRows / 8), 0.f);
+   }
+   for (int e = t; e < 16 * kRows; e += kRows) {
+      const int nn = FIN + e / kRows, k = e % kRows;
+      store_bf16(S.b, core_off(nn, k, kRows / 8), nn == FIN ? 1.f : 0.f);
+   }
+   if (t == 0) {
+      S.fail = 0;
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&S.bar)), "r"(1));
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+   }
+   if (warp == 0) {
+      asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&S.taddr)),
+                   "r"(kTmemCols));
+      asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+   }
+   fence_before();
+   __syncthreads();
+   fence_after();
+   const uint32_t tmem = S.taddr;
+   const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+   uint32_t phase = 0;
+   bool ok = true;
+   const int64_t r0 = (int64_t)blockIdx.x * rows_per_cta;
+   const int64_t r1 = imin64(n, r0 + rows_per_cta);
+   bool first = true;
+   for (int64_t rb = r0; ok && rb < r1; rb += kRows) {
+      // thread t stages row rb + t: its deltas into column t of A, its
+      // inputs into column t of B (zero beyond the last row)
+      const int64_t row = rb + t;
+      const bool live = row < r1;
+#pragma unroll 4
+      for (int m = 0; m < FOUT; m++) store_bf16(S.a, core_off(m, t, kRows / 8), live ? d[row * FOUT + m] : 0.f);
+#pragma unroll 4
+      for (int c = 0; c < FIN; c++) store_bf16(S.b, core_off(c, t, kRows / 8), live ? x[row * FIN + c] : 0.f);
+      if (!live) store_bf16(S.b, core_off(FIN, t, kRows / 8), 0.f);
+      else store_bf16(S.b, core_off(FIN, t, kRows / 8), 1.f);
+      fence_async_smem();
+      fence_before();
+      __syncthreads();
+      if (t == 0) {
+         fence_after();
+         const uint32_t idesc = instr_desc(kRows, N);
+         const uint32_t sbo = (uint32_t)(kRows / 8) * 128u;
+         for (int kk = 0; kk < kRows / 16; kk++) {
+            const uint64_t ad = smem_desc(smem_u32(S.a) + kk * 256u, 128u, sbo);
+            const uint64_t bd = smem_desc(smem_u32(S.b) + kk * 256u, 128u, sbo);
+            mma_bf16(tmem, ad, bd, idesc, (first && kk == 0) ? 0u : 1u);
+         }
+         commit(&S.bar);
+      }
+      first = false;
+      const int mine = wait_bar(&S.bar, phase) ? 1 : 0;
+      if (!__syncthreads_and(mine)) {
+         ok = false;
+         if (t == 0) S.fail = 1;
+         break;
+      }
+      phase ^= 1u;
+      fence_after();
+   }
+   if (ok) {
+      // TMEM lane m holds dW row m (columns 0..FIN-1) and db[m] (column FIN)
+      constexpr int NW = FOUT * FIN + FOUT;
+      float* out = partial + (int64_t)blockIdx.x * NW;
+      if (r0 >= r1) {
+         for (int e = t; e < NW; e += kRows) out[e] = 0.f;
+      }
+      else if (warp * 32 < FOUT) {
+         for (int c0 = 0; c0 < N; c0 += 16) {
+            float v[16];
+            ld16(tmem + lane_base + (uint32_t)c0, v);
+            wait_ld();
+            if (t < FOUT)
+#pragma unroll
+               for (int q = 0; q < 16; q++) {
+                  const int c = c0 + q;
+                  if (c < FIN)
+                     out[t * FIN + c] = v[q];
+                  else if (c == FIN)
+                     out[FOUT * FIN + t] = v[q];
+               }
+         }
+      }
+   }
+   fence_before();
+   __syncthreads();
+   if (S.fail && t == 0) atomicExch(err, 1);
+   if (warp == 0) {
+      fence_after();
+      asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
+   }
+}
+
 }  // namespace tc
 
 size_t lfsai_tc_smem_bytes() { return sizeof(tc::Smem) + 1024; }
@@ -252,6 +486,82 @@ tnlb_status lfsai_forward_tc(const tnlb_lfsai* net, const float* feat, int64_t n
    TNLB_CUDA_TRY(cudaMemcpyAsync(&h, err.ptr, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
    TNLB_CUDA_TRY(cudaStreamSynchronize(st));
    TNLB_REQUIRE(h == 0, TNLB_ERR_TIMEOUT, "tensor-core network pass: an mbarrier wait timed out");
+   return TNLB_OK;
+}
+
+
+namespace {
+
+__global__ void k_sum_partials_tc(const float* __restrict__ partial, int blocks, int nw, float* __restrict__ gW,
+                                  float* __restrict__ gb, int nwW)
+{
+   const int e = blockIdx.x * blockDim.x + threadIdx.x;
+   if (e >= nw) return;
+   double s = 0;
+   for (int b = 0; b < blocks; b++) s += partial[(int64_t)b * nw + e];
+   if (e < nwW)
+      gW[e] = (float)s;
+   else
+      gb[e - nwW] = (float)s;
+}
+
+template <int FIN, int FOUT>
+tnlb_status wgrad_tc(const float* d, const float* x, int64_t n, float* gW, float* gb, int32_t* err, cudaStream_t st)
+{
+   static bool attr_set = false;
+   const size_t smem = sizeof(tc::SmemWgrad) + 1024;
+   if (!attr_set) {
+      TNLB_CUDA_TRY(cudaFuncSetAttribute(tc::k_wgrad_tc<FIN, FOUT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem));
+      attr_set = true;
+   }
+   const int64_t chunks = (n + tc::kRows - 1) / tc::kRows;
+   const int64_t ctas = imin64(chunks, 148 * 4);
+   const int64_t rows_per_cta = ((chunks + ctas - 1) / ctas) * tc::kRows;
+   const int blocks = (int)((n + rows_per_cta - 1) / rows_per_cta);
+   constexpr int NW = FOUT * FIN + FOUT;
+   DeviceBuffer part;
+   TNLB_TRY_STATUS(part.alloc(sizeof(float) * (size_t)blocks * NW));
+   tc::k_wgrad_tc<FIN, FOUT><<<blocks, tc::kRows, smem, st>>>(d, x, n, rows_per_cta, part.as<float>(), err);
+   TNLB_CHECK_LAUNCH();
+   k_sum_partials_tc<<<(NW + 255) / 256, 256, 0, st>>>(part.as<float>(), blocks, NW, gW, gb, FOUT * FIN);
+   TNLB_CHECK_LAUNCH();
+   // the partial buffer is freed on return: wait for its readers
+   TNLB_CUDA_TRY(cudaStreamSynchronize(st));
+   return TNLB_OK;
+}
+
+}  // namespace
+
+tnlb_status lfsai_backward_tc(tnlb_lfsai* net, const float* feat, int64_t n, const float* h1, const float* h2,
+                              const float* h3, const float* dout, cudaStream_t st)
+{
+   static bool attr_set = false;
+   const size_t smem = sizeof(tc::SmemBack) + 1024;
+   if (!attr_set) {
+      TNLB_CUDA_TRY(cudaFuncSetAttribute(tc::k_backward_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      attr_set = true;
+   }
+   DeviceBuffer d3, d2, d1, err;
+   TNLB_TRY_STATUS(d3.alloc(sizeof(float) * n * kLfH));
+   TNLB_TRY_STATUS(d2.alloc(sizeof(float) * n * kLfH));
+   TNLB_TRY_STATUS(d1.alloc(sizeof(float) * n * kLfH));
+   TNLB_TRY_STATUS(err.alloc(sizeof(int32_t)));
+   TNLB_CUDA_TRY(cudaMemsetAsync(err.ptr, 0, sizeof(int32_t), st));
+   const int64_t tiles = (n + tc::kRows - 1) / tc::kRows;
+   const unsigned grid = (unsigned)imin64(tiles, 148 * 4);
+   tc::k_backward_tc<<<grid, tc::kRows, smem, st>>>(dout, n, net->wround.as<float>(), h1, h2, h3, d1.as<float>(),
+                                                    d2.as<float>(), d3.as<float>(), err.as<int32_t>());
+   TNLB_CHECK_LAUNCH();
+   float* gr = net->grad.as<float>();
+   TNLB_TRY_STATUS(wgrad_tc<kLfH, kLfK>(dout, h3, n, gr + kLfW4, gr + kLfB4, err.as<int32_t>(), st));
+   TNLB_TRY_STATUS(wgrad_tc<kLfH, kLfH>(d3.as<float>(), h2, n, gr + kLfW3, gr + kLfB3, err.as<int32_t>(), st));
+   TNLB_TRY_STATUS(wgrad_tc<kLfH, kLfH>(d2.as<float>(), h1, n, gr + kLfW2, gr + kLfB2, err.as<int32_t>(), st));
+   TNLB_TRY_STATUS(wgrad_tc<kLfF, kLfH>(d1.as<float>(), feat, n, gr + kLfW1, gr + kLfB1, err.as<int32_t>(), st));
+   int32_t h = 0;
+   TNLB_CUDA_TRY(cudaMemcpyAsync(&h, err.ptr, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+   TNLB_CUDA_TRY(cudaStreamSynchronize(st));
+   TNLB_REQUIRE(h == 0, TNLB_ERR_TIMEOUT, "tensor-core network backward pass: an mbarrier wait timed out");
    return TNLB_OK;
 }
 

@@ -6,7 +6,12 @@ features, forward and backward passes, the probe loss built from the
 library's SpMVs, and Adam.  This module only orchestrates them:
 
 * ``LearnedFSAI.fit_classical`` -- warm start: regress the network onto the
-  classical Kolotilina-Yeremin FSAI values of the training matrices;
+  classical Kolotilina-Yeremin FSAI values of the training matrices (on the
+  lower triangle of A; zero on the fill entries of the default, wider
+  pattern -- the lower triangle of the pattern of A^2);
+* ``LearnedFSAI.train_kaporin`` -- minimise the Kaporin loss
+  log(trace(G A G^T)/n) - (2/n) sum_i log G_ii (exact, no probes), the
+  log of Kaporin's condition number, which bounds CG's iteration count;
 * ``LearnedFSAI.train`` -- minimise (1/(n P)) sum_p ||z_p - G A G^T z_p||^2
   over probe vectors z_p: Rademacher vectors and residuals left by a few
   Jacobi-PCG iterations on the same matrix (the error modes a cheap
@@ -53,13 +58,20 @@ class LearnedPreconditioner:
 
 
 class LearnedFSAI:
-    NPARAMS = 9668
+    """The network handle.  ``level`` picks G's pattern: 1 (default) the
+    lower triangle of the pattern of A^2, 0 the lower triangle of A (at most
+    8 entries per row either way).  The dense layers run on tcgen05 tensor
+    cores unless ``tensor_cores=False`` (CUDA cores)."""
 
-    def __init__(self, seed: int = 0, tensor_cores: bool = False):
+    NPARAMS = 10952
+    FEATURES, OUTPUTS = 32, 8
+
+    def __init__(self, seed: int = 0, tensor_cores: bool = True, level: int = 1):
         h = C.c_void_p()
         check(capi.tnlb_lfsai_create(seed, _stream(), C.byref(h)))
         self._h = h
         self.set_tensor_cores(tensor_cores)
+        self.set_level(level)
 
     def __del__(self):
         try:
@@ -70,6 +82,10 @@ class LearnedFSAI:
 
     def set_tensor_cores(self, enable: bool) -> None:
         check(capi.tnlb_lfsai_set_tensor_cores(self._h, int(bool(enable))))
+
+    def set_level(self, level: int) -> None:
+        check(capi.tnlb_lfsai_set_level(self._h, int(level)))
+        self.level = int(level)
 
     # -- parameters ---------------------------------------------------------
     def params(self) -> np.ndarray:
@@ -94,10 +110,10 @@ class LearnedFSAI:
 
     # -- evaluation -------------------------------------------------------------
     def evaluate(self, M: SparseMatrix):
-        """(features n x 16, outputs n x 4) of a matrix."""
+        """(features n x 32, outputs n x 8) of a matrix."""
         n = M.getRows()
-        f = np.zeros((n, 16), np.float32)
-        o = np.zeros((n, 4), np.float32)
+        f = np.zeros((n, self.FEATURES), np.float32)
+        o = np.zeros((n, self.OUTPUTS), np.float32)
         check(capi.tnlb_lfsai_eval(self._h, M.segments.handle, _real_code(M.real), M.columnIndexes.data_ptr(),
                                    M.values.data_ptr(), _stream(), f.ctypes.data, o.ctypes.data))
         return f, o
@@ -110,7 +126,8 @@ class LearnedFSAI:
 
     # -- training ---------------------------------------------------------------
     def gradient(self, M: SparseMatrix, probes: torch.Tensor | None = None, mode: int = 0) -> float:
-        """Loss of one matrix; the gradient stays in the handle (see grad())."""
+        """Loss of one matrix; the gradient stays in the handle (see grad()).
+        mode 0: probe loss (probes required), 1: warm start, 2: Kaporin."""
         loss = C.c_double()
         nprobes = 0 if probes is None else probes.shape[0]
         check(capi.tnlb_lfsai_gradient(self._h, mode, M.segments.handle, _real_code(M.real),
@@ -127,6 +144,15 @@ class LearnedFSAI:
         for k in range(steps):
             M = matrices[k % len(matrices)]
             hist.append(self.gradient(M, None, mode=1))
+            self.adam_step(lr)
+        return hist
+
+    def train_kaporin(self, matrices, steps: int = 300, lr: float = 1e-3) -> list[float]:
+        """Adam on the Kaporin loss, cycling over the training matrices."""
+        hist = []
+        for k in range(steps):
+            M = matrices[k % len(matrices)]
+            hist.append(self.gradient(M, None, mode=2))
             self.adam_step(lr)
         return hist
 
@@ -182,33 +208,76 @@ def diffusion_problem(N: int, seed: int, corr_range=(0.02, 0.2), sigma_range=(1.
 
 def main(argv=None):
     """Train the learned FSAI on seeded 2D diffusion problems and save the
-    weights (float32, 9668 values):
+    weights (float32, 10952 values, level-1 pattern):
 
         python -m tnl_b200.lfsai --out tnl_b200/weights/lfsai_diffusion.npy
+
+    The default training set is the learned-preconditioner workload: 512
+    problems on 256 x 256 grids, k = exp(g) with g a Gaussian random field of
+    correlation length ~ U[0.02, 0.2] and sigma ~ U[1, 3] (seeds 0..511).
+    Phases: warm start on classical FSAI of A's own pattern, the Kaporin
+    loss on the level-1 pattern, then (``--probe-steps``) the probe loss on
+    Rademacher vectors and residuals left by the solver.  A held-out problem
+    (seed 100000) is solved by FP64 PCG after each phase; its iteration
+    counts go to the JSON summary printed at the end.
     """
     import argparse
     import json
     import sys
     import time
 
+    from . import FSAI
+    from .generators import uniform_vector
+
     ap = argparse.ArgumentParser(prog="python -m tnl_b200.lfsai")
     ap.add_argument("--out", required=True)
-    ap.add_argument("--N", type=int, default=128, help="grid side of the training problems")
-    ap.add_argument("--problems", type=int, default=8)
-    ap.add_argument("--fit-steps", type=int, default=400)
-    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--N", type=int, default=256, help="grid side of the training problems")
+    ap.add_argument("--problems", type=int, default=512)
+    ap.add_argument("--fit-steps", type=int, default=1024)
+    ap.add_argument("--kaporin-steps", type=int, default=2048)
+    ap.add_argument("--probe-steps", type=int, default=0)
     ap.add_argument("--seed", type=int, default=2)
+    ap.add_argument("--validate-N", type=int, default=512)
     args = ap.parse_args(argv)
     t0 = time.perf_counter()
     train = [diffusion_problem(args.N, s) for s in range(args.problems)]
+    t_gen = time.perf_counter() - t0
+    val = diffusion_problem(args.validate_N, 100000)
+    b = torch.tensor(uniform_vector(val.getRows(), 1), device="cuda")
+
+    def iterations(P):
+        S = CG()
+        S.setMatrix(val)
+        S.setPreconditioner(P)
+        S.setConvergenceResidue(1e-8)
+        S.setMaxIterations(100000)
+        x = torch.zeros(val.getRows(), dtype=torch.float64, device="cuda")
+        S.solve(b, x)
+        return S.getIterations()
+
+    record = {"problems": args.problems, "N": args.N, "generation_s": t_gen}
+    for level in (0, 1):
+        P = FSAI(level)
+        P.update(val)
+        record[f"validation_classical_fsai_level{level}"] = iterations(P)
     net = LearnedFSAI(seed=args.seed)
+    t1 = time.perf_counter()
     fit = net.fit_classical(train, steps=args.fit_steps, lr=3e-3)
-    hist = net.train(train, steps=args.steps, nprobes=8, lr=5e-4)
+    record["fit_loss"] = [fit[0], float(np.mean(fit[-16:]))]
+    record["validation_warm_start"] = iterations(net.preconditioner(val))
+    kap = net.train_kaporin(train, steps=args.kaporin_steps, lr=1e-3)
+    record["kaporin_loss"] = [float(np.mean(kap[:16])), float(np.mean(kap[-16:]))]
+    record["validation_after_kaporin"] = iterations(net.preconditioner(val))
+    if args.probe_steps:
+        hist = net.train(train, steps=args.probe_steps, nprobes=8, lr=2e-4)
+        record["probe_loss"] = [float(np.mean(hist[:16])), float(np.mean(hist[-16:]))]
+        record["validation_after_probe"] = iterations(net.preconditioner(val))
+    torch.cuda.synchronize()
+    record["training_s"] = time.perf_counter() - t1
     Path(args.out).parent.mkdir(parents=True, exist_ok=True)
     net.save(args.out)
-    print(json.dumps({"fit_loss": [fit[0], fit[-1]], "probe_loss": [float(np.mean(hist[:len(train)])),
-                                                                    float(np.mean(hist[-len(train):]))],
-                      "seconds": time.perf_counter() - t0, "out": str(args.out)}), file=sys.stdout)
+    record["out"] = str(args.out)
+    print(json.dumps(record), file=sys.stdout)
     return 0
 
 
