@@ -4,8 +4,9 @@
 // code changes only its includes and namespace:
 //   TNL::Matrices::SparseMatrix< Real, Devices::Cuda, int, GeneralMatrix, Segments >
 //        setDimensions, setRowCapacities, setFromCSR (the cross-format
-//        operator= from a CSR matrix), vectorProduct, transposedVectorProduct,
-//        getTransposition,
+//        operator= from a CSR matrix), forElements / forAllElements (device
+//        lambdas, CSR storage; CUDA translation units only), vectorProduct,
+//        transposedVectorProduct, getTransposition,
 //        getRows, getColumns; MatrixType GeneralMatrix or SymmetricMatrix
 //        (Matrices/SparseMatrix.h:41-57, SparseMatrixBase.h:1020-1035);
 //   TNL::Algorithms::Segments::{CSR, Ellpack, SlicedEllpack, ChunkedEllpack,
@@ -218,6 +219,22 @@ struct GeneralMatrix {};
 // MatrixType SymmetricMatrix (Matrices/MatrixType.h:48): one triangle stored.
 struct SymmetricMatrix {};
 
+#ifdef __CUDACC__
+namespace detail {
+// One thread per row of CSR storage: f(rowIdx, localIdx, columnIdx&, value&)
+// on each of the row's slots (SparseMatrixBase::forElements).
+template <typename Index, typename Real, typename F>
+__global__ void for_elements_csr(const Index* __restrict__ offsets, Index begin, Index end, Index* cols, Real* vals,
+                                 F f)
+{
+   const Index row = begin + (Index)(blockIdx.x * blockDim.x + threadIdx.x);
+   if (row >= end) return;
+   const Index b = offsets[row], e = offsets[row + 1];
+   for (Index k = b; k < e; k++) f(row, k - b, cols[k], vals[k]);
+}
+}  // namespace detail
+#endif
+
 template <typename Real = double, typename Device = Devices::Cuda, typename Index = int,
           typename MatrixType = GeneralMatrix,
           template <typename, typename, typename> class Segments = Algorithms::Segments::CSR,
@@ -394,6 +411,33 @@ public:
       values_.setSize((Index)info.storage);
       columns_idx_.setSize((Index)info.storage);
    }
+#ifdef __CUDACC__
+   // SparseMatrixBase::forElements (Matrices/SparseMatrixBase.h:858):
+   // f(rowIdx, localIdx, columnIdx&, value&) on every slot of rows [begin,
+   // end), run on the GPU by one thread per row; f is a __device__ callable
+   // (an extended __host__ __device__ lambda).  The matrix must use CSR or
+   // AdaptiveCSR segments, whose rows are contiguous in storage (other
+   // formats: assemble a CSR matrix and assign it).  Synchronous.
+   template <typename F>
+   void forElements(Index begin, Index end, F f)
+   {
+      if (begin < 0 || end > rows_ || begin > end) throw std::invalid_argument("forElements: bad row range");
+      const int32_t* offsets = nullptr;
+      tnlb::check(tnlb_segments_offsets_view(seg_, &offsets));
+      if (end == begin) return;
+      const unsigned blocks = (unsigned)((end - begin + 255) / 256);
+      detail::for_elements_csr<Index, Real, F><<<blocks, 256>>>(offsets, begin, end, columns_idx_.getData(),
+                                                                  values_.getData(), f);
+      tnlb::cuda_check(cudaGetLastError());
+      tnlb::cuda_check(cudaStreamSynchronize(nullptr));
+   }
+   // SparseMatrixBase::forAllElements (SparseMatrixBase.h:904).
+   template <typename F>
+   void forAllElements(F f)
+   {
+      forElements(0, rows_, f);
+   }
+#endif
    Index getRows() const { return rows_; }
    Index getColumns() const { return columns_; }
    static constexpr bool isSymmetric() { return std::is_same<MatrixType, SymmetricMatrix>::value; }
@@ -411,6 +455,10 @@ public:
    const tnlb_segments* segments() const { return seg_; }
    const Containers::Vector<Real>& getValues() const { return values_; }
    const Containers::Vector<Index>& getColumnIndexes() const { return columns_idx_; }
+   // SparseMatrixBase::getValues / getColumnIndexes (SparseMatrixBase.h):
+   // writable views of the storage, e.g. for a device-side assembler.
+   Containers::Vector<Real>& getValues() { return values_; }
+   Containers::Vector<Index>& getColumnIndexes() { return columns_idx_; }
 
 private:
    Index rows_ = 0, columns_ = 0;

@@ -266,6 +266,26 @@ tnlb_status tnlb_spmv_csr_noalloc(tnlb_real real, int32_t rows, int32_t columns,
                                   const int32_t* d_rowptr, const int32_t* d_cols, const void* d_values,
                                   const void* d_x, void* d_y, double alpha, double beta, tnlb_stream stream);
 
+/* ------------------------------------------------- device assembly */
+
+/* The 2D Laplace operator of an N x N grid (identity rows on the boundary,
+ * 1, 1, -4, 1, 1 inside) assembled on the GPU straight into the storage of
+ * a matrix of any format -- SparseMatrixBase::forAllRows / forElements
+ * (Matrices/SparseMatrixBase.h:589, 858) with the lambda of the reference's
+ * sparse set-up benchmark (Documentation/UsersGuide/Matrices/
+ * SparseMatrixSetup_Benchmark.cpp:157-198).  `seg` has N^2 segments whose
+ * capacities hold the stencil (5 per row suffices); unused slots keep the
+ * padding column -1.  Blocks until assembled. */
+tnlb_status tnlb_matrix_assemble_laplace_2d(const tnlb_segments* seg, tnlb_real real, int32_t grid_size,
+                                            int32_t* d_cols, void* d_values, tnlb_stream stream);
+
+/* The device row offsets of CSR or AdaptiveCSR segments (n+1 entries, valid
+ * while the segments live): row i owns storage slots [offsets[i],
+ * offsets[i+1]).  The forElements template of include/tnlb/tnlb.hpp runs a
+ * caller's device lambda on them (CSR::getGlobalIndex, CSRBase.hpp).  Other
+ * formats give TNLB_ERR_INVALID_ARGUMENT. */
+tnlb_status tnlb_segments_offsets_view(const tnlb_segments* seg, const int32_t** d_offsets);
+
 /* ------------------------------------------------------------ files */
 
 /* A CSR matrix in HOST memory, as read from a file. */

@@ -32,7 +32,7 @@ __all__ = [
     "CSR", "Ellpack", "SlicedEllpack", "ChunkedEllpack", "BiEllpack", "AdaptiveCSR", "SparseMatrix",
     "LaunchConfiguration", "ColumnMajorOrder", "RowMajorOrder", "CSRMatrix", "check", "BackendRuntimeError",
     "CG", "BICGStab", "GMRES", "FGMRES", "TFQMR", "BICGStabL", "IDRs", "Diagonal", "ILU0", "FSAI", "FSAI2",
-    "solve_mixed", "solve_mixed_reliable", "true_residual", "ILUT", "read_mtx", "write_mtx",
+    "solve_mixed", "solve_mixed_reliable", "true_residual", "ILUT", "read_mtx", "write_mtx", "assemble_laplace_2d",
 ]
 
 ColumnMajorOrder = capi.COLUMN_MAJOR
@@ -472,6 +472,24 @@ def _host_csr_to_numpy(h: "capi.HostCSR") -> CSRMatrix:
     cols = np.ctypeslib.as_array(h.cols, shape=(max(nnz, 1),))[:nnz].copy()
     vals = np.ctypeslib.as_array(h.values, shape=(max(nnz, 1),))[:nnz].copy()
     return CSRMatrix(rp, cols, vals, h.columns)
+
+
+def assemble_laplace_2d(grid_size: int, segments=None, real=torch.float64, organization: int | None = None,
+                        capacity: int = 5) -> "SparseMatrix":
+    """The 2D Laplace operator of a grid_size x grid_size grid assembled on
+    the GPU (identity rows on the boundary, 1, 1, -4, 1, 1 inside), as the
+    reference's sparse set-up benchmark builds it with forElements
+    (SparseMatrixSetup_Benchmark.cpp): row capacities `capacity` (5 in the
+    benchmark), then one thread per row writes its stencil into the
+    storage of the chosen format."""
+    seg = CSR if segments is None else segments
+    n = grid_size * grid_size
+    M = SparseMatrix(seg, real, organization)
+    M.setDimensions(n, n)
+    M.setRowCapacities(torch.full((n,), capacity, dtype=torch.int32, device="cuda"))
+    check(capi.tnlb_matrix_assemble_laplace_2d(M.segments.handle, _real_code(real), grid_size,
+                                               M.columnIndexes.data_ptr(), M.values.data_ptr(), _stream()))
+    return M
 
 
 def read_mtx(path, symmetric: bool = False) -> CSRMatrix:

@@ -119,6 +119,8 @@ tnlb_spmv_csr_noalloc = _sig("tnlb_spmv_csr_noalloc",
                              [C.c_int, _i32, _i32, C.c_int64, _p, _p, _p, _p, _p, _f64, _f64, _p])
 tnlb_dot = _sig("tnlb_dot", [C.c_int, _i64, _p, _p, _p, _p])
 tnlb_axpby = _sig("tnlb_axpby", [C.c_int, _i64, _f64, _p, _f64, _p, _p])
+tnlb_matrix_assemble_laplace_2d = _sig("tnlb_matrix_assemble_laplace_2d", [_p, C.c_int, _i32, _p, _p, _p])
+tnlb_segments_offsets_view = _sig("tnlb_segments_offsets_view", [_p, C.POINTER(_p)])
 tnlb_solver_params_default = _sig("tnlb_solver_params_default", [C.POINTER(SolverParams)], None)
 tnlb_solve = _sig("tnlb_solve", [C.c_int, C.c_int, C.POINTER(SolverParams), _p, C.c_int, _p, _p, _p, _p, _p,
                                  C.POINTER(SolveResult)])

@@ -454,6 +454,31 @@ def profile_solvers(problem: str, N: int, iterations: int, out=sys.stdout):
     print(json.dumps({"method": "FP64 FSAI-PCG", "iterations": S.getIterations()}), file=out)
 
 
+def bench_assembly(max_grid: int = 8192, reps: int = 10, out=sys.stdout):
+    """Device-side assembly of the 2D Laplace operator (the reference's
+    sparse set-up benchmark, Documentation/UsersGuide/Matrices/
+    SparseMatrixSetup_Benchmark.cpp: FP32, CSR, row capacities 5, then the
+    stencil written on the GPU), for grid sides 16, 32, ..., max_grid: mean
+    time of `reps` set-ups (setRowCapacities, storage allocation and the
+    assembly kernel), CUDA events around each, after one warm-up."""
+    import tnl_b200 as t
+
+    N = 16
+    while N <= max_grid:
+        t.assemble_laplace_2d(N, real=torch.float32)
+        torch.cuda.synchronize()
+        times = []
+        for _ in range(reps):
+            M, ms = _timed(lambda: t.assemble_laplace_2d(N, real=torch.float32))
+            times.append(ms)
+            del M
+        print(json.dumps({"bench": "assembly_laplace_2d", "grid": N, "rows": N * N, "real": "f32", "format": "CSR",
+                          "seconds_mean": float(np.mean(times)) / 1e3, "seconds_min": float(np.min(times)) / 1e3}),
+              file=out, flush=True)
+        torch.cuda.empty_cache()
+        N *= 2
+
+
 def bench_learned_eval(count: int, N: int, weights: str, ilu_count: int = 4, first_seed: int = 10000,
                        out=sys.stdout):
     """The learned preconditioner's evaluation: `count` unseen 2D diffusion
@@ -584,6 +609,8 @@ def main(argv=None):
     b.add_argument("--problem", default="laplacian", choices=["laplacian", "diffusion"])
     b.add_argument("--N", type=int, default=1024)
     b.add_argument("--weights", default=str(Path(__file__).resolve().parent / "weights" / "lfsai_diffusion.npy"))
+    asm = sub.add_parser("assembly")
+    asm.add_argument("--max-grid", type=int, default=8192)
     le = sub.add_parser("learned-eval")
     le.add_argument("--count", type=int, default=64)
     le.add_argument("--N", type=int, default=2048)
@@ -594,6 +621,9 @@ def main(argv=None):
     pr.add_argument("--N", type=int, default=2048)
     pr.add_argument("--iterations", type=int, default=40)
     args = ap.parse_args(argv)
+    if args.cmd == "assembly":
+        bench_assembly(args.max_grid)
+        return 0
     if args.cmd == "learned-eval":
         bench_learned_eval(args.count, args.N, args.weights, args.ilu_count)
         return 0
