@@ -430,9 +430,11 @@ def bench_configs(which: str, out=sys.stdout):
            s_f2, x, outer_iterations=r["outer_iterations"])
 
 
-def profile_solvers(problem: str, N: int, iterations: int, out=sys.stdout):
+def profile_solvers(problem: str, N: int, iterations: int, fsai_level: int = 0, out=sys.stdout):
     """A fixed number of iterations of the FP32 reliable-update FSAI-PCG and
-    of FP64 FSAI-PCG, for a kernel launch list (ncu) of both iterations."""
+    of FP64 FSAI-PCG, for a kernel launch list (ncu) of both iterations;
+    ``fsai_level`` 1 runs the reliable-update PCG with the classical FSAI of
+    the level-1 pattern (the pattern of the learned preconditioner)."""
     import tnl_b200 as t
     from . import generators as g
     from .lfsai import diffusion_problem
@@ -441,8 +443,15 @@ def profile_solvers(problem: str, N: int, iterations: int, out=sys.stdout):
     n = M.getRows()
     b = torch.tensor(g.uniform_vector(n, 1), device="cuda")
     x = torch.zeros(n, dtype=torch.float64, device="cuda")
-    r = t.solve_mixed_reliable(M, b, x, tol=1e-8, inner="fsai", max_iterations=iterations)
-    print(json.dumps({"method": "FP32 reliable-update PCG, FSAI", "iterations": r["iterations"]}), file=out)
+    inner = "fsai"
+    if fsai_level:
+        h = M.toHostCSR()
+        A32 = t.SparseMatrix(t.CSR, torch.float32).assign(h.rowptr, h.cols, h.vals.astype(np.float32))
+        inner = t.FSAI(fsai_level)
+        inner.update(A32)
+    r = t.solve_mixed_reliable(M, b, x, tol=1e-8, inner=inner, max_iterations=iterations)
+    print(json.dumps({"method": f"FP32 reliable-update PCG, FSAI level {fsai_level}", "iterations": r["iterations"]}),
+          file=out)
     P = t.FSAI()
     P.update(M)
     S = t.CG()
@@ -620,6 +629,7 @@ def main(argv=None):
     pr.add_argument("--problem", default="diffusion", choices=["laplacian", "diffusion"])
     pr.add_argument("--N", type=int, default=2048)
     pr.add_argument("--iterations", type=int, default=40)
+    pr.add_argument("--fsai-level", type=int, default=0, choices=[0, 1])
     args = ap.parse_args(argv)
     if args.cmd == "assembly":
         bench_assembly(args.max_grid)
@@ -628,7 +638,7 @@ def main(argv=None):
         bench_learned_eval(args.count, args.N, args.weights, args.ilu_count)
         return 0
     if args.cmd == "profile-solvers":
-        profile_solvers(args.problem, args.N, args.iterations)
+        profile_solvers(args.problem, args.N, args.iterations, args.fsai_level)
         return 0
     if args.cmd == "configs":
         bench_configs(args.which)
