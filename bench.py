@@ -352,6 +352,37 @@ def run_reference(args):
     return 0
 
 
+def gather_ceiling_ms(M, xs, stream, reps):
+    """Mean device ms of the stream-and-gather measurement kernel on the
+    matrix's own arrays (CUDA events on the launching stream)."""
+    import ctypes as C
+
+    import torch
+
+    from tnl_b200 import _capi
+
+    rp = C.c_void_p()
+    _capi.check(_capi.tnlb_segments_offsets_view(M.segments.handle, C.byref(rp)))
+    y = torch.empty(M.getRows(), dtype=torch.float64, device="cuda")
+    nnz = M.getValues().numel()
+
+    def run():
+        _capi.check(_capi.tnlb_bench_stream_gather(_capi.F64, 1, M.getRows(), nnz, rp, M.getColumnIndexes().data_ptr(),
+                                                   M.getValues().data_ptr(), xs.data_ptr(), y.data_ptr(),
+                                                   stream.cuda_stream))
+
+    for _ in range(3):
+        run()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        run()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
 def config_dict(A):
     return {"workload": "power-law CSR SpMV (Zipf 1.73, cap 4096, seed 2), FP64, int32 indices",
             "rows": A.n, "nnz": A.nnz, "mean_row_length": round(A.nnz / A.n, 3),
@@ -469,6 +500,10 @@ def run_ours(args):
     # the last y read back agrees with the device-timed product
     assert torch.equal(hy[(e2e_steps - 1) % 2], ys.cpu()), "end-to-end product differs"
 
+    # the attainable rate on this matrix: the same streamed bytes and random
+    # gathers without the row sums (a measurement kernel of the library)
+    ceiling_ms = gather_ceiling_ms(M, xs, stream, max(20, min(args.steps, 200)))
+
     if world > 1:
         torch.distributed.destroy_process_group()
     if rank != 0:
@@ -488,6 +523,10 @@ def run_ours(args):
                      "algorithmic_bytes_per_spmv": nbytes},
         "e2e": {"value": e2e_value, "unit": "GB/s", "h2d_bytes_per_step": A.ncols * 8, "d2h_bytes_per_step": A.n * 8,
                 "steps": e2e_steps},
+        "gather_ceiling": {"ms": ceiling_ms, "GB/s": nbytes / (ceiling_ms / 1e3) / 1e9,
+                           "product_frac_of_ceiling": ceiling_ms / call_ms,
+                           "what": "the product's bytes streamed and its 67M random x gathers issued, no row sums "
+                                   "(tnlb_bench_stream_gather, CUDA events)"},
         "gpu_launches": int(launches_per_step or 0) * args.steps,
         "clocks": clk.summary(),
     }

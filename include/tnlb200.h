@@ -286,6 +286,19 @@ tnlb_status tnlb_matrix_assemble_laplace_2d(const tnlb_segments* seg, tnlb_real 
  * formats give TNLB_ERR_INVALID_ARGUMENT. */
 tnlb_status tnlb_segments_offsets_view(const tnlb_segments* seg, const int32_t** d_offsets);
 
+/* ------------------------------------------------------ measurement */
+
+/* The attainable rate of a CSR product's memory traffic (no counterpart in
+ * the reference; a measurement kernel): moves exactly the bytes of
+ * y = A x -- every column index and value streamed once, the row pointer
+ * read once, y written once -- and, with mode 1, gathers x at every column
+ * as the product does, but sums nothing by rows (y receives garbage).
+ * Mode 0 streams without the gathers.  The time of this kernel bounds the
+ * product on the same matrix from below.  Asynchronous. */
+tnlb_status tnlb_bench_stream_gather(tnlb_real real, int32_t mode, int32_t rows, int64_t nnz, const int32_t* d_rowptr,
+                                     const int32_t* d_cols, const void* d_values, const void* d_x, void* d_y,
+                                     tnlb_stream stream);
+
 /* ------------------------------------------------------------ files */
 
 /* A CSR matrix in HOST memory, as read from a file. */
@@ -596,6 +609,14 @@ tnlb_status tnlb_lfsai_set_tensor_cores(tnlb_lfsai* net, int32_t enable);
 /* The pattern of G the network fills: 0 (lower triangle of A) or 1 (lower
  * triangle of the pattern of A^2, the default). */
 tnlb_status tnlb_lfsai_set_level(tnlb_lfsai* net, int32_t level);
+/* The two-factor form for nonsymmetric A (enable = 1): the network fills
+ * G_L and H = G_U^T on the lower triangle of A (at most 4 entries a row),
+ * M^-1 = G_U G_L as tnlb_precond_create with TNLB_PRECOND_FSAI2 builds it
+ * classically; features and outputs as defined for it in
+ * oracle/lfsai_ref.py; the probe loss (1/(n P)) sum_p ||z_p - G_L A G_U
+ * z_p||^2 and the warm start (mode 1, towards the classical two-factor
+ * values) train it. */
+tnlb_status tnlb_lfsai_set_two_factor(tnlb_lfsai* net, int32_t enable);
 /* Loss and gradient on one matrix, kept in the handle.  mode 0: probe loss
  * (1/(n P)) sum_p ||z_p - G A G^T z_p||^2 with P probe vectors stored one
  * after another in d_probes (device, n*P values of `real`); mode 1: warm

@@ -329,3 +329,97 @@ def fsai2_classical(A):
         gl.extend(w * s)
         h.extend(u * s)
     return np.array(gl), np.array(h)
+
+
+# ------------------------------------------------------------------------
+# Two-factor learned FSAI for a nonsymmetric A (M^-1 = G_U G_L, G_L lower
+# and G_U upper on the level-0 pattern, H = G_U^T stored on the lower one).
+#
+# * Features f (32, zero padded) of row i, with B = S A S: f[0..11] =
+#   B(J_p, J_q), B(J_q, J_p) for the 6 pairs p < q of the last four slots
+#   (slots 4..7: (4,5) (4,6) (4,7) (5,6) (5,7) (6,7)); f[12..14] = B(i, j)
+#   for the first three stored columns j > i; f[15..17] = B(j, i) for the
+#   same j; f[31] = k/8.  At most 4 entries per row.
+# * Outputs: o[4..7] the row of G'_L, o[0..3] the row of H' (right-aligned
+#   slots 4 - k .. 3 and 8 - k .. 7); the diagonals exp(o_3), exp(o_7).
+#   G_L[i, j] = G'_L s_j, H[i, j] = H' s_j (G_L A G_U = G'_L B G'_U).
+# * Probe loss L = (1/(n P)) sum_p ||z_p - G_L A G_U z_p||^2 with
+#   dL/dG_L = -(2/(n P)) sum_p u w^T on the pattern, w = A G_U z,
+#   u = z - G_L w, and dL/dH_ij = -(2/(n P)) sum_p z_i q_j, q = A^T G_L^T u.
+# * Warm start: L = (1/n) sum_i (||G'_L,i - target_L||^2 + ||H'_i -
+#   target_H||^2) towards classical two-factor FSAI (fsai2_classical).
+
+PAIRS2 = [(4, 5), (4, 6), (4, 7), (5, 6), (5, 7), (6, 7)]
+
+
+def features2(A):
+    pat = pattern(A, 0)
+    rows = _row_dict(A)
+    d = np.array([rows[i].get(i, 0.0) for i in range(A.n)], np.float64)
+    s = 1.0 / np.sqrt(d)
+    f = np.zeros((A.n, F))
+    for i in range(A.n):
+        J = pat[i]
+        k = len(J)
+        if k > 4:
+            raise ValueError("two-factor learned FSAI: more than 4 entries in a row of the lower pattern")
+        slot_col = [None] * K
+        for t, j in enumerate(J):
+            slot_col[K - k + t] = j
+        for m, (p, q) in enumerate(PAIRS2):
+            jp, jq = slot_col[p], slot_col[q]
+            if jp is not None and jq is not None:
+                f[i, 2 * m] = rows[jp].get(jq, 0.0) * s[jp] * s[jq]
+                f[i, 2 * m + 1] = rows[jq].get(jp, 0.0) * s[jp] * s[jq]
+        upper = sorted(j for j in rows[i] if j > i)[:3]
+        for m, j in enumerate(upper):
+            f[i, 12 + m] = rows[i][j] * s[i] * s[j]
+            f[i, 15 + m] = rows[j].get(i, 0.0) * s[i] * s[j]
+        f[i, 31] = k / 8.0
+    return f, s, pat
+
+
+def g2_values(o, s, pat):
+    """(G_L values, H values) on the lower pattern, CSR order."""
+    gl, h = [], []
+    for i, J in enumerate(pat):
+        k = len(J)
+        for t, j in enumerate(J):
+            sl, sh = K - k + t, 4 - k + t
+            gl.append((np.exp(o[i, K - 1]) if sl == K - 1 else o[i, sl]) * s[j])
+            h.append((np.exp(o[i, 3]) if sh == 3 else o[i, sh]) * s[j])
+    return np.array(gl), np.array(h)
+
+
+def loss_and_grad2(theta, A, probes):
+    """Two-factor probe loss and its gradient (straight-through BF16)."""
+    import scipy.sparse as sp
+
+    f, s, pat = features2(A)
+    o, cache = forward(theta, f)
+    gl, h = g2_values(o, s, pat)
+    GL = g_matrix(gl, pat, A.n)
+    H = g_matrix(h, pat, A.n)
+    As = sp.csr_matrix((A.vals, A.cols, A.rowptr), shape=(A.n, A.n))
+    n, P = probes.shape
+    Z = probes
+    W = As @ (H.T @ Z)
+    U = Z - GL @ W
+    Q = As.T @ (GL.T @ U)
+    L = float(np.sum(U * U)) / (n * P)
+    coo = GL.tocoo()
+    gi, gj = coo.row, coo.col
+    order = np.lexsort((gj, gi))
+    c = -(2.0 / (n * P))
+    dGL = (c * np.sum(U[gi] * W[gj], axis=1))[order]
+    dH = (c * np.sum(Z[gi] * Q[gj], axis=1))[order]
+    do = np.zeros_like(o)
+    q = 0
+    for i, J in enumerate(pat):
+        k = len(J)
+        for t, j in enumerate(J):
+            sl, sh = K - k + t, 4 - k + t
+            do[i, sl] += dGL[q] * s[j] * (np.exp(o[i, K - 1]) if sl == K - 1 else 1.0)
+            do[i, sh] += dH[q] * s[j] * (np.exp(o[i, 3]) if sh == 3 else 1.0)
+            q += 1
+    return L, backward(theta, cache, do)

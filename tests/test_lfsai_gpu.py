@@ -266,3 +266,77 @@ def test_training_lowers_iterations_below_the_warm_start():
     assert np.mean(hist[-8:]) < np.mean(hist[:8])
     trained = _pcg_iterations(M, net.preconditioner(M), b)
     assert trained < 0.95 * warm, (trained, warm, classical)
+
+
+def _cd_problem(N, seed):
+    import tnl_b200
+    from tnl_b200 import generators as g
+
+    return tnl_b200.SparseMatrix.from_csr(g.convection_diffusion_3d(N, seed=seed))
+
+
+@pytest.mark.parametrize("tensor_cores", [True, False])
+def test_two_factor_features_and_gradient_match_reference(tensor_cores):
+    """The two-factor (nonsymmetric) form: features, and the probe-loss
+    gradient through G_L and G_U (transposed products of G_L and A inside)
+    against the FP64 reference."""
+    from oracle import lfsai_ref as R
+    from tnl_b200 import generators as g
+    from tnl_b200.lfsai import LearnedFSAI
+    import tnl_b200
+
+    A = g.convection_diffusion_3d(6, seed=3)
+    M = tnl_b200.SparseMatrix.from_csr(A)
+    net = LearnedFSAI(seed=7, two_factor=True, tensor_cores=tensor_cores)
+    f_gpu, _ = net.evaluate(M)
+    f_ref, _, _ = R.features2(A)
+    assert np.allclose(f_gpu, f_ref, rtol=1e-6, atol=1e-7)
+    theta = net.params().astype(np.float64)
+    Z = LearnedFSAI.probes(M, 4, seed=2, residual_share=0.0)
+    loss = net.gradient(M, Z)
+    g_gpu = net.grad().astype(np.float64)
+    L_ref, g_ref = R.loss_and_grad2(theta, A, Z.cpu().numpy().T.copy())
+    assert loss == pytest.approx(L_ref, rel=1e-4)
+    rel = np.linalg.norm(g_gpu - g_ref) / np.linalg.norm(g_ref)
+    assert rel < 2e-2, rel
+    with pytest.raises(ValueError):
+        net.gradient(M, None, mode=2)
+
+
+def test_two_factor_learned_fsai_with_fgmres():
+    """Warm start on the classical two-factor FSAI, then the probe loss on
+    Rademacher vectors and BiCGStab residuals: the loss falls, and FGMRES(30)
+    with the learned factors on an unseen convection-diffusion problem
+    converges in fewer iterations than with Jacobi."""
+    import tnl_b200
+    from tnl_b200 import generators as g
+    from tnl_b200.lfsai import LearnedFSAI
+
+    train = [_cd_problem(16, s) for s in range(4)]
+    net = LearnedFSAI(seed=3, two_factor=True)
+    fit = net.fit_classical(train, steps=300, lr=3e-3)
+    assert fit[-1] < 0.2 * fit[0]
+    probes = [LearnedFSAI.probes(M, 8, 50 + i, symmetric=False) for i, M in enumerate(train)]
+    before = np.mean([net.gradient(M, Z) for M, Z in zip(train, probes)])
+    net.train(train, steps=120, nprobes=8, lr=2e-4)
+    after = np.mean([net.gradient(M, Z) for M, Z in zip(train, probes)])
+    assert after < before
+    M = _cd_problem(24, 99)
+    b = torch.tensor(g.uniform_vector(M.getRows(), 1), device="cuda")
+    its = {}
+    for name in ("jacobi", "learned"):
+        S = tnl_b200.FGMRES()
+        S.setMatrix(M)
+        if name == "jacobi":
+            P = tnl_b200.Diagonal()
+            P.update(M)
+        else:
+            P = net.preconditioner(M)
+        S.setPreconditioner(P)
+        S.setup({"convergence-residue": 1e-8, "max-iterations": 20000, "gmres-restarting-min": 30,
+                 "gmres-restarting-max": 30})
+        x = torch.zeros(M.getRows(), dtype=torch.float64, device="cuda")
+        assert S.solve(b, x), name
+        its[name] = S.getIterations()
+        assert tnl_b200.true_residual(M, b, x) < 1e-7
+    assert its["learned"] < its["jacobi"], its

@@ -212,6 +212,31 @@ def test_lfsai_reference_fd(level):
         R.ROUND = old
 
 
+def test_lfsai_two_factor_reference_fd():
+    """The two-factor (nonsymmetric) probe-loss backpropagation of the
+    learned-FSAI reference against central finite differences (BF16
+    rounding off), on an upwind convection-diffusion operator."""
+    from oracle import lfsai_ref as R
+    from tnl_b200 import generators as g
+
+    A = g.convection_diffusion_3d(5)
+    theta = R.init_params(3)
+    rng = np.random.default_rng(0)
+    Z = rng.choice([-1.0, 1.0], size=(A.n, 3))
+    old = R.ROUND
+    R.ROUND = False
+    try:
+        _, grad = R.loss_and_grad2(theta, A, Z)
+        idx = np.nonzero(np.abs(grad) > 1e-4 * np.abs(grad).max())[0]
+        for i in rng.choice(idx, 10, replace=False):
+            e = np.zeros_like(theta)
+            e[i] = 1e-6
+            fd = (R.loss_and_grad2(theta + e, A, Z)[0] - R.loss_and_grad2(theta - e, A, Z)[0]) / 2e-6
+            assert fd == pytest.approx(grad[i], rel=1e-5, abs=1e-10)
+    finally:
+        R.ROUND = old
+
+
 def test_lfsai_reference_patterns_and_classical_fsai():
     """Level-1 pattern of a 5-point operator: the 7 lower entries of its
     13-point square; classical FSAI on it is the Kaporin minimiser, so it

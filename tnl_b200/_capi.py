@@ -119,6 +119,7 @@ tnlb_spmv_csr_noalloc = _sig("tnlb_spmv_csr_noalloc",
                              [C.c_int, _i32, _i32, C.c_int64, _p, _p, _p, _p, _p, _f64, _f64, _p])
 tnlb_dot = _sig("tnlb_dot", [C.c_int, _i64, _p, _p, _p, _p])
 tnlb_axpby = _sig("tnlb_axpby", [C.c_int, _i64, _f64, _p, _f64, _p, _p])
+tnlb_bench_stream_gather = _sig("tnlb_bench_stream_gather", [C.c_int, _i32, _i32, _i64, _p, _p, _p, _p, _p, _p])
 tnlb_matrix_assemble_laplace_2d = _sig("tnlb_matrix_assemble_laplace_2d", [_p, C.c_int, _i32, _p, _p, _p])
 tnlb_segments_offsets_view = _sig("tnlb_segments_offsets_view", [_p, C.POINTER(_p)])
 tnlb_solver_params_default = _sig("tnlb_solver_params_default", [C.POINTER(SolverParams)], None)
@@ -151,6 +152,7 @@ tnlb_lfsai_set_params = _sig("tnlb_lfsai_set_params", [_p, _p, _i64])
 tnlb_lfsai_get_grad = _sig("tnlb_lfsai_get_grad", [_p, _p, _i64])
 tnlb_lfsai_set_tensor_cores = _sig("tnlb_lfsai_set_tensor_cores", [_p, _i32])
 tnlb_lfsai_set_level = _sig("tnlb_lfsai_set_level", [_p, _i32])
+tnlb_lfsai_set_two_factor = _sig("tnlb_lfsai_set_two_factor", [_p, _i32])
 tnlb_lfsai_gradient = _sig("tnlb_lfsai_gradient", [_p, _i32, _p, C.c_int, _p, _p, _p, _i32, _p, C.POINTER(_f64)])
 tnlb_lfsai_adam_step = _sig("tnlb_lfsai_adam_step", [_p, _f64, _p])
 tnlb_lfsai_precond_create = _sig("tnlb_lfsai_precond_create", [_p, _p, C.c_int, _p, _p, _p, C.POINTER(_p)])

@@ -589,6 +589,14 @@ tnlb_status tnlb_lfsai_set_level(tnlb_lfsai* net, int32_t level)
    return TNLB_OK;
 }
 
+tnlb_status tnlb_lfsai_set_two_factor(tnlb_lfsai* net, int32_t enable)
+{
+   clear_error();
+   TNLB_REQUIRE(net != nullptr, TNLB_ERR_INVALID_ARGUMENT, "null network");
+   net->two_factor = enable ? 1 : 0;
+   return TNLB_OK;
+}
+
 tnlb_status tnlb_lfsai_gradient(tnlb_lfsai* net, int32_t mode, const tnlb_segments* seg, tnlb_real real,
                                 const int32_t* d_cols, const void* d_values, const void* d_probes, int32_t nprobes,
                                 tnlb_stream stream, double* h_loss)

@@ -457,6 +457,24 @@ tnlb_status fsai_set_values(Fsai* F, const void* gvals, cudaStream_t st)
    return TNLB_OK;
 }
 
+// New values of the two factors (device arrays over G's pattern): G_L's
+// values, and H = G_U^T's, from which G_U (stored as CSR) is gathered.
+tnlb_status fsai_set_values2(Fsai* F, const void* glvals, const void* hvals, cudaStream_t st)
+{
+   TNLB_REQUIRE(F->two_factor, TNLB_ERR_INVALID_ARGUMENT, "fsai_set_values2: not a two-factor FSAI");
+   const int64_t gnnz = F->g->elements;
+   const size_t rs = F->real == TNLB_F64 ? 8 : 4;
+   TNLB_CUDA_TRY(cudaMemcpyAsync(F->g_vals.ptr, glvals, rs * gnnz, cudaMemcpyDeviceToDevice, st));
+   if (F->real == TNLB_F64)
+      k_gather_vals<double><<<grid_for(gnnz, 1024), 256, 0, st>>>(F->gt_src.as<int32_t>(), gnnz,
+                                                                  (const double*)hvals, F->gt_vals.as<double>());
+   else
+      k_gather_vals<float><<<grid_for(gnnz, 1024), 256, 0, st>>>(F->gt_src.as<int32_t>(), gnnz,
+                                                                 (const float*)hvals, F->gt_vals.as<float>());
+   TNLB_CHECK_LAUNCH();
+   return TNLB_OK;
+}
+
 // z = G^T (G r)
 tnlb_status fsai_apply(const Fsai* F, const void* r, void* z, cudaStream_t st, const int32_t* skip)
 {

@@ -362,6 +362,7 @@ void ilu0_destroy(void* ilu);
 tnlb_status fsai_create(const tnlb_segments* seg, tnlb_real real, const int32_t* cols, const void* vals,
                         bool classical, cudaStream_t st, Fsai** out, bool two_factor = false, int level = 0);
 tnlb_status fsai_apply(const Fsai* F, const void* r, void* z, cudaStream_t st, const int32_t* skip = nullptr);
+tnlb_status fsai_set_values2(Fsai* F, const void* glvals, const void* hvals, cudaStream_t st);
 // z = G^T (G r) with (r, z) = |G r|^2 summed inside the G product (symmetric
 // FSAI whose G has rows of at most 16 entries: fsai_dot_fusable).
 bool fsai_dot_fusable(const Fsai* F);

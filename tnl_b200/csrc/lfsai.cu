@@ -450,6 +450,166 @@ __global__ void k_map_target(const int32_t* __restrict__ grp, const int32_t* __r
    }
 }
 
+// ---- two factors (nonsymmetric A): G_L and H = G_U^T on the lower pattern
+// of A (at most 4 entries a row).  Features: B(J_p, J_q) and B(J_q, J_p) of
+// the 6 pairs of slots 4..7, B(i, j) and B(j, i) of the first three stored
+// columns j > i, k/8.  Outputs: o[4..7] the row of G'_L, o[0..3] that of
+// H' (diagonals exp(o_7), exp(o_3)).
+template <typename Real>
+__global__ void k_features2(const int32_t* __restrict__ arp, const int32_t* __restrict__ acols,
+                            const Real* __restrict__ avals, const int32_t* __restrict__ grp,
+                            const int32_t* __restrict__ gcols, int32_t n, float* __restrict__ f,
+                            Real* __restrict__ s, int32_t* __restrict__ err)
+{
+   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+   if (i >= n) return;
+   const int32_t b = grp[i], k = grp[i + 1] - b;
+   for (int q = 0; q < kLfF; q++) f[i * kLfF + q] = 0.f;
+   if (k > 4 || k < 1) {
+      atomicExch(err, 1);
+      return;
+   }
+   int32_t slot_col[4];
+   double slot_s[4];
+   for (int t = 0; t < 4; t++) {
+      slot_col[t] = -1;
+      slot_s[t] = 0.0;
+   }
+   for (int t = 0; t < k; t++) {
+      const int32_t j = gcols[b + t];
+      slot_col[4 - k + t] = j;
+      slot_s[4 - k + t] = 1.0 / sqrt((double)lookup(arp, acols, avals, j, j));
+   }
+   int m = 0;
+   for (int p = 0; p < 4; p++)
+      for (int q = p + 1; q < 4; q++, m++) {
+         const int32_t jp = slot_col[p], jq = slot_col[q];
+         if (jp >= 0 && jq >= 0) {
+            const double sc = slot_s[p] * slot_s[q];
+            f[i * kLfF + 2 * m] = (float)((double)lookup(arp, acols, avals, jp, jq) * sc);
+            f[i * kLfF + 2 * m + 1] = (float)((double)lookup(arp, acols, avals, jq, jp) * sc);
+         }
+      }
+   const double si = slot_s[3];
+   int up = 0;
+   for (int32_t q = arp[i]; q < arp[i + 1] && up < 3; q++) {
+      const int32_t j = acols[q];
+      if (j > i) {
+         const double sj = 1.0 / sqrt((double)lookup(arp, acols, avals, j, j));
+         f[i * kLfF + 12 + up] = (float)((double)avals[q] * si * sj);
+         f[i * kLfF + 15 + up] = (float)((double)lookup(arp, acols, avals, j, (int32_t)i) * si * sj);
+         up++;
+      }
+   }
+   f[i * kLfF + kLfF - 1] = (float)k / (float)kLfK;
+   s[i] = (Real)si;
+}
+
+// G_L and H values on the pattern from the outputs.
+template <typename Real>
+__global__ void k_g2_values(const float* __restrict__ o, const Real* __restrict__ s, const int32_t* __restrict__ grp,
+                            const int32_t* __restrict__ gcols, int32_t n, Real* __restrict__ gl, Real* __restrict__ h)
+{
+   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+   if (i >= n) return;
+   const int32_t b = grp[i], k = grp[i + 1] - b;
+   for (int t = 0; t < k; t++) {
+      const int sl = kLfK - k + t, sh = 4 - k + t;
+      const double sj = (double)s[gcols[b + t]];
+      const double vl = sl == kLfK - 1 ? exp((double)o[i * kLfK + sl]) : (double)o[i * kLfK + sl];
+      const double vh = sh == 3 ? exp((double)o[i * kLfK + sh]) : (double)o[i * kLfK + sh];
+      gl[b + t] = (Real)(vl * sj);
+      h[b + t] = (Real)(vh * sj);
+   }
+}
+
+// dG_L_ij += c u_i w_j and dH_ij += c z_i q_j on the pattern (thread per row)
+template <typename Real>
+__global__ void k_dg2(const int32_t* __restrict__ grp, const int32_t* __restrict__ gcols, int32_t n,
+                      const Real* __restrict__ u, const Real* __restrict__ w, const Real* __restrict__ z,
+                      const Real* __restrict__ q, double c, double* __restrict__ dgl, double* __restrict__ dh)
+{
+   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+   if (i >= n) return;
+   const double ui = u[i], zi = z[i];
+   for (int32_t e = grp[i]; e < grp[i + 1]; e++) {
+      const int32_t j = gcols[e];
+      dgl[e] += c * ui * (double)w[j];
+      dh[e] += c * zi * (double)q[j];
+   }
+}
+
+// dL/do from dL/dG_L (slots 4..7) and dL/dH (slots 0..3)
+template <typename Real>
+__global__ void k_do2(const double* __restrict__ dgl, const double* __restrict__ dh, const float* __restrict__ o,
+                      const Real* __restrict__ s, const int32_t* __restrict__ grp, const int32_t* __restrict__ gcols,
+                      int32_t n, float* __restrict__ dout)
+{
+   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+   if (i >= n) return;
+   float d[kLfK];
+#pragma unroll
+   for (int t = 0; t < kLfK; t++) d[t] = 0.f;
+   const int32_t b = grp[i], k = grp[i + 1] - b;
+   for (int t = 0; t < k; t++) {
+      const int sl = kLfK - k + t, sh = 4 - k + t;
+      const double sj = (double)s[gcols[b + t]];
+      double vl = dgl[b + t] * sj, vh = dh[b + t] * sj;
+      if (sl == kLfK - 1) vl *= exp((double)o[i * kLfK + sl]);
+      if (sh == 3) vh *= exp((double)o[i * kLfK + sh]);
+      d[sl] = (float)vl;
+      d[sh] = (float)vh;
+   }
+#pragma unroll
+   for (int t = 0; t < kLfK; t++) dout[i * kLfK + t] = d[t];
+}
+
+// Warm start of the two factors: dL/do and L = 1/n sum over occupied slots
+// of (G'_L - target_L)^2 + (H' - target_H)^2 in the scaled frame.
+template <typename Real>
+__global__ void __launch_bounds__(kRedThreads) k_fit2_do(const float* __restrict__ o, const Real* __restrict__ tgl,
+                                                         const Real* __restrict__ th, const Real* __restrict__ s,
+                                                         const int32_t* __restrict__ grp,
+                                                         const int32_t* __restrict__ gcols, int32_t n,
+                                                         float* __restrict__ dout, RedWork w, double* __restrict__ loss)
+{
+   double acc = 0;
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+      float d[kLfK];
+#pragma unroll
+      for (int t = 0; t < kLfK; t++) d[t] = 0.f;
+      const int32_t b = grp[i], k = grp[i + 1] - b;
+      for (int t = 0; t < k; t++) {
+         const double sj = (double)s[gcols[b + t]];
+         for (int f2 = 0; f2 < 2; f2++) {
+            const int slot = f2 == 0 ? kLfK - k + t : 4 - k + t;
+            const bool diag = f2 == 0 ? slot == kLfK - 1 : slot == 3;
+            const double tp = (double)(f2 == 0 ? tgl[b + t] : th[b + t]) / sj;
+            const double op = o[i * kLfK + slot];
+            const double gp = diag ? exp(op) : op;
+            const double e = gp - tp;
+            acc += e * e;
+            d[slot] = (float)(2.0 * e * (diag ? gp : 1.0) / n);
+         }
+      }
+      for (int t = 0; t < kLfK; t++) dout[i * kLfK + t] = d[t];
+   }
+   double vv[1] = {acc};
+   if (publish_and_arrive<1>(vv, w)) {
+      double t[1];
+      gather_totals<1>(t, w);
+      if (threadIdx.x == 0) *loss = t[0] / n;
+   }
+}
+
+template <typename Real>
+__global__ void k_scatter_src(const int32_t* __restrict__ src, int64_t nnz, const Real* __restrict__ from,
+                              Real* __restrict__ to)
+{
+   for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < nnz; q += (int64_t)gridDim.x * blockDim.x)
+      to[src[q]] = from[q];
+}
+
 __global__ void k_init_params(uint64_t seed, float* __restrict__ theta)
 {
    const int q = blockIdx.x * blockDim.x + threadIdx.x;
@@ -489,24 +649,26 @@ namespace {
 
 template <typename Real>
 tnlb_status build_matrix_ctx(const tnlb_segments* seg, tnlb_real real, const int32_t* cols, const Real* vals,
-                             int level, cudaStream_t st, LfsaiMatrix* M)
+                             int level, bool two_factor, cudaStream_t st, LfsaiMatrix* M)
 {
-   TNLB_TRY_STATUS(fsai_create(seg, real, cols, vals, false, st, &M->F, false, level));
+   TNLB_TRY_STATUS(fsai_create(seg, real, cols, vals, false, st, &M->F, two_factor, two_factor ? 0 : level));
    const int32_t n = seg->n;
    TNLB_TRY_STATUS(M->feat.alloc(sizeof(float) * (size_t)n * kLfF));
    TNLB_TRY_STATUS(M->s.alloc(sizeof(Real) * n));
    DeviceBuffer err;
    TNLB_TRY_STATUS(err.alloc(sizeof(int32_t)));
    TNLB_CUDA_TRY(cudaMemsetAsync(err.ptr, 0, sizeof(int32_t), st));
-   lf::k_features<Real><<<grid_for(n, 128), 128, 0, st>>>(
-      M->F->a_rp.as<int32_t>(), M->F->a_cols.as<int32_t>(), M->F->a_vals.as<Real>(), M->F->g->offsets.as<int32_t>(),
-      M->F->g_cols.as<int32_t>(), n, M->feat.as<float>(), M->s.as<Real>(), err.as<int32_t>());
+   auto* kf = two_factor ? lf::k_features2<Real> : lf::k_features<Real>;
+   kf<<<grid_for(n, 128), 128, 0, st>>>(M->F->a_rp.as<int32_t>(), M->F->a_cols.as<int32_t>(), M->F->a_vals.as<Real>(),
+                                        M->F->g->offsets.as<int32_t>(), M->F->g_cols.as<int32_t>(), n,
+                                        M->feat.as<float>(), M->s.as<Real>(), err.as<int32_t>());
    TNLB_CHECK_LAUNCH();
    int32_t h = 0;
    TNLB_CUDA_TRY(cudaMemcpyAsync(&h, err.ptr, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
    TNLB_CUDA_TRY(cudaStreamSynchronize(st));
    TNLB_REQUIRE(h == 0, TNLB_ERR_INVALID_ARGUMENT,
-                "learned FSAI: a row of G's pattern holds more than 8 entries");
+                two_factor ? "learned two-factor FSAI: a row of A's lower triangle holds more than 4 entries"
+                           : "learned FSAI: a row of G's pattern holds more than 8 entries");
    return TNLB_OK;
 }
 
@@ -575,7 +737,7 @@ tnlb_status gradient_t(tnlb_lfsai* net, const tnlb_segments* seg, const int32_t*
    const tnlb_real real = sizeof(Real) == 8 ? TNLB_F64 : TNLB_F32;
    const bool fit = mode == 1;
    LfsaiMatrix M;
-   TNLB_TRY_STATUS(build_matrix_ctx<Real>(seg, real, cols, vals, net->level, st, &M));
+   TNLB_TRY_STATUS(build_matrix_ctx<Real>(seg, real, cols, vals, net->level, net->two_factor, st, &M));
    Fsai* F = M.F;
    const int64_t gnnz = F->g->elements;
    lf::k_round_weights<<<(kLfParams + 255) / 256, 256, 0, st>>>(net->theta.as<float>(), net->wround.as<float>());
@@ -596,7 +758,66 @@ tnlb_status gradient_t(tnlb_lfsai* net, const tnlb_segments* seg, const int32_t*
    TNLB_TRY_STATUS(lfsai_forward(net, M.feat.as<float>(), n, o.as<float>(), h1.as<float>(), h2.as<float>(),
                                  h3.as<float>(), st));
    double kap_n = 0.0;  // Kaporin loss: n, for the host-side value
-   if (fit) {
+   if (net->two_factor) {
+      TNLB_REQUIRE(mode != 2, TNLB_ERR_INVALID_ARGUMENT,
+                   "learned two-factor FSAI: the Kaporin loss is defined for the symmetric form only");
+      DeviceBuffer tgl, th;
+      TNLB_TRY_STATUS(tgl.alloc(sizeof(Real) * gnnz));
+      TNLB_TRY_STATUS(th.alloc(sizeof(Real) * gnnz));
+      if (fit) {
+         // classical two-factor FSAI: G_L's values, and H's from G_U
+         Fsai* C = nullptr;
+         TNLB_TRY_STATUS(fsai_create(seg, real, cols, vals, true, st, &C, true));
+         TNLB_CUDA_TRY(cudaMemcpyAsync(tgl.ptr, C->g_vals.ptr, sizeof(Real) * gnnz, cudaMemcpyDeviceToDevice, st));
+         lf::k_scatter_src<Real><<<grid_for(gnnz, 1024), 256, 0, st>>>(C->gt_src.as<int32_t>(), gnnz,
+                                                                       C->gt_vals.as<Real>(), th.as<Real>());
+         TNLB_CHECK_LAUNCH();
+         TNLB_CUDA_TRY(cudaStreamSynchronize(st));
+         fsai_destroy(C);
+         lf::k_fit2_do<Real><<<vec_grid(n), kRedThreads, 0, st>>>(o.as<float>(), tgl.as<Real>(), th.as<Real>(),
+                                                                  M.s.as<Real>(), F->g->offsets.as<int32_t>(),
+                                                                  F->g_cols.as<int32_t>(), n, dout.as<float>(), rw,
+                                                                  loss.as<double>());
+         TNLB_CHECK_LAUNCH();
+         TNLB_CUDA_TRY(cudaStreamSynchronize(st));  // the targets are freed on leaving
+      }
+      else {
+         lf::k_g2_values<Real><<<grid_for(n, 128), 128, 0, st>>>(o.as<float>(), M.s.as<Real>(),
+                                                                 F->g->offsets.as<int32_t>(), F->g_cols.as<int32_t>(),
+                                                                 n, tgl.as<Real>(), th.as<Real>());
+         TNLB_CHECK_LAUNCH();
+         TNLB_TRY_STATUS(fsai_set_values2(F, tgl.ptr, th.ptr, st));
+         DeviceBuffer t, w, v, u, q, dh;
+         for (auto* b : {&t, &w, &v, &u, &q}) TNLB_TRY_STATUS(b->alloc(sizeof(Real) * n));
+         TNLB_TRY_STATUS(dh.alloc(sizeof(double) * gnnz));
+         TNLB_CUDA_TRY(cudaMemsetAsync(dh.ptr, 0, sizeof(double) * gnnz, st));
+         const double c = -2.0 / ((double)n * P);
+         for (int32_t p = 0; p < P; p++) {
+            const Real* z = probes + (int64_t)p * n;
+            // w = A G_U z; v = G_L w; u = z - v; q = A^T G_L^T u
+            TNLB_TRY_STATUS(spmv_dispatch(F->gt, real, F->gt_cols.as<int32_t>(), F->gt_vals.ptr, z, t.ptr, 1.0, 0.0, st));
+            TNLB_TRY_STATUS(spmv_dispatch(seg, real, cols, vals, t.ptr, w.ptr, 1.0, 0.0, st));
+            TNLB_TRY_STATUS(spmv_dispatch(F->g, real, F->g_cols.as<int32_t>(), F->g_vals.ptr, w.ptr, v.ptr, 1.0, 0.0, st));
+            lf::k_resid<Real><<<vec_grid(n), kRedThreads, 0, st>>>(n, z, v.as<Real>(), u.as<Real>(), rw,
+                                                                   loss.as<double>());
+            TNLB_CHECK_LAUNCH();
+            TNLB_TRY_STATUS(tnlb_spmv_transposed(F->g, real, F->g_cols.as<int32_t>(), F->g_vals.ptr, n, u.ptr, t.ptr,
+                                                 1.0, 0.0, 0, 0, (tnlb_stream)st));
+            TNLB_TRY_STATUS(tnlb_spmv_transposed(seg, real, cols, vals, n, t.ptr, q.ptr, 1.0, 0.0, 0, 0,
+                                                 (tnlb_stream)st));
+            lf::k_dg2<Real><<<grid_for(n, 256), 256, 0, st>>>(F->g->offsets.as<int32_t>(), F->g_cols.as<int32_t>(), n,
+                                                              u.as<Real>(), w.as<Real>(), z, q.as<Real>(), c,
+                                                              dg.as<double>(), dh.as<double>());
+            TNLB_CHECK_LAUNCH();
+         }
+         lf::k_do2<Real><<<grid_for(n, 128), 128, 0, st>>>(dg.as<double>(), dh.as<double>(), o.as<float>(),
+                                                           M.s.as<Real>(), F->g->offsets.as<int32_t>(),
+                                                           F->g_cols.as<int32_t>(), n, dout.as<float>());
+         TNLB_CHECK_LAUNCH();
+         TNLB_CUDA_TRY(cudaStreamSynchronize(st));
+      }
+   }
+   else if (fit) {
       // supervised warm start on the classical FSAI values of the level-0
       // pattern (zero on fill entries)
       DeviceBuffer tg;
@@ -675,7 +896,7 @@ tnlb_status precond_t(const tnlb_lfsai* net, const tnlb_segments* seg, const int
 {
    const tnlb_real real = sizeof(Real) == 8 ? TNLB_F64 : TNLB_F32;
    auto* M = new LfsaiMatrix();
-   tnlb_status s = build_matrix_ctx<Real>(seg, real, cols, vals, net->level, st, M);
+   tnlb_status s = build_matrix_ctx<Real>(seg, real, cols, vals, net->level, net->two_factor, st, M);
    if (s != TNLB_OK) {
       delete M;
       return s;
@@ -689,11 +910,24 @@ tnlb_status precond_t(const tnlb_lfsai* net, const tnlb_segments* seg, const int
    TNLB_TRY_STATUS(h3.alloc(sizeof(float) * (size_t)n * kLfH));
    TNLB_TRY_STATUS(lfsai_forward(net, M->feat.as<float>(), n, o.as<float>(), h1.as<float>(), h2.as<float>(),
                                  h3.as<float>(), st));
-   lf::k_g_values<Real><<<grid_for(n, 128), 128, 0, st>>>(o.as<float>(), M->s.as<Real>(),
-                                                          M->F->g->offsets.as<int32_t>(), M->F->g_cols.as<int32_t>(), n,
-                                                          M->F->g_vals.as<Real>());
-   TNLB_CHECK_LAUNCH();
-   TNLB_TRY_STATUS(fsai_set_values(M->F, M->F->g_vals.ptr, st));
+   if (net->two_factor) {
+      DeviceBuffer h;
+      TNLB_TRY_STATUS(h.alloc(sizeof(Real) * M->F->g->elements));
+      lf::k_g2_values<Real><<<grid_for(n, 128), 128, 0, st>>>(o.as<float>(), M->s.as<Real>(),
+                                                              M->F->g->offsets.as<int32_t>(),
+                                                              M->F->g_cols.as<int32_t>(), n, M->F->g_vals.as<Real>(),
+                                                              h.as<Real>());
+      TNLB_CHECK_LAUNCH();
+      TNLB_TRY_STATUS(fsai_set_values2(M->F, M->F->g_vals.ptr, h.ptr, st));
+      TNLB_CUDA_TRY(cudaStreamSynchronize(st));
+   }
+   else {
+      lf::k_g_values<Real><<<grid_for(n, 128), 128, 0, st>>>(o.as<float>(), M->s.as<Real>(),
+                                                             M->F->g->offsets.as<int32_t>(),
+                                                             M->F->g_cols.as<int32_t>(), n, M->F->g_vals.as<Real>());
+      TNLB_CHECK_LAUNCH();
+      TNLB_TRY_STATUS(fsai_set_values(M->F, M->F->g_vals.ptr, st));
+   }
    TNLB_CUDA_TRY(cudaStreamSynchronize(st));
    auto* P = new tnlb_precond();
    P->kind = TNLB_PRECOND_FSAI;
@@ -761,9 +995,11 @@ tnlb_status lfsai_eval(const tnlb_lfsai* net, const tnlb_segments* seg, tnlb_rea
 {
    LfsaiMatrix M;
    if (real == TNLB_F64)
-      TNLB_TRY_STATUS(build_matrix_ctx<double>(seg, real, cols, (const double*)vals, net->level, st, &M));
+      TNLB_TRY_STATUS(
+         build_matrix_ctx<double>(seg, real, cols, (const double*)vals, net->level, net->two_factor, st, &M));
    else
-      TNLB_TRY_STATUS(build_matrix_ctx<float>(seg, real, cols, (const float*)vals, net->level, st, &M));
+      TNLB_TRY_STATUS(
+         build_matrix_ctx<float>(seg, real, cols, (const float*)vals, net->level, net->two_factor, st, &M));
    const int32_t n = seg->n;
    DeviceBuffer o, h1, h2, h3;
    lf::k_round_weights<<<(kLfParams + 255) / 256, 256, 0, st>>>(net->theta.as<float>(), net->wround.as<float>());

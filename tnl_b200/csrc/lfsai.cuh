@@ -32,6 +32,7 @@ struct tnlb_lfsai {
    int64_t step = 0;
    int use_tc = 1;             // dense layers on tcgen05 tensor cores (else CUDA cores)
    int level = 1;              // pattern of G: 0 lower triangle of A, 1 of A^2
+   int two_factor = 0;         // nonsymmetric A: G_L and H = G_U^T on the level-0 pattern
 };
 
 namespace tnlb {

@@ -28,7 +28,7 @@ from pathlib import Path
 import numpy as np
 import torch
 
-from . import CG, Diagonal, SparseMatrix, _real_code, _stream, check
+from . import BICGStab, CG, Diagonal, SparseMatrix, _real_code, _stream, check
 from . import _capi as capi
 from ._capi import lib  # noqa: F401  (fails loudly without the library)
 
@@ -60,18 +60,22 @@ class LearnedPreconditioner:
 class LearnedFSAI:
     """The network handle.  ``level`` picks G's pattern: 1 (default) the
     lower triangle of the pattern of A^2, 0 the lower triangle of A (at most
-    8 entries per row either way).  The dense layers run on tcgen05 tensor
-    cores unless ``tensor_cores=False`` (CUDA cores)."""
+    8 entries per row either way).  ``two_factor=True`` is the form for a
+    nonsymmetric A: G_L and G_U on A's own pattern, M^-1 = G_U G_L (used
+    by FGMRES).  The dense layers run on tcgen05 tensor cores unless
+    ``tensor_cores=False`` (CUDA cores)."""
 
     NPARAMS = 10952
     FEATURES, OUTPUTS = 32, 8
 
-    def __init__(self, seed: int = 0, tensor_cores: bool = True, level: int = 1):
+    def __init__(self, seed: int = 0, tensor_cores: bool = True, level: int = 1, two_factor: bool = False):
         h = C.c_void_p()
         check(capi.tnlb_lfsai_create(seed, _stream(), C.byref(h)))
         self._h = h
         self.set_tensor_cores(tensor_cores)
         self.set_level(level)
+        check(capi.tnlb_lfsai_set_two_factor(self._h, int(bool(two_factor))))
+        self.two_factor = bool(two_factor)
 
     def __del__(self):
         try:
@@ -157,16 +161,18 @@ class LearnedFSAI:
         return hist
 
     @staticmethod
-    def probes(M: SparseMatrix, count: int, seed: int, residual_share: float = 0.5, pcg_iterations: int = 20):
+    def probes(M: SparseMatrix, count: int, seed: int, residual_share: float = 0.5, pcg_iterations: int = 20,
+               symmetric: bool = True):
         """Probe vectors (count x n): Rademacher, and unit-RMS residuals left by a
-        few Jacobi-PCG iterations from x = 0 on Rademacher right-hand sides."""
+        few Jacobi-PCG iterations (Jacobi-BiCGStab for a nonsymmetric matrix)
+        from x = 0 on Rademacher right-hand sides."""
         n = M.getRows()
         g = torch.Generator(device="cuda")
         g.manual_seed(seed)
         Z = (torch.randint(0, 2, (count, n), generator=g, device="cuda", dtype=torch.int8).to(M.real) * 2 - 1)
         nres = int(round(count * residual_share))
         if nres:
-            S = CG()
+            S = CG() if symmetric else BICGStab()
             S.setMatrix(M)
             P = Diagonal()
             P.update(M)
@@ -192,7 +198,7 @@ class LearnedFSAI:
             idx = k % len(matrices)
             M = matrices[idx]
             if idx not in cache or (k // len(matrices)) % probe_cache == 0:
-                cache[idx] = self.probes(M, nprobes, seed + 7919 * k + idx)
+                cache[idx] = self.probes(M, nprobes, seed + 7919 * k + idx, symmetric=not self.two_factor)
             hist.append(self.gradient(M, cache[idx], mode=0))
             self.adam_step(lr)
         return hist
