@@ -465,7 +465,7 @@ typedef struct {
    int32_t iterations;    /* getIterations() */
    double residue;        /* getResidue(): the solver's stopping residue */
    int32_t status_detail; /* 0, or a tnlb_status for breakdowns/timeouts */
-   int32_t reserved;
+   int32_t fallback_iterations; /* tnlb_solve_mixed_reliable: FP64 iterations after a stall */
 } tnlb_solve_result;
 
 void tnlb_solver_params_default(tnlb_solver_params* p);
@@ -521,10 +521,20 @@ tnlb_status tnlb_solve_mixed(const tnlb_solver_params* params, const tnlb_segmen
  * kind `inner_precond` (NONE, JACOBI or FSAI) built from the FP32 values.
  * Stops when ||b - A x|| / ||b|| < params->convergence_residue (the TRUE
  * FP64 residual, computed as tnlb_true_residual computes it) or after
- * params->max_iterations FP32 iterations.  result->iterations counts FP32
- * iterations, result->residue is the true residual,
- * result->status_detail = 1 on a breakdown ((p, A p) zero or not finite),
- * and *reliable_updates counts the updates.  Synchronous. */
+ * params->max_iterations iterations.
+ *
+ * The FP32 iteration has stalled when the true residual at the updates has
+ * not halved within the last max(16384, iterations to the best residual so
+ * far) iterations, or on a breakdown ((p, A p) zero or not finite) or a
+ * non-finite residual (x then goes back to its last finite value); an
+ * update is forced after 4096 iterations without one, so that a recursion
+ * which stops falling is checked too.  After a stall the solve finishes
+ * with FP64 Jacobi PCG from x, for the iterations left.
+ * result->iterations counts all iterations (FP32 and FP64),
+ * result->fallback_iterations the FP64 ones, result->residue is the true
+ * residual, result->status_detail is 0, 2 when the FP64 fallback ran, or 1
+ * on a stall with no iterations left, and *reliable_updates counts the
+ * updates.  Synchronous. */
 tnlb_status tnlb_solve_mixed_reliable(const tnlb_solver_params* params, const tnlb_segments* seg,
                                       const int32_t* d_cols, const double* d_values, const double* d_b, double* d_x,
                                       double delta, tnlb_real vectors, tnlb_precond_kind inner_precond,

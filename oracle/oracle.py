@@ -350,7 +350,8 @@ class Oracle:
         ok = self.L.orc_pcg_reliable(A.n, rowptr.ctypes.data, cols.ctypes.data, vals.ctypes.data, precond,
                                      b.ctypes.data, x.ctypes.data, tol, delta, maxit, int(vec64), C.byref(it),
                                      C.byref(upd), C.byref(res))
-        return {"x": x, "converged": ok == 1, "iterations": it.value, "updates": upd.value, "residue": res.value}
+        return {"x": x, "converged": ok == 1, "stalled": ok == 2, "iterations": it.value, "updates": upd.value,
+                "residue": res.value}
 
     def pcg_reliable_fsai(self, A, b, G, GT, tol=1e-8, delta=0.1, maxit=100000, vec64=False):
         """pcg_reliable with the FSAI preconditioner z = G^T (G r): G and GT

@@ -1872,8 +1872,13 @@ done:
  * update; p is kept, beta = (r, z)_new / (r, z)_old.  precond: 0 none,
  * 1 Jacobi (diagonal of the FP32 values), 2 FSAI z = G^T (G r) from the
  * factor G and its transpose as the solver applies them (CSR, FP32 values;
- * rows summed in VT in entry order) with (r, z) = |G r|^2.  Returns 1 when
- * the true FP64 residual ||b - A x|| / ||b|| < tol. */
+ * rows summed in VT in entry order) with (r, z) = |G r|^2.  An update is
+ * also due 4096 iterations after the last one.  Returns 1 when the true
+ * FP64 residual ||b - A x|| / ||b|| < tol, 2 when the iteration stalled
+ * (the true residual at the updates not halved within the last
+ * max(16384, iterations to the last halving) iterations, a breakdown, or
+ * a non-finite residual; x is then the x of the lowest true residual, from
+ * which the library finishes in FP64), else 0. */
 typedef struct {
    const int32_t *grp, *gcols, *gtrp, *gtcols;
    const float *gvals, *gtvals;
@@ -1890,6 +1895,8 @@ typedef struct {
       VT *p = (VT*)calloc((size_t)n, sizeof(VT)), *Ap = (VT*)malloc(sizeof(VT) * (size_t)n);                      \
       VT* xc = (VT*)calloc((size_t)n, sizeof(VT));                                                                \
       VT* t = (VT*)malloc(sizeof(VT) * (size_t)(n > 0 ? n : 1));                                                  \
+      double* xbest = (double*)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));                                  \
+      double lowest = HUGE_VAL;                                                                                   \
       for (int32_t k = 0; k < nnz; k++) v32[k] = (float)vals[k];                                                  \
       for (int32_t i = 0; i < n; i++) {                                                                           \
          float di = 0.0f;                                                                                         \
@@ -1897,8 +1904,8 @@ typedef struct {
             if (cols[k] == i) di = v32[k];                                                                        \
          d[i] = di;                                                                                               \
       }                                                                                                           \
-      double rz = 1.0, rz_cur = 0.0, res = 0.0;                                                                   \
-      int32_t it = 0, upd = 0, halt = 1, ok = 0;                                                                  \
+      double rz = 1.0, rz_cur = 0.0, res = 0.0, best = HUGE_VAL;                                                  \
+      int32_t it = 0, upd = 0, halt = 1, ok = 0, force_at = 0, it_best = 0;                                       \
       for (;;) {                                                                                                  \
          for (int32_t i = 0; i < n; i++) {                                                                        \
             x[i] += (double)xc[i];                                                                                \
@@ -1920,8 +1927,29 @@ typedef struct {
             ok = 1;                                                                                               \
             break;                                                                                                \
          }                                                                                                        \
-         if (halt == 2 || it >= maxit || !isfinite(res)) break;                                                   \
+         if (!isfinite(res)) {                                                                                    \
+            ok = 2;                                                                                               \
+            break;                                                                                                \
+         }                                                                                                        \
+         if (res < lowest) {                                                                                      \
+            lowest = res;                                                                                         \
+            memcpy(xbest, x, sizeof(double) * (size_t)n);                                                         \
+         }                                                                                                        \
+         if (halt == 2) {                                                                                         \
+            ok = 2;                                                                                               \
+            break;                                                                                                \
+         }                                                                                                        \
+         if (it >= maxit) break;                                                                                  \
+         if (res < 0.5 * best) {                                                                                  \
+            best = res;                                                                                           \
+            it_best = it;                                                                                         \
+         }                                                                                                        \
+         else if (it - it_best > (it_best > 16384 ? it_best : 16384)) {                                           \
+            ok = 2;                                                                                               \
+            break;                                                                                                \
+         }                                                                                                        \
          if (it > 0) upd++;                                                                                       \
+         force_at = it + 4096;                                                                                    \
          const double t1 = delta * rn, t2 = tol * bn;                                                             \
          const double trig2 = t1 > t2 ? t1 * t1 : t2 * t2;                                                        \
          halt = 0;                                                                                                \
@@ -1966,7 +1994,7 @@ typedef struct {
             it++;                                                                                                 \
             if (!isfinite(rr))                                                                                    \
                halt = 2;                                                                                          \
-            else if (rr < trig2)                                                                                  \
+            else if (rr < trig2 || it >= force_at)                                                                \
                halt = 1;                                                                                          \
             else if (it >= maxit)                                                                                 \
                halt = 3;                                                                                          \
@@ -1976,9 +2004,14 @@ typedef struct {
             for (int32_t i = 0; i < n; i++) p[i] = z[i] + beta * p[i];                                            \
          }                                                                                                        \
       }                                                                                                           \
+      if (ok == 2 && lowest < HUGE_VAL && !(res <= lowest)) { /* back to the lowest true residual */            \
+         memcpy(x, xbest, sizeof(double) * (size_t)n);                                                            \
+         res = lowest;                                                                                            \
+      }                                                                                                           \
       *iterations = it;                                                                                           \
       *updates = upd;                                                                                             \
       *resid = res;                                                                                               \
+      free(xbest);                                                                                                \
       free(v32);                                                                                                  \
       free(d);                                                                                                    \
       free(r);                                                                                                    \

@@ -55,3 +55,25 @@ def assert_spmv_close(y, y_ref, scale, rtol):
     bad = np.nonzero(err > bound)[0]
     assert bad.size == 0, (f"{bad.size} rows outside tolerance; first {bad[:5]}: got {y[bad[:5]]}, "
                            f"expected {y_ref[bad[:5]]}, bound {bound[bad[:5]]}")
+
+
+def fp32_singular_laplacian(N, eps=1e-7):
+    """The graph Laplacian of an N x N grid (Neumann rows: diagonal = degree
+    2, 3 or 4) plus eps I: SPD in FP64, but eps vanishes when the values are
+    rounded to FP32, which leaves the singular Laplacian.  With a right-hand
+    side whose mean is not zero, CG on the FP32 values cannot reduce the
+    constant component of the residual."""
+    import scipy.sparse as sp
+    from tnl_b200 import generators as g
+
+    T = sp.diags([-np.ones(N - 1), np.r_[1.0, 2.0 * np.ones(N - 2), 1.0], -np.ones(N - 1)], [-1, 0, 1])
+    E = sp.identity(N)
+    A = (sp.kron(T, E) + sp.kron(E, T) + eps * sp.identity(N * N)).tocsr()
+    A.sort_indices()
+    return g.CSRMatrix(A.indptr.astype(np.int32), A.indices.astype(np.int32), A.data.astype(np.float64))
+
+
+def nonzero_mean_rhs(n, seed=1, mean=1e-3):
+    """Standard normal entries shifted to the given mean."""
+    b = np.random.default_rng(seed).standard_normal(n)
+    return b - b.mean() + mean

@@ -366,6 +366,29 @@ def test_reliable_update_pcg_restatement(oracle):
     assert v["iterations"] <= 1.3 * f["iterations"], (v["iterations"], f["iterations"])
 
 
+def test_reliable_update_pcg_restatement_stalls(oracle):
+    """On a matrix whose FP32 values are singular (a Neumann Laplacian plus
+    1e-7 I) the restatement's FP32 iteration cannot reach the tolerance: it
+    reports a stall within the window (16384 iterations past the last
+    halving of the true residual, updates forced every 4096 iterations)
+    and returns the x of its lowest true residual.  FP64 Jacobi CG, the
+    library's fallback, solves the same system."""
+    from helpers import fp32_singular_laplacian, nonzero_mean_rhs
+
+    A = fp32_singular_laplacian(32)
+    assert np.unique(A.vals.astype(np.float32)).tolist() == [-1.0, 2.0, 3.0, 4.0]
+    b = nonzero_mean_rhs(A.n)
+    for vec64 in (False, True):
+        r = oracle.pcg_reliable(A, b, precond=1, tol=1e-10, delta=0.3, maxit=200000, vec64=vec64)
+        assert r["stalled"] and not r["converged"]
+        assert 16384 < r["iterations"] < 2 * 16384 + 4096, r["iterations"]
+        assert r["updates"] >= 4  # forced ones among them
+        assert abs(oracle.true_residual(A, b, r["x"]) - r["residue"]) < 1e-12
+        assert r["residue"] < 1e-2
+    f = oracle.solve("cg", A, b, precond=1, tol=1e-10)
+    assert f["converged"] and oracle.true_residual(A, b, f["x"]) < 1e-9
+
+
 def test_reliable_update_pcg_restatement_fsai(oracle):
     """The FSAI form of the restatement (z = G^T G r, (r, z) = |G r|^2):
     with G = I it takes the unpreconditioned steps bit for bit; with the

@@ -827,7 +827,9 @@ def solve_mixed_reliable(M: SparseMatrix, b: torch.Tensor, x: torch.Tensor, tol:
     in FP64, each time the recursive residual has fallen below ``delta``
     times its value at the last update (0.3: the fewest iterations on the
     2048^2 diffusion matrix among 0.02 ... 0.7); the search direction is
-    kept across updates.
+    kept across updates.  When the FP32 iteration stalls (the true residual
+    no longer halves, or a breakdown) the solve finishes with FP64 Jacobi
+    PCG: ``fallback`` and ``fallback_iterations`` in the result.
 
     ``inner`` is "jacobi", "fsai", "none", or an FP32 Jacobi / FSAI
     preconditioner object built for an FP32 copy of the matrix (e.g. a
@@ -859,7 +861,8 @@ def solve_mixed_reliable(M: SparseMatrix, b: torch.Tensor, x: torch.Tensor, tol:
                                          M.values.data_ptr(), b.data_ptr(), x.data_ptr(), delta,
                                          _real_code(vectors), kind, handle, _stream(), C.byref(r), C.byref(upd)))
     return {"converged": bool(r.converged), "iterations": r.iterations, "reliable_updates": upd.value,
-            "true_residual": r.residue, "breakdown": bool(r.status_detail)}
+            "true_residual": r.residue, "fallback": r.status_detail == 2,
+            "fallback_iterations": r.fallback_iterations, "stalled": r.status_detail != 0}
 
 
 def solve_mixed(M: SparseMatrix, b: torch.Tensor, x: torch.Tensor, tol: float = 1e-8, inner_tol: float = 1e-4,

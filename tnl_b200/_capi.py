@@ -80,7 +80,7 @@ class MatrixFileInfo(C.Structure):
 
 class SolveResult(C.Structure):
     _fields_ = [("converged", C.c_int32), ("iterations", C.c_int32), ("residue", C.c_double),
-                ("status_detail", C.c_int32), ("reserved", C.c_int32)]
+                ("status_detail", C.c_int32), ("fallback_iterations", C.c_int32)]
 
 
 SOLVER_CG, SOLVER_BICGSTAB, SOLVER_GMRES, SOLVER_FGMRES, SOLVER_TFQMR, SOLVER_BICGSTABL, SOLVER_IDRS = range(7)

@@ -359,7 +359,8 @@ def bench_configs(which: str, out=sys.stdout):
           plain FP64 Jacobi-PCG, to FP64 relative residual 1e-10;
     c5 -- 192^3 upwind convection-diffusion (n = 7.1M): FGMRES(30) with the
           two-factor FSAI (FP64, and as the FP32 inner solver of FP64
-          refinement) vs plain FP64 GMRES(30) + ILU(0), to 1e-8."""
+          refinement) and with the learned two-factor FSAI vs plain FP64
+          GMRES(30) + ILU(0), to 1e-8."""
     import tnl_b200 as t
     from . import generators as g
 
@@ -380,7 +381,7 @@ def bench_configs(which: str, out=sys.stdout):
         print(json.dumps(rec), file=out, flush=True)
         return rec
 
-    def krylov(name, cls, P, keys):
+    def krylov(name, cls, P, keys, setup_ms=0.0, **extra):
         S = cls()
         S.setMatrix(M)
         S.setPreconditioner(P)
@@ -388,7 +389,7 @@ def bench_configs(which: str, out=sys.stdout):
                  "gmres-restarting-max": 30, **keys})
         x = torch.zeros(n, dtype=torch.float64, device="cuda")
         ok, ms = _timed(lambda: S.solve(b, x))
-        return report(name, ok, S.getIterations(), ms, 0.0, x)
+        return report(name, ok, S.getIterations(), ms, setup_ms, x, **extra)
 
     if which == "c3":
         # each method warmed up by a short solve, then the fastest of 3 (the
@@ -418,16 +419,28 @@ def bench_configs(which: str, out=sys.stdout):
         return
     P = t.ILU0()
     _, s_ilu = _timed(lambda: P.update(M))
-    rec = krylov("FP64 GMRES(30) + ILU(0)", t.GMRES, P, {"gmres-variant": "MGSR"})
-    rec["setup_ms"] = s_ilu
+    krylov("FP64 GMRES(30) + ILU(0)", t.GMRES, P, {"gmres-variant": "MGSR"}, s_ilu)
     P = t.FSAI2()
     _, s_f2 = _timed(lambda: P.update(M))
-    krylov("FP64 FGMRES(30) + two-factor FSAI", t.FGMRES, P, {"gmres-variant": "MGSR"})
+    krylov("FP64 FGMRES(30) + two-factor FSAI", t.FGMRES, P, {"gmres-variant": "MGSR"}, s_f2)
     x = torch.zeros(n, dtype=torch.float64, device="cuda")
     r, ms = _timed(lambda: t.solve_mixed(M, b, x, tol=tol, inner_tol=1e-4, inner="fsai2", solver="fgmres",
                                          max_outer=20))
     report("FP32-inner FGMRES(30) + two-factor FSAI in FP64 refinement", r["converged"], r["inner_iterations"], ms,
            s_f2, x, outer_iterations=r["outer_iterations"])
+    # the learned two-factor FSAI: trained on the spot on small problems of
+    # the same family (24^3, seeds 0..7: warm start, then the probe loss on
+    # Rademacher vectors and BiCGStab residuals), applied to this matrix
+    from .lfsai import LearnedFSAI
+
+    train = [t.SparseMatrix.from_csr(g.convection_diffusion_3d(24, seed=s_)) for s_ in range(8)]
+    net = LearnedFSAI(seed=1, two_factor=True)
+    _, train_ms = _timed(lambda: (net.fit_classical(train, steps=400, lr=3e-3),
+                                  net.train(train, steps=200, nprobes=8, lr=2e-4)))
+    net.preconditioner(M)
+    P, s_l = _timed(lambda: net.preconditioner(M))
+    krylov("FP64 FGMRES(30) + learned two-factor FSAI", t.FGMRES, P, {"gmres-variant": "MGSR"}, s_l,
+           training_ms=train_ms)
 
 
 def profile_solvers(problem: str, N: int, iterations: int, fsai_level: int = 0, out=sys.stdout):

@@ -2132,15 +2132,20 @@ tnlb_status solve_mixed_cg(const tnlb_segments* seg, const int32_t* cols, const 
 namespace {
 
 // State of the reliable-update PCG (solve_mixed_reliable).  `halt` stops the
-// rest of a CUDA-graph batch: 1 a reliable update is due, 2 breakdown
+// rest of a CUDA-graph batch: 1 a reliable update is due (the recursive
+// |r|^2 below trig2, or the iteration force_at reached), 2 breakdown
 // ((p, A p) zero or not finite), 3 the iteration limit.
 struct RuState {
    double rz;     // (r, z) of the iteration whose alpha was formed last
    double alpha;
    double trig2;  // |r|^2 of the recursion below which an update is due
    double rr;     // |r|^2 after the last update of r
-   int32_t it, halt, maxit, pad;
+   int32_t it, halt, maxit, force_at;
 };
+
+// Iterations after which an update is due whatever the recursive residual,
+// so that the true residual of a recursion that stops falling is checked.
+constexpr int32_t kRuForceEvery = 4096;
 
 // (a, b) into *out, for matrices the fused product does not cover.
 template <typename VT>
@@ -2256,7 +2261,7 @@ __global__ void __launch_bounds__(kRedThreads) k_ru_update(int64_t n, VT* __rest
          if (mode != 2) *rz_cur = mode == 0 ? tt[0] : tt[1];
          if (!ok || !isfinite(tt[0]))
             S->halt = 2;
-         else if (tt[0] < S->trig2)
+         else if (tt[0] < S->trig2 || S->it >= S->force_at)
             S->halt = 1;
          else if (S->it >= S->maxit)
             S->halt = 3;
@@ -2351,7 +2356,7 @@ __global__ void __launch_bounds__(kRedThreads, Rows::kMinBlocks)
          *rz_cur = tot[1];
          if (!ok || !isfinite(tot[0]))
             S->halt = 2;
-         else if (tot[0] < S->trig2)
+         else if (tot[0] < S->trig2 || S->it >= S->force_at)
             S->halt = 1;
          else if (S->it >= S->maxit)
             S->halt = 3;
@@ -2514,6 +2519,7 @@ __global__ void k_ru_set(RuState* S, double trig2)
 {
    if (threadIdx.x != 0) return;
    S->trig2 = trig2;
+   S->force_at = S->it + kRuForceEvery;
    S->halt = 0;
 }
 
@@ -2742,6 +2748,18 @@ tnlb_status reliable_t(const tnlb_segments* seg, const int32_t* cols, const doub
       return TNLB_OK;
    };
 
+   // The FP32 iteration has stalled when the true residual at the updates
+   // has not halved within the last max(kStallWindow, iterations to the
+   // last halving) iterations, or when it broke down or went non-finite;
+   // the solve then finishes with FP64 Jacobi PCG from the x of the lowest
+   // true residual so far (xbest).
+   constexpr int32_t kStallWindow = 16384;
+   DeviceBuffer xbest;
+   TNLB_TRY_STATUS(xbest.alloc(sizeof(double) * n));
+   double best = HUGE_VAL, lowest = HUGE_VAL;
+   int32_t it_best = 0;
+   bool stalled = false;
+
    *updates = 0;
    double resid = 0.0, bn = 0.0;
    RuState h{};
@@ -2767,7 +2785,27 @@ tnlb_status reliable_t(const tnlb_segments* seg, const int32_t* cols, const doub
          converged = true;
          break;
       }
-      if (h.halt == 2 || h.it >= prm.max_iterations || !std::isfinite(resid)) break;
+      if (!std::isfinite(resid)) {
+         stalled = true;
+         break;
+      }
+      if (resid < lowest) {
+         lowest = resid;
+         TNLB_CUDA_TRY(cudaMemcpyAsync(xbest.ptr, x, sizeof(double) * n, cudaMemcpyDeviceToDevice, cs));
+      }
+      if (h.halt == 2) {
+         stalled = true;
+         break;
+      }
+      if (h.it >= prm.max_iterations) break;
+      if (resid < 0.5 * best) {
+         best = resid;
+         it_best = h.it;
+      }
+      else if (h.it - it_best > std::max(kStallWindow, it_best)) {
+         stalled = true;
+         break;
+      }
       if (h.it > 0) (*updates)++;
       const double t1 = delta * rn, t2 = prm.convergence_residue * bn;
       k_ru_set<<<1, 32, 0, cs>>>(S, t1 > t2 ? t1 * t1 : t2 * t2);
@@ -2792,10 +2830,40 @@ tnlb_status reliable_t(const tnlb_segments* seg, const int32_t* cols, const doub
       }
    }
    TNLB_CUDA_TRY(cudaStreamSynchronize(cs));
-   res->iterations = h.it;
+   const int32_t fp32_its = h.it;
+   int32_t fb_its = 0;
+   const bool fall_back = stalled && fp32_its < prm.max_iterations;
+   const bool restore = stalled && lowest < HUGE_VAL && !(resid <= lowest);
+   if (restore) {
+      TNLB_CUDA_TRY(cudaMemcpyAsync(x, xbest.ptr, sizeof(double) * n, cudaMemcpyDeviceToDevice, cs));
+      resid = lowest;
+   }
+   if (fall_back) {
+      tnlb_precond* jac = nullptr;
+      TNLB_TRY_STATUS(precond_create(TNLB_PRECOND_JACOBI, seg, TNLB_F64, cols, vals, cs, &jac));
+      struct JGuard {
+         tnlb_precond* p;
+         ~JGuard() { delete p; }
+      } jguard{jac};
+      // the recursion's stopping residue a little below the tolerance, so
+      // that the true residual, checked below, falls under it too
+      tnlb_solver_params p64 = prm;
+      p64.max_iterations = prm.max_iterations - fp32_its;
+      p64.min_iterations = 0;
+      p64.convergence_residue = 0.5 * prm.convergence_residue;
+      const Ctx<double> c64{seg, TNLB_F64, cols, vals, n, cs};
+      tnlb_solve_result r64{};
+      TNLB_TRY_STATUS(cg_solve<double>(c64, view<double>(jac), p64, b, x, &r64));
+      fb_its = r64.iterations;
+      TNLB_TRY_STATUS(true_residual(seg, TNLB_F64, cols, vals, b, x, cs, &resid));
+      converged = bn == 0 || resid < prm.convergence_residue;
+   }
+   TNLB_CUDA_TRY(cudaStreamSynchronize(cs));
+   res->iterations = fp32_its + fb_its;
    res->residue = resid;
    res->converged = converged ? 1 : 0;
-   res->status_detail = h.halt == 2 ? 1 : 0;
+   res->status_detail = fall_back ? 2 : stalled ? 1 : 0;
+   res->fallback_iterations = fb_its;
    return TNLB_OK;
 }
 

@@ -188,7 +188,7 @@ def gaussian_random_field(shape, corr_length: float, sigma: float, seed: int) ->
     grids = np.meshgrid(*ks, indexing="ij")
     k2 = sum(g * g for g in grids)
     W *= np.exp(-k2 * corr_length * corr_length / 8.0)
-    g = np.fft.irfftn(W, s=shape)
+    g = np.fft.irfftn(W, s=shape, axes=tuple(range(len(shape))))
     g -= g.mean()
     std = g.std()
     if std > 0:
