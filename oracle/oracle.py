@@ -122,8 +122,8 @@ class Oracle:
             ("orc_idrs", [i32, p, p, p, C.c_int, C.c_int, C.c_int, p, p, p, C.POINTER(SolverState)], C.c_int),
             ("orc_idrs_shadow", [i32, i32, p], None),
             ("orc_true_residual", [i32, p, p, p, p, p], f64),
-            ("orc_pcg_reliable", [i32, p, p, p, C.c_int, p, p, f64, f64, i32, C.c_int, p, p, p], C.c_int),
-            ("orc_pcg_reliable_fsai", [i32, p, p, p, p, p, p, p, p, p, p, p, f64, f64, i32, C.c_int, p, p, p],
+            ("orc_pcg_reliable", [i32, p, p, p, C.c_int, p, p, f64, f64, i32, C.c_int, C.c_int, p, p, p], C.c_int),
+            ("orc_pcg_reliable_fsai", [i32, p, p, p, p, p, p, p, p, p, p, p, f64, f64, i32, C.c_int, C.c_int, p, p, p],
              C.c_int),
             ("orc_ilut_factor", [i32, p, p, p, i32, f64, p, p, p], C.c_long),
             ("orc_lu_apply", [i32, p, p, p, p, p], None),
@@ -340,23 +340,30 @@ class Oracle:
         return (np.cumsum(trp).astype(np.int32), rows[order].astype(np.int32),
                 (vals[order] * real(mult)).astype(real))
 
-    def pcg_reliable(self, A, b, precond: int = 1, tol=1e-8, delta=0.1, maxit=100000, x0=None, vec64=False):
+    def pcg_reliable(self, A, b, precond: int = 1, tol=1e-8, delta=0.1, maxit=100000, x0=None, vec64=False,
+                     excess=None):
         """The library's mixed-precision PCG with reliable updates (FP32
-        values, FP32 or FP64 vectors, FP64 updates); precond 0 none, 1 Jacobi."""
+        values, FP32 or FP64 vectors, FP64 updates); precond 0 none, 1 Jacobi.
+        ``excess`` (default: with FP32 vectors, as the library's compact
+        copies do) sums the FP32 product in the row-excess form."""
+        if excess is None:
+            excess = not vec64
         rowptr, cols, vals = _i32(A.rowptr), _i32(A.cols), np.ascontiguousarray(A.vals, np.float64)
         b = np.ascontiguousarray(b, np.float64)
         x = np.zeros(A.n) if x0 is None else np.array(x0, np.float64, copy=True)
         it, upd, res = C.c_int32(), C.c_int32(), C.c_double()
         ok = self.L.orc_pcg_reliable(A.n, rowptr.ctypes.data, cols.ctypes.data, vals.ctypes.data, precond,
-                                     b.ctypes.data, x.ctypes.data, tol, delta, maxit, int(vec64), C.byref(it),
-                                     C.byref(upd), C.byref(res))
+                                     b.ctypes.data, x.ctypes.data, tol, delta, maxit, int(vec64), int(excess),
+                                     C.byref(it), C.byref(upd), C.byref(res))
         return {"x": x, "converged": ok == 1, "stalled": ok == 2, "iterations": it.value, "updates": upd.value,
                 "residue": res.value}
 
-    def pcg_reliable_fsai(self, A, b, G, GT, tol=1e-8, delta=0.1, maxit=100000, vec64=False):
+    def pcg_reliable_fsai(self, A, b, G, GT, tol=1e-8, delta=0.1, maxit=100000, vec64=False, excess=None):
         """pcg_reliable with the FSAI preconditioner z = G^T (G r): G and GT
         are (rowptr, cols, FP32 values) of the factor and of its transpose
         in the entry order the solver applies them."""
+        if excess is None:
+            excess = not vec64
         rowptr, cols, vals = _i32(A.rowptr), _i32(A.cols), np.ascontiguousarray(A.vals, np.float64)
         grp, gc, gv = _i32(G[0]), _i32(G[1]), np.ascontiguousarray(G[2], np.float32)
         trp, tc, tv = _i32(GT[0]), _i32(GT[1]), np.ascontiguousarray(GT[2], np.float32)
@@ -366,7 +373,7 @@ class Oracle:
         ok = self.L.orc_pcg_reliable_fsai(A.n, rowptr.ctypes.data, cols.ctypes.data, vals.ctypes.data,
                                           grp.ctypes.data, gc.ctypes.data, gv.ctypes.data, trp.ctypes.data,
                                           tc.ctypes.data, tv.ctypes.data, b.ctypes.data, x.ctypes.data, tol, delta,
-                                          maxit, int(vec64), C.byref(it), C.byref(upd), C.byref(res))
+                                          maxit, int(vec64), int(excess), C.byref(it), C.byref(upd), C.byref(res))
         return {"x": x, "converged": ok == 1, "iterations": it.value, "updates": upd.value, "residue": res.value}
 
     def true_residual(self, A, b, x) -> float:

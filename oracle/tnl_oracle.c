@@ -1872,7 +1872,14 @@ done:
  * update; p is kept, beta = (r, z)_new / (r, z)_old.  precond: 0 none,
  * 1 Jacobi (diagonal of the FP32 values), 2 FSAI z = G^T (G r) from the
  * factor G and its transpose as the solver applies them (CSR, FP32 values;
- * rows summed in VT in entry order) with (r, z) = |G r|^2.  An update is
+ * rows summed in VT in entry order) with (r, z) = |G r|^2.  With `excess`
+ * (when every row holds its diagonal entry) the FP32 product is the
+ * library's row-excess form: the diagonal entry replaced by the row's FP64
+ * sum rounded to FP32, rows summed as s_i p_i + sum_j a_ij (p_j - p_i) in
+ * entry order.  Row sums and vector updates use fused multiply-adds
+ * (fmaf / fma, correctly rounded in software where the CPU has none) where
+ * the GPU kernels' a * b + c compile to one: on ill-conditioned matrices the
+ * iteration counts follow that rounding.  An update is
  * also due 4096 iterations after the last one.  Returns 1 when the true
  * FP64 residual ||b - A x|| / ||b|| < tol, 2 when the iteration stalled
  * (the true residual at the updates not halved within the last
@@ -1883,13 +1890,14 @@ typedef struct {
    const int32_t *grp, *gcols, *gtrp, *gtcols;
    const float *gvals, *gtvals;
 } OrcFsaiFactors;
-#define ORC_RELIABLE(NAME, VT)                                                                                       \
+#define ORC_RELIABLE(NAME, VT, FMA)                                                                                   \
    static int NAME(int32_t n, const int32_t* rowptr, const int32_t* cols, const double* vals, int precond,         \
                    const OrcFsaiFactors* F, const double* b, double* x, double tol, double delta, int32_t maxit,  \
-                   int32_t* iterations, int32_t* updates, double* resid)                                          \
+                   int excess, int32_t* iterations, int32_t* updates, double* resid)                              \
    {                                                                                                              \
       const int32_t nnz = rowptr[n];                                                                              \
       float* v32 = (float*)malloc(sizeof(float) * (size_t)(nnz > 0 ? nnz : 1));                                   \
+      float* s32 = (float*)malloc(sizeof(float) * (size_t)(n > 0 ? n : 1));                                       \
       float* d = (float*)malloc(sizeof(float) * (size_t)n);                                                       \
       VT *r = (VT*)malloc(sizeof(VT) * (size_t)n), *z = (VT*)malloc(sizeof(VT) * (size_t)n);                      \
       VT *p = (VT*)calloc((size_t)n, sizeof(VT)), *Ap = (VT*)malloc(sizeof(VT) * (size_t)n);                      \
@@ -1898,6 +1906,16 @@ typedef struct {
       double* xbest = (double*)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));                                  \
       double lowest = HUGE_VAL;                                                                                   \
       for (int32_t k = 0; k < nnz; k++) v32[k] = (float)vals[k];                                                  \
+      for (int32_t i = 0; i < n && excess; i++) { /* row excess: the FP64 row sum; off without a diagonal */      \
+         double e = 0.0;                                                                                          \
+         int has = 0;                                                                                             \
+         for (int32_t k = rowptr[i]; k < rowptr[i + 1]; k++) {                                                    \
+            e += vals[k];                                                                                         \
+            has |= cols[k] == i;                                                                                  \
+         }                                                                                                        \
+         s32[i] = (float)e;                                                                                       \
+         if (!has) excess = 0;                                                                                    \
+      }                                                                                                           \
       for (int32_t i = 0; i < n; i++) {                                                                           \
          float di = 0.0f;                                                                                         \
          for (int32_t k = rowptr[i]; k < rowptr[i + 1]; k++)                                                      \
@@ -1963,14 +1981,21 @@ typedef struct {
             }                                                                                                     \
          {                                                                                                        \
             const VT beta = (VT)(rz_cur / rz);                                                                    \
-            for (int32_t i = 0; i < n; i++) p[i] = z[i] + beta * p[i];                                            \
+            for (int32_t i = 0; i < n; i++) p[i] = FMA(beta, p[i], z[i]);                                         \
          }                                                                                                        \
          while (!halt) {                                                                                          \
             double pap = 0.0;                                                                                     \
             for (int32_t i = 0; i < n; i++) {                                                                     \
                VT s = (VT)0;                                                                                      \
                for (int32_t k = rowptr[i]; k < rowptr[i + 1]; k++)                                                \
-                  if (cols[k] >= 0) s += (VT)v32[k] * p[cols[k]];                                                 \
+                  if (cols[k] >= 0) {                                                                             \
+                     if (!excess)                                                                                 \
+                        s = FMA((VT)v32[k], p[cols[k]], s);                                                       \
+                     else if (cols[k] == i)                                                                       \
+                        s = FMA((VT)s32[i], p[i], s);                                                             \
+                     else                                                                                         \
+                        s = FMA((VT)v32[k], p[cols[k]] - p[i], s);                                                \
+                  }                                                                                               \
                Ap[i] = s;                                                                                         \
                pap += (double)s * (double)p[i];                                                                   \
             }                                                                                                     \
@@ -1982,8 +2007,8 @@ typedef struct {
             const VT alpha = (VT)(rz / pap);                                                                      \
             double rr = 0.0, rzn = 0.0;                                                                           \
             for (int32_t i = 0; i < n; i++) {                                                                     \
-               xc[i] += alpha * p[i];                                                                             \
-               r[i] = r[i] - alpha * Ap[i];                                                                        \
+               xc[i] = FMA(alpha, p[i], xc[i]);                                                                   \
+               r[i] = FMA(-alpha, Ap[i], r[i]);                                                                    \
                rr += (double)r[i] * (double)r[i];                                                                 \
                if (precond != 2) {                                                                                \
                   z[i] = precond == 1 ? r[i] / (VT)d[i] : r[i];                                                   \
@@ -2001,7 +2026,7 @@ typedef struct {
             if (halt) break;                                                                                      \
             rz_cur = rzn;                                                                                         \
             const VT beta = (VT)(rz_cur / rz);                                                                    \
-            for (int32_t i = 0; i < n; i++) p[i] = z[i] + beta * p[i];                                            \
+            for (int32_t i = 0; i < n; i++) p[i] = FMA(beta, p[i], z[i]);                                         \
          }                                                                                                        \
       }                                                                                                           \
       if (ok == 2 && lowest < HUGE_VAL && !(res <= lowest)) { /* back to the lowest true residual */            \
@@ -2013,6 +2038,7 @@ typedef struct {
       *resid = res;                                                                                               \
       free(xbest);                                                                                                \
       free(v32);                                                                                                  \
+      free(s32);                                                                                                  \
       free(d);                                                                                                    \
       free(r);                                                                                                    \
       free(z);                                                                                                    \
@@ -2024,49 +2050,52 @@ typedef struct {
    }
 
 /* t = G r, z = G^T t, returns (t, t) = (r, z). */
-#define ORC_FSAI_APPLY(NAME, VT)                                                                                     \
+#define ORC_FSAI_APPLY(NAME, VT, FMA)                                                                                 \
    static double NAME(int32_t n, const OrcFsaiFactors* F, const VT* r, VT* t, VT* z)                             \
    {                                                                                                              \
       double rz = 0.0;                                                                                            \
       for (int32_t i = 0; i < n; i++) {                                                                           \
          VT s = (VT)0;                                                                                            \
-         for (int32_t k = F->grp[i]; k < F->grp[i + 1]; k++) s += (VT)F->gvals[k] * r[F->gcols[k]];                \
+         for (int32_t k = F->grp[i]; k < F->grp[i + 1]; k++) s = FMA((VT)F->gvals[k], r[F->gcols[k]], s);         \
          t[i] = s;                                                                                                \
          rz += (double)s * (double)s;                                                                             \
       }                                                                                                           \
       for (int32_t i = 0; i < n; i++) {                                                                           \
          VT s = (VT)0;                                                                                            \
-         for (int32_t k = F->gtrp[i]; k < F->gtrp[i + 1]; k++) s += (VT)F->gtvals[k] * t[F->gtcols[k]];           \
+         for (int32_t k = F->gtrp[i]; k < F->gtrp[i + 1]; k++) s = FMA((VT)F->gtvals[k], t[F->gtcols[k]], s);    \
          z[i] = s;                                                                                                \
       }                                                                                                           \
       return rz;                                                                                                  \
    }
-ORC_FSAI_APPLY(reliable_f32_fsai, float)
-ORC_FSAI_APPLY(reliable_f64_fsai, double)
+ORC_FSAI_APPLY(reliable_f32_fsai, float, fmaf)
+ORC_FSAI_APPLY(reliable_f64_fsai, double, fma)
 #undef ORC_FSAI_APPLY
 
-ORC_RELIABLE(reliable_f32, float)
-ORC_RELIABLE(reliable_f64, double)
+ORC_RELIABLE(reliable_f32, float, fmaf)
+ORC_RELIABLE(reliable_f64, double, fma)
 #undef ORC_RELIABLE
 
 int orc_pcg_reliable(int32_t n, const int32_t* rowptr, const int32_t* cols, const double* vals, int precond,
-                     const double* b, double* x, double tol, double delta, int32_t maxit, int vec64,
+                     const double* b, double* x, double tol, double delta, int32_t maxit, int vec64, int excess,
                      int32_t* iterations, int32_t* updates, double* resid)
 {
    if (precond == 2) return 0;
    if (vec64)
-      return reliable_f64(n, rowptr, cols, vals, precond, NULL, b, x, tol, delta, maxit, iterations, updates, resid);
-   return reliable_f32(n, rowptr, cols, vals, precond, NULL, b, x, tol, delta, maxit, iterations, updates, resid);
+      return reliable_f64(n, rowptr, cols, vals, precond, NULL, b, x, tol, delta, maxit, excess, iterations, updates,
+                          resid);
+   return reliable_f32(n, rowptr, cols, vals, precond, NULL, b, x, tol, delta, maxit, excess, iterations, updates,
+                       resid);
 }
 
 /* The same with an FSAI factor pair (precond 2). */
 int orc_pcg_reliable_fsai(int32_t n, const int32_t* rowptr, const int32_t* cols, const double* vals,
                           const int32_t* grp, const int32_t* gcols, const float* gvals, const int32_t* gtrp,
                           const int32_t* gtcols, const float* gtvals, const double* b, double* x, double tol,
-                          double delta, int32_t maxit, int vec64, int32_t* iterations, int32_t* updates,
-                          double* resid)
+                          double delta, int32_t maxit, int vec64, int excess, int32_t* iterations,
+                          int32_t* updates, double* resid)
 {
    const OrcFsaiFactors F = {grp, gcols, gtrp, gtcols, gvals, gtvals};
-   if (vec64) return reliable_f64(n, rowptr, cols, vals, 2, &F, b, x, tol, delta, maxit, iterations, updates, resid);
-   return reliable_f32(n, rowptr, cols, vals, 2, &F, b, x, tol, delta, maxit, iterations, updates, resid);
+   if (vec64)
+      return reliable_f64(n, rowptr, cols, vals, 2, &F, b, x, tol, delta, maxit, excess, iterations, updates, resid);
+   return reliable_f32(n, rowptr, cols, vals, 2, &F, b, x, tol, delta, maxit, excess, iterations, updates, resid);
 }

@@ -239,10 +239,11 @@ def _nine_point(N):
 @pytest.mark.parametrize("dim", [2, 3])
 def test_reliable_layouts_give_the_same_iterates(inner, dim):
     """The reliable-update PCG's internal FP32 copies by diagonal (2D: 5 for
-    A, 3 for the FSAI factors, four rows per thread; 3D: 7 for A, one row
-    per thread, 4 for the factors) and with 16-bit column offsets sum the
-    same terms in the same order: on these sizes iterations, updates and x
-    agree bit for bit."""
+    A, 3 for the FSAI factors; 3D: 7 for A, 4 for the factors), their
+    products staged by bulk copies ("auto") or read by ordinary loads
+    ("diagonal": four rows per thread up to 5 diagonals, one row beyond),
+    and with 16-bit column offsets sum the same terms in the same order:
+    on these sizes iterations, updates and x agree bit for bit."""
     from tnl_b200 import generators as g
 
     t = tnl()
@@ -251,14 +252,15 @@ def test_reliable_layouts_give_the_same_iterates(inner, dim):
     M = t.SparseMatrix(t.CSR, torch.float64).assign(A.rowptr, A.cols, A.vals)
     bs = torch.tensor(b, device="cuda")
     out = []
-    for layout in ("auto", "offsets"):
+    for layout in ("auto", "offsets", "diagonal"):
         xs = torch.zeros(A.n, dtype=torch.float64, device="cuda")
         r = t.solve_mixed_reliable(M, bs, xs, tol=1e-8, delta=0.1, inner=inner, layout=layout)
         assert r["converged"] and not r["stalled"]
         out.append((r, xs))
-    (ra, xa), (ro, xo) = out
-    assert (ra["iterations"], ra["reliable_updates"]) == (ro["iterations"], ro["reliable_updates"])
-    assert torch.equal(xa, xo)
+    (ra, xa) = out[0]
+    for ro, xo in out[1:]:
+        assert (ra["iterations"], ra["reliable_updates"]) == (ro["iterations"], ro["reliable_updates"])
+        assert torch.equal(xa, xo)
     with pytest.raises(ValueError):
         t.solve_mixed_reliable(M, bs, torch.zeros_like(bs), layout="dense")
 
@@ -331,18 +333,60 @@ def test_reliable_mixed_pcg_falls_back_to_fp64(oracle, inner, vec64):
     t = tnl()
     A = fp32_singular_laplacian(32)
     b = nonzero_mean_rhs(A.n)
-    o = oracle.pcg_reliable(A, b, precond=1, tol=1e-10, delta=0.3, maxit=200000, vec64=vec64)
+    o = oracle.pcg_reliable(A, b, precond=1, tol=1e-10, delta=0.3, maxit=200000, vec64=vec64, excess=False)
     assert o["stalled"]
     M = t.SparseMatrix(t.CSR, torch.float64).assign(A.rowptr, A.cols, A.vals)
     bs = torch.tensor(b, device="cuda")
     xs = torch.zeros(A.n, dtype=torch.float64, device="cuda")
     r = t.solve_mixed_reliable(M, bs, xs, tol=1e-10, delta=0.3, max_iterations=200000, inner=inner,
-                               vectors=torch.float64 if vec64 else torch.float32)
+                               vectors=torch.float64 if vec64 else torch.float32, operator="plain")
     assert r["stalled"] and r["fallback"] and r["converged"], r
     fp32_its = r["iterations"] - r["fallback_iterations"]
     assert 16384 < fp32_its < 2 * 16384 + 4096, r
     assert 0 < r["fallback_iterations"] < 2000, r
     assert r["true_residual"] < 1e-10 and oracle.true_residual(A, b, xs.cpu().numpy()) < 1e-10
+
+
+@pytest.mark.parametrize("inner", ["jacobi", "fsai"])
+def test_reliable_row_excess_form(oracle, inner):
+    """The row-excess form of the FP32 copy of A (the default) against the
+    plain form on a high-contrast diffusion matrix (sigma = 3): each within
+    5 % of the iterations of its oracle restatement, the excess form with
+    fewer; the three layouts (bulk-copy-staged diagonals, diagonals read by
+    ordinary loads, 16-bit offsets) give the same iterates bit for bit."""
+    from tnl_b200 import generators as g
+
+    t = tnl()
+    A = g.diffusion_2d(128, 0.05, 3.0, 11)
+    b = g.uniform_vector(A.n, 1)
+    M = t.SparseMatrix(t.CSR, torch.float64).assign(A.rowptr, A.cols, A.vals)
+    bs = torch.tensor(b, device="cuda")
+    P = "jacobi"
+    G = GT = None
+    if inner == "fsai":
+        M32 = t.SparseMatrix(t.CSR, torch.float32).assign(A.rowptr, A.cols, A.vals.astype(np.float32))
+        P = t.FSAI()
+        P.update(M32)
+        G, GT = P.factor(0), P.factor(1)
+        G = (G[0], G[1], G[2].astype(np.float16).astype(np.float32))
+        GT = (GT[0], GT[1], GT[2].astype(np.float16).astype(np.float32))
+    its = {}
+    for op in ("excess", "plain"):
+        if inner == "fsai":
+            o = oracle.pcg_reliable_fsai(A, b, G, GT, tol=1e-8, delta=0.3, maxit=200000, excess=op == "excess")
+        else:
+            o = oracle.pcg_reliable(A, b, precond=1, tol=1e-8, delta=0.3, maxit=200000, excess=op == "excess")
+        runs = []
+        for layout in ("auto", "diagonal", "offsets"):
+            xs = torch.zeros(A.n, dtype=torch.float64, device="cuda")
+            r = t.solve_mixed_reliable(M, bs, xs, tol=1e-8, delta=0.3, max_iterations=200000, inner=P,
+                                       layout=layout, operator=op)
+            assert r["converged"] and not r["stalled"], (op, layout, r)
+            runs.append((r["iterations"], xs))
+        assert all(k == runs[0][0] and torch.equal(x, runs[0][1]) for k, x in runs), (op, [k for k, _ in runs])
+        assert o["converged"] and abs(runs[0][0] - o["iterations"]) <= 0.05 * o["iterations"], (op, runs[0][0], o)
+        its[op] = runs[0][0]
+    assert its["excess"] < its["plain"], its
 
 
 def test_reliable_mixed_pcg_with_fsai():

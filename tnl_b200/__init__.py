@@ -820,7 +820,8 @@ def true_residual(M: SparseMatrix, b: torch.Tensor, x: torch.Tensor) -> float:
 
 def solve_mixed_reliable(M: SparseMatrix, b: torch.Tensor, x: torch.Tensor, tol: float = 1e-8, delta: float = 0.3,
                          max_iterations: int = 1000000, inner: str | _Preconditioner = "jacobi",
-                         vectors: torch.dtype = torch.float32, layout: str = "auto") -> dict:
+                         vectors: torch.dtype = torch.float32, layout: str = "auto",
+                         operator: str = "excess") -> dict:
     """Mixed-precision PCG with reliable updates (SPD matrices, FP64 matrix
     and vectors): CG iterations on FP32 values (FP32 or FP64 ``vectors``)
     whose correction is folded into the FP64 x, with the residual recomputed
@@ -836,18 +837,30 @@ def solve_mixed_reliable(M: SparseMatrix, b: torch.Tensor, x: torch.Tensor, tol:
     learned FSAI).  Stops on the true FP64 residual ``tol``.
 
     ``layout`` picks the internal FP32 copies of short-row matrices: "auto"
-    stores a matrix with few diagonals by diagonal, others as CSR with
-    16-bit column offsets; "offsets" always the latter.  Both give the same
-    row sums bit for bit (their FP64 dot products group rows differently).
+    stores a matrix with few diagonals by diagonal, its products staging
+    their operands in shared memory by bulk copies, others as CSR with
+    16-bit column offsets; "offsets" always the latter; "diagonal" the
+    diagonal copies read by ordinary loads.  All give the same row sums bit
+    for bit (their FP64 dot products group rows differently).
+
+    ``operator`` "excess" stores, in the FP32 copy of A, each row's FP64
+    sum in place of its diagonal entry and sums a row as
+    s_i x_i + sum_j a_ij (x_j - x_i): on high-contrast diffusion operators
+    the FP32 copy then keeps the small eigenvalues that FP32 rounding of
+    a_ii destroys; "plain" keeps the values as they are.
     """
     if M.real != torch.float64:
         raise TypeError("solve_mixed_reliable takes an FP64 matrix")
-    layouts = {"auto": 0, "offsets": 1}
+    layouts = {"auto": 0, "offsets": 1, "diagonal": 2}
     if layout not in layouts:
         raise ValueError(f"solve_mixed_reliable: unknown layout {layout!r}")
+    operators = {"excess": 0, "plain": 1}
+    if operator not in operators:
+        raise ValueError(f"solve_mixed_reliable: unknown operator form {operator!r}")
     p = capi.SolverParams()
     capi.tnlb_solver_params_default(C.byref(p))
     p.reliable_layout = layouts[layout]
+    p.reliable_operator = operators[operator]
     p.convergence_residue = tol
     p.max_iterations = max_iterations
     r = capi.SolveResult()

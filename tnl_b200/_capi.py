@@ -64,7 +64,7 @@ class SolverParams(C.Structure):
         ("gmres_restarting_max", C.c_int32), ("gmres_restarting_step_min", C.c_int32),
         ("gmres_restarting_step_max", C.c_int32), ("bicgstab_exact_residue", C.c_int32), ("spmv_kernel", C.c_int32),
         ("bicgstab_ell", C.c_int32), ("idr_s", C.c_int32), ("idr_residual_smoothing", C.c_int32),
-        ("reliable_layout", C.c_int32),
+        ("reliable_layout", C.c_int32), ("reliable_operator", C.c_int32),
     ]
 
 

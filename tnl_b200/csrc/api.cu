@@ -312,6 +312,7 @@ void tnlb_solver_params_default(tnlb_solver_params* p)
    p->idr_s = 4;                      // IDRs.hpp:21
    p->idr_residual_smoothing = 0;     // IDRs.hpp:22
    p->reliable_layout = 0;
+   p->reliable_operator = 0;
 }
 
 static tnlb_status check_solve_args(const tnlb_segments* seg, tnlb_real real, const void* b, void* x)
@@ -409,6 +410,10 @@ tnlb_status tnlb_solve_mixed_reliable(const tnlb_solver_params* params, const tn
    tnlb_solver_params_default(&p);
    if (params) p = *params;
    TNLB_REQUIRE(p.max_iterations >= 0, TNLB_ERR_INVALID_ARGUMENT, "negative max_iterations");
+   TNLB_REQUIRE(p.reliable_layout >= 0 && p.reliable_layout <= 2, TNLB_ERR_INVALID_ARGUMENT,
+                "reliable_layout must be 0, 1 or 2");
+   TNLB_REQUIRE(p.reliable_operator == 0 || p.reliable_operator == 1, TNLB_ERR_INVALID_ARGUMENT,
+                "reliable_operator must be 0 or 1");
    *result = tnlb_solve_result{};
    *reliable_updates = 0;
    return tnlb::solve_mixed_reliable(seg, d_cols, d_values, d_b, d_x, p, delta, vectors, (cudaStream_t)stream, result,

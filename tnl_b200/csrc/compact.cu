@@ -23,6 +23,7 @@
 #include <cstring>
 #include <vector>
 
+#include "band.cuh"
 #include "compact.cuh"
 #include "internal.cuh"
 #include "reduce.cuh"
@@ -136,6 +137,53 @@ __global__ void k_diag_fill(const int32_t* __restrict__ rowptr, const int32_t* _
    }
 }
 
+// s[r] = the FP64 sum of row r's values in entry order, rounded to FP32
+// (the row excess a_rr + sum_{c != r} a_rc); *bad = 1 when a row holds no
+// diagonal entry.
+__global__ void k_row_excess(const int32_t* __restrict__ rowptr, const int32_t* __restrict__ cols,
+                             const double* __restrict__ v, int32_t n, float* __restrict__ s,
+                             int32_t* __restrict__ bad)
+{
+   const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+   if (r >= n) return;
+   double t = 0.0;
+   bool diag = false;
+   for (int32_t k = rowptr[r]; k < rowptr[r + 1]; k++) {
+      t += v[k];
+      diag |= cols[k] == (int32_t)r;
+   }
+   s[r] = (float)t;
+   if (!diag) *bad = 1;
+}
+
+// The diagonal entries of a CSR copy (FP32 values) replaced by s.
+__global__ void k_set_diagonal_csr(const int32_t* __restrict__ rowptr, const int32_t* __restrict__ cols,
+                                   const float* __restrict__ s, int32_t n, float* __restrict__ vals)
+{
+   const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+   if (r >= n) return;
+   for (int32_t k = rowptr[r]; k < rowptr[r + 1]; k++)
+      if (cols[k] == (int32_t)r) vals[k] = s[r];
+}
+
+// The row excesses of an FP64 CSR matrix into `s` (n floats); *ok false
+// when a row has no diagonal entry.
+tnlb_status row_excess(const int32_t* rowptr, const int32_t* cols, const double* v, int32_t n, cudaStream_t st,
+                       DeviceBuffer* s, bool* ok)
+{
+   DeviceBuffer bad;
+   TNLB_TRY_STATUS(bad.alloc(sizeof(int32_t)));
+   TNLB_TRY_STATUS(s->alloc(sizeof(float) * (n > 0 ? n : 1)));
+   TNLB_CUDA_TRY(cudaMemsetAsync(bad.ptr, 0, sizeof(int32_t), st));
+   k_row_excess<<<grid_for(n, 256), 256, 0, st>>>(rowptr, cols, v, n, s->as<float>(), bad.as<int32_t>());
+   TNLB_CHECK_LAUNCH();
+   int32_t h = 0;
+   TNLB_CUDA_TRY(cudaMemcpyAsync(&h, bad.ptr, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+   TNLB_CUDA_TRY(cudaStreamSynchronize(st));
+   *ok = h == 0;
+   return TNLB_OK;
+}
+
 // y = A x and (x, y) -- or (y, y) with `self` -- as k_csr_short_dot does.
 // Four-row policies (kQuad) store and read the rows' own entries as
 // vectors when all four rows exist (the vectors are 16-byte aligned).
@@ -209,6 +257,64 @@ __global__ void __launch_bounds__(256, Rows::kMinBlocks) k_cmp_xpby(Rows A, cons
    }
 }
 
+// k_cmp_dot on a diagonal copy with its operands staged by bulk copies
+// (band.cuh): y = A x and (x, y) -- (y, y) with `self` -- summing each row
+// as DiaRows and DiaRow1 do (the same terms in the same order, the
+// row-excess form included).  A wait that gave up makes the dot NaN.
+template <typename TV, int D>
+__global__ void __launch_bounds__(kBandThreads) k_band_dot(const TV* __restrict__ vals, int64_t pitch, DiaOffsets o,
+                                                           int32_t self_slot, BandPlan P, const float* __restrict__ x,
+                                                           float* __restrict__ y, int32_t n, int64_t npad, RedWork w,
+                                                           double* __restrict__ dot_out,
+                                                           const int32_t* __restrict__ skip, int self)
+{
+   if (band_block_flag(skip)) return;
+   extern __shared__ __align__(128) unsigned char smem[];
+   __shared__ __align__(8) uint64_t bars[2];
+   const float* const bin[1] = {x};
+   const float* const oin[1] = {nullptr};
+   double d = 0.0;
+   const bool ok = band_loop<TV, D, 1, 0>(smem, bars, P, vals, pitch, bin, oin, n, npad,
+                                          [&](int64_t i0, const unsigned char* st) {
+      const BandStage<TV> S{st, &P, i0};
+#pragma unroll 1
+      for (int q = 0; q < kBandRows; q++) {
+         const int rl = threadIdx.x + q * kBandThreads;
+         const int64_t i = i0 + rl;
+         if (i >= n) break;
+         float v[D], xx[D];
+#pragma unroll
+         for (int j = 0; j < D; j++) {
+            const int64_t c = i + o.o[j];
+            const bool in = c >= 0 && c < n;
+            v[j] = in ? S.val(j, rl) : 0.0f;
+            xx[j] = in ? S.in(0, j, c) : 0.0f;
+         }
+         if (self_slot >= 0) {
+            float xi = 0.0f;
+#pragma unroll
+            for (int j = 0; j < D; j++)
+               if (j == self_slot) xi = xx[j];
+#pragma unroll
+            for (int j = 0; j < D; j++)
+               if (j != self_slot) xx[j] -= xi;
+         }
+         float t = 0.0f;
+#pragma unroll
+         for (int j = 0; j < D; j++) t += v[j] * xx[j];
+         y[i] = t;
+         d += (double)t * (self ? (double)t : (double)S.self(0, i));
+      }
+   });
+   if (!ok) d = __longlong_as_double(0x7ff8000000000000ll);  // NaN: the caller sees a breakdown
+   double vv[1] = {d};
+   if (publish_and_arrive<1>(vv, w)) {
+      double t[1];
+      gather_totals<1>(t, w);
+      if (threadIdx.x == 0) *dot_out = t[0];
+   }
+}
+
 template <typename Rows>
 void launch_cmp_dot(const Rows& rows, int32_t n, const float* x, float* y, RedWork w, double* dot_out,
                     cudaStream_t st, const int32_t* skip, int self)
@@ -229,7 +335,7 @@ void launch_cmp_xpby(const Rows& rows, int32_t n, const float* x, float* y, cons
 
 // The diagonal layout, when the matrix has one: *ok false otherwise.
 tnlb_status diag_build(const tnlb_segments* seg, const int32_t* cols, const float* vals, bool half, float scale,
-                       cudaStream_t st, CompactCopy* out, bool* ok)
+                       const float* excess, cudaStream_t st, CompactCopy* out, bool* ok)
 {
    *ok = false;
    const int32_t n = seg->n;
@@ -255,7 +361,9 @@ tnlb_status diag_build(const tnlb_segments* seg, const int32_t* cols, const floa
    std::sort(d.begin(), d.end());
    DiaOffsets dd{};
    for (size_t j = 0; j < d.size(); j++) dd.o[j] = d[j];
-   const int64_t pitch = ((int64_t)n + 3) / 4 * 4;  // four-row vector loads stay aligned
+   // four-row vector loads stay aligned, and so do bulk copies of 8 FP16
+   // values
+   const int64_t pitch = ((int64_t)n + 7) / 8 * 8;
    const size_t elem = half ? sizeof(__half) : sizeof(float);
    const size_t bytes = elem * d.size() * (size_t)pitch;
    TNLB_TRY_STATUS(out->vals.alloc(bytes));
@@ -267,6 +375,16 @@ tnlb_status diag_build(const tnlb_segments* seg, const int32_t* cols, const floa
       k_diag_fill<float><<<grid_for(n, 256), 256, 0, st>>>(rp, cols, vals, n, dd, (int32_t)d.size(), pitch,
                                                             1.0f, out->vals.as<float>());
    TNLB_CHECK_LAUNCH();
+   out->self_slot = -1;
+   if (excess && !half) {
+      const auto z = std::find(d.begin(), d.end(), 0);
+      if (z != d.end()) {
+         const int64_t j0 = z - d.begin();
+         TNLB_CUDA_TRY(cudaMemcpyAsync(out->vals.as<float>() + j0 * pitch, excess, sizeof(float) * n,
+                                       cudaMemcpyDeviceToDevice, st));
+         out->self_slot = (int32_t)j0;
+      }
+   }
    out->kind = CompactCopy::kDia;
    out->n = n;
    out->width = (int32_t)d.size();
@@ -305,15 +423,24 @@ tnlb_status half_scale(const float* vals, int64_t nnz, cudaStream_t st, float* s
 }
 
 tnlb_status compact_build(const tnlb_segments* seg, const int32_t* cols, const float* vals, bool half, float scale,
-                          bool allow_dia, cudaStream_t st, CompactCopy* out)
+                          bool allow_dia, cudaStream_t st, CompactCopy* out, const double* vals64)
 {
    out->kind = CompactCopy::kNone;
+   out->self_slot = -1;
    if (!spmv_dot_fusable(seg)) return TNLB_OK;
    if (!half) scale = 1.0f;
+   DeviceBuffer excess;
+   bool use_excess = false;
+   if (vals64 && !half)
+      TNLB_TRY_STATUS(row_excess(seg->offsets.as<int32_t>(), cols, vals64, seg->n, st, &excess, &use_excess));
+   const float* ex = use_excess ? excess.as<float>() : nullptr;
    if (allow_dia) {
       bool ok = false;
-      TNLB_TRY_STATUS(diag_build(seg, cols, vals, half, scale, st, out, &ok));
-      if (ok) return TNLB_OK;
+      TNLB_TRY_STATUS(diag_build(seg, cols, vals, half, scale, ex, st, out, &ok));
+      if (ok) {
+         TNLB_CUDA_TRY(cudaStreamSynchronize(st));  // `excess` is released on return
+         return TNLB_OK;
+      }
    }
    const int32_t n = seg->n;
    const int64_t nnz = seg->elements;
@@ -335,6 +462,11 @@ tnlb_status compact_build(const tnlb_segments* seg, const int32_t* cols, const f
    else {
       TNLB_TRY_STATUS(out->vals.alloc(sizeof(float) * (nnz > 0 ? nnz : 1)));
       if (nnz) TNLB_CUDA_TRY(cudaMemcpyAsync(out->vals.ptr, vals, sizeof(float) * nnz, cudaMemcpyDeviceToDevice, st));
+      if (ex) {
+         k_set_diagonal_csr<<<grid_for(n, 256), 256, 0, st>>>(out->rowptr, cols, ex, n, out->vals.as<float>());
+         TNLB_CHECK_LAUNCH();
+         out->self_slot = 0;
+      }
    }
    int32_t h = 0;
    TNLB_CUDA_TRY(cudaMemcpyAsync(&h, bad.ptr, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
@@ -355,6 +487,42 @@ tnlb_status compact_spmv_dot(const CompactCopy& A, const float* x, float* y, dou
       TNLB_COMPACT_ROWS(A, __half, launch_cmp_dot(rows_, A.n, x, y, w, dot_out, st, skip, self));
    else
       TNLB_COMPACT_ROWS(A, float, launch_cmp_dot(rows_, A.n, x, y, w, dot_out, st, skip, self));
+   TNLB_CHECK_LAUNCH();
+   return TNLB_OK;
+}
+
+bool compact_band_capable(const CompactCopy& A)
+{
+   if (A.kind != CompactCopy::kDia || A.width < 1 || A.width > 8 || A.pitch % 8 != 0) return false;
+   return band_plan(A.diag, A.width, A.half ? 2 : 4, 1, 0).zero;
+}
+
+tnlb_status compact_band_dot(const CompactCopy& A, const float* x, float* y, double* partials, unsigned* counter,
+                             double* dot_out, cudaStream_t st, const int32_t* skip, bool self_dot)
+{
+   TNLB_REQUIRE(compact_band_capable(A), TNLB_ERR_INVALID_ARGUMENT, "compact_band_dot: not a banded diagonal copy");
+   TNLB_REQUIRE(aligned16(x), TNLB_ERR_INVALID_ARGUMENT, "compact_band_dot: x must be 16-byte aligned");
+   const RedWork w{partials, counter};
+   const BandPlan P = band_plan(A.diag, A.width, A.half ? 2 : 4, 1, 0);
+   DiaOffsets o{};
+   for (int j = 0; j < 8; j++) o.o[j] = A.diag[j];
+   const int64_t npad = ((int64_t)A.n + 3) / 4 * 4;
+   const int self = self_dot ? 1 : 0;
+   const size_t smem = 2 * (size_t)P.bytes;
+   auto go = [&](auto tv_tag, auto d_tag) {
+      using TV = decltype(tv_tag);
+      constexpr int D = decltype(d_tag)::value;
+      auto* k = k_band_dot<TV, D>;
+      const unsigned grid = band_grid((const void*)k, smem, A.n, kRedMaxBlocks);
+      k<<<grid, kBandThreads, smem, st>>>(A.vals.as<TV>(), A.pitch, o, A.self_slot, P, x, y, A.n, npad, w, dot_out,
+                                           skip, self);
+   };
+   TNLB_DIA_WIDTH(A.width, {
+      if (A.half)
+         go(__half(), std::integral_constant<int, D>());
+      else
+         go(float(), std::integral_constant<int, D>());
+   });
    TNLB_CHECK_LAUNCH();
    return TNLB_OK;
 }

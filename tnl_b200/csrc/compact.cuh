@@ -21,6 +21,15 @@
 // (diagonals, one row, 6 to 8 diagonals).  All sum the same terms in the
 // same order -- a missing diagonal slot adds fma(0, x, s) = s -- so for
 // finite inputs their row sums are bitwise equal.
+//
+// Row-excess form (`self` >= 0 / `excess`): the diagonal entry holds the
+// row's excess s_i = a_ii + sum_{j != i} a_ij instead of a_ii, and a row
+// sums s_i x_i + sum_{j != i} a_ij (x_j - x_i).  On a diagonally dominant
+// operator with nonpositive off-diagonals (a diffusion stencil) rounding
+// the a_ij to FP32 then perturbs the operator by a Laplacian of relative
+// size 2^-24, instead of by 2^-24 ||A|| on every eigenvalue, and x_j - x_i
+// of a smooth x is exact (Sterbenz), so the FP32 product keeps the small
+// eigenvalues that high-contrast coefficients create.
 #pragma once
 
 #include <cuda_fp16.h>
@@ -43,6 +52,7 @@ struct RelRows {
    const int32_t* __restrict__ rowptr;
    const int16_t* __restrict__ off;
    const TV* __restrict__ vals;
+   bool excess;  // row-excess form
 
    __device__ __forceinline__ int64_t first() const { return ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * R; }
    __device__ __forceinline__ int64_t step() const { return (int64_t)gridDim.x * blockDim.x * R; }
@@ -70,10 +80,16 @@ struct RelRows {
          }
 #pragma unroll
       for (int k = 0; k < R; k++) {
+         const int32_t row = (int32_t)(r0 + k);
+         const float xi = excess && r0 + k < n ? xv(row) : 0.0f;
          float t = 0.0f;
 #pragma unroll
          for (int j = 0; j < L; j++)
-            if (c[k][j] >= 0) t += v[k][j] * xv(c[k][j]);
+            if (c[k][j] >= 0) {
+               float xx = xv(c[k][j]);
+               if (excess && c[k][j] != row) xx -= xi;
+               t += v[k][j] * xx;
+            }
          s[k] = t;
       }
    }
@@ -129,6 +145,7 @@ struct DiaRows {
    const TV* __restrict__ vals;
    DiaOffsets d;
    int64_t pitch;
+   int32_t self;  // row-excess form: the slot of offset 0; -1 plain
 
    __device__ __forceinline__ int64_t first() const
    {
@@ -173,6 +190,19 @@ struct DiaRows {
                if (!in) v[j][k] = 0.0f;
             }
       }
+      if (self >= 0) {
+         float xi[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+         for (int j = 0; j < D; j++)
+            if (j == self)
+#pragma unroll
+               for (int k = 0; k < 4; k++) xi[k] = x[j][k];
+#pragma unroll
+         for (int j = 0; j < D; j++)
+            if (j != self)
+#pragma unroll
+               for (int k = 0; k < 4; k++) x[j][k] -= xi[k];
+      }
 #pragma unroll
       for (int k = 0; k < 4; k++) {
          float t = 0.0f;
@@ -195,6 +225,7 @@ struct DiaRow1 {
    const TV* __restrict__ vals;
    DiaOffsets d;
    int64_t pitch;
+   int32_t self;  // row-excess form: the slot of offset 0; -1 plain
 
    __device__ __forceinline__ int64_t first() const { return (int64_t)blockIdx.x * blockDim.x + threadIdx.x; }
    __device__ __forceinline__ int64_t step() const { return (int64_t)gridDim.x * blockDim.x; }
@@ -214,6 +245,15 @@ struct DiaRow1 {
          const bool in = rin && (uint32_t)c < (uint32_t)nr;
          v[j] = in ? rel_to_f(__ldg(vp + (int64_t)j * pitch)) : 0.0f;
          x[j] = in ? xv(c) : 0.0f;
+      }
+      if (self >= 0) {
+         float xi = 0.0f;
+#pragma unroll
+         for (int j = 0; j < D; j++)
+            if (j == self) xi = x[j];
+#pragma unroll
+         for (int j = 0; j < D; j++)
+            if (j != self) x[j] -= xi;
       }
       float t = 0.0f;
 #pragma unroll
@@ -286,14 +326,15 @@ constexpr int rel_rows_per_thread()
             using Rows = std::conditional_t<(D <= 5), DiaRows<TV, D>, DiaRow1<TV, D>>;                 \
             DiaOffsets dd_;                                                                            \
             for (int q_ = 0; q_ < 8; q_++) dd_.o[q_] = (C).diag[q_];                                   \
-            const Rows rows_{(C).vals.template as<TV>(), dd_, (C).pitch};                              \
+            const Rows rows_{(C).vals.template as<TV>(), dd_, (C).pitch, (C).self_slot};              \
             __VA_ARGS__;                                                                               \
          });                                                                                           \
       }                                                                                                \
       else {                                                                                           \
          TNLB_REL_WIDTH((C).width, {                                                                   \
             using Rows = RelRows<TV, L, rel_rows_per_thread<L>()>;                                     \
-            const Rows rows_{(C).rowptr, (C).off.template as<int16_t>(), (C).vals.template as<TV>()};  \
+            const Rows rows_{(C).rowptr, (C).off.template as<int16_t>(), (C).vals.template as<TV>(),   \
+                             (C).self_slot >= 0};                                                      \
             __VA_ARGS__;                                                                               \
          });                                                                                           \
       }                                                                                                \

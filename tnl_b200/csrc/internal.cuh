@@ -302,22 +302,35 @@ struct CompactCopy {
    bool half = false;
    const int32_t* rowptr = nullptr;
    int32_t diag[8] = {};
-   int64_t pitch = 0;  // kDia: values of diagonal j at vals[j * pitch ...], pitch a multiple of 4
+   int64_t pitch = 0;  // kDia: values of diagonal j at vals[j * pitch ...], pitch a multiple of 8
+   // row-excess form (compact.cuh): kDia the slot of offset 0, kRel 0; -1
+   // when the diagonal entries hold a_ii
+   int32_t self_slot = -1;
    DeviceBuffer off, vals;
 };
 inline bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
 // Builds the copy (kind kNone when the matrix is not short-row CSR or a
 // column lies 32768 or more from its row): kDia when allowed and the
 // diagonals hold at least 3/4 of their slots, else kRel.  FP16 values
-// (`half`) are stored times `scale`.
+// (`half`) are stored times `scale`.  With `vals64` (the FP64 values of the
+// same entries, FP32 copies only) the copy takes the row-excess form when
+// every row holds its diagonal entry: that entry stores the row's FP64 sum
+// rounded to FP32.
 tnlb_status compact_build(const tnlb_segments* seg, const int32_t* cols, const float* vals, bool half, float scale,
-                          bool allow_dia, cudaStream_t st, CompactCopy* out);
+                          bool allow_dia, cudaStream_t st, CompactCopy* out, const double* vals64 = nullptr);
 // The power of two that brings the largest |vals| into [2^13, 2^14): FP16
 // copies times it neither overflow nor lose normal-range precision (1 for
 // an all-zero array).
 tnlb_status half_scale(const float* vals, int64_t nnz, cudaStream_t st, float* scale);
 // y = A x and (x, y) -- (y, y) with self_dot -- into *dot_out.
 tnlb_status compact_spmv_dot(const CompactCopy& A, const float* x, float* y, double* partials, unsigned* counter,
+                             double* dot_out, cudaStream_t st, const int32_t* skip, bool self_dot);
+// A diagonal copy the bulk-copy-staged kernels take (band.cuh): at most 8
+// diagonals, offset 0 among them.
+bool compact_band_capable(const CompactCopy& A);
+// compact_spmv_dot on a band-capable copy, operands staged by bulk copies;
+// x must hold a multiple of 4 entries (n rounded up).
+tnlb_status compact_band_dot(const CompactCopy& A, const float* x, float* y, double* partials, unsigned* counter,
                              double* dot_out, cudaStream_t st, const int32_t* skip, bool self_dot);
 // y = A x + (*num / *den) y.
 tnlb_status compact_spmv_xpby(const CompactCopy& A, const float* x, float* y, const double* num, const double* den,

@@ -23,6 +23,7 @@
 #include "reduce.cuh"
 #include "segview.cuh"
 #include "compact.cuh"
+#include "band.cuh"
 
 namespace tnlb {
 
@@ -2425,6 +2426,148 @@ void launch_ru_gt_xpby(const Rows& GT, const float* t, float* p, float* xc, int3
    k<<<g, kRedThreads, 0, st>>>(GT, t, p, xc, n, rz_cur, S);
 }
 
+// k_ru_g_update on a diagonal copy of G with r and Ap staged by bulk copies
+// (band.cuh): each gathered r - alpha Ap formed by ru_rnext from the staged
+// entries, the row sums in the order of DiaRows / DiaRow1.  The own row's
+// new residual comes from the band of offset 0.  A wait that gave up makes
+// the block's sums NaN, which the last block turns into a breakdown.
+template <typename TV, int D>
+__global__ void __launch_bounds__(kBandThreads)
+   k_band_g_update(const TV* __restrict__ vals, int64_t pitch, DiaOffsets o, BandPlan P, const float* __restrict__ r,
+                   const float* __restrict__ Ap, float* __restrict__ rn, float* __restrict__ t, int32_t n,
+                   int64_t npad, RedWork w, RuState* S, double* __restrict__ rz_cur, const double* __restrict__ pap)
+{
+   if (band_block_flag(&S->halt)) return;
+   extern __shared__ __align__(128) unsigned char smem[];
+   __shared__ __align__(8) uint64_t bars[2];
+   const double rz = *rz_cur, tp = *pap;
+   const bool okp = tp != 0.0 && isfinite(tp);
+   const float alpha = okp ? (float)(rz / tp) : 0.0f;
+   const float* const bin[2] = {r, Ap};
+   const float* const oin[1] = {nullptr};
+   double rr = 0, tt = 0;
+   const bool ok = band_loop<TV, D, 2, 0>(smem, bars, P, vals, pitch, bin, oin, n, npad,
+                                          [&](int64_t i0, const unsigned char* st) {
+      const BandStage<TV> B{st, &P, i0};
+#pragma unroll 1
+      for (int q = 0; q < kBandRows; q++) {
+         const int rl = threadIdx.x + q * kBandThreads;
+         const int64_t i = i0 + rl;
+         if (i >= n) break;
+         float v[D], x[D];
+#pragma unroll
+         for (int j = 0; j < D; j++) {
+            const int64_t c = i + o.o[j];
+            const bool in = c >= 0 && c < n;
+            v[j] = in ? B.val(j, rl) : 0.0f;
+            x[j] = in ? ru_rnext(B.in(0, j, c), alpha, B.in(1, j, c)) : 0.0f;
+         }
+         float s = 0.0f;
+#pragma unroll
+         for (int j = 0; j < D; j++) s += v[j] * x[j];
+         const float rv = ru_rnext(B.self(0, i), alpha, B.self(1, i));
+         rn[i] = rv;
+         t[i] = s;
+         rr += (double)rv * (double)rv;
+         tt += (double)s * (double)s;
+      }
+   });
+   if (!ok) rr = __longlong_as_double(0x7ff8000000000000ll);
+   double v[2] = {rr, tt};
+   if (publish_and_arrive<2>(v, w)) {
+      double tot[2];
+      gather_totals<2>(tot, w);
+      if (threadIdx.x == 0) {
+         S->rz = rz;
+         S->alpha = (double)alpha;
+         S->it++;
+         S->rr = tot[0];
+         *rz_cur = tot[1];
+         if (!okp || !isfinite(tot[0]))
+            S->halt = 2;
+         else if (tot[0] < S->trig2 || S->it >= S->force_at)
+            S->halt = 1;
+         else if (S->it >= S->maxit)
+            S->halt = 3;
+      }
+   }
+}
+
+// k_ru_gt_xpby on a diagonal copy of G^T: t staged by bands, the tile's own
+// p and xc by bulk copies.  A wait that gave up raises a breakdown.
+template <typename TV, int D>
+__global__ void __launch_bounds__(kBandThreads)
+   k_band_gt_xpby(const TV* __restrict__ vals, int64_t pitch, DiaOffsets o, BandPlan P, const float* __restrict__ t,
+                  float* __restrict__ p, float* __restrict__ xc, int32_t n, int64_t npad,
+                  const double* __restrict__ rz_cur, RuState* S)
+{
+   if (band_block_flag(&S->halt)) return;
+   extern __shared__ __align__(128) unsigned char smem[];
+   __shared__ __align__(8) uint64_t bars[2];
+   const float beta = (float)(*rz_cur / S->rz);
+   const float alpha = (float)S->alpha;
+   const float* const bin[1] = {t};
+   const float* const oin[2] = {p, xc};
+   const bool ok = band_loop<TV, D, 1, 2>(smem, bars, P, vals, pitch, bin, oin, n, npad,
+                                          [&](int64_t i0, const unsigned char* st) {
+      const BandStage<TV> B{st, &P, i0};
+#pragma unroll 1
+      for (int q = 0; q < kBandRows; q++) {
+         const int rl = threadIdx.x + q * kBandThreads;
+         const int64_t i = i0 + rl;
+         if (i >= n) break;
+         float v[D], x[D];
+#pragma unroll
+         for (int j = 0; j < D; j++) {
+            const int64_t c = i + o.o[j];
+            const bool in = c >= 0 && c < n;
+            v[j] = in ? B.val(j, rl) : 0.0f;
+            x[j] = in ? B.in(0, j, c) : 0.0f;
+         }
+         float s = 0.0f;
+#pragma unroll
+         for (int j = 0; j < D; j++) s += v[j] * x[j];
+         const float po = B.own(0, rl);
+         xc[i] = B.own(1, rl) + alpha * po;
+         p[i] = s + beta * po;
+      }
+   });
+   if (!ok && threadIdx.x == 0) S->halt = 2;
+}
+
+// The banded forms of launch_ru_g_update / launch_ru_gt_xpby on a
+// band-capable diagonal copy (compact_band_capable) with FP16 values.
+void launch_band_g_update(const CompactCopy& G, const float* r, const float* Ap, float* rn, float* t, int32_t n,
+                          RedWork w, RuState* S, double* rz_cur, const double* pap, cudaStream_t st)
+{
+   const BandPlan P = band_plan(G.diag, G.width, (int)sizeof(__half), 2, 0);
+   DiaOffsets o{};
+   for (int j = 0; j < 8; j++) o.o[j] = G.diag[j];
+   const int64_t npad = ((int64_t)n + 3) / 4 * 4;
+   const size_t smem = 2 * (size_t)P.bytes;
+   TNLB_DIA_WIDTH(G.width, {
+      auto* k = k_band_g_update<__half, D>;
+      const unsigned grid = band_grid((const void*)k, smem, n, kRedMaxBlocks);
+      k<<<grid, kBandThreads, smem, st>>>(G.vals.as<__half>(), G.pitch, o, P, r, Ap, rn, t, n, npad, w, S, rz_cur,
+                                           pap);
+   });
+}
+
+void launch_band_gt_xpby(const CompactCopy& GT, const float* t, float* p, float* xc, int32_t n, const double* rz_cur,
+                         RuState* S, cudaStream_t st)
+{
+   const BandPlan P = band_plan(GT.diag, GT.width, (int)sizeof(__half), 1, 2);
+   DiaOffsets o{};
+   for (int j = 0; j < 8; j++) o.o[j] = GT.diag[j];
+   const int64_t npad = ((int64_t)n + 3) / 4 * 4;
+   const size_t smem = 2 * (size_t)P.bytes;
+   TNLB_DIA_WIDTH(GT.width, {
+      auto* k = k_band_gt_xpby<__half, D>;
+      const unsigned grid = band_grid((const void*)k, smem, n, kRedMaxBlocks);
+      k<<<grid, kBandThreads, smem, st>>>(GT.vals.as<__half>(), GT.pitch, o, P, t, p, xc, n, npad, rz_cur, S);
+   });
+}
+
 // x += xc + alpha p, the step k_ru_gt_xpby skips when the iteration that
 // formed alpha raised `halt` (alpha is 0 before the first iteration); xc = 0.
 template <typename VT>
@@ -2532,14 +2675,17 @@ tnlb_status reliable_t(const tnlb_segments* seg, const int32_t* cols, const doub
 {
    constexpr tnlb_real kVec = sizeof(VT) == 8 ? TNLB_F64 : TNLB_F32;
    const int64_t n = seg->n;
+   // vectors hold a multiple of 4 entries: the bulk copies of the banded
+   // kernels (band.cuh) read whole 16-byte groups
+   const int64_t npad = (n + 3) / 4 * 4;
    DeviceBuffer v32, ax, r, z, p, Ap, xc, scal;
    TNLB_TRY_STATUS(v32.alloc(sizeof(float) * (seg->storage > 0 ? seg->storage : 1)));
    TNLB_TRY_STATUS(ax.alloc(sizeof(double) * n));
-   TNLB_TRY_STATUS(r.alloc(sizeof(VT) * n));
-   TNLB_TRY_STATUS(z.alloc(sizeof(VT) * n));
-   TNLB_TRY_STATUS(p.alloc(sizeof(VT) * n));
-   TNLB_TRY_STATUS(Ap.alloc(sizeof(VT) * n));
-   TNLB_TRY_STATUS(xc.alloc(sizeof(VT) * n));
+   TNLB_TRY_STATUS(r.alloc(sizeof(VT) * npad));
+   TNLB_TRY_STATUS(z.alloc(sizeof(VT) * npad));
+   TNLB_TRY_STATUS(p.alloc(sizeof(VT) * npad));
+   TNLB_TRY_STATUS(Ap.alloc(sizeof(VT) * npad));
+   TNLB_TRY_STATUS(xc.alloc(sizeof(VT) * npad));
    TNLB_TRY_STATUS(scal.alloc(sizeof(double) * 4));  // [0] (p, Ap), [1] (r, z), [2..3] residual sums
    k_convert<float, double><<<grid_for(seg->storage, 256 * 8), 256, 0, st>>>(seg->storage, vals, v32.as<float>());
    TNLB_CHECK_LAUNCH();
@@ -2588,9 +2734,11 @@ tnlb_status reliable_t(const tnlb_segments* seg, const int32_t* cols, const doub
    // (compact.cu), which the FP32 products read instead of the 8-byte
    // entries
    CompactCopy cA, cG, cGT;
-   const bool compact_dia = prm.reliable_layout == 0;
+   const bool compact_dia = prm.reliable_layout != 1;
    if (kVec == TNLB_F32) {
-      if (fused_a) TNLB_TRY_STATUS(compact_build(seg, cols, v32f, false, 1.0f, compact_dia, st, &cA));
+      if (fused_a)
+         TNLB_TRY_STATUS(compact_build(seg, cols, v32f, false, 1.0f, compact_dia, st, &cA,
+                                       prm.reliable_operator == 0 ? vals : nullptr));
       if (fused_m) {
          // G and G^T in FP16 times one power of two (PCG's iterates do not
          // change when M is scaled), so that no entry overflows
@@ -2605,13 +2753,20 @@ tnlb_status reliable_t(const tnlb_segments* seg, const int32_t* cols, const doub
    }
    const bool cmp_a = cA.kind != CompactCopy::kNone;
    const bool cmp_m = cG.kind != CompactCopy::kNone && cGT.kind != CompactCopy::kNone;
-   float* tvec = mode == 2 ? (float*)fsai_view(pobj->fsai).tmp : nullptr;
+   // diagonal copies whose products stage their operands by bulk copies
+   const bool band_a = prm.reliable_layout == 0 && cmp_a && compact_band_capable(cA);
+   const bool band_m = prm.reliable_layout == 0 && cmp_m && compact_band_capable(cG) && compact_band_capable(cGT);
    // with the compact FSAI copies the update of xc and r goes into the two
    // factor products (k_ru_g_update, k_ru_gt_xpby); the new residual goes
-   // to the other of two buffers, iteration by iteration
+   // to the other of two buffers, iteration by iteration, and t = G r to a
+   // buffer of its own
    const bool fused_u = cmp_m;
-   DeviceBuffer r2;
-   if (fused_u) TNLB_TRY_STATUS(r2.alloc(sizeof(float) * n));
+   DeviceBuffer r2, tb;
+   if (fused_u) {
+      TNLB_TRY_STATUS(r2.alloc(sizeof(float) * npad));
+      TNLB_TRY_STATUS(tb.alloc(sizeof(float) * npad));
+   }
+   float* tvec = fused_u ? tb.as<float>() : mode == 2 ? (float*)fsai_view(pobj->fsai).tmp : nullptr;
    TNLB_REQUIRE(!fused_u || aligned16(tvec), TNLB_ERR_INVALID_ARGUMENT,
                 "solve_mixed_reliable: the FSAI work vector must be 16-byte aligned");
 
@@ -2636,7 +2791,10 @@ tnlb_status reliable_t(const tnlb_segments* seg, const int32_t* cols, const doub
       return TNLB_OK;
    };
    auto iteration = [&](cudaStream_t s, int k) -> tnlb_status {
-      if (cmp_a)
+      if (band_a)
+         TNLB_TRY_STATUS(compact_band_dot(cA, (const float*)p.ptr, (float*)Ap.ptr, WA.partials.as<double>(),
+                                          WA.counter.as<unsigned>(), pap, s, halt, false));
+      else if (cmp_a)
          TNLB_TRY_STATUS(compact_spmv_dot(cA, (const float*)p.ptr, (float*)Ap.ptr, WA.partials.as<double>(),
                                           WA.counter.as<unsigned>(), pap, s, halt, false));
       else if (fused_a)
@@ -2654,6 +2812,13 @@ tnlb_status reliable_t(const tnlb_segments* seg, const int32_t* cols, const doub
          // even iterations r -> r2, odd ones r2 -> r: a batch (even) ends in r
          const float* rin = (const float*)(k & 1 ? r2.ptr : r.ptr);
          float* rout = (float*)(k & 1 ? r.ptr : r2.ptr);
+         if (band_m) {
+            launch_band_g_update(cG, rin, (const float*)Ap.ptr, rout, tvec, (int32_t)n, W.red(), S, rz_cur, pap, s);
+            TNLB_CHECK_LAUNCH();
+            launch_band_gt_xpby(cGT, tvec, (float*)p.ptr, (float*)xc.ptr, (int32_t)n, rz_cur, S, s);
+            TNLB_CHECK_LAUNCH();
+            return TNLB_OK;
+         }
          TNLB_COMPACT_ROWS(cG, __half,
                            launch_ru_g_update(rows_, rin, (const float*)Ap.ptr, rout, tvec, (int32_t)n, W.red(), S,
                                               rz_cur, pap, s));
@@ -2845,17 +3010,24 @@ tnlb_status reliable_t(const tnlb_segments* seg, const int32_t* cols, const doub
          tnlb_precond* p;
          ~JGuard() { delete p; }
       } jguard{jac};
-      // the recursion's stopping residue a little below the tolerance, so
-      // that the true residual, checked below, falls under it too
+      // CG stops on sqrt((r, M^-1 r)) / ||M^-1 b||, which on a badly scaled
+      // matrix lies orders of magnitude away from the true residual: each
+      // run that ends above the tolerance is followed by one from its x
+      // with the stopping residue scaled by the gap it showed
       tnlb_solver_params p64 = prm;
-      p64.max_iterations = prm.max_iterations - fp32_its;
       p64.min_iterations = 0;
-      p64.convergence_residue = 0.5 * prm.convergence_residue;
+      double tau = 0.5 * prm.convergence_residue;
       const Ctx<double> c64{seg, TNLB_F64, cols, vals, n, cs};
-      tnlb_solve_result r64{};
-      TNLB_TRY_STATUS(cg_solve<double>(c64, view<double>(jac), p64, b, x, &r64));
-      fb_its = r64.iterations;
-      TNLB_TRY_STATUS(true_residual(seg, TNLB_F64, cols, vals, b, x, cs, &resid));
+      for (int run = 0; run < 8 && fp32_its + fb_its < prm.max_iterations; run++) {
+         p64.max_iterations = prm.max_iterations - fp32_its - fb_its;
+         p64.convergence_residue = tau;
+         tnlb_solve_result r64{};
+         TNLB_TRY_STATUS(cg_solve<double>(c64, view<double>(jac), p64, b, x, &r64));
+         fb_its += r64.iterations;
+         TNLB_TRY_STATUS(true_residual(seg, TNLB_F64, cols, vals, b, x, cs, &resid));
+         if (bn == 0 || resid < prm.convergence_residue || !std::isfinite(resid)) break;
+         tau *= 0.5 * prm.convergence_residue / resid;
+      }
       converged = bn == 0 || resid < prm.convergence_residue;
    }
    TNLB_CUDA_TRY(cudaStreamSynchronize(cs));
