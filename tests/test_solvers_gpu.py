@@ -235,15 +235,17 @@ def _nine_point(N):
     return g.CSRMatrix(A.indptr.astype(np.int32), A.indices.astype(np.int32), A.data.astype(np.float64))
 
 
-@pytest.mark.parametrize("inner", ["fsai", "jacobi", "none"])
+@pytest.mark.parametrize("inner", ["fsai", "fsai1", "jacobi", "none"])
 @pytest.mark.parametrize("dim", [2, 3])
 def test_reliable_layouts_give_the_same_iterates(inner, dim):
     """The reliable-update PCG's internal FP32 copies by diagonal (2D: 5 for
-    A, 3 for the FSAI factors; 3D: 7 for A, 4 for the factors), their
-    products staged by bulk copies ("auto") or read by ordinary loads
-    ("diagonal": four rows per thread up to 5 diagonals, one row beyond),
-    and with 16-bit column offsets sum the same terms in the same order:
-    on these sizes iterations, updates and x agree bit for bit."""
+    A, 3 for the FSAI factors, 7 for those of the level-1 pattern; 3D: 7
+    for A, 4 for the factors, whose level-1 form -- 13 entries a row --
+    takes 16-bit offsets), with their products staged by bulk copies beyond
+    5 diagonals ("auto") or read by ordinary loads ("diagonal": four rows
+    per thread up to 5 diagonals, one row beyond), and with 16-bit column
+    offsets sum the same terms in the same order: on these sizes
+    iterations, updates and x agree bit for bit."""
     from tnl_b200 import generators as g
 
     t = tnl()
@@ -251,6 +253,10 @@ def test_reliable_layouts_give_the_same_iterates(inner, dim):
     b = g.uniform_vector(A.n, 1)
     M = t.SparseMatrix(t.CSR, torch.float64).assign(A.rowptr, A.cols, A.vals)
     bs = torch.tensor(b, device="cuda")
+    if inner == "fsai1":
+        M32 = t.SparseMatrix(t.CSR, torch.float32).assign(A.rowptr, A.cols, A.vals.astype(np.float32))
+        inner = t.FSAI(1)
+        inner.update(M32)
     out = []
     for layout in ("auto", "offsets", "diagonal"):
         xs = torch.zeros(A.n, dtype=torch.float64, device="cuda")

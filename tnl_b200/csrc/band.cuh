@@ -6,19 +6,23 @@
 // D inputs with ordinary loads.  Profiled on the 2048^2 5-point operator
 // and its FSAI factors they ran at 28-47% of the DRAM bandwidth, their
 // warps stalled on long-scoreboard loads: latency-bound, too few bytes in
-// flight per SM.  Here a block works on tiles of kBandT consecutive rows.
-// One thread issues, for the next tile, bulk copies of
+// flight per SM.  Here a block works on tiles of kBandT consecutive rows
+// held in up to kBandStages shared-memory stages.  A producer warp issues,
+// for each tile, bulk copies of
 //   * the D value runs of the tile's rows (contiguous in the DIA layout),
 //   * for every input vector, one run per "band" -- a group of diagonals
 //     whose offsets lie within kBandGap of each other (a 5-point operator
 //     has three: -N; -1, 0, 1; +N) -- covering the inputs of all the
 //     tile's rows on those diagonals, and
 //   * for some kernels, the tile's own entries of vectors it updates,
-// all completing on one mbarrier, while the block computes the current
-// tile from the other of two stages.  Up to two stages of tens of KB are
-// in flight per block, against a few KB for the register-staged kernels.
-// A tile's rows are spread over the threads with a stride of the block
-// size, so that the shared-memory reads of a warp are consecutive words.
+// all completing on the stage's "full" mbarrier; eight consumer warps wait
+// on it, compute the tile and release the stage on its "empty" mbarrier,
+// which the producer waits on before it refills the stage.  No block-wide
+// barrier separates the tiles: with two blocks of 2-3 stages of 30-40 KB
+// per SM, about 100 KB are in flight per SM (a microbenchmark of this
+// scheme streamed 6.3-6.7 TB/s out of DRAM).  A tile's rows are spread
+// over the consumer threads with a stride of their count, so that the
+// shared-memory reads of a warp are consecutive words.
 // Each row sums the same terms in the same order as DiaRows / DiaRow1.
 //
 // Bulk copies need 16-byte-aligned addresses and sizes: the value pitch is
@@ -35,12 +39,17 @@
 #include <cstdint>
 
 #include "compact.cuh"
+#include "internal.cuh"
+#include "reduce.cuh"
 
 namespace tnlb {
 
-constexpr int kBandT = 1024;       // rows of a tile
-constexpr int kBandThreads = 256;  // threads of a block
-constexpr int kBandGap = 16;       // diagonals closer than this share a band
+constexpr int kBandT = 1024;                    // rows of a tile
+constexpr int kBandThreads = 256;               // consumer threads of a block (8 warps)
+constexpr int kBandBlock = kBandThreads + 32;   // and one producer warp
+constexpr int kBandStages = 4;                  // at most this many tiles a block holds
+constexpr uint32_t kBandSmem = 110 * 1024;      // stage bytes a block may take (two blocks per SM)
+constexpr int kBandGap = 16;                    // diagonals closer than this share a band
 constexpr int kBandRows = kBandT / kBandThreads;
 constexpr long kBandSpin = 1L << 24;  // mbarrier polls before a wait gives up
 
@@ -59,6 +68,12 @@ struct BandPlan {
    int32_t zlo = 0;            // the band of offset 0
    uint32_t zband[2] = {};
    bool zero = false;  // offset 0 among the diagonals
+   int32_t minlo = 0, maxhi = 0;  // the smallest and largest offsets
+   // interior tiles (no band run clipped at row 0): the byte offset, from
+   // the stage, of input k on diagonal j at the tile's row 0, and of input
+   // k at the own row 0; independent of the tile
+   uint32_t xoff[2][8] = {}, selfoff[2] = {};
+   int32_t stages = 2;  // stages a block holds (<= kBandStages)
 };
 
 // The plan for ascending offsets o[0..D-1] (D <= 8), values of vbytes
@@ -91,15 +106,26 @@ inline BandPlan band_plan(const int32_t* o, int D, int vbytes, int KB, int KO)
       off += kBandT * 4;
    }
    P.bytes = (off + 127) & ~127u;
+   P.minlo = D > 0 ? o[0] : 0;
+   P.maxhi = D > 0 ? o[D - 1] : 0;
    for (int j = 0; j < D; j++) {
       P.dlo[j] = P.lo[of[j]];
-      for (int k = 0; k < KB; k++) P.dband[k][j] = P.band[k][of[j]];
+      for (int k = 0; k < KB; k++) {
+         P.dband[k][j] = P.band[k][of[j]];
+         // run start i0 + (lo & ~3) when i0 + lo >= 0 (i0 a multiple of 4)
+         P.xoff[k][j] = P.band[k][of[j]] + 4u * (uint32_t)(o[j] - (P.lo[of[j]] & ~3));
+      }
       if (o[j] == 0) {
          P.zero = true;
          P.zlo = P.lo[of[j]];
-         for (int k = 0; k < KB; k++) P.zband[k] = P.band[k][of[j]];
+         for (int k = 0; k < KB; k++) {
+            P.zband[k] = P.band[k][of[j]];
+            P.selfoff[k] = P.band[k][of[j]] + 4u * (uint32_t)(-(P.lo[of[j]] & ~3));
+         }
       }
    }
+   const uint32_t fit = kBandSmem / (P.bytes > 0 ? P.bytes : 1);
+   P.stages = (int32_t)(fit < 2 ? 2 : fit > (uint32_t)kBandStages ? (uint32_t)kBandStages : fit);
    return P;
 }
 
@@ -191,52 +217,122 @@ __device__ __forceinline__ void band_issue(unsigned char* st, uint64_t* bar, con
    for (int k = 0; k < KO; k++) band_copy(st + P.own[k], oin[k] + i0, (uint32_t)(orows * 4), bar);
 }
 
-// The tile loop: stage s of tile k, the next tile's copies issued before
-// the current one is computed.  tile(i0, stage) computes a tile.  Returns
-// false, in every thread, after a wait gave up (the block then stops
-// taking tiles).
+__device__ __forceinline__ void band_arrive(uint64_t* bar)
+{
+   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(band_smem(bar)) : "memory");
+}
+
+// The tile loop.  Warp kBandThreads / 32 (lane 0) produces: tile k goes to
+// stage k % kBandStages once the consumers released the tile before it in
+// that stage.  The other warps consume: wait for the stage, tile(i0,
+// stage), release it.  Returns false in every thread after a wait gave up;
+// the producer then waits (bounded) for its copies still in flight before
+// the block's shared memory is released.
 template <typename TV, int D, int KB, int KO, typename Tile>
-__device__ __forceinline__ bool band_loop(unsigned char* smem, uint64_t* bars, const BandPlan& P, const TV* vals,
-                                          int64_t pitch, const float* const (&bin)[KB > 0 ? KB : 1],
+__device__ __forceinline__ bool band_loop(unsigned char* smem, uint64_t* full, uint64_t* empty, const BandPlan& P,
+                                          const TV* vals, int64_t pitch, const float* const (&bin)[KB > 0 ? KB : 1],
                                           const float* const (&oin)[KO > 0 ? KO : 1], int64_t n, int64_t npad,
                                           Tile&& tile)
 {
    const int64_t tiles = (n + kBandT - 1) / kBandT;
+   const int S = P.stages;
+   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
    if (threadIdx.x == 0) {
-      band_bar_init(&bars[0]);
-      band_bar_init(&bars[1]);
+      for (int s = 0; s < S; s++) {
+         band_bar_init(&full[s]);
+         asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(band_smem(&empty[s])), "r"(kBandThreads / 32)
+                      : "memory");
+      }
       asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
    }
    __syncthreads();
-   int64_t t = blockIdx.x;
-   if (threadIdx.x == 0 && t < tiles)
-      band_issue<TV, D, KB, KO>(smem, &bars[0], P, vals, pitch, bin, oin, npad, t * kBandT);
-   uint32_t phase[2] = {0u, 0u};
    bool ok = true;
-   for (int k = 0; t < tiles; k++, t += gridDim.x) {
-      const int s = k & 1;
-      const int64_t next = t + gridDim.x;
-      const bool issued_next = next < tiles;
-      if (issued_next && threadIdx.x == 0) {
-         // the stage was last read by the generic proxy (the tile before)
-         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-         band_issue<TV, D, KB, KO>(smem + (size_t)(s ^ 1) * P.bytes, &bars[s ^ 1], P, vals, pitch, bin, oin, npad,
-                                   next * kBandT);
+   if (warp == kBandThreads / 32) {
+      if (lane == 0) {
+         int64_t k = 0;  // tiles issued
+         for (int64_t t = blockIdx.x; t < tiles; t += gridDim.x, k++) {
+            const int s = (int)(k % S);
+            if (k >= S && !band_wait(&empty[s], (uint32_t)((k / S - 1) & 1))) {
+               ok = false;
+               break;
+            }
+            // the stage was last read by the generic proxy
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            band_issue<TV, D, KB, KO>(smem + (size_t)s * P.bytes, &full[s], P, vals, pitch, bin, oin, npad,
+                                      t * kBandT);
+         }
+         if (!ok)  // the last tile issued to each stage: k - 1, k - 2, ...
+            for (int64_t q = k - 1; q >= 0 && q >= k - S; q--) band_wait(&full[q % S], (uint32_t)((q / S) & 1));
       }
-      // every thread polls; the block goes on only when all saw the phase
-      if (!__syncthreads_and(band_wait(&bars[s], phase[s]) ? 1 : 0)) {
-         // let the other stage's copies land (or give up on them) before
-         // the block's shared memory is released
-         if (issued_next && threadIdx.x == 0) band_wait(&bars[s ^ 1], phase[s ^ 1]);
-         ok = false;
-         break;
+   }
+   else {
+      int64_t k = 0;
+      for (int64_t t = blockIdx.x; t < tiles; t += gridDim.x, k++) {
+         const int s = (int)(k % S);
+         if (!__all_sync(0xffffffffu, band_wait(&full[s], (uint32_t)((k / S) & 1)))) {
+            ok = false;
+            break;
+         }
+         tile(t * kBandT, smem + (size_t)s * P.bytes);
+         __syncwarp();
+         if (lane == 0) band_arrive(&empty[s]);
       }
-      phase[s] ^= 1u;
-      tile(t * kBandT, smem + (size_t)s * P.bytes);
-      __syncthreads();
+   }
+   return __syncthreads_and(ok ? 1 : 0) != 0;
+}
+
+// Block and grid sums of the band kernels (any block size): as
+// publish_and_arrive / gather_totals of reduce.cuh.
+template <int K>
+__device__ __forceinline__ bool band_publish(const double (&v)[K], RedWork w)
+{
+   __shared__ double s_ws[K][kBandBlock / 32];
+   __shared__ bool s_last;
+   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+   for (int k = 0; k < K; k++) {
+      const double x = warp_sum(v[k]);
+      if (lane == 0) s_ws[k][wid] = x;
    }
    __syncthreads();
-   return ok;
+   if (threadIdx.x == 0) {
+#pragma unroll
+      for (int k = 0; k < K; k++) {
+         double r = 0.0;
+         for (int q = 0; q < (int)(blockDim.x >> 5); q++) r += s_ws[k][q];
+         w.partials[(size_t)k * kRedMaxBlocks + blockIdx.x] = r;
+      }
+      __threadfence();
+      const unsigned t = atomicAdd(w.counter, 1u);
+      s_last = (t == gridDim.x - 1);
+   }
+   __syncthreads();
+   return s_last;
+}
+
+template <int K>
+__device__ __forceinline__ void band_totals(double (&out)[K], RedWork w)
+{
+   __shared__ double s_ws[K][kBandBlock / 32];
+   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+   for (int k = 0; k < K; k++) {
+      double v = 0.0;
+      for (unsigned i = threadIdx.x; i < gridDim.x; i += blockDim.x)
+         v += __ldcg(w.partials + (size_t)k * kRedMaxBlocks + i);
+      v = warp_sum(v);
+      if (lane == 0) s_ws[k][wid] = v;
+   }
+   __syncthreads();
+   if (threadIdx.x == 0) {
+#pragma unroll
+      for (int k = 0; k < K; k++) {
+         double r = 0.0;
+         for (int q = 0; q < (int)(blockDim.x >> 5); q++) r += s_ws[k][q];
+         out[k] = r;
+      }
+      *w.counter = 0;
+   }
 }
 
 // Blocks of a band kernel with `smem` bytes of dynamic shared memory kept
@@ -249,7 +345,7 @@ inline unsigned band_grid(const void* kernel, size_t smem, int64_t n, int max_bl
        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
       sms = 148;
    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, kBandThreads, smem) != cudaSuccess || occ < 1) {
+   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, kBandBlock, smem) != cudaSuccess || occ < 1) {
       cudaGetLastError();
       occ = 1;
    }
@@ -258,6 +354,50 @@ inline unsigned band_grid(const void* kernel, size_t smem, int64_t n, int max_bl
    if (g > max_blocks) g = max_blocks;
    return (unsigned)(g < 1 ? 1 : g);
 }
+
+// Per-tile pointers into a stage, at this thread's first row (the tile's
+// row threadIdx.x; its rows q follow at + q * kBandThreads): the value run
+// of diagonal 0 (diagonal j at + j * kBandT), input k on diagonal j, and
+// input k at the own row.  `interior`: every column of the tile's rows lies
+// in [0, n) and the tile is full, so no row or column needs a check.  The
+// pointers are formed once per tile; each tap is then one shared-memory
+// load at a fixed offset.
+template <typename TV, int D, int KB>
+struct BandPtrs {
+   const TV* v;
+   const float* x[KB > 0 ? KB : 1][D];
+   const float* self[KB > 0 ? KB : 1];
+   const float* own[2];
+   bool interior;
+   __device__ __forceinline__ BandPtrs(const unsigned char* st, const BandPlan& P, const DiaOffsets& o, int64_t i0,
+                                       int64_t n)
+   {
+      interior = i0 + P.minlo >= 0 && i0 + kBandT + P.maxhi <= n && i0 + kBandT <= n;
+      const unsigned char* me = st + 4 * threadIdx.x;
+      v = reinterpret_cast<const TV*>(st + P.vals) + threadIdx.x;
+      if (interior) {
+#pragma unroll
+         for (int k = 0; k < KB; k++) {
+#pragma unroll
+            for (int j = 0; j < D; j++) x[k][j] = reinterpret_cast<const float*>(me + P.xoff[k][j]);
+            self[k] = reinterpret_cast<const float*>(me + P.selfoff[k]);
+         }
+      }
+      else {
+#pragma unroll
+         for (int k = 0; k < KB; k++) {
+#pragma unroll
+            for (int j = 0; j < D; j++)
+               x[k][j] = reinterpret_cast<const float*>(st + P.dband[k][j]) +
+                         (int32_t)(i0 + o.o[j] - band_start(P.dlo[j], i0)) + (int32_t)threadIdx.x;
+            self[k] = reinterpret_cast<const float*>(st + P.zband[k]) + (int32_t)(i0 - band_start(P.zlo, i0)) +
+                      (int32_t)threadIdx.x;
+         }
+      }
+      own[0] = reinterpret_cast<const float*>(me + P.own[0]);
+      own[1] = reinterpret_cast<const float*>(me + P.own[1]);
+   }
+};
 
 // The staged operands of one tile.
 template <typename TV>

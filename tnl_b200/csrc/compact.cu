@@ -262,7 +262,7 @@ __global__ void __launch_bounds__(256, Rows::kMinBlocks) k_cmp_xpby(Rows A, cons
 // as DiaRows and DiaRow1 do (the same terms in the same order, the
 // row-excess form included).  A wait that gave up makes the dot NaN.
 template <typename TV, int D>
-__global__ void __launch_bounds__(kBandThreads) k_band_dot(const TV* __restrict__ vals, int64_t pitch, DiaOffsets o,
+__global__ void __launch_bounds__(kBandBlock) k_band_dot(const TV* __restrict__ vals, int64_t pitch, DiaOffsets o,
                                                            int32_t self_slot, BandPlan P, const float* __restrict__ x,
                                                            float* __restrict__ y, int32_t n, int64_t npad, RedWork w,
                                                            double* __restrict__ dot_out,
@@ -270,47 +270,57 @@ __global__ void __launch_bounds__(kBandThreads) k_band_dot(const TV* __restrict_
 {
    if (band_block_flag(skip)) return;
    extern __shared__ __align__(128) unsigned char smem[];
-   __shared__ __align__(8) uint64_t bars[2];
+   __shared__ __align__(8) uint64_t full[kBandStages], empty[kBandStages];
    const float* const bin[1] = {x};
    const float* const oin[1] = {nullptr};
    double d = 0.0;
-   const bool ok = band_loop<TV, D, 1, 0>(smem, bars, P, vals, pitch, bin, oin, n, npad,
+   const bool ok = band_loop<TV, D, 1, 0>(smem, full, empty, P, vals, pitch, bin, oin, n, npad,
                                           [&](int64_t i0, const unsigned char* st) {
-      const BandStage<TV> S{st, &P, i0};
-#pragma unroll 1
-      for (int q = 0; q < kBandRows; q++) {
-         const int rl = threadIdx.x + q * kBandThreads;
-         const int64_t i = i0 + rl;
-         if (i >= n) break;
-         float v[D], xx[D];
+      const BandPtrs<TV, D, 1> B(st, P, o, i0, n);
+      auto rows = [&](auto check) {
+         constexpr bool C = decltype(check)::value;
 #pragma unroll
-         for (int j = 0; j < D; j++) {
-            const int64_t c = i + o.o[j];
-            const bool in = c >= 0 && c < n;
-            v[j] = in ? S.val(j, rl) : 0.0f;
-            xx[j] = in ? S.in(0, j, c) : 0.0f;
+         for (int q = 0; q < kBandRows; q++) {
+            const int rl = q * kBandThreads;
+            const int64_t i = i0 + threadIdx.x + rl;
+            if (C && i >= n) break;
+            float v[D], xx[D];
+#pragma unroll
+            for (int j = 0; j < D; j++) {
+               bool in = true;
+               if (C) {
+                  const int64_t c = i + o.o[j];
+                  in = c >= 0 && c < n;
+               }
+               v[j] = in ? rel_to_f(B.v[j * kBandT + rl]) : 0.0f;
+               xx[j] = in ? B.x[0][j][rl] : 0.0f;
+            }
+            if (self_slot >= 0) {
+               float xi = 0.0f;
+#pragma unroll
+               for (int j = 0; j < D; j++)
+                  if (j == self_slot) xi = xx[j];
+#pragma unroll
+               for (int j = 0; j < D; j++)
+                  if (j != self_slot) xx[j] -= xi;
+            }
+            float t = 0.0f;
+#pragma unroll
+            for (int j = 0; j < D; j++) t += v[j] * xx[j];
+            y[i] = t;
+            d += (double)t * (self ? (double)t : (double)B.self[0][rl]);
          }
-         if (self_slot >= 0) {
-            float xi = 0.0f;
-#pragma unroll
-            for (int j = 0; j < D; j++)
-               if (j == self_slot) xi = xx[j];
-#pragma unroll
-            for (int j = 0; j < D; j++)
-               if (j != self_slot) xx[j] -= xi;
-         }
-         float t = 0.0f;
-#pragma unroll
-         for (int j = 0; j < D; j++) t += v[j] * xx[j];
-         y[i] = t;
-         d += (double)t * (self ? (double)t : (double)S.self(0, i));
-      }
+      };
+      if (B.interior)
+         rows(std::false_type{});
+      else
+         rows(std::true_type{});
    });
    if (!ok) d = __longlong_as_double(0x7ff8000000000000ll);  // NaN: the caller sees a breakdown
    double vv[1] = {d};
-   if (publish_and_arrive<1>(vv, w)) {
+   if (band_publish<1>(vv, w)) {
       double t[1];
-      gather_totals<1>(t, w);
+      band_totals<1>(t, w);
       if (threadIdx.x == 0) *dot_out = t[0];
    }
 }
@@ -508,13 +518,13 @@ tnlb_status compact_band_dot(const CompactCopy& A, const float* x, float* y, dou
    for (int j = 0; j < 8; j++) o.o[j] = A.diag[j];
    const int64_t npad = ((int64_t)A.n + 3) / 4 * 4;
    const int self = self_dot ? 1 : 0;
-   const size_t smem = 2 * (size_t)P.bytes;
+   const size_t smem = (size_t)P.stages * P.bytes;
    auto go = [&](auto tv_tag, auto d_tag) {
       using TV = decltype(tv_tag);
       constexpr int D = decltype(d_tag)::value;
       auto* k = k_band_dot<TV, D>;
       const unsigned grid = band_grid((const void*)k, smem, A.n, kRedMaxBlocks);
-      k<<<grid, kBandThreads, smem, st>>>(A.vals.as<TV>(), A.pitch, o, A.self_slot, P, x, y, A.n, npad, w, dot_out,
+      k<<<grid, kBandBlock, smem, st>>>(A.vals.as<TV>(), A.pitch, o, A.self_slot, P, x, y, A.n, npad, w, dot_out,
                                            skip, self);
    };
    TNLB_DIA_WIDTH(A.width, {

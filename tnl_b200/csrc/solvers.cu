@@ -2432,51 +2432,61 @@ void launch_ru_gt_xpby(const Rows& GT, const float* t, float* p, float* xc, int3
 // new residual comes from the band of offset 0.  A wait that gave up makes
 // the block's sums NaN, which the last block turns into a breakdown.
 template <typename TV, int D>
-__global__ void __launch_bounds__(kBandThreads)
+__global__ void __launch_bounds__(kBandBlock)
    k_band_g_update(const TV* __restrict__ vals, int64_t pitch, DiaOffsets o, BandPlan P, const float* __restrict__ r,
                    const float* __restrict__ Ap, float* __restrict__ rn, float* __restrict__ t, int32_t n,
                    int64_t npad, RedWork w, RuState* S, double* __restrict__ rz_cur, const double* __restrict__ pap)
 {
    if (band_block_flag(&S->halt)) return;
    extern __shared__ __align__(128) unsigned char smem[];
-   __shared__ __align__(8) uint64_t bars[2];
+   __shared__ __align__(8) uint64_t full[kBandStages], empty[kBandStages];
    const double rz = *rz_cur, tp = *pap;
    const bool okp = tp != 0.0 && isfinite(tp);
    const float alpha = okp ? (float)(rz / tp) : 0.0f;
    const float* const bin[2] = {r, Ap};
    const float* const oin[1] = {nullptr};
    double rr = 0, tt = 0;
-   const bool ok = band_loop<TV, D, 2, 0>(smem, bars, P, vals, pitch, bin, oin, n, npad,
+   const bool ok = band_loop<TV, D, 2, 0>(smem, full, empty, P, vals, pitch, bin, oin, n, npad,
                                           [&](int64_t i0, const unsigned char* st) {
-      const BandStage<TV> B{st, &P, i0};
-#pragma unroll 1
-      for (int q = 0; q < kBandRows; q++) {
-         const int rl = threadIdx.x + q * kBandThreads;
-         const int64_t i = i0 + rl;
-         if (i >= n) break;
-         float v[D], x[D];
+      const BandPtrs<TV, D, 2> B(st, P, o, i0, n);
+      auto rows = [&](auto check) {
+         constexpr bool C = decltype(check)::value;
 #pragma unroll
-         for (int j = 0; j < D; j++) {
-            const int64_t c = i + o.o[j];
-            const bool in = c >= 0 && c < n;
-            v[j] = in ? B.val(j, rl) : 0.0f;
-            x[j] = in ? ru_rnext(B.in(0, j, c), alpha, B.in(1, j, c)) : 0.0f;
+         for (int q = 0; q < kBandRows; q++) {
+            const int rl = q * kBandThreads;
+            const int64_t i = i0 + threadIdx.x + rl;
+            if (C && i >= n) break;
+            float v[D], x[D];
+#pragma unroll
+            for (int j = 0; j < D; j++) {
+               bool in = true;
+               if (C) {
+                  const int64_t c = i + o.o[j];
+                  in = c >= 0 && c < n;
+               }
+               v[j] = in ? rel_to_f(B.v[j * kBandT + rl]) : 0.0f;
+               x[j] = in ? ru_rnext(B.x[0][j][rl], alpha, B.x[1][j][rl]) : 0.0f;
+            }
+            float s = 0.0f;
+#pragma unroll
+            for (int j = 0; j < D; j++) s += v[j] * x[j];
+            const float rv = ru_rnext(B.self[0][rl], alpha, B.self[1][rl]);
+            rn[i] = rv;
+            t[i] = s;
+            rr += (double)rv * (double)rv;
+            tt += (double)s * (double)s;
          }
-         float s = 0.0f;
-#pragma unroll
-         for (int j = 0; j < D; j++) s += v[j] * x[j];
-         const float rv = ru_rnext(B.self(0, i), alpha, B.self(1, i));
-         rn[i] = rv;
-         t[i] = s;
-         rr += (double)rv * (double)rv;
-         tt += (double)s * (double)s;
-      }
+      };
+      if (B.interior)
+         rows(std::false_type{});
+      else
+         rows(std::true_type{});
    });
    if (!ok) rr = __longlong_as_double(0x7ff8000000000000ll);
    double v[2] = {rr, tt};
-   if (publish_and_arrive<2>(v, w)) {
+   if (band_publish<2>(v, w)) {
       double tot[2];
-      gather_totals<2>(tot, w);
+      band_totals<2>(tot, w);
       if (threadIdx.x == 0) {
          S->rz = rz;
          S->alpha = (double)alpha;
@@ -2496,41 +2506,51 @@ __global__ void __launch_bounds__(kBandThreads)
 // k_ru_gt_xpby on a diagonal copy of G^T: t staged by bands, the tile's own
 // p and xc by bulk copies.  A wait that gave up raises a breakdown.
 template <typename TV, int D>
-__global__ void __launch_bounds__(kBandThreads)
+__global__ void __launch_bounds__(kBandBlock)
    k_band_gt_xpby(const TV* __restrict__ vals, int64_t pitch, DiaOffsets o, BandPlan P, const float* __restrict__ t,
                   float* __restrict__ p, float* __restrict__ xc, int32_t n, int64_t npad,
                   const double* __restrict__ rz_cur, RuState* S)
 {
    if (band_block_flag(&S->halt)) return;
    extern __shared__ __align__(128) unsigned char smem[];
-   __shared__ __align__(8) uint64_t bars[2];
+   __shared__ __align__(8) uint64_t full[kBandStages], empty[kBandStages];
    const float beta = (float)(*rz_cur / S->rz);
    const float alpha = (float)S->alpha;
    const float* const bin[1] = {t};
    const float* const oin[2] = {p, xc};
-   const bool ok = band_loop<TV, D, 1, 2>(smem, bars, P, vals, pitch, bin, oin, n, npad,
+   const bool ok = band_loop<TV, D, 1, 2>(smem, full, empty, P, vals, pitch, bin, oin, n, npad,
                                           [&](int64_t i0, const unsigned char* st) {
-      const BandStage<TV> B{st, &P, i0};
-#pragma unroll 1
-      for (int q = 0; q < kBandRows; q++) {
-         const int rl = threadIdx.x + q * kBandThreads;
-         const int64_t i = i0 + rl;
-         if (i >= n) break;
-         float v[D], x[D];
+      const BandPtrs<TV, D, 1> B(st, P, o, i0, n);
+      auto rows = [&](auto check) {
+         constexpr bool C = decltype(check)::value;
 #pragma unroll
-         for (int j = 0; j < D; j++) {
-            const int64_t c = i + o.o[j];
-            const bool in = c >= 0 && c < n;
-            v[j] = in ? B.val(j, rl) : 0.0f;
-            x[j] = in ? B.in(0, j, c) : 0.0f;
+         for (int q = 0; q < kBandRows; q++) {
+            const int rl = q * kBandThreads;
+            const int64_t i = i0 + threadIdx.x + rl;
+            if (C && i >= n) break;
+            float v[D], x[D];
+#pragma unroll
+            for (int j = 0; j < D; j++) {
+               bool in = true;
+               if (C) {
+                  const int64_t c = i + o.o[j];
+                  in = c >= 0 && c < n;
+               }
+               v[j] = in ? rel_to_f(B.v[j * kBandT + rl]) : 0.0f;
+               x[j] = in ? B.x[0][j][rl] : 0.0f;
+            }
+            float s = 0.0f;
+#pragma unroll
+            for (int j = 0; j < D; j++) s += v[j] * x[j];
+            const float po = B.own[0][rl];
+            xc[i] = B.own[1][rl] + alpha * po;
+            p[i] = s + beta * po;
          }
-         float s = 0.0f;
-#pragma unroll
-         for (int j = 0; j < D; j++) s += v[j] * x[j];
-         const float po = B.own(0, rl);
-         xc[i] = B.own(1, rl) + alpha * po;
-         p[i] = s + beta * po;
-      }
+      };
+      if (B.interior)
+         rows(std::false_type{});
+      else
+         rows(std::true_type{});
    });
    if (!ok && threadIdx.x == 0) S->halt = 2;
 }
@@ -2544,11 +2564,11 @@ void launch_band_g_update(const CompactCopy& G, const float* r, const float* Ap,
    DiaOffsets o{};
    for (int j = 0; j < 8; j++) o.o[j] = G.diag[j];
    const int64_t npad = ((int64_t)n + 3) / 4 * 4;
-   const size_t smem = 2 * (size_t)P.bytes;
+   const size_t smem = (size_t)P.stages * P.bytes;
    TNLB_DIA_WIDTH(G.width, {
       auto* k = k_band_g_update<__half, D>;
       const unsigned grid = band_grid((const void*)k, smem, n, kRedMaxBlocks);
-      k<<<grid, kBandThreads, smem, st>>>(G.vals.as<__half>(), G.pitch, o, P, r, Ap, rn, t, n, npad, w, S, rz_cur,
+      k<<<grid, kBandBlock, smem, st>>>(G.vals.as<__half>(), G.pitch, o, P, r, Ap, rn, t, n, npad, w, S, rz_cur,
                                            pap);
    });
 }
@@ -2560,11 +2580,11 @@ void launch_band_gt_xpby(const CompactCopy& GT, const float* t, float* p, float*
    DiaOffsets o{};
    for (int j = 0; j < 8; j++) o.o[j] = GT.diag[j];
    const int64_t npad = ((int64_t)n + 3) / 4 * 4;
-   const size_t smem = 2 * (size_t)P.bytes;
+   const size_t smem = (size_t)P.stages * P.bytes;
    TNLB_DIA_WIDTH(GT.width, {
       auto* k = k_band_gt_xpby<__half, D>;
       const unsigned grid = band_grid((const void*)k, smem, n, kRedMaxBlocks);
-      k<<<grid, kBandThreads, smem, st>>>(GT.vals.as<__half>(), GT.pitch, o, P, t, p, xc, n, npad, rz_cur, S);
+      k<<<grid, kBandBlock, smem, st>>>(GT.vals.as<__half>(), GT.pitch, o, P, t, p, xc, n, npad, rz_cur, S);
    });
 }
 
@@ -2753,9 +2773,16 @@ tnlb_status reliable_t(const tnlb_segments* seg, const int32_t* cols, const doub
    }
    const bool cmp_a = cA.kind != CompactCopy::kNone;
    const bool cmp_m = cG.kind != CompactCopy::kNone && cGT.kind != CompactCopy::kNone;
-   // diagonal copies whose products stage their operands by bulk copies
-   const bool band_a = prm.reliable_layout == 0 && cmp_a && compact_band_capable(cA);
-   const bool band_m = prm.reliable_layout == 0 && cmp_m && compact_band_capable(cG) && compact_band_capable(cGT);
+   // diagonal copies of more than 5 diagonals stage their products'
+   // operands by bulk copies (band.cuh); up to 5 diagonals the four-row
+   // register form (DiaRows) measured as fast or faster (2048^2 5-point
+   // operator: Jacobi iteration 63.6 against 64.7 us, 3-diagonal FSAI
+   // 84.1 against 87.4 us; 7-diagonal FSAI 93.7 against 142.6 us)
+   auto banded = [&](const CompactCopy& C) {
+      return prm.reliable_layout == 0 && C.kind == CompactCopy::kDia && C.width > 5 && compact_band_capable(C);
+   };
+   const bool band_a = cmp_a && banded(cA);
+   const bool band_g = cmp_m && banded(cG), band_gt = cmp_m && banded(cGT);
    // with the compact FSAI copies the update of xc and r goes into the two
    // factor products (k_ru_g_update, k_ru_gt_xpby); the new residual goes
    // to the other of two buffers, iteration by iteration, and t = G r to a
@@ -2812,19 +2839,18 @@ tnlb_status reliable_t(const tnlb_segments* seg, const int32_t* cols, const doub
          // even iterations r -> r2, odd ones r2 -> r: a batch (even) ends in r
          const float* rin = (const float*)(k & 1 ? r2.ptr : r.ptr);
          float* rout = (float*)(k & 1 ? r.ptr : r2.ptr);
-         if (band_m) {
+         if (band_g)
             launch_band_g_update(cG, rin, (const float*)Ap.ptr, rout, tvec, (int32_t)n, W.red(), S, rz_cur, pap, s);
-            TNLB_CHECK_LAUNCH();
-            launch_band_gt_xpby(cGT, tvec, (float*)p.ptr, (float*)xc.ptr, (int32_t)n, rz_cur, S, s);
-            TNLB_CHECK_LAUNCH();
-            return TNLB_OK;
-         }
-         TNLB_COMPACT_ROWS(cG, __half,
-                           launch_ru_g_update(rows_, rin, (const float*)Ap.ptr, rout, tvec, (int32_t)n, W.red(), S,
-                                              rz_cur, pap, s));
+         else
+            TNLB_COMPACT_ROWS(cG, __half,
+                              launch_ru_g_update(rows_, rin, (const float*)Ap.ptr, rout, tvec, (int32_t)n, W.red(), S,
+                                                 rz_cur, pap, s));
          TNLB_CHECK_LAUNCH();
-         TNLB_COMPACT_ROWS(cGT, __half,
-                           launch_ru_gt_xpby(rows_, tvec, (float*)p.ptr, (float*)xc.ptr, (int32_t)n, rz_cur, S, s));
+         if (band_gt)
+            launch_band_gt_xpby(cGT, tvec, (float*)p.ptr, (float*)xc.ptr, (int32_t)n, rz_cur, S, s);
+         else
+            TNLB_COMPACT_ROWS(cGT, __half,
+                              launch_ru_gt_xpby(rows_, tvec, (float*)p.ptr, (float*)xc.ptr, (int32_t)n, rz_cur, S, s));
          TNLB_CHECK_LAUNCH();
          return TNLB_OK;
       }
