@@ -219,9 +219,9 @@ def solver_leg():
     """PCG time to an FP64 true residual ||b - A x|| / ||b|| <= 1e-8 on one
     B200 (CUDA events around each call on the launching stream), every
     method warmed up by one 20-iteration run first:
-      * FP64 Jacobi-PCG, its convergence residue halved until the TRUE
+      * FP64 Jacobi-PCG, its convergence residue lowered until the TRUE
         residual is below 1e-8 (the reference's rule stops on the
-        preconditioned residue);
+        preconditioned residue; each retry scales it by the gap seen);
       * FP32 PCG with reliable FP64 updates and the learned FSAI (network
         inference on the GPU = set-up), and the same with classical FSAI;
     plus each solution's error against a tightly converged FP64 solve."""
@@ -273,9 +273,12 @@ def solver_leg():
         S = pcg(Pj, tol)
         x = zeros()
         S.solve(b, x)
-        if t.true_residual(M, b, x) < SOLVER_TOL or tol < 1e-12:
+        tr = t.true_residual(M, b, x)
+        if tr < SOLVER_TOL or tol < 1e-13:
             break
-        tol *= 0.5
+        # the stopping residue and the true residual differ by a factor
+        # the next run's tolerance corrects
+        tol *= 0.5 * SOLVER_TOL / tr
     x = zeros()
     ok, ms = timed(lambda: S.solve(b, x))
     fp64 = {"method": "FP64 Jacobi-PCG", "solve_ms": ms, "setup_ms": jac_setup, "iterations": S.getIterations(),

@@ -1866,7 +1866,8 @@ done:
 /* Mixed-precision PCG with reliable updates -- the library's own solver
  * (no counterpart in the reference), restated for its tests: CG on FP32
  * values with vectors of type VT (float or double; rows summed in VT, dot
- * products in FP64); the correction xc is folded into the FP64 x and r
+ * products in FP64); the correction xc (FP64: the exact product of the VT
+ * alpha and p added in FP64) is folded into the FP64 x and r
  * replaced by (VT)(b - A x) (FP64 product) whenever the recursive |r|^2
  * falls below max(delta |r_u|, tol |b|)^2, r_u the residual of the last
  * update; p is kept, beta = (r, z)_new / (r, z)_old.  precond: 0 none,
@@ -1901,7 +1902,7 @@ typedef struct {
       float* d = (float*)malloc(sizeof(float) * (size_t)n);                                                       \
       VT *r = (VT*)malloc(sizeof(VT) * (size_t)n), *z = (VT*)malloc(sizeof(VT) * (size_t)n);                      \
       VT *p = (VT*)calloc((size_t)n, sizeof(VT)), *Ap = (VT*)malloc(sizeof(VT) * (size_t)n);                      \
-      VT* xc = (VT*)calloc((size_t)n, sizeof(VT));                                                                \
+      double* xc = (double*)calloc((size_t)n, sizeof(double)); /* the correction is FP64 */                      \
       VT* t = (VT*)malloc(sizeof(VT) * (size_t)(n > 0 ? n : 1));                                                  \
       double* xbest = (double*)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));                                  \
       double lowest = HUGE_VAL;                                                                                   \
@@ -1926,8 +1927,8 @@ typedef struct {
       int32_t it = 0, upd = 0, halt = 1, ok = 0, force_at = 0, it_best = 0;                                       \
       for (;;) {                                                                                                  \
          for (int32_t i = 0; i < n; i++) {                                                                        \
-            x[i] += (double)xc[i];                                                                                \
-            xc[i] = (VT)0;                                                                                        \
+            x[i] += xc[i];                                                                                        \
+            xc[i] = 0.0;                                                                                          \
          }                                                                                                        \
          double rn2 = 0.0, bn2 = 0.0;                                                                             \
          for (int32_t i = 0; i < n; i++) {                                                                        \
@@ -2007,7 +2008,7 @@ typedef struct {
             const VT alpha = (VT)(rz / pap);                                                                      \
             double rr = 0.0, rzn = 0.0;                                                                           \
             for (int32_t i = 0; i < n; i++) {                                                                     \
-               xc[i] = FMA(alpha, p[i], xc[i]);                                                                   \
+               xc[i] += (double)alpha * (double)p[i];                                                             \
                r[i] = FMA(-alpha, Ap[i], r[i]);                                                                    \
                rr += (double)r[i] * (double)r[i];                                                                 \
                if (precond != 2) {                                                                                \

@@ -56,6 +56,8 @@ def _matrix(config: str):
         return g.laplacian_2d(1024)
     if config == "power_law":
         return g.power_law(4_194_304, 1.73, 4096, 2)
+    if config == "power_law_15":  # the literal Zipf 1.5 of the power-law config: mean ~49, ~2.06e8 nonzeros
+        return g.power_law(4_194_304, 1.5, 4096, 2)
     if config == "diffusion3d":
         return g.diffusion_3d(256)
     raise ValueError(config)
@@ -416,6 +418,15 @@ def bench_configs(which: str, out=sys.stdout):
                                                                               inner="jacobi"), n), reps=3)
         report("FP32 Jacobi-PCG with reliable FP64 updates", r["converged"], r["iterations"], ms, 0.0, x,
                reliable_updates=r["reliable_updates"], solve_ms_runs=times)
+        # the same with the 7-diagonal copy of A read by ordinary loads
+        # instead of the bulk-copy-staged product
+        t.solve_mixed_reliable(M, b, torch.zeros(n, dtype=torch.float64, device="cuda"), tol=tol, inner="jacobi",
+                               max_iterations=20, layout="diagonal")
+        r, x, ms, times = _median_timed(_Run(lambda x: t.solve_mixed_reliable(M, b, x, tol=tol, delta=0.3,
+                                                                              inner="jacobi", layout="diagonal"), n),
+                                        reps=3)
+        report("FP32 Jacobi-PCG with reliable FP64 updates, diagonal copy read by ordinary loads", r["converged"],
+               r["iterations"], ms, 0.0, x, reliable_updates=r["reliable_updates"], solve_ms_runs=times)
         return
     P = t.ILU0()
     _, s_ilu = _timed(lambda: P.update(M))
@@ -507,8 +518,8 @@ def bench_learned_eval(count: int, N: int, weights: str, ilu_count: int = 4, fir
     problems (seeds first_seed.., GRF correlation length ~ U[0.02, 0.2],
     sigma ~ U[1, 3]) on N x N grids, each solved to an FP64 true residual of
     1e-8 by
-      * FP64 Jacobi-PCG (convergence residue halved until the true residual
-        is below 1e-8) -- the baseline,
+      * FP64 Jacobi-PCG (convergence residue lowered until the true
+        residual is below 1e-8) -- the baseline,
       * FP32 PCG with reliable FP64 updates and the learned FSAI (network
         inference = set-up time), the classical FSAI of A's pattern, and the
         classical FSAI of the level-1 pattern,
@@ -547,9 +558,10 @@ def bench_learned_eval(count: int, N: int, weights: str, ilu_count: int = 4, fir
             S.setMaxIterations(200000)
             x = zeros()
             ok, ms = _timed(lambda: S.solve(b, x))
-            if t.true_residual(M, b, x) < 1e-8 or tol < 1e-12:
+            tr = t.true_residual(M, b, x)
+            if tr < 1e-8 or tol < 1e-13:
                 break
-            tol *= 0.5
+            tol *= 0.5 * 1e-8 / tr  # the next run's stopping residue scaled by the gap seen
         rec["fp64_jacobi"] = {"iterations": S.getIterations(), "solve_ms": ms, "converged": bool(ok),
                               "true_residual": t.true_residual(M, b, x)}
 
@@ -558,7 +570,8 @@ def bench_learned_eval(count: int, N: int, weights: str, ilu_count: int = 4, fir
             t.solve_mixed_reliable(M, b, zeros(), tol=1e-8, inner=Pm, max_iterations=20)
             x = zeros()
             r, ms = _timed(lambda: t.solve_mixed_reliable(M, b, x, tol=1e-8, delta=0.3, inner=Pm))
-            rec[key] = {"iterations": r["iterations"], "solve_ms": ms, "setup_ms": setup,
+            rec[key] = {"iterations": r["iterations"], "fallback_iterations": r["fallback_iterations"],
+                        "solve_ms": ms, "setup_ms": setup,
                         "converged": bool(r["converged"]), "true_residual": t.true_residual(M, b, x),
                         "speedup_vs_fp64_jacobi": rec["fp64_jacobi"]["solve_ms"] / ms,
                         "speedup_with_setup": rec["fp64_jacobi"]["solve_ms"] / (ms + setup)}
@@ -605,6 +618,8 @@ def bench_learned_eval(count: int, N: int, weights: str, ilu_count: int = 4, fir
         if key.startswith("fp32"):
             sp = [r[key]["speedup_with_setup"] for r in rows]
             ent["speedup_with_setup_vs_fp64_jacobi"] = [float(np.min(sp)), float(np.median(sp)), float(np.max(sp))]
+            ent["share_at_least_2x_with_setup"] = float(np.mean([v >= 2.0 for v in sp]))
+            ent["fallbacks"] = int(sum(r[key]["fallback_iterations"] > 0 for r in rows))
             ent["setup_ms_median"] = float(np.median([r[key]["setup_ms"] for r in rows]))
         summary[key] = ent
     summary["learned_vs_fsai_level0_iterations_median"] = float(np.median(

@@ -2200,12 +2200,17 @@ __device__ __forceinline__ void st4(double* p, const double (&v)[4])
    *reinterpret_cast<double2*>(p + 2) = make_double2(v[2], v[3]);
 }
 
-// One entry of k_ru_update.
+// One entry of k_ru_update.  The correction xc is FP64 for either vector
+// type: summed in FP32, the small late steps of a long run between updates
+// lose their low bits, and on high-contrast matrices that cost up to 1.7x
+// the iterations (an emulation of the iteration on a 512^2 GRF problem:
+// 10473 against 6258 with xc in FP64, 5785 all in FP64).  The product of
+// the FP32 alpha and p is exact in FP64.
 template <typename VT>
-__device__ __forceinline__ void ru_entry(VT alpha, VT& xc, VT& r, VT p, VT ap, float d, VT& z, int mode, double& rr,
-                                         double& rzn)
+__device__ __forceinline__ void ru_entry(VT alpha, double& xc, VT& r, VT p, VT ap, float d, VT& z, int mode,
+                                         double& rr, double& rzn)
 {
-   xc += alpha * p;
+   xc += (double)alpha * (double)p;
    r = r - alpha * ap;
    rr += (double)r * (double)r;
    if (mode == 1) {
@@ -2215,7 +2220,7 @@ __device__ __forceinline__ void ru_entry(VT alpha, VT& xc, VT& r, VT p, VT ap, f
 }
 
 template <typename VT>
-__global__ void __launch_bounds__(kRedThreads) k_ru_update(int64_t n, VT* __restrict__ xc, VT* __restrict__ r,
+__global__ void __launch_bounds__(kRedThreads) k_ru_update(int64_t n, double* __restrict__ xc, VT* __restrict__ r,
                                                            const VT* __restrict__ p, const VT* __restrict__ Ap,
                                                            const float* __restrict__ d, VT* __restrict__ z, int mode,
                                                            RedWork w, RuState* S, double* __restrict__ rz_cur,
@@ -2230,7 +2235,8 @@ __global__ void __launch_bounds__(kRedThreads) k_ru_update(int64_t n, VT* __rest
    // four entries per thread and pass (16-byte loads), then the tail
    for (int64_t q = tid; q < n / 4; q += stride) {
       const int64_t i = 4 * q;
-      VT xv[4], rv[4], pv[4], av[4], zv[4];
+      double xv[4];
+      VT rv[4], pv[4], av[4], zv[4];
       float dv[4] = {1.0f, 1.0f, 1.0f, 1.0f};
       ld4(xc + i, xv);
       ld4(r + i, rv);
@@ -2244,7 +2250,8 @@ __global__ void __launch_bounds__(kRedThreads) k_ru_update(int64_t n, VT* __rest
       if (mode == 1) st4(z + i, zv);
    }
    for (int64_t i = 4 * (n / 4) + tid; i < n; i += stride) {
-      VT xv = xc[i], rv = r[i], zv = VT(0);
+      double xv = xc[i];
+      VT rv = r[i], zv = VT(0);
       ru_entry(alpha, xv, rv, p[i], Ap[i], mode == 1 ? d[i] : 1.0f, zv, mode, rr, rzn);
       xc[i] = xv;
       r[i] = rv;
@@ -2369,7 +2376,7 @@ __global__ void __launch_bounds__(kRedThreads, Rows::kMinBlocks)
 // G^T, and xc += alpha p with the p that alpha was formed for.
 template <typename Rows>
 __global__ void __launch_bounds__(kRedThreads, Rows::kMinBlocks)
-   k_ru_gt_xpby(Rows GT, const float* __restrict__ t, float* __restrict__ p, float* __restrict__ xc, int32_t n,
+   k_ru_gt_xpby(Rows GT, const float* __restrict__ t, float* __restrict__ p, double* __restrict__ xc, int32_t n,
                 const double* __restrict__ rz_cur, const RuState* S)
 {
    if (S->halt) return;
@@ -2384,14 +2391,14 @@ __global__ void __launch_bounds__(kRedThreads, Rows::kMinBlocks)
       if constexpr (Rows::kQuad) {
          if (base + 3 < n) {
             float4* pp = reinterpret_cast<float4*>(p + base);
-            float4* xp = reinterpret_cast<float4*>(xc + base);
             const float4 po = *pp;
-            float4 xo = *xp;
-            xo.x += alpha * po.x;
-            xo.y += alpha * po.y;
-            xo.z += alpha * po.z;
-            xo.w += alpha * po.w;
-            *xp = xo;
+            double xo[4];
+            ld4(xc + base, xo);
+            xo[0] += (double)alpha * (double)po.x;
+            xo[1] += (double)alpha * (double)po.y;
+            xo[2] += (double)alpha * (double)po.z;
+            xo[3] += (double)alpha * (double)po.w;
+            st4(xc + base, xo);
             *pp = make_float4(s[0] + beta * po.x, s[1] + beta * po.y, s[2] + beta * po.z, s[3] + beta * po.w);
             continue;
          }
@@ -2401,7 +2408,7 @@ __global__ void __launch_bounds__(kRedThreads, Rows::kMinBlocks)
          const int64_t i = GT.row(base, k);
          if (i < n) {
             const float po = p[i];
-            xc[i] += alpha * po;
+            xc[i] += (double)alpha * (double)po;
             p[i] = s[k] + beta * po;
          }
       }
@@ -2418,7 +2425,7 @@ void launch_ru_g_update(const Rows& G, const float* r, const float* Ap, float* r
 }
 
 template <typename Rows>
-void launch_ru_gt_xpby(const Rows& GT, const float* t, float* p, float* xc, int32_t n, const double* rz_cur,
+void launch_ru_gt_xpby(const Rows& GT, const float* t, float* p, double* xc, int32_t n, const double* rz_cur,
                        const RuState* S, cudaStream_t st)
 {
    auto* k = k_ru_gt_xpby<Rows>;
@@ -2504,11 +2511,12 @@ __global__ void __launch_bounds__(kBandBlock)
 }
 
 // k_ru_gt_xpby on a diagonal copy of G^T: t staged by bands, the tile's own
-// p and xc by bulk copies.  A wait that gave up raises a breakdown.
+// p by a bulk copy, the FP64 xc read and written in place.  A wait that
+// gave up raises a breakdown.
 template <typename TV, int D>
 __global__ void __launch_bounds__(kBandBlock)
    k_band_gt_xpby(const TV* __restrict__ vals, int64_t pitch, DiaOffsets o, BandPlan P, const float* __restrict__ t,
-                  float* __restrict__ p, float* __restrict__ xc, int32_t n, int64_t npad,
+                  float* __restrict__ p, double* __restrict__ xc, int32_t n, int64_t npad,
                   const double* __restrict__ rz_cur, RuState* S)
 {
    if (band_block_flag(&S->halt)) return;
@@ -2517,8 +2525,8 @@ __global__ void __launch_bounds__(kBandBlock)
    const float beta = (float)(*rz_cur / S->rz);
    const float alpha = (float)S->alpha;
    const float* const bin[1] = {t};
-   const float* const oin[2] = {p, xc};
-   const bool ok = band_loop<TV, D, 1, 2>(smem, full, empty, P, vals, pitch, bin, oin, n, npad,
+   const float* const oin[1] = {p};
+   const bool ok = band_loop<TV, D, 1, 1>(smem, full, empty, P, vals, pitch, bin, oin, n, npad,
                                           [&](int64_t i0, const unsigned char* st) {
       const BandPtrs<TV, D, 1> B(st, P, o, i0, n);
       auto rows = [&](auto check) {
@@ -2543,7 +2551,7 @@ __global__ void __launch_bounds__(kBandBlock)
 #pragma unroll
             for (int j = 0; j < D; j++) s += v[j] * x[j];
             const float po = B.own[0][rl];
-            xc[i] = B.own[1][rl] + alpha * po;
+            xc[i] += (double)alpha * (double)po;
             p[i] = s + beta * po;
          }
       };
@@ -2573,10 +2581,10 @@ void launch_band_g_update(const CompactCopy& G, const float* r, const float* Ap,
    });
 }
 
-void launch_band_gt_xpby(const CompactCopy& GT, const float* t, float* p, float* xc, int32_t n, const double* rz_cur,
+void launch_band_gt_xpby(const CompactCopy& GT, const float* t, float* p, double* xc, int32_t n, const double* rz_cur,
                          RuState* S, cudaStream_t st)
 {
-   const BandPlan P = band_plan(GT.diag, GT.width, (int)sizeof(__half), 1, 2);
+   const BandPlan P = band_plan(GT.diag, GT.width, (int)sizeof(__half), 1, 1);
    DiaOffsets o{};
    for (int j = 0; j < 8; j++) o.o[j] = GT.diag[j];
    const int64_t npad = ((int64_t)n + 3) / 4 * 4;
@@ -2591,15 +2599,15 @@ void launch_band_gt_xpby(const CompactCopy& GT, const float* t, float* p, float*
 // x += xc + alpha p, the step k_ru_gt_xpby skips when the iteration that
 // formed alpha raised `halt` (alpha is 0 before the first iteration); xc = 0.
 template <typename VT>
-__global__ void k_ru_fold_p(int64_t n, VT* __restrict__ xc, const VT* __restrict__ p, const RuState* S,
+__global__ void k_ru_fold_p(int64_t n, double* __restrict__ xc, const VT* __restrict__ p, const RuState* S,
                             double* __restrict__ x)
 {
    const VT alpha = (VT)S->alpha;
    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-      VT xv = xc[i];
-      xv += alpha * p[i];
-      x[i] += (double)xv;
-      xc[i] = VT(0);
+      double xv = xc[i];
+      xv += (double)alpha * (double)p[i];
+      x[i] += xv;
+      xc[i] = 0.0;
    }
 }
 
@@ -2643,13 +2651,12 @@ __global__ void k_ru_p(int64_t n, VT* __restrict__ p, const VT* __restrict__ z, 
    for (int64_t i = 4 * (n / 4) + tid; i < n; i += stride) p[i] = z[i] + beta * p[i];
 }
 
-// x += xc (FP64); xc = 0.
-template <typename VT>
-__global__ void k_ru_fold(int64_t n, VT* __restrict__ xc, double* __restrict__ x)
+// x += xc; xc = 0.
+__global__ void k_ru_fold(int64_t n, double* __restrict__ xc, double* __restrict__ x)
 {
    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-      x[i] += (double)xc[i];
-      xc[i] = VT(0);
+      x[i] += xc[i];
+      xc[i] = 0.0;
    }
 }
 
@@ -2705,7 +2712,7 @@ tnlb_status reliable_t(const tnlb_segments* seg, const int32_t* cols, const doub
    TNLB_TRY_STATUS(z.alloc(sizeof(VT) * npad));
    TNLB_TRY_STATUS(p.alloc(sizeof(VT) * npad));
    TNLB_TRY_STATUS(Ap.alloc(sizeof(VT) * npad));
-   TNLB_TRY_STATUS(xc.alloc(sizeof(VT) * npad));
+   TNLB_TRY_STATUS(xc.alloc(sizeof(double) * npad));  // the correction is FP64 (ru_entry)
    TNLB_TRY_STATUS(scal.alloc(sizeof(double) * 4));  // [0] (p, Ap), [1] (r, z), [2..3] residual sums
    k_convert<float, double><<<grid_for(seg->storage, 256 * 8), 256, 0, st>>>(seg->storage, vals, v32.as<float>());
    TNLB_CHECK_LAUNCH();
@@ -2847,14 +2854,14 @@ tnlb_status reliable_t(const tnlb_segments* seg, const int32_t* cols, const doub
                                                  rz_cur, pap, s));
          TNLB_CHECK_LAUNCH();
          if (band_gt)
-            launch_band_gt_xpby(cGT, tvec, (float*)p.ptr, (float*)xc.ptr, (int32_t)n, rz_cur, S, s);
+            launch_band_gt_xpby(cGT, tvec, (float*)p.ptr, xc.as<double>(), (int32_t)n, rz_cur, S, s);
          else
             TNLB_COMPACT_ROWS(cGT, __half,
-                              launch_ru_gt_xpby(rows_, tvec, (float*)p.ptr, (float*)xc.ptr, (int32_t)n, rz_cur, S, s));
+                              launch_ru_gt_xpby(rows_, tvec, (float*)p.ptr, xc.as<double>(), (int32_t)n, rz_cur, S, s));
          TNLB_CHECK_LAUNCH();
          return TNLB_OK;
       }
-      k_ru_update<VT><<<Gu, kRedThreads, 0, s>>>(n, xc.as<VT>(), r.as<VT>(), p.as<VT>(), Ap.as<VT>(), d, z.as<VT>(),
+      k_ru_update<VT><<<Gu, kRedThreads, 0, s>>>(n, xc.as<double>(), r.as<VT>(), p.as<VT>(), Ap.as<VT>(), d, z.as<VT>(),
                                                  mode, W.red(), S, rz_cur, pap);
       TNLB_CHECK_LAUNCH();
       return precondition(s, halt);
@@ -2867,7 +2874,7 @@ tnlb_status reliable_t(const tnlb_segments* seg, const int32_t* cols, const doub
    s0.halt = 1;
    TNLB_CUDA_TRY(cudaMemcpyAsync(S, &s0, sizeof(s0), cudaMemcpyHostToDevice, st));
    TNLB_CUDA_TRY(cudaMemsetAsync(p.ptr, 0, sizeof(VT) * n, st));
-   TNLB_CUDA_TRY(cudaMemsetAsync(xc.ptr, 0, sizeof(VT) * n, st));
+   TNLB_CUDA_TRY(cudaMemsetAsync(xc.ptr, 0, sizeof(double) * n, st));
 
    // CUDA graph of a batch of iterations, captured once on a side stream
    const int kBatch = n < (1 << 22) ? 32 : 16;
@@ -2958,9 +2965,9 @@ tnlb_status reliable_t(const tnlb_segments* seg, const int32_t* cols, const doub
    for (;;) {
       // reliable update: x += xc, r = b - A x in FP64, r = (VT) r
       if (fused_u)
-         k_ru_fold_p<VT><<<G, kRedThreads, 0, cs>>>(n, xc.as<VT>(), p.as<VT>(), S, x);
+         k_ru_fold_p<VT><<<G, kRedThreads, 0, cs>>>(n, xc.as<double>(), p.as<VT>(), S, x);
       else
-         k_ru_fold<VT><<<G, kRedThreads, 0, cs>>>(n, xc.as<VT>(), x);
+         k_ru_fold<<<G, kRedThreads, 0, cs>>>(n, xc.as<double>(), x);
       TNLB_CHECK_LAUNCH();
       TNLB_TRY_STATUS(spmv_dispatch(seg, TNLB_F64, cols, vals, x, ax.ptr, 1.0, 0.0, cs));
       k_ru_resid<VT><<<G, kRedThreads, 0, cs>>>(n, b, ax.as<double>(), r.as<VT>(), W.red(), rsum);
