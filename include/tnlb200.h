@@ -455,10 +455,11 @@ typedef struct {
    int32_t idr_s;                /* idr-s (IDR(s) shadow space), default 4 */
    int32_t idr_residual_smoothing; /* idr-residual-smoothing, default 0 */
    int32_t reliable_layout;      /* tnlb_solve_mixed_reliable's internal FP32 copies: 0 (default) the
-                                    diagonal layout where the matrix fits it, its products staged in
-                                    shared memory by bulk copies, else CSR with 16-bit column offsets;
-                                    1 the 16-bit offsets only; 2 the diagonal layout read by ordinary
-                                    loads.  All give the same row sums bit for bit */
+                                    diagonal layout where the matrix fits it (the products of FSAI
+                                    factors of more than 5 diagonals staged in shared memory by bulk
+                                    copies), else CSR with 16-bit column offsets; 1 the 16-bit offsets
+                                    only; 2 the diagonal layout read by ordinary loads throughout.
+                                    All give the same row sums bit for bit */
    int32_t reliable_operator;    /* its FP32 copy of A: 0 (default) the row-excess form (each diagonal
                                     entry holds the row's FP64 sum; rows summed as
                                     s_i x_i + sum a_ij (x_j - x_i)) when every row has its diagonal

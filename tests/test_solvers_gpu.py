@@ -241,11 +241,11 @@ def test_reliable_layouts_give_the_same_iterates(inner, dim):
     """The reliable-update PCG's internal FP32 copies by diagonal (2D: 5 for
     A, 3 for the FSAI factors, 7 for those of the level-1 pattern; 3D: 7
     for A, 4 for the factors, whose level-1 form -- 13 entries a row --
-    takes 16-bit offsets), with their products staged by bulk copies beyond
-    5 diagonals ("auto") or read by ordinary loads ("diagonal": four rows
-    per thread up to 5 diagonals, one row beyond), and with 16-bit column
-    offsets sum the same terms in the same order: on these sizes
-    iterations, updates and x agree bit for bit."""
+    takes 16-bit offsets), with the products of factors beyond 5 diagonals
+    staged by bulk copies ("auto") or read by ordinary loads ("diagonal":
+    four rows per thread up to 5 diagonals, one row beyond), and with
+    16-bit column offsets sum the same terms in the same order: on these
+    sizes iterations, updates and x agree bit for bit."""
     from tnl_b200 import generators as g
 
     t = tnl()
@@ -356,10 +356,14 @@ def test_reliable_mixed_pcg_falls_back_to_fp64(oracle, inner, vec64):
 @pytest.mark.parametrize("inner", ["jacobi", "fsai"])
 def test_reliable_row_excess_form(oracle, inner):
     """The row-excess form of the FP32 copy of A (the default) against the
-    plain form on a high-contrast diffusion matrix (sigma = 3): each within
-    5 % of the iterations of its oracle restatement, the excess form with
-    fewer; the three layouts (bulk-copy-staged diagonals, diagonals read by
-    ordinary loads, 16-bit offsets) give the same iterates bit for bit."""
+    plain form on a high-contrast diffusion matrix (sigma = 3), the excess
+    form with fewer iterations; the three layouts (bulk-copy-staged
+    diagonals, diagonals read by ordinary loads, 16-bit offsets) give the
+    same iterates bit for bit.  On this matrix the iteration count moves
+    with rounding: the oracle restatement itself, given b perturbed by
+    1e-15 relative, takes 1755 or 2143 iterations in the excess form and
+    2856-3092 in the plain one, so the GPU count must lie within that
+    spread (five perturbations, 5 % slack)."""
     from tnl_b200 import generators as g
 
     t = tnl()
@@ -377,11 +381,17 @@ def test_reliable_row_excess_form(oracle, inner):
         G = (G[0], G[1], G[2].astype(np.float16).astype(np.float32))
         GT = (GT[0], GT[1], GT[2].astype(np.float16).astype(np.float32))
     its = {}
+    rng = np.random.default_rng(0)
+    perturbed = [b] + [b * (1 + 1e-15 * rng.standard_normal(b.size)) for _ in range(4)]
     for op in ("excess", "plain"):
-        if inner == "fsai":
-            o = oracle.pcg_reliable_fsai(A, b, G, GT, tol=1e-8, delta=0.3, maxit=200000, excess=op == "excess")
-        else:
-            o = oracle.pcg_reliable(A, b, precond=1, tol=1e-8, delta=0.3, maxit=200000, excess=op == "excess")
+        spread = []
+        for bp in perturbed:
+            if inner == "fsai":
+                o = oracle.pcg_reliable_fsai(A, bp, G, GT, tol=1e-8, delta=0.3, maxit=200000, excess=op == "excess")
+            else:
+                o = oracle.pcg_reliable(A, bp, precond=1, tol=1e-8, delta=0.3, maxit=200000, excess=op == "excess")
+            assert o["converged"]
+            spread.append(o["iterations"])
         runs = []
         for layout in ("auto", "diagonal", "offsets"):
             xs = torch.zeros(A.n, dtype=torch.float64, device="cuda")
@@ -390,7 +400,7 @@ def test_reliable_row_excess_form(oracle, inner):
             assert r["converged"] and not r["stalled"], (op, layout, r)
             runs.append((r["iterations"], xs))
         assert all(k == runs[0][0] and torch.equal(x, runs[0][1]) for k, x in runs), (op, [k for k, _ in runs])
-        assert o["converged"] and abs(runs[0][0] - o["iterations"]) <= 0.05 * o["iterations"], (op, runs[0][0], o)
+        assert 0.95 * min(spread) <= runs[0][0] <= 1.05 * max(spread), (op, runs[0][0], spread)
         its[op] = runs[0][0]
     assert its["excess"] < its["plain"], its
 

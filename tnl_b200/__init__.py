@@ -837,11 +837,12 @@ def solve_mixed_reliable(M: SparseMatrix, b: torch.Tensor, x: torch.Tensor, tol:
     learned FSAI).  Stops on the true FP64 residual ``tol``.
 
     ``layout`` picks the internal FP32 copies of short-row matrices: "auto"
-    stores a matrix with few diagonals by diagonal, its products staging
-    their operands in shared memory by bulk copies, others as CSR with
-    16-bit column offsets; "offsets" always the latter; "diagonal" the
-    diagonal copies read by ordinary loads.  All give the same row sums bit
-    for bit (their FP64 dot products group rows differently).
+    stores a matrix with few diagonals by diagonal (the products of FSAI
+    factors of more than 5 diagonals staging their operands in shared
+    memory by bulk copies), others as CSR with 16-bit column offsets;
+    "offsets" always the latter; "diagonal" the diagonal copies read by
+    ordinary loads throughout.  All give the same row sums bit for bit
+    (their FP64 dot products group rows differently).
 
     ``operator`` "excess" stores, in the FP32 copy of A, each row's FP64
     sum in place of its diagonal entry and sums a row as

@@ -1,6 +1,8 @@
 // band.cuh -- products on a diagonal (DIA) copy with every operand staged in
 // shared memory by bulk copies (cp.async.bulk, the TMA's one-dimensional
-// form; no multicast), for the FP32 iterations of the reliable-update PCG.
+// form; no multicast), for the FP32 iterations of the reliable-update PCG:
+// the two FSAI factor products of an iteration when the factors have more
+// than 5 diagonals (the level-1 pattern of a 5-point operator has 7).
 //
 // The diagonal kernels of compact.cuh read each row's D values and gather
 // D inputs with ordinary loads.  Profiled on the 2048^2 5-point operator
@@ -62,7 +64,7 @@ constexpr long kBandSpin = 1L << 24;  // mbarrier polls before a wait gives up
 struct BandPlan {
    int32_t D = 0, nb = 0;
    int32_t lo[8] = {}, hi[8] = {};
-   uint32_t vals = 0, band[2][8] = {}, own[2] = {}, bytes = 0;
+   uint32_t vals = 0, band[2][8] = {}, own[2] = {}, ownd[1] = {}, bytes = 0;
    int32_t dlo[8] = {};        // lo of diagonal j's band
    uint32_t dband[2][8] = {};  // its run for input k
    int32_t zlo = 0;            // the band of offset 0
@@ -77,8 +79,9 @@ struct BandPlan {
 };
 
 // The plan for ascending offsets o[0..D-1] (D <= 8), values of vbytes
-// bytes, KB banded input vectors and KO own-row vectors (KB, KO <= 2).
-inline BandPlan band_plan(const int32_t* o, int D, int vbytes, int KB, int KO)
+// bytes, KB banded input vectors, KO own-row FP32 vectors and KD own-row
+// FP64 vectors (KB, KO <= 2, KD <= 1).
+inline BandPlan band_plan(const int32_t* o, int D, int vbytes, int KB, int KO, int KD = 0)
 {
    BandPlan P;
    P.D = D;
@@ -104,6 +107,10 @@ inline BandPlan band_plan(const int32_t* o, int D, int vbytes, int KB, int KO)
    for (int k = 0; k < KO; k++) {
       P.own[k] = off;
       off += kBandT * 4;
+   }
+   for (int k = 0; k < KD; k++) {
+      P.ownd[k] = off;
+      off += kBandT * 8;
    }
    P.bytes = (off + 127) & ~127u;
    P.minlo = D > 0 ? o[0] : 0;
@@ -187,15 +194,17 @@ __device__ __forceinline__ bool band_block_flag(const int32_t* flag)
 // Issues the copies of the tile at i0 into stage `st` (one thread).  The
 // band loop runs over all 8 slots with a guard, so that the plan's arrays
 // are read at fixed indexes.
-template <typename TV, int D, int KB, int KO>
+template <typename TV, int D, int KB, int KO, int KD>
 __device__ __forceinline__ void band_issue(unsigned char* st, uint64_t* bar, const BandPlan& P, const TV* vals,
                                            int64_t pitch, const float* const (&bin)[KB > 0 ? KB : 1],
-                                           const float* const (&oin)[KO > 0 ? KO : 1], int64_t npad, int64_t i0)
+                                           const float* const (&oin)[KO > 0 ? KO : 1],
+                                           const double* const (&din)[KD > 0 ? KD : 1], int64_t npad, int64_t i0)
 {
    const int64_t vrows = pitch - i0 < kBandT ? pitch - i0 : kBandT;
    const int64_t orows = npad - i0 < kBandT ? npad - i0 : kBandT;
    int64_t gs[8], ge[8];
-   uint32_t total = (uint32_t)(D * vrows * (int64_t)sizeof(TV)) + (uint32_t)(KO * orows * 4);
+   uint32_t total =
+      (uint32_t)(D * vrows * (int64_t)sizeof(TV)) + (uint32_t)(KO * orows * 4) + (uint32_t)(KD * orows * 8);
 #pragma unroll
    for (int b = 0; b < 8; b++) {
       gs[b] = band_start(P.lo[b], i0);
@@ -215,6 +224,8 @@ __device__ __forceinline__ void band_issue(unsigned char* st, uint64_t* bar, con
          if (ge[b] > gs[b]) band_copy(st + P.band[k][b], bin[k] + gs[b], (uint32_t)((ge[b] - gs[b]) * 4), bar);
 #pragma unroll
    for (int k = 0; k < KO; k++) band_copy(st + P.own[k], oin[k] + i0, (uint32_t)(orows * 4), bar);
+#pragma unroll
+   for (int k = 0; k < KD; k++) band_copy(st + P.ownd[k], din[k] + i0, (uint32_t)(orows * 8), bar);
 }
 
 __device__ __forceinline__ void band_arrive(uint64_t* bar)
@@ -228,10 +239,11 @@ __device__ __forceinline__ void band_arrive(uint64_t* bar)
 // stage), release it.  Returns false in every thread after a wait gave up;
 // the producer then waits (bounded) for its copies still in flight before
 // the block's shared memory is released.
-template <typename TV, int D, int KB, int KO, typename Tile>
+template <typename TV, int D, int KB, int KO, int KD, typename Tile>
 __device__ __forceinline__ bool band_loop(unsigned char* smem, uint64_t* full, uint64_t* empty, const BandPlan& P,
                                           const TV* vals, int64_t pitch, const float* const (&bin)[KB > 0 ? KB : 1],
-                                          const float* const (&oin)[KO > 0 ? KO : 1], int64_t n, int64_t npad,
+                                          const float* const (&oin)[KO > 0 ? KO : 1],
+                                          const double* const (&din)[KD > 0 ? KD : 1], int64_t n, int64_t npad,
                                           Tile&& tile)
 {
    const int64_t tiles = (n + kBandT - 1) / kBandT;
@@ -258,8 +270,8 @@ __device__ __forceinline__ bool band_loop(unsigned char* smem, uint64_t* full, u
             }
             // the stage was last read by the generic proxy
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            band_issue<TV, D, KB, KO>(smem + (size_t)s * P.bytes, &full[s], P, vals, pitch, bin, oin, npad,
-                                      t * kBandT);
+            band_issue<TV, D, KB, KO, KD>(smem + (size_t)s * P.bytes, &full[s], P, vals, pitch, bin, oin, din,
+                                          npad, t * kBandT);
          }
          if (!ok)  // the last tile issued to each stage: k - 1, k - 2, ...
             for (int64_t q = k - 1; q >= 0 && q >= k - S; q--) band_wait(&full[q % S], (uint32_t)((q / S) & 1));
@@ -368,6 +380,7 @@ struct BandPtrs {
    const float* x[KB > 0 ? KB : 1][D];
    const float* self[KB > 0 ? KB : 1];
    const float* own[2];
+   const double* ownd;
    bool interior;
    __device__ __forceinline__ BandPtrs(const unsigned char* st, const BandPlan& P, const DiaOffsets& o, int64_t i0,
                                        int64_t n)
@@ -396,6 +409,7 @@ struct BandPtrs {
       }
       own[0] = reinterpret_cast<const float*>(me + P.own[0]);
       own[1] = reinterpret_cast<const float*>(me + P.own[1]);
+      ownd = reinterpret_cast<const double*>(st + P.ownd[0]) + threadIdx.x;
    }
 };
 

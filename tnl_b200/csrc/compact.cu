@@ -257,74 +257,6 @@ __global__ void __launch_bounds__(256, Rows::kMinBlocks) k_cmp_xpby(Rows A, cons
    }
 }
 
-// k_cmp_dot on a diagonal copy with its operands staged by bulk copies
-// (band.cuh): y = A x and (x, y) -- (y, y) with `self` -- summing each row
-// as DiaRows and DiaRow1 do (the same terms in the same order, the
-// row-excess form included).  A wait that gave up makes the dot NaN.
-template <typename TV, int D>
-__global__ void __launch_bounds__(kBandBlock) k_band_dot(const TV* __restrict__ vals, int64_t pitch, DiaOffsets o,
-                                                           int32_t self_slot, BandPlan P, const float* __restrict__ x,
-                                                           float* __restrict__ y, int32_t n, int64_t npad, RedWork w,
-                                                           double* __restrict__ dot_out,
-                                                           const int32_t* __restrict__ skip, int self)
-{
-   if (band_block_flag(skip)) return;
-   extern __shared__ __align__(128) unsigned char smem[];
-   __shared__ __align__(8) uint64_t full[kBandStages], empty[kBandStages];
-   const float* const bin[1] = {x};
-   const float* const oin[1] = {nullptr};
-   double d = 0.0;
-   const bool ok = band_loop<TV, D, 1, 0>(smem, full, empty, P, vals, pitch, bin, oin, n, npad,
-                                          [&](int64_t i0, const unsigned char* st) {
-      const BandPtrs<TV, D, 1> B(st, P, o, i0, n);
-      auto rows = [&](auto check) {
-         constexpr bool C = decltype(check)::value;
-#pragma unroll
-         for (int q = 0; q < kBandRows; q++) {
-            const int rl = q * kBandThreads;
-            const int64_t i = i0 + threadIdx.x + rl;
-            if (C && i >= n) break;
-            float v[D], xx[D];
-#pragma unroll
-            for (int j = 0; j < D; j++) {
-               bool in = true;
-               if (C) {
-                  const int64_t c = i + o.o[j];
-                  in = c >= 0 && c < n;
-               }
-               v[j] = in ? rel_to_f(B.v[j * kBandT + rl]) : 0.0f;
-               xx[j] = in ? B.x[0][j][rl] : 0.0f;
-            }
-            if (self_slot >= 0) {
-               float xi = 0.0f;
-#pragma unroll
-               for (int j = 0; j < D; j++)
-                  if (j == self_slot) xi = xx[j];
-#pragma unroll
-               for (int j = 0; j < D; j++)
-                  if (j != self_slot) xx[j] -= xi;
-            }
-            float t = 0.0f;
-#pragma unroll
-            for (int j = 0; j < D; j++) t += v[j] * xx[j];
-            y[i] = t;
-            d += (double)t * (self ? (double)t : (double)B.self[0][rl]);
-         }
-      };
-      if (B.interior)
-         rows(std::false_type{});
-      else
-         rows(std::true_type{});
-   });
-   if (!ok) d = __longlong_as_double(0x7ff8000000000000ll);  // NaN: the caller sees a breakdown
-   double vv[1] = {d};
-   if (band_publish<1>(vv, w)) {
-      double t[1];
-      band_totals<1>(t, w);
-      if (threadIdx.x == 0) *dot_out = t[0];
-   }
-}
-
 template <typename Rows>
 void launch_cmp_dot(const Rows& rows, int32_t n, const float* x, float* y, RedWork w, double* dot_out,
                     cudaStream_t st, const int32_t* skip, int self)
@@ -505,36 +437,6 @@ bool compact_band_capable(const CompactCopy& A)
 {
    if (A.kind != CompactCopy::kDia || A.width < 1 || A.width > 8 || A.pitch % 8 != 0) return false;
    return band_plan(A.diag, A.width, A.half ? 2 : 4, 1, 0).zero;
-}
-
-tnlb_status compact_band_dot(const CompactCopy& A, const float* x, float* y, double* partials, unsigned* counter,
-                             double* dot_out, cudaStream_t st, const int32_t* skip, bool self_dot)
-{
-   TNLB_REQUIRE(compact_band_capable(A), TNLB_ERR_INVALID_ARGUMENT, "compact_band_dot: not a banded diagonal copy");
-   TNLB_REQUIRE(aligned16(x), TNLB_ERR_INVALID_ARGUMENT, "compact_band_dot: x must be 16-byte aligned");
-   const RedWork w{partials, counter};
-   const BandPlan P = band_plan(A.diag, A.width, A.half ? 2 : 4, 1, 0);
-   DiaOffsets o{};
-   for (int j = 0; j < 8; j++) o.o[j] = A.diag[j];
-   const int64_t npad = ((int64_t)A.n + 3) / 4 * 4;
-   const int self = self_dot ? 1 : 0;
-   const size_t smem = (size_t)P.stages * P.bytes;
-   auto go = [&](auto tv_tag, auto d_tag) {
-      using TV = decltype(tv_tag);
-      constexpr int D = decltype(d_tag)::value;
-      auto* k = k_band_dot<TV, D>;
-      const unsigned grid = band_grid((const void*)k, smem, A.n, kRedMaxBlocks);
-      k<<<grid, kBandBlock, smem, st>>>(A.vals.as<TV>(), A.pitch, o, A.self_slot, P, x, y, A.n, npad, w, dot_out,
-                                           skip, self);
-   };
-   TNLB_DIA_WIDTH(A.width, {
-      if (A.half)
-         go(__half(), std::integral_constant<int, D>());
-      else
-         go(float(), std::integral_constant<int, D>());
-   });
-   TNLB_CHECK_LAUNCH();
-   return TNLB_OK;
 }
 
 tnlb_status compact_spmv_xpby(const CompactCopy& A, const float* x, float* y, const double* num, const double* den,

@@ -328,10 +328,6 @@ tnlb_status compact_spmv_dot(const CompactCopy& A, const float* x, float* y, dou
 // A diagonal copy the bulk-copy-staged kernels take (band.cuh): at most 8
 // diagonals, offset 0 among them.
 bool compact_band_capable(const CompactCopy& A);
-// compact_spmv_dot on a band-capable copy, operands staged by bulk copies;
-// x must hold a multiple of 4 entries (n rounded up).
-tnlb_status compact_band_dot(const CompactCopy& A, const float* x, float* y, double* partials, unsigned* counter,
-                             double* dot_out, cudaStream_t st, const int32_t* skip, bool self_dot);
 // y = A x + (*num / *den) y.
 tnlb_status compact_spmv_xpby(const CompactCopy& A, const float* x, float* y, const double* num, const double* den,
                               cudaStream_t st, const int32_t* skip);

@@ -2452,8 +2452,9 @@ __global__ void __launch_bounds__(kBandBlock)
    const float alpha = okp ? (float)(rz / tp) : 0.0f;
    const float* const bin[2] = {r, Ap};
    const float* const oin[1] = {nullptr};
+   const double* const din[1] = {nullptr};
    double rr = 0, tt = 0;
-   const bool ok = band_loop<TV, D, 2, 0>(smem, full, empty, P, vals, pitch, bin, oin, n, npad,
+   const bool ok = band_loop<TV, D, 2, 0, 0>(smem, full, empty, P, vals, pitch, bin, oin, din, n, npad,
                                           [&](int64_t i0, const unsigned char* st) {
       const BandPtrs<TV, D, 2> B(st, P, o, i0, n);
       auto rows = [&](auto check) {
@@ -2511,8 +2512,7 @@ __global__ void __launch_bounds__(kBandBlock)
 }
 
 // k_ru_gt_xpby on a diagonal copy of G^T: t staged by bands, the tile's own
-// p by a bulk copy, the FP64 xc read and written in place.  A wait that
-// gave up raises a breakdown.
+// p and FP64 xc by bulk copies.  A wait that gave up raises a breakdown.
 template <typename TV, int D>
 __global__ void __launch_bounds__(kBandBlock)
    k_band_gt_xpby(const TV* __restrict__ vals, int64_t pitch, DiaOffsets o, BandPlan P, const float* __restrict__ t,
@@ -2526,7 +2526,8 @@ __global__ void __launch_bounds__(kBandBlock)
    const float alpha = (float)S->alpha;
    const float* const bin[1] = {t};
    const float* const oin[1] = {p};
-   const bool ok = band_loop<TV, D, 1, 1>(smem, full, empty, P, vals, pitch, bin, oin, n, npad,
+   const double* const din[1] = {xc};
+   const bool ok = band_loop<TV, D, 1, 1, 1>(smem, full, empty, P, vals, pitch, bin, oin, din, n, npad,
                                           [&](int64_t i0, const unsigned char* st) {
       const BandPtrs<TV, D, 1> B(st, P, o, i0, n);
       auto rows = [&](auto check) {
@@ -2551,7 +2552,7 @@ __global__ void __launch_bounds__(kBandBlock)
 #pragma unroll
             for (int j = 0; j < D; j++) s += v[j] * x[j];
             const float po = B.own[0][rl];
-            xc[i] += (double)alpha * (double)po;
+            xc[i] = B.ownd[rl] + (double)alpha * (double)po;
             p[i] = s + beta * po;
          }
       };
@@ -2584,7 +2585,7 @@ void launch_band_g_update(const CompactCopy& G, const float* r, const float* Ap,
 void launch_band_gt_xpby(const CompactCopy& GT, const float* t, float* p, double* xc, int32_t n, const double* rz_cur,
                          RuState* S, cudaStream_t st)
 {
-   const BandPlan P = band_plan(GT.diag, GT.width, (int)sizeof(__half), 1, 1);
+   const BandPlan P = band_plan(GT.diag, GT.width, (int)sizeof(__half), 1, 1, 1);
    DiaOffsets o{};
    for (int j = 0; j < 8; j++) o.o[j] = GT.diag[j];
    const int64_t npad = ((int64_t)n + 3) / 4 * 4;
@@ -2780,15 +2781,16 @@ tnlb_status reliable_t(const tnlb_segments* seg, const int32_t* cols, const doub
    }
    const bool cmp_a = cA.kind != CompactCopy::kNone;
    const bool cmp_m = cG.kind != CompactCopy::kNone && cGT.kind != CompactCopy::kNone;
-   // diagonal copies of more than 5 diagonals stage their products'
-   // operands by bulk copies (band.cuh); up to 5 diagonals the four-row
-   // register form (DiaRows) measured as fast or faster (2048^2 5-point
-   // operator: Jacobi iteration 63.6 against 64.7 us, 3-diagonal FSAI
-   // 84.1 against 87.4 us; 7-diagonal FSAI 93.7 against 142.6 us)
+   // FSAI factor copies of more than 5 diagonals stage their products'
+   // operands by bulk copies (band.cuh): on the 2048^2 diffusion matrix
+   // the iteration with the 7-diagonal level-1 factors took 99.7 against
+   // 149.4 us.  Up to 5 diagonals the four-row register form (DiaRows)
+   // measured as fast (3-diagonal factors: 87.6 against 88.1 us), and for
+   // A (FP32 values) the register forms were faster: 788 against 901 ms on
+   // the 256^3 7-point Jacobi solve.
    auto banded = [&](const CompactCopy& C) {
       return prm.reliable_layout == 0 && C.kind == CompactCopy::kDia && C.width > 5 && compact_band_capable(C);
    };
-   const bool band_a = cmp_a && banded(cA);
    const bool band_g = cmp_m && banded(cG), band_gt = cmp_m && banded(cGT);
    // with the compact FSAI copies the update of xc and r goes into the two
    // factor products (k_ru_g_update, k_ru_gt_xpby); the new residual goes
@@ -2825,10 +2827,7 @@ tnlb_status reliable_t(const tnlb_segments* seg, const int32_t* cols, const doub
       return TNLB_OK;
    };
    auto iteration = [&](cudaStream_t s, int k) -> tnlb_status {
-      if (band_a)
-         TNLB_TRY_STATUS(compact_band_dot(cA, (const float*)p.ptr, (float*)Ap.ptr, WA.partials.as<double>(),
-                                          WA.counter.as<unsigned>(), pap, s, halt, false));
-      else if (cmp_a)
+      if (cmp_a)
          TNLB_TRY_STATUS(compact_spmv_dot(cA, (const float*)p.ptr, (float*)Ap.ptr, WA.partials.as<double>(),
                                           WA.counter.as<unsigned>(), pap, s, halt, false));
       else if (fused_a)
