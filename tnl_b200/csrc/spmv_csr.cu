@@ -136,13 +136,18 @@ __global__ void __launch_bounds__(256) k_csr_adaptive(const tnlb_acsr_block* __r
    tnlb_acsr_block d{};
    if (active) d = blocks[w];
    if (active && d.type == 1) {  // STREAM: many short rows, staged per warp
+      // the block's entries 12 per lane and pass (FP64: the whole block in
+      // one pass), every load and then every x gather issued before any is
+      // used: 3x the gathers in flight of a 4-wide loop, which left the
+      // kernel at a third of the tile kernel's rate on power-law rows
+      constexpr int U = 12;
       const int32_t first = d.first_segment;
       const int32_t b = rowptr[first];
-      for (int32_t k = lane; k < d.block_size; k += 128) {
-         int32_t c[4];
-         Real v[4];
+      for (int32_t k = lane; k < d.block_size; k += 32 * U) {
+         int32_t c[U];
+         Real v[U], g[U];
 #pragma unroll
-         for (int u = 0; u < 4; u++) {
+         for (int u = 0; u < U; u++) {
             c[u] = -1;
             v[u] = Real(0);
             if (k + 32 * u < d.block_size) {
@@ -151,8 +156,10 @@ __global__ void __launch_bounds__(256) k_csr_adaptive(const tnlb_acsr_block* __r
             }
          }
 #pragma unroll
-         for (int u = 0; u < 4; u++)
-            if (k + 32 * u < d.block_size) stream_buf[wib][k + 32 * u] = c[u] >= 0 ? v[u] * ld_gather(x + c[u]) : Real(0);
+         for (int u = 0; u < U; u++) g[u] = c[u] >= 0 ? ld_gather(x + c[u]) : Real(0);
+#pragma unroll
+         for (int u = 0; u < U; u++)
+            if (k + 32 * u < d.block_size) stream_buf[wib][k + 32 * u] = v[u] * g[u];
       }
       __syncwarp();
       for (int32_t r = first + lane; r < first + d.segments_in_block; r += 32) {
