@@ -501,18 +501,97 @@ __global__ void __launch_bounds__(kTileThreads) k_csr_tile(const int32_t* __rest
    uint32_t m[kTileItems];
 #pragma unroll
    for (int j = 0; j < kTileItems; j++) m[j] = 0u;
+   bool all_marked = true;  // every row of the tile ends in it (no empty row)
    for (int32_t q = 0; q * 32 < nrows; q++) {
       const int32_t i = q * 32 + lane;
       int32_t eb, ee;
       row_ends(q, eb, ee);
       const bool mark = i < nrows && ee > k0 && ee > eb;
       if (i < nrows && !mark) keep(y, r0 + i, Real(0), alpha, beta);
+      all_marked = all_marked && (i >= nrows || mark);
       const int32_t pos = mark ? ee - k0 - 1 : -1;
 #pragma unroll
       for (int j = 0; j < kTileItems; j++) {
          const uint32_t bit = (mark && (pos >> 5) == j) ? (1u << (pos & 31)) : 0u;
          m[j] |= __reduce_or_sync(kAll, bit);
       }
+   }
+
+   // Blocked form (FP32), for tiles whose rows all end in them (then the
+   // k-th marked position ends row r0 + k): the products go through shared
+   // memory from striped to blocked order (lane l takes positions 8l ..
+   // 8l + 7; one pad word every 32 keeps the stores free of bank
+   // conflicts), each lane sums its positions in order, writing the rows
+   // that start and end among them, and one segmented scan over the lanes
+   // finishes the rows that cross lanes, in place of the striped form's
+   // segmented scan per 32-nonzero step.  On the power-law matrix it took
+   // the FP32 product from 319 to 292 us; in FP64 it measured 351 against
+   // 344 us (the load pipe that serves the gathers, not the issue slots,
+   // binds the FP64 product), so FP64 keeps the striped form.
+   if (sizeof(Real) == 4 && __all_sync(kAll, all_marked)) {
+      __shared__ Real s_prod[kWarps][kTileSize + kTileItems];
+      __shared__ uint32_t s_mask[kWarps][kTileItems];
+      Real* sp = s_prod[warp];
+#pragma unroll
+      for (int j = 0; j < kTileItems; j++) sp[j * 33 + lane] = v[j];  // position k = 32 j + lane at k + (k >> 5)
+      uint32_t mw = 0u, lm = 0u;
+#pragma unroll
+      for (int j = 0; j < kTileItems; j++) {
+         if (lane == j) mw = m[j];
+         if (((nk - 1) >> 5) == j) lm = m[j];
+      }
+      if (lane < kTileItems) s_mask[warp][lane] = mw;
+      __syncwarp();
+      const uint32_t bits = (s_mask[warp][lane >> 2] >> ((lane & 3) * 8)) & 0xffu;
+      Real pv[kTileItems];
+#pragma unroll
+      for (int i = 0; i < kTileItems; i++) pv[i] = sp[8 * lane + i + (lane >> 2)];
+      // rank of this lane's first row end among the tile's
+      const int nends = __popc(bits);
+      int incl = nends;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+         const int u = __shfl_up_sync(kAll, incl, o);
+         if (lane >= o) incl += u;
+      }
+      const int32_t row0 = r0 + incl - nends;
+      Real run = Real(0), head = Real(0);
+      int ended = 0;
+#pragma unroll
+      for (int i = 0; i < kTileItems; i++) {
+         run += pv[i];
+         if ((bits >> i) & 1u) {
+            if (ended == 0)
+               head = run;
+            else
+               keep(y, row0 + ended, run, alpha, beta);
+            ended++;
+            run = Real(0);
+         }
+      }
+      // (open sum, row ended) scanned over the lanes: the sum carried into
+      // a lane's first row end
+      Real sc = run;
+      bool fl = ended > 0;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+         const Real su = __shfl_up_sync(kAll, sc, o);
+         const bool fu = __shfl_up_sync(kAll, fl, o);
+         if (lane >= o) {
+            if (!fl) sc += su;
+            fl = fl || fu;
+         }
+      }
+      Real cin = __shfl_up_sync(kAll, sc, 1);
+      if (lane == 0) cin = Real(0);
+      if (ended > 0) keep(y, row0, head + cin, alpha, beta);
+      const Real open_sum = __shfl_sync(kAll, sc, 31);
+      if (lane == 0) {
+         const bool has = nk > 0 && !((lm >> ((nk - 1) & 31)) & 1u);
+         carry_row[t] = (has && r1 < n) ? r1 : -1;
+         carry_val[t] = open_sum;
+      }
+      return;
    }
 
    // The open row's partial sum: `carry` (one value) plus, after steps with
