@@ -337,6 +337,32 @@ def reference_solver_leg(iterations=200):
             "sample": f"{iterations} iterations of a solve, not run to the tolerance"}
 
 
+def reference_c1_solves(maxit=20000):
+    """The reference's Host solvers of its linear-solver benchmark on the 2D
+    Laplacian of the plain-method config (1024 x 1024, Dirichlet, b ~ U[-1,1)
+    seed 1, tolerance 1e-8 on the reference's own residue): CG and BiCGStab
+    with Jacobi, GMRES(30) with ILU(0) in its MGSR and CWY variants; one JSON
+    line each with the reference's own timing, iterations and the true
+    residual.  Reported beside the library's GPU solves of the same problems
+    (`python -m tnl_b200.benchmarks c1-solvers`)."""
+    from oracle.oracle import REF_SO, Oracle, Reference  # reference arm only
+
+    if not REF_SO.exists():
+        return
+    g = generators()
+    A = g.laplacian_2d(1024)
+    b = g.uniform_vector(A.n, 1)
+    R = Reference()
+    O = Oracle()
+    for name, solver, pre, variant in (("CG + Jacobi", "cg", 1, 3), ("BiCGStab + Jacobi", "bicgstab", 1, 3),
+                                       ("GMRES(30) MGSR + ILU(0)", "gmres", 2, 3),
+                                       ("GMRES(30) CWY + ILU(0)", "gmres", 2, 4)):
+        r = R.solve(solver, A, b, precond=pre, tol=1e-8, maxit=maxit, gmres_m=30, gmres_variant=variant)
+        print(json.dumps({"impl": "reference", "bench": "c1_solve", "method": name, "cores": R.threads(),
+                          "converged": r["converged"], "iterations": r["iterations"], "seconds": r["seconds"],
+                          "residue": r["residue"], "true_residual": O.true_residual(A, b, r["x"])}), flush=True)
+
+
 def run_reference(args):
     world, rank, local = dist_env()
     if rank != 0:
@@ -352,6 +378,8 @@ def run_reference(args):
     if not args.no_solver:
         line["solver"] = reference_solver_leg()
     print(json.dumps(line), flush=True)
+    if args.reference_solvers:
+        reference_c1_solves()
     return 0
 
 
@@ -551,6 +579,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-solver", action="store_true", help="skip the PCG time-to-1e-8 leg")
+    ap.add_argument("--reference-solvers", action="store_true",
+                    help="with --impl reference: also the reference's Host CG, BiCGStab and GMRES(30)+ILU(0) "
+                         "solves of the 1024^2 Laplacian, one JSON line each after the bench line")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -8,6 +8,9 @@ on seeded synthetic matrices.  One JSON object per line on stdout.
     python -m tnl_b200.benchmarks sweep   [--problem laplacian|diffusion|convection_diffusion] [--N 1024]
     python -m tnl_b200.benchmarks profile-solvers [--problem diffusion] [--N 2048] [--iterations 40]
     python -m tnl_b200.benchmarks configs --which c3|c5
+    python -m tnl_b200.benchmarks learned-eval [--count 64] [--N 2048]
+    python -m tnl_b200.benchmarks c1-solves
+    python -m tnl_b200.benchmarks assembly [--max-grid 8192]
 
 spmv: every segment format and kernel on the 1024^2 5-point Laplacian
 (n = 1,048,576), the power-law matrix (n = 4,194,304, Zipf 1.73 row
@@ -454,6 +457,36 @@ def bench_configs(which: str, out=sys.stdout):
            training_ms=train_ms)
 
 
+def bench_c1_solves(out=sys.stdout):
+    """The library's GPU solves of the reference's linear-solver benchmark
+    on the 1024 x 1024 Laplacian (b ~ U[-1,1) seed 1, tolerance 1e-8 on the
+    reference's residue): CG and BiCGStab with Jacobi, GMRES(30) with ILU(0)
+    in the MGSR and CWY variants; CUDA-event time of one solve after a
+    warm-up solve (set-up excluded, as the reference times only solve())."""
+    import tnl_b200 as t
+    from . import generators as g
+
+    A = g.laplacian_2d(1024)
+    M = t.SparseMatrix.from_csr(A)
+    b = torch.tensor(g.uniform_vector(A.n, 1), device="cuda")
+    for name, cls, pre, variant in (("CG + Jacobi", t.CG, "jacobi", "MGSR"), ("BiCGStab + Jacobi", t.BICGStab, "jacobi", "MGSR"),
+                                    ("GMRES(30) MGSR + ILU(0)", t.GMRES, "ilu0", "MGSR"),
+                                    ("GMRES(30) CWY + ILU(0)", t.GMRES, "ilu0", "CWY")):
+        P = t.Diagonal() if pre == "jacobi" else t.ILU0()
+        P.update(M)
+        S = cls()
+        S.setMatrix(M)
+        S.setPreconditioner(P)
+        S.setup({"convergence-residue": 1e-8, "max-iterations": 20000, "gmres-variant": variant,
+                 "gmres-restarting-min": 30, "gmres-restarting-max": 30})
+        S.solve(b, torch.zeros(A.n, dtype=torch.float64, device="cuda"))
+        x = torch.zeros(A.n, dtype=torch.float64, device="cuda")
+        ok, ms = _timed(lambda: S.solve(b, x))
+        print(json.dumps({"bench": "c1_solve", "method": name, "converged": bool(ok), "iterations": S.getIterations(),
+                          "seconds": ms / 1e3, "residue": S.getResidue(), "true_residual": t.true_residual(M, b, x)}),
+              file=out, flush=True)
+
+
 def profile_solvers(problem: str, N: int, iterations: int, fsai_level: int = 0, out=sys.stdout):
     """A fixed number of iterations of the FP32 reliable-update FSAI-PCG and
     of FP64 FSAI-PCG, for a kernel launch list (ncu) of both iterations;
@@ -648,6 +681,7 @@ def main(argv=None):
     b.add_argument("--weights", default=str(Path(__file__).resolve().parent / "weights" / "lfsai_diffusion.npy"))
     asm = sub.add_parser("assembly")
     asm.add_argument("--max-grid", type=int, default=8192)
+    sub.add_parser("c1-solves")
     le = sub.add_parser("learned-eval")
     le.add_argument("--count", type=int, default=64)
     le.add_argument("--N", type=int, default=2048)
@@ -664,6 +698,9 @@ def main(argv=None):
         return 0
     if args.cmd == "learned-eval":
         bench_learned_eval(args.count, args.N, args.weights, args.ilu_count)
+        return 0
+    if args.cmd == "c1-solves":
+        bench_c1_solves()
         return 0
     if args.cmd == "profile-solvers":
         profile_solvers(args.problem, args.N, args.iterations, args.fsai_level)
