@@ -430,6 +430,19 @@ def bench_configs(which: str, out=sys.stdout):
                                         reps=3)
         report("FP32 Jacobi-PCG with reliable FP64 updates, diagonal copy read by ordinary loads", r["converged"],
                r["iterations"], ms, 0.0, x, reliable_updates=r["reliable_updates"], solve_ms_runs=times)
+        # beyond the config: the same solver with the classical FSAI of A's
+        # pattern (4-diagonal factors), set-up timed apart
+        A32 = t.SparseMatrix(t.CSR, torch.float32).assign(A.rowptr, A.cols, A.vals.astype(np.float32))
+        Pf = t.FSAI()
+        Pf.update(A32)
+        Pf = t.FSAI()
+        _, s_f = _timed(lambda: Pf.update(A32))
+        t.solve_mixed_reliable(M, b, torch.zeros(n, dtype=torch.float64, device="cuda"), tol=tol, inner=Pf,
+                               max_iterations=20)
+        r, x, ms, times = _median_timed(_Run(lambda x: t.solve_mixed_reliable(M, b, x, tol=tol, delta=0.3,
+                                                                              inner=Pf), n), reps=3)
+        report("FP32 FSAI-PCG with reliable FP64 updates", r["converged"], r["iterations"], ms, s_f, x,
+               reliable_updates=r["reliable_updates"], solve_ms_runs=times)
         return
     P = t.ILU0()
     _, s_ilu = _timed(lambda: P.update(M))
