@@ -217,8 +217,8 @@ def solver_problem():
 
 def solver_leg():
     """PCG time to an FP64 true residual ||b - A x|| / ||b|| <= 1e-8 on one
-    B200 (CUDA events around each call on the launching stream), every
-    method warmed up by one 20-iteration run first:
+    B200 (CUDA events around each call on the launching stream; the fastest
+    of three solves), every method warmed up by one 20-iteration run first:
       * FP64 Jacobi-PCG, its convergence residue lowered until the TRUE
         residual is below 1e-8 (the reference's rule stops on the
         preconditioned residue; each retry scales it by the gap seen);
@@ -279,11 +279,23 @@ def solver_leg():
         # the stopping residue and the true residual differ by a factor
         # the next run's tolerance corrects
         tol *= 0.5 * SOLVER_TOL / tr
-    x = zeros()
-    ok, ms = timed(lambda: S.solve(b, x))
+    def best_of(run, reps=3):
+        # the fastest of `reps` solves from x = 0: single host-loop stalls of
+        # hundreds of ms occur on the shared machine
+        best = None
+        times = []
+        for _ in range(reps):
+            x = zeros()
+            r, ms = timed(lambda: run(x))
+            times.append(ms)
+            if best is None or ms < best[2]:
+                best = (r, x, ms)
+        return best[0], best[1], best[2], times
+
+    ok, x, ms, runs = best_of(lambda x: S.solve(b, x))
     fp64 = {"method": "FP64 Jacobi-PCG", "solve_ms": ms, "setup_ms": jac_setup, "iterations": S.getIterations(),
             "converged": bool(ok), "true_residual": t.true_residual(M, b, x), "convergence_residue": tol,
-            "error_vs_fp64_solution": err(x)}
+            "error_vs_fp64_solution": err(x), "solve_ms_runs": runs}
 
     A32 = t.SparseMatrix(t.CSR, torch.float32)
     A32.assign(A.rowptr, A.cols, A.vals.astype(np.float32))
@@ -291,9 +303,8 @@ def solver_leg():
     def reliable(name, make_prec):
         P, setup = make_prec()
         t.solve_mixed_reliable(M, b, zeros(), tol=SOLVER_TOL, inner=P, max_iterations=20)
-        x = zeros()
-        r, ms = timed(lambda: t.solve_mixed_reliable(M, b, x, tol=SOLVER_TOL, delta=0.3, inner=P))
-        return {"method": name, "solve_ms": ms, "setup_ms": setup, "iterations": r["iterations"],
+        r, x, ms, runs = best_of(lambda x: t.solve_mixed_reliable(M, b, x, tol=SOLVER_TOL, delta=0.3, inner=P))
+        return {"method": name, "solve_ms": ms, "solve_ms_runs": runs, "setup_ms": setup, "iterations": r["iterations"],
                 "reliable_updates": r["reliable_updates"], "converged": bool(r["converged"]),
                 "true_residual": t.true_residual(M, b, x), "error_vs_fp64_solution": err(x),
                 "speedup_vs_fp64_jacobi": fp64["solve_ms"] / ms,
