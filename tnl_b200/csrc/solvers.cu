@@ -2142,6 +2142,7 @@ struct RuState {
    double trig2;  // |r|^2 of the recursion below which an update is due
    double rr;     // |r|^2 after the last update of r
    int32_t it, halt, maxit, force_at;
+   int32_t loops, pad;  // batches run by the device-side loop since k_ru_set
 };
 
 // Iterations after which an update is due whatever the recursive residual,
@@ -2692,6 +2693,17 @@ __global__ void k_ru_set(RuState* S, double trig2)
    S->trig2 = trig2;
    S->force_at = S->it + kRuForceEvery;
    S->halt = 0;
+   S->loops = 0;
+}
+
+// Last node of the batch body under a conditional WHILE node: run the body
+// again until the state halts (an update is due, a breakdown, the iteration
+// limit), and at most `cap` times per launch whatever the state holds.
+__global__ void k_ru_continue(cudaGraphConditionalHandle loop, RuState* S, int32_t cap)
+{
+   if (threadIdx.x != 0) return;
+   const int32_t l = ++S->loops;
+   cudaGraphSetConditional(loop, S->halt == 0 && l < cap ? 1u : 0u);
 }
 
 // The solver body for vectors of type VT (float: FP32 vectors; double: FP64
@@ -2875,7 +2887,8 @@ tnlb_status reliable_t(const tnlb_segments* seg, const int32_t* cols, const doub
    TNLB_CUDA_TRY(cudaMemsetAsync(p.ptr, 0, sizeof(VT) * n, st));
    TNLB_CUDA_TRY(cudaMemsetAsync(xc.ptr, 0, sizeof(double) * n, st));
 
-   // CUDA graph of a batch of iterations, captured once on a side stream
+   // CUDA graph of the iterations between updates, captured once on a side
+   // stream
    const int kBatch = n < (1 << 22) ? 32 : 16;
    cudaStream_t cs;
    TNLB_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
@@ -2895,19 +2908,64 @@ tnlb_status reliable_t(const tnlb_segments* seg, const int32_t* cols, const doub
    cudaGraph_t graph = nullptr;
    cudaGraphExec_t exec = nullptr;
    tnlb_status status = TNLB_OK;
-   if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
-      for (int k = 0; k < kBatch && status == TNLB_OK; k++) status = iteration(cs, k);
-      cudaError_t e = cudaStreamEndCapture(cs, &graph);
-      if (e == cudaSuccess && status == TNLB_OK) e = cudaGraphInstantiate(&exec, graph, 0);
-      if (e != cudaSuccess) {
-         cudaGetLastError();
-         exec = nullptr;
+   // Preferred form: a conditional WHILE node whose body is the batch and
+   // k_ru_continue, so that the device repeats the batch until the state
+   // halts with no host round trip between batches. The state halts at the
+   // latest kRuForceEvery iterations after k_ru_set, within kCap bodies.
+   const int32_t kCap = kRuForceEvery / kBatch + 2;
+   bool device_loop = false;
+   if (cudaGraphCreate(&graph, 0) == cudaSuccess) {
+      cudaGraphConditionalHandle loop{};
+      cudaGraphNodeParams np{};
+      np.type = cudaGraphNodeTypeConditional;
+      cudaGraphNode_t node = nullptr;
+      bool ok = cudaGraphConditionalHandleCreate(&loop, graph, 1, cudaGraphCondAssignDefault) == cudaSuccess;
+      if (ok) {
+         np.conditional.handle = loop;
+         np.conditional.type = cudaGraphCondTypeWhile;
+         np.conditional.size = 1;
+         ok = cudaGraphAddNode(&node, graph, nullptr, 0, &np) == cudaSuccess;
       }
-      status = TNLB_OK;  // a failed capture falls back to direct launches
+      if (ok)
+         ok = cudaStreamBeginCaptureToGraph(cs, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                            cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+      if (ok) {
+         for (int k = 0; k < kBatch && status == TNLB_OK; k++) status = iteration(cs, k);
+         if (status == TNLB_OK) k_ru_continue<<<1, 32, 0, cs>>>(loop, S, kCap);
+         cudaGraph_t body = nullptr;
+         ok = cudaStreamEndCapture(cs, &body) == cudaSuccess && status == TNLB_OK &&
+              cudaGetLastError() == cudaSuccess && cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+      }
+      if (!ok) {
+         cudaGetLastError();
+         if (exec) cudaGraphExecDestroy(exec);
+         cudaGraphDestroy(graph);
+         exec = nullptr;
+         graph = nullptr;
+      }
+      device_loop = ok;
+      status = TNLB_OK;  // a failed build falls back to the batch graph
       clear_error();
    }
    else
       cudaGetLastError();
+   // Otherwise a graph of the batch alone, relaunched by the host; where its
+   // capture fails too, the iterations are launched directly.
+   if (!device_loop) {
+      if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+         for (int k = 0; k < kBatch && status == TNLB_OK; k++) status = iteration(cs, k);
+         cudaError_t e = cudaStreamEndCapture(cs, &graph);
+         if (e == cudaSuccess && status == TNLB_OK) e = cudaGraphInstantiate(&exec, graph, 0);
+         if (e != cudaSuccess) {
+            cudaGetLastError();
+            exec = nullptr;
+         }
+         status = TNLB_OK;
+         clear_error();
+      }
+      else
+         cudaGetLastError();
+   }
    struct GraphGuard {  // released after the stream has drained
       cudaStream_t s;
       cudaGraph_t g;
@@ -3012,6 +3070,12 @@ tnlb_status reliable_t(const tnlb_segments* seg, const int32_t* cols, const doub
          TNLB_CHECK_LAUNCH();
       }
       TNLB_TRY_STATUS(precondition(cs, halt));
+      if (device_loop) {
+         // iterations until an update is due, looped on the device; the
+         // next update reads the state it halted in
+         TNLB_CUDA_TRY(cudaGraphLaunch(exec, cs));
+         continue;
+      }
       // iterations until an update is due, one batch queued ahead of the
       // host's check of the state (a batch after the halt skips itself)
       TNLB_TRY_STATUS(launch_batch());
