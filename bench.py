@@ -218,7 +218,7 @@ def solver_problem():
 def solver_leg():
     """PCG time to an FP64 true residual ||b - A x|| / ||b|| <= 1e-8 on one
     B200 (CUDA events around each call on the launching stream; the fastest
-    of three solves), every method warmed up by one 20-iteration run first:
+    of five solves), every method warmed up by one 20-iteration run first:
       * FP64 Jacobi-PCG, its convergence residue lowered until the TRUE
         residual is below 1e-8 (the reference's rule stops on the
         preconditioned residue; each retry scales it by the gap seen);
@@ -279,9 +279,10 @@ def solver_leg():
         # the stopping residue and the true residual differ by a factor
         # the next run's tolerance corrects
         tol *= 0.5 * SOLVER_TOL / tr
-    def best_of(run, reps=3):
-        # the fastest of `reps` solves from x = 0: single host-loop stalls of
-        # hundreds of ms occur on the shared machine
+    def best_of(run, reps=5):
+        # the fastest of `reps` solves from x = 0: on the shared machine,
+        # periods of a second or two occur in which consecutive solves take
+        # up to twice their usual time at full SM clock
         best = None
         times = []
         for _ in range(reps):
