@@ -32,7 +32,8 @@ struct DevState {
    double normb, s1, s2, alpha, beta, omega, rho, rho_old, r_ast_sqnorm, residue;
    double conv, div;
    int32_t it, done, maxit, minit;
-   int32_t flag, pad;
+   int32_t flag;
+   uint32_t loops;  // bodies run by the current launch of a looping iteration graph
 };
 
 __device__ __forceinline__ bool check_next(const DevState& S)
@@ -561,6 +562,78 @@ struct Work {
    DevState* S() const { return state.as<DevState>(); }
 };
 
+// The iteration graph of a solver, captured on stream s: preferably a
+// conditional WHILE node whose body is body(s) followed by cont(loop, s), a
+// one-thread kernel that sets the loop's condition, so that the device
+// repeats the body with no host round trip; where the driver cannot build
+// that node, body(s) alone. Returns whether the graph loops. When capture
+// fails both ways, *exec stays null and the caller launches the body's
+// kernels directly.
+template <typename Body, typename Cont>
+bool build_iteration_graph(cudaStream_t s, Body&& body, Cont&& cont, cudaGraph_t* graph, cudaGraphExec_t* exec)
+{
+   *graph = nullptr;
+   *exec = nullptr;
+   if (cudaGraphCreate(graph, 0) == cudaSuccess) {
+      cudaGraphConditionalHandle loop{};
+      cudaGraphNodeParams np{};
+      np.type = cudaGraphNodeTypeConditional;
+      cudaGraphNode_t node = nullptr;
+      bool ok = cudaGraphConditionalHandleCreate(&loop, *graph, 1, cudaGraphCondAssignDefault) == cudaSuccess;
+      if (ok) {
+         np.conditional.handle = loop;
+         np.conditional.type = cudaGraphCondTypeWhile;
+         np.conditional.size = 1;
+         ok = cudaGraphAddNode(&node, *graph, nullptr, 0, &np) == cudaSuccess;
+      }
+      if (ok)
+         ok = cudaStreamBeginCaptureToGraph(s, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                            cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+      if (ok) {
+         const tnlb_status rc = body(s);
+         if (rc == TNLB_OK) cont(loop, s);
+         cudaGraph_t captured = nullptr;
+         ok = cudaStreamEndCapture(s, &captured) == cudaSuccess && rc == TNLB_OK &&
+              cudaGetLastError() == cudaSuccess && cudaGraphInstantiate(exec, *graph, 0) == cudaSuccess;
+      }
+      clear_error();
+      if (ok) return true;
+      cudaGetLastError();
+      if (*exec) cudaGraphExecDestroy(*exec);
+      cudaGraphDestroy(*graph);
+      *exec = nullptr;
+      *graph = nullptr;
+   }
+   else
+      cudaGetLastError();
+   if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+      const tnlb_status rc = body(s);
+      cudaError_t e = cudaStreamEndCapture(s, graph);
+      if (e == cudaSuccess && rc == TNLB_OK) e = cudaGraphInstantiate(exec, *graph, 0);
+      if (e != cudaSuccess) {
+         cudaGetLastError();
+         *exec = nullptr;
+      }
+      clear_error();
+   }
+   else
+      cudaGetLastError();
+   return false;
+}
+
+// Last node of CG's looping batch body: run the body again until the state
+// is done, at most `cap` bodies per launch, after which the host reads the
+// state and launches again. The counter restarts at each exit, and a counter
+// found at `cap` or above ends the loop at once.
+__global__ void k_cg_continue(cudaGraphConditionalHandle loop, DevState* S, uint32_t cap)
+{
+   if (threadIdx.x != 0) return;
+   const uint32_t l = S->loops + 1u;
+   const bool go = !S->done && l < cap;
+   S->loops = go ? l : 0u;
+   cudaGraphSetConditional(loop, go ? 1u : 0u);
+}
+
 DevState initial_state(const tnlb_solver_params& p)
 {
    DevState s{};
@@ -671,8 +744,11 @@ tnlb_status cg_solve(const Ctx<Real>& c, const Precond<Real>& P, const tnlb_solv
       TNLB_CHECK_LAUNCH();
       return TNLB_OK;
    };
-   // Batches of iterations replayed from a CUDA graph (captured on a side stream).
+   // Batches of iterations replayed from a CUDA graph (captured on a side
+   // stream), looped on the device up to kCap batches per launch where the
+   // driver builds the conditional node.
    const int kBatch = n < (1 << 22) ? 32 : 8;
+   constexpr uint32_t kCap = 64;
    cudaStream_t cs;
    TNLB_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
    cudaEvent_t ev;
@@ -682,21 +758,18 @@ tnlb_status cg_solve(const Ctx<Real>& c, const Precond<Real>& P, const tnlb_solv
    cudaGraph_t graph = nullptr;
    cudaGraphExec_t exec = nullptr;
    tnlb_status status = TNLB_OK;
-   if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
-      for (int k = 0; k < kBatch && status == TNLB_OK; k++) status = enqueue_iteration(cs);
-      cudaError_t e = cudaStreamEndCapture(cs, &graph);
-      if (e == cudaSuccess && status == TNLB_OK) e = cudaGraphInstantiate(&exec, graph, 0);
-      if (e != cudaSuccess) {
-         cudaGetLastError();
-         exec = nullptr;
-      }
-      status = TNLB_OK;  // a failed capture falls back to direct launches
-      clear_error();
-   }
-   else
-      cudaGetLastError();
-   // One batch stays queued ahead of the host's check of the state (a batch
-   // launched after the stop returns at once, kernel by kernel).
+   // a failed capture falls back to direct launches
+   build_iteration_graph(
+      cs,
+      [&](cudaStream_t s) {
+         tnlb_status rc = TNLB_OK;
+         for (int k = 0; k < kBatch && rc == TNLB_OK; k++) rc = enqueue_iteration(s);
+         return rc;
+      },
+      [&](cudaGraphConditionalHandle loop, cudaStream_t s) { k_cg_continue<<<1, 32, 0, s>>>(loop, W.S(), kCap); },
+      &graph, &exec);
+   // One launch stays queued ahead of the host's check of the state (a launch
+   // after the stop runs one batch that returns at once, kernel by kernel).
    DevState* hs = nullptr;
    cudaEvent_t copied = nullptr;
    auto launch_batch = [&]() {
@@ -2907,65 +2980,21 @@ tnlb_status reliable_t(const tnlb_segments* seg, const int32_t* cols, const doub
    cudaEventDestroy(ev);
    cudaGraph_t graph = nullptr;
    cudaGraphExec_t exec = nullptr;
-   tnlb_status status = TNLB_OK;
-   // Preferred form: a conditional WHILE node whose body is the batch and
-   // k_ru_continue, so that the device repeats the batch until the state
-   // halts with no host round trip between batches. The state halts at the
-   // latest kRuForceEvery iterations after k_ru_set, within kCap bodies.
+   // The device repeats the batch and k_ru_continue until the state halts,
+   // with no host round trip between batches: the state halts at the latest
+   // kRuForceEvery iterations after k_ru_set, within kCap bodies. Otherwise
+   // the batch alone is relaunched by the host; where its capture fails too,
+   // the iterations are launched directly.
    const int32_t kCap = kRuForceEvery / kBatch + 2;
-   bool device_loop = false;
-   if (cudaGraphCreate(&graph, 0) == cudaSuccess) {
-      cudaGraphConditionalHandle loop{};
-      cudaGraphNodeParams np{};
-      np.type = cudaGraphNodeTypeConditional;
-      cudaGraphNode_t node = nullptr;
-      bool ok = cudaGraphConditionalHandleCreate(&loop, graph, 1, cudaGraphCondAssignDefault) == cudaSuccess;
-      if (ok) {
-         np.conditional.handle = loop;
-         np.conditional.type = cudaGraphCondTypeWhile;
-         np.conditional.size = 1;
-         ok = cudaGraphAddNode(&node, graph, nullptr, 0, &np) == cudaSuccess;
-      }
-      if (ok)
-         ok = cudaStreamBeginCaptureToGraph(cs, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
-                                            cudaStreamCaptureModeThreadLocal) == cudaSuccess;
-      if (ok) {
-         for (int k = 0; k < kBatch && status == TNLB_OK; k++) status = iteration(cs, k);
-         if (status == TNLB_OK) k_ru_continue<<<1, 32, 0, cs>>>(loop, S, kCap);
-         cudaGraph_t body = nullptr;
-         ok = cudaStreamEndCapture(cs, &body) == cudaSuccess && status == TNLB_OK &&
-              cudaGetLastError() == cudaSuccess && cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
-      }
-      if (!ok) {
-         cudaGetLastError();
-         if (exec) cudaGraphExecDestroy(exec);
-         cudaGraphDestroy(graph);
-         exec = nullptr;
-         graph = nullptr;
-      }
-      device_loop = ok;
-      status = TNLB_OK;  // a failed build falls back to the batch graph
-      clear_error();
-   }
-   else
-      cudaGetLastError();
-   // Otherwise a graph of the batch alone, relaunched by the host; where its
-   // capture fails too, the iterations are launched directly.
-   if (!device_loop) {
-      if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
-         for (int k = 0; k < kBatch && status == TNLB_OK; k++) status = iteration(cs, k);
-         cudaError_t e = cudaStreamEndCapture(cs, &graph);
-         if (e == cudaSuccess && status == TNLB_OK) e = cudaGraphInstantiate(&exec, graph, 0);
-         if (e != cudaSuccess) {
-            cudaGetLastError();
-            exec = nullptr;
-         }
-         status = TNLB_OK;
-         clear_error();
-      }
-      else
-         cudaGetLastError();
-   }
+   const bool device_loop = build_iteration_graph(
+      cs,
+      [&](cudaStream_t s) {
+         tnlb_status rc = TNLB_OK;
+         for (int k = 0; k < kBatch && rc == TNLB_OK; k++) rc = iteration(s, k);
+         return rc;
+      },
+      [&](cudaGraphConditionalHandle loop, cudaStream_t s) { k_ru_continue<<<1, 32, 0, s>>>(loop, S, kCap); },
+      &graph, &exec);
    struct GraphGuard {  // released after the stream has drained
       cudaStream_t s;
       cudaGraph_t g;
