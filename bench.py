@@ -17,13 +17,13 @@ e2e       -- the same metric through the public API with host buffers: each
              does across the products of a solver); the copies of
              neighbouring steps overlap the product on separate streams.
 roofline  -- achieved GB/s of the SpMV call against the measured HBM copy
-             bandwidth (MEASURED_PEAKS.json, else the pool's fallback).
+             bandwidth (MEASURED_PEAKS.json, else a fallback of 6650 GB/s).
 cpu_baseline -- the reference's own Host/OpenMP vectorProduct on the host
              cores (oracle/_ref, compiled from the reference's headers),
              else the oracle's C restatement; a bounded sample of repeated
              products of the same matrix.
 
-solver    -- BASELINE's second metric, PCG time to an FP64 true residual of
+solver    -- the solver metric, PCG time to an FP64 true residual of
              1e-8 on the learned-preconditioner evaluation problem (2D
              diffusion, 2048 x 2048, GRF coefficients): FP64 Jacobi-PCG
              against FP32 PCG with reliable FP64 updates and the learned
