@@ -356,7 +356,7 @@ def reference_c1_solves(maxit=20000):
     with Jacobi, GMRES(30) with ILU(0) in its MGSR and CWY variants; one JSON
     line each with the reference's own timing, iterations and the true
     residual.  Reported beside the library's GPU solves of the same problems
-    (`python -m tnl_b200.benchmarks c1-solvers`)."""
+    (`python -m tnl_b200.benchmarks c1-solves`)."""
     from oracle.oracle import REF_SO, Oracle, Reference  # reference arm only
 
     if not REF_SO.exists():
