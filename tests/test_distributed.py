@@ -204,3 +204,61 @@ def test_distributed_cg_on_one_rank_matches_cg():
         assert t.true_residual(M, b, x) < 1e-7
     finally:
         dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [1, 2, 3, 5])
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_halo_plans_exchange_and_products_on_random_matrices(world, seed):
+    """Irregular matrices (random row lengths, columns anywhere, some rows
+    empty, padding -1 entries), all ranks' plans built in one process and
+    the all-to-all emulated: every rank's send lists are what the others
+    request, its received values are x at its ghosts in plan order, and its
+    local product over [x_local, x_ghost] equals the global product's rows;
+    padding stays -1 after the remap."""
+    import scipy.sparse as sp
+
+    from tnl_b200.distributed import HaloPlan, split_range
+
+    rng = np.random.default_rng(seed)
+    n = int(rng.integers(world, 300))
+    lens = rng.integers(0, 12, n)
+    lens[rng.random(n) < 0.1] = 0
+    rowptr = np.concatenate([[0], np.cumsum(lens)]).astype(np.int64)
+    cols = np.concatenate([np.sort(rng.choice(n, size=int(k), replace=False)) if k <= n else np.arange(n)
+                           for k in lens]).astype(np.int64) if rowptr[-1] else np.zeros(0, np.int64)
+    vals = rng.uniform(-1, 1, cols.size)
+    G = sp.csr_matrix((vals, cols, rowptr), shape=(n, n))
+    x = rng.uniform(-1, 1, n)
+    ranges = [split_range(n, r, world) for r in range(world)]
+    plans = []
+    for r, (b, e) in enumerate(ranges):
+        c = cols[rowptr[b]:rowptr[e]].copy()
+        pad = rng.random(c.size) < 0.05
+        c[pad] = -1
+        P = HaloPlan(c, r, ranges)
+        assert np.array_equal(P.local_cols[pad], np.full(int(pad.sum()), -1))
+        assert np.all(np.diff(P.ghosts) > 0)
+        assert not np.any((P.ghosts >= b) & (P.ghosts < e))
+        plans.append((P, c))
+    for r, (P, _) in enumerate(plans):
+        P.set_send_lists([plans[q][0].requests()[r] for q in range(world)])
+    for r, (P, c) in enumerate(plans):
+        b, e = ranges[r]
+        # what rank r receives from p: p's send buffer segment for r
+        recv = []
+        for p, (Q, _) in enumerate(plans):
+            o = int(Q.send_counts[:r].sum())
+            seg = Q.send_idx[o:o + int(Q.send_counts[r])] + ranges[p][0]
+            recv.append(x[seg])
+        recv = np.concatenate(recv) if recv else np.zeros(0)
+        assert np.array_equal(recv, x[P.ghosts])
+        xe = np.concatenate([x[b:e], recv])
+        keep = P.local_cols >= 0
+        rl = np.diff(rowptr[b:e + 1])
+        counts = np.array([keep[s:s + k].sum() for s, k in zip(rowptr[b:e] - rowptr[b], rl)], np.int64)
+        rp = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+        L = sp.csr_matrix((vals[rowptr[b]:rowptr[e]][keep], P.local_cols[keep], rp),
+                          shape=(e - b, P.n_local + P.n_ghost))
+        Gk = sp.csr_matrix((vals[rowptr[b]:rowptr[e]][keep], c[keep], rp), shape=(e - b, n))
+        assert np.allclose(L @ xe, Gk @ x, rtol=0, atol=1e-13)
+    assert sum(int(P.send_counts.sum()) for P, _ in plans) == sum(P.n_ghost for P, _ in plans)
