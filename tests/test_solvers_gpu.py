@@ -13,8 +13,6 @@ import numpy as np
 import pytest
 import torch
 
-from helpers import FORMATS
-
 pytestmark = pytest.mark.gpu
 
 

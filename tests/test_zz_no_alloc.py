@@ -3,8 +3,6 @@ against tnlb_spmv with the tile kernel on CSR segments: the same kernels and til
 the results must be bit-identical, on two calls in a row that reuse the
 scratch without any reset.  Collected last so that it also runs after every
 other GPU test in the same process."""
-import ctypes as C
-
 import numpy as np
 import pytest
 import scipy.sparse
